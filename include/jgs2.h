@@ -1,0 +1,312 @@
+/*
+ * jgs2.h — C-ABI of the B200 (sm_100a) JGS2 elastodynamics step.
+ *
+ * This header is the drop-in boundary for the per-frame simulation loop of
+ * CallumFerguson/webgpu-physics.  Every entry point replaces one public member
+ * of `class JGS2GpuSolver` (src/simulation/gpu/jgs2-solver.ts:905-3051); the
+ * citation beside each declaration names the member it stands in for.  The
+ * input record mirrors `interface JGS2GpuInput` (src/simulation/gpu/layout.ts:41-90)
+ * and the settings record mirrors `interface JGS2StepSettings`
+ * (src/simulation/gpu/jgs2-solver.ts:64-100).
+ *
+ * Conventions
+ *  - Plain pointers and sizes only.  Arrays use the reference's packing: vec4
+ *    per vertex (xyz + w), four u32 per tetrahedron, three padded vec4 columns
+ *    of inverse Dm per tetrahedron, row-major 3x3 cubature blocks.
+ *  - Every call returns a jgs2_status.  A non-OK status leaves a message that
+ *    jgs2_last_error() returns (per solver) or jgs2_global_last_error() returns
+ *    (for failures before a solver exists).  The reference throws RangeError /
+ *    TypeError / Error with the same conditions.
+ *  - One solver owns one CUDA stream and all of its device memory.  Calls on
+ *    one solver must come from one host thread at a time.
+ *  - Host output buffers are caller owned; the library copies inputs at
+ *    create time (the reference copies typed arrays into GPU buffers).
+ */
+#ifndef JGS2_H_
+#define JGS2_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define JGS2_ABI_VERSION 1u
+
+typedef enum jgs2_status {
+  JGS2_OK = 0,
+  JGS2_INVALID_ARGUMENT = 1,  /* RangeError / TypeError in the reference */
+  JGS2_INFEASIBLE_INPUT = 2,  /* initial pose fails the determinant / contact preflight */
+  JGS2_OUT_OF_MEMORY = 3,
+  JGS2_DEVICE_ERROR = 4,      /* CUDA runtime error; message carries the CUDA string */
+  JGS2_TIMEOUT = 5,           /* a bounded device wait gave up */
+  JGS2_DESTROYED = 6,         /* use after jgs2_destroy (reference: "has been destroyed") */
+  JGS2_UNSUPPORTED = 7,       /* feature not built into this library */
+  JGS2_NOT_READY = 8          /* diagnostics requested before any stable iteration */
+} jgs2_status;
+
+/* Material tags stored in tetMeta.w (src/simulation/gpu/layout.ts:29-30). */
+#define JGS2_MATERIAL_COROTATED_LINEAR 0u
+#define JGS2_MATERIAL_STABLE_NEO_HOOKEAN 1u
+
+/* Schedules (src/simulation/gpu/jgs2-solver.ts:62). */
+#define JGS2_SCHEDULE_JACOBI 0u
+#define JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL 1u
+
+/* Limits (src/simulation/gpu/jgs2-solver.ts:145,154,255;
+ * src/simulation/gpu/jgs2-globalization.ts:2). */
+#define JGS2_MAX_BATCH_FRAMES 240u
+#define JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION 2048u
+#define JGS2_MAX_SCHEDULE_COLORS 256u
+#define JGS2_HISTORY_CAPACITY 64u
+
+/* Record widths in floats (src/simulation/gpu/jgs2-globalization.ts:5-15). */
+#define JGS2_LOCAL_DIAGNOSTIC_FLOATS 16u
+#define JGS2_HISTORY_RECORD_FLOATS 32u
+#define JGS2_CONTROL_RECORD_FLOATS 16u
+
+/*
+ * Input record: JGS2GpuInput (src/simulation/gpu/layout.ts:41-90).
+ * Optional arrays may be NULL.  tet_rest_stiffness may be NULL when every
+ * tetrahedron is stable Neo-Hookean (the stable path never reads it).
+ */
+typedef struct jgs2_input {
+  uint32_t vertex_count;
+  uint32_t tet_count;
+  uint32_t cubature_k;
+  uint32_t reserved0;
+  const float* positions;          /* 4 * V; w is normalised to one */
+  const float* velocities;         /* 4 * V or NULL */
+  const float* vertex_rest;        /* 4 * V: rest / pin target xyz, mass w */
+  const float* vertex_colors;      /* 4 * V or NULL (render colour, unused by the step) */
+  const uint32_t* vertex_info;     /* 4 * V: adjacency start, count, pinned, body */
+  const float* external_forces;    /* 3 * V or NULL (objectives.externalForces) */
+  const float* target_positions;   /* 3 * V or NULL (objectives.targetPositions) */
+  const float* target_stiffnesses; /* V or NULL (objectives.targetStiffnesses) */
+  const uint32_t* tet_indices;     /* 4 * T */
+  const float* tet_inverse_dm;     /* 12 * T, three padded columns */
+  const float* tet_meta;           /* 4 * T: volume, lambda, mu, model tag */
+  const float* tet_rest_stiffness; /* 144 * T row-major, or NULL when all stable */
+  const uint32_t* adjacency;       /* CSR payload of incident tetrahedra */
+  uint64_t adjacency_length;
+  const uint32_t* cubature_tet_ids;  /* V * K; 0xffffffff = empty slot */
+  const float* cubature_weights;     /* V * K */
+  const float* cubature_basis;       /* V * K * 36: four row-major Ubar blocks */
+} jgs2_input;
+
+/*
+ * Step settings: JGS2StepSettings (src/simulation/gpu/jgs2-solver.ts:64-100),
+ * defaults DEFAULT_JGS2_STEP_SETTINGS (:164-187).
+ */
+typedef struct jgs2_settings {
+  uint32_t schedule;               /* JGS2_SCHEDULE_* */
+  uint32_t iterations;
+  float timestep;
+  float gravity[3];
+  float floor_height;
+  float floor_stiffness;
+  float velocity_damping;
+  float regularization;
+  float rotation_epsilon;
+  float max_step;
+  float residual_tolerance;
+  float normalized_update_tolerance;
+  float contact_tangential_damping;
+  float contact_margin;
+  float ipc_activation_distance;
+  float ipc_minimum_distance;
+  float ipc_barrier_stiffness;
+  float ipc_friction_coefficient;
+  float ipc_friction_velocity_epsilon;
+  float ipc_step_safety;
+  uint32_t horizontal_body_correction;
+  uint32_t parity_mode;
+} jgs2_settings;
+
+/* Bits of the override mask: set bit i to take field i from an override
+ * record (the reference's Partial<JGS2StepSettings>). */
+enum {
+  JGS2_SET_SCHEDULE = 1u << 0,
+  JGS2_SET_ITERATIONS = 1u << 1,
+  JGS2_SET_TIMESTEP = 1u << 2,
+  JGS2_SET_GRAVITY = 1u << 3,
+  JGS2_SET_FLOOR_HEIGHT = 1u << 4,
+  JGS2_SET_FLOOR_STIFFNESS = 1u << 5,
+  JGS2_SET_VELOCITY_DAMPING = 1u << 6,
+  JGS2_SET_REGULARIZATION = 1u << 7,
+  JGS2_SET_ROTATION_EPSILON = 1u << 8,
+  JGS2_SET_MAX_STEP = 1u << 9,
+  JGS2_SET_RESIDUAL_TOLERANCE = 1u << 10,
+  JGS2_SET_NORMALIZED_UPDATE_TOLERANCE = 1u << 11,
+  JGS2_SET_CONTACT_TANGENTIAL_DAMPING = 1u << 12,
+  JGS2_SET_CONTACT_MARGIN = 1u << 13,
+  JGS2_SET_IPC_ACTIVATION_DISTANCE = 1u << 14,
+  JGS2_SET_IPC_MINIMUM_DISTANCE = 1u << 15,
+  JGS2_SET_IPC_BARRIER_STIFFNESS = 1u << 16,
+  JGS2_SET_IPC_FRICTION_COEFFICIENT = 1u << 17,
+  JGS2_SET_IPC_FRICTION_VELOCITY_EPSILON = 1u << 18,
+  JGS2_SET_IPC_STEP_SAFETY = 1u << 19,
+  JGS2_SET_HORIZONTAL_BODY_CORRECTION = 1u << 20,
+  JGS2_SET_PARITY_MODE = 1u << 21,
+  JGS2_SET_ALL = (1u << 22) - 1u
+};
+
+typedef struct jgs2_solver jgs2_solver;
+
+/* Solver shape and activity, the reference's readonly members and getters
+ * (src/simulation/gpu/jgs2-solver.ts:905-969, 1504-1575). */
+typedef struct jgs2_info {
+  uint32_t vertex_count;
+  uint32_t tet_count;
+  uint32_t cubature_k;
+  uint32_t body_count;
+  uint32_t schedule_color_count;
+  uint32_t globalization_enabled;  /* 1 for the stable Neo-Hookean path */
+  uint32_t objective_flags;        /* bit0 forces, bit1 targets */
+  uint32_t external_force_vertex_count;
+  uint32_t quadratic_target_vertex_count;
+  uint32_t objective_revision;
+  uint32_t last_submitted_iterations;
+  uint32_t history_count;          /* executed records of the last frame */
+  float scene_scale;               /* initial dynamic AABB diagonal */
+  float preprocessing_timestep;
+  uint32_t current_position_buffer;/* 0 = A, reported for zero-copy consumers */
+  uint32_t reserved;
+} jgs2_info;
+
+/* ---- library ---------------------------------------------------------- */
+
+/* ABI version and build string. */
+uint32_t jgs2_version(void);
+const char* jgs2_build_string(void);
+/* Message of the last failure that happened without a solver (create). */
+const char* jgs2_global_last_error(void);
+
+/* DEFAULT_JGS2_STEP_SETTINGS (src/simulation/gpu/jgs2-solver.ts:164-187). */
+void jgs2_default_settings(jgs2_settings* out);
+
+/* resolveJGS2StepSettings + validateStepSettings
+ * (src/simulation/gpu/jgs2-solver.ts:429-550): merge, apply parity, validate. */
+jgs2_status jgs2_resolve_settings(const jgs2_settings* defaults,
+                                  const jgs2_settings* overrides,
+                                  uint32_t override_mask, jgs2_settings* out);
+
+/* validateJGS2GpuInput (src/simulation/gpu/layout.ts:223-416). */
+jgs2_status jgs2_validate_input(const jgs2_input* input);
+
+/* buildJGS2InputVertexColoring + buildGreedyVertexColoring
+ * (src/simulation/gpu/jgs2-solver.ts:308-367;
+ *  src/simulation/cpu/vertex-coloring.ts:20-110).  colors has V entries. */
+jgs2_status jgs2_build_vertex_coloring(const jgs2_input* input,
+                                       uint32_t* colors,
+                                       uint32_t* color_count);
+
+/* ---- lifetime --------------------------------------------------------- */
+
+/* static JGS2GpuSolver.create(device, input, settings)
+ * (src/simulation/gpu/jgs2-solver.ts:971-1502).  device is a CUDA ordinal. */
+jgs2_status jgs2_create(const jgs2_input* input, const jgs2_settings* settings,
+                        uint32_t settings_mask, int device, jgs2_solver** out);
+
+/* destroy() (src/simulation/gpu/jgs2-solver.ts:3029-3044); idempotent, NULL ok. */
+void jgs2_destroy(jgs2_solver* solver);
+
+/* Message of this solver's last failure. */
+const char* jgs2_last_error(const jgs2_solver* solver);
+
+/* Shape / activity getters. */
+jgs2_status jgs2_get_info(jgs2_solver* solver, jgs2_info* out);
+
+/* Settings getters: defaultStepSettings / lastSubmittedSettings (:1550-1556). */
+jgs2_status jgs2_get_default_settings(jgs2_solver* solver, jgs2_settings* out);
+jgs2_status jgs2_get_last_submitted_settings(jgs2_solver* solver,
+                                             jgs2_settings* out);
+
+/* ---- stepping (all asynchronous on the solver stream) ----------------- */
+
+/* step(overrides) (src/simulation/gpu/jgs2-solver.ts:1767-1782): odd
+ * iteration normalisation and the convergence stop latch. */
+jgs2_status jgs2_step(jgs2_solver* solver, const jgs2_settings* overrides,
+                      uint32_t override_mask);
+
+/* stepFrames(n, overrides) (:1791-1810). */
+jgs2_status jgs2_step_frames(jgs2_solver* solver, uint32_t frame_count,
+                             const jgs2_settings* overrides,
+                             uint32_t override_mask);
+
+/* stepExactIterations(iterations, overrides) (:1817-1835). */
+jgs2_status jgs2_step_exact_iterations(jgs2_solver* solver, uint32_t iterations,
+                                       const jgs2_settings* overrides,
+                                       uint32_t override_mask);
+
+/* stepFramesExactIterations(n, iterations, overrides) (:1842-1862). */
+jgs2_status jgs2_step_frames_exact_iterations(jgs2_solver* solver,
+                                              uint32_t frame_count,
+                                              uint32_t iterations,
+                                              const jgs2_settings* overrides,
+                                              uint32_t override_mask);
+
+/* awaitIdle() (:2496-2499). */
+jgs2_status jgs2_sync(jgs2_solver* solver);
+
+/* ---- objectives -------------------------------------------------------- */
+
+/* setExternalForce (:1576-1611). */
+jgs2_status jgs2_set_external_force(jgs2_solver* solver, uint32_t vertex,
+                                    const float force[3]);
+/* replaceExternalForces (:1614-1642); forces has 3 * V floats. */
+jgs2_status jgs2_replace_external_forces(jgs2_solver* solver,
+                                         const float* forces);
+/* clearExternalForces (:1644-1646). */
+jgs2_status jgs2_clear_external_forces(jgs2_solver* solver);
+/* setQuadraticTarget (:1649-1688). */
+jgs2_status jgs2_set_quadratic_target(jgs2_solver* solver, uint32_t vertex,
+                                      const float target[3], float stiffness);
+/* replaceQuadraticTargets (:1691-1733). */
+jgs2_status jgs2_replace_quadratic_targets(jgs2_solver* solver,
+                                           const float* target_positions,
+                                           const float* target_stiffnesses);
+/* releaseQuadraticTarget (:1736-1750). */
+jgs2_status jgs2_release_quadratic_target(jgs2_solver* solver, uint32_t vertex);
+/* releaseAllQuadraticTargets (:1753-1760). */
+jgs2_status jgs2_release_all_quadratic_targets(jgs2_solver* solver);
+
+/* ---- reads (synchronous: they wait for the solver stream) -------------- */
+
+/* readPositions (:2501-2508); out has 4 * V floats. */
+jgs2_status jgs2_read_positions(jgs2_solver* solver, float* out, size_t floats);
+/* readVelocities (:2510-2518). */
+jgs2_status jgs2_read_velocities(jgs2_solver* solver, float* out, size_t floats);
+/* readPredictedPositions (:2520-2528). */
+jgs2_status jgs2_read_predicted_positions(jgs2_solver* solver, float* out,
+                                          size_t floats);
+/* readFinalIterationUpdates (:2535-2543). */
+jgs2_status jgs2_read_final_iteration_updates(jgs2_solver* solver, float* out,
+                                              size_t floats);
+/* readVertexRotations (:2863-2870); 12 * V floats (three padded columns). */
+jgs2_status jgs2_read_vertex_rotations(jgs2_solver* solver, float* out,
+                                       size_t floats);
+/* readGlobalizationDiagnostics (:2548-2604).  local: 16 * V floats (may be
+ * NULL), control: 16 floats (may be NULL), history: 32 * 64 floats (may be
+ * NULL).  *history_count receives the executed record count. */
+jgs2_status jgs2_read_globalization(jgs2_solver* solver, float* local,
+                                    size_t local_floats, float* control,
+                                    float* history, size_t history_floats,
+                                    uint32_t* history_count);
+
+/* Zero-copy consumers (the reference's currentPositionBuffer, :1504-1507):
+ * device address of the canonical vec4 position array and the solver's
+ * cudaStream_t.  Valid until jgs2_destroy. */
+jgs2_status jgs2_device_positions(jgs2_solver* solver, void** device_ptr,
+                                  void** cuda_stream);
+
+/* Device kernels launched by this solver since creation (every launch the
+ * library issues is counted, including graph replays). */
+uint64_t jgs2_kernel_launch_count(const jgs2_solver* solver);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JGS2_H_ */

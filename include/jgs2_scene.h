@@ -1,0 +1,143 @@
+/*
+ * jgs2_scene.h — C-ABI of the host-side scene builder and JGS2 precompute
+ * that produce a jgs2_input for the step.
+ *
+ * The reference builds scenes in TypeScript: procedural tetrahedral meshes
+ * (src/simulation/cpu/mesh.ts:101-201), FEM rest data and lumped masses
+ * (src/simulation/cpu/fem.ts:70-335), the exact full-coordinate JGS2 bases
+ * (src/simulation/cpu/precompute.ts:141-206), the nonlinear cubature pose
+ * corpus and training (src/simulation/cpu/nonlinear-cubature.ts:452-620;
+ * src/simulation/cpu/nonlinear-cubature-training.ts:689-843) and the GPU
+ * packer toJGS2GpuInput (src/scenes/index.ts:975-1114).  This library restates
+ * that pipeline in C++ (double precision, OpenMP over source vertices).
+ *
+ * Two precompute methods:
+ *  - JGS2_PRECOMPUTE_EXACT: the reference's method on the whole mesh (dense
+ *    rest Hessian + Cholesky, global low-frequency pose corpus, candidate
+ *    tetrahedra = all tetrahedra).  Cost grows as O(n^3); meant for meshes of a
+ *    few thousand vertices.
+ *  - JGS2_PRECOMPUTE_PATCH: the same algorithm applied to a local patch around
+ *    each source vertex (free vertices within `patch_radius` graph rings,
+ *    everything beyond held fixed, candidate tetrahedra = tetrahedra incident
+ *    to the free vertices).  Patches with identical rest geometry, topology,
+ *    material, masses and pin flags share one training result, so regular
+ *    grids precompute in seconds at millions of vertices.
+ */
+#ifndef JGS2_SCENE_H_
+#define JGS2_SCENE_H_
+
+#include "jgs2.h"
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef struct jgs2_scene jgs2_scene;
+
+#define JGS2_PRECOMPUTE_EXACT 0u
+#define JGS2_PRECOMPUTE_PATCH 1u
+
+/* Face bits for generated cuboids: a vertex is pinned when it lies on any
+ * selected face (the reference passes a predicate, src/simulation/cpu/mesh.ts:142). */
+#define JGS2_FACE_X_MIN (1u << 0)
+#define JGS2_FACE_X_MAX (1u << 1)
+#define JGS2_FACE_Y_MIN (1u << 2)
+#define JGS2_FACE_Y_MAX (1u << 3)
+#define JGS2_FACE_Z_MIN (1u << 4)
+#define JGS2_FACE_Z_MAX (1u << 5)
+
+typedef struct jgs2_precompute_options {
+  double timestep;          /* the step's timestep; bases include M / h^2 */
+  uint32_t cubature_k;      /* settings.cubatureSamples (6 in every reference scene) */
+  uint32_t method;          /* JGS2_PRECOMPUTE_* */
+  uint32_t patch_radius;    /* free rings around the source vertex (patch method) */
+  uint32_t threads;         /* 0 = all hardware threads */
+  uint32_t mode_count;      /* training modes, 8 (nonlinear-cubature.ts:13) */
+  uint32_t inverse_iterations; /* 24 (nonlinear-cubature.ts:15) */
+  double training_amplitude;   /* 0.12 (nonlinear-cubature.ts:16) */
+  uint32_t refinement_passes;  /* 12 (nonlinear-cubature-training.ts:737) */
+  /* Nonzero: skip training and write the exact complement instead — one
+   * weight-1 record per candidate tetrahedron (the "exact-all remainder" of
+   * assembleStableNeoHookeanJGS2LocalSystem, nonlinear-cubature-training.ts:
+   * 620-660).  cubature_k must then be at least the candidate count. */
+  uint32_t exact_complement;
+} jgs2_precompute_options;
+
+typedef struct jgs2_precompute_stats {
+  uint32_t source_vertices;    /* active vertices that received records */
+  uint32_t training_classes;   /* distinct trainings run (patch caching) */
+  uint32_t records_written;    /* positive-weight records */
+  uint32_t max_records_per_vertex;
+  double max_residual;         /* max normalized training residual (f64) */
+  double mean_residual;
+  uint32_t vertices_over_tolerance; /* residual > 1% */
+  uint32_t reduced_amplitude_classes; /* corpora whose amplitude was halved */
+  double seconds;
+} jgs2_precompute_stats;
+
+jgs2_scene* jgs2_scene_new(void);
+void jgs2_scene_destroy(jgs2_scene* scene);
+const char* jgs2_scene_last_error(const jgs2_scene* scene);
+
+/* Defaults of jgs2_precompute_options. */
+void jgs2_default_precompute_options(jgs2_precompute_options* out);
+
+/* LinearMaterial (src/simulation/cpu/types.ts) with its model tag.  Returns the
+ * material id (>= 0) or -1. */
+int32_t jgs2_scene_add_material(jgs2_scene* scene, double density,
+                                double young_modulus, double poisson_ratio,
+                                uint32_t model);
+
+/* generateRegularCuboidMesh (src/simulation/cpu/mesh.ts:101-201) appended as
+ * one body.  Returns the first vertex id of the new body or -1. */
+int64_t jgs2_scene_add_cuboid(jgs2_scene* scene, const uint32_t cells[3],
+                              const double origin[3], const double size[3],
+                              uint32_t material, uint32_t body,
+                              uint32_t pinned_faces);
+
+/* Generic tetrahedral body (appendTetrahedralMeshes, mesh.ts:254-301).
+ * tet_materials may be NULL (all `material`). pinned may be NULL. */
+int64_t jgs2_scene_add_mesh(jgs2_scene* scene, uint32_t vertex_count,
+                            const double* positions, uint32_t tet_count,
+                            const uint32_t* tets, const uint32_t* tet_materials,
+                            uint32_t material, const uint8_t* pinned,
+                            uint32_t body);
+
+/* Replace the pin flags of every vertex (V bytes, nonzero = pinned); the
+ * reference's cuboid generator takes an arbitrary predicate (mesh.ts:142). */
+jgs2_status jgs2_scene_set_pinned(jgs2_scene* scene, const uint8_t* pinned);
+
+uint32_t jgs2_scene_vertex_count(const jgs2_scene* scene);
+uint32_t jgs2_scene_tet_count(const jgs2_scene* scene);
+/* Rest positions (3 * V doubles). */
+jgs2_status jgs2_scene_rest_positions(const jgs2_scene* scene, double* out);
+
+/* Run the precompute.  options may be NULL for defaults. */
+jgs2_status jgs2_scene_precompute(jgs2_scene* scene,
+                                  const jgs2_precompute_options* options,
+                                  jgs2_precompute_stats* stats);
+
+/* Initial pose (4 * V floats, xyz used) and optional velocities (4 * V).
+ * With pin_at_initial != 0 the pin targets (vertex_rest.xyz of pinned
+ * vertices) are set to the initial positions instead of the rest positions. */
+jgs2_status jgs2_scene_set_initial_state(jgs2_scene* scene,
+                                         const float* positions,
+                                         const float* velocities,
+                                         uint32_t pin_at_initial);
+
+/* Objectives packed into the input (objectives.*, layout.ts:32-39). */
+jgs2_status jgs2_scene_set_objectives(jgs2_scene* scene,
+                                      const float* external_forces,
+                                      const float* target_positions,
+                                      const float* target_stiffnesses);
+
+/* packJGS2GpuInput (src/scenes/index.ts:975-1109): fill `out` with pointers
+ * into arrays owned by the scene (valid until the next mutating call or
+ * jgs2_scene_destroy).  Requires a finished precompute. */
+jgs2_status jgs2_scene_pack(jgs2_scene* scene, jgs2_input* out);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* JGS2_SCENE_H_ */

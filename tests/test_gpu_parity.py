@@ -1,0 +1,175 @@
+"""GPU parity: the sm_100a step through the C-ABI against the CPU oracle.
+
+Tolerances follow the reference's parity bar: positions and velocities within
+1e-4 of the scene bounding-box diagonal after N frames (the relative error is
+reported per test), per-iteration history records within f32 tolerance, and
+acceptance decisions equal.
+"""
+import numpy as np
+import pytest
+
+from jgs2_b200 import scenes, solver
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+POSITION_TOL = 1e-4  # of the bounding-box diagonal
+
+
+def _settings(**kw):
+    base = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=10)
+    base.update(kw)
+    return base
+
+
+def _camel(s):
+    inv = {v: k for k, v in solver.CAMEL.items()}
+    return {inv.get(k, k): (bool(v) if k in ("parity_mode", "horizontal_body_correction") else v)
+            for k, v in s.items()}
+
+
+def _pair(inp, **kw):
+    s = _settings(**kw)
+    gpu = solver.JGS2GpuSolver.create(inp, _camel(s))
+    cpu = O.OracleSolver(inp, s, precision=32)
+    return gpu, cpu
+
+
+def _bar(cells=(10, 2, 2), size=(0.5, 0.1, 0.1), young=1e5, exact=False, k=6):
+    sc = scenes.Scene()
+    m = sc.add_material(1000.0, young, 0.4)
+    sc.add_cuboid(cells, (0.0, 0.0, 0.0), size, m, 0, scenes.FACE_X_MIN)
+    kk = sc.tet_count if exact else k
+    sc.precompute(timestep=1 / 60, cubature_k=kk, exact_complement=1 if exact else 0)
+    return sc.pack()
+
+
+def _compare(inp, gpu, cpu, tol=POSITION_TOL):
+    diag = inp.bbox_diagonal()
+    g = gpu.readPositions().reshape(-1, 4)[:, :3]
+    c = cpu.read("positions").reshape(-1, 4)[:, :3]
+    pe = float(np.abs(g - c).max()) / diag
+    gv = gpu.readVelocities().reshape(-1, 4)[:, :3]
+    cv = cpu.read("velocities").reshape(-1, 4)[:, :3]
+    ve = float(np.abs(gv - cv).max()) * (1 / 60) / diag
+    assert pe <= tol, f"position error {pe:.3e} of bbox diagonal"
+    assert ve <= tol, f"velocity error (x dt) {ve:.3e} of bbox diagonal"
+    return pe, ve
+
+
+def test_exact_complement_trajectory_jacobi():
+    inp = _bar(exact=True)
+    gpu, cpu = _pair(inp)
+    for frame in range(30):
+        gpu.stepExactIterations(10)
+        cpu.step_exact_iterations(10)
+    _compare(inp, gpu, cpu)
+    d = gpu.readGlobalizationDiagnostics()
+    h = cpu.read("history").reshape(64, 32)
+    assert d["historyCount"] == 10
+    np.testing.assert_array_equal(d["history"][:, 4], h[:10, 4])  # accepted flags
+    # relative residual curve tracks the oracle
+    np.testing.assert_allclose(d["history"][:, 19], h[:10, 19], rtol=5e-2, atol=1e-6)
+
+
+def test_cubature_first_frame_jacobi():
+    # Six trained cubature records per vertex make this bar's Jacobi iteration
+    # expansive: the oracle's own f32 and f64 runs part after a few frames, so
+    # only the first frame is a meaningful f32 comparison.
+    inp = _bar()
+    gpu, cpu = _pair(inp)
+    gpu.stepExactIterations(10)
+    cpu.step_exact_iterations(10)
+    _compare(inp, gpu, cpu, tol=1e-5)
+    np.testing.assert_array_equal(gpu.readGlobalizationDiagnostics()["history"][:, 4],
+                                  cpu.read("history").reshape(64, 32)[:10, 4])
+
+
+def test_ggs2_trajectory():
+    inp = _bar(exact=True)
+    gpu, cpu = _pair(inp, schedule=1)
+    assert gpu.scheduleColorCount == cpu.color_count
+    for frame in range(10):
+        gpu.stepExactIterations(6)
+        cpu.step_exact_iterations(6)
+    _compare(inp, gpu, cpu)
+
+
+def test_ggs2_cubature_first_frame():
+    inp = _bar()
+    gpu, cpu = _pair(inp, schedule=1)
+    gpu.stepExactIterations(6)
+    cpu.step_exact_iterations(6)
+    _compare(inp, gpu, cpu, tol=1e-5)
+
+
+def test_cantilever_config0_frames():
+    # The 525-vertex cantilever with K = 6 trained records reaches a whole-pose
+    # revert within a few frames in the reference algorithm; the f32 oracle
+    # and f64 oracle agree to ~1e-6 of the diagonal over 60 frames.
+    inp = scenes.cantilever()
+    gpu, cpu = _pair(inp)
+    for frame in range(30):
+        gpu.stepExactIterations(10)
+        cpu.step_exact_iterations(10)
+    _compare(inp, gpu, cpu)
+
+
+def test_objectives_force_and_target():
+    inp = _bar(exact=True)
+    gpu, cpu = _pair(inp)
+    V = inp.vertex_count
+    forces = np.zeros(3 * V, dtype=np.float32)
+    pin = inp.vertex_info.reshape(-1, 4)[:, 2]
+    free = np.nonzero(pin == 0)[0]
+    forces[3 * free[-1] + 0] = 2.0
+    targets = inp.positions.reshape(-1, 4)[:, :3].copy().reshape(-1)
+    stiff = np.zeros(V, dtype=np.float32)
+    stiff[free[-2]] = 500.0
+    targets[3 * free[-2] + 1] += 0.05
+    gpu.replaceExternalForces(forces)
+    gpu.replaceQuadraticTargets(targets, stiff)
+    cpu.set_objectives(forces, targets, stiff)
+    assert gpu.objectiveActivity["flags"] == 3
+    for frame in range(10):
+        gpu.stepExactIterations(8)
+        cpu.step_exact_iterations(8)
+    _compare(inp, gpu, cpu)
+
+
+def test_production_step_latch_matches():
+    inp = _bar(exact=True)
+    s = _settings(iterations=9)
+    s["parity_mode"] = 1
+    gpu = solver.JGS2GpuSolver.create(inp, _camel(s))
+    cpu = O.OracleSolver(inp, s, precision=32)
+    for frame in range(15):
+        gpu.step()
+        cpu.step()
+    _compare(inp, gpu, cpu)
+    d = gpu.readGlobalizationDiagnostics()
+    h = cpu.read("control")
+    assert d["historyCount"] == int(h[7])
+
+
+def test_deterministic_replay():
+    inp = _bar()
+    a, _ = _pair(inp)
+    b, _ = _pair(inp)
+    for _i in range(5):
+        a.stepExactIterations(10)
+        b.stepExactIterations(10)
+    np.testing.assert_array_equal(a.readPositions(), b.readPositions())
+    np.testing.assert_array_equal(a.readGlobalizationDiagnostics()["history"],
+                                  b.readGlobalizationDiagnostics()["history"])
+
+
+def test_local_diagnostics_status_match():
+    inp = _bar(exact=True)
+    gpu, cpu = _pair(inp)
+    gpu.stepExactIterations(3)
+    cpu.step_exact_iterations(3)
+    gl = gpu.readGlobalizationDiagnostics()["local"]
+    cl = cpu.read("local").reshape(-1, 16)
+    np.testing.assert_array_equal(gl[:, 15], cl[:, 15])  # status per vertex
+    np.testing.assert_allclose(gl[:, 0:3], cl[:, 0:3], rtol=1e-2, atol=1e-6)  # Newton direction

@@ -1,0 +1,1088 @@
+// JGS2 step kernels for sm_100a.
+//
+// One frame of the stable Neo-Hookean Jacobi schedule runs as
+//   prologue            predict + iteration-0 vertex frames + source preflight
+//   per iteration:
+//     solve             warp-cooperative per-vertex JGS2 local solve
+//     gate              assembled determinant / energy reduction + accept
+//     convergence       whole-pose revert, five-component residual, history,
+//                       and the next iteration's vertex frames
+//   epilogue            canonical copy, optional body correction, finalize
+// which covers the reference's predict, tetPolarRotation, vertexPolarRotation,
+// jgs2Solve, assembledVertexEnergy, candidateTetrahedron, reduceCandidate,
+// applyCandidate, convergenceGradient, reduceConvergence, copyPosition,
+// bodyHorizontalCorrection and finalize entry points
+// (src/simulation/gpu/jgs2-shader.ts:2660-4589).  The graph-coloured schedule
+// adds a copy and, per colour, a frame pass over the vertices that colour
+// reads plus an in-place solve over the colour's vertices.
+//
+// Grid-wide reductions finish in the last block to arrive (a ticket counter);
+// sums are combined in block order so results are deterministic.  No kernel
+// waits on another block.
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "jgs2_device.cuh"
+#include "jgs2_kernels.cuh"
+
+namespace jgs2 {
+namespace {
+
+constexpr int kBlock = 128;
+constexpr int kGroup = 8;  // lanes per vertex in the solve kernel
+constexpr int kRecFloats = 56;  // cached cubature record state
+
+struct TetRec {
+  float3 g1, g2, g3;
+  float vol, lambda, mu;
+  uint4 idx;
+};
+
+__device__ __forceinline__ TetRec loadTet(const float4* __restrict__ tets, uint32_t t) {
+  const float4 a = __ldg(&tets[4ull * t]);
+  const float4 b = __ldg(&tets[4ull * t + 1]);
+  const float4 c = __ldg(&tets[4ull * t + 2]);
+  const uint4 q = __ldg(reinterpret_cast<const uint4*>(tets) + 4ull * t + 3);
+  TetRec r;
+  r.g1 = f3(a.x, a.y, a.z);
+  r.g2 = f3(b.x, b.y, b.z);
+  r.g3 = f3(c.x, c.y, c.z);
+  r.vol = a.w;
+  r.lambda = b.w;
+  r.mu = c.w;
+  r.idx = q;
+  return r;
+}
+
+__device__ __forceinline__ float3 shapeGradient(const TetRec& r, uint32_t slot) {
+  if (slot == 1) return r.g1;
+  if (slot == 2) return r.g2;
+  if (slot == 3) return r.g3;
+  return -(r.g1 + r.g2 + r.g3);
+}
+
+__device__ __forceinline__ uint32_t idxAt(const uint4& q, uint32_t l) {
+  return l == 0 ? q.x : (l == 1 ? q.y : (l == 2 ? q.z : q.w));
+}
+
+__device__ __forceinline__ M3 deformation(const TetRec& r, float3 x0, float3 x1, float3 x2, float3 x3) {
+  return outer(x1 - x0, r.g1) + outer(x2 - x0, r.g2) + outer(x3 - x0, r.g3);
+}
+
+__device__ __forceinline__ M3 deformationAt(const TetRec& r, const float4* __restrict__ x) {
+  return deformation(r, xyz(x[r.idx.x]), xyz(x[r.idx.y]), xyz(x[r.idx.z]), xyz(x[r.idx.w]));
+}
+
+__device__ __forceinline__ M3 loadRot(const float4* __restrict__ rot, uint32_t v) {
+  const float4 a = rot[3ull * v], b = rot[3ull * v + 1], c = rot[3ull * v + 2];
+  return {f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z)};
+}
+
+__device__ __forceinline__ void storeRot(float4* __restrict__ rot, uint32_t v, const M3& m) {
+  rot[3ull * v] = make_float4(m.c0.x, m.c0.y, m.c0.z, 0.f);
+  rot[3ull * v + 1] = make_float4(m.c1.x, m.c1.y, m.c1.z, 0.f);
+  rot[3ull * v + 2] = make_float4(m.c2.x, m.c2.y, m.c2.z, 0.f);
+}
+
+// Row-major stored Ubar block -> columns (cubatureBlock, jgs2-shader.ts:1204-1212).
+__device__ __forceinline__ M3 loadBlock(const float* __restrict__ b) {
+  return {f3(b[0], b[3], b[6]), f3(b[1], b[4], b[7]), f3(b[2], b[5], b[8])};
+}
+
+// Order-preserving encodings so atomicMin/atomicMax on uint give float min/max.
+__device__ __forceinline__ uint32_t orderedEncode(float f) {
+  const uint32_t u = __float_as_uint(f);
+  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
+}
+__device__ __forceinline__ float orderedDecode(uint32_t u) {
+  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
+}
+
+__device__ __forceinline__ uint32_t controlBits(float packed) {
+  if (!finiteS(packed) || packed < 0.0f || packed > float(kControlMask) || packed != floorf(packed)) return 0u;
+  return static_cast<uint32_t>(packed);
+}
+
+__device__ __forceinline__ bool latched(const DevParams& p, const FrameState* fs) {
+  if (!p.stopEnabled) return false;
+  return (controlBits(fs->control[0].w) & kStopLatchBit) != 0u;
+}
+
+__device__ __forceinline__ bool finiteNonnegInt(float v, float maximum) {
+  return finiteS(v) && v >= 0.0f && v <= maximum && v == floorf(v);
+}
+
+__device__ __forceinline__ bool isPinned(const uint4& info) { return info.z != 0u; }
+
+__device__ __forceinline__ float distributedInertiaWeight(const float4& rm, const uint4& info, float invDt2) {
+  if (isPinned(info)) return 0.0f;
+  return rm.w * invDt2 / float(info.y > 1u ? info.y : 1u);
+}
+
+// vertexObjectiveGradient (jgs2-shader.ts:1926-1938).
+__device__ __forceinline__ float3 objectiveGradient(const DevParams& p, const float4* __restrict__ obj, uint32_t v,
+                                                    float3 pos) {
+  float3 r = f3(0, 0, 0);
+  if (p.objectiveFlags & 1u) r = r - xyz(obj[2ull * v]);
+  if (p.objectiveFlags & 2u) {
+    const float4 t = obj[2ull * v + 1];
+    if (t.w > 0.0f) r = r + t.w * (pos - xyz(t));
+  }
+  return r;
+}
+
+__device__ __forceinline__ float targetStiffness(const DevParams& p, const float4* __restrict__ obj, uint32_t v) {
+  return (p.objectiveFlags & 2u) ? obj[2ull * v + 1].w : 0.0f;
+}
+
+// vertexObjectiveEnergyDelta (jgs2-shader.ts:1903-1924).
+__device__ __forceinline__ float objectiveDelta(const DevParams& p, const float4* __restrict__ obj, uint32_t v,
+                                                float3 base, float3 d) {
+  float r = 0.0f;
+  if (p.objectiveFlags & 1u) r -= dot3(xyz(obj[2ull * v]), d);
+  if (p.objectiveFlags & 2u) {
+    const float4 t = obj[2ull * v + 1];
+    if (t.w > 0.0f) r += t.w * (dot3(base - xyz(t), d) + 0.5f * dot3(d, d));
+  }
+  return r;
+}
+
+__device__ __forceinline__ float floorDelta(const DevParams& p, float baseY, float dY) {
+  if (!(p.floorStiffness > 0.0f)) return 0.0f;
+  const float i = fminf(0.0f, baseY - p.floorHeight);
+  const float f = fminf(0.0f, baseY + dY - p.floorHeight);
+  return 0.5f * p.floorStiffness * (f - i) * (f + i);
+}
+
+// vertexImplicitEnergyAt without cloth/IPC terms (jgs2-shader.ts:2557-2645).
+__device__ __forceinline__ float implicitEnergy(const DevParams& p, const Buffers& b, uint32_t v, float3 x,
+                                                const uint4& info) {
+  if (isPinned(info)) return 0.0f;
+  const float4 rm = b.restMass[v];
+  const float3 r = x - xyz(b.predicted[v]);
+  float e = 0.5f * (rm.w * p.invDt2) * dot3(r, r);
+  if (p.objectiveFlags != 0u) {
+    if (p.objectiveFlags & 1u) e -= dot3(xyz(b.objectives[2ull * v]), x);
+    if (p.objectiveFlags & 2u) {
+      const float4 t = b.objectives[2ull * v + 1];
+      if (t.w > 0.0f) {
+        const float3 q = x - xyz(t);
+        e += 0.5f * t.w * dot3(q, q);
+      }
+    }
+  }
+  if (p.floorStiffness > 0.0f) {
+    const float pen = fminf(0.0f, x.y - p.floorHeight);
+    e += 0.5f * p.floorStiffness * pen * pen;
+  }
+  return e;
+}
+
+template <int W>
+__device__ __forceinline__ float groupSum(float v, unsigned mask) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, W);
+  return v;
+}
+template <int W>
+__device__ __forceinline__ float groupMin(float v, unsigned mask) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(mask, v, o, W));
+  return v;
+}
+
+// Deterministic block sum of doubles (fixed tree order).
+template <int N>
+__device__ __forceinline__ void blockSumDoubles(double (&vals)[N], double* scratch /* N * kBlock */) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) scratch[i * kBlock + threadIdx.x] = vals[i];
+  __syncthreads();
+  for (int stride = kBlock / 2; stride > 0; stride >>= 1) {
+    if (threadIdx.x < stride) {
+#pragma unroll
+      for (int i = 0; i < N; ++i)
+        scratch[i * kBlock + threadIdx.x] += scratch[i * kBlock + threadIdx.x + stride];
+    }
+    __syncthreads();
+  }
+#pragma unroll
+  for (int i = 0; i < N; ++i) vals[i] = scratch[i * kBlock];
+}
+
+// Vertex frame: polar of the volume-weighted average F over incident tets
+// (vertexPolarRotation, jgs2-shader.ts:2959-2989).
+__device__ __forceinline__ M3 vertexFrame(const Buffers& b, const float4* __restrict__ x, uint32_t v, float eps) {
+  const uint4 info = b.vinfo[v];
+  if (info.y == 0u) return midentity();
+  M3 avg = mzero();
+  float total = 0.0f;
+  for (uint32_t a = 0; a < info.y; ++a) {
+    const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
+    const TetRec r = loadTet(b.tets, entry >> 2);
+    avg = avg + r.vol * deformationAt(r, x);
+    total += r.vol;
+  }
+  avg = total > 0.0f ? (1.0f / total) * avg : midentity();
+  return polarRotation(avg, eps);
+}
+
+// ---------------------------------------------------------------------------
+// Prologue: predict (jgs2-shader.ts:2660-2692), iteration-0 vertex frames and
+// the source feasibility preflight (candidateTetrahedron + reduceCandidate on
+// the accepted pose, jgs2-solver.ts:2240-2259).
+__global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevParams* __restrict__ pp, uint32_t V,
+                                                         uint32_t T, int glob) {
+  __shared__ double scratch[2 * kBlock];
+  __shared__ bool isLast;
+  const DevParams p = *pp;
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  FrameState* fs = b.frame;
+  if (i < V) {
+    const float4 o = b.pos[0][i];
+    b.old[i] = make_float4(o.x, o.y, o.z, 1.0f);
+    const uint4 info = b.vinfo[i];
+    const float4 rm = b.restMass[i];
+    float3 pred = xyz(rm);
+    if (!isPinned(info)) {
+      const float3 vel = p.velocityDamping * xyz(b.velocity[i]);
+      pred = xyz(o) + p.dt * vel + (p.dt * p.dt) * f3(p.gravity[0], p.gravity[1], p.gravity[2]);
+    } else {
+      b.velocity[i] = make_float4(0, 0, 0, 0);
+    }
+    b.predicted[i] = make_float4(pred.x, pred.y, pred.z, 1.0f);
+    const float3 src = glob ? xyz(o) : pred;
+    b.pos[1][i] = make_float4(src.x, src.y, src.z, 1.0f);
+    b.finalUpdate[i] = 0.0f;
+    // Iteration-0 frames from the accepted pose (the stable iteration source).
+    if (glob) storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
+  }
+  if (!glob) return;
+  double sums[2] = {0.0, 0.0};
+  float localMin = kF32Max;
+  uint32_t bits = kSourceGeometryValid | kCandidateGeometryValid | kSourceEnergyValid | kCandidateEnergyValid;
+  if (i < T) {
+    const TetRec r = loadTet(b.tets, i);
+    const M3 F = deformationAt(r, b.pos[0]);
+    const float J = mdet(F);
+    if (finiteS(J)) {
+      localMin = J;
+      if (J > kDeterminantFloor) {
+        const float e = r.vol * snhEnergy(F, r.lambda, r.mu);
+        if (finiteS(e)) { sums[0] += e; sums[1] += e; }
+        else bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
+      } else {
+        bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
+      }
+    } else {
+      bits &= ~(kSourceGeometryValid | kCandidateGeometryValid | kSourceEnergyValid | kCandidateEnergyValid);
+    }
+  }
+  if (i < V) {
+    const uint4 info = b.vinfo[i];
+    const float e = implicitEnergy(p, b, i, xyz(b.pos[0][i]), info);
+    if (finiteS(e)) { sums[0] += e; sums[1] += e; }
+    else bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
+  }
+  const uint32_t wmin = __reduce_min_sync(0xffffffffu, orderedEncode(localMin));
+  const uint32_t wbits = __reduce_and_sync(0xffffffffu, bits);
+  if ((threadIdx.x & 31) == 0) {
+    atomicMin(&fs->gateMinSource, wmin);
+    if (wbits != 0xffffffffu) atomicAnd(&fs->gateBits, wbits);
+  }
+  blockSumDoubles<2>(sums, scratch);
+  if (threadIdx.x == 0) {
+    b.gatePartials[2 * blockIdx.x] = sums[0];
+    b.gatePartials[2 * blockIdx.x + 1] = sums[1];
+    __threadfence();
+    const uint32_t ticket = atomicAdd(&fs->prologueTicket, 1u);
+    isLast = ticket == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!isLast || threadIdx.x != 0) return;
+  __threadfence();
+  double e0 = 0.0;
+  for (uint32_t k = 0; k < gridDim.x; ++k) e0 += b.gatePartials[2 * k];
+  const float m = orderedDecode(atomicAdd(&fs->gateMinSource, 0u));
+  uint32_t vb = atomicAdd(&fs->gateBits, 0u);
+  if (T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
+  const bool gv = (vb & kSourceGeometryValid) != 0u;
+  const bool ev = (vb & kSourceEnergyValid) != 0u && finiteS(float(e0));
+  const bool accepted = gv && m > kDeterminantFloor;
+  uint32_t cbits = (vb & (kSourceGeometryValid | kCandidateGeometryValid)) | kLocalNumericsValid;
+  if (gv) cbits |= kAcceptedMinimumValid;
+  // predict clears the control records; the preflight then writes them with
+  // history index 0 (jgs2-shader.ts:2687-2691, 3916-3953).
+  fs->control[0] = make_float4(gv ? m : 0.f, gv ? m : 0.f, gv ? m : 0.f, float(cbits));
+  fs->control[1] = make_float4(accepted ? 1.f : 0.f, accepted ? 0.f : 1.f, 0.f, 0.f);
+  fs->control[2] = make_float4(ev ? float(e0) : 0.f, ev ? float(e0) : 0.f, ev ? float(e0) : 0.f, ev ? 1.f : 0.f);
+  fs->control[3] = make_float4(0, 0, 0, 0);
+  fs->gateMinSource = orderedEncode(kF32Max);
+  fs->gateMinCandidate = orderedEncode(kF32Max);
+  fs->gateBits = 0xffffffffu;
+  fs->prologueTicket = 0u;
+}
+
+// Vertex frames for a list of vertices (or all) from pose x.
+__global__ void __launch_bounds__(kBlock) vertexPolarKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                            const float4* __restrict__ x,
+                                                            const uint32_t* __restrict__ list, uint32_t count) {
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= count) return;
+  const DevParams p = *pp;
+  if (latched(p, b.frame)) return;
+  const uint32_t v = list ? list[i] : i;
+  storeRot(b.vertexRot, v, vertexFrame(b, x, v, p.rotationEpsilon));
+}
+
+// tetPolarRotation (jgs2-shader.ts:2931-2957) for the co-rotated path.
+__global__ void __launch_bounds__(kBlock) tetPolarKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                         const float4* __restrict__ x, uint32_t T) {
+  const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
+  if (t >= T) return;
+  const DevParams p = *pp;
+  const TetRec r = loadTet(b.tets, t);
+  storeRot(b.tetRot, t, polarRotation(deformationAt(r, x), p.rotationEpsilon));
+}
+
+__global__ void __launch_bounds__(kBlock) copyKernel(const float4* __restrict__ src, float4* __restrict__ dst,
+                                                     uint32_t V) {
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i < V) {
+    const float4 s = src[i];
+    dst[i] = make_float4(s.x, s.y, s.z, 1.0f);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// The per-vertex JGS2 local solve, stable Neo-Hookean path
+// (jgs2Solve, jgs2-shader.ts:2991-3473).  W lanes cooperate on one vertex:
+// item u < K is cubature record u, item u >= K is incident tet u - K; lane j
+// takes items j, j + W, ...  Cubature record state is cached in shared memory
+// for the line search; incident deformation gradients are recomputed per
+// trial from L1-resident data.
+struct CubState {
+  M3 F;
+  float I0, J0;
+  M3 dF0, dF1, dF2;
+  float3 gQ;
+  S3 HQ;
+  float w, vol, lambda, mu;
+  uint32_t slot;
+  float3 gs;
+};
+static_assert(sizeof(CubState) <= kRecFloats * 4, "cubature cache record too small");
+
+template <int W>
+__global__ void __launch_bounds__(kBlock) solveKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                      const float4* __restrict__ src, float4* tgt,
+                                                      const uint32_t* __restrict__ list, uint32_t count,
+                                                      uint32_t K) {
+  extern __shared__ float4 cache4[];
+  CubState* cache = reinterpret_cast<CubState*>(cache4);
+  __shared__ uint32_t sFail, sMaxBack, sSkip, sEvals, sMaxShift, sValid;
+  const DevParams p = *pp;
+  FrameState* fs = b.frame;
+  if (threadIdx.x == 0) { sFail = 0; sMaxBack = 0; sSkip = 0; sEvals = 0; sMaxShift = 0; sValid = 1; }
+  __syncthreads();
+  const uint32_t lane = threadIdx.x % W;
+  const uint32_t group = threadIdx.x / W;
+  const uint32_t groupsPerBlock = kBlock / W;
+  const uint32_t item = blockIdx.x * groupsPerBlock + group;
+  const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x & 31u) / W * W));
+  const bool isLatched = latched(p, fs);
+  // Per-vertex outputs owned by lane 0.
+  uint32_t status = kNonfinite, backtracks = 0, evals = 0;
+  float shiftN = 0.0f;
+  bool localValid = true, haveRecord = false;
+  if (item < count) {
+    const uint32_t v = list ? list[item] : item;
+    const uint4 info = b.vinfo[v];
+    const float4 rm = b.restMass[v];
+    if (isLatched) {
+      if (lane == 0) tgt[v] = src[v];
+    } else if (isPinned(info)) {
+      if (lane == 0) {
+        tgt[v] = make_float4(rm.x, rm.y, rm.z, 1.0f);
+        b.finalUpdate[v] = 0.0f;
+        float4* L = &b.local[4ull * v];
+        L[0] = L[1] = L[2] = make_float4(0, 0, 0, 0);
+        L[3] = make_float4(0, 0, 0, float(kPinned));
+        status = kPinned;
+        haveRecord = true;
+      }
+    } else {
+      const float4 c0 = fs->control[0];
+      const uint32_t vb = controlBits(c0.w) & kValidityMask;
+      const bool amv = (vb & kAcceptedMinimumValid) != 0u && finiteS(c0.z);
+      if (!(amv && c0.z > kDeterminantFloor)) {
+        // Preflight rejection before any material evaluation (jgs2-shader.ts:3042-3081).
+        if (lane == 0) {
+          tgt[v] = src[v];
+          b.finalUpdate[v] = 0.0f;
+          float4* L = &b.local[4ull * v];
+          L[0] = L[1] = L[2] = make_float4(0, 0, 0, 0);
+          status = amv ? kLineSearchFailed : kNonfinite;
+          L[3] = make_float4(amv ? c0.z : 0.f, 0, 0, float(status));
+          localValid = status != kNonfinite;
+          haveRecord = true;
+        }
+      } else {
+        const float3 position = xyz(src[v]);
+        const float3 predV = xyz(b.predicted[v]);
+        const float inertia = rm.w * p.invDt2;
+        const float dWs = distributedInertiaWeight(rm, info, p.invDt2);
+        const float nS = float(info.y > 1u ? info.y : 1u);
+        const bool objActive = p.objectiveFlags != 0u;
+        const float3 objS = objActive ? objectiveGradient(p, b.objectives, v, position) : f3(0, 0, 0);
+        const float ktS = targetStiffness(p, b.objectives, v);
+        float3 grad = f3(0, 0, 0);
+        S3 hess = szero();
+        const M3 RsT = mtrans(loadRot(b.vertexRot, v));
+        const uint32_t nItems = K + info.y;
+        CubState* myCache = cache + static_cast<size_t>(group) * K;
+        for (uint32_t u = lane; u < nItems; u += W) {
+          if (u < K) {
+            // ---- cubature record (jgs2-shader.ts:3197-3263) ----
+            CubState st;
+            const size_t rec = static_cast<size_t>(v) * K + u;
+            const uint32_t t = __ldg(&b.cubTet[rec]);
+            const float w = __ldg(&b.cubWeight[rec]);
+            st.w = 0.0f;
+            if (t != kEmptyTet && t < p.tetCount && w > 0.0f) {
+              const TetRec r = loadTet(b.tets, t);
+              const float* U = reinterpret_cast<const float*>(b.cubBasis + 9ull * rec);
+              M3 B[4];
+              float3 x[4];
+              float3 gQ = f3(0, 0, 0);
+              S3 HQ = szero();
+              uint32_t slot = 4;
+#pragma unroll
+              for (int l = 0; l < 4; ++l) {
+                const uint32_t q = idxAt(r.idx, l);
+                if (q == v) slot = l;
+                B[l] = mm(mm(loadRot(b.vertexRot, q), loadBlock(U + 9 * l)), RsT);
+                x[l] = xyz(src[q]);
+                const uint4 qi = b.vinfo[q];
+                const float4 qr = b.restMass[q];
+                const float dW = distributedInertiaWeight(qr, qi, p.invDt2);
+                float3 lin = dW * (x[l] - xyz(b.predicted[q]));
+                float quad = dW;
+                if (objActive && !isPinned(qi)) {
+                  const float nq = float(qi.y > 1u ? qi.y : 1u);
+                  lin = lin + objectiveGradient(p, b.objectives, q, x[l]) * (1.0f / nq);
+                  quad += targetStiffness(p, b.objectives, q) / nq;
+                }
+                gQ = gQ + mtv(B[l], lin);
+                saddScaled(HQ, quad, gramColumns(B[l]));
+              }
+              const M3 F = deformation(r, x[0], x[1], x[2], x[3]);
+              const float3 g0 = -(r.g1 + r.g2 + r.g3);
+              const M3 dF0 = outer(B[0].c0, g0) + outer(B[1].c0, r.g1) + outer(B[2].c0, r.g2) + outer(B[3].c0, r.g3);
+              const M3 dF1 = outer(B[0].c1, g0) + outer(B[1].c1, r.g1) + outer(B[2].c1, r.g2) + outer(B[3].c1, r.g3);
+              const M3 dF2 = outer(B[0].c2, g0) + outer(B[1].c2, r.g1) + outer(B[2].c2, r.g2) + outer(B[3].c2, r.g3);
+              const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
+              const M3 P = piola(F, pt);
+              float3 pg = r.vol * f3(frob(dF0, P), frob(dF1, P), frob(dF2, P)) + gQ;
+              // Reduced material Hessian vol <dF_r, DP[dF_c]>.
+              const float p0 = frob(F, dF0), p1 = frob(F, dF1), p2 = frob(F, dF2);
+              const float q0 = frob(pt.cof, dF0), q1 = frob(pt.cof, dF1), q2 = frob(pt.cof, dF2);
+              const M3 D0 = dcofactor(F, dF0), D1 = dcofactor(F, dF1), D2 = dcofactor(F, dF2);
+              S3 ph;
+              ph.xx = pt.a * frob(dF0, dF0) + pt.c1 * p0 * p0 + r.lambda * q0 * q0 + pt.b * frob(dF0, D0);
+              ph.yy = pt.a * frob(dF1, dF1) + pt.c1 * p1 * p1 + r.lambda * q1 * q1 + pt.b * frob(dF1, D1);
+              ph.zz = pt.a * frob(dF2, dF2) + pt.c1 * p2 * p2 + r.lambda * q2 * q2 + pt.b * frob(dF2, D2);
+              ph.xy = pt.a * frob(dF0, dF1) + pt.c1 * p0 * p1 + r.lambda * q0 * q1 + pt.b * frob(dF0, D1);
+              ph.xz = pt.a * frob(dF0, dF2) + pt.c1 * p0 * p2 + r.lambda * q0 * q2 + pt.b * frob(dF0, D2);
+              ph.yz = pt.a * frob(dF1, dF2) + pt.c1 * p1 * p2 + r.lambda * q1 * q2 + pt.b * frob(dF1, D2);
+              ph.xx *= r.vol; ph.yy *= r.vol; ph.zz *= r.vol; ph.xy *= r.vol; ph.xz *= r.vol; ph.yz *= r.vol;
+              sadd(ph, HQ);
+              float3 gs = f3(0, 0, 0);
+              if (slot < 4) {
+                // Remove the exact source block already in the local gather.
+                gs = shapeGradient(r, slot);
+                pg = pg - (r.vol * mv(P, gs) + dWs * (position - predV));
+                if (objActive) pg = pg - objS * (1.0f / nS);
+                const float3 u1 = mv(F, gs), w1 = mv(pt.cof, gs);
+                S3 blk = szero();
+                saddDiag(blk, pt.a * dot3(gs, gs));
+                saddOuter(blk, pt.c1, u1);
+                saddOuter(blk, r.lambda, w1);
+                saddScaled(ph, -r.vol, blk);
+                saddDiag(ph, -(dWs + ktS / nS));
+              }
+              grad = grad + w * pg;
+              saddScaled(hess, w, ph);
+              st.F = F;
+              st.I0 = pt.I1;
+              st.J0 = pt.J;
+              st.dF0 = dF0; st.dF1 = dF1; st.dF2 = dF2;
+              st.gQ = gQ;
+              st.HQ = HQ;
+              st.w = w;
+              st.vol = r.vol; st.lambda = r.lambda; st.mu = r.mu;
+              st.slot = slot;
+              st.gs = gs;
+            }
+            myCache[u] = st;
+          } else {
+            // ---- incident tetrahedron (jgs2-shader.ts:3097-3111) ----
+            const uint32_t entry = __ldg(&b.adjacency[info.x + (u - K)]);
+            const TetRec r = loadTet(b.tets, entry >> 2);
+            const uint32_t slot = entry & 3u;
+            const M3 F = deformationAt(r, src);
+            const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
+            const float3 g = shapeGradient(r, slot);
+            grad = grad + r.vol * mv(piola(F, pt), g);
+            const float3 u1 = mv(F, g), w1 = mv(pt.cof, g);
+            S3 blk = szero();
+            saddDiag(blk, pt.a * dot3(g, g));
+            saddOuter(blk, pt.c1, u1);
+            saddOuter(blk, r.lambda, w1);
+            saddScaled(hess, r.vol, blk);
+          }
+        }
+        // Group reduction of the gather.
+        grad.x = groupSum<W>(grad.x, mask);
+        grad.y = groupSum<W>(grad.y, mask);
+        grad.z = groupSum<W>(grad.z, mask);
+        hess.xx = groupSum<W>(hess.xx, mask);
+        hess.yy = groupSum<W>(hess.yy, mask);
+        hess.zz = groupSum<W>(hess.zz, mask);
+        hess.xy = groupSum<W>(hess.xy, mask);
+        hess.xz = groupSum<W>(hess.xz, mask);
+        hess.yz = groupSum<W>(hess.yz, mask);
+        // Own terms: inertia, objectives, floor (jgs2-shader.ts:3083-3092, 3188-3191).
+        grad = grad + inertia * (position - predV);
+        saddDiag(hess, inertia);
+        if (objActive) grad = grad + objS;
+        if (p.objectiveFlags & 2u) saddDiag(hess, ktS);
+        if (p.floorStiffness > 0.0f && position.y < p.floorHeight) {
+          grad.y += p.floorStiffness * (position.y - p.floorHeight);
+          hess.yy += p.floorStiffness;
+        }
+        // ---- globalization and line search (jgs2-shader.ts:3265-3473) ----
+        const SolveResult dr = globalizationSolve(hess, grad, inertia);
+        status = kNonfinite;
+        const float3 fullP = position + dr.direction;
+        const float3 fullD = fullP - position;
+        const float scs = fmaxf(fabsf(position.x), fmaxf(fabsf(position.y), fabsf(position.z)));
+        const float resolution =
+            fmaxf(p.sceneScale, fmaxf(scs, 1.0e-12f)) * kUnitRoundoff * kPositionResolutionMultiplier;
+        const bool below = dr.status == kAccepted && finiteV(fullP) && finiteV(fullD) && scaledLength(fullD) <= resolution;
+        if (dr.status == kAccepted) status = below ? kZeroGradient : kLineSearchFailed;
+        else if (dr.status == kZeroGradient) status = kZeroGradient;
+        else if (dr.status == kShiftLimit) status = kShiftLimit;
+        else if (dr.status == kCholeskyFailed) status = kCholeskyFailed;
+        else if (dr.status == kNonDescent) status = kNonDescent;
+        float alpha = 0.0f, acceptedDelta = 0.0f, bound = 0.0f, minTrialDet = 0.0f;
+        float3 acceptedD = f3(0, 0, 0), acceptedP = position;
+        if (dr.status == kAccepted && !below) {
+          float ta = 1.0f;
+          const float dl = scaledLength(dr.direction);
+          if (p.maxStep > 0.0f && dl > p.maxStep) ta = p.maxStep / dl;
+          const float controlMin = c0.z;  // accepted-source minimum (finite here)
+          for (uint32_t bt = 0; bt <= kMaxBacktracks; ++bt) {
+            const float3 tp = position + ta * dr.direction;
+            const float3 td = tp - position;
+            if (!finiteV(tp) || !finiteV(td)) { status = kNonfinite; minTrialDet = 0.f; backtracks = bt; break; }
+            const float tl = scaledLength(td);
+            if (p.maxStep > 0.0f && tl > p.maxStep) { ta *= kBacktrackFactor; continue; }
+            if (tl <= resolution) { status = kZeroGradient; minTrialDet = 0.f; backtracks = bt; break; }
+            const float gd = dot3(grad, td);
+            if (!finiteS(gd)) { status = kNonfinite; minTrialDet = 0.f; backtracks = bt; break; }
+            if (!(gd < 0.0f)) { status = kZeroGradient; minTrialDet = 0.f; backtracks = bt; break; }
+            // Restricted geometry and energy in one pass over the items
+            // (restrictedMinimumDeformationDeterminant :1980-2118 and
+            // restrictedEnergyDelta :2120-2337); the energy is used only
+            // when the geometry is feasible, as in the reference order.
+            float jmin = kF32Max, de = 0.0f;
+            bool geomFinite = true;
+            for (uint32_t u = lane; u < nItems; u += W) {
+              float J = 0.0f;
+              if (u < K) {
+                const CubState& st = myCache[u];
+                if (!(st.w > 0.0f)) continue;
+                const M3 D = td.x * st.dF0 + td.y * st.dF1 + td.z * st.dF2;
+                const float dm = st.vol * snhEnergyDelta(st.F, st.I0, st.J0, D, st.lambda, st.mu, &J);
+                float comp = dm + dot3(td, st.gQ) + 0.5f * dot3(td, smv(st.HQ, td));
+                if (st.slot < 4) {
+                  float Js;
+                  comp -= st.vol * snhEnergyDelta(st.F, st.I0, st.J0, outer(td, st.gs), st.lambda, st.mu, &Js);
+                  comp -= dWs * (dot3(position - predV, td) + 0.5f * dot3(td, td));
+                  if (objActive) comp -= objectiveDelta(p, b.objectives, v, position, td) / nS;
+                }
+                de += st.w * comp;
+              } else {
+                const uint32_t entry = __ldg(&b.adjacency[info.x + (u - K)]);
+                const TetRec r = loadTet(b.tets, entry >> 2);
+                const M3 F = deformationAt(r, src);
+                const float I0 = frob(F, F);
+                const float J0 = mdet(F);
+                de += r.vol * snhEnergyDelta(F, I0, J0, outer(td, shapeGradient(r, entry & 3u)), r.lambda, r.mu, &J);
+              }
+              if (!finiteS(J)) geomFinite = false;
+              jmin = fminf(jmin, J);
+            }
+            jmin = groupMin<W>(jmin, mask);
+            const bool allFinite = __all_sync(mask, geomFinite);
+            de = groupSum<W>(de, mask);
+            if (!allFinite) { status = kNonfinite; minTrialDet = 0.f; backtracks = bt; break; }
+            const float trialMin = fminf(controlMin, jmin);
+            minTrialDet = trialMin;
+            if (trialMin > kDeterminantFloor) {
+              de += inertia * (dot3(position - predV, td) + 0.5f * dot3(td, td)) + floorDelta(p, position.y, td.y);
+              if (objActive) de += objectiveDelta(p, b.objectives, v, position, td);
+              evals += 1;
+              if (!finiteS(de)) { status = kNonfinite; backtracks = bt; break; }
+              const float tb = kArmijoC1 * gd;
+              if (de <= tb) {
+                alpha = ta; acceptedDelta = de; bound = tb; backtracks = bt; status = kAccepted;
+                acceptedD = td; acceptedP = tp;
+                break;
+              }
+            }
+            ta *= kBacktrackFactor;
+          }
+          if (status == kLineSearchFailed) backtracks = kMaxBacktracks;
+        }
+        if (lane == 0) {
+          tgt[v] = make_float4(acceptedP.x, acceptedP.y, acceptedP.z, 1.0f);
+          b.finalUpdate[v] = scaledLength(acceptedD);
+          float4* L = &b.local[4ull * v];
+          const float4 l0 = make_float4(dr.direction.x, dr.direction.y, dr.direction.z, alpha);
+          const float4 l1 = make_float4(dr.minEig * dr.scale, dr.scale, dr.shift * dr.scale, dr.shift);
+          const float4 l2 = make_float4(acceptedDelta, bound, dr.gdd, dr.residual);
+          const float4 l3 = make_float4(minTrialDet, float(backtracks), float(evals), float(status));
+          L[0] = l0; L[1] = l1; L[2] = l2; L[3] = l3;
+          localValid = finiteS(l0.x) && finiteS(l0.y) && finiteS(l0.z) && finiteS(l0.w) && finiteS(l1.x) &&
+                       finiteS(l1.y) && finiteS(l1.z) && finiteS(l1.w) && finiteS(l2.x) && finiteS(l2.y) &&
+                       finiteS(l2.z) && finiteS(l2.w) && finiteS(l3.x) && status != kNonfinite && l1.w >= 0.0f;
+          shiftN = dr.shift;
+          haveRecord = true;
+        }
+      }
+    }
+  }
+  // Local aggregates of reduceCandidate's vertex loop (jgs2-shader.ts:3689-3790).
+  if (haveRecord && lane == 0) {
+    const bool failure = status == kShiftLimit || status == kNonDescent || status == kLineSearchFailed ||
+                         status == kNonfinite || status == kCholeskyFailed;
+    uint32_t trials = 0;
+    if (status == kAccepted) trials = backtracks + 1;
+    else if (status == kLineSearchFailed && backtracks == kMaxBacktracks) trials = kTrialCount;
+    else if (status == kZeroGradient && backtracks > 0) trials = backtracks;
+    else if (status == kNonfinite) trials = backtracks;  // a nonfinite trial never has J above the floor here
+    const uint32_t skipped = trials - (trials < evals ? trials : evals);
+    if (failure) atomicAdd(&sFail, 1u);
+    if (backtracks) atomicMax(&sMaxBack, backtracks);
+    if (skipped) atomicAdd(&sSkip, skipped);
+    if (evals) atomicAdd(&sEvals, evals);
+    if (shiftN > 0.0f && finiteS(shiftN)) atomicMax(&sMaxShift, __float_as_uint(shiftN));
+    if (!localValid) sValid = 0;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    if (sFail) atomicAdd(&fs->localFailures, sFail);
+    if (sMaxBack) atomicMax(&fs->localMaxBacktracks, sMaxBack);
+    if (sSkip) atomicAdd(&fs->localSkipped, sSkip);
+    if (sEvals) atomicAdd(&fs->localEvaluations, sEvals);
+    if (sMaxShift) atomicMax(&fs->localMaxShift, sMaxShift);
+    if (!sValid) atomicAnd(&fs->localNumericsValid, 0u);
+  }
+}
+
+// ---------------------------------------------------------------------------
+// Gate: candidateTetrahedron (jgs2-shader.ts:3498-3601) + vertex energies
+// (assembledVertexEnergy :3489-3496) + reduceCandidate (:3611-3955).
+__global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                     const float4* __restrict__ src,
+                                                     const float4* __restrict__ tgt, uint32_t V, uint32_t T) {
+  __shared__ double scratch[2 * kBlock];
+  __shared__ bool isLast;
+  const DevParams p = *pp;
+  FrameState* fs = b.frame;
+  if (latched(p, fs)) return;  // uniform across the grid
+  double sums[2] = {0.0, 0.0};
+  uint32_t bits = kSourceGeometryValid | kCandidateGeometryValid | kSourceEnergyValid | kCandidateEnergyValid;
+  float minS = kF32Max, minC = kF32Max;
+  for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < (T > V ? T : V); i += gridDim.x * kBlock) {
+    if (i < T) {
+      const TetRec r = loadTet(b.tets, i);
+      const M3 sF = deformationAt(r, src);
+      const M3 cF = deformationAt(r, tgt);
+      const float sJ = mdet(sF), cJ = mdet(cF);
+      const bool sgv = finiteS(sJ), cgv = finiteS(cJ);
+      if (sgv) minS = fminf(minS, sJ); else bits &= ~kSourceGeometryValid;
+      if (cgv) minC = fminf(minC, cJ); else bits &= ~kCandidateGeometryValid;
+      bool sev = false, cev = false;
+      if (sgv && sJ > kDeterminantFloor) {
+        const float e = r.vol * snhEnergy(sF, r.lambda, r.mu);
+        sev = finiteS(e);
+        if (sev) sums[0] += e;
+      }
+      if (cgv && cJ > kDeterminantFloor) {
+        const float e = r.vol * snhEnergy(cF, r.lambda, r.mu);
+        cev = finiteS(e);
+        if (cev) sums[1] += e;
+      }
+      if (!sev) bits &= ~kSourceEnergyValid;
+      if (!cev) bits &= ~kCandidateEnergyValid;
+    }
+    if (i < V) {
+      const uint4 info = b.vinfo[i];
+      const float es = implicitEnergy(p, b, i, xyz(src[i]), info);
+      const float ec = implicitEnergy(p, b, i, xyz(tgt[i]), info);
+      if (finiteS(es)) sums[0] += es; else bits &= ~kSourceEnergyValid;
+      if (finiteS(ec)) sums[1] += ec; else bits &= ~kCandidateEnergyValid;
+    }
+  }
+  const uint32_t wminS = __reduce_min_sync(0xffffffffu, orderedEncode(minS));
+  const uint32_t wminC = __reduce_min_sync(0xffffffffu, orderedEncode(minC));
+  const uint32_t wbits = __reduce_and_sync(0xffffffffu, bits);
+  if ((threadIdx.x & 31u) == 0u) {
+    atomicMin(&fs->gateMinSource, wminS);
+    atomicMin(&fs->gateMinCandidate, wminC);
+    if (wbits != 0xffffffffu) atomicAnd(&fs->gateBits, wbits);
+  }
+  blockSumDoubles<2>(sums, scratch);
+  if (threadIdx.x == 0) {
+    b.gatePartials[2 * blockIdx.x] = sums[0];
+    b.gatePartials[2 * blockIdx.x + 1] = sums[1];
+    __threadfence();
+    isLast = atomicAdd(&fs->gateTicket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!isLast || threadIdx.x != 0) return;
+  __threadfence();
+  double e0 = 0.0, e1 = 0.0;
+  for (uint32_t k = 0; k < gridDim.x; ++k) {
+    e0 += b.gatePartials[2 * k];
+    e1 += b.gatePartials[2 * k + 1];
+  }
+  uint32_t vb = atomicAdd(&fs->gateBits, 0u) & (kSourceGeometryValid | kCandidateGeometryValid |
+                                                  kSourceEnergyValid | kCandidateEnergyValid);
+  if (!atomicAdd(&fs->localNumericsValid, 0u)) vb &= ~kLocalNumericsValid; else vb |= kLocalNumericsValid;
+  const float eS = float(e0), eC = float(e1);
+  if (!finiteS(eS)) vb &= ~kSourceEnergyValid;
+  if (!finiteS(eC)) vb &= ~kCandidateEnergyValid;
+  if (T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
+  const float sm = orderedDecode(atomicAdd(&fs->gateMinSource, 0u));
+  const float cm = orderedDecode(atomicAdd(&fs->gateMinCandidate, 0u));
+  const bool sgv = (vb & kSourceGeometryValid) != 0u, cgv = (vb & kCandidateGeometryValid) != 0u;
+  const bool sev = (vb & kSourceEnergyValid) != 0u, cev = (vb & kCandidateEnergyValid) != 0u;
+  const bool accepted = (sgv && sm > kDeterminantFloor) && (cgv && cm > kDeterminantFloor);
+  const float am = accepted ? cm : sm;
+  const bool amv = accepted ? cgv : sgv;
+  const float ae = accepted ? eC : eS;
+  const bool aev = accepted ? cev : sev;
+  if (amv) vb |= kAcceptedMinimumValid;
+  uint32_t historyIndex = 0;
+  const float packed = fs->control[1].w;
+  if (finiteNonnegInt(packed, float(kHistoryCapacity))) historyIndex = static_cast<uint32_t>(packed);
+  else vb &= ~kLocalNumericsValid;
+  const uint32_t cb = vb & kValidityMask;
+  const uint32_t failures = atomicAdd(&fs->localFailures, 0u);
+  fs->control[0] = make_float4(sgv ? sm : 0.f, cgv ? cm : 0.f, amv ? am : 0.f, float(cb));
+  fs->control[1] = make_float4(accepted ? 1.f : 0.f, accepted ? 0.f : 1.f, float(failures), float(historyIndex));
+  fs->control[2] = make_float4(sev ? eS : 0.f, cev ? eC : 0.f, aev ? ae : 0.f, (sev && cev) ? 1.f : 0.f);
+  fs->control[3] = make_float4(__uint_as_float(atomicAdd(&fs->localMaxShift, 0u)),
+                               float(atomicAdd(&fs->localMaxBacktracks, 0u)),
+                               float(atomicAdd(&fs->localSkipped, 0u)),
+                               float(atomicAdd(&fs->localEvaluations, 0u)));
+  // Reset the accumulators for the next sweep.
+  fs->gateMinSource = orderedEncode(kF32Max);
+  fs->gateMinCandidate = orderedEncode(kF32Max);
+  fs->gateBits = 0xffffffffu;
+  fs->localFailures = 0u;
+  fs->localMaxBacktracks = 0u;
+  fs->localSkipped = 0u;
+  fs->localEvaluations = 0u;
+  fs->localMaxShift = 0u;
+  fs->localNumericsValid = 1u;
+  fs->gateTicket = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// applyCandidate (:3957-3983) + convergenceGradient (:3985-4097) +
+// reduceConvergence (:4105-4486), and the next iteration's vertex frames.
+__global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                            const float4* __restrict__ src, float4* tgt,
+                                                            uint32_t V, int nextRotations) {
+  __shared__ double scratch[6 * kBlock];
+  __shared__ bool isLast;
+  const DevParams p = *pp;
+  FrameState* fs = b.frame;
+  if (latched(p, fs)) return;  // uniform across the grid
+  const bool accepted = fs->control[1].x == 1.0f;
+  const float4* __restrict__ acc = accepted ? tgt : src;
+  double sq[6] = {0, 0, 0, 0, 0, 0};
+  float scale[6] = {0, 0, 0, 0, 0, 0};
+  float maxUpdate = 0.0f;
+  bool valid = true;
+  const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
+  if (v < V) {
+    float upd = 0.0f;
+    if (!accepted) {
+      tgt[v] = src[v];
+    } else {
+      upd = scaledLength(xyz(tgt[v]) - xyz(src[v]));
+    }
+    b.finalUpdate[v] = upd;
+    if (!(finiteS(upd) && upd >= 0.0f)) valid = false; else maxUpdate = upd;
+    const uint4 info = b.vinfo[v];
+    if (!isPinned(info)) {
+      const float3 x = xyz(acc[v]);
+      float3 comps[5];
+      comps[0] = (b.restMass[v].w * p.invDt2) * (x - xyz(b.predicted[v]));
+      float3 material = f3(0, 0, 0);
+      for (uint32_t a = 0; a < info.y; ++a) {
+        const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
+        const TetRec r = loadTet(b.tets, entry >> 2);
+        const M3 F = deformationAt(r, acc);
+        const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
+        material = material + r.vol * mv(piola(F, pt), shapeGradient(r, entry & 3u));
+      }
+      comps[1] = material;
+      comps[2] = f3(0, 0, 0);
+      comps[3] = f3(0, 0, 0);
+      if (p.objectiveFlags != 0u) {
+        if (p.objectiveFlags & 1u) comps[2] = -xyz(b.objectives[2ull * v]);
+        if (p.objectiveFlags & 2u) {
+          const float4 t = b.objectives[2ull * v + 1];
+          if (t.w > 0.0f) comps[3] = t.w * (x - xyz(t));
+        }
+      }
+      comps[4] = f3(0, 0, 0);
+      if (p.floorStiffness > 0.0f && x.y < p.floorHeight) comps[4].y = p.floorStiffness * (x.y - p.floorHeight);
+      float3 total = f3(0, 0, 0);
+      bool tv = true;
+#pragma unroll
+      for (int c = 0; c < 5; ++c) {
+        const bool ok = finiteV(comps[c]);
+        const float3 val = ok ? comps[c] : f3(0, 0, 0);
+        scale[c] = fmaxf(fabsf(val.x), fmaxf(fabsf(val.y), fabsf(val.z)));
+        sq[c] = double(val.x) * val.x + double(val.y) * val.y + double(val.z) * val.z;
+        total = total + val;
+        tv = tv && ok;
+      }
+      tv = tv && finiteV(total);
+      if (tv) {
+        scale[5] = fmaxf(fabsf(total.x), fmaxf(fabsf(total.y), fabsf(total.z)));
+        sq[5] = double(total.x) * total.x + double(total.y) * total.y + double(total.z) * total.z;
+      } else {
+        valid = false;
+      }
+    }
+    if (nextRotations) storeRot(b.vertexRot, v, vertexFrame(b, acc, v, p.rotationEpsilon));
+  }
+#pragma unroll
+  for (int c = 0; c < 6; ++c) {
+    const uint32_t m = __reduce_max_sync(0xffffffffu, __float_as_uint(scale[c]));
+    if ((threadIdx.x & 31u) == 0u && m) atomicMax(&fs->convScale[c], m);
+  }
+  {
+    const uint32_t m = __reduce_max_sync(0xffffffffu, __float_as_uint(maxUpdate));
+    const bool allValid = __all_sync(0xffffffffu, valid);
+    if ((threadIdx.x & 31u) == 0u) {
+      if (m) atomicMax(&fs->convMaxUpdate, m);
+      if (!allValid) atomicAnd(&fs->convValid, 0u);
+    }
+  }
+  blockSumDoubles<6>(sq, scratch);
+  if (threadIdx.x == 0) {
+#pragma unroll
+    for (int c = 0; c < 6; ++c) b.convPartials[6ull * blockIdx.x + c] = sq[c];
+    __threadfence();
+    isLast = atomicAdd(&fs->convTicket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  if (!isLast || threadIdx.x != 0) return;
+  __threadfence();
+  double tot[6] = {0, 0, 0, 0, 0, 0};
+  for (uint32_t k = 0; k < gridDim.x; ++k)
+    for (int c = 0; c < 6; ++c) tot[c] += b.convPartials[6ull * k + c];
+  float norms[5];
+  bool cnv = atomicAdd(&fs->convValid, 0u) != 0u;
+  for (int c = 0; c < 5; ++c) {
+    norms[c] = float(sqrt(tot[c]));
+    cnv = cnv && finiteS(norms[c]) && norms[c] >= 0.0f;
+  }
+  const float gnorm = float(sqrt(tot[5]));
+  const float den = fmaxf(1.0f, norms[0] + norms[1] + norms[2] + norms[3] + norms[4]);
+  const float rel = gnorm / den;
+  const bool rnv = cnv && finiteS(gnorm) && finiteS(den) && den >= 1.0f && finiteS(rel) && rel >= 0.0f;
+  const float mu = __uint_as_float(atomicAdd(&fs->convMaxUpdate, 0u));
+  const bool ssv = finiteS(p.sceneScale) && p.sceneScale >= 0.0f;
+  const float nmu = mu / fmaxf(ssv ? p.sceneScale : 1.0e-12f, 1.0e-12f);
+  const bool unv = (atomicAdd(&fs->convValid, 0u) != 0u) && ssv && finiteS(mu) && mu >= 0.0f && finiteS(nmu);
+  const float4 geometry = fs->control[0];
+  const uint32_t cb = controlBits(geometry.w) & kValidityMask;
+  const bool sgv = (cb & kSourceGeometryValid) != 0u && finiteS(geometry.x);
+  const bool cgv = (cb & kCandidateGeometryValid) != 0u && finiteS(geometry.y);
+  const bool amv = (cb & kAcceptedMinimumValid) != 0u && finiteS(geometry.z);
+  const bool lnv = (cb & kLocalNumericsValid) != 0u;
+  const float4 accept = fs->control[1];
+  const bool aav = finiteNonnegInt(accept.x, 1.0f), arv = finiteNonnegInt(accept.y, 1.0f);
+  const bool lfv = finiteNonnegInt(accept.z, float(V));
+  const bool hiv = finiteNonnegInt(accept.w, float(kHistoryCapacity));
+  const bool aa = aav && accept.x == 1.0f, ar = arv && accept.y == 1.0f;
+  const uint32_t failures = lfv ? static_cast<uint32_t>(accept.z) : 0u;
+  const uint32_t hi = hiv ? static_cast<uint32_t>(accept.w) : 0u;
+  const float4 cmx = fs->control[3];
+  const bool cmv = finiteS(cmx.x) && cmx.x >= 0.0f && finiteNonnegInt(cmx.y, float(kMaxBacktracks)) &&
+                   finiteNonnegInt(cmx.z, float(V) * float(kTrialCount)) &&
+                   finiteNonnegInt(cmx.w, float(V) * float(kTrialCount));
+  const bool fin = rnv && unv && sgv && cgv && amv && lnv && aav && arv && lfv && hiv && cmv;
+  const bool rs = fin && rel <= p.residualTolerance;
+  const bool us = fin && nmu <= p.normalizedUpdateTolerance;
+  const bool conv = rs && us && aa && !ar && failures == 0u;
+  if (hiv && hi < kHistoryCapacity) {
+    float4* h = &fs->history[8 * hi];
+    h[0] = fs->control[0];
+    h[1] = make_float4(accept.x, accept.y, accept.z, ar ? 1.f : 0.f);
+    h[2] = fs->control[2];
+    h[3] = make_float4(cnv ? norms[0] : 0.f, cnv ? norms[1] : 0.f, cnv ? norms[2] : 0.f, cnv ? norms[3] : 0.f);
+    h[4] = make_float4(cnv ? norms[4] : 0.f, rnv ? gnorm : 0.f, rnv ? den : 0.f, rnv ? rel : 0.f);
+    h[5] = make_float4(unv ? mu : 0.f, unv ? nmu : 0.f, rs ? 1.f : 0.f, us ? 1.f : 0.f);
+    h[6] = make_float4(conv ? 1.f : 0.f, fin ? 1.f : 0.f, float(hi), cmv ? cmx.x : 0.f);
+    h[7] = make_float4(cmv ? cmx.y : 0.f, cmv ? cmx.z : 0.f, cmv ? cmx.w : 0.f, 1.f);
+  }
+  fs->control[1].w = float(hi + 1);
+  if (conv && p.stopEnabled) fs->control[0].w = float(cb | kStopLatchBit);
+  for (int c = 0; c < 6; ++c) fs->convScale[c] = 0u;
+  fs->convMaxUpdate = 0u;
+  fs->convValid = 1u;
+  fs->convTicket = 0u;
+}
+
+// ---------------------------------------------------------------------------
+// Epilogue: even-count copy (copyPosition, :4488-4496), optional body
+// correction (:4498-4551), finalize (:4553-4589).
+__global__ void __launch_bounds__(kBlock) bodyAccumulateKernel(Buffers b, const float4* __restrict__ finalPos,
+                                                               uint32_t V) {
+  const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
+  if (v >= V) return;
+  float4 x = finalPos[v];
+  if (finalPos != b.pos[0]) b.pos[0][v] = make_float4(x.x, x.y, x.z, 1.0f);
+  const uint4 info = b.vinfo[v];
+  const double m = fmax(double(b.restMass[v].w), 0.0);
+  const float4 pr = b.predicted[v];
+  // Per body: total mass, solved x/z moments, predicted x/z moments, pinned
+  // count.  Double atomics: the summation order varies from run to run, so
+  // the correction is reproducible to double rounding, not bitwise.
+  double* acc = &b.bodyAccum[6ull * info.w];
+  atomicAdd(&acc[0], m);
+  atomicAdd(&acc[1], m * x.x);
+  atomicAdd(&acc[2], m * x.z);
+  atomicAdd(&acc[3], m * pr.x);
+  atomicAdd(&acc[4], m * pr.z);
+  if (isPinned(info)) atomicAdd(&acc[5], 1.0);
+}
+
+__global__ void __launch_bounds__(kBlock) finalizeKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                         const float4* __restrict__ finalPos, uint32_t V, int glob,
+                                                         int bodyCorrection) {
+  const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
+  if (v >= V) return;
+  const DevParams p = *pp;
+  const uint4 info = b.vinfo[v];
+  float4 x = bodyCorrection ? b.pos[0][v] : finalPos[v];
+  if (isPinned(info)) {
+    if (!glob) {
+      const float4 rm = b.restMass[v];
+      x = make_float4(rm.x, rm.y, rm.z, 1.0f);
+    }
+    b.pos[0][v] = make_float4(x.x, x.y, x.z, 1.0f);
+    b.velocity[v] = make_float4(0, 0, 0, 0);
+    return;
+  }
+  if (bodyCorrection && info.w < p.bodyCount) {
+    const double* acc = &b.bodyAccum[6ull * info.w];
+    if (acc[5] == 0.0 && acc[0] > 0.0) {
+      x.x += float((acc[3] - acc[1]) / acc[0]);
+      x.z += float((acc[4] - acc[2]) / acc[0]);
+    }
+  }
+  b.pos[0][v] = make_float4(x.x, x.y, x.z, 1.0f);
+  const float3 o = xyz(b.old[v]);
+  float3 vel = (xyz(x) - o) * p.invDt;
+  if (p.floorStiffness > 0.0f && p.contactTangentialDamping > 0.0f && x.y <= p.floorHeight + p.contactMargin) {
+    const float s = expf(-p.contactTangentialDamping * p.dt);
+    vel.x *= s;
+    vel.z *= s;
+  }
+  b.velocity[v] = make_float4(vel.x, vel.y, vel.z, 0.0f);
+}
+
+inline uint32_t blocksFor(uint32_t n) { return (n + kBlock - 1) / kBlock; }
+
+}  // namespace
+
+uint32_t gateBlockCount(uint32_t V, uint32_t T) {
+  const uint32_t n = T > V ? T : V;
+  const uint32_t blocks = blocksFor(n);
+  return blocks < 1u ? 1u : blocks;
+}
+
+uint32_t convBlockCount(uint32_t V) { return blocksFor(V) < 1u ? 1u : blocksFor(V); }
+
+int launchPrologue(const Buffers& b, const DevParams* p, uint32_t V, uint32_t T, bool glob, cudaStream_t s) {
+  const uint32_t n = T > V ? T : V;
+  prologueKernel<<<blocksFor(n), kBlock, 0, s>>>(b, p, V, T, glob ? 1 : 0);
+  return 1;
+}
+
+int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, const uint32_t* list,
+                      uint32_t count, cudaStream_t s) {
+  if (count == 0) return 0;
+  vertexPolarKernel<<<blocksFor(count), kBlock, 0, s>>>(b, p, src, list, count);
+  return 1;
+}
+
+int launchTetPolar(const Buffers& b, const DevParams* p, const float4* src, uint32_t T, cudaStream_t s) {
+  if (T == 0) return 0;
+  tetPolarKernel<<<blocksFor(T), kBlock, 0, s>>>(b, p, src, T);
+  return 1;
+}
+
+int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
+                uint32_t count, uint32_t K, bool glob, cudaStream_t s) {
+  (void)glob;
+  if (count == 0) return 0;
+  constexpr int groups = kBlock / kGroup;
+  const size_t smem = static_cast<size_t>(groups) * K * sizeof(CubState);
+  const uint32_t blocks = (count + groups - 1) / groups;
+  solveKernel<kGroup><<<blocks, kBlock, smem, s>>>(b, p, src, tgt, list, count, K);
+  return 1;
+}
+
+int launchCopy(const float4* src, float4* dst, uint32_t V, cudaStream_t s) {
+  copyKernel<<<blocksFor(V), kBlock, 0, s>>>(src, dst, V);
+  return 1;
+}
+
+int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V, uint32_t T,
+               cudaStream_t s) {
+  gateKernel<<<b.gateBlocks, kBlock, 0, s>>>(b, p, src, tgt, V, T);
+  return 1;
+}
+
+int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, uint32_t V,
+                      bool computeNextRotations, cudaStream_t s) {
+  convergenceKernel<<<b.convBlocks, kBlock, 0, s>>>(b, p, src, tgt, V, computeNextRotations ? 1 : 0);
+  return 1;
+}
+
+int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool glob,
+                   bool bodyCorrection, uint32_t bodies, cudaStream_t s) {
+  int n = 0;
+  if (bodyCorrection) {
+    cudaMemsetAsync(b.bodyAccum, 0, sizeof(double) * 6ull * bodies, s);
+    bodyAccumulateKernel<<<blocksFor(V), kBlock, 0, s>>>(b, finalPos, V);
+    ++n;
+  }
+  finalizeKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, finalPos, V, glob ? 1 : 0, bodyCorrection ? 1 : 0);
+  return n + 1;
+}
+
+}  // namespace jgs2

@@ -1,0 +1,100 @@
+// Device buffers, per-call parameters and kernel launch entry points of the
+// JGS2 step.  Shared by jgs2_kernels.cu (device) and jgs2_runtime.cpp (host).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace jgs2 {
+
+// Per-call settings, copied to device memory before each step so captured
+// CUDA graphs stay valid across setting changes.  Mirrors the uniform block
+// SimParams (src/simulation/gpu/jgs2-shader.ts:141-164).
+struct DevParams {
+  float dt, invDt, invDt2, maxStep;
+  float gravity[3];
+  float floorHeight;
+  float floorStiffness, regularization, rotationEpsilon, velocityDamping;
+  float contactTangentialDamping, contactMargin;
+  float residualTolerance, normalizedUpdateTolerance;
+  float sceneScale;
+  uint32_t objectiveFlags;  // bit0 forces, bit1 targets
+  uint32_t stopEnabled;     // convergence latch active (production step)
+  uint32_t globalization;   // stable Neo-Hookean path
+  uint32_t historyCapacity;
+  uint32_t vertexCount, tetCount, cubatureK, bodyCount;
+};
+
+// Reduction scratch and the GPU-resident control/history records
+// (dynamic arena regions globalizationControl/globalizationHistory,
+// src/simulation/gpu/layout.ts:418-503).
+struct FrameState {
+  float4 control[4];
+  float4 history[64 * 8];
+  // Gate reduction (candidateTetrahedron + reduceCandidate).
+  uint32_t gateTicket;
+  uint32_t gateMinSource, gateMinCandidate;  // order-preserving float encodings
+  uint32_t gateBits;                          // AND of validity bits
+  // Local diagnostics aggregates of the current sweep (reduceCandidate's
+  // vertex loop), accumulated by the solve kernel with order-free atomics.
+  uint32_t localFailures, localMaxBacktracks, localSkipped, localEvaluations;
+  uint32_t localMaxShift;  // float bits of a non-negative value
+  uint32_t localNumericsValid;
+  // Convergence reduction.
+  uint32_t convTicket;
+  uint32_t convScale[6];    // float bits (non-negative maxima)
+  uint32_t convMaxUpdate;   // float bits
+  uint32_t convValid;
+  uint32_t prologueTicket;
+  uint32_t pad[2];
+};
+
+// All device arrays of one solver.
+struct Buffers {
+  // dynamic
+  float4* pos[2];         // A, B
+  float4* predicted;
+  float4* velocity;
+  float4* old;
+  float4* vertexRot;      // 3 per vertex (columns)
+  float4* tetRot;         // 3 per tet (co-rotated only)
+  float* finalUpdate;     // per vertex update norm
+  float4* local;          // 4 per vertex (local diagnostics)
+  FrameState* frame;
+  double* gatePartials;   // 2 per gate block (source / candidate energy)
+  double* convPartials;   // 6 per convergence block
+  double* bodyAccum;      // 6 per body (mass, solved xz, predicted xz, pinned count)
+  // static
+  const float4* restMass;     // rest xyz (pin target), mass
+  const uint4* vinfo;         // adjacency start, count, pinned, body
+  const float4* tets;         // 4 per tet: [g1 vol] [g2 lambda] [g3 mu] [indices as uint]
+  const uint32_t* adjacency;  // incident tet * 4 + local slot
+  const uint32_t* cubTet;
+  const float* cubWeight;
+  const float4* cubBasis;     // 9 float4 per record (36 floats, row-major blocks)
+  const float* stiffness;     // 144 per tet (co-rotated only)
+  float4* objectives;         // 2 per vertex: force, target + stiffness
+  const uint32_t* colors;     // per vertex colour
+  uint32_t gateBlocks, convBlocks;
+};
+
+// Kernel launch entry points (jgs2_kernels.cu).  Every launcher returns the
+// number of kernels it launched.
+int launchPrologue(const Buffers& b, const DevParams* p, uint32_t V, uint32_t T, bool glob, cudaStream_t s);
+int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, const uint32_t* list,
+                      uint32_t count, cudaStream_t s);
+int launchTetPolar(const Buffers& b, const DevParams* p, const float4* src, uint32_t T, cudaStream_t s);
+int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
+                uint32_t count, uint32_t K, bool glob, cudaStream_t s);
+int launchCopy(const float4* src, float4* dst, uint32_t V, cudaStream_t s);
+int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V, uint32_t T,
+               cudaStream_t s);
+int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, uint32_t V,
+                      bool computeNextRotations, cudaStream_t s);
+int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool glob,
+                   bool bodyCorrection, uint32_t bodies, cudaStream_t s);
+
+uint32_t gateBlockCount(uint32_t V, uint32_t T);
+uint32_t convBlockCount(uint32_t V);
+
+}  // namespace jgs2

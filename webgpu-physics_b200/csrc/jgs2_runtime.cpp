@@ -1,0 +1,1269 @@
+// Host runtime of the JGS2 step: the C-ABI of include/jgs2.h.
+//
+// Restates the host half of `class JGS2GpuSolver`
+// (src/simulation/gpu/jgs2-solver.ts:905-3051): settings resolution and
+// validation (:429-550), input validation (layout.ts:223-416), greedy
+// colouring (:308-367 with src/simulation/cpu/vertex-coloring.ts:20-110),
+// create-time feasibility checks (:1041-1083, 820-893), the per-frame
+// dispatch order (:2207-2494) and the objective / readback API
+// (:1576-1760, 2501-2604).  Device work is issued on one CUDA stream per
+// solver; each frame shape is captured once into a CUDA graph and replayed.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <map>
+#include <memory>
+#include <mutex>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "jgs2.h"
+#include "jgs2_kernels.cuh"
+
+namespace {
+
+using jgs2::Buffers;
+using jgs2::DevParams;
+using jgs2::FrameState;
+
+constexpr float kDeterminantFloor = 1e-4f;
+// jgs2-globalization.ts:40; compared in f32 because settings cross the ABI as f32.
+constexpr float kMaxRuntimeTolerance = 1e-3f;
+constexpr double kDegenerateSceneScale = 1e-12;    // jgs2-solver.ts:162
+constexpr uint32_t kEmptyTet = 0xffffffffu;
+
+thread_local std::string gGlobalError;
+
+struct Error {
+  jgs2_status status;
+  std::string message;
+};
+
+std::string format(const char* fmt, ...) {
+  char buf[1024];
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(buf, sizeof(buf), fmt, ap);
+  va_end(ap);
+  return buf;
+}
+
+// ---- settings ---------------------------------------------------------------
+
+void defaults(jgs2_settings* s) {
+  std::memset(s, 0, sizeof(*s));
+  s->schedule = JGS2_SCHEDULE_JACOBI;
+  s->iterations = 9;
+  s->timestep = static_cast<float>(1.0 / 60.0);
+  s->gravity[0] = 0.f;
+  s->gravity[1] = -9.81f;
+  s->gravity[2] = 0.f;
+  s->floor_height = 0.f;
+  s->floor_stiffness = 20000.f;
+  s->velocity_damping = 0.999f;
+  s->regularization = 1e-6f;
+  s->rotation_epsilon = 1e-7f;
+  s->max_step = 0.1f;
+  s->residual_tolerance = 1e-3f;
+  s->normalized_update_tolerance = 1e-3f;
+  s->contact_tangential_damping = 8.f;
+  s->contact_margin = 0.01f;
+  s->ipc_activation_distance = 0.05f;
+  s->ipc_minimum_distance = 0.001f;
+  s->ipc_barrier_stiffness = 0.f;
+  s->ipc_friction_coefficient = 0.f;
+  s->ipc_friction_velocity_epsilon = 0.01f;
+  s->ipc_step_safety = 0.9f;
+  s->horizontal_body_correction = 1;
+  s->parity_mode = 0;
+}
+
+void merge(jgs2_settings* out, const jgs2_settings* o, uint32_t m) {
+  if (!o) return;
+  if (m & JGS2_SET_SCHEDULE) out->schedule = o->schedule;
+  if (m & JGS2_SET_ITERATIONS) out->iterations = o->iterations;
+  if (m & JGS2_SET_TIMESTEP) out->timestep = o->timestep;
+  if (m & JGS2_SET_GRAVITY) std::memcpy(out->gravity, o->gravity, sizeof(out->gravity));
+  if (m & JGS2_SET_FLOOR_HEIGHT) out->floor_height = o->floor_height;
+  if (m & JGS2_SET_FLOOR_STIFFNESS) out->floor_stiffness = o->floor_stiffness;
+  if (m & JGS2_SET_VELOCITY_DAMPING) out->velocity_damping = o->velocity_damping;
+  if (m & JGS2_SET_REGULARIZATION) out->regularization = o->regularization;
+  if (m & JGS2_SET_ROTATION_EPSILON) out->rotation_epsilon = o->rotation_epsilon;
+  if (m & JGS2_SET_MAX_STEP) out->max_step = o->max_step;
+  if (m & JGS2_SET_RESIDUAL_TOLERANCE) out->residual_tolerance = o->residual_tolerance;
+  if (m & JGS2_SET_NORMALIZED_UPDATE_TOLERANCE) out->normalized_update_tolerance = o->normalized_update_tolerance;
+  if (m & JGS2_SET_CONTACT_TANGENTIAL_DAMPING) out->contact_tangential_damping = o->contact_tangential_damping;
+  if (m & JGS2_SET_CONTACT_MARGIN) out->contact_margin = o->contact_margin;
+  if (m & JGS2_SET_IPC_ACTIVATION_DISTANCE) out->ipc_activation_distance = o->ipc_activation_distance;
+  if (m & JGS2_SET_IPC_MINIMUM_DISTANCE) out->ipc_minimum_distance = o->ipc_minimum_distance;
+  if (m & JGS2_SET_IPC_BARRIER_STIFFNESS) out->ipc_barrier_stiffness = o->ipc_barrier_stiffness;
+  if (m & JGS2_SET_IPC_FRICTION_COEFFICIENT) out->ipc_friction_coefficient = o->ipc_friction_coefficient;
+  if (m & JGS2_SET_IPC_FRICTION_VELOCITY_EPSILON)
+    out->ipc_friction_velocity_epsilon = o->ipc_friction_velocity_epsilon;
+  if (m & JGS2_SET_IPC_STEP_SAFETY) out->ipc_step_safety = o->ipc_step_safety;
+  if (m & JGS2_SET_HORIZONTAL_BODY_CORRECTION) out->horizontal_body_correction = o->horizontal_body_correction;
+  if (m & JGS2_SET_PARITY_MODE) out->parity_mode = o->parity_mode;
+}
+
+bool finite(float v) { return std::isfinite(v); }
+
+// validateStepSettings (src/simulation/gpu/jgs2-solver.ts:429-529).
+bool validateSettings(const jgs2_settings& s, std::string* err) {
+  if (s.schedule != JGS2_SCHEDULE_JACOBI && s.schedule != JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL) {
+    *err = format("Unknown JGS2 schedule: %u.", s.schedule);
+    return false;
+  }
+  const std::pair<const char*, float> values[] = {
+      {"timestep", s.timestep}, {"floorHeight", s.floor_height}, {"floorStiffness", s.floor_stiffness},
+      {"velocityDamping", s.velocity_damping}, {"regularization", s.regularization},
+      {"rotationEpsilon", s.rotation_epsilon}, {"maxStep", s.max_step},
+      {"residualTolerance", s.residual_tolerance}, {"normalizedUpdateTolerance", s.normalized_update_tolerance},
+      {"contactTangentialDamping", s.contact_tangential_damping}, {"contactMargin", s.contact_margin},
+      {"ipcActivationDistance", s.ipc_activation_distance}, {"ipcMinimumDistance", s.ipc_minimum_distance},
+      {"ipcBarrierStiffness", s.ipc_barrier_stiffness}, {"ipcFrictionCoefficient", s.ipc_friction_coefficient},
+      {"ipcFrictionVelocityEpsilon", s.ipc_friction_velocity_epsilon}, {"ipcStepSafety", s.ipc_step_safety},
+      {"gravity.x", s.gravity[0]}, {"gravity.y", s.gravity[1]}, {"gravity.z", s.gravity[2]}};
+  for (const auto& kv : values)
+    if (!finite(kv.second)) { *err = format("%s must be finite; got %g.", kv.first, kv.second); return false; }
+  if (!(s.timestep > 0)) { *err = "timestep must be positive."; return false; }
+  if (s.floor_stiffness < 0) { *err = "floorStiffness must be nonnegative."; return false; }
+  if (s.velocity_damping < 0 || s.velocity_damping > 1) { *err = "velocityDamping must be between zero and one."; return false; }
+  if (!(s.regularization > 0)) { *err = "regularization must be positive."; return false; }
+  if (!(s.rotation_epsilon > 0)) { *err = "rotationEpsilon must be positive."; return false; }
+  if (s.max_step < 0) { *err = "maxStep must be nonnegative."; return false; }
+  if (!(s.residual_tolerance > 0) || s.residual_tolerance > kMaxRuntimeTolerance) {
+    *err = format("residualTolerance must be positive and no greater than %g.", kMaxRuntimeTolerance);
+    return false;
+  }
+  if (!(s.normalized_update_tolerance > 0) || s.normalized_update_tolerance > kMaxRuntimeTolerance) {
+    *err = format("normalizedUpdateTolerance must be positive and no greater than %g.", kMaxRuntimeTolerance);
+    return false;
+  }
+  if (s.contact_tangential_damping < 0) { *err = "contactTangentialDamping must be finite and nonnegative."; return false; }
+  if (s.contact_margin < 0) { *err = "contactMargin must be finite and nonnegative."; return false; }
+  if (!(s.ipc_activation_distance > 0)) { *err = "ipcActivationDistance must be positive."; return false; }
+  if (s.ipc_minimum_distance < 0 || s.ipc_minimum_distance >= s.ipc_activation_distance) {
+    *err = "ipcMinimumDistance must be nonnegative and below ipcActivationDistance.";
+    return false;
+  }
+  if (s.ipc_barrier_stiffness < 0) { *err = "ipcBarrierStiffness must be nonnegative."; return false; }
+  if (s.ipc_friction_coefficient < 0) { *err = "ipcFrictionCoefficient must be nonnegative."; return false; }
+  if (!(s.ipc_friction_velocity_epsilon > 0)) { *err = "ipcFrictionVelocityEpsilon must be positive."; return false; }
+  if (!(s.ipc_step_safety > 0) || !(s.ipc_step_safety < 1)) {
+    *err = "ipcStepSafety must be strictly between zero and one.";
+    return false;
+  }
+  if (s.horizontal_body_correction > 1) { *err = "horizontalBodyCorrection must be a boolean."; return false; }
+  if (s.parity_mode > 1) { *err = "parityMode must be a boolean."; return false; }
+  return true;
+}
+
+// resolveJGS2StepSettings (src/simulation/gpu/jgs2-solver.ts:531-550).
+bool resolve(const jgs2_settings& base, const jgs2_settings* o, uint32_t mask, jgs2_settings* out,
+             std::string* err) {
+  *out = base;
+  merge(out, o, mask);
+  if (out->parity_mode) {
+    out->velocity_damping = 1.f;
+    out->contact_tangential_damping = 0.f;
+    out->horizontal_body_correction = 0;
+  }
+  return validateSettings(*out, err);
+}
+
+// ---- input validation (src/simulation/gpu/layout.ts:223-416) ---------------
+
+bool validateInput(const jgs2_input* in, std::string* err) {
+  if (!in) { *err = "input is NULL."; return false; }
+  const uint32_t V = in->vertex_count, T = in->tet_count, K = in->cubature_k;
+  if (V < 1) { *err = format("vertexCount must be an integer >= 1; got %u.", V); return false; }
+  if (T < 1) { *err = format("tetCount must be an integer >= 1; got %u.", T); return false; }
+  if (!in->positions || !in->vertex_rest || !in->vertex_info || !in->tet_indices || !in->tet_inverse_dm ||
+      !in->tet_meta || !in->adjacency || (K > 0 && (!in->cubature_tet_ids || !in->cubature_weights ||
+                                                    !in->cubature_basis))) {
+    *err = "A required input array is NULL.";
+    return false;
+  }
+  if (V >= (1u << 30) || T >= (1u << 30)) { *err = "vertexCount and tetCount must be below 2^30."; return false; }
+  if ((in->target_positions == nullptr) != (in->target_stiffnesses == nullptr)) {
+    *err = "objectives.targetPositions and objectives.targetStiffnesses must be provided together.";
+    return false;
+  }
+  auto finiteArray = [&](const float* a, size_t n, const char* name) {
+    if (!a) return true;
+    for (size_t i = 0; i < n; ++i)
+      if (!std::isfinite(a[i])) { *err = format("%s[%zu] must be finite.", name, i); return false; }
+    return true;
+  };
+  if (!finiteArray(in->positions, 4ull * V, "positions") || !finiteArray(in->velocities, 4ull * V, "velocities") ||
+      !finiteArray(in->vertex_rest, 4ull * V, "vertexRest") ||
+      !finiteArray(in->vertex_colors, 4ull * V, "vertexColors") ||
+      !finiteArray(in->external_forces, 3ull * V, "objectives.externalForces") ||
+      !finiteArray(in->target_positions, 3ull * V, "objectives.targetPositions") ||
+      !finiteArray(in->target_stiffnesses, V, "objectives.targetStiffnesses") ||
+      !finiteArray(in->tet_inverse_dm, 12ull * T, "tetInverseDm") || !finiteArray(in->tet_meta, 4ull * T, "tetMeta") ||
+      !finiteArray(in->tet_rest_stiffness, 144ull * T, "tetRestStiffness") ||
+      !finiteArray(in->cubature_weights, static_cast<size_t>(V) * K, "cubatureWeights") ||
+      !finiteArray(in->cubature_basis, static_cast<size_t>(V) * K * 36, "cubatureBasis"))
+    return false;
+  if (in->target_stiffnesses)
+    for (uint32_t v = 0; v < V; ++v)
+      if (in->target_stiffnesses[v] < 0) {
+        *err = format("objectives.targetStiffnesses[%u] must be nonnegative.", v);
+        return false;
+      }
+  for (uint32_t v = 0; v < V; ++v) {
+    if (in->vertex_info[4ull * v + 2] == 0) continue;
+    const bool force = in->external_forces && (in->external_forces[3ull * v] != 0 ||
+                                               in->external_forces[3ull * v + 1] != 0 ||
+                                               in->external_forces[3ull * v + 2] != 0);
+    const bool target = in->target_stiffnesses && in->target_stiffnesses[v] != 0;
+    if (force || target) {
+      *err = format("Pinned vertex %u cannot have a nonzero external force or quadratic-target stiffness.", v);
+      return false;
+    }
+  }
+  uint32_t maxBody = 0;
+  for (uint32_t v = 0; v < V; ++v) maxBody = std::max(maxBody, in->vertex_info[4ull * v + 3]);
+  if (static_cast<uint64_t>(maxBody) + 1 > V) {
+    *err = format("vertexInfo body ids must be compact nonnegative values whose maximum is smaller than "
+                  "vertexCount (%u); got %u.", V, maxBody);
+    return false;
+  }
+  for (size_t i = 0; i < 4ull * T; ++i)
+    if (in->tet_indices[i] >= V) {
+      *err = format("tetIndices[%zu] references vertex %u, but vertexCount is %u.", i, in->tet_indices[i], V);
+      return false;
+    }
+  bool anyCorotated = false;
+  for (uint32_t t = 0; t < T; ++t) {
+    const float vol = in->tet_meta[4ull * t], lambda = in->tet_meta[4ull * t + 1], mu = in->tet_meta[4ull * t + 2];
+    const float model = in->tet_meta[4ull * t + 3];
+    if (!(vol > 0) || !(mu > 0)) {
+      *err = format("tetMeta for tetrahedron %u requires positive volume and mu.", t);
+      return false;
+    }
+    if (model != 0.0f && model != 1.0f) {
+      *err = format("tetMeta for tetrahedron %u has unknown material model %g.", t, model);
+      return false;
+    }
+    if (model == 1.0f && !(lambda > 0)) {
+      *err = format("Stable Neo-Hookean tetMeta for tetrahedron %u requires positive lambda.", t);
+      return false;
+    }
+    if (model == 0.0f) {
+      anyCorotated = true;
+      if (!(3 * lambda + 2 * mu > 0)) {
+        *err = format("Co-rotated tetMeta for tetrahedron %u requires positive bulk modulus.", t);
+        return false;
+      }
+    }
+  }
+  if (anyCorotated && !in->tet_rest_stiffness) {
+    *err = "tetRestStiffness is required when any tetrahedron is co-rotated.";
+    return false;
+  }
+  for (uint64_t i = 0; i < in->adjacency_length; ++i)
+    if (in->adjacency[i] >= T) {
+      *err = format("adjacency[%llu] references tetrahedron %u, but tetCount is %u.",
+                    static_cast<unsigned long long>(i), in->adjacency[i], T);
+      return false;
+    }
+  // Canonical CSR of unique incident tets (layout.ts:359-398).
+  std::vector<uint32_t> counts(V, 0), last(V, kEmptyTet);
+  for (uint32_t t = 0; t < T; ++t)
+    for (int l = 0; l < 4; ++l) {
+      const uint32_t v = in->tet_indices[4ull * t + l];
+      if (last[v] != t) { counts[v]++; last[v] = t; }
+    }
+  uint64_t offset = 0;
+  std::vector<uint64_t> starts(V);
+  for (uint32_t v = 0; v < V; ++v) {
+    const uint32_t start = in->vertex_info[4ull * v], count = in->vertex_info[4ull * v + 1];
+    if (static_cast<uint64_t>(start) + count > in->adjacency_length) {
+      *err = format("vertexInfo for vertex %u addresses adjacency range [%u, %llu), beyond %llu.", v, start,
+                    static_cast<unsigned long long>(start) + count,
+                    static_cast<unsigned long long>(in->adjacency_length));
+      return false;
+    }
+    if (start != offset) {
+      *err = format("vertexInfo for vertex %u must start at canonical adjacency offset %llu; got %u.", v,
+                    static_cast<unsigned long long>(offset), start);
+      return false;
+    }
+    if (count != counts[v]) {
+      *err = format("vertexInfo for vertex %u must list exactly %u unique incident tetrahedra; got %u.", v,
+                    counts[v], count);
+      return false;
+    }
+    starts[v] = offset;
+    offset += count;
+    const float mass = in->vertex_rest[4ull * v + 3];
+    if (in->vertex_info[4ull * v + 2] == 0 && !(mass > 0)) {
+      *err = format("Unpinned vertex %u must have positive mass.", v);
+      return false;
+    }
+  }
+  if (offset != in->adjacency_length) {
+    *err = format("adjacency contains %llu unused entries.",
+                  static_cast<unsigned long long>(in->adjacency_length - offset));
+    return false;
+  }
+  {
+    std::vector<uint64_t> cursor(starts);
+    std::fill(last.begin(), last.end(), kEmptyTet);
+    for (uint32_t t = 0; t < T; ++t)
+      for (int l = 0; l < 4; ++l) {
+        const uint32_t v = in->tet_indices[4ull * t + l];
+        if (last[v] == t) continue;
+        last[v] = t;
+        const uint64_t at = cursor[v]++;
+        if (in->adjacency[at] != t) {
+          *err = format("adjacency[%llu] for vertex %u must equal incident tetrahedron %u; got %u.",
+                        static_cast<unsigned long long>(at), v, t, in->adjacency[at]);
+          return false;
+        }
+      }
+  }
+  const size_t R = static_cast<size_t>(V) * K;
+  for (size_t r = 0; r < R; ++r) {
+    const float w = in->cubature_weights[r];
+    const uint32_t t = in->cubature_tet_ids[r];
+    if (w < 0) { *err = format("cubatureWeights[%zu] must be nonnegative.", r); return false; }
+    if (w > 0 && t >= T) {
+      *err = format("Positive cubature record %zu references tetrahedron %u, but tetCount is %u.", r, t, T);
+      return false;
+    }
+  }
+  return true;
+}
+
+// buildJGS2InputVertexColoring + buildGreedyVertexColoring.
+std::vector<uint32_t> colorInput(const jgs2_input* in, uint32_t* count) {
+  const uint32_t V = in->vertex_count;
+  // Conflict adjacency as CSR built from the groups in the reference order.
+  std::vector<std::vector<uint32_t>> adj(V);
+  auto group = [&](const uint32_t* g, int n) {
+    uint32_t u[8];
+    int m = 0;
+    for (int i = 0; i < n; ++i) {
+      bool seen = false;
+      for (int j = 0; j < m; ++j) seen |= u[j] == g[i];
+      if (!seen) u[m++] = g[i];
+    }
+    for (int a = 0; a < m; ++a)
+      for (int b = a + 1; b < m; ++b) {
+        adj[u[a]].push_back(u[b]);
+        adj[u[b]].push_back(u[a]);
+      }
+  };
+  for (uint32_t t = 0; t < in->tet_count; ++t) group(&in->tet_indices[4ull * t], 4);
+  for (uint32_t v = 0; v < V; ++v)
+    for (uint32_t s = 0; s < in->cubature_k; ++s) {
+      const size_t r = static_cast<size_t>(v) * in->cubature_k + s;
+      const uint32_t t = in->cubature_tet_ids[r];
+      if (t == kEmptyTet || !(in->cubature_weights[r] > 0)) continue;
+      const uint32_t g[5] = {v, in->tet_indices[4ull * t], in->tet_indices[4ull * t + 1],
+                             in->tet_indices[4ull * t + 2], in->tet_indices[4ull * t + 3]};
+      group(g, 5);
+    }
+  std::vector<uint32_t> colors(V, 0xffffffffu), stamp(V + 1, 0);
+  uint32_t n = 0, st = 0;
+  for (uint32_t v = 0; v < V; ++v) {
+    st += 1;
+    for (uint32_t u : adj[v])
+      if (colors[u] != 0xffffffffu) stamp[colors[u]] = st;
+    uint32_t c = 0;
+    while (c < n && stamp[c] == st) c += 1;
+    colors[v] = c;
+    n = std::max(n, c + 1);
+  }
+  *count = n;
+  return colors;
+}
+
+// minimumJGS2InputDeformationDeterminant (src/simulation/gpu/layout.ts:541-583).
+double minimumInputDeterminant(const jgs2_input* in) {
+  auto det = [](double a0, double a1, double a2, double b0, double b1, double b2, double c0, double c1, double c2) {
+    return a0 * (b1 * c2 - b2 * c1) - b0 * (a1 * c2 - a2 * c1) + c0 * (a1 * b2 - a2 * b1);
+  };
+  double m = INFINITY;
+  for (uint32_t t = 0; t < in->tet_count; ++t) {
+    const uint32_t* q = &in->tet_indices[4ull * t];
+    const float* p = in->positions;
+    const double ds = det(p[4 * q[1]] - p[4 * q[0]], p[4 * q[1] + 1] - p[4 * q[0] + 1], p[4 * q[1] + 2] - p[4 * q[0] + 2],
+                          p[4 * q[2]] - p[4 * q[0]], p[4 * q[2] + 1] - p[4 * q[0] + 1], p[4 * q[2] + 2] - p[4 * q[0] + 2],
+                          p[4 * q[3]] - p[4 * q[0]], p[4 * q[3] + 1] - p[4 * q[0] + 1], p[4 * q[3] + 2] - p[4 * q[0] + 2]);
+    const float* d = &in->tet_inverse_dm[12ull * t];
+    const double di = det(d[0], d[1], d[2], d[4], d[5], d[6], d[8], d[9], d[10]);
+    const double v = ds * di;
+    if (!std::isfinite(v)) return v;
+    m = std::min(m, v);
+  }
+  return m;
+}
+
+}  // namespace
+
+// ---- solver -------------------------------------------------------------------
+
+struct jgs2_solver {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool destroyed = false;
+  std::string error;
+  uint32_t V = 0, T = 0, K = 0, bodies = 1;
+  bool glob = true;
+  float sceneScale = 1.f;
+  float preprocessingTimestep = 0.f;
+  jgs2_settings defaults{};
+  jgs2_settings submitted{};
+  uint32_t submittedIterations = 0;
+  bool recordsAvailable = false;
+  // colouring
+  uint32_t colorCount = 1;
+  std::vector<uint32_t> colors;
+  std::vector<uint32_t> colorOffsets;   // colorCount + 1 into colorVertices
+  std::vector<uint32_t> needOffsets;    // colorCount + 1 into needVertices
+  // objectives (host mirror: force xyz, 0, target xyz, stiffness)
+  std::vector<float> objectives;
+  std::vector<uint8_t> pinned;
+  uint32_t objectiveFlags = 0, forceCount = 0, targetCount = 0, objectiveRevision = 0;
+  // device
+  Buffers b{};
+  DevParams* dParams = nullptr;
+  uint32_t* dColorVertices = nullptr;
+  uint32_t* dNeedVertices = nullptr;
+  std::vector<void*> allocations;
+  uint64_t launches = 0;
+  // graphs: (iterations, schedule, bodyCorrection) -> exec, launches per replay
+  std::map<std::tuple<uint32_t, uint32_t, bool>, std::pair<cudaGraphExec_t, int>> graphs;
+  bool useGraphs = true;
+};
+
+namespace {
+
+jgs2_status fail(jgs2_solver* s, jgs2_status st, const std::string& msg) {
+  if (s) s->error = msg;
+  else gGlobalError = msg;
+  return st;
+}
+
+jgs2_status cudaFail(jgs2_solver* s, cudaError_t e, const char* what) {
+  return fail(s, e == cudaErrorMemoryAllocation ? JGS2_OUT_OF_MEMORY : JGS2_DEVICE_ERROR,
+              format("%s: %s", what, cudaGetErrorString(e)));
+}
+
+#define CUDA_TRY(s, call)                               \
+  do {                                                  \
+    cudaError_t _e = (call);                            \
+    if (_e != cudaSuccess) return cudaFail((s), _e, #call); \
+  } while (0)
+
+template <class T>
+jgs2_status deviceAlloc(jgs2_solver* s, T** out, size_t count) {
+  void* p = nullptr;
+  const size_t bytes = std::max<size_t>(16, count * sizeof(T));
+  cudaError_t e = cudaMalloc(&p, bytes);
+  if (e != cudaSuccess) return cudaFail(s, e, "cudaMalloc");
+  s->allocations.push_back(p);
+  *out = static_cast<T*>(p);
+  return JGS2_OK;
+}
+
+template <class T>
+jgs2_status upload(jgs2_solver* s, T** out, const T* host, size_t count) {
+  jgs2_status st = deviceAlloc(s, out, count);
+  if (st != JGS2_OK) return st;
+  if (count) CUDA_TRY(s, cudaMemcpyAsync(*out, host, count * sizeof(T), cudaMemcpyHostToDevice, s->stream));
+  return JGS2_OK;
+}
+
+void releaseDevice(jgs2_solver* s) {
+  for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second.first);
+  s->graphs.clear();
+  if (s->stream) cudaStreamSynchronize(s->stream);
+  for (void* p : s->allocations) cudaFree(p);
+  s->allocations.clear();
+  if (s->stream) cudaStreamDestroy(s->stream);
+  s->stream = nullptr;
+}
+
+void refreshObjectiveActivity(jgs2_solver* s) {
+  uint32_t f = 0, t = 0;
+  for (uint32_t v = 0; v < s->V; ++v) {
+    const float* o = &s->objectives[8ull * v];
+    if (o[0] != 0 || o[1] != 0 || o[2] != 0) f++;
+    if (o[7] > 0) t++;
+  }
+  s->forceCount = f;
+  s->targetCount = t;
+  s->objectiveFlags = (f ? 1u : 0u) | (t ? 2u : 0u);
+}
+
+DevParams makeParams(const jgs2_solver* s, const jgs2_settings& st, bool stop) {
+  DevParams p{};
+  // packUniforms (jgs2-solver.ts:604-730): (dt, 1/dt, 1/dt^2) formed in
+  // double from the timestep and stored as f32.
+  const double dt = st.timestep;
+  const double inv = 1.0 / dt;
+  p.dt = static_cast<float>(dt);
+  p.invDt = static_cast<float>(inv);
+  p.invDt2 = static_cast<float>(inv * inv);
+  p.maxStep = st.max_step;
+  for (int i = 0; i < 3; ++i) p.gravity[i] = st.gravity[i];
+  p.floorHeight = st.floor_height;
+  p.floorStiffness = st.floor_stiffness;
+  p.regularization = st.regularization;
+  p.rotationEpsilon = st.rotation_epsilon;
+  p.velocityDamping = st.velocity_damping;
+  p.contactTangentialDamping = st.contact_tangential_damping;
+  p.contactMargin = st.contact_margin;
+  p.residualTolerance = st.residual_tolerance;
+  p.normalizedUpdateTolerance = st.normalized_update_tolerance;
+  p.sceneScale = s->sceneScale;
+  p.objectiveFlags = s->objectiveFlags;
+  p.stopEnabled = (s->glob && stop) ? 1u : 0u;
+  p.globalization = s->glob ? 1u : 0u;
+  p.historyCapacity = JGS2_HISTORY_CAPACITY;
+  p.vertexCount = s->V;
+  p.tetCount = s->T;
+  p.cubatureK = s->K;
+  p.bodyCount = s->bodies;
+  return p;
+}
+
+// encodeFrame (src/simulation/gpu/jgs2-solver.ts:2207-2494) on the stream.
+int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bodyCorrection) {
+  const Buffers& b = s->b;
+  cudaStream_t st = s->stream;
+  int n = 0;
+  n += jgs2::launchPrologue(b, s->dParams, s->V, s->T, s->glob, st);
+  if (!s->glob) n += jgs2::launchVertexPolar(b, s->dParams, b.pos[1], nullptr, s->V, st);
+  const bool colored = schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL;
+  for (uint32_t it = 0; it < iterations; ++it) {
+    float4* src = (it % 2 == 0) ? b.pos[1] : b.pos[0];
+    float4* tgt = (it % 2 == 0) ? b.pos[0] : b.pos[1];
+    const bool last = it + 1 == iterations;
+    if (colored) {
+      n += jgs2::launchCopy(src, tgt, s->V, st);
+      for (uint32_t c = 0; c < s->colorCount; ++c) {
+        if (!s->glob) n += jgs2::launchTetPolar(b, s->dParams, tgt, s->T, st);
+        const uint32_t nb = s->needOffsets[c], ne = s->needOffsets[c + 1];
+        if (last && c + 1 == s->colorCount)
+          n += jgs2::launchVertexPolar(b, s->dParams, tgt, nullptr, s->V, st);
+        else
+          n += jgs2::launchVertexPolar(b, s->dParams, tgt, s->dNeedVertices + nb, ne - nb, st);
+        const uint32_t cb = s->colorOffsets[c], ce = s->colorOffsets[c + 1];
+        n += jgs2::launchSolve(b, s->dParams, tgt, tgt, s->dColorVertices + cb, ce - cb, s->K, s->glob, st);
+      }
+    } else {
+      if (!s->glob) {
+        n += jgs2::launchTetPolar(b, s->dParams, src, s->T, st);
+        if (it > 0) n += jgs2::launchVertexPolar(b, s->dParams, src, nullptr, s->V, st);
+      }
+      n += jgs2::launchSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, s->glob, st);
+    }
+    if (s->glob) {
+      n += jgs2::launchGate(b, s->dParams, src, tgt, s->V, s->T, st);
+      n += jgs2::launchConvergence(b, s->dParams, src, tgt, s->V, !colored && !last, st);
+    }
+  }
+  const float4* finalPos = (iterations % 2 == 0) ? b.pos[1] : b.pos[0];
+  n += jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, s->glob, bodyCorrection, s->bodies, st);
+  return n;
+}
+
+jgs2_status runFrames(jgs2_solver* s, const jgs2_settings& st, uint32_t frames, uint32_t iterations, bool stop) {
+  if (s->glob && iterations > JGS2_HISTORY_CAPACITY)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("Stable JGS2 records at most %u nonlinear iterations per frame; got %u.",
+                       JGS2_HISTORY_CAPACITY, iterations));
+  if (s->glob) {
+    const uint32_t sub = st.schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL ? s->colorCount : 1u;
+    if (static_cast<uint64_t>(iterations) * sub > JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION / frames)
+      return fail(s, JGS2_INVALID_ARGUMENT,
+                  format("Stable JGS2 may encode at most %u total nonlinear iterations per submission; got %u "
+                         "frames * %u iterations.",
+                         JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION, frames, iterations * sub));
+  }
+  const DevParams p = makeParams(s, st, stop);
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaMemcpyAsync(s->dParams, &p, sizeof(p), cudaMemcpyHostToDevice, s->stream));
+  const bool body = st.horizontal_body_correction != 0;
+  const auto key = std::make_tuple(iterations, st.schedule, body);
+  if (s->useGraphs) {
+    auto it = s->graphs.find(key);
+    if (it == s->graphs.end()) {
+      cudaGraph_t graph = nullptr;
+      CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
+      const int n = encodeFrame(s, iterations, st.schedule, body);
+      cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
+      if (e != cudaSuccess) return cudaFail(s, e, "cudaStreamEndCapture");
+      cudaGraphExec_t exec = nullptr;
+      e = cudaGraphInstantiate(&exec, graph, 0);
+      cudaGraphDestroy(graph);
+      if (e != cudaSuccess) return cudaFail(s, e, "cudaGraphInstantiate");
+      it = s->graphs.emplace(key, std::make_pair(exec, n)).first;
+    }
+    for (uint32_t f = 0; f < frames; ++f) {
+      CUDA_TRY(s, cudaGraphLaunch(it->second.first, s->stream));
+      s->launches += static_cast<uint64_t>(it->second.second);
+    }
+  } else {
+    for (uint32_t f = 0; f < frames; ++f) s->launches += encodeFrame(s, iterations, st.schedule, body);
+  }
+  CUDA_TRY(s, cudaGetLastError());
+  s->submitted = st;
+  s->submittedIterations = iterations;
+  if (s->glob) s->recordsAvailable = true;
+  return JGS2_OK;
+}
+
+uint32_t normalizeOdd(uint32_t it) {
+  const uint32_t i = std::max(1u, it);
+  return i % 2 == 0 ? i + 1 : i;
+}
+
+jgs2_status stepCommon(jgs2_solver* s, uint32_t frames, int exactIterations, const jgs2_settings* o,
+                       uint32_t mask, bool batch) {
+  if (!s) return fail(nullptr, JGS2_INVALID_ARGUMENT, "solver is NULL.");
+  if (s->destroyed) return fail(s, JGS2_DESTROYED, "JGS2GpuSolver has been destroyed.");
+  if (batch && (frames < 1 || frames > JGS2_MAX_BATCH_FRAMES))
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("frameCount must be a positive safe integer no greater than %u; got %u.",
+                       JGS2_MAX_BATCH_FRAMES, frames));
+  if (exactIterations == 0) return fail(s, JGS2_INVALID_ARGUMENT, "iterations must be a positive safe integer; got 0.");
+  if (o && (mask & JGS2_SET_TIMESTEP) && static_cast<float>(o->timestep) != s->preprocessingTimestep)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("JGS2 was precomputed for timestep %g, but the step requested %g. Regenerate the "
+                       "precomputation before changing timestep.",
+                       s->preprocessingTimestep, o->timestep));
+  // resolveStepSettings (jgs2-solver.ts:1974-2005).
+  if (o && (mask & JGS2_SET_IPC_MINIMUM_DISTANCE) && o->ipc_minimum_distance != s->defaults.ipc_minimum_distance &&
+      false /* no IPC candidates in this build */)
+    return fail(s, JGS2_INVALID_ARGUMENT, "ipcMinimumDistance is fixed when an IPC solver is created.");
+  jgs2_settings st;
+  std::string err;
+  if (!resolve(s->defaults, o, mask, &st, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
+  if (s->glob && s->objectiveFlags != 0 && st.horizontal_body_correction) st.horizontal_body_correction = 0;
+  const bool production = exactIterations < 0;
+  const uint32_t iterations = production ? normalizeOdd(st.iterations) : static_cast<uint32_t>(exactIterations);
+  return runFrames(s, st, frames, iterations, production);
+}
+
+jgs2_status readRegion(jgs2_solver* s, const void* dev, size_t bytes, void* host) {
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return JGS2_OK;
+}
+
+jgs2_status usable(jgs2_solver* s) {
+  if (!s) return fail(nullptr, JGS2_INVALID_ARGUMENT, "solver is NULL.");
+  if (s->destroyed) return fail(s, JGS2_DESTROYED, "JGS2GpuSolver has been destroyed.");
+  return JGS2_OK;
+}
+
+jgs2_status writeObjectives(jgs2_solver* s, uint32_t firstVertex, uint32_t vertexCount) {
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaMemcpyAsync(s->b.objectives + 2ull * firstVertex, &s->objectives[8ull * firstVertex],
+                              32ull * vertexCount, cudaMemcpyHostToDevice, s->stream));
+  refreshObjectiveActivity(s);
+  s->objectiveRevision += 1;
+  return JGS2_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+uint32_t jgs2_version(void) { return JGS2_ABI_VERSION; }
+
+const char* jgs2_build_string(void) {
+  return "jgs2-b200 sm_100a (CUDA " __DATE__ ")";
+}
+
+const char* jgs2_global_last_error(void) { return gGlobalError.c_str(); }
+
+void jgs2_default_settings(jgs2_settings* out) {
+  if (out) defaults(out);
+}
+
+jgs2_status jgs2_resolve_settings(const jgs2_settings* base, const jgs2_settings* overrides, uint32_t mask,
+                                  jgs2_settings* out) {
+  if (!out) return fail(nullptr, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  jgs2_settings d;
+  defaults(&d);
+  std::string err;
+  if (!resolve(base ? *base : d, overrides, mask, out, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_validate_input(const jgs2_input* input) {
+  std::string err;
+  if (!validateInput(input, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_build_vertex_coloring(const jgs2_input* input, uint32_t* colors, uint32_t* count) {
+  std::string err;
+  if (!validateInput(input, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  if (!colors || !count) return fail(nullptr, JGS2_INVALID_ARGUMENT, "output is NULL.");
+  const auto c = colorInput(input, count);
+  std::memcpy(colors, c.data(), c.size() * sizeof(uint32_t));
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uint32_t mask, int device,
+                        jgs2_solver** out) {
+  if (!out) return fail(nullptr, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  *out = nullptr;
+  std::string err;
+  if (!validateInput(in, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  // inferJGS2MaterialMode (layout.ts:509-522).
+  uint32_t stable = 0;
+  for (uint32_t t = 0; t < in->tet_count; ++t) stable += in->tet_meta[4ull * t + 3] == 1.0f ? 1u : 0u;
+  if (stable != 0 && stable != in->tet_count)
+    return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                "A production JGS2 solve cannot mix stable Neo-Hookean and co-rotated regression tetrahedra in one "
+                "precomputation.");
+  const bool glob = stable == in->tet_count;
+  if (!glob)
+    return fail(nullptr, JGS2_UNSUPPORTED,
+                "The co-rotated regression material path is not built into this library; use stable Neo-Hookean "
+                "tetrahedra.");
+  uint32_t colorCount = 0;
+  std::vector<uint32_t> colors = colorInput(in, &colorCount);
+  if (colorCount > JGS2_MAX_SCHEDULE_COLORS)
+    return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                format("Colored Gauss-Seidel supports at most %u colors; the small-scene conflict graph needs %u.",
+                       JGS2_MAX_SCHEDULE_COLORS, colorCount));
+  jgs2_settings base;
+  defaults(&base);
+  jgs2_settings resolved;
+  if (!resolve(base, settings, mask, &resolved, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  if (glob) {
+    const double m = minimumInputDeterminant(in);
+    if (!std::isfinite(m) || !(m > kDeterminantFloor))
+      return fail(nullptr, JGS2_INFEASIBLE_INPUT,
+                  format("A stable Neo-Hookean production solve requires an initially feasible pose with minimum J "
+                         "greater than %g; got %g.", kDeterminantFloor, m));
+  }
+  std::unique_ptr<jgs2_solver> s(new jgs2_solver());
+  s->device = device;
+  s->V = in->vertex_count;
+  s->T = in->tet_count;
+  s->K = in->cubature_k;
+  s->glob = glob;
+  s->defaults = resolved;
+  s->submitted = resolved;
+  s->preprocessingTimestep = resolved.timestep;
+  s->colors = colors;
+  s->colorCount = colorCount;
+  uint32_t maxBody = 0;
+  for (uint32_t v = 0; v < s->V; ++v) maxBody = std::max(maxBody, in->vertex_info[4ull * v + 3]);
+  s->bodies = maxBody + 1;
+  // computeJGS2InitialDynamicSceneScale (jgs2-solver.ts:732-768).
+  {
+    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+    uint32_t dyn = 0;
+    for (uint32_t v = 0; v < s->V; ++v) {
+      if (in->vertex_info[4ull * v + 2] != 0) continue;
+      dyn++;
+      for (int k = 0; k < 3; ++k) {
+        lo[k] = std::min(lo[k], static_cast<double>(in->positions[4ull * v + k]));
+        hi[k] = std::max(hi[k], static_cast<double>(in->positions[4ull * v + k]));
+      }
+    }
+    const double d = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                               (hi[2] - lo[2]) * (hi[2] - lo[2]));
+    s->sceneScale = static_cast<float>(dyn > 0 && std::isfinite(d) && d > 0 ? d : kDegenerateSceneScale);
+  }
+  // Objectives (packJGS2VertexObjectives, layout.ts:635-668).
+  s->objectives.assign(8ull * s->V, 0.f);
+  s->pinned.assign(s->V, 0);
+  for (uint32_t v = 0; v < s->V; ++v) {
+    float* o = &s->objectives[8ull * v];
+    if (in->external_forces)
+      for (int k = 0; k < 3; ++k) o[k] = in->external_forces[3ull * v + k];
+    for (int k = 0; k < 3; ++k)
+      o[4 + k] = in->target_positions ? in->target_positions[3ull * v + k] : in->positions[4ull * v + k];
+    o[7] = in->target_stiffnesses ? in->target_stiffnesses[v] : 0.f;
+    s->pinned[v] = in->vertex_info[4ull * v + 2] != 0;
+  }
+  refreshObjectiveActivity(s.get());
+  // Colour lists and per-colour frame lists.
+  std::vector<uint32_t> byColor(s->V);
+  s->colorOffsets.assign(colorCount + 1, 0);
+  for (uint32_t v = 0; v < s->V; ++v) s->colorOffsets[colors[v] + 1]++;
+  for (uint32_t c = 0; c < colorCount; ++c) s->colorOffsets[c + 1] += s->colorOffsets[c];
+  {
+    std::vector<uint32_t> cur(s->colorOffsets.begin(), s->colorOffsets.end() - 1);
+    for (uint32_t v = 0; v < s->V; ++v) byColor[cur[colors[v]]++] = v;
+  }
+  std::vector<uint32_t> need;
+  s->needOffsets.assign(colorCount + 1, 0);
+  {
+    std::vector<uint32_t> mark(s->V, 0xffffffffu);
+    for (uint32_t c = 0; c < colorCount; ++c) {
+      std::vector<uint32_t> list;
+      auto add = [&](uint32_t u) {
+        if (mark[u] != c) { mark[u] = c; list.push_back(u); }
+      };
+      for (uint32_t i = s->colorOffsets[c]; i < s->colorOffsets[c + 1]; ++i) {
+        const uint32_t v = byColor[i];
+        add(v);
+        for (uint32_t k = 0; k < s->K; ++k) {
+          const size_t r = static_cast<size_t>(v) * s->K + k;
+          const uint32_t t = in->cubature_tet_ids[r];
+          if (t == kEmptyTet || t >= s->T || !(in->cubature_weights[r] > 0)) continue;
+          for (int l = 0; l < 4; ++l) add(in->tet_indices[4ull * t + l]);
+        }
+      }
+      std::sort(list.begin(), list.end());
+      need.insert(need.end(), list.begin(), list.end());
+      s->needOffsets[c + 1] = static_cast<uint32_t>(need.size());
+    }
+  }
+  // Device packing.
+  jgs2_solver* sp = s.get();
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, format("cudaSetDevice: %s", cudaGetErrorString(ce)));
+  ce = cudaStreamCreateWithFlags(&sp->stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, format("cudaStreamCreate: %s", cudaGetErrorString(ce)));
+  auto bail = [&](jgs2_status st) {
+    gGlobalError = sp->error;
+    releaseDevice(sp);
+    return st;
+  };
+  const uint32_t V = s->V, T = s->T, K = s->K;
+  std::vector<float4> pos(V), rest(V);
+  std::vector<uint4> info(V);
+  for (uint32_t v = 0; v < V; ++v) {
+    pos[v] = make_float4(in->positions[4ull * v], in->positions[4ull * v + 1], in->positions[4ull * v + 2], 1.f);
+    rest[v] = make_float4(in->vertex_rest[4ull * v], in->vertex_rest[4ull * v + 1], in->vertex_rest[4ull * v + 2],
+                          in->vertex_rest[4ull * v + 3]);
+    info[v] = make_uint4(in->vertex_info[4ull * v], in->vertex_info[4ull * v + 1], in->vertex_info[4ull * v + 2],
+                         in->vertex_info[4ull * v + 3]);
+  }
+  std::vector<float4> vel(V, make_float4(0, 0, 0, 0));
+  if (in->velocities)
+    for (uint32_t v = 0; v < V; ++v)
+      vel[v] = make_float4(in->velocities[4ull * v], in->velocities[4ull * v + 1], in->velocities[4ull * v + 2], 0.f);
+  // Tet record: rows of inverse Dm (shape gradients g1..g3) with volume,
+  // lambda, mu in w, then the four indices.
+  std::vector<float4> tets(4ull * T);
+  for (uint32_t t = 0; t < T; ++t) {
+    const float* m = &in->tet_inverse_dm[12ull * t];
+    const float* meta = &in->tet_meta[4ull * t];
+    tets[4ull * t] = make_float4(m[0], m[4], m[8], meta[0]);
+    tets[4ull * t + 1] = make_float4(m[1], m[5], m[9], meta[1]);
+    tets[4ull * t + 2] = make_float4(m[2], m[6], m[10], meta[2]);
+    uint4 q = make_uint4(in->tet_indices[4ull * t], in->tet_indices[4ull * t + 1], in->tet_indices[4ull * t + 2],
+                         in->tet_indices[4ull * t + 3]);
+    std::memcpy(&tets[4ull * t + 3], &q, sizeof(q));
+  }
+  std::vector<uint32_t> adjacency(in->adjacency_length);
+  for (uint32_t v = 0; v < V; ++v) {
+    const uint32_t start = in->vertex_info[4ull * v], count = in->vertex_info[4ull * v + 1];
+    for (uint32_t a = 0; a < count; ++a) {
+      const uint32_t t = in->adjacency[start + a];
+      uint32_t slot = 0;
+      for (uint32_t l = 0; l < 4; ++l)
+        if (in->tet_indices[4ull * t + l] == v) { slot = l; break; }
+      adjacency[start + a] = t * 4u + slot;
+    }
+  }
+  const size_t R = static_cast<size_t>(V) * K;
+  std::vector<uint32_t> cubTet(in->cubature_tet_ids, in->cubature_tet_ids + R);
+  std::vector<float> cubW(in->cubature_weights, in->cubature_weights + R);
+  jgs2_status st = JGS2_OK;
+  Buffers& b = sp->b;
+#define STEP(x) do { st = (x); if (st != JGS2_OK) return bail(st); } while (0)
+  STEP(upload(sp, &b.pos[0], pos.data(), V));
+  STEP(upload(sp, &b.pos[1], pos.data(), V));
+  STEP(upload(sp, &b.predicted, pos.data(), V));
+  STEP(upload(sp, &b.old, pos.data(), V));
+  STEP(upload(sp, &b.velocity, vel.data(), V));
+  std::vector<float4> identity(3ull * V);
+  for (uint32_t v = 0; v < V; ++v) {
+    identity[3ull * v] = make_float4(1, 0, 0, 0);
+    identity[3ull * v + 1] = make_float4(0, 1, 0, 0);
+    identity[3ull * v + 2] = make_float4(0, 0, 1, 0);
+  }
+  STEP(upload(sp, &b.vertexRot, identity.data(), 3ull * V));
+  b.tetRot = nullptr;
+  STEP(deviceAlloc(sp, &b.finalUpdate, V));
+  STEP(deviceAlloc(sp, &b.local, 4ull * V));
+  CUDA_TRY(sp, cudaMemsetAsync(b.finalUpdate, 0, sizeof(float) * V, sp->stream));
+  CUDA_TRY(sp, cudaMemsetAsync(b.local, 0, sizeof(float4) * 4ull * V, sp->stream));
+  STEP(deviceAlloc(sp, &b.frame, 1));
+  {
+    FrameState fs;
+    std::memset(&fs, 0, sizeof(fs));
+    fs.gateMinSource = fs.gateMinCandidate = 0xffffffffu;  // encodes the largest float
+    fs.gateBits = 0xffffffffu;
+    fs.localNumericsValid = 1;
+    fs.convValid = 1;
+    // Encode +3e38 exactly as the kernels do.
+    uint32_t u;
+    const float big = 3.0e38f;
+    std::memcpy(&u, &big, 4);
+    fs.gateMinSource = fs.gateMinCandidate = u | 0x80000000u;
+    CUDA_TRY(sp, cudaMemcpyAsync(b.frame, &fs, sizeof(fs), cudaMemcpyHostToDevice, sp->stream));
+    CUDA_TRY(sp, cudaStreamSynchronize(sp->stream));
+  }
+  b.gateBlocks = jgs2::gateBlockCount(V, T);
+  b.convBlocks = jgs2::convBlockCount(V);
+  STEP(deviceAlloc(sp, &b.gatePartials, 2ull * b.gateBlocks));
+  STEP(deviceAlloc(sp, &b.convPartials, 6ull * b.convBlocks));
+  STEP(deviceAlloc(sp, &b.bodyAccum, 6ull * sp->bodies));
+  {
+    float4* p = nullptr;
+    STEP(upload(sp, &p, rest.data(), V));
+    b.restMass = p;
+    uint4* q = nullptr;
+    STEP(upload(sp, &q, info.data(), V));
+    b.vinfo = q;
+    float4* tt = nullptr;
+    STEP(upload(sp, &tt, tets.data(), 4ull * T));
+    b.tets = tt;
+    uint32_t* a = nullptr;
+    STEP(upload(sp, &a, adjacency.data(), adjacency.size()));
+    b.adjacency = a;
+    uint32_t* ct = nullptr;
+    STEP(upload(sp, &ct, cubTet.data(), R));
+    b.cubTet = ct;
+    float* cw = nullptr;
+    STEP(upload(sp, &cw, cubW.data(), R));
+    b.cubWeight = cw;
+    float4* cb = nullptr;
+    STEP(deviceAlloc(sp, &cb, 9 * R));
+    if (R) CUDA_TRY(sp, cudaMemcpyAsync(cb, in->cubature_basis, sizeof(float) * 36 * R, cudaMemcpyHostToDevice,
+                                        sp->stream));
+    b.cubBasis = cb;
+    b.stiffness = nullptr;
+    float4* ob = nullptr;
+    STEP(deviceAlloc(sp, &ob, 2ull * V));
+    b.objectives = ob;
+    CUDA_TRY(sp, cudaMemcpyAsync(ob, sp->objectives.data(), 32ull * V, cudaMemcpyHostToDevice, sp->stream));
+    uint32_t* cl = nullptr;
+    STEP(upload(sp, &cl, colors.data(), V));
+    b.colors = cl;
+    STEP(upload(sp, &sp->dColorVertices, byColor.data(), byColor.size()));
+    STEP(upload(sp, &sp->dNeedVertices, need.data(), need.size()));
+    STEP(deviceAlloc(sp, &sp->dParams, 1));
+  }
+#undef STEP
+  // GPU preflight of the uploaded pose (validateGpuInitialStableSource,
+  // jgs2-solver.ts:820-893): the gate on (posA, posA) must accept.
+  if (glob) {
+    DevParams p = makeParams(sp, resolved, false);
+    CUDA_TRY(sp, cudaMemcpyAsync(sp->dParams, &p, sizeof(p), cudaMemcpyHostToDevice, sp->stream));
+    jgs2::launchGate(b, sp->dParams, b.pos[0], b.pos[0], V, T, sp->stream);
+    sp->launches += 1;
+    float4 control[4];
+    CUDA_TRY(sp, cudaMemcpyAsync(control, b.frame->control, sizeof(control), cudaMemcpyDeviceToHost, sp->stream));
+    ce = cudaStreamSynchronize(sp->stream);
+    if (ce != cudaSuccess) { cudaFail(sp, ce, "preflight"); return bail(JGS2_DEVICE_ERROR); }
+    const uint32_t required = 1u | 2u | 4u;
+    const float vb = control[0].w;
+    const bool ok = std::isfinite(control[0].x) && std::isfinite(control[0].y) && std::isfinite(control[0].z) &&
+                    control[0].x > kDeterminantFloor && control[0].y > kDeterminantFloor &&
+                    control[0].z > kDeterminantFloor && vb == std::floor(vb) &&
+                    ((static_cast<uint32_t>(vb) & required) == required);
+    if (!ok) {
+      sp->error = format("The uploaded stable Neo-Hookean source pose is not feasible under the production GPU f32 "
+                         "determinant calculation; source J=%g, candidate J=%g, accepted J=%g.",
+                         control[0].x, control[0].y, control[0].z);
+      return bail(JGS2_INFEASIBLE_INPUT);
+    }
+  }
+  *out = s.release();
+  return JGS2_OK;
+}
+
+void jgs2_destroy(jgs2_solver* s) {
+  if (!s) return;
+  if (!s->destroyed) {
+    cudaSetDevice(s->device);
+    releaseDevice(s);
+    s->destroyed = true;
+  }
+  delete s;
+}
+
+const char* jgs2_last_error(const jgs2_solver* s) { return s ? s->error.c_str() : gGlobalError.c_str(); }
+
+jgs2_status jgs2_get_info(jgs2_solver* s, jgs2_info* out) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  std::memset(out, 0, sizeof(*out));
+  out->vertex_count = s->V;
+  out->tet_count = s->T;
+  out->cubature_k = s->K;
+  out->body_count = s->bodies;
+  out->schedule_color_count = s->colorCount;
+  out->globalization_enabled = s->glob ? 1 : 0;
+  out->objective_flags = s->objectiveFlags;
+  out->external_force_vertex_count = s->forceCount;
+  out->quadratic_target_vertex_count = s->targetCount;
+  out->objective_revision = s->objectiveRevision;
+  out->last_submitted_iterations = s->submittedIterations;
+  out->scene_scale = s->sceneScale;
+  out->preprocessing_timestep = s->preprocessingTimestep;
+  out->current_position_buffer = 0;
+  if (s->recordsAvailable) {
+    float4 c1;
+    if (readRegion(s, &s->b.frame->control[1], sizeof(c1), &c1) == JGS2_OK)
+      out->history_count = static_cast<uint32_t>(c1.w);
+  }
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_get_default_settings(jgs2_solver* s, jgs2_settings* out) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  *out = s->defaults;
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_get_last_submitted_settings(jgs2_solver* s, jgs2_settings* out) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  *out = s->submitted;
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_step(jgs2_solver* s, const jgs2_settings* o, uint32_t mask) {
+  return stepCommon(s, 1, -1, o, mask, false);
+}
+
+jgs2_status jgs2_step_frames(jgs2_solver* s, uint32_t frames, const jgs2_settings* o, uint32_t mask) {
+  return stepCommon(s, frames, -1, o, mask, true);
+}
+
+jgs2_status jgs2_step_exact_iterations(jgs2_solver* s, uint32_t iterations, const jgs2_settings* o, uint32_t mask) {
+  return stepCommon(s, 1, static_cast<int>(iterations), o, mask, false);
+}
+
+jgs2_status jgs2_step_frames_exact_iterations(jgs2_solver* s, uint32_t frames, uint32_t iterations,
+                                              const jgs2_settings* o, uint32_t mask) {
+  return stepCommon(s, frames, static_cast<int>(iterations), o, mask, true);
+}
+
+jgs2_status jgs2_sync(jgs2_solver* s) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_set_external_force(jgs2_solver* s, uint32_t vertex, const float force[3]) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (vertex >= s->V) return fail(s, JGS2_INVALID_ARGUMENT, format("vertex %u is out of range.", vertex));
+  if (!force) return fail(s, JGS2_INVALID_ARGUMENT, "force is NULL.");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(force[k]))
+      return fail(s, JGS2_INVALID_ARGUMENT,
+                  format("External force %d for vertex %u must be finite after f32 conversion.", k, vertex));
+  if (s->pinned[vertex] && (force[0] != 0 || force[1] != 0 || force[2] != 0))
+    return fail(s, JGS2_INVALID_ARGUMENT, format("Pinned vertex %u cannot have a nonzero external force.", vertex));
+  float* o = &s->objectives[8ull * vertex];
+  o[0] = force[0]; o[1] = force[1]; o[2] = force[2]; o[3] = 0.f;
+  return writeObjectives(s, vertex, 1);
+}
+
+jgs2_status jgs2_replace_external_forces(jgs2_solver* s, const float* forces) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!forces) return fail(s, JGS2_INVALID_ARGUMENT, "forces is NULL.");
+  for (uint32_t v = 0; v < s->V; ++v) {
+    bool nonzero = false;
+    for (int k = 0; k < 3; ++k) {
+      if (!std::isfinite(forces[3ull * v + k]))
+        return fail(s, JGS2_INVALID_ARGUMENT, format("External forces[%llu] must be finite after f32 conversion.",
+                                                     static_cast<unsigned long long>(3ull * v + k)));
+      nonzero |= forces[3ull * v + k] != 0;
+    }
+    if (s->pinned[v] && nonzero)
+      return fail(s, JGS2_INVALID_ARGUMENT, format("Pinned vertex %u cannot have a nonzero external force.", v));
+  }
+  for (uint32_t v = 0; v < s->V; ++v) {
+    float* o = &s->objectives[8ull * v];
+    o[0] = forces[3ull * v]; o[1] = forces[3ull * v + 1]; o[2] = forces[3ull * v + 2]; o[3] = 0.f;
+  }
+  return writeObjectives(s, 0, s->V);
+}
+
+jgs2_status jgs2_clear_external_forces(jgs2_solver* s) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  std::vector<float> zeros(3ull * s->V, 0.f);
+  return jgs2_replace_external_forces(s, zeros.data());
+}
+
+jgs2_status jgs2_set_quadratic_target(jgs2_solver* s, uint32_t vertex, const float target[3], float stiffness) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (vertex >= s->V) return fail(s, JGS2_INVALID_ARGUMENT, format("vertex %u is out of range.", vertex));
+  if (!target) return fail(s, JGS2_INVALID_ARGUMENT, "target is NULL.");
+  for (int k = 0; k < 3; ++k)
+    if (!std::isfinite(target[k]))
+      return fail(s, JGS2_INVALID_ARGUMENT,
+                  format("Quadratic target %d for vertex %u must be finite after f32 conversion.", k, vertex));
+  if (!std::isfinite(stiffness))
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("Quadratic-target stiffness for vertex %u must be finite after f32 conversion.", vertex));
+  if (stiffness < 0)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("Quadratic-target stiffness for vertex %u must be nonnegative.", vertex));
+  if (s->pinned[vertex] && stiffness != 0)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("Pinned vertex %u cannot have a nonzero quadratic-target stiffness.", vertex));
+  float* o = &s->objectives[8ull * vertex];
+  o[4] = target[0]; o[5] = target[1]; o[6] = target[2]; o[7] = stiffness;
+  return writeObjectives(s, vertex, 1);
+}
+
+jgs2_status jgs2_replace_quadratic_targets(jgs2_solver* s, const float* positions, const float* stiffnesses) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!positions || !stiffnesses) return fail(s, JGS2_INVALID_ARGUMENT, "targets are NULL.");
+  for (uint32_t v = 0; v < s->V; ++v) {
+    for (int k = 0; k < 3; ++k)
+      if (!std::isfinite(positions[3ull * v + k]))
+        return fail(s, JGS2_INVALID_ARGUMENT,
+                    format("Quadratic target positions[%llu] must be finite after f32 conversion.",
+                           static_cast<unsigned long long>(3ull * v + k)));
+    if (!std::isfinite(stiffnesses[v]))
+      return fail(s, JGS2_INVALID_ARGUMENT,
+                  format("Quadratic target stiffnesses[%u] must be finite after f32 conversion.", v));
+    if (stiffnesses[v] < 0)
+      return fail(s, JGS2_INVALID_ARGUMENT, format("Quadratic target stiffnesses[%u] must be nonnegative.", v));
+    if (s->pinned[v] && stiffnesses[v] != 0)
+      return fail(s, JGS2_INVALID_ARGUMENT,
+                  format("Pinned vertex %u cannot have a nonzero quadratic-target stiffness.", v));
+  }
+  for (uint32_t v = 0; v < s->V; ++v) {
+    float* o = &s->objectives[8ull * v];
+    o[4] = positions[3ull * v]; o[5] = positions[3ull * v + 1]; o[6] = positions[3ull * v + 2]; o[7] = stiffnesses[v];
+  }
+  return writeObjectives(s, 0, s->V);
+}
+
+jgs2_status jgs2_release_quadratic_target(jgs2_solver* s, uint32_t vertex) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (vertex >= s->V) return fail(s, JGS2_INVALID_ARGUMENT, format("vertex %u is out of range.", vertex));
+  s->objectives[8ull * vertex + 7] = 0.f;
+  return writeObjectives(s, vertex, 1);
+}
+
+jgs2_status jgs2_release_all_quadratic_targets(jgs2_solver* s) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  for (uint32_t v = 0; v < s->V; ++v) s->objectives[8ull * v + 7] = 0.f;
+  return writeObjectives(s, 0, s->V);
+}
+
+static jgs2_status readVec4(jgs2_solver* s, const float4* dev, float* out, size_t floats, size_t perVertex) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out || floats < perVertex * s->V)
+    return fail(s, JGS2_INVALID_ARGUMENT, format("output needs %zu floats.", perVertex * s->V));
+  return readRegion(s, dev, sizeof(float) * perVertex * s->V, out);
+}
+
+jgs2_status jgs2_read_positions(jgs2_solver* s, float* out, size_t floats) {
+  if (usable(s) != JGS2_OK) return usable(s);
+  return readVec4(s, s->b.pos[0], out, floats, 4);
+}
+
+jgs2_status jgs2_read_velocities(jgs2_solver* s, float* out, size_t floats) {
+  if (usable(s) != JGS2_OK) return usable(s);
+  return readVec4(s, s->b.velocity, out, floats, 4);
+}
+
+jgs2_status jgs2_read_predicted_positions(jgs2_solver* s, float* out, size_t floats) {
+  if (usable(s) != JGS2_OK) return usable(s);
+  return readVec4(s, s->b.predicted, out, floats, 4);
+}
+
+jgs2_status jgs2_read_final_iteration_updates(jgs2_solver* s, float* out, size_t floats) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out || floats < 4ull * s->V) return fail(s, JGS2_INVALID_ARGUMENT, format("output needs %u floats.", 4 * s->V));
+  std::vector<float> u(s->V);
+  st = readRegion(s, s->b.finalUpdate, sizeof(float) * s->V, u.data());
+  if (st != JGS2_OK) return st;
+  const float w = s->submittedIterations > 0 ? 1.f : 0.f;
+  for (uint32_t v = 0; v < s->V; ++v) {
+    out[4ull * v] = u[v];
+    out[4ull * v + 1] = 0.f;
+    out[4ull * v + 2] = 0.f;
+    out[4ull * v + 3] = w;
+  }
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_read_vertex_rotations(jgs2_solver* s, float* out, size_t floats) {
+  if (usable(s) != JGS2_OK) return usable(s);
+  return readVec4(s, s->b.vertexRot, out, floats, 12);
+}
+
+jgs2_status jgs2_read_globalization(jgs2_solver* s, float* local, size_t localFloats, float* control,
+                                    float* history, size_t historyFloats, uint32_t* historyCount) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!s->glob)
+    return fail(s, JGS2_UNSUPPORTED,
+                "Globalization diagnostics are available only for stable Neo-Hookean production solves.");
+  if (!s->recordsAvailable)
+    return fail(s, JGS2_NOT_READY,
+                "Globalization diagnostics are unavailable until a stable nonlinear iteration or diagnostic test "
+                "kernel has produced records.");
+  if (local) {
+    if (localFloats < 16ull * s->V) return fail(s, JGS2_INVALID_ARGUMENT, "local output too small.");
+    st = readRegion(s, s->b.local, sizeof(float) * 16ull * s->V, local);
+    if (st != JGS2_OK) return st;
+  }
+  float4 ctl[4];
+  st = readRegion(s, s->b.frame->control, sizeof(ctl), ctl);
+  if (st != JGS2_OK) return st;
+  if (control) std::memcpy(control, ctl, sizeof(ctl));
+  const float raw = ctl[1].w;
+  if (!(raw >= 0 && raw <= float(JGS2_HISTORY_CAPACITY) && raw == std::floor(raw)))
+    return fail(s, JGS2_DEVICE_ERROR, format("GPU returned invalid globalization history count %g.", raw));
+  const uint32_t count = static_cast<uint32_t>(raw);
+  if (historyCount) *historyCount = count;
+  if (history) {
+    if (historyFloats < 32ull * JGS2_HISTORY_CAPACITY) return fail(s, JGS2_INVALID_ARGUMENT, "history output too small.");
+    st = readRegion(s, s->b.frame->history, sizeof(float) * 32ull * JGS2_HISTORY_CAPACITY, history);
+    if (st != JGS2_OK) return st;
+  }
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_device_positions(jgs2_solver* s, void** ptr, void** stream) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (ptr) *ptr = s->b.pos[0];
+  if (stream) *stream = s->stream;
+  return JGS2_OK;
+}
+
+uint64_t jgs2_kernel_launch_count(const jgs2_solver* s) { return s ? s->launches : 0; }
+
+}  // extern "C"

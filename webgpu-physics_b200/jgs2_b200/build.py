@@ -1,0 +1,101 @@
+"""Build recipe of the native libraries (in-tree, into webgpu-physics_b200/lib).
+
+  libjgs2.so        CUDA step for sm_100a + the C-ABI runtime (include/jgs2.h)
+  libjgs2_scene.so  CPU scene builder / precompute (include/jgs2_scene.h)
+
+Run as `python -m jgs2_b200.build` from webgpu-physics_b200/ or through
+__graft_entry__.build().  nvcc cross-compiles for sm_100a without a GPU.
+"""
+from __future__ import annotations
+
+import os
+import shutil
+import subprocess
+import sys
+
+PKG_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+REPO_ROOT = os.path.dirname(PKG_ROOT)
+CSRC = os.path.join(PKG_ROOT, "csrc")
+LIB = os.path.join(PKG_ROOT, "lib")
+INCLUDE = os.path.join(REPO_ROOT, "include")
+
+ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+
+
+def _nvcc() -> str:
+    for cand in (os.environ.get("NVCC"), "/usr/local/cuda/bin/nvcc", shutil.which("nvcc")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("nvcc not found")
+
+
+def _cxx() -> str:
+    # The system g++ carries libgomp; an overriding $CXX may not.
+    for cand in ("/usr/bin/g++", shutil.which("g++")):
+        if cand and os.path.exists(cand):
+            return cand
+    raise RuntimeError("g++ not found")
+
+
+def _run(cmd, verbose=False):
+    if verbose:
+        print(" ".join(cmd), flush=True)
+    res = subprocess.run(cmd, capture_output=True, text=True)
+    if res.returncode != 0:
+        raise RuntimeError(f"build step failed ({res.returncode}): {' '.join(cmd)}\n{res.stdout}\n{res.stderr}")
+    return res
+
+
+def _stale(target, sources) -> bool:
+    if not os.path.exists(target):
+        return True
+    t = os.path.getmtime(target)
+    return any(os.path.getmtime(s) > t for s in sources)
+
+
+def build_step_library(force=False, verbose=False) -> str:
+    os.makedirs(LIB, exist_ok=True)
+    target = os.path.join(LIB, "libjgs2.so")
+    sources = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cu", "jgs2_runtime.cpp")]
+    headers = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cuh", "jgs2_device.cuh")] + [
+        os.path.join(INCLUDE, "jgs2.h")]
+    if not force and not _stale(target, sources + headers):
+        return target
+    nvcc = _nvcc()
+    objs = []
+    for src in sources:
+        obj = os.path.join(LIB, os.path.basename(src) + ".o")
+        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
+               "-c", src, "-o", obj]
+        if src.endswith(".cpp"):
+            cmd.insert(1, "-x")
+            cmd.insert(2, "cu")
+        _run(cmd, verbose)
+        objs.append(obj)
+    _run([nvcc, *ARCH, "-shared", "-o", target, *objs, "-lcudart"], verbose)
+    for obj in objs:
+        os.remove(obj)
+    return target
+
+
+def build_scene_library(force=False, verbose=False) -> str:
+    os.makedirs(LIB, exist_ok=True)
+    target = os.path.join(LIB, "libjgs2_scene.so")
+    sdir = os.path.join(CSRC, "scene")
+    sources = [os.path.join(sdir, f) for f in ("scene.cpp", "precompute.cpp")]
+    headers = [os.path.join(sdir, "scene_internal.hpp"), os.path.join(INCLUDE, "jgs2_scene.h"),
+               os.path.join(INCLUDE, "jgs2.h")]
+    if not force and not _stale(target, sources + headers):
+        return target
+    _run([_cxx(), "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-std=c++17", "-I", INCLUDE,
+          "-I", sdir, *sources, "-o", target], verbose)
+    return target
+
+
+def build_all(force=False, verbose=False):
+    return [build_step_library(force, verbose), build_scene_library(force, verbose)]
+
+
+if __name__ == "__main__":
+    for path in build_all(force="--force" in sys.argv, verbose=True):
+        print(path)

@@ -1,0 +1,331 @@
+"""Scene construction and the packed step input (the reference's
+src/scenes/index.ts + src/simulation/cpu/precompute.ts), driving the native
+scene/precompute library through include/jgs2_scene.h.
+
+`SceneInput` is the JGS2GpuInput (src/simulation/gpu/layout.ts:41-90) as numpy
+arrays; `SceneInput.as_ctypes()` yields the jgs2_input record the step library
+takes.  The named workloads below are the seeded synthetic scenes the
+benchmarks and parity tests run on.
+"""
+from __future__ import annotations
+
+import ctypes
+import dataclasses
+import math
+from ctypes import c_double, c_uint32
+from typing import Optional
+
+import numpy as np
+
+from . import _ffi
+
+MATERIAL_COROTATED_LINEAR = 0
+MATERIAL_STABLE_NEO_HOOKEAN = 1
+PRECOMPUTE_EXACT = 0
+PRECOMPUTE_PATCH = 1
+FACE_X_MIN, FACE_X_MAX, FACE_Y_MIN, FACE_Y_MAX, FACE_Z_MIN, FACE_Z_MAX = (
+    1, 2, 4, 8, 16, 32)
+EMPTY_TET = 0xFFFFFFFF
+
+
+def mulberry32(seed: int):
+    """createCorpusRandom (src/scenes/phase1.ts:106-115): uniform [0, 1)."""
+    state = seed & 0xFFFFFFFF
+
+    def imul(a, b):
+        return (a * b) & 0xFFFFFFFF
+
+    def rand():
+        nonlocal state
+        state = (state + 0x6D2B79F5) & 0xFFFFFFFF
+        value = state
+        value = imul(value ^ (value >> 15), value | 1)
+        value ^= (value + imul(value ^ (value >> 7), value | 61)) & 0xFFFFFFFF
+        return ((value ^ (value >> 14)) & 0xFFFFFFFF) / 4294967296.0
+
+    return rand
+
+
+@dataclasses.dataclass
+class SceneInput:
+    """JGS2GpuInput as contiguous numpy arrays."""
+
+    vertex_count: int
+    tet_count: int
+    cubature_k: int
+    positions: np.ndarray
+    vertex_rest: np.ndarray
+    vertex_info: np.ndarray
+    tet_indices: np.ndarray
+    tet_inverse_dm: np.ndarray
+    tet_meta: np.ndarray
+    adjacency: np.ndarray
+    cubature_tet_ids: np.ndarray
+    cubature_weights: np.ndarray
+    cubature_basis: np.ndarray
+    velocities: Optional[np.ndarray] = None
+    vertex_colors: Optional[np.ndarray] = None
+    tet_rest_stiffness: Optional[np.ndarray] = None
+    external_forces: Optional[np.ndarray] = None
+    target_positions: Optional[np.ndarray] = None
+    target_stiffnesses: Optional[np.ndarray] = None
+    rest_positions: Optional[np.ndarray] = None  # float64 FEM rest shape
+    stats: Optional[dict] = None
+
+    def as_ctypes(self) -> _ffi.Input:
+        rec = _ffi.Input()
+        rec.vertex_count = self.vertex_count
+        rec.tet_count = self.tet_count
+        rec.cubature_k = self.cubature_k
+        rec.positions = _ffi.fptr(self.positions)
+        rec.velocities = _ffi.fptr(self.velocities)
+        rec.vertex_rest = _ffi.fptr(self.vertex_rest)
+        rec.vertex_colors = _ffi.fptr(self.vertex_colors)
+        rec.vertex_info = _ffi.uptr(self.vertex_info)
+        rec.external_forces = _ffi.fptr(self.external_forces)
+        rec.target_positions = _ffi.fptr(self.target_positions)
+        rec.target_stiffnesses = _ffi.fptr(self.target_stiffnesses)
+        rec.tet_indices = _ffi.uptr(self.tet_indices)
+        rec.tet_inverse_dm = _ffi.fptr(self.tet_inverse_dm)
+        rec.tet_meta = _ffi.fptr(self.tet_meta)
+        rec.tet_rest_stiffness = _ffi.fptr(self.tet_rest_stiffness)
+        rec.adjacency = _ffi.uptr(self.adjacency)
+        rec.adjacency_length = int(self.adjacency.size)
+        rec.cubature_tet_ids = _ffi.uptr(self.cubature_tet_ids)
+        rec.cubature_weights = _ffi.fptr(self.cubature_weights)
+        rec.cubature_basis = _ffi.fptr(self.cubature_basis)
+        # Keep the arrays alive as long as the record.
+        rec._owner = self  # type: ignore[attr-defined]
+        return rec
+
+    def copy(self) -> "SceneInput":
+        return dataclasses.replace(
+            self, **{f.name: (getattr(self, f.name).copy()
+                              if isinstance(getattr(self, f.name), np.ndarray)
+                              else getattr(self, f.name))
+                     for f in dataclasses.fields(self)})
+
+    def bbox_diagonal(self) -> float:
+        p = self.positions.reshape(-1, 4)[:, :3].astype(np.float64)
+        return float(np.linalg.norm(p.max(axis=0) - p.min(axis=0)))
+
+    def active_vertex_count(self) -> int:
+        return int(np.count_nonzero(self.vertex_info.reshape(-1, 4)[:, 2] == 0))
+
+
+class Scene:
+    """Owner of a native jgs2_scene handle (include/jgs2_scene.h)."""
+
+    def __init__(self):
+        self._lib = _ffi.scene_lib()
+        self._h = self._lib.jgs2_scene_new()
+        if not self._h:
+            raise MemoryError("jgs2_scene_new failed")
+
+    def __del__(self):
+        h = getattr(self, "_h", None)
+        if h:
+            self._lib.jgs2_scene_destroy(h)
+            self._h = None
+
+    def _error(self) -> str:
+        return self._lib.jgs2_scene_last_error(self._h).decode()
+
+    def add_material(self, density, young, poisson, model=MATERIAL_STABLE_NEO_HOOKEAN) -> int:
+        mid = self._lib.jgs2_scene_add_material(self._h, density, young, poisson, model)
+        if mid < 0:
+            raise ValueError(self._error())
+        return mid
+
+    def add_cuboid(self, cells, origin, size, material=0, body=0, pinned_faces=0) -> int:
+        c = (c_uint32 * 3)(*cells)
+        o = (c_double * 3)(*origin)
+        s = (c_double * 3)(*size)
+        base = self._lib.jgs2_scene_add_cuboid(self._h, c, o, s, material, body, pinned_faces)
+        if base < 0:
+            raise ValueError(self._error())
+        return base
+
+    def add_mesh(self, positions, tets, material=0, pinned=None, body=0, tet_materials=None) -> int:
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
+        q = np.ascontiguousarray(tets, dtype=np.uint32).reshape(-1)
+        pin = None if pinned is None else np.ascontiguousarray(pinned, dtype=np.uint8)
+        mats = None if tet_materials is None else np.ascontiguousarray(tet_materials, dtype=np.uint32)
+        base = self._lib.jgs2_scene_add_mesh(
+            self._h, pos.size // 3, _ffi.dptr(pos), q.size // 4, _ffi.uptr(q),
+            _ffi.uptr(mats), material,
+            None if pin is None else pin.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), body)
+        if base < 0:
+            raise ValueError(self._error())
+        return base
+
+    def set_pinned(self, pinned):
+        pin = np.ascontiguousarray(pinned, dtype=np.uint8)
+        if pin.size != self.vertex_count:
+            raise ValueError("pinned must have one entry per vertex")
+        status = self._lib.jgs2_scene_set_pinned(
+            self._h, pin.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)))
+        if status != 0:
+            raise _ffi.JGS2Error(status, self._error())
+
+    @property
+    def vertex_count(self) -> int:
+        return self._lib.jgs2_scene_vertex_count(self._h)
+
+    @property
+    def tet_count(self) -> int:
+        return self._lib.jgs2_scene_tet_count(self._h)
+
+    def rest_positions(self) -> np.ndarray:
+        out = np.empty(3 * self.vertex_count, dtype=np.float64)
+        self._lib.jgs2_scene_rest_positions(self._h, _ffi.dptr(out))
+        return out.reshape(-1, 3)
+
+    def precompute(self, timestep=1 / 60, cubature_k=6, method=PRECOMPUTE_EXACT,
+                   patch_radius=2, threads=0, **overrides) -> dict:
+        opt = _ffi.PrecomputeOptions()
+        self._lib.jgs2_default_precompute_options(ctypes.byref(opt))
+        opt.timestep = timestep
+        opt.cubature_k = cubature_k
+        opt.method = method
+        opt.patch_radius = patch_radius
+        opt.threads = threads
+        for key, value in overrides.items():
+            setattr(opt, key, value)
+        st = _ffi.PrecomputeStats()
+        status = self._lib.jgs2_scene_precompute(self._h, ctypes.byref(opt), ctypes.byref(st))
+        if status != 0:
+            raise _ffi.JGS2Error(status, self._error())
+        return {name: getattr(st, name) for name, _t in _ffi.PrecomputeStats._fields_}
+
+    def set_initial_state(self, positions=None, velocities=None, pin_at_initial=False):
+        p = None if positions is None else np.ascontiguousarray(positions, dtype=np.float32)
+        v = None if velocities is None else np.ascontiguousarray(velocities, dtype=np.float32)
+        self._keep_state = (p, v)
+        self._lib.jgs2_scene_set_initial_state(self._h, _ffi.fptr(p), _ffi.fptr(v),
+                                               1 if pin_at_initial else 0)
+
+    def set_objectives(self, external_forces=None, target_positions=None,
+                       target_stiffnesses=None):
+        arrs = [None if a is None else np.ascontiguousarray(a, dtype=np.float32)
+                for a in (external_forces, target_positions, target_stiffnesses)]
+        status = self._lib.jgs2_scene_set_objectives(self._h, *[_ffi.fptr(a) for a in arrs])
+        if status != 0:
+            raise _ffi.JGS2Error(status, self._error())
+
+    def pack(self) -> SceneInput:
+        rec = _ffi.Input()
+        status = self._lib.jgs2_scene_pack(self._h, ctypes.byref(rec))
+        if status != 0:
+            raise _ffi.JGS2Error(status, self._error())
+        V, T, K = rec.vertex_count, rec.tet_count, rec.cubature_k
+
+        def f(ptr, n):
+            if not ptr:
+                return None
+            return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+
+        return SceneInput(
+            vertex_count=V, tet_count=T, cubature_k=K,
+            positions=f(rec.positions, 4 * V), vertex_rest=f(rec.vertex_rest, 4 * V),
+            vertex_info=f(rec.vertex_info, 4 * V), tet_indices=f(rec.tet_indices, 4 * T),
+            tet_inverse_dm=f(rec.tet_inverse_dm, 12 * T), tet_meta=f(rec.tet_meta, 4 * T),
+            adjacency=f(rec.adjacency, rec.adjacency_length),
+            cubature_tet_ids=f(rec.cubature_tet_ids, V * K),
+            cubature_weights=f(rec.cubature_weights, V * K),
+            cubature_basis=f(rec.cubature_basis, V * K * 36),
+            velocities=f(rec.velocities, 4 * V), vertex_colors=f(rec.vertex_colors, 4 * V),
+            tet_rest_stiffness=f(rec.tet_rest_stiffness, 144 * T),
+            external_forces=f(rec.external_forces, 3 * V),
+            target_positions=f(rec.target_positions, 3 * V),
+            target_stiffnesses=f(rec.target_stiffnesses, V),
+            rest_positions=self.rest_positions(),
+        )
+
+
+# ---- named workloads -----------------------------------------------------------
+
+def cantilever(cells=(20, 4, 4), size=(1.0, 0.2, 0.2), young=1e5, poisson=0.4,
+               density=1000.0, timestep=1 / 60, cubature_k=6,
+               method=PRECOMPUTE_EXACT, patch_radius=2, threads=0) -> SceneInput:
+    """Minimal cantilever: a bar of hexes x6 tets with its x=0 face pinned,
+    stable Neo-Hookean (the 525-vertex / 1920-tet configuration)."""
+    sc = Scene()
+    m = sc.add_material(density, young, poisson, MATERIAL_STABLE_NEO_HOOKEAN)
+    sc.add_cuboid(cells, (0.0, 0.0, 0.0), size, m, 0, FACE_X_MIN)
+    stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=method,
+                          patch_radius=patch_radius, threads=threads)
+    inp = sc.pack()
+    inp.stats = stats
+    return inp
+
+
+def cantilever_target(inp: SceneInput, frame: int, lift=0.15, stiffness=1000.0):
+    """Soft target on the free-end (x = max) vertices for frames 60-180: the
+    rest position raised by `lift` along a smoothstep over frames 60-120, held
+    until 180, released afterwards.  Returns (positions 3V, stiffnesses V)."""
+    rest = inp.rest_positions
+    xmax = rest[:, 0].max()
+    tip = np.isclose(rest[:, 0], xmax)
+    targets = rest.astype(np.float32).copy()
+    stiff = np.zeros(inp.vertex_count, dtype=np.float32)
+    if 60 <= frame < 180:
+        u = min(1.0, (frame - 60) / 60.0)
+        progress = u * u * (3 - 2 * u)
+        targets[tip, 1] += np.float32(lift * progress)
+        stiff[tip] = stiffness
+    return targets.reshape(-1), stiff
+
+
+def unit_cube(cells=100, young=1e6, poisson=0.45, density=1000.0, timestep=1 / 60,
+              cubature_k=6, seed=1048583, patch_radius=2, threads=0,
+              method=PRECOMPUTE_PATCH) -> SceneInput:
+    """Single large body: unit cube of cells^3 hexes x6 tets, bottom face
+    pinned, initial pose = rest stretched per axis by U[0.9, 1.1] (Mulberry32
+    seeded) about the bottom-face centre, the pinned face clamped in its
+    stretched position."""
+    sc = Scene()
+    m = sc.add_material(density, young, poisson, MATERIAL_STABLE_NEO_HOOKEAN)
+    sc.add_cuboid((cells, cells, cells), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), m, 0, FACE_Y_MIN)
+    stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=method,
+                          patch_radius=patch_radius, threads=threads)
+    rand = mulberry32(seed)
+    stretch = np.array([0.9 + 0.2 * rand() for _ in range(3)])
+    rest = sc.rest_positions()
+    centre = np.array([0.5, 0.0, 0.5])
+    pos = centre + (rest - centre) * stretch
+    p4 = np.ones((rest.shape[0], 4), dtype=np.float32)
+    p4[:, :3] = pos
+    sc.set_initial_state(p4.reshape(-1), None, pin_at_initial=True)
+    inp = sc.pack()
+    stats["stretch"] = stretch.tolist()
+    inp.stats = stats
+    return inp
+
+
+def batched_bodies(count=256, seed=65537, min_cells=4, max_cells=32, soft=5e4, stiff=5e6,
+                   poisson=0.4, density=1000.0, timestep=1 / 60, cubature_k=6,
+                   patch_radius=2, threads=0, spacing=0.25) -> SceneInput:
+    """Batched uneven bodies: `count` hex-grid boxes with per-axis cell counts
+    drawn uniformly from [min_cells, max_cells] (Mulberry32 seeded), cell size
+    1/32 m, alternating soft/stiff materials, laid out on a square grid above
+    a penalty floor at y = 0."""
+    rand = mulberry32(seed)
+    sc = Scene()
+    m_soft = sc.add_material(density, soft, poisson, MATERIAL_STABLE_NEO_HOOKEAN)
+    m_stiff = sc.add_material(density, stiff, poisson, MATERIAL_STABLE_NEO_HOOKEAN)
+    side = int(math.ceil(math.sqrt(count)))
+    h = 1.0 / 32.0
+    pitch = max_cells * h + spacing
+    for b in range(count):
+        cells = [min_cells + min(max_cells - min_cells,
+                                 int(rand() * (max_cells - min_cells + 1))) for _ in range(3)]
+        gx, gz = b % side, b // side
+        origin = (gx * pitch, 0.25, gz * pitch)
+        size = tuple(c * h for c in cells)
+        sc.add_cuboid(cells, origin, size, m_soft if b % 2 == 0 else m_stiff, b, 0)
+    stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=PRECOMPUTE_PATCH,
+                          patch_radius=patch_radius, threads=threads)
+    inp = sc.pack()
+    inp.stats = stats
+    return inp

@@ -1,0 +1,323 @@
+"""Host-side mirror of the reference's `class JGS2GpuSolver`
+(src/simulation/gpu/jgs2-solver.ts:905-3051) over the C-ABI in include/jgs2.h.
+
+Method names, argument meaning and error conditions follow the reference:
+`JGS2GpuSolver.create(input, settings)`, `step(overrides)`,
+`stepFrames(n, overrides)`, `stepExactIterations(n, overrides)`,
+`stepFramesExactIterations(frames, n, overrides)`, the objective setters,
+`readPositions()` and the other reads, `awaitIdle()` and `destroy()`.  Where
+the reference throws RangeError/TypeError this raises `JGS2RangeError`
+(a ValueError); device failures raise `JGS2Error`.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_float, c_uint32, c_void_p
+from typing import Optional
+
+import numpy as np
+
+from . import _ffi
+
+DEFAULT_SETTINGS_KEYS = [name for name, _t in _ffi.SETTINGS_FIELDS]
+SCHEDULES = {"jacobi": 0, "graph-colored-gauss-seidel": 1}
+# Settings keys in the reference's camelCase spelling.
+CAMEL = {
+    "schedule": "schedule", "timestep": "timestep", "gravity": "gravity", "iterations": "iterations",
+    "floorHeight": "floor_height", "floorStiffness": "floor_stiffness",
+    "velocityDamping": "velocity_damping", "regularization": "regularization",
+    "rotationEpsilon": "rotation_epsilon", "maxStep": "max_step",
+    "residualTolerance": "residual_tolerance", "normalizedUpdateTolerance": "normalized_update_tolerance",
+    "contactTangentialDamping": "contact_tangential_damping", "contactMargin": "contact_margin",
+    "ipcActivationDistance": "ipc_activation_distance", "ipcMinimumDistance": "ipc_minimum_distance",
+    "ipcBarrierStiffness": "ipc_barrier_stiffness", "ipcFrictionCoefficient": "ipc_friction_coefficient",
+    "ipcFrictionVelocityEpsilon": "ipc_friction_velocity_epsilon", "ipcStepSafety": "ipc_step_safety",
+    "horizontalBodyCorrection": "horizontal_body_correction", "parityMode": "parity_mode",
+}
+
+
+class JGS2RangeError(_ffi.JGS2Error, ValueError):
+    """Invalid argument, input or state (the reference's RangeError/TypeError)."""
+
+
+def _raise(status: int, message: str):
+    if status in (1, 2, 6, 7, 8):
+        raise JGS2RangeError(status, message)
+    raise _ffi.JGS2Error(status, message)
+
+
+def settings_struct(overrides: Optional[dict]):
+    """(jgs2_settings, mask) for a Partial<JGS2StepSettings> dict."""
+    rec = _ffi.Settings()
+    mask = 0
+    for key, value in (overrides or {}).items():
+        name = CAMEL.get(key, key)
+        if name not in _ffi.SETTINGS_BITS:
+            raise JGS2RangeError(1, f"Unknown JGS2 setting: {key}.")
+        if name == "schedule" and isinstance(value, str):
+            if value not in SCHEDULES:
+                raise JGS2RangeError(1, f"Unknown JGS2 schedule: {value}.")
+            value = SCHEDULES[value]
+        if name == "gravity":
+            rec.gravity[:] = [float(x) for x in value]
+        elif name in ("horizontal_body_correction", "parity_mode"):
+            if not isinstance(value, (bool, int, np.bool_)):
+                raise JGS2RangeError(1, f"{key} must be a boolean.")
+            setattr(rec, name, 1 if value else 0)
+        elif name in ("schedule", "iterations"):
+            value = int(value)
+            if value < 0:
+                raise JGS2RangeError(1, f"{key} must be nonnegative; got {value}.")
+            setattr(rec, name, value)
+        else:
+            setattr(rec, name, float(value))
+        mask |= _ffi.SETTINGS_BITS[name]
+    return rec, mask
+
+
+def settings_dict(rec) -> dict:
+    out = {}
+    for name, _t in _ffi.SETTINGS_FIELDS:
+        value = getattr(rec, name)
+        out[name] = list(value) if name == "gravity" else value
+    return out
+
+
+def default_settings() -> dict:
+    rec = _ffi.Settings()
+    _ffi.step_lib().jgs2_default_settings(byref(rec))
+    return settings_dict(rec)
+
+
+def resolve_settings(overrides: Optional[dict] = None, defaults: Optional[dict] = None) -> dict:
+    L = _ffi.step_lib()
+    base = None
+    if defaults is not None:
+        base, _m = settings_struct(defaults)
+    o, mask = settings_struct(overrides)
+    out = _ffi.Settings()
+    st = L.jgs2_resolve_settings(byref(base) if base is not None else None, byref(o), mask, byref(out))
+    if st != 0:
+        _raise(st, L.jgs2_global_last_error().decode())
+    return settings_dict(out)
+
+
+def build_vertex_coloring(scene_input):
+    """buildJGS2InputVertexColoring: (colors uint32[V], colorCount)."""
+    L = _ffi.step_lib()
+    rec = scene_input.as_ctypes()
+    colors = np.zeros(scene_input.vertex_count, dtype=np.uint32)
+    count = c_uint32(0)
+    st = L.jgs2_build_vertex_coloring(byref(rec), colors.ctypes.data_as(ctypes.POINTER(c_uint32)), byref(count))
+    if st != 0:
+        _raise(st, L.jgs2_global_last_error().decode())
+    return colors, int(count.value)
+
+
+def validate_input(scene_input):
+    L = _ffi.step_lib()
+    rec = scene_input.as_ctypes()
+    st = L.jgs2_validate_input(byref(rec))
+    if st != 0:
+        _raise(st, L.jgs2_global_last_error().decode())
+
+
+class JGS2GpuSolver:
+    """One solver = one CUDA stream and its device memory."""
+
+    def __init__(self, handle, lib, vertex_count):
+        self._h = handle
+        self._L = lib
+        self.vertexCount = vertex_count
+        self._destroyed = False
+
+    # ---- lifetime ----------------------------------------------------------------
+    @classmethod
+    def create(cls, scene_input, settings: Optional[dict] = None, device: int = 0) -> "JGS2GpuSolver":
+        L = _ffi.step_lib()
+        rec = scene_input.as_ctypes()
+        s, mask = settings_struct(settings)
+        h = c_void_p()
+        st = L.jgs2_create(byref(rec), byref(s), mask, int(device), byref(h))
+        if st != 0:
+            _raise(st, L.jgs2_global_last_error().decode())
+        return cls(h, L, scene_input.vertex_count)
+
+    def destroy(self):
+        if not self._destroyed and self._h:
+            self._L.jgs2_destroy(self._h)
+        self._destroyed = True
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            msg = self._L.jgs2_last_error(self._h).decode() if self._h else "destroyed"
+            _raise(st, msg)
+
+    def _usable(self):
+        if self._destroyed:
+            raise JGS2RangeError(6, "JGS2GpuSolver has been destroyed.")
+
+    # ---- info ----------------------------------------------------------------------
+    def info(self) -> dict:
+        self._usable()
+        out = _ffi.Info()
+        self._check(self._L.jgs2_get_info(self._h, byref(out)))
+        return {name: getattr(out, name) for name, _t in _ffi.Info._fields_}
+
+    @property
+    def scheduleColorCount(self) -> int:
+        return self.info()["schedule_color_count"]
+
+    @property
+    def globalizationEnabled(self) -> bool:
+        return bool(self.info()["globalization_enabled"])
+
+    @property
+    def objectiveActivity(self) -> dict:
+        i = self.info()
+        return {"flags": i["objective_flags"], "externalForces": bool(i["objective_flags"] & 1),
+                "quadraticTargets": bool(i["objective_flags"] & 2),
+                "externalForceVertexCount": i["external_force_vertex_count"],
+                "quadraticTargetVertexCount": i["quadratic_target_vertex_count"]}
+
+    @property
+    def lastSubmittedIterationCount(self) -> int:
+        return self.info()["last_submitted_iterations"]
+
+    @property
+    def defaultStepSettings(self) -> dict:
+        self._usable()
+        out = _ffi.Settings()
+        self._check(self._L.jgs2_get_default_settings(self._h, byref(out)))
+        return settings_dict(out)
+
+    @property
+    def lastSubmittedSettings(self) -> dict:
+        self._usable()
+        out = _ffi.Settings()
+        self._check(self._L.jgs2_get_last_submitted_settings(self._h, byref(out)))
+        return settings_dict(out)
+
+    def kernelLaunchCount(self) -> int:
+        return int(self._L.jgs2_kernel_launch_count(self._h)) if self._h else 0
+
+    def devicePositions(self):
+        """(device pointer, cudaStream_t) of the canonical position array."""
+        self._usable()
+        p, s = c_void_p(), c_void_p()
+        self._check(self._L.jgs2_device_positions(self._h, byref(p), byref(s)))
+        return p.value, s.value
+
+    # ---- stepping --------------------------------------------------------------------
+    def step(self, overrides: Optional[dict] = None):
+        self._usable()
+        o, m = settings_struct(overrides)
+        self._check(self._L.jgs2_step(self._h, byref(o), m))
+
+    def stepFrames(self, frameCount: int, overrides: Optional[dict] = None):
+        self._usable()
+        o, m = settings_struct(overrides)
+        self._check(self._L.jgs2_step_frames(self._h, int(frameCount), byref(o), m))
+
+    def stepExactIterations(self, iterations: int, overrides: Optional[dict] = None):
+        self._usable()
+        if int(iterations) < 1:
+            raise JGS2RangeError(1, f"iterations must be a positive safe integer; got {iterations}.")
+        o, m = settings_struct(overrides)
+        self._check(self._L.jgs2_step_exact_iterations(self._h, int(iterations), byref(o), m))
+
+    def stepFramesExactIterations(self, frameCount: int, iterations: int, overrides: Optional[dict] = None):
+        self._usable()
+        if int(iterations) < 1:
+            raise JGS2RangeError(1, f"iterations must be a positive safe integer; got {iterations}.")
+        o, m = settings_struct(overrides)
+        self._check(self._L.jgs2_step_frames_exact_iterations(self._h, int(frameCount), int(iterations),
+                                                              byref(o), m))
+
+    def awaitIdle(self):
+        self._usable()
+        self._check(self._L.jgs2_sync(self._h))
+
+    # ---- objectives ---------------------------------------------------------------------
+    def setExternalForce(self, vertex: int, force):
+        self._usable()
+        f = (c_float * 3)(*[float(x) for x in force])
+        self._check(self._L.jgs2_set_external_force(self._h, int(vertex), f))
+
+    def replaceExternalForces(self, forces):
+        self._usable()
+        a = np.ascontiguousarray(forces, dtype=np.float32).reshape(-1)
+        if a.size != 3 * self.vertexCount:
+            raise JGS2RangeError(1, f"External forces must contain {3 * self.vertexCount} values; got {a.size}.")
+        self._check(self._L.jgs2_replace_external_forces(self._h, _ffi.fptr(a)))
+
+    def clearExternalForces(self):
+        self._usable()
+        self._check(self._L.jgs2_clear_external_forces(self._h))
+
+    def setQuadraticTarget(self, vertex: int, target, stiffness: float):
+        self._usable()
+        t = (c_float * 3)(*[float(x) for x in target])
+        self._check(self._L.jgs2_set_quadratic_target(self._h, int(vertex), t, float(stiffness)))
+
+    def replaceQuadraticTargets(self, targetPositions, targetStiffnesses):
+        self._usable()
+        p = np.ascontiguousarray(targetPositions, dtype=np.float32).reshape(-1)
+        k = np.ascontiguousarray(targetStiffnesses, dtype=np.float32).reshape(-1)
+        if p.size != 3 * self.vertexCount:
+            raise JGS2RangeError(1, f"Quadratic target positions must contain {3 * self.vertexCount} values; "
+                                    f"got {p.size}.")
+        if k.size != self.vertexCount:
+            raise JGS2RangeError(1, f"Quadratic target stiffnesses must contain {self.vertexCount} values; "
+                                    f"got {k.size}.")
+        self._check(self._L.jgs2_replace_quadratic_targets(self._h, _ffi.fptr(p), _ffi.fptr(k)))
+
+    def releaseQuadraticTarget(self, vertex: int):
+        self._usable()
+        self._check(self._L.jgs2_release_quadratic_target(self._h, int(vertex)))
+
+    def releaseAllQuadraticTargets(self):
+        self._usable()
+        self._check(self._L.jgs2_release_all_quadratic_targets(self._h))
+
+    # ---- reads -----------------------------------------------------------------------------
+    def _read(self, fn, per_vertex):
+        self._usable()
+        out = np.empty(per_vertex * self.vertexCount, dtype=np.float32)
+        self._check(fn(self._h, _ffi.fptr(out), out.size))
+        return out
+
+    def readPositions(self) -> np.ndarray:
+        return self._read(self._L.jgs2_read_positions, 4)
+
+    def readVelocities(self) -> np.ndarray:
+        return self._read(self._L.jgs2_read_velocities, 4)
+
+    def readPredictedPositions(self) -> np.ndarray:
+        return self._read(self._L.jgs2_read_predicted_positions, 4)
+
+    def readFinalIterationUpdates(self) -> np.ndarray:
+        return self._read(self._L.jgs2_read_final_iteration_updates, 4)
+
+    def readVertexRotations(self) -> np.ndarray:
+        return self._read(self._L.jgs2_read_vertex_rotations, 12)
+
+    def readGlobalizationDiagnostics(self) -> dict:
+        """{'local': (V,16), 'control': (16,), 'history': (count,32), 'historyCount': n}."""
+        self._usable()
+        local = np.empty(16 * self.vertexCount, dtype=np.float32)
+        control = np.empty(16, dtype=np.float32)
+        history = np.empty(32 * 64, dtype=np.float32)
+        count = c_uint32(0)
+        self._check(self._L.jgs2_read_globalization(self._h, _ffi.fptr(local), local.size, _ffi.fptr(control),
+                                                    _ffi.fptr(history), history.size, byref(count)))
+        n = int(count.value)
+        return {"local": local.reshape(-1, 16), "control": control,
+                "history": history.reshape(64, 32)[:n], "historyCount": n}
