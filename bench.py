@@ -1,0 +1,383 @@
+#!/usr/bin/env python
+"""Benchmark of the B200 JGS2 step.
+
+Workload (one GPU): the single large body — a unit cube of 100^3 hexes x 6
+tets (1,030,301 vertices, 6,000,000 tets), stable Neo-Hookean E = 1e6 Pa,
+nu = 0.45, bottom face pinned, seeded per-axis initial stretch, K = 6
+patch-trained cubature records per vertex, 20 exact Jacobi iterations per
+frame, dt = 1/60 s.  A step is one frame.  `value` is vertex-updates/s
+(active vertices x iterations / second) over the timed frames with the state
+resident in HBM; `e2e` runs the same frames through the public API with a
+pinned host->device upload of a per-vertex external-force array and a
+device->host read of the positions every frame.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+With N > 1 (torchrun, one process per GPU) every rank steps an independent
+replica of the body (the single-body step has no data-parallel split here),
+`value` sums the ranks' vertex updates over the slowest rank's time.
+`--impl reference` times the CPU restatement of the reference step (the
+oracle) on the host cores instead: the reference is TypeScript + WGSL and
+cannot run on this machine.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "webgpu-physics_b200"))
+
+METRIC = "JGS2 vertex-updates/s & served frames/s + p99 latency vs plain, at <=1e-4 err"
+UNIT = "vertex-updates/s"
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cells", type=int, default=100, help="hexes per cube edge")
+    ap.add_argument("--iterations", type=int, default=20)
+    ap.add_argument("--schedule", default="jacobi", choices=["jacobi", "graph-colored-gauss-seidel"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def cache_dir() -> str:
+    d = os.environ.get("JGS2_CACHE_DIR", "/tmp/jgs2-bench-cache")
+    os.makedirs(d, exist_ok=True)
+    return d
+
+
+def workload(cells: int):
+    """Build (or load from the local cache) the cube's packed step input."""
+    from jgs2_b200 import scenes
+
+    path = os.path.join(cache_dir(), f"cube{cells}_k6_r2_v1.npz")
+    if os.path.exists(path):
+        try:
+            return scenes.SceneInput.load(path), True
+        except Exception:
+            os.remove(path)
+    inp = scenes.unit_cube(cells=cells)
+    try:
+        inp.save(path)
+    except OSError:
+        pass
+    return inp, False
+
+
+def workload_config(inp, args, precompute_info):
+    return {
+        "workload": (f"unit cube {args.cells}^3 hexes x6 tets ({inp.vertex_count} vertices, {inp.tet_count} tets), "
+                     f"stable Neo-Hookean E=1e6 nu=0.45, bottom face pinned, seeded per-axis stretch U[0.9,1.1], "
+                     f"K=6 patch-trained cubature, {args.iterations} exact {args.schedule} iterations per frame, "
+                     f"dt=1/60"),
+        "vertices": inp.vertex_count,
+        "active_vertices": inp.active_vertex_count(),
+        "tets": inp.tet_count,
+        "cubature_k": inp.cubature_k,
+        "iterations": args.iterations,
+        "schedule": args.schedule,
+        "step": "one frame",
+        "l2": "no flush: the resident state per iteration (~1.5 GB) exceeds the 126 MB L2",
+        "precompute": precompute_info,
+    }
+
+
+class ClockSampler:
+    """nvidia-smi clock/throttle samples during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, device_index: int):
+        self.device_index = device_index
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "200",
+                 "-i", str(self.device_index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except OSError:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.lines = []
+        if self.proc is not None:
+            self.proc.terminate()
+            try:
+                out, _ = self.proc.communicate(timeout=5)
+            except subprocess.TimeoutExpired:
+                self.proc.kill()
+                out, _ = self.proc.communicate()
+            self.lines = [ln for ln in out.splitlines() if ln.strip()]
+        return False
+
+    def summary(self):
+        sms, maxes, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in getattr(self, "lines", []):
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sms.append(float(parts[1]))
+                maxes.append(float(parts[2]))
+            except ValueError:
+                continue
+            for name, flag in zip(names, parts[5:9]):
+                if flag.lower() == "active":
+                    reasons.add(name)
+        if not sms:
+            return None
+        return {"sm_mhz": statistics.median(sms), "sm_max_mhz": max(maxes), "reasons": sorted(reasons),
+                "samples": len(sms)}
+
+
+def peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic():
+    """Per-launch DRAM traffic of the solve kernel from the committed ncu
+    summary (a `traffic_bytes_per_vertex:` line, scaled by the vertices one
+    launch processes), or None."""
+    path = os.path.join(ROOT, "profiles", "solve_kernel_cube.md")
+    try:
+        with open(path) as f:
+            for line in f:
+                if line.strip().startswith("traffic_bytes_per_vertex:"):
+                    return float(line.split(":", 1)[1].split()[0])
+    except OSError:
+        return None
+    return None
+
+
+def run_cpu_baseline(inp, args, threads=None):
+    """The CPU oracle (restatement of the reference step) on this host's cores
+    for one frame with two iterations of the same workload."""
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+
+    if threads:
+        O.set_threads(threads)
+    cores = O.max_threads()
+    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1)
+    o = O.OracleSolver(inp, s, precision=32)
+    iters = 2
+    t0 = time.perf_counter()
+    o.step_exact_iterations(iters)
+    dt = time.perf_counter() - t0
+    value = inp.active_vertex_count() * iters / dt
+    return {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"1 frame x {iters} iterations of the full {args.cells}^3 cube ({dt:.2f} s)"}, o
+
+
+def dist_env():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+def init_dist(world, backend):
+    if world <= 1:
+        return None
+    import datetime
+
+    import torch.distributed as dist
+
+    os.environ.setdefault("MASTER_ADDR", "127.0.0.1")
+    dist.init_process_group(backend=backend, timeout=datetime.timedelta(seconds=600))
+    return dist
+
+
+def reference_arm(args):
+    world, rank, _local = dist_env()
+    if rank != 0:
+        return 0
+    inp, cached = workload(args.cells)
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+
+    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1)
+    o = O.OracleSolver(inp, s, precision=32)
+    iters = 2  # bounded sample per step: one frame with two iterations
+    for _ in range(args.warmup):
+        o.step_exact_iterations(iters)
+    times = []
+    for _ in range(args.steps):
+        t0 = time.perf_counter()
+        o.step_exact_iterations(iters)
+        times.append(time.perf_counter() - t0)
+    total = sum(times)
+    active = inp.active_vertex_count()
+    value = active * iters * args.steps / total
+    cores = O.max_threads()
+    line = {
+        "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+        "config": workload_config(inp, args, {"cached": cached}) | {
+            "step": f"one frame with {iters} iterations (bounded CPU sample)"},
+        "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} steps of 1 frame x {iters} iterations of the full "
+                                   f"{args.cells}^3 cube on {cores} host threads"},
+        "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        "note": ("The reference step is TypeScript + WGSL for browser WebGPU and cannot run here; its Dawn "
+                 "SwiftShader CPU route is unavailable on this box.  This arm times the CPU restatement of the "
+                 "reference step (oracle/) on all host cores."),
+    }
+    print(json.dumps(line), flush=True)
+    return 0
+
+
+def ours_arm(args):
+    import numpy as np
+    import torch
+
+    from jgs2_b200 import solver
+
+    world, rank, local = dist_env()
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    device = local
+    # Rank 0 builds the precompute once; the others read it from the cache.
+    if rank == 0:
+        t0 = time.perf_counter()
+        inp, cached = workload(args.cells)
+        build_s = time.perf_counter() - t0
+    if dist is not None:
+        dist.barrier()
+    if rank != 0:
+        t0 = time.perf_counter()
+        inp, cached = workload(args.cells)
+        build_s = time.perf_counter() - t0
+    settings = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floorStiffness=0.0, parityMode=True,
+                    iterations=args.iterations, schedule=args.schedule)
+    s = solver.JGS2GpuSolver.create(inp, settings, device=device)
+    ptr, stream_ptr = s.devicePositions()
+    stream = torch.cuda.ExternalStream(stream_ptr, device=device)
+    iters = args.iterations
+    active = inp.active_vertex_count()
+
+    for _ in range(args.warmup):
+        s.stepExactIterations(iters)
+    s.awaitIdle()
+
+    # ---- device-resident timed region ---------------------------------------
+    launches0 = s.kernelLaunchCount()
+    start_ev = torch.cuda.Event(enable_timing=True)
+    end_ev = torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clocks:
+        start_ev.record(stream)
+        for _ in range(args.steps):
+            s.stepExactIterations(iters)
+        end_ev.record(stream)
+        end_ev.synchronize()
+    ms = start_ev.elapsed_time(end_ev)
+    launches = s.kernelLaunchCount() - launches0
+    torch.cuda.synchronize(device)
+    if dist is not None:
+        t = torch.tensor([ms], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms = float(t.item())
+    ms_per_step = ms / args.steps
+    value = world * active * iters * args.steps / (ms / 1e3)
+
+    # ---- per-kernel event timing (same workload, same stream) -----------------
+    prof = s.stepWithGpuTimestamps(max(1, min(args.steps, 3)), iters)
+    solve_launches, solve_ms = prof["solve"]
+    solve_avg_ms = solve_ms / max(1, solve_launches)
+    K = inp.cubature_k
+    algorithmic = inp.vertex_count * (84 + 152 * K) + 80 * inp.tet_count
+    achieved = algorithmic / (solve_avg_ms / 1e3) / 1e9
+    peak, peak_kind = peaks()
+    traffic_pv = profile_traffic()
+    roofline = {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "traffic": (traffic_pv * inp.vertex_count) if traffic_pv else None,
+                "kernel": "solve (per-vertex JGS2 local solve, one launch per iteration)",
+                "algorithmic_bytes_per_launch": algorithmic,
+                "algorithmic_bytes_formula": "V*(84+152K)+80T",
+                "avg_launch_ms": solve_avg_ms, "peak_source": f"{peak_kind} hbm_gbs",
+                "kernel_ms_per_frame": {k: v[1] / max(1, min(args.steps, 3)) for k, v in prof.items() if v[0]}}
+
+    # ---- end-to-end through the public API ------------------------------------
+    V = inp.vertex_count
+    forces_host = torch.zeros(3 * V, dtype=torch.float32).pin_memory()
+    pos_host = torch.empty(4 * V, dtype=torch.float32).pin_memory()
+    f_np = forces_host.numpy()
+    p_np = pos_host.numpy()
+    e2e_steps = max(1, min(args.steps, 5))
+    torch.cuda.synchronize(device)
+    lat = []
+    t_e2e = time.perf_counter()
+    for _ in range(e2e_steps):
+        t0 = time.perf_counter()
+        s.replaceExternalForces(f_np)
+        s.stepExactIterations(iters)
+        s.readPositions(out=p_np)
+        lat.append(time.perf_counter() - t0)
+    e2e_total = time.perf_counter() - t_e2e
+    if dist is not None:
+        t = torch.tensor([e2e_total], device=f"cuda:{device}")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_total = float(t.item())
+    e2e_value = world * active * iters * e2e_steps / e2e_total
+
+    cpu = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        cpu, _o = run_cpu_baseline(inp, args)
+    s.destroy()
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": workload_config(inp, args, {"cached": cached, "seconds": round(build_s, 1)}) | {
+                "parallelism": "replicas" if world > 1 else "single GPU"},
+            "frames_per_s": world * 1e3 / ms_per_step,
+            "gpu_launches": int(launches),
+            "roofline": roofline,
+            "cpu_baseline": cpu,
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(forces_host.numel() * 4),
+                    "d2h_bytes_per_step": int(pos_host.numel() * 4),
+                    "p50_ms": 1e3 * statistics.median(lat), "steps": e2e_steps},
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse_args()
+    if args.impl == "reference":
+        return reference_arm(args)
+    return ours_arm(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

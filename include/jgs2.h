@@ -250,6 +250,24 @@ jgs2_status jgs2_step_frames_exact_iterations(jgs2_solver* solver,
 /* awaitIdle() (:2496-2499). */
 jgs2_status jgs2_sync(jgs2_solver* solver);
 
+/* Per-kernel GPU timing of stepped frames: the counterpart of the reference's
+ * GPU-timestamp step variants (stepWithGpuTimestamp / stepFramesWith-
+ * GpuTimestampWrites, :1869-1972).  Frames run exactly like
+ * jgs2_step_frames_exact_iterations but without graph replay, with a CUDA
+ * event pair around every kernel on the solver stream; the call waits for the
+ * frames and fills one entry per kernel kind. */
+#define JGS2_PROFILE_KINDS 8
+typedef struct jgs2_kernel_profile {
+  uint32_t kinds;
+  uint32_t launches[JGS2_PROFILE_KINDS];
+  double milliseconds[JGS2_PROFILE_KINDS];
+  char names[JGS2_PROFILE_KINDS][24];
+} jgs2_kernel_profile;
+
+jgs2_status jgs2_step_with_gpu_timestamps(jgs2_solver* solver, uint32_t frame_count, uint32_t iterations,
+                                          const jgs2_settings* overrides, uint32_t override_mask,
+                                          jgs2_kernel_profile* out);
+
 /* ---- objectives -------------------------------------------------------- */
 
 /* setExternalForce (:1576-1611). */

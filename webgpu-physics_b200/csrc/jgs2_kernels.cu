@@ -22,6 +22,8 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 
+#include <algorithm>
+
 #include "jgs2_device.cuh"
 #include "jgs2_kernels.cuh"
 
@@ -386,7 +388,7 @@ __global__ void __launch_bounds__(kBlock) solveKernel(Buffers b, const DevParams
   __syncthreads();
   const uint32_t lane = threadIdx.x % W;
   const uint32_t group = threadIdx.x / W;
-  const uint32_t groupsPerBlock = kBlock / W;
+  const uint32_t groupsPerBlock = blockDim.x / W;
   const uint32_t item = blockIdx.x * groupsPerBlock + group;
   const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x & 31u) / W * W));
   const bool isLatched = latched(p, fs);
@@ -1049,11 +1051,30 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
                 uint32_t count, uint32_t K, bool glob, cudaStream_t s) {
   (void)glob;
   if (count == 0) return 0;
-  constexpr int groups = kBlock / kGroup;
+  const uint32_t groups = solveGroupsPerBlock(K);
+  if (groups == 0) return 0;
   const size_t smem = static_cast<size_t>(groups) * K * sizeof(CubState);
   const uint32_t blocks = (count + groups - 1) / groups;
-  solveKernel<kGroup><<<blocks, kBlock, smem, s>>>(b, p, src, tgt, list, count, K);
+  solveKernel<kGroup><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K);
   return 1;
+}
+
+uint32_t solveGroupsPerBlock(uint32_t K) {
+  // Shared memory holds one cached record state per cubature record of each
+  // vertex in the block; large K (an exact complement) trades vertices per
+  // block for cache.
+  static int optin = -1;
+  if (optin < 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) optin = 48 * 1024;
+    optin -= 1024;  // static shared memory of the kernel
+    cudaFuncSetAttribute(solveKernel<kGroup>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+  }
+  const uint32_t perVertex = static_cast<uint32_t>(K * sizeof(CubState));
+  uint32_t groups = kBlock / kGroup;
+  if (perVertex > 0) groups = std::min<uint32_t>(groups, static_cast<uint32_t>(optin) / perVertex);
+  return groups;
 }
 
 int launchCopy(const float4* src, float4* dst, uint32_t V, cudaStream_t s) {

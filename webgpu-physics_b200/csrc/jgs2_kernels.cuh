@@ -94,6 +94,8 @@ int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, f
 int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool glob,
                    bool bodyCorrection, uint32_t bodies, cudaStream_t s);
 
+// Vertices per solve block for cubature width K (0: K too large to cache).
+uint32_t solveGroupsPerBlock(uint32_t K);
 uint32_t gateBlockCount(uint32_t V, uint32_t T);
 uint32_t convBlockCount(uint32_t V);
 

@@ -539,47 +539,95 @@ DevParams makeParams(const jgs2_solver* s, const jgs2_settings& st, bool stop) {
 }
 
 // encodeFrame (src/simulation/gpu/jgs2-solver.ts:2207-2494) on the stream.
-int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bodyCorrection) {
+// Optional per-kernel CUDA event timing of an encoded frame.
+struct KernelProfiler {
+  static constexpr const char* kNames[JGS2_PROFILE_KINDS] = {"prologue", "vertex_frames", "tet_frames", "solve",
+                                                              "gate", "convergence", "copy", "epilogue"};
+  enum Kind { kPrologue = 0, kVertexFrames, kTetFrames, kSolve, kGate, kConvergence, kCopy, kEpilogue };
+  std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
+  std::vector<int> kinds;
+  size_t used = 0;
+  ~KernelProfiler() {
+    for (auto& e : pool) {
+      cudaEventDestroy(e.first);
+      cudaEventDestroy(e.second);
+    }
+  }
+  std::pair<cudaEvent_t, cudaEvent_t> next(int kind) {
+    if (used == pool.size()) {
+      cudaEvent_t a, b;
+      cudaEventCreate(&a);
+      cudaEventCreate(&b);
+      pool.emplace_back(a, b);
+      kinds.push_back(kind);
+    }
+    kinds[used] = kind;
+    return pool[used++];
+  }
+};
+
+// encodeFrame (src/simulation/gpu/jgs2-solver.ts:2207-2494) on the stream.
+int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bodyCorrection,
+                KernelProfiler* prof = nullptr) {
   const Buffers& b = s->b;
   cudaStream_t st = s->stream;
+  auto timed = [&](int kind, auto&& launch) -> int {
+    if (!prof) return launch();
+    const auto ev = prof->next(kind);
+    cudaEventRecord(ev.first, st);
+    const int k = launch();
+    cudaEventRecord(ev.second, st);
+    return k;
+  };
+  using P = KernelProfiler;
   int n = 0;
-  n += jgs2::launchPrologue(b, s->dParams, s->V, s->T, s->glob, st);
-  if (!s->glob) n += jgs2::launchVertexPolar(b, s->dParams, b.pos[1], nullptr, s->V, st);
+  n += timed(P::kPrologue, [&] { return jgs2::launchPrologue(b, s->dParams, s->V, s->T, s->glob, st); });
+  if (!s->glob)
+    n += timed(P::kVertexFrames, [&] { return jgs2::launchVertexPolar(b, s->dParams, b.pos[1], nullptr, s->V, st); });
   const bool colored = schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL;
   for (uint32_t it = 0; it < iterations; ++it) {
     float4* src = (it % 2 == 0) ? b.pos[1] : b.pos[0];
     float4* tgt = (it % 2 == 0) ? b.pos[0] : b.pos[1];
     const bool last = it + 1 == iterations;
     if (colored) {
-      n += jgs2::launchCopy(src, tgt, s->V, st);
+      n += timed(P::kCopy, [&] { return jgs2::launchCopy(src, tgt, s->V, st); });
       for (uint32_t c = 0; c < s->colorCount; ++c) {
-        if (!s->glob) n += jgs2::launchTetPolar(b, s->dParams, tgt, s->T, st);
+        if (!s->glob) n += timed(P::kTetFrames, [&] { return jgs2::launchTetPolar(b, s->dParams, tgt, s->T, st); });
         const uint32_t nb = s->needOffsets[c], ne = s->needOffsets[c + 1];
-        if (last && c + 1 == s->colorCount)
-          n += jgs2::launchVertexPolar(b, s->dParams, tgt, nullptr, s->V, st);
-        else
-          n += jgs2::launchVertexPolar(b, s->dParams, tgt, s->dNeedVertices + nb, ne - nb, st);
+        n += timed(P::kVertexFrames, [&] {
+          // The final colour of the frame refreshes every frame so the stored
+          // frames match a full vertexPolarRotation pass.
+          if (last && c + 1 == s->colorCount) return jgs2::launchVertexPolar(b, s->dParams, tgt, nullptr, s->V, st);
+          return jgs2::launchVertexPolar(b, s->dParams, tgt, s->dNeedVertices + nb, ne - nb, st);
+        });
         const uint32_t cb = s->colorOffsets[c], ce = s->colorOffsets[c + 1];
-        n += jgs2::launchSolve(b, s->dParams, tgt, tgt, s->dColorVertices + cb, ce - cb, s->K, s->glob, st);
+        n += timed(P::kSolve, [&] {
+          return jgs2::launchSolve(b, s->dParams, tgt, tgt, s->dColorVertices + cb, ce - cb, s->K, s->glob, st);
+        });
       }
     } else {
       if (!s->glob) {
-        n += jgs2::launchTetPolar(b, s->dParams, src, s->T, st);
-        if (it > 0) n += jgs2::launchVertexPolar(b, s->dParams, src, nullptr, s->V, st);
+        n += timed(P::kTetFrames, [&] { return jgs2::launchTetPolar(b, s->dParams, src, s->T, st); });
+        if (it > 0)
+          n += timed(P::kVertexFrames, [&] { return jgs2::launchVertexPolar(b, s->dParams, src, nullptr, s->V, st); });
       }
-      n += jgs2::launchSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, s->glob, st);
+      n += timed(P::kSolve, [&] { return jgs2::launchSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, s->glob, st); });
     }
     if (s->glob) {
-      n += jgs2::launchGate(b, s->dParams, src, tgt, s->V, s->T, st);
-      n += jgs2::launchConvergence(b, s->dParams, src, tgt, s->V, !colored && !last, st);
+      n += timed(P::kGate, [&] { return jgs2::launchGate(b, s->dParams, src, tgt, s->V, s->T, st); });
+      n += timed(P::kConvergence,
+                 [&] { return jgs2::launchConvergence(b, s->dParams, src, tgt, s->V, !colored && !last, st); });
     }
   }
   const float4* finalPos = (iterations % 2 == 0) ? b.pos[1] : b.pos[0];
-  n += jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, s->glob, bodyCorrection, s->bodies, st);
+  n += timed(P::kEpilogue, [&] {
+    return jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, s->glob, bodyCorrection, s->bodies, st);
+  });
   return n;
 }
 
-jgs2_status runFrames(jgs2_solver* s, const jgs2_settings& st, uint32_t frames, uint32_t iterations, bool stop) {
+jgs2_status runFrames(jgs2_solver* s, const jgs2_settings& st, uint32_t frames, uint32_t iterations, bool stop,
+                      KernelProfiler* prof = nullptr) {
   if (s->glob && iterations > JGS2_HISTORY_CAPACITY)
     return fail(s, JGS2_INVALID_ARGUMENT,
                 format("Stable JGS2 records at most %u nonlinear iterations per frame; got %u.",
@@ -597,7 +645,7 @@ jgs2_status runFrames(jgs2_solver* s, const jgs2_settings& st, uint32_t frames, 
   CUDA_TRY(s, cudaMemcpyAsync(s->dParams, &p, sizeof(p), cudaMemcpyHostToDevice, s->stream));
   const bool body = st.horizontal_body_correction != 0;
   const auto key = std::make_tuple(iterations, st.schedule, body);
-  if (s->useGraphs) {
+  if (s->useGraphs && !prof) {
     auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
       cudaGraph_t graph = nullptr;
@@ -616,7 +664,7 @@ jgs2_status runFrames(jgs2_solver* s, const jgs2_settings& st, uint32_t frames, 
       s->launches += static_cast<uint64_t>(it->second.second);
     }
   } else {
-    for (uint32_t f = 0; f < frames; ++f) s->launches += encodeFrame(s, iterations, st.schedule, body);
+    for (uint32_t f = 0; f < frames; ++f) s->launches += encodeFrame(s, iterations, st.schedule, body, prof);
   }
   CUDA_TRY(s, cudaGetLastError());
   s->submitted = st;
@@ -631,7 +679,7 @@ uint32_t normalizeOdd(uint32_t it) {
 }
 
 jgs2_status stepCommon(jgs2_solver* s, uint32_t frames, int exactIterations, const jgs2_settings* o,
-                       uint32_t mask, bool batch) {
+                       uint32_t mask, bool batch, KernelProfiler* prof = nullptr) {
   if (!s) return fail(nullptr, JGS2_INVALID_ARGUMENT, "solver is NULL.");
   if (s->destroyed) return fail(s, JGS2_DESTROYED, "JGS2GpuSolver has been destroyed.");
   if (batch && (frames < 1 || frames > JGS2_MAX_BATCH_FRAMES))
@@ -654,7 +702,7 @@ jgs2_status stepCommon(jgs2_solver* s, uint32_t frames, int exactIterations, con
   if (s->glob && s->objectiveFlags != 0 && st.horizontal_body_correction) st.horizontal_body_correction = 0;
   const bool production = exactIterations < 0;
   const uint32_t iterations = production ? normalizeOdd(st.iterations) : static_cast<uint32_t>(exactIterations);
-  return runFrames(s, st, frames, iterations, production);
+  return runFrames(s, st, frames, iterations, production, prof);
 }
 
 jgs2_status readRegion(jgs2_solver* s, const void* dev, size_t bytes, void* host) {
@@ -757,6 +805,8 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
   }
   std::unique_ptr<jgs2_solver> s(new jgs2_solver());
   s->device = device;
+  // JGS2_NO_GRAPHS=1 launches each frame's kernels directly (debugging).
+  s->useGraphs = std::getenv("JGS2_NO_GRAPHS") == nullptr;
   s->V = in->vertex_count;
   s->T = in->tet_count;
   s->K = in->cubature_k;
@@ -835,6 +885,10 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
   jgs2_solver* sp = s.get();
   cudaError_t ce = cudaSetDevice(device);
   if (ce != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, format("cudaSetDevice: %s", cudaGetErrorString(ce)));
+  if (jgs2::solveGroupsPerBlock(in->cubature_k) == 0)
+    return fail(nullptr, JGS2_UNSUPPORTED,
+                format("cubatureK %u is too large for the shared-memory record cache of one vertex.",
+                       in->cubature_k));
   ce = cudaStreamCreateWithFlags(&sp->stream, cudaStreamNonBlocking);
   if (ce != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, format("cudaStreamCreate: %s", cudaGetErrorString(ce)));
   auto bail = [&](jgs2_status st) {
@@ -1059,6 +1113,26 @@ jgs2_status jgs2_step_exact_iterations(jgs2_solver* s, uint32_t iterations, cons
 jgs2_status jgs2_step_frames_exact_iterations(jgs2_solver* s, uint32_t frames, uint32_t iterations,
                                               const jgs2_settings* o, uint32_t mask) {
   return stepCommon(s, frames, static_cast<int>(iterations), o, mask, true);
+}
+
+jgs2_status jgs2_step_with_gpu_timestamps(jgs2_solver* s, uint32_t frames, uint32_t iterations,
+                                          const jgs2_settings* o, uint32_t mask, jgs2_kernel_profile* out) {
+  if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  KernelProfiler prof;
+  jgs2_status st = stepCommon(s, frames, static_cast<int>(iterations), o, mask, true, &prof);
+  if (st != JGS2_OK) return st;
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  std::memset(out, 0, sizeof(*out));
+  out->kinds = JGS2_PROFILE_KINDS;
+  for (int k = 0; k < JGS2_PROFILE_KINDS; ++k)
+    std::snprintf(out->names[k], sizeof(out->names[k]), "%s", KernelProfiler::kNames[k]);
+  for (size_t i = 0; i < prof.used; ++i) {
+    float ms = 0.f;
+    CUDA_TRY(s, cudaEventElapsedTime(&ms, prof.pool[i].first, prof.pool[i].second));
+    out->milliseconds[prof.kinds[i]] += ms;
+    out->launches[prof.kinds[i]] += 1;
+  }
+  return JGS2_OK;
 }
 
 jgs2_status jgs2_sync(jgs2_solver* s) {

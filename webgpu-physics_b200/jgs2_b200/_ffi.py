@@ -83,6 +83,16 @@ class Info(Structure):
     ]
 
 
+PROFILE_KINDS = 8
+
+
+class KernelProfile(Structure):
+    _fields_ = [
+        ("kinds", c_uint32), ("launches", c_uint32 * PROFILE_KINDS),
+        ("milliseconds", c_double * PROFILE_KINDS), ("names", (ctypes.c_char * 24) * PROFILE_KINDS),
+    ]
+
+
 class PrecomputeOptions(Structure):
     _fields_ = [
         ("timestep", c_double), ("cubature_k", c_uint32), ("method", c_uint32),
@@ -179,6 +189,8 @@ def step_lib() -> ctypes.CDLL:
         lib.jgs2_step_exact_iterations.argtypes = [vp, c_uint32, S, c_uint32]
         lib.jgs2_step_frames_exact_iterations.argtypes = [vp, c_uint32, c_uint32, S, c_uint32]
         lib.jgs2_sync.argtypes = [vp]
+        lib.jgs2_step_with_gpu_timestamps.argtypes = [vp, c_uint32, c_uint32, S, c_uint32,
+                                                      POINTER(KernelProfile)]
         lib.jgs2_set_external_force.argtypes = [vp, c_uint32, POINTER(c_float)]
         lib.jgs2_replace_external_forces.argtypes = [vp, POINTER(c_float)]
         lib.jgs2_clear_external_forces.argtypes = [vp]

@@ -105,6 +105,22 @@ class SceneInput:
                               else getattr(self, f.name))
                      for f in dataclasses.fields(self)})
 
+    def save(self, path: str):
+        arrays = {f.name: getattr(self, f.name) for f in dataclasses.fields(self)
+                  if isinstance(getattr(self, f.name), np.ndarray)}
+        meta = np.array([self.vertex_count, self.tet_count, self.cubature_k], dtype=np.int64)
+        tmp = path + ".tmp.npz"
+        np.savez(tmp, __meta=meta, **arrays)
+        import os
+        os.replace(tmp, path)
+
+    @classmethod
+    def load(cls, path: str) -> "SceneInput":
+        with np.load(path) as z:
+            meta = z["__meta"]
+            kwargs = {k: z[k] for k in z.files if k != "__meta"}
+        return cls(vertex_count=int(meta[0]), tet_count=int(meta[1]), cubature_k=int(meta[2]), **kwargs)
+
     def bbox_diagonal(self) -> float:
         p = self.positions.reshape(-1, 4)[:, :3].astype(np.float64)
         return float(np.linalg.norm(p.max(axis=0) - p.min(axis=0)))

@@ -241,6 +241,17 @@ class JGS2GpuSolver:
         self._check(self._L.jgs2_step_frames_exact_iterations(self._h, int(frameCount), int(iterations),
                                                               byref(o), m))
 
+    def stepWithGpuTimestamps(self, frameCount: int, iterations: int, overrides: Optional[dict] = None) -> dict:
+        """Step frames with CUDA events around every kernel; returns
+        {kind: (launches, milliseconds)} (waits for the frames)."""
+        self._usable()
+        o, m = settings_struct(overrides)
+        prof = _ffi.KernelProfile()
+        self._check(self._L.jgs2_step_with_gpu_timestamps(self._h, int(frameCount), int(iterations), byref(o), m,
+                                                          byref(prof)))
+        return {prof.names[k].value.decode(): (int(prof.launches[k]), float(prof.milliseconds[k]))
+                for k in range(prof.kinds)}
+
     def awaitIdle(self):
         self._usable()
         self._check(self._L.jgs2_sync(self._h))
@@ -294,8 +305,16 @@ class JGS2GpuSolver:
         self._check(fn(self._h, _ffi.fptr(out), out.size))
         return out
 
-    def readPositions(self) -> np.ndarray:
-        return self._read(self._L.jgs2_read_positions, 4)
+    def readPositions(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        """Positions (4 floats per vertex); `out` may be a caller-owned
+        (e.g. pinned) float32 array to read into."""
+        if out is None:
+            return self._read(self._L.jgs2_read_positions, 4)
+        self._usable()
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size < 4 * self.vertexCount:
+            raise JGS2RangeError(1, "out must be a contiguous float32 array with 4 floats per vertex.")
+        self._check(self._L.jgs2_read_positions(self._h, _ffi.fptr(out), out.size))
+        return out
 
     def readVelocities(self) -> np.ndarray:
         return self._read(self._L.jgs2_read_velocities, 4)
