@@ -313,6 +313,17 @@ jgs2_status jgs2_read_globalization(jgs2_solver* solver, float* local,
                                     float* history, size_t history_floats,
                                     uint32_t* history_count);
 
+/* evaluateAssembledCandidateForTest(source, candidate, overrides)
+ * (:2611-2726): run the production assembled gate (vertex energies,
+ * candidate determinants, reduce, whole-pose revert) and the convergence
+ * reduction once on a given source / candidate pose pair (4 * V floats each,
+ * host).  The canonical pose becomes the accepted one.  positions_out (4 * V),
+ * control_out (16) and history_out (32: the single record) may be NULL. */
+jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* solver, const float* source_positions,
+                                              const float* candidate_positions,
+                                              const jgs2_settings* overrides, uint32_t override_mask,
+                                              float* positions_out, float* control_out, float* history_out);
+
 /* Zero-copy consumers (the reference's currentPositionBuffer, :1504-1507):
  * device address of the canonical vec4 position array and the solver's
  * cudaStream_t.  Valid until jgs2_destroy. */

@@ -1643,6 +1643,36 @@ int jgs2_oracle_local_system(void* handle, const jgs2_settings* settings, uint32
   return 0;
 }
 
+// evaluateAssembledCandidateForTest (src/simulation/gpu/jgs2-solver.ts:2611-2726):
+// posB = source, posA = candidate, predicted = source, local records and
+// control cleared, then assembled energies, the determinant gate and the
+// convergence reduction of one iteration.  Poses are 4 floats per vertex.
+int jgs2_oracle_evaluate_candidate(void* handle, const jgs2_settings* settings, const float* source,
+                                   const float* candidate) {
+  Handle* h = static_cast<Handle*>(handle);
+  if (!h || !settings || !source || !candidate) return 1;
+  auto body = [&](auto& o, auto zero) {
+    using T = decltype(zero);
+    applySettings(o, settings, false);
+    for (uint32_t v = 0; v < o.V; ++v) {
+      o.posB[v] = v3<T>(source[4 * v], source[4 * v + 1], source[4 * v + 2]);
+      o.posA[v] = v3<T>(candidate[4 * v], candidate[4 * v + 1], candidate[4 * v + 2]);
+      o.predicted[v] = o.posB[v];
+    }
+    for (auto& l : o.local) l = {0, 0, 0, 0};
+    for (auto& c : o.control) c = {0, 0, 0, 0};
+    o.bind(&o.posB, &o.posA, -1);
+    o.assembledVertexEnergyAll();
+    o.candidateTetrahedron();
+    o.reduceCandidate();
+    o.applyCandidate();
+    o.convergenceGradient();
+    o.reduceConvergence();
+  };
+  if (h->dbl) body(h->d, 0.0); else body(h->f, 0.0f);
+  return 0;
+}
+
 // Replace the objective records (forces 3V, targets 3V + stiffness V); NULL
 // arrays are left unchanged.  Recomputes the activity flags.
 int jgs2_oracle_set_objectives(void* handle, const float* forces, const float* targets, const float* stiffness) {

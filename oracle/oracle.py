@@ -79,6 +79,7 @@ def lib():
         L.jgs2_oracle_read.argtypes = [c_void_p, c_int, POINTER(c_float)]
         L.jgs2_oracle_set_objectives.argtypes = [c_void_p, POINTER(c_float), POINTER(c_float),
                                                  POINTER(c_float)]
+        L.jgs2_oracle_evaluate_candidate.argtypes = [c_void_p, c_void_p, POINTER(c_float), POINTER(c_float)]
         _lib = L
     return _lib
 
@@ -147,6 +148,21 @@ class OracleSolver:
 
     def step_frames_exact_iterations(self, frames, iterations, **overrides):
         self._run(frames, iterations, False, overrides)
+
+    def evaluate_assembled_candidate(self, source, candidate, **overrides) -> dict:
+        """Gate + convergence of one source/candidate pose pair (4 floats per
+        vertex); {'positions', 'control', 'history'} like the product call."""
+        s = resolve_settings(self.defaults, **overrides)
+        rec = _settings_struct(s)
+        src = np.ascontiguousarray(source, dtype=np.float32).reshape(-1)
+        cand = np.ascontiguousarray(candidate, dtype=np.float32).reshape(-1)
+        assert src.size == cand.size == 4 * self.vertex_count
+        rc = self._L.jgs2_oracle_evaluate_candidate(self._h, ctypes.byref(rec), src.ctypes.data_as(POINTER(c_float)),
+                                                    cand.ctypes.data_as(POINTER(c_float)))
+        if rc != 0:
+            raise RuntimeError("oracle candidate evaluation failed")
+        return {"positions": self.read("positions"), "control": self.read("control"),
+                "history": self.read("history")[:32]}
 
     def read(self, what: str) -> np.ndarray:
         which, per_vertex = self.READS[what]

@@ -91,15 +91,6 @@ __device__ __forceinline__ M3 loadBlock(const float* __restrict__ b) {
   return {f3(b[0], b[3], b[6]), f3(b[1], b[4], b[7]), f3(b[2], b[5], b[8])};
 }
 
-// Order-preserving encodings so atomicMin/atomicMax on uint give float min/max.
-__device__ __forceinline__ uint32_t orderedEncode(float f) {
-  const uint32_t u = __float_as_uint(f);
-  return (u & 0x80000000u) ? ~u : (u | 0x80000000u);
-}
-__device__ __forceinline__ float orderedDecode(uint32_t u) {
-  return __uint_as_float((u & 0x80000000u) ? (u & 0x7fffffffu) : ~u);
-}
-
 __device__ __forceinline__ uint32_t controlBits(float packed) {
   if (!finiteS(packed) || packed < 0.0f || packed > float(kControlMask) || packed != floorf(packed)) return 0u;
   return static_cast<uint32_t>(packed);
@@ -228,102 +219,6 @@ __device__ __forceinline__ M3 vertexFrame(const Buffers& b, const float4* __rest
   return polarRotation(avg, eps);
 }
 
-// ---------------------------------------------------------------------------
-// Prologue: predict (jgs2-shader.ts:2660-2692), iteration-0 vertex frames and
-// the source feasibility preflight (candidateTetrahedron + reduceCandidate on
-// the accepted pose, jgs2-solver.ts:2240-2259).
-__global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevParams* __restrict__ pp, uint32_t V,
-                                                         uint32_t T, int glob) {
-  __shared__ double scratch[2 * kBlock];
-  __shared__ bool isLast;
-  const DevParams p = *pp;
-  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  FrameState* fs = b.frame;
-  if (i < V) {
-    const float4 o = b.pos[0][i];
-    b.old[i] = make_float4(o.x, o.y, o.z, 1.0f);
-    const uint4 info = b.vinfo[i];
-    const float4 rm = b.restMass[i];
-    float3 pred = xyz(rm);
-    if (!isPinned(info)) {
-      const float3 vel = p.velocityDamping * xyz(b.velocity[i]);
-      pred = xyz(o) + p.dt * vel + (p.dt * p.dt) * f3(p.gravity[0], p.gravity[1], p.gravity[2]);
-    } else {
-      b.velocity[i] = make_float4(0, 0, 0, 0);
-    }
-    b.predicted[i] = make_float4(pred.x, pred.y, pred.z, 1.0f);
-    const float3 src = glob ? xyz(o) : pred;
-    b.pos[1][i] = make_float4(src.x, src.y, src.z, 1.0f);
-    b.finalUpdate[i] = 0.0f;
-    // Iteration-0 frames from the accepted pose (the stable iteration source).
-    if (glob) storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
-  }
-  if (!glob) return;
-  double sums[2] = {0.0, 0.0};
-  float localMin = kF32Max;
-  uint32_t bits = kSourceGeometryValid | kCandidateGeometryValid | kSourceEnergyValid | kCandidateEnergyValid;
-  if (i < T) {
-    const TetRec r = loadTet(b.tets, i);
-    const M3 F = deformationAt(r, b.pos[0]);
-    const float J = mdet(F);
-    if (finiteS(J)) {
-      localMin = J;
-      if (J > kDeterminantFloor) {
-        const float e = r.vol * snhEnergy(F, r.lambda, r.mu);
-        if (finiteS(e)) { sums[0] += e; sums[1] += e; }
-        else bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
-      } else {
-        bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
-      }
-    } else {
-      bits &= ~(kSourceGeometryValid | kCandidateGeometryValid | kSourceEnergyValid | kCandidateEnergyValid);
-    }
-  }
-  if (i < V) {
-    const uint4 info = b.vinfo[i];
-    const float e = implicitEnergy(p, b, i, xyz(b.pos[0][i]), info);
-    if (finiteS(e)) { sums[0] += e; sums[1] += e; }
-    else bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
-  }
-  const uint32_t wmin = __reduce_min_sync(0xffffffffu, orderedEncode(localMin));
-  const uint32_t wbits = __reduce_and_sync(0xffffffffu, bits);
-  if ((threadIdx.x & 31) == 0) {
-    atomicMin(&fs->gateMinSource, wmin);
-    if (wbits != 0xffffffffu) atomicAnd(&fs->gateBits, wbits);
-  }
-  blockSumDoubles<2>(sums, scratch);
-  if (threadIdx.x == 0) {
-    b.gatePartials[2 * blockIdx.x] = sums[0];
-    b.gatePartials[2 * blockIdx.x + 1] = sums[1];
-    __threadfence();
-    const uint32_t ticket = atomicAdd(&fs->prologueTicket, 1u);
-    isLast = ticket == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!isLast || threadIdx.x != 0) return;
-  __threadfence();
-  double e0 = 0.0;
-  for (uint32_t k = 0; k < gridDim.x; ++k) e0 += b.gatePartials[2 * k];
-  const float m = orderedDecode(atomicAdd(&fs->gateMinSource, 0u));
-  uint32_t vb = atomicAdd(&fs->gateBits, 0u);
-  if (T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
-  const bool gv = (vb & kSourceGeometryValid) != 0u;
-  const bool ev = (vb & kSourceEnergyValid) != 0u && finiteS(float(e0));
-  const bool accepted = gv && m > kDeterminantFloor;
-  uint32_t cbits = (vb & (kSourceGeometryValid | kCandidateGeometryValid)) | kLocalNumericsValid;
-  if (gv) cbits |= kAcceptedMinimumValid;
-  // predict clears the control records; the preflight then writes them with
-  // history index 0 (jgs2-shader.ts:2687-2691, 3916-3953).
-  fs->control[0] = make_float4(gv ? m : 0.f, gv ? m : 0.f, gv ? m : 0.f, float(cbits));
-  fs->control[1] = make_float4(accepted ? 1.f : 0.f, accepted ? 0.f : 1.f, 0.f, 0.f);
-  fs->control[2] = make_float4(ev ? float(e0) : 0.f, ev ? float(e0) : 0.f, ev ? float(e0) : 0.f, ev ? 1.f : 0.f);
-  fs->control[3] = make_float4(0, 0, 0, 0);
-  fs->gateMinSource = orderedEncode(kF32Max);
-  fs->gateMinCandidate = orderedEncode(kF32Max);
-  fs->gateBits = 0xffffffffu;
-  fs->prologueTicket = 0u;
-}
-
 // Vertex frames for a list of vertices (or all) from pose x.
 __global__ void __launch_bounds__(kBlock) vertexPolarKernel(Buffers b, const DevParams* __restrict__ pp,
                                                             const float4* __restrict__ x,
@@ -375,7 +270,10 @@ struct CubState {
 static_assert(sizeof(CubState) <= kRecFloats * 4, "cubature cache record too small");
 
 template <int W>
-__global__ void __launch_bounds__(kBlock) solveKernel(Buffers b, const DevParams* __restrict__ pp,
+#ifndef JGS2_SOLVE_MIN_BLOCKS
+#define JGS2_SOLVE_MIN_BLOCKS 4
+#endif
+__global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
                                                       const float4* __restrict__ src, float4* tgt,
                                                       const uint32_t* __restrict__ list, uint32_t count,
                                                       uint32_t K) {
@@ -389,14 +287,15 @@ __global__ void __launch_bounds__(kBlock) solveKernel(Buffers b, const DevParams
   const uint32_t lane = threadIdx.x % W;
   const uint32_t group = threadIdx.x / W;
   const uint32_t groupsPerBlock = blockDim.x / W;
-  const uint32_t item = blockIdx.x * groupsPerBlock + group;
   const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x & 31u) / W * W));
   const bool isLatched = latched(p, fs);
+  // Persistent grid: each lane group walks vertices with a grid stride.
+  for (uint32_t item = blockIdx.x * groupsPerBlock + group; item < count; item += gridDim.x * groupsPerBlock) {
   // Per-vertex outputs owned by lane 0.
   uint32_t status = kNonfinite, backtracks = 0, evals = 0;
   float shiftN = 0.0f;
   bool localValid = true, haveRecord = false;
-  if (item < count) {
+  {
     const uint32_t v = list ? list[item] : item;
     const uint4 info = b.vinfo[v];
     const float4 rm = b.restMass[v];
@@ -453,49 +352,65 @@ __global__ void __launch_bounds__(kBlock) solveKernel(Buffers b, const DevParams
             if (t != kEmptyTet && t < p.tetCount && w > 0.0f) {
               const TetRec r = loadTet(b.tets, t);
               const float* U = reinterpret_cast<const float*>(b.cubBasis + 9ull * rec);
-              M3 B[4];
-              float3 x[4];
+              // One basis block B_l = R_l Ubar_l R_s^T at a time: accumulate F,
+              // the projected directions dF_c = sum_l B_l[:,c] g_l^T and the
+              // inertia / objective quadratic (gQ, HQ) of the record.
+              M3 F = mzero(), dF0 = mzero(), dF1 = mzero(), dF2 = mzero();
               float3 gQ = f3(0, 0, 0);
               S3 HQ = szero();
               uint32_t slot = 4;
+              const float3 x0 = xyz(src[r.idx.x]);
 #pragma unroll
               for (int l = 0; l < 4; ++l) {
                 const uint32_t q = idxAt(r.idx, l);
                 if (q == v) slot = l;
-                B[l] = mm(mm(loadRot(b.vertexRot, q), loadBlock(U + 9 * l)), RsT);
-                x[l] = xyz(src[q]);
+                const float3 gl = shapeGradient(r, l);
+                const M3 B = mm(mm(loadRot(b.vertexRot, q), loadBlock(U + 9 * l)), RsT);
+                const float3 xl = l == 0 ? x0 : xyz(src[q]);
+                if (l > 0) F = F + outer(xl - x0, gl);
+                dF0 = dF0 + outer(B.c0, gl);
+                dF1 = dF1 + outer(B.c1, gl);
+                dF2 = dF2 + outer(B.c2, gl);
                 const uint4 qi = b.vinfo[q];
                 const float4 qr = b.restMass[q];
                 const float dW = distributedInertiaWeight(qr, qi, p.invDt2);
-                float3 lin = dW * (x[l] - xyz(b.predicted[q]));
+                float3 lin = dW * (xl - xyz(b.predicted[q]));
                 float quad = dW;
                 if (objActive && !isPinned(qi)) {
                   const float nq = float(qi.y > 1u ? qi.y : 1u);
-                  lin = lin + objectiveGradient(p, b.objectives, q, x[l]) * (1.0f / nq);
+                  lin = lin + objectiveGradient(p, b.objectives, q, xl) * (1.0f / nq);
                   quad += targetStiffness(p, b.objectives, q) / nq;
                 }
-                gQ = gQ + mtv(B[l], lin);
-                saddScaled(HQ, quad, gramColumns(B[l]));
+                gQ = gQ + mtv(B, lin);
+                saddScaled(HQ, quad, gramColumns(B));
               }
-              const M3 F = deformation(r, x[0], x[1], x[2], x[3]);
-              const float3 g0 = -(r.g1 + r.g2 + r.g3);
-              const M3 dF0 = outer(B[0].c0, g0) + outer(B[1].c0, r.g1) + outer(B[2].c0, r.g2) + outer(B[3].c0, r.g3);
-              const M3 dF1 = outer(B[0].c1, g0) + outer(B[1].c1, r.g1) + outer(B[2].c1, r.g2) + outer(B[3].c1, r.g3);
-              const M3 dF2 = outer(B[0].c2, g0) + outer(B[1].c2, r.g1) + outer(B[2].c2, r.g2) + outer(B[3].c2, r.g3);
               const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
               const M3 P = piola(F, pt);
               float3 pg = r.vol * f3(frob(dF0, P), frob(dF1, P), frob(dF2, P)) + gQ;
-              // Reduced material Hessian vol <dF_r, DP[dF_c]>.
+              // Reduced material Hessian vol <dF_r, DP[dF_c]>; the cofactor
+              // term <A, Dcof[B]> is symmetric, so one directional cofactor is
+              // live at a time.
               const float p0 = frob(F, dF0), p1 = frob(F, dF1), p2 = frob(F, dF2);
               const float q0 = frob(pt.cof, dF0), q1 = frob(pt.cof, dF1), q2 = frob(pt.cof, dF2);
-              const M3 D0 = dcofactor(F, dF0), D1 = dcofactor(F, dF1), D2 = dcofactor(F, dF2);
               S3 ph;
-              ph.xx = pt.a * frob(dF0, dF0) + pt.c1 * p0 * p0 + r.lambda * q0 * q0 + pt.b * frob(dF0, D0);
-              ph.yy = pt.a * frob(dF1, dF1) + pt.c1 * p1 * p1 + r.lambda * q1 * q1 + pt.b * frob(dF1, D1);
-              ph.zz = pt.a * frob(dF2, dF2) + pt.c1 * p2 * p2 + r.lambda * q2 * q2 + pt.b * frob(dF2, D2);
-              ph.xy = pt.a * frob(dF0, dF1) + pt.c1 * p0 * p1 + r.lambda * q0 * q1 + pt.b * frob(dF0, D1);
-              ph.xz = pt.a * frob(dF0, dF2) + pt.c1 * p0 * p2 + r.lambda * q0 * q2 + pt.b * frob(dF0, D2);
-              ph.yz = pt.a * frob(dF1, dF2) + pt.c1 * p1 * p2 + r.lambda * q1 * q2 + pt.b * frob(dF1, D2);
+              {
+                const M3 D0 = dcofactor(F, dF0);
+                ph.xx = pt.b * frob(dF0, D0);
+                ph.xy = pt.b * frob(dF1, D0);
+                ph.xz = pt.b * frob(dF2, D0);
+              }
+              {
+                const M3 D1 = dcofactor(F, dF1);
+                ph.yy = pt.b * frob(dF1, D1);
+                ph.yz = pt.b * frob(dF2, D1);
+              }
+              ph.zz = pt.b * frob(dF2, dcofactor(F, dF2));
+              ph.xx += pt.a * frob(dF0, dF0) + pt.c1 * p0 * p0 + r.lambda * q0 * q0;
+              ph.yy += pt.a * frob(dF1, dF1) + pt.c1 * p1 * p1 + r.lambda * q1 * q1;
+              ph.zz += pt.a * frob(dF2, dF2) + pt.c1 * p2 * p2 + r.lambda * q2 * q2;
+              ph.xy += pt.a * frob(dF0, dF1) + pt.c1 * p0 * p1 + r.lambda * q0 * q1;
+              ph.xz += pt.a * frob(dF0, dF2) + pt.c1 * p0 * p2 + r.lambda * q0 * q2;
+              ph.yz += pt.a * frob(dF1, dF2) + pt.c1 * p1 * p2 + r.lambda * q1 * q2;
               ph.xx *= r.vol; ph.yy *= r.vol; ph.zz *= r.vol; ph.xy *= r.vol; ph.xz *= r.vol; ph.yz *= r.vol;
               sadd(ph, HQ);
               float3 gs = f3(0, 0, 0);
@@ -682,6 +597,7 @@ __global__ void __launch_bounds__(kBlock) solveKernel(Buffers b, const DevParams
     if (shiftN > 0.0f && finiteS(shiftN)) atomicMax(&sMaxShift, __float_as_uint(shiftN));
     if (!localValid) sValid = 0;
   }
+  }  // vertex loop
   __syncthreads();
   if (threadIdx.x == 0) {
     if (sFail) atomicAdd(&fs->localFailures, sFail);
@@ -694,82 +610,220 @@ __global__ void __launch_bounds__(kBlock) solveKernel(Buffers b, const DevParams
 }
 
 // ---------------------------------------------------------------------------
+// Grid-wide reductions.  Each of the prologue, gate and convergence kernels
+// runs on a persistent grid (a few blocks per SM, grid-stride loops), folds
+// its elements into one partial per block with a fixed tree, writes the
+// partial, and the last block to take a ticket folds all partials in block
+// order.  Results are deterministic for a given device; nothing waits.
+struct GatePartial {
+  double e0, e1;      // source / candidate assembled energy
+  float minS, minC;   // minimum determinant, source / candidate
+  uint32_t bits;      // AND of geometry / energy validity bits
+  uint32_t pad;
+};
+constexpr uint32_t kGateBits = kSourceGeometryValid | kCandidateGeometryValid | kSourceEnergyValid |
+                               kCandidateEnergyValid;
+
+__device__ __forceinline__ GatePartial gateIdentity() { return {0.0, 0.0, kF32Max, kF32Max, kGateBits, 0u}; }
+__device__ __forceinline__ void gateCombine(GatePartial& a, const GatePartial& b) {
+  a.e0 += b.e0;
+  a.e1 += b.e1;
+  a.minS = fminf(a.minS, b.minS);
+  a.minC = fminf(a.minC, b.minC);
+  a.bits &= b.bits;
+}
+
+struct ConvPartial {
+  double sq[6];     // squared norms: five components and their sum
+  float scale[6];   // max-abs entries (validity of the robust norm)
+  float maxUpdate;
+  uint32_t valid;
+};
+__device__ __forceinline__ ConvPartial convIdentity() {
+  ConvPartial p;
+  for (int c = 0; c < 6; ++c) { p.sq[c] = 0.0; p.scale[c] = 0.0f; }
+  p.maxUpdate = 0.0f;
+  p.valid = 1u;
+  return p;
+}
+__device__ __forceinline__ void convCombine(ConvPartial& a, const ConvPartial& b) {
+  for (int c = 0; c < 6; ++c) {
+    a.sq[c] += b.sq[c];
+    a.scale[c] = fmaxf(a.scale[c], b.scale[c]);
+  }
+  a.maxUpdate = fmaxf(a.maxUpdate, b.maxUpdate);
+  a.valid &= b.valid;
+}
+
+template <class P, class C>
+__device__ __forceinline__ P blockFold(P v, P* smem, C combine) {
+  smem[threadIdx.x] = v;
+  __syncthreads();
+  for (unsigned s = blockDim.x / 2; s > 0; s >>= 1) {
+    if (threadIdx.x < s) combine(smem[threadIdx.x], smem[threadIdx.x + s]);
+    __syncthreads();
+  }
+  P r = smem[0];
+  __syncthreads();
+  return r;
+}
+
+// Publishes the block partial; returns true in every thread of the last block.
+template <class P>
+__device__ __forceinline__ bool publishPartial(const P& blockValue, P* partials, uint32_t* ticket, bool* isLast) {
+  if (threadIdx.x == 0) {
+    partials[blockIdx.x] = blockValue;
+    __threadfence();
+    *isLast = atomicAdd(ticket, 1u) == gridDim.x - 1;
+  }
+  __syncthreads();
+  const bool last = *isLast;
+  if (last) __threadfence();
+  return last;
+}
+
+template <class P, class I, class C>
+__device__ __forceinline__ P foldPartials(const P* partials, P* smem, I identity, C combine) {
+  P acc = identity();
+  static_assert(sizeof(P) % 4 == 0, "partials are read as 32-bit words");
+  for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+    // Other blocks wrote these partials: read them from L2.
+    uint32_t words[sizeof(P) / 4];
+    const uint32_t* w = reinterpret_cast<const uint32_t*>(partials + k);
+#pragma unroll
+    for (unsigned i = 0; i < sizeof(P) / 4; ++i) words[i] = __ldcg(w + i);
+    P v;
+    memcpy(&v, words, sizeof(P));
+    combine(acc, v);
+  }
+  return blockFold(acc, smem, combine);
+}
+
+__device__ __forceinline__ void accumulateTet(GatePartial& acc, const TetRec& r, const M3& sF, const M3& cF) {
+  const float sJ = mdet(sF), cJ = mdet(cF);
+  const bool sgv = finiteS(sJ), cgv = finiteS(cJ);
+  if (sgv) acc.minS = fminf(acc.minS, sJ); else acc.bits &= ~kSourceGeometryValid;
+  if (cgv) acc.minC = fminf(acc.minC, cJ); else acc.bits &= ~kCandidateGeometryValid;
+  bool sev = false, cev = false;
+  if (sgv && sJ > kDeterminantFloor) {
+    const float e = r.vol * snhEnergy(sF, r.lambda, r.mu);
+    sev = finiteS(e);
+    if (sev) acc.e0 += e;
+  }
+  if (cgv && cJ > kDeterminantFloor) {
+    const float e = r.vol * snhEnergy(cF, r.lambda, r.mu);
+    cev = finiteS(e);
+    if (cev) acc.e1 += e;
+  }
+  if (!sev) acc.bits &= ~kSourceEnergyValid;
+  if (!cev) acc.bits &= ~kCandidateEnergyValid;
+}
+
+// ---------------------------------------------------------------------------
+// Prologue: predict (jgs2-shader.ts:2660-2692), iteration-0 vertex frames and
+// the source feasibility preflight (candidateTetrahedron + reduceCandidate on
+// the accepted pose, jgs2-solver.ts:2240-2259).
+__global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevParams* __restrict__ pp, uint32_t V,
+                                                         uint32_t T, int glob) {
+  __shared__ GatePartial smem[kBlock];
+  __shared__ bool isLast;
+  const DevParams p = *pp;
+  FrameState* fs = b.frame;
+  GatePartial acc = gateIdentity();
+  const uint32_t n = T > V ? T : V;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+    if (i < V) {
+      const float4 o = b.pos[0][i];
+      b.old[i] = make_float4(o.x, o.y, o.z, 1.0f);
+      const uint4 info = b.vinfo[i];
+      const float4 rm = b.restMass[i];
+      float3 pred = xyz(rm);
+      if (!isPinned(info)) {
+        const float3 vel = p.velocityDamping * xyz(b.velocity[i]);
+        pred = xyz(o) + p.dt * vel + (p.dt * p.dt) * f3(p.gravity[0], p.gravity[1], p.gravity[2]);
+      } else {
+        b.velocity[i] = make_float4(0, 0, 0, 0);
+      }
+      b.predicted[i] = make_float4(pred.x, pred.y, pred.z, 1.0f);
+      const float3 src = glob ? xyz(o) : pred;
+      b.pos[1][i] = make_float4(src.x, src.y, src.z, 1.0f);
+      b.finalUpdate[i] = 0.0f;
+      if (glob) {
+        // Iteration-0 frames from the accepted pose (the stable iteration source).
+        storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
+        const float e = implicitEnergy(p, b, i, xyz(o), info);
+        if (finiteS(e)) { acc.e0 += e; acc.e1 += e; }
+        else acc.bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
+      }
+    }
+    if (glob && i < T) {
+      const TetRec r = loadTet(b.tets, i);
+      const M3 F = deformationAt(r, b.pos[0]);
+      accumulateTet(acc, r, F, F);
+    }
+  }
+  if (!glob) return;  // uniform
+  const GatePartial blk = blockFold(acc, smem, gateCombine);
+  GatePartial* partials = reinterpret_cast<GatePartial*>(b.gatePartials);
+  if (!publishPartial(blk, partials, &fs->prologueTicket, &isLast)) return;
+  const GatePartial tot = foldPartials(partials, smem, gateIdentity, gateCombine);
+  if (threadIdx.x != 0) return;
+  uint32_t vb = tot.bits;
+  if (T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
+  const bool gv = (vb & kSourceGeometryValid) != 0u;
+  const float e0 = float(tot.e0);
+  const bool ev = (vb & kSourceEnergyValid) != 0u && finiteS(e0);
+  const float m = tot.minS;
+  const bool accepted = gv && m > kDeterminantFloor;
+  uint32_t cbits = (vb & (kSourceGeometryValid | kCandidateGeometryValid)) | kLocalNumericsValid;
+  if (gv) cbits |= kAcceptedMinimumValid;
+  // predict clears the control records; the preflight then writes them with
+  // history index 0 (jgs2-shader.ts:2687-2691, 3916-3953).
+  fs->control[0] = make_float4(gv ? m : 0.f, gv ? m : 0.f, gv ? m : 0.f, float(cbits));
+  fs->control[1] = make_float4(accepted ? 1.f : 0.f, accepted ? 0.f : 1.f, 0.f, 0.f);
+  fs->control[2] = make_float4(ev ? e0 : 0.f, ev ? e0 : 0.f, ev ? e0 : 0.f, ev ? 1.f : 0.f);
+  fs->control[3] = make_float4(0, 0, 0, 0);
+  fs->prologueTicket = 0u;
+}
+
+// ---------------------------------------------------------------------------
 // Gate: candidateTetrahedron (jgs2-shader.ts:3498-3601) + vertex energies
 // (assembledVertexEnergy :3489-3496) + reduceCandidate (:3611-3955).
 __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams* __restrict__ pp,
                                                      const float4* __restrict__ src,
                                                      const float4* __restrict__ tgt, uint32_t V, uint32_t T) {
-  __shared__ double scratch[2 * kBlock];
+  __shared__ GatePartial smem[kBlock];
   __shared__ bool isLast;
   const DevParams p = *pp;
   FrameState* fs = b.frame;
   if (latched(p, fs)) return;  // uniform across the grid
-  double sums[2] = {0.0, 0.0};
-  uint32_t bits = kSourceGeometryValid | kCandidateGeometryValid | kSourceEnergyValid | kCandidateEnergyValid;
-  float minS = kF32Max, minC = kF32Max;
-  for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < (T > V ? T : V); i += gridDim.x * kBlock) {
+  GatePartial acc = gateIdentity();
+  const uint32_t n = T > V ? T : V;
+  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
     if (i < T) {
       const TetRec r = loadTet(b.tets, i);
-      const M3 sF = deformationAt(r, src);
-      const M3 cF = deformationAt(r, tgt);
-      const float sJ = mdet(sF), cJ = mdet(cF);
-      const bool sgv = finiteS(sJ), cgv = finiteS(cJ);
-      if (sgv) minS = fminf(minS, sJ); else bits &= ~kSourceGeometryValid;
-      if (cgv) minC = fminf(minC, cJ); else bits &= ~kCandidateGeometryValid;
-      bool sev = false, cev = false;
-      if (sgv && sJ > kDeterminantFloor) {
-        const float e = r.vol * snhEnergy(sF, r.lambda, r.mu);
-        sev = finiteS(e);
-        if (sev) sums[0] += e;
-      }
-      if (cgv && cJ > kDeterminantFloor) {
-        const float e = r.vol * snhEnergy(cF, r.lambda, r.mu);
-        cev = finiteS(e);
-        if (cev) sums[1] += e;
-      }
-      if (!sev) bits &= ~kSourceEnergyValid;
-      if (!cev) bits &= ~kCandidateEnergyValid;
+      accumulateTet(acc, r, deformationAt(r, src), deformationAt(r, tgt));
     }
     if (i < V) {
       const uint4 info = b.vinfo[i];
       const float es = implicitEnergy(p, b, i, xyz(src[i]), info);
       const float ec = implicitEnergy(p, b, i, xyz(tgt[i]), info);
-      if (finiteS(es)) sums[0] += es; else bits &= ~kSourceEnergyValid;
-      if (finiteS(ec)) sums[1] += ec; else bits &= ~kCandidateEnergyValid;
+      if (finiteS(es)) acc.e0 += es; else acc.bits &= ~kSourceEnergyValid;
+      if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
     }
   }
-  const uint32_t wminS = __reduce_min_sync(0xffffffffu, orderedEncode(minS));
-  const uint32_t wminC = __reduce_min_sync(0xffffffffu, orderedEncode(minC));
-  const uint32_t wbits = __reduce_and_sync(0xffffffffu, bits);
-  if ((threadIdx.x & 31u) == 0u) {
-    atomicMin(&fs->gateMinSource, wminS);
-    atomicMin(&fs->gateMinCandidate, wminC);
-    if (wbits != 0xffffffffu) atomicAnd(&fs->gateBits, wbits);
-  }
-  blockSumDoubles<2>(sums, scratch);
-  if (threadIdx.x == 0) {
-    b.gatePartials[2 * blockIdx.x] = sums[0];
-    b.gatePartials[2 * blockIdx.x + 1] = sums[1];
-    __threadfence();
-    isLast = atomicAdd(&fs->gateTicket, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!isLast || threadIdx.x != 0) return;
-  __threadfence();
-  double e0 = 0.0, e1 = 0.0;
-  for (uint32_t k = 0; k < gridDim.x; ++k) {
-    e0 += b.gatePartials[2 * k];
-    e1 += b.gatePartials[2 * k + 1];
-  }
-  uint32_t vb = atomicAdd(&fs->gateBits, 0u) & (kSourceGeometryValid | kCandidateGeometryValid |
-                                                  kSourceEnergyValid | kCandidateEnergyValid);
-  if (!atomicAdd(&fs->localNumericsValid, 0u)) vb &= ~kLocalNumericsValid; else vb |= kLocalNumericsValid;
-  const float eS = float(e0), eC = float(e1);
+  const GatePartial blk = blockFold(acc, smem, gateCombine);
+  GatePartial* partials = reinterpret_cast<GatePartial*>(b.gatePartials);
+  if (!publishPartial(blk, partials, &fs->gateTicket, &isLast)) return;
+  const GatePartial tot = foldPartials(partials, smem, gateIdentity, gateCombine);
+  if (threadIdx.x != 0) return;
+  uint32_t vb = tot.bits;
+  if (__ldcg(&fs->localNumericsValid)) vb |= kLocalNumericsValid;
+  const float eS = float(tot.e0), eC = float(tot.e1);
   if (!finiteS(eS)) vb &= ~kSourceEnergyValid;
   if (!finiteS(eC)) vb &= ~kCandidateEnergyValid;
   if (T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
-  const float sm = orderedDecode(atomicAdd(&fs->gateMinSource, 0u));
-  const float cm = orderedDecode(atomicAdd(&fs->gateMinCandidate, 0u));
+  const float sm = tot.minS, cm = tot.minC;
   const bool sgv = (vb & kSourceGeometryValid) != 0u, cgv = (vb & kCandidateGeometryValid) != 0u;
   const bool sev = (vb & kSourceEnergyValid) != 0u, cev = (vb & kCandidateEnergyValid) != 0u;
   const bool accepted = (sgv && sm > kDeterminantFloor) && (cgv && cm > kDeterminantFloor);
@@ -783,18 +837,13 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
   if (finiteNonnegInt(packed, float(kHistoryCapacity))) historyIndex = static_cast<uint32_t>(packed);
   else vb &= ~kLocalNumericsValid;
   const uint32_t cb = vb & kValidityMask;
-  const uint32_t failures = atomicAdd(&fs->localFailures, 0u);
+  const uint32_t failures = __ldcg(&fs->localFailures);
   fs->control[0] = make_float4(sgv ? sm : 0.f, cgv ? cm : 0.f, amv ? am : 0.f, float(cb));
   fs->control[1] = make_float4(accepted ? 1.f : 0.f, accepted ? 0.f : 1.f, float(failures), float(historyIndex));
   fs->control[2] = make_float4(sev ? eS : 0.f, cev ? eC : 0.f, aev ? ae : 0.f, (sev && cev) ? 1.f : 0.f);
-  fs->control[3] = make_float4(__uint_as_float(atomicAdd(&fs->localMaxShift, 0u)),
-                               float(atomicAdd(&fs->localMaxBacktracks, 0u)),
-                               float(atomicAdd(&fs->localSkipped, 0u)),
-                               float(atomicAdd(&fs->localEvaluations, 0u)));
-  // Reset the accumulators for the next sweep.
-  fs->gateMinSource = orderedEncode(kF32Max);
-  fs->gateMinCandidate = orderedEncode(kF32Max);
-  fs->gateBits = 0xffffffffu;
+  fs->control[3] = make_float4(__uint_as_float(__ldcg(&fs->localMaxShift)), float(__ldcg(&fs->localMaxBacktracks)),
+                               float(__ldcg(&fs->localSkipped)), float(__ldcg(&fs->localEvaluations)));
+  // Reset the sweep accumulators for the next iteration.
   fs->localFailures = 0u;
   fs->localMaxBacktracks = 0u;
   fs->localSkipped = 0u;
@@ -807,22 +856,20 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
 // ---------------------------------------------------------------------------
 // applyCandidate (:3957-3983) + convergenceGradient (:3985-4097) +
 // reduceConvergence (:4105-4486), and the next iteration's vertex frames.
+// The five component norms are exact Euclidean norms accumulated in double;
+// the reference forms the same norms in f32 as scale * sqrt(sum((g/scale)^2)).
 __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const DevParams* __restrict__ pp,
                                                             const float4* __restrict__ src, float4* tgt,
                                                             uint32_t V, int nextRotations) {
-  __shared__ double scratch[6 * kBlock];
+  __shared__ ConvPartial smem[kBlock];
   __shared__ bool isLast;
   const DevParams p = *pp;
   FrameState* fs = b.frame;
   if (latched(p, fs)) return;  // uniform across the grid
   const bool accepted = fs->control[1].x == 1.0f;
   const float4* __restrict__ acc = accepted ? tgt : src;
-  double sq[6] = {0, 0, 0, 0, 0, 0};
-  float scale[6] = {0, 0, 0, 0, 0, 0};
-  float maxUpdate = 0.0f;
-  bool valid = true;
-  const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
-  if (v < V) {
+  ConvPartial part = convIdentity();
+  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
     float upd = 0.0f;
     if (!accepted) {
       tgt[v] = src[v];
@@ -830,19 +877,23 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
       upd = scaledLength(xyz(tgt[v]) - xyz(src[v]));
     }
     b.finalUpdate[v] = upd;
-    if (!(finiteS(upd) && upd >= 0.0f)) valid = false; else maxUpdate = upd;
+    if (!(finiteS(upd) && upd >= 0.0f)) part.valid = 0u; else part.maxUpdate = fmaxf(part.maxUpdate, upd);
     const uint4 info = b.vinfo[v];
     if (!isPinned(info)) {
       const float3 x = xyz(acc[v]);
       float3 comps[5];
       comps[0] = (b.restMass[v].w * p.invDt2) * (x - xyz(b.predicted[v]));
       float3 material = f3(0, 0, 0);
+      M3 avg = mzero();
+      float total = 0.0f;
       for (uint32_t a = 0; a < info.y; ++a) {
         const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
         const TetRec r = loadTet(b.tets, entry >> 2);
         const M3 F = deformationAt(r, acc);
         const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
         material = material + r.vol * mv(piola(F, pt), shapeGradient(r, entry & 3u));
+        avg = avg + r.vol * F;
+        total += r.vol;
       }
       comps[1] = material;
       comps[2] = f3(0, 0, 0);
@@ -856,67 +907,53 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
       }
       comps[4] = f3(0, 0, 0);
       if (p.floorStiffness > 0.0f && x.y < p.floorHeight) comps[4].y = p.floorStiffness * (x.y - p.floorHeight);
-      float3 total = f3(0, 0, 0);
+      float3 totalG = f3(0, 0, 0);
       bool tv = true;
 #pragma unroll
       for (int c = 0; c < 5; ++c) {
         const bool ok = finiteV(comps[c]);
         const float3 val = ok ? comps[c] : f3(0, 0, 0);
-        scale[c] = fmaxf(fabsf(val.x), fmaxf(fabsf(val.y), fabsf(val.z)));
-        sq[c] = double(val.x) * val.x + double(val.y) * val.y + double(val.z) * val.z;
-        total = total + val;
+        part.scale[c] = fmaxf(part.scale[c], fmaxf(fabsf(val.x), fmaxf(fabsf(val.y), fabsf(val.z))));
+        part.sq[c] += double(val.x) * val.x + double(val.y) * val.y + double(val.z) * val.z;
+        totalG = totalG + val;
         tv = tv && ok;
       }
-      tv = tv && finiteV(total);
+      tv = tv && finiteV(totalG);
       if (tv) {
-        scale[5] = fmaxf(fabsf(total.x), fmaxf(fabsf(total.y), fabsf(total.z)));
-        sq[5] = double(total.x) * total.x + double(total.y) * total.y + double(total.z) * total.z;
+        part.scale[5] = fmaxf(part.scale[5], fmaxf(fabsf(totalG.x), fmaxf(fabsf(totalG.y), fabsf(totalG.z))));
+        part.sq[5] += double(totalG.x) * totalG.x + double(totalG.y) * totalG.y + double(totalG.z) * totalG.z;
       } else {
-        valid = false;
+        part.valid = 0u;
       }
-    }
-    if (nextRotations) storeRot(b.vertexRot, v, vertexFrame(b, acc, v, p.rotationEpsilon));
-  }
-#pragma unroll
-  for (int c = 0; c < 6; ++c) {
-    const uint32_t m = __reduce_max_sync(0xffffffffu, __float_as_uint(scale[c]));
-    if ((threadIdx.x & 31u) == 0u && m) atomicMax(&fs->convScale[c], m);
-  }
-  {
-    const uint32_t m = __reduce_max_sync(0xffffffffu, __float_as_uint(maxUpdate));
-    const bool allValid = __all_sync(0xffffffffu, valid);
-    if ((threadIdx.x & 31u) == 0u) {
-      if (m) atomicMax(&fs->convMaxUpdate, m);
-      if (!allValid) atomicAnd(&fs->convValid, 0u);
+      // The next iteration's frame from the same deformation gradients
+      // (vertexPolarRotation on the accepted pose).
+      if (nextRotations) {
+        const M3 favg = total > 0.0f ? (1.0f / total) * avg : midentity();
+        storeRot(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, p.rotationEpsilon));
+      }
+    } else if (nextRotations) {
+      storeRot(b.vertexRot, v, vertexFrame(b, acc, v, p.rotationEpsilon));
     }
   }
-  blockSumDoubles<6>(sq, scratch);
-  if (threadIdx.x == 0) {
-#pragma unroll
-    for (int c = 0; c < 6; ++c) b.convPartials[6ull * blockIdx.x + c] = sq[c];
-    __threadfence();
-    isLast = atomicAdd(&fs->convTicket, 1u) == gridDim.x - 1;
-  }
-  __syncthreads();
-  if (!isLast || threadIdx.x != 0) return;
-  __threadfence();
-  double tot[6] = {0, 0, 0, 0, 0, 0};
-  for (uint32_t k = 0; k < gridDim.x; ++k)
-    for (int c = 0; c < 6; ++c) tot[c] += b.convPartials[6ull * k + c];
+  const ConvPartial blk = blockFold(part, smem, convCombine);
+  ConvPartial* partials = reinterpret_cast<ConvPartial*>(b.convPartials);
+  if (!publishPartial(blk, partials, &fs->convTicket, &isLast)) return;
+  const ConvPartial tot = foldPartials(partials, smem, convIdentity, convCombine);
+  if (threadIdx.x != 0) return;
   float norms[5];
-  bool cnv = atomicAdd(&fs->convValid, 0u) != 0u;
+  bool cnv = tot.valid != 0u;
   for (int c = 0; c < 5; ++c) {
-    norms[c] = float(sqrt(tot[c]));
+    norms[c] = float(sqrt(tot.sq[c]));
     cnv = cnv && finiteS(norms[c]) && norms[c] >= 0.0f;
   }
-  const float gnorm = float(sqrt(tot[5]));
+  const float gnorm = float(sqrt(tot.sq[5]));
   const float den = fmaxf(1.0f, norms[0] + norms[1] + norms[2] + norms[3] + norms[4]);
   const float rel = gnorm / den;
   const bool rnv = cnv && finiteS(gnorm) && finiteS(den) && den >= 1.0f && finiteS(rel) && rel >= 0.0f;
-  const float mu = __uint_as_float(atomicAdd(&fs->convMaxUpdate, 0u));
+  const float mu = tot.maxUpdate;
   const bool ssv = finiteS(p.sceneScale) && p.sceneScale >= 0.0f;
   const float nmu = mu / fmaxf(ssv ? p.sceneScale : 1.0e-12f, 1.0e-12f);
-  const bool unv = (atomicAdd(&fs->convValid, 0u) != 0u) && ssv && finiteS(mu) && mu >= 0.0f && finiteS(nmu);
+  const bool unv = tot.valid != 0u && ssv && finiteS(mu) && mu >= 0.0f && finiteS(nmu);
   const float4 geometry = fs->control[0];
   const uint32_t cb = controlBits(geometry.w) & kValidityMask;
   const bool sgv = (cb & kSourceGeometryValid) != 0u && finiteS(geometry.x);
@@ -951,9 +988,6 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
   }
   fs->control[1].w = float(hi + 1);
   if (conv && p.stopEnabled) fs->control[0].w = float(cb | kStopLatchBit);
-  for (int c = 0; c < 6; ++c) fs->convScale[c] = 0u;
-  fs->convMaxUpdate = 0u;
-  fs->convValid = 1u;
   fs->convTicket = 0u;
 }
 
@@ -1016,21 +1050,29 @@ __global__ void __launch_bounds__(kBlock) finalizeKernel(Buffers b, const DevPar
   b.velocity[v] = make_float4(vel.x, vel.y, vel.z, 0.0f);
 }
 
+}  // namespace
+
 inline uint32_t blocksFor(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 
-}  // namespace
+uint32_t smCount() {
+  static int sms = 0;
+  if (sms == 0) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || sms <= 0) sms = 148;
+  }
+  return static_cast<uint32_t>(sms);
+}
 
 uint32_t gateBlockCount(uint32_t V, uint32_t T) {
   const uint32_t n = T > V ? T : V;
-  const uint32_t blocks = blocksFor(n);
-  return blocks < 1u ? 1u : blocks;
+  return std::max(1u, std::min(blocksFor(n), smCount() * 8u));
 }
 
-uint32_t convBlockCount(uint32_t V) { return blocksFor(V) < 1u ? 1u : blocksFor(V); }
+uint32_t convBlockCount(uint32_t V) { return std::max(1u, std::min(blocksFor(V), smCount() * 8u)); }
 
 int launchPrologue(const Buffers& b, const DevParams* p, uint32_t V, uint32_t T, bool glob, cudaStream_t s) {
-  const uint32_t n = T > V ? T : V;
-  prologueKernel<<<blocksFor(n), kBlock, 0, s>>>(b, p, V, T, glob ? 1 : 0);
+  prologueKernel<<<b.gateBlocks, kBlock, 0, s>>>(b, p, V, T, glob ? 1 : 0);
   return 1;
 }
 
@@ -1054,7 +1096,9 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   const uint32_t groups = solveGroupsPerBlock(K);
   if (groups == 0) return 0;
   const size_t smem = static_cast<size_t>(groups) * K * sizeof(CubState);
-  const uint32_t blocks = (count + groups - 1) / groups;
+  // One vertex per lane group: the line search makes per-vertex work uneven,
+  // and the block scheduler balances it better than a fixed grid stride.
+  const uint32_t blocks = std::max(1u, (count + groups - 1) / groups);
   solveKernel<kGroup><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K);
   return 1;
 }

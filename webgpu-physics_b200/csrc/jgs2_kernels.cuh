@@ -61,8 +61,8 @@ struct Buffers {
   float* finalUpdate;     // per vertex update norm
   float4* local;          // 4 per vertex (local diagnostics)
   FrameState* frame;
-  double* gatePartials;   // 2 per gate block (source / candidate energy)
-  double* convPartials;   // 6 per convergence block
+  void* gatePartials;     // one GatePartial (32 bytes) per gate / prologue block
+  void* convPartials;     // one ConvPartial (80 bytes) per convergence block
   double* bodyAccum;      // 6 per body (mass, solved xz, predicted xz, pinned count)
   // static
   const float4* restMass;     // rest xyz (pin target), mass
@@ -96,7 +96,10 @@ int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos,
 
 // Vertices per solve block for cubature width K (0: K too large to cache).
 uint32_t solveGroupsPerBlock(uint32_t K);
+// Persistent grid sizes (a few blocks per SM) of the reduction kernels.
 uint32_t gateBlockCount(uint32_t V, uint32_t T);
 uint32_t convBlockCount(uint32_t V);
+constexpr size_t kGatePartialBytes = 32;
+constexpr size_t kConvPartialBytes = 80;
 
 }  // namespace jgs2

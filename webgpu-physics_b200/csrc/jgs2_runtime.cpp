@@ -975,8 +975,14 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
   }
   b.gateBlocks = jgs2::gateBlockCount(V, T);
   b.convBlocks = jgs2::convBlockCount(V);
-  STEP(deviceAlloc(sp, &b.gatePartials, 2ull * b.gateBlocks));
-  STEP(deviceAlloc(sp, &b.convPartials, 6ull * b.convBlocks));
+  {
+    double* gp = nullptr;
+    double* cp = nullptr;
+    STEP(deviceAlloc(sp, &gp, jgs2::kGatePartialBytes / sizeof(double) * b.gateBlocks));
+    STEP(deviceAlloc(sp, &cp, jgs2::kConvPartialBytes / sizeof(double) * b.convBlocks));
+    b.gatePartials = gp;
+    b.convPartials = cp;
+  }
   STEP(deviceAlloc(sp, &b.bodyAccum, 6ull * sp->bodies));
   {
     float4* p = nullptr;
@@ -1328,6 +1334,62 @@ jgs2_status jgs2_read_globalization(jgs2_solver* s, float* local, size_t localFl
     if (st != JGS2_OK) return st;
   }
   return JGS2_OK;
+}
+
+jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* s, const float* source, const float* candidate,
+                                              const jgs2_settings* o, uint32_t mask, float* positionsOut,
+                                              float* controlOut, float* historyOut) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!s->glob) return fail(s, JGS2_UNSUPPORTED, "Assembled candidate tests require stable globalization.");
+  if (!source || !candidate) return fail(s, JGS2_INVALID_ARGUMENT, "Assembled candidate poses must not be NULL.");
+  const size_t n = 4ull * s->V;
+  for (size_t i = 0; i < n; ++i) {
+    if (!std::isfinite(source[i])) return fail(s, JGS2_INVALID_ARGUMENT, "source candidate pose must be finite.");
+    if (!std::isfinite(candidate[i]))
+      return fail(s, JGS2_INVALID_ARGUMENT, "candidate candidate pose must be finite.");
+  }
+  jgs2_settings settings;
+  std::string err;
+  if (!resolve(s->defaults, o, mask, &settings, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
+  const DevParams p = makeParams(s, settings, false);
+  const Buffers& b = s->b;
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaMemcpyAsync(s->dParams, &p, sizeof(p), cudaMemcpyHostToDevice, s->stream));
+  // posB = source, posA = candidate, predicted = source; local records and
+  // the control record cleared (jgs2-solver.ts:2644-2679).
+  CUDA_TRY(s, cudaMemcpyAsync(b.pos[1], source, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaMemcpyAsync(b.pos[0], candidate, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaMemcpyAsync(b.predicted, source, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaMemsetAsync(b.local, 0, sizeof(float4) * 4ull * s->V, s->stream));
+  CUDA_TRY(s, cudaMemsetAsync(b.frame->control, 0, sizeof(float4) * 4, s->stream));
+  // The sweep aggregates the gate reads, as a cleared record per vertex
+  // gives them: status 0 (accepted) with no backtracks and no evaluations,
+  // i.e. one skipped trial per vertex and valid numerics.
+  const uint32_t aggregates[6] = {0u, 0u, s->V, 0u, 0u, 1u};
+  static_assert(offsetof(FrameState, localNumericsValid) - offsetof(FrameState, localFailures) == 20,
+                "sweep aggregates are six consecutive words");
+  CUDA_TRY(s, cudaMemcpyAsync(&b.frame->localFailures, aggregates, sizeof(aggregates), cudaMemcpyHostToDevice,
+                              s->stream));
+  s->launches += jgs2::launchGate(b, s->dParams, b.pos[1], b.pos[0], s->V, s->T, s->stream);
+  s->launches += jgs2::launchConvergence(b, s->dParams, b.pos[1], b.pos[0], s->V, false, s->stream);
+  CUDA_TRY(s, cudaGetLastError());
+  s->recordsAvailable = true;
+  s->submitted = settings;
+  s->submittedIterations = 1;
+  if (positionsOut) {
+    st = readRegion(s, b.pos[0], sizeof(float) * n, positionsOut);
+    if (st != JGS2_OK) return st;
+  }
+  if (controlOut) {
+    st = readRegion(s, b.frame->control, sizeof(float4) * 4, controlOut);
+    if (st != JGS2_OK) return st;
+  }
+  if (historyOut) {
+    st = readRegion(s, b.frame->history, sizeof(float4) * 8, historyOut);
+    if (st != JGS2_OK) return st;
+  }
+  return jgs2_sync(s);
 }
 
 jgs2_status jgs2_device_positions(jgs2_solver* s, void** ptr, void** stream) {

@@ -9,7 +9,7 @@ from ctypes import (POINTER, Structure, c_char_p, c_double, c_float, c_int,
                     c_void_p)
 
 PACKAGE_ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
-LIB_DIR = os.path.join(PACKAGE_ROOT, "lib")
+LIB_DIR = os.environ.get("JGS2_LIB_DIR") or os.path.join(PACKAGE_ROOT, "lib")
 
 STATUS_NAMES = {
     0: "OK", 1: "INVALID_ARGUMENT", 2: "INFEASIBLE_INPUT", 3: "OUT_OF_MEMORY",
@@ -207,6 +207,8 @@ def step_lib() -> ctypes.CDLL:
                                                 POINTER(c_float), POINTER(c_float),
                                                 c_size_t, POINTER(c_uint32)]
         lib.jgs2_device_positions.argtypes = [vp, POINTER(c_void_p), POINTER(c_void_p)]
+        lib.jgs2_evaluate_assembled_candidate.argtypes = [vp, POINTER(c_float), POINTER(c_float), S, c_uint32,
+                                                          POINTER(c_float), POINTER(c_float), POINTER(c_float)]
         lib.jgs2_kernel_launch_count.argtypes = [vp]
         lib.jgs2_kernel_launch_count.restype = c_uint64
         _step_lib = lib

@@ -276,6 +276,17 @@ def cantilever(cells=(20, 4, 4), size=(1.0, 0.2, 0.2), young=1e5, poisson=0.4,
     return inp
 
 
+def single_tetrahedron(timestep=1 / 60, cubature_k=4) -> SceneInput:
+    """The single stable Neo-Hookean tetrahedron of the material parity
+    fixture (src/scenes/phase1.ts:44-64, 246-271): rest A=(0,0,0),
+    B=(1,0,0), C=(0,1,0), D=(0,0,1), A pinned, density 1000, E=8e4, nu=0.3."""
+    sc = Scene()
+    m = sc.add_material(1000.0, 80000.0, 0.3, MATERIAL_STABLE_NEO_HOOKEAN)
+    sc.add_mesh([0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1], [0, 1, 2, 3], m, pinned=[1, 0, 0, 0])
+    sc.precompute(timestep=timestep, cubature_k=cubature_k)
+    return sc.pack()
+
+
 def cantilever_target(inp: SceneInput, frame: int, lift=0.15, stiffness=1000.0):
     """Soft target on the free-end (x = max) vertices for frames 60-180: the
     rest position raised by `lift` along a smoothstep over frames 60-120, held

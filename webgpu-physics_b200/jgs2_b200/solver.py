@@ -328,6 +328,25 @@ class JGS2GpuSolver:
     def readVertexRotations(self) -> np.ndarray:
         return self._read(self._L.jgs2_read_vertex_rotations, 12)
 
+    def evaluateAssembledCandidateForTest(self, sourcePositions, candidatePositions,
+                                          overrides: Optional[dict] = None) -> dict:
+        """Run the assembled gate and convergence reduction once on a source /
+        candidate pose pair; {'positions', 'control', 'history'}."""
+        self._usable()
+        src = np.ascontiguousarray(sourcePositions, dtype=np.float32).reshape(-1)
+        cand = np.ascontiguousarray(candidatePositions, dtype=np.float32).reshape(-1)
+        n = 4 * self.vertexCount
+        if src.size != n or cand.size != n:
+            raise JGS2RangeError(1, f"Assembled candidate poses must each contain {n} floats.")
+        o, m = settings_struct(overrides)
+        pos = np.empty(n, dtype=np.float32)
+        control = np.empty(16, dtype=np.float32)
+        history = np.empty(32, dtype=np.float32)
+        self._check(self._L.jgs2_evaluate_assembled_candidate(
+            self._h, _ffi.fptr(src), _ffi.fptr(cand), byref(o), m, _ffi.fptr(pos), _ffi.fptr(control),
+            _ffi.fptr(history)))
+        return {"positions": pos, "control": control, "history": history}
+
     def readGlobalizationDiagnostics(self) -> dict:
         """{'local': (V,16), 'control': (16,), 'history': (count,32), 'historyCount': n}."""
         self._usable()
