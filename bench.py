@@ -209,6 +209,23 @@ def init_dist(world, backend):
     return dist
 
 
+def max_over_ranks(dist, value: float, device=None) -> float:
+    """The maximum of a per-rank scalar over all ranks; every rank calls it at
+    the same point (identity without a process group)."""
+    if dist is None:
+        return value
+    import torch
+
+    t = torch.tensor([value], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def whole_job_rate(world: int, units_per_rank: float, seconds: float) -> float:
+    """Units all replicas processed per second of the slowest rank."""
+    return world * units_per_rank / seconds
+
+
 def reference_arm(args):
     world, rank, _local = dist_env()
     if rank != 0:
@@ -298,12 +315,9 @@ def ours_arm(args):
     ms = start_ev.elapsed_time(end_ev)
     launches = s.kernelLaunchCount() - launches0
     torch.cuda.synchronize(device)
-    if dist is not None:
-        t = torch.tensor([ms], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        ms = float(t.item())
+    ms = max_over_ranks(dist, ms, f"cuda:{device}")
     ms_per_step = ms / args.steps
-    value = world * active * iters * args.steps / (ms / 1e3)
+    value = whole_job_rate(world, active * iters * args.steps, ms / 1e3)
 
     # ---- per-kernel event timing (same workload, same stream) -----------------
     prof = s.stepWithGpuTimestamps(max(1, min(args.steps, 3)), iters)
@@ -338,12 +352,8 @@ def ours_arm(args):
         s.stepExactIterations(iters)
         s.readPositions(out=p_np)
         lat.append(time.perf_counter() - t0)
-    e2e_total = time.perf_counter() - t_e2e
-    if dist is not None:
-        t = torch.tensor([e2e_total], device=f"cuda:{device}")
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_total = float(t.item())
-    e2e_value = world * active * iters * e2e_steps / e2e_total
+    e2e_total = max_over_ranks(dist, time.perf_counter() - t_e2e, f"cuda:{device}")
+    e2e_value = whole_job_rate(world, active * iters * e2e_steps, e2e_total)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
