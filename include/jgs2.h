@@ -324,6 +324,32 @@ jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* solver, const float* 
                                               const jgs2_settings* overrides, uint32_t override_mask,
                                               float* positions_out, float* control_out, float* history_out);
 
+/* Allocation-free assembled gate.  This entry point has no counterpart in
+ * the reference.  It evaluates the same determinant gate and assembled
+ * energies as jgs2_evaluate_assembled_candidate, with the sweep records
+ * taken as cleared, over caller DEVICE arrays: source, candidate and
+ * predicted positions (4 * V floats each, 16-byte aligned), and writes the
+ * 16-float control record (minimum determinants and validity bits, accept /
+ * revert flags, energies, sweep aggregates; history slot 0) to the device
+ * array control_out.  It reads the solver's static mesh data and changes no
+ * solver state.
+ *
+ * It allocates no device memory: its reduction scratch is a fixed static
+ * device array of 262,400 bytes (8192 block partials of 32 bytes after a
+ * 256-byte header).  So max(vertex_count, tet_count) may be at most
+ * 1,048,576 (8192 blocks of 128); larger solvers get JGS2_INVALID_ARGUMENT.
+ * The first call on each device looks up the scratch address there (this may
+ * load the kernel module onto the device), so make one call before any stream
+ * capture begins.  The scratch's ticket word must start at zero: module load
+ * zeroes it and every launch leaves it zero.  Calls whose launches overlap in
+ * time on one device (different streams, threads or solvers) share the
+ * scratch and race; order them.  stream is a cudaStream_t, or NULL for the
+ * solver's stream; the call is asynchronous on it. */
+jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* solver, const float* device_source,
+                                         const float* device_candidate, const float* device_predicted,
+                                         const jgs2_settings* overrides, uint32_t override_mask,
+                                         float* device_control_out, void* stream);
+
 /* Zero-copy consumers (the reference's currentPositionBuffer, :1504-1507):
  * device address of the canonical vec4 position array and the solver's
  * cudaStream_t.  Valid until jgs2_destroy. */

@@ -1050,6 +1050,67 @@ __global__ void __launch_bounds__(kBlock) finalizeKernel(Buffers b, const DevPar
   b.velocity[v] = make_float4(vel.x, vel.y, vel.z, 0.0f);
 }
 
+// ---------------------------------------------------------------------------
+// Allocation-free variant of the gate.  Its reduction scratch is a static
+// device array instead of solver buffers: a 256-byte header whose first word
+// is the block ticket, then one GatePartial per block.  The ticket must be
+// zero when a launch starts; module load zero-fills the array and the last
+// block of every launch writes the ticket back to zero.  Two launches that
+// overlap in time share the array and corrupt each other's result.
+static_assert(sizeof(GatePartial) == kGatePartialBytes, "partial size");
+static __device__ __align__(256) unsigned char gGateScratch[kGateScratchBytes];
+
+// One element per thread (tet i and vertex i), so the grid, and with it the
+// number of partials, grows with max(V, T); the launcher rejects sizes whose
+// partials do not fit.  The sweep records are taken as cleared: no local
+// failures, valid numerics, history slot 0, one skipped trial per vertex.
+__global__ void __launch_bounds__(kBlock) gateScratchKernel(Buffers b, DevParams p, const float4* __restrict__ src,
+                                                            const float4* __restrict__ tgt, uint32_t V, uint32_t T,
+                                                            float4* __restrict__ control,
+                                                            unsigned char* __restrict__ scratch) {
+  __shared__ GatePartial smem[kBlock];
+  __shared__ bool isLast;
+  uint32_t* ticket = reinterpret_cast<uint32_t*>(scratch);
+  GatePartial* partials = reinterpret_cast<GatePartial*>(scratch + kGateScratchHeaderBytes);
+  GatePartial acc = gateIdentity();
+  const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i < T) {
+    const TetRec r = loadTet(b.tets, i);
+    accumulateTet(acc, r, deformationAt(r, src), deformationAt(r, tgt));
+  }
+  if (i < V) {
+    const uint4 info = b.vinfo[i];
+    const float es = implicitEnergy(p, b, i, xyz(src[i]), info);
+    const float ec = implicitEnergy(p, b, i, xyz(tgt[i]), info);
+    if (finiteS(es)) acc.e0 += es; else acc.bits &= ~kSourceEnergyValid;
+    if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
+  }
+  const GatePartial blk = blockFold(acc, smem, gateCombine);
+  if (!publishPartial(blk, partials, ticket, &isLast)) return;
+  const GatePartial tot = foldPartials(partials, smem, gateIdentity, gateCombine);
+  if (threadIdx.x != 0) return;
+  uint32_t vb = tot.bits | kLocalNumericsValid;
+  const float eS = float(tot.e0), eC = float(tot.e1);
+  if (!finiteS(eS)) vb &= ~kSourceEnergyValid;
+  if (!finiteS(eC)) vb &= ~kCandidateEnergyValid;
+  if (T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
+  const float sm = tot.minS, cm = tot.minC;
+  const bool sgv = (vb & kSourceGeometryValid) != 0u, cgv = (vb & kCandidateGeometryValid) != 0u;
+  const bool sev = (vb & kSourceEnergyValid) != 0u, cev = (vb & kCandidateEnergyValid) != 0u;
+  const bool accepted = (sgv && sm > kDeterminantFloor) && (cgv && cm > kDeterminantFloor);
+  const float am = accepted ? cm : sm;
+  const bool amv = accepted ? cgv : sgv;
+  const float ae = accepted ? eC : eS;
+  const bool aev = accepted ? cev : sev;
+  if (amv) vb |= kAcceptedMinimumValid;
+  const uint32_t cb = vb & kValidityMask;
+  control[0] = make_float4(sgv ? sm : 0.f, cgv ? cm : 0.f, amv ? am : 0.f, float(cb));
+  control[1] = make_float4(accepted ? 1.f : 0.f, accepted ? 0.f : 1.f, 0.f, 0.f);
+  control[2] = make_float4(sev ? eS : 0.f, cev ? eC : 0.f, aev ? ae : 0.f, (sev && cev) ? 1.f : 0.f);
+  control[3] = make_float4(0.f, 0.f, float(V), 0.f);
+  *ticket = 0u;
+}
+
 }  // namespace
 
 inline uint32_t blocksFor(uint32_t n) { return (n + kBlock - 1) / kBlock; }
@@ -1148,6 +1209,21 @@ int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos,
   }
   finalizeKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, finalPos, V, glob ? 1 : 0, bodyCorrection ? 1 : 0);
   return n + 1;
+}
+
+cudaError_t gateScratchAddress(void** out) { return cudaGetSymbolAddress(out, gGateScratch); }
+
+uint32_t gateScratchMaxElements() { return kGateScratchMaxBlocks * static_cast<uint32_t>(kBlock); }
+
+int launchGateScratch(const Buffers& b, const DevParams& p, const float4* predicted, const float4* src,
+                      const float4* tgt, uint32_t V, uint32_t T, float4* control, void* scratch, cudaStream_t s) {
+  const uint32_t n = T > V ? T : V;
+  if (n == 0 || n > gateScratchMaxElements()) return 0;
+  Buffers view = b;
+  view.predicted = const_cast<float4*>(predicted);
+  gateScratchKernel<<<blocksFor(n), kBlock, 0, s>>>(view, p, src, tgt, V, T, control,
+                                                   static_cast<unsigned char*>(scratch));
+  return 1;
 }
 
 }  // namespace jgs2

@@ -102,4 +102,18 @@ uint32_t convBlockCount(uint32_t V);
 constexpr size_t kGatePartialBytes = 32;
 constexpr size_t kConvPartialBytes = 80;
 
+// Allocation-free gate: static device scratch of a 256-byte header (the block
+// ticket) and one partial per block, for at most kGateScratchMaxBlocks blocks
+// of one element per thread (gateScratchMaxElements() = max(V, T) limit).
+constexpr uint32_t kGateScratchMaxBlocks = 8192;
+constexpr size_t kGateScratchHeaderBytes = 256;
+constexpr size_t kGateScratchBytes = kGateScratchHeaderBytes + kGateScratchMaxBlocks * kGatePartialBytes;
+cudaError_t gateScratchAddress(void** out);
+uint32_t gateScratchMaxElements();
+// Launches the gate over caller device arrays with `scratch` (the address of
+// the static array on the current device); writes 4 float4 to `control`.
+// Returns 0 without launching when max(V, T) is 0 or over the limit.
+int launchGateScratch(const Buffers& b, const DevParams& p, const float4* predicted, const float4* src,
+                      const float4* tgt, uint32_t V, uint32_t T, float4* control, void* scratch, cudaStream_t s);
+
 }  // namespace jgs2

@@ -1392,6 +1392,63 @@ jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* s, const float* sourc
   return jgs2_sync(s);
 }
 
+// For callers that may not allocate device memory while they run: hosts that
+// give the library a fixed device-memory budget up front, and per-frame loops
+// where a device allocation would synchronise the device and stall the frame.
+// The gate's scratch is a static device array whose address is looked up once
+// per device; nothing here calls cudaMalloc or cudaFree.
+jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* s, const float* source, const float* candidate,
+                                         const float* predicted, const jgs2_settings* o, uint32_t mask,
+                                         float* control, void* stream) {
+  constexpr int kMaxScratchDevices = 64;
+  static std::mutex scratchMutex;
+  static void* scratchAddress[kMaxScratchDevices] = {};
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!s->glob) return fail(s, JGS2_UNSUPPORTED, "The assembled gate requires stable globalization.");
+  if (!source || !candidate || !predicted || !control)
+    return fail(s, JGS2_INVALID_ARGUMENT, "The no-allocation gate's device arrays must not be NULL.");
+  for (const void* p : {static_cast<const void*>(source), static_cast<const void*>(candidate),
+                        static_cast<const void*>(predicted), static_cast<const void*>(control)})
+    if (reinterpret_cast<uintptr_t>(p) % 16 != 0)
+      return fail(s, JGS2_INVALID_ARGUMENT, "The no-allocation gate's device arrays must be 16-byte aligned.");
+  const uint32_t limit = jgs2::gateScratchMaxElements();
+  if (std::max(s->V, s->T) > limit)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("The no-allocation gate handles at most %u vertices and %u tetrahedra (its static scratch "
+                       "holds %u block partials); this solver has %u vertices and %u tetrahedra.",
+                       limit, limit, jgs2::kGateScratchMaxBlocks, s->V, s->T));
+  if (s->device < 0 || s->device >= kMaxScratchDevices)
+    return fail(s, JGS2_UNSUPPORTED, format("The no-allocation gate supports device ordinals below %d.",
+                                            kMaxScratchDevices));
+  jgs2_settings settings;
+  std::string err;
+  if (!resolve(s->defaults, o, mask, &settings, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
+  const DevParams p = makeParams(s, settings, false);
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  void* scratch = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(scratchMutex);
+    if (!scratchAddress[s->device]) {
+      void* address = nullptr;
+      const cudaError_t e = jgs2::gateScratchAddress(&address);
+      if (e != cudaSuccess || !address)
+        return cudaFail(s, e != cudaSuccess ? e : cudaErrorInvalidSymbol, "cudaGetSymbolAddress(gate scratch)");
+      scratchAddress[s->device] = address;
+    }
+    scratch = scratchAddress[s->device];
+  }
+  cudaStream_t launchStream = stream ? static_cast<cudaStream_t>(stream) : s->stream;
+  const int launched = jgs2::launchGateScratch(
+      s->b, p, reinterpret_cast<const float4*>(predicted), reinterpret_cast<const float4*>(source),
+      reinterpret_cast<const float4*>(candidate), s->V, s->T, reinterpret_cast<float4*>(control), scratch,
+      launchStream);
+  if (launched == 0) return fail(s, JGS2_INVALID_ARGUMENT, "The no-allocation gate was given an empty mesh.");
+  CUDA_TRY(s, cudaGetLastError());
+  s->launches += static_cast<uint64_t>(launched);
+  return JGS2_OK;
+}
+
 jgs2_status jgs2_device_positions(jgs2_solver* s, void** ptr, void** stream) {
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
