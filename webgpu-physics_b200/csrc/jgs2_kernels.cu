@@ -31,7 +31,7 @@ namespace jgs2 {
 namespace {
 
 constexpr int kBlock = 128;
-constexpr int kGroup = 8;  // lanes per vertex in the solve kernel
+constexpr int kGroup = 4;  // lanes per vertex in the solve kernel
 constexpr int kRecFloats = 56;  // cached cubature record state
 
 struct TetRec {
@@ -202,6 +202,52 @@ __device__ __forceinline__ void blockSumDoubles(double (&vals)[N], double* scrat
   for (int i = 0; i < N; ++i) vals[i] = scratch[i * kBlock];
 }
 
+// Exact incident block of the local Hessian for shape gradient g
+// (jgs2-shader.ts:3097-3111): vol (a |g|^2 I + c1 u u^T + lambda w w^T) with
+// u = F g and w = cof(F) g, the stable Neo-Hookean tangent applied to the
+// rank-one direction e_i g^T.
+__device__ __forceinline__ void addIncidentBlock(S3& hess, const TetRec& r, const M3& F, const PiolaTerms& pt,
+                                                 float3 g) {
+  const float3 u1 = mv(F, g), w1 = mv(pt.cof, g);
+  S3 blk = szero();
+  saddDiag(blk, pt.a * dot3(g, g));
+  saddOuter(blk, pt.c1, u1);
+  saddOuter(blk, r.lambda, w1);
+  saddScaled(hess, r.vol, blk);
+}
+
+__device__ __forceinline__ void storeIncident(float4* __restrict__ inc, uint32_t v, float3 g, const S3& h) {
+  inc[3ull * v] = make_float4(g.x, g.y, g.z, h.xx);
+  inc[3ull * v + 1] = make_float4(h.yy, h.zz, h.xy, h.xz);
+  inc[3ull * v + 2] = make_float4(h.yz, 0.0f, 0.0f, 0.0f);
+}
+
+// Vertex frame and incident system of a free vertex at pose x in one pass
+// over its incident tets: the frame is the polar of the volume-weighted
+// average F (vertexPolarRotation, jgs2-shader.ts:2959-2989), the system the
+// incident material gradient sum vol P(F) g and Hessian blocks.
+__device__ __forceinline__ void frameAndIncident(const Buffers& b, const float4* __restrict__ x, uint32_t v,
+                                                 const uint4& info, float eps) {
+  M3 avg = mzero();
+  float total = 0.0f;
+  float3 grad = f3(0, 0, 0);
+  S3 hess = szero();
+  for (uint32_t a = 0; a < info.y; ++a) {
+    const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
+    const TetRec r = loadTet(b.tets, entry >> 2);
+    const M3 F = deformationAt(r, x);
+    const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
+    const float3 g = shapeGradient(r, entry & 3u);
+    grad = grad + r.vol * mv(piola(F, pt), g);
+    addIncidentBlock(hess, r, F, pt, g);
+    avg = avg + r.vol * F;
+    total += r.vol;
+  }
+  const M3 favg = total > 0.0f ? (1.0f / total) * avg : midentity();
+  storeRot(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, eps));
+  storeIncident(b.incident, v, grad, hess);
+}
+
 // Vertex frame: polar of the volume-weighted average F over incident tets
 // (vertexPolarRotation, jgs2-shader.ts:2959-2989).
 __device__ __forceinline__ M3 vertexFrame(const Buffers& b, const float4* __restrict__ x, uint32_t v, float eps) {
@@ -276,7 +322,7 @@ template <int W>
 __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
                                                       const float4* __restrict__ src, float4* tgt,
                                                       const uint32_t* __restrict__ list, uint32_t count,
-                                                      uint32_t K) {
+                                                      uint32_t K, int cachedIncident) {
   extern __shared__ float4 cache4[];
   CubState* cache = reinterpret_cast<CubState*>(cache4);
   __shared__ uint32_t sFail, sMaxBack, sSkip, sEvals, sMaxShift, sValid;
@@ -341,8 +387,10 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
         const M3 RsT = mtrans(loadRot(b.vertexRot, v));
         const uint32_t nItems = K + info.y;
         CubState* myCache = cache + static_cast<size_t>(group) * K;
-        for (uint32_t u = lane; u < nItems; u += W) {
-          if (u < K) {
+        // Cubature records first, then (unless cached) the incident tets, in
+        // separate loops so the two kinds of item never share a divergent pass.
+        for (uint32_t u = lane; u < K; u += W) {
+          {
             // ---- cubature record (jgs2-shader.ts:3197-3263) ----
             CubState st;
             const size_t rec = static_cast<size_t>(v) * K + u;
@@ -441,21 +489,18 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
               st.gs = gs;
             }
             myCache[u] = st;
-          } else {
+          }
+        }
+        if (!cachedIncident) {
+          for (uint32_t a = lane; a < info.y; a += W) {
             // ---- incident tetrahedron (jgs2-shader.ts:3097-3111) ----
-            const uint32_t entry = __ldg(&b.adjacency[info.x + (u - K)]);
+            const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
             const TetRec r = loadTet(b.tets, entry >> 2);
-            const uint32_t slot = entry & 3u;
             const M3 F = deformationAt(r, src);
             const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
-            const float3 g = shapeGradient(r, slot);
+            const float3 g = shapeGradient(r, entry & 3u);
             grad = grad + r.vol * mv(piola(F, pt), g);
-            const float3 u1 = mv(F, g), w1 = mv(pt.cof, g);
-            S3 blk = szero();
-            saddDiag(blk, pt.a * dot3(g, g));
-            saddOuter(blk, pt.c1, u1);
-            saddOuter(blk, r.lambda, w1);
-            saddScaled(hess, r.vol, blk);
+            addIncidentBlock(hess, r, F, pt, g);
           }
         }
         // Group reduction of the gather.
@@ -468,6 +513,16 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
         hess.xy = groupSum<W>(hess.xy, mask);
         hess.xz = groupSum<W>(hess.xz, mask);
         hess.yz = groupSum<W>(hess.yz, mask);
+        if (cachedIncident) {
+          const float4 i0 = b.incident[3ull * v], i1 = b.incident[3ull * v + 1], i2 = b.incident[3ull * v + 2];
+          grad = grad + f3(i0.x, i0.y, i0.z);
+          hess.xx += i0.w;
+          hess.yy += i1.x;
+          hess.zz += i1.y;
+          hess.xy += i1.z;
+          hess.xz += i1.w;
+          hess.yz += i2.x;
+        }
         // Own terms: inertia, objectives, floor (jgs2-shader.ts:3083-3092, 3188-3191).
         grad = grad + inertia * (position - predV);
         saddDiag(hess, inertia);
@@ -749,8 +804,10 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
       b.pos[1][i] = make_float4(src.x, src.y, src.z, 1.0f);
       b.finalUpdate[i] = 0.0f;
       if (glob) {
-        // Iteration-0 frames from the accepted pose (the stable iteration source).
-        storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
+        // Iteration-0 frames (and, for free vertices, the incident system)
+        // from the accepted pose, the stable iteration source.
+        if (isPinned(info)) storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
+        else frameAndIncident(b, b.pos[0], i, info, p.rotationEpsilon);
         const float e = implicitEnergy(p, b, i, xyz(o), info);
         if (finiteS(e)) { acc.e0 += e; acc.e1 += e; }
         else acc.bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
@@ -886,12 +943,15 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
       float3 material = f3(0, 0, 0);
       M3 avg = mzero();
       float total = 0.0f;
+      S3 hess = szero();
       for (uint32_t a = 0; a < info.y; ++a) {
         const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
         const TetRec r = loadTet(b.tets, entry >> 2);
         const M3 F = deformationAt(r, acc);
         const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
-        material = material + r.vol * mv(piola(F, pt), shapeGradient(r, entry & 3u));
+        const float3 g = shapeGradient(r, entry & 3u);
+        material = material + r.vol * mv(piola(F, pt), g);
+        if (nextRotations) addIncidentBlock(hess, r, F, pt, g);
         avg = avg + r.vol * F;
         total += r.vol;
       }
@@ -925,11 +985,12 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
       } else {
         part.valid = 0u;
       }
-      // The next iteration's frame from the same deformation gradients
-      // (vertexPolarRotation on the accepted pose).
+      // The next iteration's frame and incident system from the same
+      // deformation gradients (the accepted pose is the next source).
       if (nextRotations) {
         const M3 favg = total > 0.0f ? (1.0f / total) * avg : midentity();
         storeRot(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, p.rotationEpsilon));
+        storeIncident(b.incident, v, material, hess);
       }
     } else if (nextRotations) {
       storeRot(b.vertexRot, v, vertexFrame(b, acc, v, p.rotationEpsilon));
@@ -1151,7 +1212,7 @@ int launchTetPolar(const Buffers& b, const DevParams* p, const float4* src, uint
 }
 
 int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
-                uint32_t count, uint32_t K, bool glob, cudaStream_t s) {
+                uint32_t count, uint32_t K, bool glob, bool cachedIncident, cudaStream_t s) {
   (void)glob;
   if (count == 0) return 0;
   const uint32_t groups = solveGroupsPerBlock(K);
@@ -1160,7 +1221,8 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   // One vertex per lane group: the line search makes per-vertex work uneven,
   // and the block scheduler balances it better than a fixed grid stride.
   const uint32_t blocks = std::max(1u, (count + groups - 1) / groups);
-  solveKernel<kGroup><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K);
+  solveKernel<kGroup><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
+                                                               cachedIncident ? 1 : 0);
   return 1;
 }
 

@@ -60,6 +60,10 @@ struct Buffers {
   float4* tetRot;         // 3 per tet (co-rotated only)
   float* finalUpdate;     // per vertex update norm
   float4* local;          // 4 per vertex (local diagnostics)
+  // 3 per vertex: the incident-tet part of the local system at the next
+  // Jacobi source pose, (g.xyz, Hxx) (Hyy, Hzz, Hxy, Hxz) (Hyz, 0, 0, 0),
+  // written by the pass that computes that pose's vertex frames.
+  float4* incident;
   FrameState* frame;
   void* gatePartials;     // one GatePartial (32 bytes) per gate / prologue block
   void* convPartials;     // one ConvPartial (80 bytes) per convergence block
@@ -84,8 +88,11 @@ int launchPrologue(const Buffers& b, const DevParams* p, uint32_t V, uint32_t T,
 int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, const uint32_t* list,
                       uint32_t count, cudaStream_t s);
 int launchTetPolar(const Buffers& b, const DevParams* p, const float4* src, uint32_t T, cudaStream_t s);
+// cachedIncident: take the incident-tet gradient and Hessian of each vertex
+// from Buffers::incident (valid for a Jacobi source pose) instead of
+// gathering them.
 int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
-                uint32_t count, uint32_t K, bool glob, cudaStream_t s);
+                uint32_t count, uint32_t K, bool glob, bool cachedIncident, cudaStream_t s);
 int launchCopy(const float4* src, float4* dst, uint32_t V, cudaStream_t s);
 int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V, uint32_t T,
                cudaStream_t s);

@@ -602,7 +602,8 @@ int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bod
         });
         const uint32_t cb = s->colorOffsets[c], ce = s->colorOffsets[c + 1];
         n += timed(P::kSolve, [&] {
-          return jgs2::launchSolve(b, s->dParams, tgt, tgt, s->dColorVertices + cb, ce - cb, s->K, s->glob, st);
+          return jgs2::launchSolve(b, s->dParams, tgt, tgt, s->dColorVertices + cb, ce - cb, s->K, s->glob, false,
+                                   st);
         });
       }
     } else {
@@ -611,7 +612,11 @@ int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bod
         if (it > 0)
           n += timed(P::kVertexFrames, [&] { return jgs2::launchVertexPolar(b, s->dParams, src, nullptr, s->V, st); });
       }
-      n += timed(P::kSolve, [&] { return jgs2::launchSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, s->glob, st); });
+      // Stable Jacobi: the prologue (iteration 0) and the previous iteration's
+      // convergence pass leave the source pose's incident system in b.incident.
+      n += timed(P::kSolve, [&] {
+        return jgs2::launchSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, s->glob, s->glob, st);
+      });
     }
     if (s->glob) {
       n += timed(P::kGate, [&] { return jgs2::launchGate(b, s->dParams, src, tgt, s->V, s->T, st); });
@@ -955,8 +960,10 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
   b.tetRot = nullptr;
   STEP(deviceAlloc(sp, &b.finalUpdate, V));
   STEP(deviceAlloc(sp, &b.local, 4ull * V));
+  STEP(deviceAlloc(sp, &b.incident, 3ull * V));
   CUDA_TRY(sp, cudaMemsetAsync(b.finalUpdate, 0, sizeof(float) * V, sp->stream));
   CUDA_TRY(sp, cudaMemsetAsync(b.local, 0, sizeof(float4) * 4ull * V, sp->stream));
+  CUDA_TRY(sp, cudaMemsetAsync(b.incident, 0, sizeof(float4) * 3ull * V, sp->stream));
   STEP(deviceAlloc(sp, &b.frame, 1));
   {
     FrameState fs;
