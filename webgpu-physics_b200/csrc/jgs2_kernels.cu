@@ -394,8 +394,10 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             // ---- cubature record (jgs2-shader.ts:3197-3263) ----
             CubState st;
             const size_t rec = static_cast<size_t>(v) * K + u;
-            const uint32_t t = __ldg(&b.cubTet[rec]);
-            const float w = __ldg(&b.cubWeight[rec]);
+            const uint4 head = __ldg(&b.cubHead[2 * rec]);
+            const uint4 idx = __ldg(&b.cubHead[2 * rec + 1]);
+            const uint32_t t = head.x;
+            const float w = __uint_as_float(head.y);
             st.w = 0.0f;
             if (t != kEmptyTet && t < p.tetCount && w > 0.0f) {
               const TetRec r = loadTet(b.tets, t);
@@ -407,10 +409,10 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
               float3 gQ = f3(0, 0, 0);
               S3 HQ = szero();
               uint32_t slot = 4;
-              const float3 x0 = xyz(src[r.idx.x]);
+              const float3 x0 = xyz(src[idx.x]);
 #pragma unroll
               for (int l = 0; l < 4; ++l) {
-                const uint32_t q = idxAt(r.idx, l);
+                const uint32_t q = idxAt(idx, l);
                 if (q == v) slot = l;
                 const float3 gl = shapeGradient(r, l);
                 const M3 B = mm(mm(loadRot(b.vertexRot, q), loadBlock(U + 9 * l)), RsT);
@@ -419,11 +421,12 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                 dF0 = dF0 + outer(B.c0, gl);
                 dF1 = dF1 + outer(B.c1, gl);
                 dF2 = dF2 + outer(B.c2, gl);
-                const uint4 qi = b.vinfo[q];
-                const float4 qr = b.restMass[q];
-                const float dW = distributedInertiaWeight(qr, qi, p.invDt2);
-                float3 lin = dW * (xl - xyz(b.predicted[q]));
+                // predicted w = distributed inertia weight (0 when pinned).
+                const float4 pq = b.predicted[q];
+                const float dW = pq.w;
+                float3 lin = dW * (xl - xyz(pq));
                 float quad = dW;
+                const uint4 qi = objActive ? b.vinfo[q] : make_uint4(0u, 0u, 1u, 0u);
                 if (objActive && !isPinned(qi)) {
                   const float nq = float(qi.y > 1u ? qi.y : 1u);
                   lin = lin + objectiveGradient(p, b.objectives, q, xl) * (1.0f / nq);
@@ -799,7 +802,7 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
       } else {
         b.velocity[i] = make_float4(0, 0, 0, 0);
       }
-      b.predicted[i] = make_float4(pred.x, pred.y, pred.z, 1.0f);
+      b.predicted[i] = make_float4(pred.x, pred.y, pred.z, distributedInertiaWeight(rm, info, p.invDt2));
       const float3 src = glob ? xyz(o) : pred;
       b.pos[1][i] = make_float4(src.x, src.y, src.z, 1.0f);
       b.finalUpdate[i] = 0.0f;

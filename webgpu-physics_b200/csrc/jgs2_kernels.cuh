@@ -53,7 +53,7 @@ struct FrameState {
 struct Buffers {
   // dynamic
   float4* pos[2];         // A, B
-  float4* predicted;
+  float4* predicted;       // inertial target xyz, distributed inertia weight m/(h^2 n) (0 pinned)
   float4* velocity;
   float4* old;
   float4* vertexRot;      // 3 per vertex (columns)
@@ -73,8 +73,7 @@ struct Buffers {
   const uint4* vinfo;         // adjacency start, count, pinned, body
   const float4* tets;         // 4 per tet: [g1 vol] [g2 lambda] [g3 mu] [indices as uint]
   const uint32_t* adjacency;  // incident tet * 4 + local slot
-  const uint32_t* cubTet;
-  const float* cubWeight;
+  const uint4* cubHead;       // 2 per record: (tet, weight bits, 0, 0), the tet's vertex indices
   const float4* cubBasis;     // 9 float4 per record (36 floats, row-major blocks)
   const float* stiffness;     // 144 per tet (co-rotated only)
   float4* objectives;         // 2 per vertex: force, target + stiffness

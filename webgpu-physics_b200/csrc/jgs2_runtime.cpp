@@ -1004,12 +1004,21 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
     uint32_t* a = nullptr;
     STEP(upload(sp, &a, adjacency.data(), adjacency.size()));
     b.adjacency = a;
-    uint32_t* ct = nullptr;
-    STEP(upload(sp, &ct, cubTet.data(), R));
-    b.cubTet = ct;
-    float* cw = nullptr;
-    STEP(upload(sp, &cw, cubW.data(), R));
-    b.cubWeight = cw;
+    // Record headers: tet id and weight, then the tet's vertex indices, so a
+    // record's vertex data can be fetched without waiting for its tet.
+    std::vector<uint4> head(2 * R);
+    for (size_t rec = 0; rec < R; ++rec) {
+      const uint32_t t = cubTet[rec];
+      uint32_t wbits;
+      std::memcpy(&wbits, &cubW[rec], 4);
+      head[2 * rec] = make_uint4(t, wbits, 0u, 0u);
+      head[2 * rec + 1] = t < T ? make_uint4(in->tet_indices[4ull * t], in->tet_indices[4ull * t + 1],
+                                             in->tet_indices[4ull * t + 2], in->tet_indices[4ull * t + 3])
+                                : make_uint4(0u, 0u, 0u, 0u);
+    }
+    uint4* ch = nullptr;
+    STEP(upload(sp, &ch, head.data(), 2 * R));
+    b.cubHead = ch;
     float4* cb = nullptr;
     STEP(deviceAlloc(sp, &cb, 9 * R));
     if (R) CUDA_TRY(sp, cudaMemcpyAsync(cb, in->cubature_basis, sizeof(float) * 36 * R, cudaMemcpyHostToDevice,
@@ -1285,7 +1294,11 @@ jgs2_status jgs2_read_velocities(jgs2_solver* s, float* out, size_t floats) {
 
 jgs2_status jgs2_read_predicted_positions(jgs2_solver* s, float* out, size_t floats) {
   if (usable(s) != JGS2_OK) return usable(s);
-  return readVec4(s, s->b.predicted, out, floats, 4);
+  const jgs2_status st = readVec4(s, s->b.predicted, out, floats, 4);
+  if (st != JGS2_OK) return st;
+  // The device copy keeps the distributed inertia weight in w.
+  for (uint32_t v = 0; v < s->V; ++v) out[4ull * v + 3] = 1.0f;
+  return JGS2_OK;
 }
 
 jgs2_status jgs2_read_final_iteration_updates(jgs2_solver* s, float* out, size_t floats) {
