@@ -86,9 +86,17 @@ __device__ __forceinline__ void storeRot(float4* __restrict__ rot, uint32_t v, c
   rot[3ull * v + 2] = make_float4(m.c2.x, m.c2.y, m.c2.z, 0.f);
 }
 
-// Row-major stored Ubar block -> columns (cubatureBlock, jgs2-shader.ts:1204-1212).
-__device__ __forceinline__ M3 loadBlock(const float* __restrict__ b) {
-  return {f3(b[0], b[3], b[6]), f3(b[1], b[4], b[7]), f3(b[2], b[5], b[8])};
+// Row-major stored Ubar block l -> columns (cubatureBlock, jgs2-shader.ts:1204-1212).
+// The record's 36 basis floats are 9 float4: floats [9l, 9l + 9) lie
+// in the three float4 starting at (9l) / 4, so three vector loads replace nine
+// scalar ones.  l must be a compile-time constant after unrolling.
+__device__ __forceinline__ M3 loadBlockVec(const float4* __restrict__ rec, int l) {
+  const int k0 = (9 * l) >> 2;
+  const int off = 9 * l - 4 * k0;
+  const float4 a = __ldg(rec + k0), b = __ldg(rec + k0 + 1), c = __ldg(rec + k0 + 2);
+  const float f[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+  return {f3(f[off + 0], f[off + 3], f[off + 6]), f3(f[off + 1], f[off + 4], f[off + 7]),
+          f3(f[off + 2], f[off + 5], f[off + 8])};
 }
 
 __device__ __forceinline__ uint32_t controlBits(float packed) {
@@ -401,7 +409,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             st.w = 0.0f;
             if (t != kEmptyTet && t < p.tetCount && w > 0.0f) {
               const TetRec r = loadTet(b.tets, t);
-              const float* U = reinterpret_cast<const float*>(b.cubBasis + 9ull * rec);
+              const float4* U = b.cubBasis + 9ull * rec;
               // One basis block B_l = R_l Ubar_l R_s^T at a time: accumulate F,
               // the projected directions dF_c = sum_l B_l[:,c] g_l^T and the
               // inertia / objective quadratic (gQ, HQ) of the record.
@@ -415,7 +423,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                 const uint32_t q = idxAt(idx, l);
                 if (q == v) slot = l;
                 const float3 gl = shapeGradient(r, l);
-                const M3 B = mm(mm(loadRot(b.vertexRot, q), loadBlock(U + 9 * l)), RsT);
+                const M3 B = mm(mm(loadRot(b.vertexRot, q), loadBlockVec(U, l)), RsT);
                 const float3 xl = l == 0 ? x0 : xyz(src[q]);
                 if (l > 0) F = F + outer(xl - x0, gl);
                 dF0 = dF0 + outer(B.c0, gl);
