@@ -323,10 +323,11 @@ struct CubState {
 };
 static_assert(sizeof(CubState) <= kRecFloats * 4, "cubature cache record too small");
 
-template <int W>
 #ifndef JGS2_SOLVE_MIN_BLOCKS
 #define JGS2_SOLVE_MIN_BLOCKS 4
 #endif
+
+template <int W>
 __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
                                                       const float4* __restrict__ src, float4* tgt,
                                                       const uint32_t* __restrict__ list, uint32_t count,
@@ -393,7 +394,6 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
         float3 grad = f3(0, 0, 0);
         S3 hess = szero();
         const M3 RsT = mtrans(loadRot(b.vertexRot, v));
-        const uint32_t nItems = K + info.y;
         CubState* myCache = cache + static_cast<size_t>(group) * K;
         // Cubature records first, then (unless cached) the incident tets, in
         // separate loops so the two kinds of item never share a divergent pass.
@@ -580,29 +580,35 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             // when the geometry is feasible, as in the reference order.
             float jmin = kF32Max, de = 0.0f;
             bool geomFinite = true;
-            for (uint32_t u = lane; u < nItems; u += W) {
+            // A lane's items in order: its cached cubature records, then its
+            // incident tets (the same per-lane order as one merged loop).
+            for (uint32_t u = lane; u < K; u += W) {
+              const CubState& st = myCache[u];
+              if (!(st.w > 0.0f)) continue;
               float J = 0.0f;
-              if (u < K) {
-                const CubState& st = myCache[u];
-                if (!(st.w > 0.0f)) continue;
-                const M3 D = td.x * st.dF0 + td.y * st.dF1 + td.z * st.dF2;
-                const float dm = st.vol * snhEnergyDelta(st.F, st.I0, st.J0, D, st.lambda, st.mu, &J);
-                float comp = dm + dot3(td, st.gQ) + 0.5f * dot3(td, smv(st.HQ, td));
-                if (st.slot < 4) {
-                  float Js;
-                  comp -= st.vol * snhEnergyDelta(st.F, st.I0, st.J0, outer(td, st.gs), st.lambda, st.mu, &Js);
-                  comp -= dWs * (dot3(position - predV, td) + 0.5f * dot3(td, td));
-                  if (objActive) comp -= objectiveDelta(p, b.objectives, v, position, td) / nS;
-                }
-                de += st.w * comp;
-              } else {
-                const uint32_t entry = __ldg(&b.adjacency[info.x + (u - K)]);
-                const TetRec r = loadTet(b.tets, entry >> 2);
-                const M3 F = deformationAt(r, src);
-                const float I0 = frob(F, F);
-                const float J0 = mdet(F);
-                de += r.vol * snhEnergyDelta(F, I0, J0, outer(td, shapeGradient(r, entry & 3u)), r.lambda, r.mu, &J);
+              const M3 D = td.x * st.dF0 + td.y * st.dF1 + td.z * st.dF2;
+              const float dm = st.vol * snhEnergyDelta(st.F, st.I0, st.J0, D, st.lambda, st.mu, &J);
+              float comp = dm + dot3(td, st.gQ) + 0.5f * dot3(td, smv(st.HQ, td));
+              if (st.slot < 4) {
+                float Js;
+                comp -= st.vol * snhEnergyDelta(st.F, st.I0, st.J0, outer(td, st.gs), st.lambda, st.mu, &Js);
+                comp -= dWs * (dot3(position - predV, td) + 0.5f * dot3(td, td));
+                if (objActive) comp -= objectiveDelta(p, b.objectives, v, position, td) / nS;
               }
+              de += st.w * comp;
+              if (!finiteS(J)) geomFinite = false;
+              jmin = fminf(jmin, J);
+            }
+            // Incident tets of lane-order index u >= K, i.e. adjacency slot u - K.
+            const uint32_t firstInc = lane >= K % W ? lane - K % W : lane + W - K % W;
+            for (uint32_t a = firstInc; a < info.y; a += W) {
+              float J = 0.0f;
+              const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
+              const TetRec r = loadTet(b.tets, entry >> 2);
+              const M3 F = deformationAt(r, src);
+              const float I0 = frob(F, F);
+              const float J0 = mdet(F);
+              de += r.vol * snhEnergyDelta(F, I0, J0, outer(td, shapeGradient(r, entry & 3u)), r.lambda, r.mu, &J);
               if (!finiteS(J)) geomFinite = false;
               jmin = fminf(jmin, J);
             }
