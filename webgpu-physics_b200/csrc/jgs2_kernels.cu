@@ -121,28 +121,27 @@ __device__ __forceinline__ float distributedInertiaWeight(const float4& rm, cons
 }
 
 // vertexObjectiveGradient (jgs2-shader.ts:1926-1938).
-__device__ __forceinline__ float3 objectiveGradient(const DevParams& p, const float4* __restrict__ obj, uint32_t v,
-                                                    float3 pos) {
+__device__ __forceinline__ float3 objectiveGradient(const DevParams& p, const Buffers& b, uint32_t v, float3 pos) {
   float3 r = f3(0, 0, 0);
-  if (p.objectiveFlags & 1u) r = r - xyz(obj[2ull * v]);
+  if (p.objectiveFlags & 1u) r = r - xyz(b.forces[v]);
   if (p.objectiveFlags & 2u) {
-    const float4 t = obj[2ull * v + 1];
+    const float4 t = b.targets[v];
     if (t.w > 0.0f) r = r + t.w * (pos - xyz(t));
   }
   return r;
 }
 
-__device__ __forceinline__ float targetStiffness(const DevParams& p, const float4* __restrict__ obj, uint32_t v) {
-  return (p.objectiveFlags & 2u) ? obj[2ull * v + 1].w : 0.0f;
+__device__ __forceinline__ float targetStiffness(const DevParams& p, const Buffers& b, uint32_t v) {
+  return (p.objectiveFlags & 2u) ? b.targets[v].w : 0.0f;
 }
 
 // vertexObjectiveEnergyDelta (jgs2-shader.ts:1903-1924).
-__device__ __forceinline__ float objectiveDelta(const DevParams& p, const float4* __restrict__ obj, uint32_t v,
-                                                float3 base, float3 d) {
+__device__ __forceinline__ float objectiveDelta(const DevParams& p, const Buffers& b, uint32_t v, float3 base,
+                                                float3 d) {
   float r = 0.0f;
-  if (p.objectiveFlags & 1u) r -= dot3(xyz(obj[2ull * v]), d);
+  if (p.objectiveFlags & 1u) r -= dot3(xyz(b.forces[v]), d);
   if (p.objectiveFlags & 2u) {
-    const float4 t = obj[2ull * v + 1];
+    const float4 t = b.targets[v];
     if (t.w > 0.0f) r += t.w * (dot3(base - xyz(t), d) + 0.5f * dot3(d, d));
   }
   return r;
@@ -163,9 +162,9 @@ __device__ __forceinline__ float implicitEnergy(const DevParams& p, const Buffer
   const float3 r = x - xyz(b.predicted[v]);
   float e = 0.5f * (rm.w * p.invDt2) * dot3(r, r);
   if (p.objectiveFlags != 0u) {
-    if (p.objectiveFlags & 1u) e -= dot3(xyz(b.objectives[2ull * v]), x);
+    if (p.objectiveFlags & 1u) e -= dot3(xyz(b.forces[v]), x);
     if (p.objectiveFlags & 2u) {
-      const float4 t = b.objectives[2ull * v + 1];
+      const float4 t = b.targets[v];
       if (t.w > 0.0f) {
         const float3 q = x - xyz(t);
         e += 0.5f * t.w * dot3(q, q);
@@ -389,8 +388,8 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
         const float dWs = distributedInertiaWeight(rm, info, p.invDt2);
         const float nS = float(info.y > 1u ? info.y : 1u);
         const bool objActive = p.objectiveFlags != 0u;
-        const float3 objS = objActive ? objectiveGradient(p, b.objectives, v, position) : f3(0, 0, 0);
-        const float ktS = targetStiffness(p, b.objectives, v);
+        const float3 objS = objActive ? objectiveGradient(p, b, v, position) : f3(0, 0, 0);
+        const float ktS = targetStiffness(p, b, v);
         float3 grad = f3(0, 0, 0);
         S3 hess = szero();
         const M3 RsT = mtrans(loadRot(b.vertexRot, v));
@@ -437,8 +436,8 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                 const uint4 qi = objActive ? b.vinfo[q] : make_uint4(0u, 0u, 1u, 0u);
                 if (objActive && !isPinned(qi)) {
                   const float nq = float(qi.y > 1u ? qi.y : 1u);
-                  lin = lin + objectiveGradient(p, b.objectives, q, xl) * (1.0f / nq);
-                  quad += targetStiffness(p, b.objectives, q) / nq;
+                  lin = lin + objectiveGradient(p, b, q, xl) * (1.0f / nq);
+                  quad += targetStiffness(p, b, q) / nq;
                 }
                 gQ = gQ + mtv(B, lin);
                 saddScaled(HQ, quad, gramColumns(B));
@@ -593,7 +592,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                 float Js;
                 comp -= st.vol * snhEnergyDelta(st.F, st.I0, st.J0, outer(td, st.gs), st.lambda, st.mu, &Js);
                 comp -= dWs * (dot3(position - predV, td) + 0.5f * dot3(td, td));
-                if (objActive) comp -= objectiveDelta(p, b.objectives, v, position, td) / nS;
+                if (objActive) comp -= objectiveDelta(p, b, v, position, td) / nS;
               }
               de += st.w * comp;
               if (!finiteS(J)) geomFinite = false;
@@ -620,7 +619,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             minTrialDet = trialMin;
             if (trialMin > kDeterminantFloor) {
               de += inertia * (dot3(position - predV, td) + 0.5f * dot3(td, td)) + floorDelta(p, position.y, td.y);
-              if (objActive) de += objectiveDelta(p, b.objectives, v, position, td);
+              if (objActive) de += objectiveDelta(p, b, v, position, td);
               evals += 1;
               if (!finiteS(de)) { status = kNonfinite; backtracks = bt; break; }
               const float tb = kArmijoC1 * gd;
@@ -976,9 +975,9 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
       comps[2] = f3(0, 0, 0);
       comps[3] = f3(0, 0, 0);
       if (p.objectiveFlags != 0u) {
-        if (p.objectiveFlags & 1u) comps[2] = -xyz(b.objectives[2ull * v]);
+        if (p.objectiveFlags & 1u) comps[2] = -xyz(b.forces[v]);
         if (p.objectiveFlags & 2u) {
-          const float4 t = b.objectives[2ull * v + 1];
+          const float4 t = b.targets[v];
           if (t.w > 0.0f) comps[3] = t.w * (x - xyz(t));
         }
       }

@@ -76,7 +76,8 @@ struct Buffers {
   const uint4* cubHead;       // 2 per record: (tet, weight bits, 0, 0), the tet's vertex indices
   const float4* cubBasis;     // 9 float4 per record (36 floats, row-major blocks)
   const float* stiffness;     // 144 per tet (co-rotated only)
-  float4* objectives;         // 2 per vertex: force, target + stiffness
+  float4* forces;             // external force xyz per vertex
+  float4* targets;            // quadratic target xyz, stiffness per vertex
   const uint32_t* colors;     // per vertex colour
   uint32_t gateBlocks, convBlocks;
 };

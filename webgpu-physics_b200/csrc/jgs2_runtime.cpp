@@ -430,8 +430,12 @@ struct jgs2_solver {
   std::vector<uint32_t> colors;
   std::vector<uint32_t> colorOffsets;   // colorCount + 1 into colorVertices
   std::vector<uint32_t> needOffsets;    // colorCount + 1 into needVertices
-  // objectives (host mirror: force xyz, 0, target xyz, stiffness)
-  std::vector<float> objectives;
+  // Objectives: pinned host mirrors of the device force and target arrays
+  // (force xyz, 0) and (target xyz, stiffness); uploads copy from them.
+  float4* hForces = nullptr;
+  float4* hTargets = nullptr;
+  cudaEvent_t objectiveUpload = nullptr;  // recorded after the last upload
+  bool objectiveUploadPending = false;
   std::vector<uint8_t> pinned;
   uint32_t objectiveFlags = 0, forceCount = 0, targetCount = 0, objectiveRevision = 0;
   // device
@@ -490,21 +494,21 @@ void releaseDevice(jgs2_solver* s) {
   if (s->stream) cudaStreamSynchronize(s->stream);
   for (void* p : s->allocations) cudaFree(p);
   s->allocations.clear();
+  if (s->hForces) cudaFreeHost(s->hForces);
+  if (s->hTargets) cudaFreeHost(s->hTargets);
+  s->hForces = s->hTargets = nullptr;
+  if (s->objectiveUpload) cudaEventDestroy(s->objectiveUpload);
+  s->objectiveUpload = nullptr;
   if (s->stream) cudaStreamDestroy(s->stream);
   s->stream = nullptr;
 }
 
-void refreshObjectiveActivity(jgs2_solver* s) {
-  uint32_t f = 0, t = 0;
-  for (uint32_t v = 0; v < s->V; ++v) {
-    const float* o = &s->objectives[8ull * v];
-    if (o[0] != 0 || o[1] != 0 || o[2] != 0) f++;
-    if (o[7] > 0) t++;
-  }
-  s->forceCount = f;
-  s->targetCount = t;
-  s->objectiveFlags = (f ? 1u : 0u) | (t ? 2u : 0u);
+bool forceActive(const float4& f) { return f.x != 0 || f.y != 0 || f.z != 0; }
+
+void refreshObjectiveFlags(jgs2_solver* s) {
+  s->objectiveFlags = (s->forceCount ? 1u : 0u) | (s->targetCount ? 2u : 0u);
 }
+
 
 DevParams makeParams(const jgs2_solver* s, const jgs2_settings& st, bool stop) {
   DevParams p{};
@@ -723,11 +727,26 @@ jgs2_status usable(jgs2_solver* s) {
   return JGS2_OK;
 }
 
-jgs2_status writeObjectives(jgs2_solver* s, uint32_t firstVertex, uint32_t vertexCount) {
+// The host mirrors may change only after the previous upload from them has
+// been consumed by the copy engine.
+jgs2_status waitObjectiveMirror(jgs2_solver* s) {
+  if (!s->objectiveUploadPending) return JGS2_OK;
+  CUDA_TRY(s, cudaEventSynchronize(s->objectiveUpload));
+  s->objectiveUploadPending = false;
+  return JGS2_OK;
+}
+
+jgs2_status writeObjectives(jgs2_solver* s, uint32_t firstVertex, uint32_t vertexCount, bool forces, bool targets) {
   CUDA_TRY(s, cudaSetDevice(s->device));
-  CUDA_TRY(s, cudaMemcpyAsync(s->b.objectives + 2ull * firstVertex, &s->objectives[8ull * firstVertex],
-                              32ull * vertexCount, cudaMemcpyHostToDevice, s->stream));
-  refreshObjectiveActivity(s);
+  if (forces)
+    CUDA_TRY(s, cudaMemcpyAsync(s->b.forces + firstVertex, s->hForces + firstVertex,
+                                sizeof(float4) * vertexCount, cudaMemcpyHostToDevice, s->stream));
+  if (targets)
+    CUDA_TRY(s, cudaMemcpyAsync(s->b.targets + firstVertex, s->hTargets + firstVertex,
+                                sizeof(float4) * vertexCount, cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaEventRecord(s->objectiveUpload, s->stream));
+  s->objectiveUploadPending = true;
+  refreshObjectiveFlags(s);
   s->objectiveRevision += 1;
   return JGS2_OK;
 }
@@ -840,19 +859,21 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
                                (hi[2] - lo[2]) * (hi[2] - lo[2]));
     s->sceneScale = static_cast<float>(dyn > 0 && std::isfinite(d) && d > 0 ? d : kDegenerateSceneScale);
   }
-  // Objectives (packJGS2VertexObjectives, layout.ts:635-668).
-  s->objectives.assign(8ull * s->V, 0.f);
+  // Objectives (packJGS2VertexObjectives, layout.ts:635-668); copied into
+  // the pinned mirrors once the device is set up.
+  std::vector<float4> initialForces(s->V), initialTargets(s->V);
   s->pinned.assign(s->V, 0);
+  s->forceCount = s->targetCount = 0;
   for (uint32_t v = 0; v < s->V; ++v) {
-    float* o = &s->objectives[8ull * v];
-    if (in->external_forces)
-      for (int k = 0; k < 3; ++k) o[k] = in->external_forces[3ull * v + k];
-    for (int k = 0; k < 3; ++k)
-      o[4 + k] = in->target_positions ? in->target_positions[3ull * v + k] : in->positions[4ull * v + k];
-    o[7] = in->target_stiffnesses ? in->target_stiffnesses[v] : 0.f;
+    const float* f = in->external_forces ? &in->external_forces[3ull * v] : nullptr;
+    initialForces[v] = f ? make_float4(f[0], f[1], f[2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+    const float* tp = in->target_positions ? &in->target_positions[3ull * v] : &in->positions[4ull * v];
+    initialTargets[v] = make_float4(tp[0], tp[1], tp[2], in->target_stiffnesses ? in->target_stiffnesses[v] : 0.f);
+    if (forceActive(initialForces[v])) s->forceCount++;
+    if (initialTargets[v].w > 0) s->targetCount++;
     s->pinned[v] = in->vertex_info[4ull * v + 2] != 0;
   }
-  refreshObjectiveActivity(s.get());
+  refreshObjectiveFlags(s.get());
   // Colour lists and per-colour frame lists.
   std::vector<uint32_t> byColor(s->V);
   s->colorOffsets.assign(colorCount + 1, 0);
@@ -1025,10 +1046,21 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
                                         sp->stream));
     b.cubBasis = cb;
     b.stiffness = nullptr;
-    float4* ob = nullptr;
-    STEP(deviceAlloc(sp, &ob, 2ull * V));
-    b.objectives = ob;
-    CUDA_TRY(sp, cudaMemcpyAsync(ob, sp->objectives.data(), 32ull * V, cudaMemcpyHostToDevice, sp->stream));
+    float4* df = nullptr;
+    float4* dt = nullptr;
+    STEP(deviceAlloc(sp, &df, V));
+    STEP(deviceAlloc(sp, &dt, V));
+    b.forces = df;
+    b.targets = dt;
+    CUDA_TRY(sp, cudaMallocHost(reinterpret_cast<void**>(&sp->hForces), sizeof(float4) * std::max<size_t>(1, V)));
+    CUDA_TRY(sp, cudaMallocHost(reinterpret_cast<void**>(&sp->hTargets), sizeof(float4) * std::max<size_t>(1, V)));
+    CUDA_TRY(sp, cudaEventCreateWithFlags(&sp->objectiveUpload, cudaEventDisableTiming));
+    std::memcpy(sp->hForces, initialForces.data(), sizeof(float4) * V);
+    std::memcpy(sp->hTargets, initialTargets.data(), sizeof(float4) * V);
+    CUDA_TRY(sp, cudaMemcpyAsync(df, sp->hForces, sizeof(float4) * V, cudaMemcpyHostToDevice, sp->stream));
+    CUDA_TRY(sp, cudaMemcpyAsync(dt, sp->hTargets, sizeof(float4) * V, cudaMemcpyHostToDevice, sp->stream));
+    CUDA_TRY(sp, cudaEventRecord(sp->objectiveUpload, sp->stream));
+    sp->objectiveUploadPending = true;
     uint32_t* cl = nullptr;
     STEP(upload(sp, &cl, colors.data(), V));
     b.colors = cl;
@@ -1176,9 +1208,13 @@ jgs2_status jgs2_set_external_force(jgs2_solver* s, uint32_t vertex, const float
                   format("External force %d for vertex %u must be finite after f32 conversion.", k, vertex));
   if (s->pinned[vertex] && (force[0] != 0 || force[1] != 0 || force[2] != 0))
     return fail(s, JGS2_INVALID_ARGUMENT, format("Pinned vertex %u cannot have a nonzero external force.", vertex));
-  float* o = &s->objectives[8ull * vertex];
-  o[0] = force[0]; o[1] = force[1]; o[2] = force[2]; o[3] = 0.f;
-  return writeObjectives(s, vertex, 1);
+  st = waitObjectiveMirror(s);
+  if (st != JGS2_OK) return st;
+  float4& f = s->hForces[vertex];
+  s->forceCount -= forceActive(f) ? 1u : 0u;
+  f = make_float4(force[0], force[1], force[2], 0.f);
+  s->forceCount += forceActive(f) ? 1u : 0u;
+  return writeObjectives(s, vertex, 1, true, false);
 }
 
 jgs2_status jgs2_replace_external_forces(jgs2_solver* s, const float* forces) {
@@ -1196,11 +1232,16 @@ jgs2_status jgs2_replace_external_forces(jgs2_solver* s, const float* forces) {
     if (s->pinned[v] && nonzero)
       return fail(s, JGS2_INVALID_ARGUMENT, format("Pinned vertex %u cannot have a nonzero external force.", v));
   }
+  st = waitObjectiveMirror(s);
+  if (st != JGS2_OK) return st;
+  uint32_t count = 0;
   for (uint32_t v = 0; v < s->V; ++v) {
-    float* o = &s->objectives[8ull * v];
-    o[0] = forces[3ull * v]; o[1] = forces[3ull * v + 1]; o[2] = forces[3ull * v + 2]; o[3] = 0.f;
+    const float4 f = make_float4(forces[3ull * v], forces[3ull * v + 1], forces[3ull * v + 2], 0.f);
+    s->hForces[v] = f;
+    count += forceActive(f) ? 1u : 0u;
   }
-  return writeObjectives(s, 0, s->V);
+  s->forceCount = count;
+  return writeObjectives(s, 0, s->V, true, false);
 }
 
 jgs2_status jgs2_clear_external_forces(jgs2_solver* s) {
@@ -1228,9 +1269,13 @@ jgs2_status jgs2_set_quadratic_target(jgs2_solver* s, uint32_t vertex, const flo
   if (s->pinned[vertex] && stiffness != 0)
     return fail(s, JGS2_INVALID_ARGUMENT,
                 format("Pinned vertex %u cannot have a nonzero quadratic-target stiffness.", vertex));
-  float* o = &s->objectives[8ull * vertex];
-  o[4] = target[0]; o[5] = target[1]; o[6] = target[2]; o[7] = stiffness;
-  return writeObjectives(s, vertex, 1);
+  st = waitObjectiveMirror(s);
+  if (st != JGS2_OK) return st;
+  float4& t = s->hTargets[vertex];
+  s->targetCount -= t.w > 0 ? 1u : 0u;
+  t = make_float4(target[0], target[1], target[2], stiffness);
+  s->targetCount += t.w > 0 ? 1u : 0u;
+  return writeObjectives(s, vertex, 1, false, true);
 }
 
 jgs2_status jgs2_replace_quadratic_targets(jgs2_solver* s, const float* positions, const float* stiffnesses) {
@@ -1252,26 +1297,36 @@ jgs2_status jgs2_replace_quadratic_targets(jgs2_solver* s, const float* position
       return fail(s, JGS2_INVALID_ARGUMENT,
                   format("Pinned vertex %u cannot have a nonzero quadratic-target stiffness.", v));
   }
+  st = waitObjectiveMirror(s);
+  if (st != JGS2_OK) return st;
+  uint32_t count = 0;
   for (uint32_t v = 0; v < s->V; ++v) {
-    float* o = &s->objectives[8ull * v];
-    o[4] = positions[3ull * v]; o[5] = positions[3ull * v + 1]; o[6] = positions[3ull * v + 2]; o[7] = stiffnesses[v];
+    s->hTargets[v] = make_float4(positions[3ull * v], positions[3ull * v + 1], positions[3ull * v + 2], stiffnesses[v]);
+    count += stiffnesses[v] > 0 ? 1u : 0u;
   }
-  return writeObjectives(s, 0, s->V);
+  s->targetCount = count;
+  return writeObjectives(s, 0, s->V, false, true);
 }
 
 jgs2_status jgs2_release_quadratic_target(jgs2_solver* s, uint32_t vertex) {
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
   if (vertex >= s->V) return fail(s, JGS2_INVALID_ARGUMENT, format("vertex %u is out of range.", vertex));
-  s->objectives[8ull * vertex + 7] = 0.f;
-  return writeObjectives(s, vertex, 1);
+  st = waitObjectiveMirror(s);
+  if (st != JGS2_OK) return st;
+  s->targetCount -= s->hTargets[vertex].w > 0 ? 1u : 0u;
+  s->hTargets[vertex].w = 0.f;
+  return writeObjectives(s, vertex, 1, false, true);
 }
 
 jgs2_status jgs2_release_all_quadratic_targets(jgs2_solver* s) {
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
-  for (uint32_t v = 0; v < s->V; ++v) s->objectives[8ull * v + 7] = 0.f;
-  return writeObjectives(s, 0, s->V);
+  st = waitObjectiveMirror(s);
+  if (st != JGS2_OK) return st;
+  for (uint32_t v = 0; v < s->V; ++v) s->hTargets[v].w = 0.f;
+  s->targetCount = 0;
+  return writeObjectives(s, 0, s->V, false, true);
 }
 
 static jgs2_status readVec4(jgs2_solver* s, const float4* dev, float* out, size_t floats, size_t perVertex) {
