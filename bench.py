@@ -44,10 +44,17 @@ def parse_args():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cells", type=int, default=100, help="hexes per cube edge")
-    ap.add_argument("--iterations", type=int, default=20)
+    ap.add_argument("--iterations", type=int, default=None,
+                    help="iterations per frame (default 20 for the cube, 10 for the batched bodies)")
     ap.add_argument("--schedule", default="jacobi", choices=["jacobi", "graph-colored-gauss-seidel"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    return ap.parse_args()
+    ap.add_argument("--workload", default="cube", choices=["cube", "batched"],
+                    help="cube: one large body (headline); batched: independent uneven bodies in one batch")
+    ap.add_argument("--bodies", type=int, default=256, help="scenes of the batched workload")
+    args = ap.parse_args()
+    if args.iterations is None:
+        args.iterations = 10 if args.workload == "batched" else 20
+    return args
 
 
 def cache_dir() -> str:
@@ -87,9 +94,37 @@ def workload_config(inp, args, precompute_info):
         "iterations": args.iterations,
         "schedule": args.schedule,
         "step": "one frame",
-        "l2": "no flush: the resident state per iteration (~1.5 GB) exceeds the 126 MB L2",
+        "l2": (f"no flush: one iteration touches {algorithmic_bytes(inp) / 1e9:.2f} GB of resident state, "
+               "more than the 126 MB L2"),
         "precompute": precompute_info,
     }
+
+
+def algorithmic_bytes(inp) -> int:
+    """Bytes one Jacobi iteration must move at least: V(84 + 152K) + 80T."""
+    return inp.vertex_count * (84 + 152 * inp.cubature_k) + 80 * inp.tet_count
+
+
+def batched_workload(count: int):
+    """The batched uneven bodies as independent scenes (cached packed input)."""
+    from jgs2_b200 import scenes
+
+    path = os.path.join(cache_dir(), f"batched{count}_k6_r2_v1.npz")
+    cached = False
+    inp = None
+    if os.path.exists(path):
+        try:
+            inp = scenes.SceneInput.load(path)
+            cached = True
+        except Exception:
+            os.remove(path)
+    if inp is None:
+        inp = scenes.batched_bodies(count=count)
+        try:
+            inp.save(path)
+        except OSError:
+            pass
+    return inp, inp.split_bodies(), cached
 
 
 class ClockSampler:
@@ -266,6 +301,115 @@ def reference_arm(args):
     return 0
 
 
+def batched_arm(args):
+    """Independent uneven bodies (hex boxes with U{4..32} cells per axis, soft
+    and stiff materials, free fall onto the penalty floor), one scene each,
+    stepped as one batch; the plain per-scene path (one solver per scene,
+    stepped one after another) is timed beside it."""
+    import torch
+
+    from jgs2_b200 import solver
+
+    world, rank, local = dist_env()
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    device = local
+    t0 = time.perf_counter()
+    whole, parts, cached = batched_workload(args.bodies)
+    build_s = time.perf_counter() - t0
+    settings = dict(timestep=1 / 60)
+    iters = args.iterations
+    batch = solver.JGS2Batch.create(parts, settings, device=device)
+    stream = torch.cuda.ExternalStream(batch.stream(), device=device)
+    active = sum(p.active_vertex_count() for p in parts)
+    V = sum(p.vertex_count for p in parts)
+    for _ in range(args.warmup):
+        batch.stepFrames(1, exactIterations=iters)
+    batch.awaitIdle()
+    launches0 = batch.kernelLaunchCount()
+    start_ev = torch.cuda.Event(enable_timing=True)
+    end_ev = torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clocks:
+        start_ev.record(stream)
+        for _ in range(args.steps):
+            batch.stepFrames(1, exactIterations=iters)
+        end_ev.record(stream)
+        end_ev.synchronize()
+    ms = max_over_ranks(dist, start_ev.elapsed_time(end_ev), f"cuda:{device}")
+    launches = batch.kernelLaunchCount() - launches0
+    value = whole_job_rate(world, active * iters * args.steps, ms / 1e3)
+    # End to end: each frame's settings upload and a read of every scene's positions.
+    pos_host = torch.empty(4 * V, dtype=torch.float32).pin_memory()
+    p_np = pos_host.numpy()
+    e2e_steps = max(1, min(args.steps, 5))
+    t_e2e = time.perf_counter()
+    for _ in range(e2e_steps):
+        batch.stepFrames(1, exactIterations=iters)
+        batch.readAllPositions(out=p_np)
+    e2e_total = max_over_ranks(dist, time.perf_counter() - t_e2e, f"cuda:{device}")
+    batch.destroy()
+    # The plain per-scene path: one solver per scene, each frame launched per scene.
+    plain = [solver.JGS2GpuSolver.create(p, settings, device=device) for p in parts]
+    for _ in range(max(1, args.warmup)):
+        for s in plain:
+            s.stepExactIterations(iters)
+    torch.cuda.synchronize(device)
+    plain_steps = max(1, min(args.steps, 5))
+    t_plain = time.perf_counter()
+    for _ in range(plain_steps):
+        for s in plain:
+            s.stepExactIterations(iters)
+    torch.cuda.synchronize(device)
+    plain_s = max_over_ranks(dist, time.perf_counter() - t_plain, f"cuda:{device}")
+    for s in plain:
+        s.destroy()
+    plain_value = whole_job_rate(world, active * iters * plain_steps, plain_s)
+    algorithmic = sum(algorithmic_bytes(p) for p in parts) * iters
+    peak, peak_kind = peaks()
+    achieved = algorithmic / (ms / args.steps / 1e3) / 1e9
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+            "config": {
+                "workload": (f"{len(parts)} independent hex-grid bodies, U{{4..32}} cells per axis (Mulberry32 seed "
+                             f"65537), soft E=5e4 / stiff E=5e6 alternating, nu=0.4, free fall onto the penalty "
+                             f"floor, K=6 patch-trained cubature, {iters} exact Jacobi iterations per frame, "
+                             f"dt=1/60, one batch"),
+                "scenes": len(parts), "vertices": V, "active_vertices": active,
+                "tets": sum(p.tet_count for p in parts), "iterations": iters, "step": "one frame of every scene",
+                "l2": (f"no flush: one iteration touches {algorithmic / iters / 1e9:.2f} GB of resident state, "
+                       "more than the 126 MB L2"),
+                "precompute": {"cached": cached, "seconds": round(build_s, 1)},
+                "parallelism": "replicas" if world > 1 else "single GPU"},
+            "frames_per_s": world * len(parts) * 1e3 * args.steps / ms,
+            "gpu_launches": int(launches),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": None,
+                         "kernel": "whole frame (all kernels of one batched frame)",
+                         "algorithmic_bytes_per_launch": algorithmic,
+                         "peak_source": f"{peak_kind} hbm_gbs"},
+            "plain_per_scene": {"value": plain_value, "unit": UNIT,
+                                "frames_per_s": world * len(parts) * plain_steps / plain_s,
+                                "batched_speedup": value / plain_value,
+                                "timing": "wall clock around device-synchronised frames"},
+            "cpu_baseline": None,
+            "e2e": {"value": whole_job_rate(world, active * iters * e2e_steps, e2e_total), "unit": UNIT,
+                    "h2d_bytes_per_step": int(len(parts) * 128), "d2h_bytes_per_step": int(16 * V),
+                    "steps": e2e_steps},
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def ours_arm(args):
     import numpy as np
     import torch
@@ -386,6 +530,8 @@ def main():
     args = parse_args()
     if args.impl == "reference":
         return reference_arm(args)
+    if args.workload == "batched":
+        return batched_arm(args)
     return ours_arm(args)
 
 

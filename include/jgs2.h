@@ -360,6 +360,48 @@ jgs2_status jgs2_device_positions(jgs2_solver* solver, void** device_ptr,
  * library issues is counted, including graph replays). */
 uint64_t jgs2_kernel_launch_count(const jgs2_solver* solver);
 
+/* ---- batched form ---------------------------------------------------------
+ * Many independent scenes stepped together by one launch sequence.  The
+ * reference has no batched solver: each scene would be its own
+ * JGS2GpuSolver.  A batch keeps every scene's semantics: its own settings,
+ * its own assembled gate (a rejected candidate reverts only that scene), its
+ * own convergence history and stop latch.  Scenes are concatenated in device
+ * memory; kernels look up the scene of each vertex and the gate and
+ * convergence reductions are segmented per scene. */
+typedef struct jgs2_batch jgs2_batch;
+
+/* inputs: scene_count scene inputs (validated and copied as jgs2_create
+ * does); settings / masks: NULL or one per scene. */
+jgs2_status jgs2_batch_create(const jgs2_input* const* inputs, uint32_t scene_count,
+                              const jgs2_settings* settings, const uint32_t* masks, int device,
+                              jgs2_batch** out);
+void jgs2_batch_destroy(jgs2_batch* batch);
+const char* jgs2_batch_last_error(const jgs2_batch* batch);
+uint32_t jgs2_batch_scene_count(const jgs2_batch* batch);
+/* Total vertices over all scenes. */
+uint32_t jgs2_batch_vertex_count(const jgs2_batch* batch);
+
+/* Advance every scene `frames` frames.  exact_iterations > 0 runs exactly
+ * that many iterations per frame (stepFramesExactIterations); 0 runs the
+ * production step (odd-normalised iteration count with the stop latch), and
+ * then every scene's normalised count must agree.  overrides / masks: NULL or
+ * one per scene.  All scenes must use the same schedule. */
+jgs2_status jgs2_batch_step_frames(jgs2_batch* batch, uint32_t frames, uint32_t exact_iterations,
+                                   const jgs2_settings* overrides, const uint32_t* masks);
+jgs2_status jgs2_batch_sync(jgs2_batch* batch);
+jgs2_status jgs2_batch_get_info(jgs2_batch* batch, uint32_t scene, jgs2_info* out);
+/* Per-scene reads, laid out as the solver reads. */
+jgs2_status jgs2_batch_read_positions(jgs2_batch* batch, uint32_t scene, float* out, size_t floats);
+jgs2_status jgs2_batch_read_velocities(jgs2_batch* batch, uint32_t scene, float* out, size_t floats);
+jgs2_status jgs2_batch_read_globalization(jgs2_batch* batch, uint32_t scene, float* local,
+                                          size_t local_floats, float* control, float* history,
+                                          size_t history_floats, uint32_t* history_count);
+/* Positions of all scenes, concatenated in scene order (4 floats per vertex). */
+jgs2_status jgs2_batch_read_all_positions(jgs2_batch* batch, float* out, size_t floats);
+uint64_t jgs2_batch_kernel_launch_count(const jgs2_batch* batch);
+/* The batch's CUDA stream (a cudaStream_t), for event timing and ordering. */
+void* jgs2_batch_stream(const jgs2_batch* batch);
+
 #ifdef __cplusplus
 }
 #endif

@@ -278,20 +278,11 @@ __global__ void __launch_bounds__(kBlock) vertexPolarKernel(Buffers b, const Dev
                                                             const uint32_t* __restrict__ list, uint32_t count) {
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
   if (i >= count) return;
-  const DevParams p = *pp;
-  if (latched(p, b.frame)) return;
   const uint32_t v = list ? list[i] : i;
+  const uint32_t scene = b.vertexScene[v];
+  const DevParams& p = pp[scene];
+  if (latched(p, &b.frames[scene])) return;
   storeRot(b.vertexRot, v, vertexFrame(b, x, v, p.rotationEpsilon));
-}
-
-// tetPolarRotation (jgs2-shader.ts:2931-2957) for the co-rotated path.
-__global__ void __launch_bounds__(kBlock) tetPolarKernel(Buffers b, const DevParams* __restrict__ pp,
-                                                         const float4* __restrict__ x, uint32_t T) {
-  const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
-  if (t >= T) return;
-  const DevParams p = *pp;
-  const TetRec r = loadTet(b.tets, t);
-  storeRot(b.tetRot, t, polarRotation(deformationAt(r, x), p.rotationEpsilon));
 }
 
 __global__ void __launch_bounds__(kBlock) copyKernel(const float4* __restrict__ src, float4* __restrict__ dst,
@@ -333,24 +324,30 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                                                       uint32_t K, int cachedIncident) {
   extern __shared__ float4 cache4[];
   CubState* cache = reinterpret_cast<CubState*>(cache4);
-  __shared__ uint32_t sFail, sMaxBack, sSkip, sEvals, sMaxShift, sValid;
-  const DevParams p = *pp;
-  FrameState* fs = b.frame;
-  if (threadIdx.x == 0) { sFail = 0; sMaxBack = 0; sSkip = 0; sEvals = 0; sMaxShift = 0; sValid = 1; }
-  __syncthreads();
+  __shared__ uint32_t sFail, sMaxBack, sSkip, sEvals, sMaxShift, sValid, sScene;
   const uint32_t lane = threadIdx.x % W;
   const uint32_t group = threadIdx.x / W;
   const uint32_t groupsPerBlock = blockDim.x / W;
   const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x & 31u) / W * W));
-  const bool isLatched = latched(p, fs);
-  // Persistent grid: each lane group walks vertices with a grid stride.
-  for (uint32_t item = blockIdx.x * groupsPerBlock + group; item < count; item += gridDim.x * groupsPerBlock) {
+  if (threadIdx.x == 0) {
+    sFail = 0; sMaxBack = 0; sSkip = 0; sEvals = 0; sMaxShift = 0; sValid = 1;
+    const uint32_t first = blockIdx.x * groupsPerBlock;
+    sScene = b.vertexScene[list ? list[first] : first];
+  }
+  __syncthreads();
+  // One vertex per lane group; its scene selects the settings and records.
+  const uint32_t item = blockIdx.x * groupsPerBlock + group;
+  const bool haveVertex = item < count;
+  const uint32_t v = haveVertex ? (list ? list[item] : item) : 0u;
+  const uint32_t scene = haveVertex ? b.vertexScene[v] : sScene;
   // Per-vertex outputs owned by lane 0.
   uint32_t status = kNonfinite, backtracks = 0, evals = 0;
   float shiftN = 0.0f;
   bool localValid = true, haveRecord = false;
-  {
-    const uint32_t v = list ? list[item] : item;
+  if (haveVertex) {
+    const DevParams p = pp[scene];
+    FrameState* fs = &b.frames[scene];
+    const bool isLatched = latched(p, fs);
     const uint4 info = b.vinfo[v];
     const float4 rm = b.restMass[v];
     if (isLatched) {
@@ -406,7 +403,8 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             const uint32_t t = head.x;
             const float w = __uint_as_float(head.y);
             st.w = 0.0f;
-            if (t != kEmptyTet && t < p.tetCount && w > 0.0f) {
+            // Headers hold global tet ids; out-of-range records were emptied at create.
+            if (t != kEmptyTet && w > 0.0f) {
               const TetRec r = loadTet(b.tets, t);
               const float4* U = b.cubBasis + 9ull * rec;
               // One basis block B_l = R_l Ubar_l R_s^T at a time: accumulate F,
@@ -651,7 +649,10 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
       }
     }
   }
-  // Local aggregates of reduceCandidate's vertex loop (jgs2-shader.ts:3689-3790).
+  // Local aggregates of reduceCandidate's vertex loop (jgs2-shader.ts:3689-3790),
+  // per scene: folded in shared memory when the block's vertices share one
+  // scene, otherwise added per vertex.
+  const bool oneScene = __syncthreads_and(!haveVertex || scene == sScene) != 0;
   if (haveRecord && lane == 0) {
     const bool failure = status == kShiftLimit || status == kNonDescent || status == kLineSearchFailed ||
                          status == kNonfinite || status == kCholeskyFailed;
@@ -661,16 +662,27 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
     else if (status == kZeroGradient && backtracks > 0) trials = backtracks;
     else if (status == kNonfinite) trials = backtracks;  // a nonfinite trial never has J above the floor here
     const uint32_t skipped = trials - (trials < evals ? trials : evals);
-    if (failure) atomicAdd(&sFail, 1u);
-    if (backtracks) atomicMax(&sMaxBack, backtracks);
-    if (skipped) atomicAdd(&sSkip, skipped);
-    if (evals) atomicAdd(&sEvals, evals);
-    if (shiftN > 0.0f && finiteS(shiftN)) atomicMax(&sMaxShift, __float_as_uint(shiftN));
-    if (!localValid) sValid = 0;
+    const uint32_t shiftBits = (shiftN > 0.0f && finiteS(shiftN)) ? __float_as_uint(shiftN) : 0u;
+    if (oneScene) {
+      if (failure) atomicAdd(&sFail, 1u);
+      if (backtracks) atomicMax(&sMaxBack, backtracks);
+      if (skipped) atomicAdd(&sSkip, skipped);
+      if (evals) atomicAdd(&sEvals, evals);
+      if (shiftBits) atomicMax(&sMaxShift, shiftBits);
+      if (!localValid) sValid = 0;
+    } else {
+      FrameState* fs = &b.frames[scene];
+      if (failure) atomicAdd(&fs->localFailures, 1u);
+      if (backtracks) atomicMax(&fs->localMaxBacktracks, backtracks);
+      if (skipped) atomicAdd(&fs->localSkipped, skipped);
+      if (evals) atomicAdd(&fs->localEvaluations, evals);
+      if (shiftBits) atomicMax(&fs->localMaxShift, shiftBits);
+      if (!localValid) atomicAnd(&fs->localNumericsValid, 0u);
+    }
   }
-  }  // vertex loop
   __syncthreads();
-  if (threadIdx.x == 0) {
+  if (oneScene && threadIdx.x == 0) {
+    FrameState* fs = &b.frames[sScene];
     if (sFail) atomicAdd(&fs->localFailures, sFail);
     if (sMaxBack) atomicMax(&fs->localMaxBacktracks, sMaxBack);
     if (sSkip) atomicAdd(&fs->localSkipped, sSkip);
@@ -739,13 +751,15 @@ __device__ __forceinline__ P blockFold(P v, P* smem, C combine) {
   return r;
 }
 
-// Publishes the block partial; returns true in every thread of the last block.
+// Publishes the block partial at `slot`; returns true in every thread of the
+// last of the `count` blocks sharing `ticket`.
 template <class P>
-__device__ __forceinline__ bool publishPartial(const P& blockValue, P* partials, uint32_t* ticket, bool* isLast) {
+__device__ __forceinline__ bool publishPartial(const P& blockValue, P* partials, uint32_t slot, uint32_t count,
+                                               uint32_t* ticket, bool* isLast) {
   if (threadIdx.x == 0) {
-    partials[blockIdx.x] = blockValue;
+    partials[slot] = blockValue;
     __threadfence();
-    *isLast = atomicAdd(ticket, 1u) == gridDim.x - 1;
+    *isLast = atomicAdd(ticket, 1u) == count - 1;
   }
   __syncthreads();
   const bool last = *isLast;
@@ -753,11 +767,12 @@ __device__ __forceinline__ bool publishPartial(const P& blockValue, P* partials,
   return last;
 }
 
+// Folds partials[0, count) in index order (deterministic).
 template <class P, class I, class C>
-__device__ __forceinline__ P foldPartials(const P* partials, P* smem, I identity, C combine) {
+__device__ __forceinline__ P foldPartials(const P* partials, uint32_t count, P* smem, I identity, C combine) {
   P acc = identity();
   static_assert(sizeof(P) % 4 == 0, "partials are read as 32-bit words");
-  for (uint32_t k = threadIdx.x; k < gridDim.x; k += blockDim.x) {
+  for (uint32_t k = threadIdx.x; k < count; k += blockDim.x) {
     // Other blocks wrote these partials: read them from L2.
     uint32_t words[sizeof(P) / 4];
     const uint32_t* w = reinterpret_cast<const uint32_t*>(partials + k);
@@ -794,16 +809,17 @@ __device__ __forceinline__ void accumulateTet(GatePartial& acc, const TetRec& r,
 // Prologue: predict (jgs2-shader.ts:2660-2692), iteration-0 vertex frames and
 // the source feasibility preflight (candidateTetrahedron + reduceCandidate on
 // the accepted pose, jgs2-solver.ts:2240-2259).
-__global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevParams* __restrict__ pp, uint32_t V,
-                                                         uint32_t T, int glob) {
+__global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevParams* __restrict__ pp) {
   __shared__ GatePartial smem[kBlock];
   __shared__ bool isLast;
-  const DevParams p = *pp;
-  FrameState* fs = b.frame;
+  const RedBlock rb = b.gateTable[blockIdx.x];
+  const SceneRange sr = b.scenes[rb.scene];
+  const DevParams p = pp[rb.scene];
+  FrameState* fs = &b.frames[rb.scene];
   GatePartial acc = gateIdentity();
-  const uint32_t n = T > V ? T : V;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (i < V) {
+  for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
+    if (k < sr.V) {
+      const uint32_t i = sr.vOff + k;
       const float4 o = b.pos[0][i];
       b.old[i] = make_float4(o.x, o.y, o.z, 1.0f);
       const uint4 info = b.vinfo[i];
@@ -816,33 +832,29 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
         b.velocity[i] = make_float4(0, 0, 0, 0);
       }
       b.predicted[i] = make_float4(pred.x, pred.y, pred.z, distributedInertiaWeight(rm, info, p.invDt2));
-      const float3 src = glob ? xyz(o) : pred;
-      b.pos[1][i] = make_float4(src.x, src.y, src.z, 1.0f);
+      // The stable iteration source is the accepted pose.
+      b.pos[1][i] = make_float4(o.x, o.y, o.z, 1.0f);
       b.finalUpdate[i] = 0.0f;
-      if (glob) {
-        // Iteration-0 frames (and, for free vertices, the incident system)
-        // from the accepted pose, the stable iteration source.
-        if (isPinned(info)) storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
-        else frameAndIncident(b, b.pos[0], i, info, p.rotationEpsilon);
-        const float e = implicitEnergy(p, b, i, xyz(o), info);
-        if (finiteS(e)) { acc.e0 += e; acc.e1 += e; }
-        else acc.bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
-      }
+      // Iteration-0 frames (and, for free vertices, the incident system).
+      if (isPinned(info)) storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
+      else frameAndIncident(b, b.pos[0], i, info, p.rotationEpsilon);
+      const float e = implicitEnergy(p, b, i, xyz(o), info);
+      if (finiteS(e)) { acc.e0 += e; acc.e1 += e; }
+      else acc.bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
     }
-    if (glob && i < T) {
-      const TetRec r = loadTet(b.tets, i);
+    if (k < sr.T) {
+      const TetRec r = loadTet(b.tets, sr.tOff + k);
       const M3 F = deformationAt(r, b.pos[0]);
       accumulateTet(acc, r, F, F);
     }
   }
-  if (!glob) return;  // uniform
   const GatePartial blk = blockFold(acc, smem, gateCombine);
   GatePartial* partials = reinterpret_cast<GatePartial*>(b.gatePartials);
-  if (!publishPartial(blk, partials, &fs->prologueTicket, &isLast)) return;
-  const GatePartial tot = foldPartials(partials, smem, gateIdentity, gateCombine);
+  if (!publishPartial(blk, partials, rb.slot, sr.gateBlocks, &fs->prologueTicket, &isLast)) return;
+  const GatePartial tot = foldPartials(partials + sr.gateBase, sr.gateBlocks, smem, gateIdentity, gateCombine);
   if (threadIdx.x != 0) return;
   uint32_t vb = tot.bits;
-  if (T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
+  if (sr.T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
   const bool gv = (vb & kSourceGeometryValid) != 0u;
   const float e0 = float(tot.e0);
   const bool ev = (vb & kSourceEnergyValid) != 0u && finiteS(e0);
@@ -864,20 +876,22 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
 // (assembledVertexEnergy :3489-3496) + reduceCandidate (:3611-3955).
 __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams* __restrict__ pp,
                                                      const float4* __restrict__ src,
-                                                     const float4* __restrict__ tgt, uint32_t V, uint32_t T) {
+                                                     const float4* __restrict__ tgt) {
   __shared__ GatePartial smem[kBlock];
   __shared__ bool isLast;
-  const DevParams p = *pp;
-  FrameState* fs = b.frame;
-  if (latched(p, fs)) return;  // uniform across the grid
+  const RedBlock rb = b.gateTable[blockIdx.x];
+  const SceneRange sr = b.scenes[rb.scene];
+  const DevParams p = pp[rb.scene];
+  FrameState* fs = &b.frames[rb.scene];
+  if (latched(p, fs)) return;  // uniform across the scene's blocks
   GatePartial acc = gateIdentity();
-  const uint32_t n = T > V ? T : V;
-  for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-    if (i < T) {
-      const TetRec r = loadTet(b.tets, i);
+  for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
+    if (k < sr.T) {
+      const TetRec r = loadTet(b.tets, sr.tOff + k);
       accumulateTet(acc, r, deformationAt(r, src), deformationAt(r, tgt));
     }
-    if (i < V) {
+    if (k < sr.V) {
+      const uint32_t i = sr.vOff + k;
       const uint4 info = b.vinfo[i];
       const float es = implicitEnergy(p, b, i, xyz(src[i]), info);
       const float ec = implicitEnergy(p, b, i, xyz(tgt[i]), info);
@@ -887,15 +901,15 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
   }
   const GatePartial blk = blockFold(acc, smem, gateCombine);
   GatePartial* partials = reinterpret_cast<GatePartial*>(b.gatePartials);
-  if (!publishPartial(blk, partials, &fs->gateTicket, &isLast)) return;
-  const GatePartial tot = foldPartials(partials, smem, gateIdentity, gateCombine);
+  if (!publishPartial(blk, partials, rb.slot, sr.gateBlocks, &fs->gateTicket, &isLast)) return;
+  const GatePartial tot = foldPartials(partials + sr.gateBase, sr.gateBlocks, smem, gateIdentity, gateCombine);
   if (threadIdx.x != 0) return;
   uint32_t vb = tot.bits;
   if (__ldcg(&fs->localNumericsValid)) vb |= kLocalNumericsValid;
   const float eS = float(tot.e0), eC = float(tot.e1);
   if (!finiteS(eS)) vb &= ~kSourceEnergyValid;
   if (!finiteS(eC)) vb &= ~kCandidateEnergyValid;
-  if (T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
+  if (sr.T == 0) vb &= ~(kSourceGeometryValid | kCandidateGeometryValid);
   const float sm = tot.minS, cm = tot.minC;
   const bool sgv = (vb & kSourceGeometryValid) != 0u, cgv = (vb & kCandidateGeometryValid) != 0u;
   const bool sev = (vb & kSourceEnergyValid) != 0u, cev = (vb & kCandidateEnergyValid) != 0u;
@@ -933,16 +947,20 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
 // the reference forms the same norms in f32 as scale * sqrt(sum((g/scale)^2)).
 __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const DevParams* __restrict__ pp,
                                                             const float4* __restrict__ src, float4* tgt,
-                                                            uint32_t V, int nextRotations) {
+                                                            int nextRotations) {
   __shared__ ConvPartial smem[kBlock];
   __shared__ bool isLast;
-  const DevParams p = *pp;
-  FrameState* fs = b.frame;
-  if (latched(p, fs)) return;  // uniform across the grid
+  const RedBlock rb = b.convTable[blockIdx.x];
+  const SceneRange sr = b.scenes[rb.scene];
+  const DevParams p = pp[rb.scene];
+  FrameState* fs = &b.frames[rb.scene];
+  if (latched(p, fs)) return;  // uniform across the scene's blocks
   const bool accepted = fs->control[1].x == 1.0f;
   const float4* __restrict__ acc = accepted ? tgt : src;
+  const uint32_t V = sr.V;
   ConvPartial part = convIdentity();
-  for (uint32_t v = blockIdx.x * blockDim.x + threadIdx.x; v < V; v += gridDim.x * blockDim.x) {
+  for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
+    const uint32_t v = sr.vOff + k;
     float upd = 0.0f;
     if (!accepted) {
       tgt[v] = src[v];
@@ -1014,8 +1032,8 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
   }
   const ConvPartial blk = blockFold(part, smem, convCombine);
   ConvPartial* partials = reinterpret_cast<ConvPartial*>(b.convPartials);
-  if (!publishPartial(blk, partials, &fs->convTicket, &isLast)) return;
-  const ConvPartial tot = foldPartials(partials, smem, convIdentity, convCombine);
+  if (!publishPartial(blk, partials, rb.slot, sr.convBlocks, &fs->convTicket, &isLast)) return;
+  const ConvPartial tot = foldPartials(partials + sr.convBase, sr.convBlocks, smem, convIdentity, convCombine);
   if (threadIdx.x != 0) return;
   float norms[5];
   bool cnv = tot.valid != 0u;
@@ -1092,24 +1110,21 @@ __global__ void __launch_bounds__(kBlock) bodyAccumulateKernel(Buffers b, const 
   if (isPinned(info)) atomicAdd(&acc[5], 1.0);
 }
 
+// accumulated: bodyAccumulateKernel ran (and left the final pose in pos[0]).
 __global__ void __launch_bounds__(kBlock) finalizeKernel(Buffers b, const DevParams* __restrict__ pp,
-                                                         const float4* __restrict__ finalPos, uint32_t V, int glob,
-                                                         int bodyCorrection) {
+                                                         const float4* __restrict__ finalPos, uint32_t V,
+                                                         int accumulated) {
   const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
   if (v >= V) return;
-  const DevParams p = *pp;
+  const DevParams& p = pp[b.vertexScene[v]];
   const uint4 info = b.vinfo[v];
-  float4 x = bodyCorrection ? b.pos[0][v] : finalPos[v];
+  float4 x = accumulated ? b.pos[0][v] : finalPos[v];
   if (isPinned(info)) {
-    if (!glob) {
-      const float4 rm = b.restMass[v];
-      x = make_float4(rm.x, rm.y, rm.z, 1.0f);
-    }
     b.pos[0][v] = make_float4(x.x, x.y, x.z, 1.0f);
     b.velocity[v] = make_float4(0, 0, 0, 0);
     return;
   }
-  if (bodyCorrection && info.w < p.bodyCount) {
+  if (accumulated && p.bodyCorrection) {
     const double* acc = &b.bodyAccum[6ull * info.w];
     if (acc[5] == 0.0 && acc[0] > 0.0) {
       x.x += float((acc[3] - acc[1]) / acc[0]);
@@ -1163,8 +1178,8 @@ __global__ void __launch_bounds__(kBlock) gateScratchKernel(Buffers b, DevParams
     if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
   }
   const GatePartial blk = blockFold(acc, smem, gateCombine);
-  if (!publishPartial(blk, partials, ticket, &isLast)) return;
-  const GatePartial tot = foldPartials(partials, smem, gateIdentity, gateCombine);
+  if (!publishPartial(blk, partials, blockIdx.x, gridDim.x, ticket, &isLast)) return;
+  const GatePartial tot = foldPartials(partials, gridDim.x, smem, gateIdentity, gateCombine);
   if (threadIdx.x != 0) return;
   uint32_t vb = tot.bits | kLocalNumericsValid;
   const float eS = float(tot.e0), eC = float(tot.e1);
@@ -1202,15 +1217,8 @@ uint32_t smCount() {
   return static_cast<uint32_t>(sms);
 }
 
-uint32_t gateBlockCount(uint32_t V, uint32_t T) {
-  const uint32_t n = T > V ? T : V;
-  return std::max(1u, std::min(blocksFor(n), smCount() * 8u));
-}
-
-uint32_t convBlockCount(uint32_t V) { return std::max(1u, std::min(blocksFor(V), smCount() * 8u)); }
-
-int launchPrologue(const Buffers& b, const DevParams* p, uint32_t V, uint32_t T, bool glob, cudaStream_t s) {
-  prologueKernel<<<b.gateBlocks, kBlock, 0, s>>>(b, p, V, T, glob ? 1 : 0);
+int launchPrologue(const Buffers& b, const DevParams* p, cudaStream_t s) {
+  prologueKernel<<<b.gateBlocks, kBlock, 0, s>>>(b, p);
   return 1;
 }
 
@@ -1221,15 +1229,8 @@ int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, c
   return 1;
 }
 
-int launchTetPolar(const Buffers& b, const DevParams* p, const float4* src, uint32_t T, cudaStream_t s) {
-  if (T == 0) return 0;
-  tetPolarKernel<<<blocksFor(T), kBlock, 0, s>>>(b, p, src, T);
-  return 1;
-}
-
 int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
-                uint32_t count, uint32_t K, bool glob, bool cachedIncident, cudaStream_t s) {
-  (void)glob;
+                uint32_t count, uint32_t K, bool cachedIncident, cudaStream_t s) {
   if (count == 0) return 0;
   const uint32_t groups = solveGroupsPerBlock(K);
   if (groups == 0) return 0;
@@ -1265,27 +1266,26 @@ int launchCopy(const float4* src, float4* dst, uint32_t V, cudaStream_t s) {
   return 1;
 }
 
-int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V, uint32_t T,
-               cudaStream_t s) {
-  gateKernel<<<b.gateBlocks, kBlock, 0, s>>>(b, p, src, tgt, V, T);
+int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s) {
+  gateKernel<<<b.gateBlocks, kBlock, 0, s>>>(b, p, src, tgt);
   return 1;
 }
 
-int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, uint32_t V,
+int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt,
                       bool computeNextRotations, cudaStream_t s) {
-  convergenceKernel<<<b.convBlocks, kBlock, 0, s>>>(b, p, src, tgt, V, computeNextRotations ? 1 : 0);
+  convergenceKernel<<<b.convBlocks, kBlock, 0, s>>>(b, p, src, tgt, computeNextRotations ? 1 : 0);
   return 1;
 }
 
-int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool glob,
-                   bool bodyCorrection, uint32_t bodies, cudaStream_t s) {
+int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool bodyCorrection,
+                   uint32_t bodies, cudaStream_t s) {
   int n = 0;
   if (bodyCorrection) {
     cudaMemsetAsync(b.bodyAccum, 0, sizeof(double) * 6ull * bodies, s);
     bodyAccumulateKernel<<<blocksFor(V), kBlock, 0, s>>>(b, finalPos, V);
     ++n;
   }
-  finalizeKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, finalPos, V, glob ? 1 : 0, bodyCorrection ? 1 : 0);
+  finalizeKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, finalPos, V, bodyCorrection ? 1 : 0);
   return n + 1;
 }
 

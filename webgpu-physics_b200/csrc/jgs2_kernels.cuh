@@ -23,7 +23,26 @@ struct DevParams {
   uint32_t globalization;   // stable Neo-Hookean path
   uint32_t historyCapacity;
   uint32_t vertexCount, tetCount, cubatureK, bodyCount;
+  uint32_t bodyCorrection;  // horizontal body correction in the epilogue
+  uint32_t pad[3];
 };
+
+// One scene of a batch: its slices of the concatenated vertex and tet arrays
+// and its slots in the reduction partial arrays.  A single solver is a batch
+// of one scene.
+struct SceneRange {
+  uint32_t vOff, V, tOff, T;
+  uint32_t gateBase, gateBlocks;  // prologue / gate partials of this scene
+  uint32_t convBase, convBlocks;  // convergence partials of this scene
+};
+
+// One block of a segmented reduction: elements [begin, end) of `scene`,
+// publishing its partial at index `slot`.
+struct RedBlock {
+  uint32_t scene, begin, end, slot;
+};
+constexpr uint32_t kGateChunk = 2048;  // tets / vertices per prologue or gate block
+constexpr uint32_t kConvChunk = 1024;  // vertices per convergence block
 
 // Reduction scratch and the GPU-resident control/history records
 // (dynamic arena regions globalizationControl/globalizationHistory,
@@ -31,22 +50,14 @@ struct DevParams {
 struct FrameState {
   float4 control[4];
   float4 history[64 * 8];
-  // Gate reduction (candidateTetrahedron + reduceCandidate).
-  uint32_t gateTicket;
-  uint32_t gateMinSource, gateMinCandidate;  // order-preserving float encodings
-  uint32_t gateBits;                          // AND of validity bits
+  // Tickets of the segmented reductions (the last block of the scene folds).
+  uint32_t gateTicket, convTicket, prologueTicket;
   // Local diagnostics aggregates of the current sweep (reduceCandidate's
   // vertex loop), accumulated by the solve kernel with order-free atomics.
   uint32_t localFailures, localMaxBacktracks, localSkipped, localEvaluations;
   uint32_t localMaxShift;  // float bits of a non-negative value
   uint32_t localNumericsValid;
-  // Convergence reduction.
-  uint32_t convTicket;
-  uint32_t convScale[6];    // float bits (non-negative maxima)
-  uint32_t convMaxUpdate;   // float bits
-  uint32_t convValid;
-  uint32_t prologueTicket;
-  uint32_t pad[2];
+  uint32_t pad[7];
 };
 
 // All device arrays of one solver.
@@ -64,7 +75,7 @@ struct Buffers {
   // Jacobi source pose, (g.xyz, Hxx) (Hyy, Hzz, Hxy, Hxz) (Hyz, 0, 0, 0),
   // written by the pass that computes that pose's vertex frames.
   float4* incident;
-  FrameState* frame;
+  FrameState* frames;     // one per scene
   void* gatePartials;     // one GatePartial (32 bytes) per gate / prologue block
   void* convPartials;     // one ConvPartial (80 bytes) per convergence block
   double* bodyAccum;      // 6 per body (mass, solved xz, predicted xz, pinned count)
@@ -79,33 +90,33 @@ struct Buffers {
   float4* forces;             // external force xyz per vertex
   float4* targets;            // quadratic target xyz, stiffness per vertex
   const uint32_t* colors;     // per vertex colour
-  uint32_t gateBlocks, convBlocks;
+  const uint32_t* vertexScene;  // scene of each vertex
+  const SceneRange* scenes;
+  const RedBlock* gateTable;    // prologue / gate blocks
+  const RedBlock* convTable;    // convergence blocks
+  uint32_t gateBlocks, convBlocks, sceneCount, pad;
 };
 
-// Kernel launch entry points (jgs2_kernels.cu).  Every launcher returns the
-// number of kernels it launched.
-int launchPrologue(const Buffers& b, const DevParams* p, uint32_t V, uint32_t T, bool glob, cudaStream_t s);
+// Kernel launch entry points (jgs2_kernels.cu).  `p` points at one DevParams
+// per scene.  Every launcher returns the number of kernels it launched.
+int launchPrologue(const Buffers& b, const DevParams* p, cudaStream_t s);
 int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, const uint32_t* list,
                       uint32_t count, cudaStream_t s);
-int launchTetPolar(const Buffers& b, const DevParams* p, const float4* src, uint32_t T, cudaStream_t s);
 // cachedIncident: take the incident-tet gradient and Hessian of each vertex
 // from Buffers::incident (valid for a Jacobi source pose) instead of
 // gathering them.
 int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
-                uint32_t count, uint32_t K, bool glob, bool cachedIncident, cudaStream_t s);
+                uint32_t count, uint32_t K, bool cachedIncident, cudaStream_t s);
 int launchCopy(const float4* src, float4* dst, uint32_t V, cudaStream_t s);
-int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V, uint32_t T,
-               cudaStream_t s);
-int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, uint32_t V,
+int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s);
+int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt,
                       bool computeNextRotations, cudaStream_t s);
-int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool glob,
-                   bool bodyCorrection, uint32_t bodies, cudaStream_t s);
+// bodyCorrection: some scene of the batch corrects its bodies this frame.
+int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool bodyCorrection,
+                   uint32_t bodies, cudaStream_t s);
 
 // Vertices per solve block for cubature width K (0: K too large to cache).
 uint32_t solveGroupsPerBlock(uint32_t K);
-// Persistent grid sizes (a few blocks per SM) of the reduction kernels.
-uint32_t gateBlockCount(uint32_t V, uint32_t T);
-uint32_t convBlockCount(uint32_t V);
 constexpr size_t kGatePartialBytes = 32;
 constexpr size_t kConvPartialBytes = 80;
 

@@ -410,26 +410,44 @@ double minimumInputDeterminant(const jgs2_input* in) {
 
 }  // namespace
 
-// ---- solver -------------------------------------------------------------------
+// ---- engine -------------------------------------------------------------------
+//
+// One engine steps one or more independent scenes together: their vertex, tet
+// and cubature arrays are concatenated in device memory, every kernel looks up
+// the scene of the element it works on, and the gate / convergence reductions
+// are segmented per scene.  `jgs2_solver` is an engine of one scene (the
+// reference's JGS2GpuSolver); `jgs2_batch` is an engine of many.
 
-struct jgs2_solver {
-  int device = 0;
-  cudaStream_t stream = nullptr;
-  bool destroyed = false;
-  std::string error;
-  uint32_t V = 0, T = 0, K = 0, bodies = 1;
-  bool glob = true;
+namespace {
+
+// Host state of one scene.
+struct SceneHost {
+  uint32_t V = 0, T = 0, K = 0, vOff = 0, tOff = 0, bodyOff = 0, bodies = 1;
   float sceneScale = 1.f;
   float preprocessingTimestep = 0.f;
   jgs2_settings defaults{};
   jgs2_settings submitted{};
   uint32_t submittedIterations = 0;
   bool recordsAvailable = false;
-  // colouring
   uint32_t colorCount = 1;
-  std::vector<uint32_t> colors;
-  std::vector<uint32_t> colorOffsets;   // colorCount + 1 into colorVertices
-  std::vector<uint32_t> needOffsets;    // colorCount + 1 into needVertices
+  std::vector<uint32_t> colors;  // scene-local colouring
+  uint32_t objectiveFlags = 0, forceCount = 0, targetCount = 0, objectiveRevision = 0;
+};
+
+}  // namespace
+
+struct Engine {
+  int device = 0;
+  cudaStream_t stream = nullptr;
+  bool destroyed = false;
+  std::string error;
+  uint32_t V = 0, T = 0, K = 0, bodies = 1;  // totals over the scenes; K = widest record count
+  bool glob = true;
+  std::vector<SceneHost> scenes;
+  // Colour lists over all scenes: colour c holds every scene's colour-c vertices.
+  uint32_t colorCount = 1;
+  std::vector<uint32_t> colorOffsets;  // colorCount + 1 into colorVertices
+  std::vector<uint32_t> needOffsets;   // colorCount + 1 into needVertices
   // Objectives: pinned host mirrors of the device force and target arrays
   // (force xyz, 0) and (target xyz, stiffness); uploads copy from them.
   float4* hForces = nullptr;
@@ -437,10 +455,10 @@ struct jgs2_solver {
   cudaEvent_t objectiveUpload = nullptr;  // recorded after the last upload
   bool objectiveUploadPending = false;
   std::vector<uint8_t> pinned;
-  uint32_t objectiveFlags = 0, forceCount = 0, targetCount = 0, objectiveRevision = 0;
   // device
   Buffers b{};
-  DevParams* dParams = nullptr;
+  DevParams* dParams = nullptr;  // one per scene
+  std::vector<DevParams> hParams;
   uint32_t* dColorVertices = nullptr;
   uint32_t* dNeedVertices = nullptr;
   std::vector<void*> allocations;
@@ -450,15 +468,18 @@ struct jgs2_solver {
   bool useGraphs = true;
 };
 
+struct jgs2_solver : Engine {};
+struct jgs2_batch : Engine {};
+
 namespace {
 
-jgs2_status fail(jgs2_solver* s, jgs2_status st, const std::string& msg) {
+jgs2_status fail(Engine* s, jgs2_status st, const std::string& msg) {
   if (s) s->error = msg;
   else gGlobalError = msg;
   return st;
 }
 
-jgs2_status cudaFail(jgs2_solver* s, cudaError_t e, const char* what) {
+jgs2_status cudaFail(Engine* s, cudaError_t e, const char* what) {
   return fail(s, e == cudaErrorMemoryAllocation ? JGS2_OUT_OF_MEMORY : JGS2_DEVICE_ERROR,
               format("%s: %s", what, cudaGetErrorString(e)));
 }
@@ -470,7 +491,7 @@ jgs2_status cudaFail(jgs2_solver* s, cudaError_t e, const char* what) {
   } while (0)
 
 template <class T>
-jgs2_status deviceAlloc(jgs2_solver* s, T** out, size_t count) {
+jgs2_status deviceAlloc(Engine* s, T** out, size_t count) {
   void* p = nullptr;
   const size_t bytes = std::max<size_t>(16, count * sizeof(T));
   cudaError_t e = cudaMalloc(&p, bytes);
@@ -481,14 +502,14 @@ jgs2_status deviceAlloc(jgs2_solver* s, T** out, size_t count) {
 }
 
 template <class T>
-jgs2_status upload(jgs2_solver* s, T** out, const T* host, size_t count) {
+jgs2_status upload(Engine* s, T** out, const T* host, size_t count) {
   jgs2_status st = deviceAlloc(s, out, count);
   if (st != JGS2_OK) return st;
   if (count) CUDA_TRY(s, cudaMemcpyAsync(*out, host, count * sizeof(T), cudaMemcpyHostToDevice, s->stream));
   return JGS2_OK;
 }
 
-void releaseDevice(jgs2_solver* s) {
+void releaseDevice(Engine* s) {
   for (auto& kv : s->graphs) cudaGraphExecDestroy(kv.second.first);
   s->graphs.clear();
   if (s->stream) cudaStreamSynchronize(s->stream);
@@ -505,12 +526,12 @@ void releaseDevice(jgs2_solver* s) {
 
 bool forceActive(const float4& f) { return f.x != 0 || f.y != 0 || f.z != 0; }
 
-void refreshObjectiveFlags(jgs2_solver* s) {
-  s->objectiveFlags = (s->forceCount ? 1u : 0u) | (s->targetCount ? 2u : 0u);
+void refreshObjectiveFlags(SceneHost& sc) {
+  sc.objectiveFlags = (sc.forceCount ? 1u : 0u) | (sc.targetCount ? 2u : 0u);
 }
 
-
-DevParams makeParams(const jgs2_solver* s, const jgs2_settings& st, bool stop) {
+DevParams makeParams(const Engine* s, uint32_t scene, const jgs2_settings& st, bool stop) {
+  const SceneHost& sc = s->scenes[scene];
   DevParams p{};
   // packUniforms (jgs2-solver.ts:604-730): (dt, 1/dt, 1/dt^2) formed in
   // double from the timestep and stored as f32.
@@ -530,19 +551,19 @@ DevParams makeParams(const jgs2_solver* s, const jgs2_settings& st, bool stop) {
   p.contactMargin = st.contact_margin;
   p.residualTolerance = st.residual_tolerance;
   p.normalizedUpdateTolerance = st.normalized_update_tolerance;
-  p.sceneScale = s->sceneScale;
-  p.objectiveFlags = s->objectiveFlags;
+  p.sceneScale = sc.sceneScale;
+  p.objectiveFlags = sc.objectiveFlags;
   p.stopEnabled = (s->glob && stop) ? 1u : 0u;
   p.globalization = s->glob ? 1u : 0u;
   p.historyCapacity = JGS2_HISTORY_CAPACITY;
-  p.vertexCount = s->V;
-  p.tetCount = s->T;
-  p.cubatureK = s->K;
-  p.bodyCount = s->bodies;
+  p.vertexCount = sc.V;
+  p.tetCount = sc.T;
+  p.cubatureK = sc.K;
+  p.bodyCount = sc.bodies;
+  p.bodyCorrection = st.horizontal_body_correction ? 1u : 0u;
   return p;
 }
 
-// encodeFrame (src/simulation/gpu/jgs2-solver.ts:2207-2494) on the stream.
 // Optional per-kernel CUDA event timing of an encoded frame.
 struct KernelProfiler {
   static constexpr const char* kNames[JGS2_PROFILE_KINDS] = {"prologue", "vertex_frames", "tet_frames", "solve",
@@ -570,8 +591,9 @@ struct KernelProfiler {
   }
 };
 
-// encodeFrame (src/simulation/gpu/jgs2-solver.ts:2207-2494) on the stream.
-int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bodyCorrection,
+// encodeFrame (src/simulation/gpu/jgs2-solver.ts:2207-2494) on the stream,
+// for every scene of the engine at once.
+int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorrection,
                 KernelProfiler* prof = nullptr) {
   const Buffers& b = s->b;
   cudaStream_t st = s->stream;
@@ -585,9 +607,7 @@ int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bod
   };
   using P = KernelProfiler;
   int n = 0;
-  n += timed(P::kPrologue, [&] { return jgs2::launchPrologue(b, s->dParams, s->V, s->T, s->glob, st); });
-  if (!s->glob)
-    n += timed(P::kVertexFrames, [&] { return jgs2::launchVertexPolar(b, s->dParams, b.pos[1], nullptr, s->V, st); });
+  n += timed(P::kPrologue, [&] { return jgs2::launchPrologue(b, s->dParams, st); });
   const bool colored = schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL;
   for (uint32_t it = 0; it < iterations; ++it) {
     float4* src = (it % 2 == 0) ? b.pos[1] : b.pos[0];
@@ -596,7 +616,6 @@ int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bod
     if (colored) {
       n += timed(P::kCopy, [&] { return jgs2::launchCopy(src, tgt, s->V, st); });
       for (uint32_t c = 0; c < s->colorCount; ++c) {
-        if (!s->glob) n += timed(P::kTetFrames, [&] { return jgs2::launchTetPolar(b, s->dParams, tgt, s->T, st); });
         const uint32_t nb = s->needOffsets[c], ne = s->needOffsets[c + 1];
         n += timed(P::kVertexFrames, [&] {
           // The final colour of the frame refreshes every frame so the stored
@@ -606,60 +625,56 @@ int encodeFrame(jgs2_solver* s, uint32_t iterations, uint32_t schedule, bool bod
         });
         const uint32_t cb = s->colorOffsets[c], ce = s->colorOffsets[c + 1];
         n += timed(P::kSolve, [&] {
-          return jgs2::launchSolve(b, s->dParams, tgt, tgt, s->dColorVertices + cb, ce - cb, s->K, s->glob, false,
-                                   st);
+          return jgs2::launchSolve(b, s->dParams, tgt, tgt, s->dColorVertices + cb, ce - cb, s->K, false, st);
         });
       }
     } else {
-      if (!s->glob) {
-        n += timed(P::kTetFrames, [&] { return jgs2::launchTetPolar(b, s->dParams, src, s->T, st); });
-        if (it > 0)
-          n += timed(P::kVertexFrames, [&] { return jgs2::launchVertexPolar(b, s->dParams, src, nullptr, s->V, st); });
-      }
       // Stable Jacobi: the prologue (iteration 0) and the previous iteration's
       // convergence pass leave the source pose's incident system in b.incident.
-      n += timed(P::kSolve, [&] {
-        return jgs2::launchSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, s->glob, s->glob, st);
-      });
+      n += timed(P::kSolve, [&] { return jgs2::launchSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, true, st); });
     }
-    if (s->glob) {
-      n += timed(P::kGate, [&] { return jgs2::launchGate(b, s->dParams, src, tgt, s->V, s->T, st); });
-      n += timed(P::kConvergence,
-                 [&] { return jgs2::launchConvergence(b, s->dParams, src, tgt, s->V, !colored && !last, st); });
-    }
+    n += timed(P::kGate, [&] { return jgs2::launchGate(b, s->dParams, src, tgt, st); });
+    n += timed(P::kConvergence,
+               [&] { return jgs2::launchConvergence(b, s->dParams, src, tgt, !colored && !last, st); });
   }
   const float4* finalPos = (iterations % 2 == 0) ? b.pos[1] : b.pos[0];
-  n += timed(P::kEpilogue, [&] {
-    return jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, s->glob, bodyCorrection, s->bodies, st);
-  });
+  n += timed(P::kEpilogue,
+             [&] { return jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, bodyCorrection, s->bodies, st); });
   return n;
 }
 
-jgs2_status runFrames(jgs2_solver* s, const jgs2_settings& st, uint32_t frames, uint32_t iterations, bool stop,
-                      KernelProfiler* prof = nullptr) {
-  if (s->glob && iterations > JGS2_HISTORY_CAPACITY)
+// Encodes `frames` frames of `iterations` iterations for every scene with its
+// resolved settings (one per scene; the schedule must agree).
+jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t frames, uint32_t iterations,
+                      bool stop, KernelProfiler* prof = nullptr) {
+  if (iterations > JGS2_HISTORY_CAPACITY)
     return fail(s, JGS2_INVALID_ARGUMENT,
                 format("Stable JGS2 records at most %u nonlinear iterations per frame; got %u.",
                        JGS2_HISTORY_CAPACITY, iterations));
-  if (s->glob) {
-    const uint32_t sub = st.schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL ? s->colorCount : 1u;
-    if (static_cast<uint64_t>(iterations) * sub > JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION / frames)
-      return fail(s, JGS2_INVALID_ARGUMENT,
-                  format("Stable JGS2 may encode at most %u total nonlinear iterations per submission; got %u "
-                         "frames * %u iterations.",
-                         JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION, frames, iterations * sub));
+  const uint32_t schedule = st[0].schedule;
+  bool body = false;
+  for (size_t i = 0; i < st.size(); ++i) {
+    if (st[i].schedule != schedule)
+      return fail(s, JGS2_INVALID_ARGUMENT, "All scenes of one batched step must use the same schedule.");
+    body = body || st[i].horizontal_body_correction != 0;
   }
-  const DevParams p = makeParams(s, st, stop);
+  const uint32_t sub = schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL ? s->colorCount : 1u;
+  if (static_cast<uint64_t>(iterations) * sub > JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION / frames)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("Stable JGS2 may encode at most %u total nonlinear iterations per submission; got %u "
+                       "frames * %u iterations.",
+                       JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION, frames, iterations * sub));
+  for (uint32_t i = 0; i < s->scenes.size(); ++i) s->hParams[i] = makeParams(s, i, st[i], stop);
   CUDA_TRY(s, cudaSetDevice(s->device));
-  CUDA_TRY(s, cudaMemcpyAsync(s->dParams, &p, sizeof(p), cudaMemcpyHostToDevice, s->stream));
-  const bool body = st.horizontal_body_correction != 0;
-  const auto key = std::make_tuple(iterations, st.schedule, body);
+  CUDA_TRY(s, cudaMemcpyAsync(s->dParams, s->hParams.data(), sizeof(DevParams) * s->hParams.size(),
+                              cudaMemcpyHostToDevice, s->stream));
+  const auto key = std::make_tuple(iterations, schedule, body);
   if (s->useGraphs && !prof) {
     auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
       cudaGraph_t graph = nullptr;
       CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-      const int n = encodeFrame(s, iterations, st.schedule, body);
+      const int n = encodeFrame(s, iterations, schedule, body);
       cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
       if (e != cudaSuccess) return cudaFail(s, e, "cudaStreamEndCapture");
       cudaGraphExec_t exec = nullptr;
@@ -673,18 +688,40 @@ jgs2_status runFrames(jgs2_solver* s, const jgs2_settings& st, uint32_t frames, 
       s->launches += static_cast<uint64_t>(it->second.second);
     }
   } else {
-    for (uint32_t f = 0; f < frames; ++f) s->launches += encodeFrame(s, iterations, st.schedule, body, prof);
+    for (uint32_t f = 0; f < frames; ++f) s->launches += encodeFrame(s, iterations, schedule, body, prof);
   }
   CUDA_TRY(s, cudaGetLastError());
-  s->submitted = st;
-  s->submittedIterations = iterations;
-  if (s->glob) s->recordsAvailable = true;
+  for (uint32_t i = 0; i < s->scenes.size(); ++i) {
+    s->scenes[i].submitted = st[i];
+    s->scenes[i].submittedIterations = iterations;
+    s->scenes[i].recordsAvailable = true;
+  }
   return JGS2_OK;
 }
 
 uint32_t normalizeOdd(uint32_t it) {
   const uint32_t i = std::max(1u, it);
   return i % 2 == 0 ? i + 1 : i;
+}
+
+jgs2_status usable(Engine* s) {
+  if (!s) return fail(nullptr, JGS2_INVALID_ARGUMENT, "solver is NULL.");
+  if (s->destroyed) return fail(s, JGS2_DESTROYED, "JGS2GpuSolver has been destroyed.");
+  return JGS2_OK;
+}
+
+// resolveStepSettings (jgs2-solver.ts:1974-2005) for one scene.
+jgs2_status resolveStep(Engine* s, uint32_t scene, const jgs2_settings* o, uint32_t mask, jgs2_settings* out) {
+  const SceneHost& sc = s->scenes[scene];
+  if (o && (mask & JGS2_SET_TIMESTEP) && static_cast<float>(o->timestep) != sc.preprocessingTimestep)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("JGS2 was precomputed for timestep %g, but the step requested %g. Regenerate the "
+                       "precomputation before changing timestep.",
+                       sc.preprocessingTimestep, o->timestep));
+  std::string err;
+  if (!resolve(sc.defaults, o, mask, out, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
+  if (s->glob && sc.objectiveFlags != 0 && out->horizontal_body_correction) out->horizontal_body_correction = 0;
+  return JGS2_OK;
 }
 
 jgs2_status stepCommon(jgs2_solver* s, uint32_t frames, int exactIterations, const jgs2_settings* o,
@@ -696,58 +733,491 @@ jgs2_status stepCommon(jgs2_solver* s, uint32_t frames, int exactIterations, con
                 format("frameCount must be a positive safe integer no greater than %u; got %u.",
                        JGS2_MAX_BATCH_FRAMES, frames));
   if (exactIterations == 0) return fail(s, JGS2_INVALID_ARGUMENT, "iterations must be a positive safe integer; got 0.");
-  if (o && (mask & JGS2_SET_TIMESTEP) && static_cast<float>(o->timestep) != s->preprocessingTimestep)
-    return fail(s, JGS2_INVALID_ARGUMENT,
-                format("JGS2 was precomputed for timestep %g, but the step requested %g. Regenerate the "
-                       "precomputation before changing timestep.",
-                       s->preprocessingTimestep, o->timestep));
-  // resolveStepSettings (jgs2-solver.ts:1974-2005).
-  if (o && (mask & JGS2_SET_IPC_MINIMUM_DISTANCE) && o->ipc_minimum_distance != s->defaults.ipc_minimum_distance &&
-      false /* no IPC candidates in this build */)
-    return fail(s, JGS2_INVALID_ARGUMENT, "ipcMinimumDistance is fixed when an IPC solver is created.");
-  jgs2_settings st;
-  std::string err;
-  if (!resolve(s->defaults, o, mask, &st, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
-  if (s->glob && s->objectiveFlags != 0 && st.horizontal_body_correction) st.horizontal_body_correction = 0;
+  std::vector<jgs2_settings> st(1);
+  const jgs2_status rs = resolveStep(s, 0, o, mask, &st[0]);
+  if (rs != JGS2_OK) return rs;
   const bool production = exactIterations < 0;
-  const uint32_t iterations = production ? normalizeOdd(st.iterations) : static_cast<uint32_t>(exactIterations);
+  const uint32_t iterations = production ? normalizeOdd(st[0].iterations) : static_cast<uint32_t>(exactIterations);
   return runFrames(s, st, frames, iterations, production, prof);
 }
 
-jgs2_status readRegion(jgs2_solver* s, const void* dev, size_t bytes, void* host) {
+jgs2_status readRegion(Engine* s, const void* dev, size_t bytes, void* host) {
   CUDA_TRY(s, cudaSetDevice(s->device));
   CUDA_TRY(s, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s->stream));
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return JGS2_OK;
 }
 
-jgs2_status usable(jgs2_solver* s) {
-  if (!s) return fail(nullptr, JGS2_INVALID_ARGUMENT, "solver is NULL.");
-  if (s->destroyed) return fail(s, JGS2_DESTROYED, "JGS2GpuSolver has been destroyed.");
-  return JGS2_OK;
-}
-
 // The host mirrors may change only after the previous upload from them has
 // been consumed by the copy engine.
-jgs2_status waitObjectiveMirror(jgs2_solver* s) {
+jgs2_status waitObjectiveMirror(Engine* s) {
   if (!s->objectiveUploadPending) return JGS2_OK;
   CUDA_TRY(s, cudaEventSynchronize(s->objectiveUpload));
   s->objectiveUploadPending = false;
   return JGS2_OK;
 }
 
-jgs2_status writeObjectives(jgs2_solver* s, uint32_t firstVertex, uint32_t vertexCount, bool forces, bool targets) {
+jgs2_status writeObjectives(Engine* s, uint32_t scene, uint32_t firstVertex, uint32_t vertexCount, bool forces,
+                            bool targets) {
   CUDA_TRY(s, cudaSetDevice(s->device));
   if (forces)
-    CUDA_TRY(s, cudaMemcpyAsync(s->b.forces + firstVertex, s->hForces + firstVertex,
-                                sizeof(float4) * vertexCount, cudaMemcpyHostToDevice, s->stream));
+    CUDA_TRY(s, cudaMemcpyAsync(s->b.forces + firstVertex, s->hForces + firstVertex, sizeof(float4) * vertexCount,
+                                cudaMemcpyHostToDevice, s->stream));
   if (targets)
     CUDA_TRY(s, cudaMemcpyAsync(s->b.targets + firstVertex, s->hTargets + firstVertex,
                                 sizeof(float4) * vertexCount, cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(s, cudaEventRecord(s->objectiveUpload, s->stream));
   s->objectiveUploadPending = true;
-  refreshObjectiveFlags(s);
-  s->objectiveRevision += 1;
+  SceneHost& sc = s->scenes[scene];
+  refreshObjectiveFlags(sc);
+  sc.objectiveRevision += 1;
+  return JGS2_OK;
+}
+
+// ---- engine construction -------------------------------------------------------
+
+// Host-side checks and derived data of one scene input (create, :971-1083).
+struct PreparedScene {
+  const jgs2_input* in = nullptr;
+  jgs2_settings resolved{};
+  uint32_t colorCount = 0;
+  std::vector<uint32_t> colors;
+};
+
+jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, uint32_t mask, PreparedScene* out) {
+  std::string err;
+  if (!validateInput(in, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  // inferJGS2MaterialMode (layout.ts:509-522).
+  uint32_t stable = 0;
+  for (uint32_t t = 0; t < in->tet_count; ++t) stable += in->tet_meta[4ull * t + 3] == 1.0f ? 1u : 0u;
+  if (stable != 0 && stable != in->tet_count)
+    return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                "A production JGS2 solve cannot mix stable Neo-Hookean and co-rotated regression tetrahedra in one "
+                "precomputation.");
+  if (stable != in->tet_count)
+    return fail(nullptr, JGS2_UNSUPPORTED,
+                "The co-rotated regression material path is not built into this library; use stable Neo-Hookean "
+                "tetrahedra.");
+  out->in = in;
+  out->colors = colorInput(in, &out->colorCount);
+  if (out->colorCount > JGS2_MAX_SCHEDULE_COLORS)
+    return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                format("Colored Gauss-Seidel supports at most %u colors; the small-scene conflict graph needs %u.",
+                       JGS2_MAX_SCHEDULE_COLORS, out->colorCount));
+  jgs2_settings base;
+  defaults(&base);
+  if (!resolve(base, settings, mask, &out->resolved, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  const double m = minimumInputDeterminant(in);
+  if (!std::isfinite(m) || !(m > kDeterminantFloor))
+    return fail(nullptr, JGS2_INFEASIBLE_INPUT,
+                format("A stable Neo-Hookean production solve requires an initially feasible pose with minimum J "
+                       "greater than %g; got %g.", kDeterminantFloor, m));
+  return JGS2_OK;
+}
+
+// computeJGS2InitialDynamicSceneScale (jgs2-solver.ts:732-768).
+float initialSceneScale(const jgs2_input* in) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  uint32_t dyn = 0;
+  for (uint32_t v = 0; v < in->vertex_count; ++v) {
+    if (in->vertex_info[4ull * v + 2] != 0) continue;
+    dyn++;
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], static_cast<double>(in->positions[4ull * v + k]));
+      hi[k] = std::max(hi[k], static_cast<double>(in->positions[4ull * v + k]));
+    }
+  }
+  const double d = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                             (hi[2] - lo[2]) * (hi[2] - lo[2]));
+  return static_cast<float>(dyn > 0 && std::isfinite(d) && d > 0 ? d : kDegenerateSceneScale);
+}
+
+// Concatenates the scenes into one device arena, builds the reduction block
+// tables and runs the GPU preflight of every scene's initial pose.
+jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int device) {
+  const uint32_t S = static_cast<uint32_t>(prep.size());
+  sp->device = device;
+  // JGS2_NO_GRAPHS=1 launches each frame's kernels directly (debugging).
+  sp->useGraphs = std::getenv("JGS2_NO_GRAPHS") == nullptr;
+  sp->glob = true;
+  sp->scenes.resize(S);
+  uint64_t V = 0, T = 0, bodies = 0;
+  uint32_t K = 0, colorCount = 1;
+  for (uint32_t i = 0; i < S; ++i) {
+    const jgs2_input* in = prep[i].in;
+    SceneHost& sc = sp->scenes[i];
+    sc.V = in->vertex_count;
+    sc.T = in->tet_count;
+    sc.K = in->cubature_k;
+    sc.vOff = static_cast<uint32_t>(V);
+    sc.tOff = static_cast<uint32_t>(T);
+    sc.bodyOff = static_cast<uint32_t>(bodies);
+    uint32_t maxBody = 0;
+    for (uint32_t v = 0; v < sc.V; ++v) maxBody = std::max(maxBody, in->vertex_info[4ull * v + 3]);
+    sc.bodies = maxBody + 1;
+    sc.defaults = prep[i].resolved;
+    sc.submitted = prep[i].resolved;
+    sc.preprocessingTimestep = prep[i].resolved.timestep;
+    sc.colors = prep[i].colors;
+    sc.colorCount = prep[i].colorCount;
+    sc.sceneScale = initialSceneScale(in);
+    V += sc.V;
+    T += sc.T;
+    bodies += sc.bodies;
+    K = std::max(K, sc.K);
+    colorCount = std::max(colorCount, sc.colorCount);
+  }
+  if (V > 0xffffffffull / 16 || T > 0xffffffffull / 16)
+    return fail(nullptr, JGS2_INVALID_ARGUMENT, "The scenes together exceed the engine's index range.");
+  sp->V = static_cast<uint32_t>(V);
+  sp->T = static_cast<uint32_t>(T);
+  sp->K = K;
+  sp->bodies = static_cast<uint32_t>(bodies);
+  sp->colorCount = colorCount;
+  const uint32_t nV = sp->V, nT = sp->T;
+
+  // Objectives (packJGS2VertexObjectives, layout.ts:635-668).
+  std::vector<float4> initialForces(nV), initialTargets(nV);
+  sp->pinned.assign(nV, 0);
+  for (uint32_t i = 0; i < S; ++i) {
+    const jgs2_input* in = prep[i].in;
+    SceneHost& sc = sp->scenes[i];
+    sc.forceCount = sc.targetCount = 0;
+    for (uint32_t v = 0; v < sc.V; ++v) {
+      const uint32_t g = sc.vOff + v;
+      const float* f = in->external_forces ? &in->external_forces[3ull * v] : nullptr;
+      initialForces[g] = f ? make_float4(f[0], f[1], f[2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
+      const float* tp = in->target_positions ? &in->target_positions[3ull * v] : &in->positions[4ull * v];
+      initialTargets[g] = make_float4(tp[0], tp[1], tp[2], in->target_stiffnesses ? in->target_stiffnesses[v] : 0.f);
+      if (forceActive(initialForces[g])) sc.forceCount++;
+      if (initialTargets[g].w > 0) sc.targetCount++;
+      sp->pinned[g] = in->vertex_info[4ull * v + 2] != 0;
+    }
+    refreshObjectiveFlags(sc);
+  }
+
+  // Colour lists (union over scenes) and per-colour frame lists.
+  std::vector<uint32_t> byColor;
+  std::vector<uint32_t> need;
+  sp->colorOffsets.assign(colorCount + 1, 0);
+  sp->needOffsets.assign(colorCount + 1, 0);
+  {
+    std::vector<uint32_t> mark(nV, 0xffffffffu);
+    for (uint32_t c = 0; c < colorCount; ++c) {
+      std::vector<uint32_t> needList;
+      for (uint32_t i = 0; i < S; ++i) {
+        const jgs2_input* in = prep[i].in;
+        const SceneHost& sc = sp->scenes[i];
+        auto add = [&](uint32_t u) {
+          if (mark[u] != c) { mark[u] = c; needList.push_back(u); }
+        };
+        for (uint32_t v = 0; v < sc.V; ++v) {
+          if (sc.colors[v] != c) continue;
+          byColor.push_back(sc.vOff + v);
+          add(sc.vOff + v);
+          for (uint32_t k = 0; k < sc.K; ++k) {
+            const size_t r = static_cast<size_t>(v) * sc.K + k;
+            const uint32_t t = in->cubature_tet_ids[r];
+            if (t == kEmptyTet || t >= sc.T || !(in->cubature_weights[r] > 0)) continue;
+            for (int l = 0; l < 4; ++l) add(sc.vOff + in->tet_indices[4ull * t + l]);
+          }
+        }
+      }
+      std::sort(needList.begin(), needList.end());
+      need.insert(need.end(), needList.begin(), needList.end());
+      sp->colorOffsets[c + 1] = static_cast<uint32_t>(byColor.size());
+      sp->needOffsets[c + 1] = static_cast<uint32_t>(need.size());
+    }
+  }
+
+  // Device packing.
+  cudaError_t ce = cudaSetDevice(device);
+  if (ce != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, format("cudaSetDevice: %s", cudaGetErrorString(ce)));
+  if (jgs2::solveGroupsPerBlock(K) == 0)
+    return fail(nullptr, JGS2_UNSUPPORTED,
+                format("cubatureK %u is too large for the shared-memory record cache of one vertex.", K));
+  ce = cudaStreamCreateWithFlags(&sp->stream, cudaStreamNonBlocking);
+  if (ce != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, format("cudaStreamCreate: %s", cudaGetErrorString(ce)));
+  auto bail = [&](jgs2_status st) {
+    gGlobalError = sp->error;
+    releaseDevice(sp);
+    return st;
+  };
+  std::vector<float4> pos(nV), rest(nV), vel(nV, make_float4(0, 0, 0, 0));
+  std::vector<uint4> info(nV);
+  std::vector<uint32_t> vertexScene(nV), colors(nV);
+  // Tet record: rows of inverse Dm (shape gradients g1..g3) with volume,
+  // lambda, mu in w, then the four (global) indices.
+  std::vector<float4> tets(4ull * nT);
+  std::vector<uint32_t> adjacency;
+  const size_t R = static_cast<size_t>(nV) * K;
+  // Record headers: tet id and weight, then the tet's vertex indices, so a
+  // record's vertex data can be fetched without waiting for its tet.  Scenes
+  // with fewer records per vertex than the widest are padded with empty ones.
+  std::vector<uint4> head(2 * R, make_uint4(kEmptyTet, 0u, 0u, 0u));
+  for (size_t r = 0; r < R; ++r) head[2 * r + 1] = make_uint4(0u, 0u, 0u, 0u);
+  std::vector<float> basis(36 * R, 0.f);
+  for (uint32_t i = 0; i < S; ++i) {
+    const jgs2_input* in = prep[i].in;
+    const SceneHost& sc = sp->scenes[i];
+    const uint32_t adjOff = static_cast<uint32_t>(adjacency.size());
+    for (uint32_t v = 0; v < sc.V; ++v) {
+      const uint32_t g = sc.vOff + v;
+      pos[g] = make_float4(in->positions[4ull * v], in->positions[4ull * v + 1], in->positions[4ull * v + 2], 1.f);
+      rest[g] = make_float4(in->vertex_rest[4ull * v], in->vertex_rest[4ull * v + 1], in->vertex_rest[4ull * v + 2],
+                            in->vertex_rest[4ull * v + 3]);
+      info[g] = make_uint4(adjOff + in->vertex_info[4ull * v], in->vertex_info[4ull * v + 1],
+                           in->vertex_info[4ull * v + 2], sc.bodyOff + in->vertex_info[4ull * v + 3]);
+      if (in->velocities)
+        vel[g] = make_float4(in->velocities[4ull * v], in->velocities[4ull * v + 1], in->velocities[4ull * v + 2], 0.f);
+      vertexScene[g] = i;
+      colors[g] = sc.colors[v];
+    }
+    for (uint32_t t = 0; t < sc.T; ++t) {
+      const float* m = &in->tet_inverse_dm[12ull * t];
+      const float* meta = &in->tet_meta[4ull * t];
+      const size_t g = sc.tOff + t;
+      tets[4 * g] = make_float4(m[0], m[4], m[8], meta[0]);
+      tets[4 * g + 1] = make_float4(m[1], m[5], m[9], meta[1]);
+      tets[4 * g + 2] = make_float4(m[2], m[6], m[10], meta[2]);
+      const uint4 q = make_uint4(sc.vOff + in->tet_indices[4ull * t], sc.vOff + in->tet_indices[4ull * t + 1],
+                                 sc.vOff + in->tet_indices[4ull * t + 2], sc.vOff + in->tet_indices[4ull * t + 3]);
+      std::memcpy(&tets[4 * g + 3], &q, sizeof(q));
+    }
+    adjacency.resize(adjOff + in->adjacency_length);
+    for (uint32_t v = 0; v < sc.V; ++v) {
+      const uint32_t start = in->vertex_info[4ull * v], count = in->vertex_info[4ull * v + 1];
+      for (uint32_t a = 0; a < count; ++a) {
+        const uint32_t t = in->adjacency[start + a];
+        uint32_t slot = 0;
+        for (uint32_t l = 0; l < 4; ++l)
+          if (in->tet_indices[4ull * t + l] == v) { slot = l; break; }
+        adjacency[adjOff + start + a] = (sc.tOff + t) * 4u + slot;
+      }
+    }
+    for (uint32_t v = 0; v < sc.V; ++v) {
+      for (uint32_t k = 0; k < sc.K; ++k) {
+        const size_t src = static_cast<size_t>(v) * sc.K + k;
+        const size_t dst = static_cast<size_t>(sc.vOff + v) * K + k;
+        const uint32_t t = in->cubature_tet_ids[src];
+        uint32_t wbits;
+        std::memcpy(&wbits, &in->cubature_weights[src], 4);
+        const bool valid = t != kEmptyTet && t < sc.T;
+        head[2 * dst] = make_uint4(valid ? sc.tOff + t : kEmptyTet, wbits, 0u, 0u);
+        if (valid)
+          head[2 * dst + 1] =
+              make_uint4(sc.vOff + in->tet_indices[4ull * t], sc.vOff + in->tet_indices[4ull * t + 1],
+                         sc.vOff + in->tet_indices[4ull * t + 2], sc.vOff + in->tet_indices[4ull * t + 3]);
+        std::memcpy(&basis[36 * dst], &in->cubature_basis[36 * src], sizeof(float) * 36);
+      }
+    }
+  }
+  // Segmented reduction tables: each scene's elements in fixed chunks.
+  std::vector<jgs2::SceneRange> ranges(S);
+  std::vector<jgs2::RedBlock> gateTable, convTable;
+  for (uint32_t i = 0; i < S; ++i) {
+    const SceneHost& sc = sp->scenes[i];
+    jgs2::SceneRange& r = ranges[i];
+    r.vOff = sc.vOff; r.V = sc.V; r.tOff = sc.tOff; r.T = sc.T;
+    const uint32_t n = std::max(sc.V, sc.T);
+    r.gateBase = static_cast<uint32_t>(gateTable.size());
+    for (uint32_t b0 = 0; b0 < std::max(n, 1u); b0 += jgs2::kGateChunk)
+      gateTable.push_back({i, b0, std::min(n, b0 + jgs2::kGateChunk), static_cast<uint32_t>(gateTable.size())});
+    r.gateBlocks = static_cast<uint32_t>(gateTable.size()) - r.gateBase;
+    r.convBase = static_cast<uint32_t>(convTable.size());
+    for (uint32_t b0 = 0; b0 < std::max(sc.V, 1u); b0 += jgs2::kConvChunk)
+      convTable.push_back({i, b0, std::min(sc.V, b0 + jgs2::kConvChunk), static_cast<uint32_t>(convTable.size())});
+    r.convBlocks = static_cast<uint32_t>(convTable.size()) - r.convBase;
+  }
+
+  jgs2_status st = JGS2_OK;
+  Buffers& b = sp->b;
+#define STEP(x) do { st = (x); if (st != JGS2_OK) return bail(st); } while (0)
+  STEP(upload(sp, &b.pos[0], pos.data(), nV));
+  STEP(upload(sp, &b.pos[1], pos.data(), nV));
+  STEP(upload(sp, &b.predicted, pos.data(), nV));
+  STEP(upload(sp, &b.old, pos.data(), nV));
+  STEP(upload(sp, &b.velocity, vel.data(), nV));
+  {
+    std::vector<float4> identity(3ull * nV);
+    for (uint32_t v = 0; v < nV; ++v) {
+      identity[3ull * v] = make_float4(1, 0, 0, 0);
+      identity[3ull * v + 1] = make_float4(0, 1, 0, 0);
+      identity[3ull * v + 2] = make_float4(0, 0, 1, 0);
+    }
+    STEP(upload(sp, &b.vertexRot, identity.data(), 3ull * nV));
+  }
+  b.tetRot = nullptr;
+  STEP(deviceAlloc(sp, &b.finalUpdate, nV));
+  STEP(deviceAlloc(sp, &b.local, 4ull * nV));
+  STEP(deviceAlloc(sp, &b.incident, 3ull * nV));
+  CUDA_TRY(sp, cudaMemsetAsync(b.finalUpdate, 0, sizeof(float) * nV, sp->stream));
+  CUDA_TRY(sp, cudaMemsetAsync(b.local, 0, sizeof(float4) * 4ull * nV, sp->stream));
+  CUDA_TRY(sp, cudaMemsetAsync(b.incident, 0, sizeof(float4) * 3ull * nV, sp->stream));
+  {
+    FrameState fs;
+    std::memset(&fs, 0, sizeof(fs));
+    fs.localNumericsValid = 1;
+    std::vector<FrameState> frames(S, fs);
+    STEP(upload(sp, &b.frames, frames.data(), S));
+  }
+  b.gateBlocks = static_cast<uint32_t>(gateTable.size());
+  b.convBlocks = static_cast<uint32_t>(convTable.size());
+  b.sceneCount = S;
+  {
+    double* gp = nullptr;
+    double* cp = nullptr;
+    STEP(deviceAlloc(sp, &gp, jgs2::kGatePartialBytes / sizeof(double) * b.gateBlocks));
+    STEP(deviceAlloc(sp, &cp, jgs2::kConvPartialBytes / sizeof(double) * b.convBlocks));
+    b.gatePartials = gp;
+    b.convPartials = cp;
+    jgs2::RedBlock* gt = nullptr;
+    jgs2::RedBlock* ct = nullptr;
+    STEP(upload(sp, &gt, gateTable.data(), gateTable.size()));
+    STEP(upload(sp, &ct, convTable.data(), convTable.size()));
+    b.gateTable = gt;
+    b.convTable = ct;
+    jgs2::SceneRange* rg = nullptr;
+    STEP(upload(sp, &rg, ranges.data(), ranges.size()));
+    b.scenes = rg;
+    uint32_t* vs = nullptr;
+    STEP(upload(sp, &vs, vertexScene.data(), vertexScene.size()));
+    b.vertexScene = vs;
+  }
+  STEP(deviceAlloc(sp, &b.bodyAccum, 6ull * sp->bodies));
+  {
+    float4* p = nullptr;
+    STEP(upload(sp, &p, rest.data(), nV));
+    b.restMass = p;
+    uint4* q = nullptr;
+    STEP(upload(sp, &q, info.data(), nV));
+    b.vinfo = q;
+    float4* tt = nullptr;
+    STEP(upload(sp, &tt, tets.data(), 4ull * nT));
+    b.tets = tt;
+    uint32_t* a = nullptr;
+    STEP(upload(sp, &a, adjacency.data(), adjacency.size()));
+    b.adjacency = a;
+    uint4* ch = nullptr;
+    STEP(upload(sp, &ch, head.data(), 2 * R));
+    b.cubHead = ch;
+    float4* cb = nullptr;
+    STEP(upload(sp, &cb, reinterpret_cast<const float4*>(basis.data()), 9 * R));
+    b.cubBasis = cb;
+    b.stiffness = nullptr;
+    float4* df = nullptr;
+    float4* dt = nullptr;
+    STEP(deviceAlloc(sp, &df, nV));
+    STEP(deviceAlloc(sp, &dt, nV));
+    b.forces = df;
+    b.targets = dt;
+    CUDA_TRY(sp, cudaMallocHost(reinterpret_cast<void**>(&sp->hForces), sizeof(float4) * std::max<size_t>(1, nV)));
+    CUDA_TRY(sp, cudaMallocHost(reinterpret_cast<void**>(&sp->hTargets), sizeof(float4) * std::max<size_t>(1, nV)));
+    CUDA_TRY(sp, cudaEventCreateWithFlags(&sp->objectiveUpload, cudaEventDisableTiming));
+    std::memcpy(sp->hForces, initialForces.data(), sizeof(float4) * nV);
+    std::memcpy(sp->hTargets, initialTargets.data(), sizeof(float4) * nV);
+    CUDA_TRY(sp, cudaMemcpyAsync(df, sp->hForces, sizeof(float4) * nV, cudaMemcpyHostToDevice, sp->stream));
+    CUDA_TRY(sp, cudaMemcpyAsync(dt, sp->hTargets, sizeof(float4) * nV, cudaMemcpyHostToDevice, sp->stream));
+    CUDA_TRY(sp, cudaEventRecord(sp->objectiveUpload, sp->stream));
+    sp->objectiveUploadPending = true;
+    uint32_t* cl = nullptr;
+    STEP(upload(sp, &cl, colors.data(), nV));
+    b.colors = cl;
+    STEP(upload(sp, &sp->dColorVertices, byColor.data(), byColor.size()));
+    STEP(upload(sp, &sp->dNeedVertices, need.data(), need.size()));
+    STEP(deviceAlloc(sp, &sp->dParams, S));
+    sp->hParams.resize(S);
+  }
+#undef STEP
+  // GPU preflight of the uploaded pose (validateGpuInitialStableSource,
+  // jgs2-solver.ts:820-893): the gate on (posA, posA) must accept in every scene.
+  for (uint32_t i = 0; i < S; ++i) sp->hParams[i] = makeParams(sp, i, sp->scenes[i].defaults, false);
+  CUDA_TRY(sp, cudaMemcpyAsync(sp->dParams, sp->hParams.data(), sizeof(DevParams) * S, cudaMemcpyHostToDevice,
+                               sp->stream));
+  jgs2::launchGate(b, sp->dParams, b.pos[0], b.pos[0], sp->stream);
+  sp->launches += 1;
+  std::vector<FrameState> frames(S);
+  CUDA_TRY(sp, cudaMemcpyAsync(frames.data(), b.frames, sizeof(FrameState) * S, cudaMemcpyDeviceToHost, sp->stream));
+  ce = cudaStreamSynchronize(sp->stream);
+  if (ce != cudaSuccess) { cudaFail(sp, ce, "preflight"); return bail(JGS2_DEVICE_ERROR); }
+  for (uint32_t i = 0; i < S; ++i) {
+    const float4* control = frames[i].control;
+    const uint32_t required = 1u | 2u | 4u;
+    const float vb = control[0].w;
+    const bool ok = std::isfinite(control[0].x) && std::isfinite(control[0].y) && std::isfinite(control[0].z) &&
+                    control[0].x > kDeterminantFloor && control[0].y > kDeterminantFloor &&
+                    control[0].z > kDeterminantFloor && vb == std::floor(vb) &&
+                    ((static_cast<uint32_t>(vb) & required) == required);
+    if (!ok) {
+      sp->error = format("The uploaded stable Neo-Hookean source pose%s is not feasible under the production GPU "
+                         "f32 determinant calculation; source J=%g, candidate J=%g, accepted J=%g.",
+                         S > 1 ? format(" of scene %u", i).c_str() : "", control[0].x, control[0].y, control[0].z);
+      return bail(JGS2_INFEASIBLE_INPUT);
+    }
+  }
+  return JGS2_OK;
+}
+
+jgs2_status readSceneVec4(Engine* s, uint32_t scene, const float4* dev, float* out, size_t floats,
+                          size_t perVertex) {
+  const SceneHost& sc = s->scenes[scene];
+  if (!out || floats < perVertex * sc.V)
+    return fail(s, JGS2_INVALID_ARGUMENT, format("output needs %zu floats.", perVertex * sc.V));
+  return readRegion(s, dev + (perVertex / 4) * sc.vOff, sizeof(float) * perVertex * sc.V, out);
+}
+
+jgs2_status readSceneGlobalization(Engine* s, uint32_t scene, float* local, size_t localFloats, float* control,
+                                   float* history, size_t historyFloats, uint32_t* historyCount) {
+  const SceneHost& sc = s->scenes[scene];
+  if (!sc.recordsAvailable)
+    return fail(s, JGS2_NOT_READY,
+                "Globalization diagnostics are unavailable until a stable nonlinear iteration or diagnostic test "
+                "kernel has produced records.");
+  jgs2_status st = JGS2_OK;
+  if (local) {
+    if (localFloats < 16ull * sc.V) return fail(s, JGS2_INVALID_ARGUMENT, "local output too small.");
+    st = readRegion(s, s->b.local + 4ull * sc.vOff, sizeof(float) * 16ull * sc.V, local);
+    if (st != JGS2_OK) return st;
+  }
+  float4 ctl[4];
+  st = readRegion(s, s->b.frames[scene].control, sizeof(ctl), ctl);
+  if (st != JGS2_OK) return st;
+  if (control) std::memcpy(control, ctl, sizeof(ctl));
+  const float raw = ctl[1].w;
+  if (!(raw >= 0 && raw <= float(JGS2_HISTORY_CAPACITY) && raw == std::floor(raw)))
+    return fail(s, JGS2_DEVICE_ERROR, format("GPU returned invalid globalization history count %g.", raw));
+  const uint32_t count = static_cast<uint32_t>(raw);
+  if (historyCount) *historyCount = count;
+  if (history) {
+    if (historyFloats < 32ull * JGS2_HISTORY_CAPACITY) return fail(s, JGS2_INVALID_ARGUMENT, "history output too small.");
+    st = readRegion(s, s->b.frames[scene].history, sizeof(float) * 32ull * JGS2_HISTORY_CAPACITY, history);
+    if (st != JGS2_OK) return st;
+  }
+  return JGS2_OK;
+}
+
+jgs2_status sceneInfo(Engine* s, uint32_t scene, jgs2_info* out) {
+  const SceneHost& sc = s->scenes[scene];
+  std::memset(out, 0, sizeof(*out));
+  out->vertex_count = sc.V;
+  out->tet_count = sc.T;
+  out->cubature_k = sc.K;
+  out->body_count = sc.bodies;
+  out->schedule_color_count = sc.colorCount;
+  out->globalization_enabled = s->glob ? 1 : 0;
+  out->objective_flags = sc.objectiveFlags;
+  out->external_force_vertex_count = sc.forceCount;
+  out->quadratic_target_vertex_count = sc.targetCount;
+  out->objective_revision = sc.objectiveRevision;
+  out->last_submitted_iterations = sc.submittedIterations;
+  out->scene_scale = sc.sceneScale;
+  out->preprocessing_timestep = sc.preprocessingTimestep;
+  out->current_position_buffer = 0;
+  if (sc.recordsAvailable) {
+    float4 c1;
+    if (readRegion(s, &s->b.frames[scene].control[1], sizeof(c1), &c1) == JGS2_OK)
+      out->history_count = static_cast<uint32_t>(c1.w);
+  }
   return JGS2_OK;
 }
 
@@ -796,303 +1266,12 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
                         jgs2_solver** out) {
   if (!out) return fail(nullptr, JGS2_INVALID_ARGUMENT, "out is NULL.");
   *out = nullptr;
-  std::string err;
-  if (!validateInput(in, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
-  // inferJGS2MaterialMode (layout.ts:509-522).
-  uint32_t stable = 0;
-  for (uint32_t t = 0; t < in->tet_count; ++t) stable += in->tet_meta[4ull * t + 3] == 1.0f ? 1u : 0u;
-  if (stable != 0 && stable != in->tet_count)
-    return fail(nullptr, JGS2_INVALID_ARGUMENT,
-                "A production JGS2 solve cannot mix stable Neo-Hookean and co-rotated regression tetrahedra in one "
-                "precomputation.");
-  const bool glob = stable == in->tet_count;
-  if (!glob)
-    return fail(nullptr, JGS2_UNSUPPORTED,
-                "The co-rotated regression material path is not built into this library; use stable Neo-Hookean "
-                "tetrahedra.");
-  uint32_t colorCount = 0;
-  std::vector<uint32_t> colors = colorInput(in, &colorCount);
-  if (colorCount > JGS2_MAX_SCHEDULE_COLORS)
-    return fail(nullptr, JGS2_INVALID_ARGUMENT,
-                format("Colored Gauss-Seidel supports at most %u colors; the small-scene conflict graph needs %u.",
-                       JGS2_MAX_SCHEDULE_COLORS, colorCount));
-  jgs2_settings base;
-  defaults(&base);
-  jgs2_settings resolved;
-  if (!resolve(base, settings, mask, &resolved, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
-  if (glob) {
-    const double m = minimumInputDeterminant(in);
-    if (!std::isfinite(m) || !(m > kDeterminantFloor))
-      return fail(nullptr, JGS2_INFEASIBLE_INPUT,
-                  format("A stable Neo-Hookean production solve requires an initially feasible pose with minimum J "
-                         "greater than %g; got %g.", kDeterminantFloor, m));
-  }
+  std::vector<PreparedScene> prep(1);
+  jgs2_status st = prepareScene(in, settings, mask, &prep[0]);
+  if (st != JGS2_OK) return st;
   std::unique_ptr<jgs2_solver> s(new jgs2_solver());
-  s->device = device;
-  // JGS2_NO_GRAPHS=1 launches each frame's kernels directly (debugging).
-  s->useGraphs = std::getenv("JGS2_NO_GRAPHS") == nullptr;
-  s->V = in->vertex_count;
-  s->T = in->tet_count;
-  s->K = in->cubature_k;
-  s->glob = glob;
-  s->defaults = resolved;
-  s->submitted = resolved;
-  s->preprocessingTimestep = resolved.timestep;
-  s->colors = colors;
-  s->colorCount = colorCount;
-  uint32_t maxBody = 0;
-  for (uint32_t v = 0; v < s->V; ++v) maxBody = std::max(maxBody, in->vertex_info[4ull * v + 3]);
-  s->bodies = maxBody + 1;
-  // computeJGS2InitialDynamicSceneScale (jgs2-solver.ts:732-768).
-  {
-    double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
-    uint32_t dyn = 0;
-    for (uint32_t v = 0; v < s->V; ++v) {
-      if (in->vertex_info[4ull * v + 2] != 0) continue;
-      dyn++;
-      for (int k = 0; k < 3; ++k) {
-        lo[k] = std::min(lo[k], static_cast<double>(in->positions[4ull * v + k]));
-        hi[k] = std::max(hi[k], static_cast<double>(in->positions[4ull * v + k]));
-      }
-    }
-    const double d = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
-                               (hi[2] - lo[2]) * (hi[2] - lo[2]));
-    s->sceneScale = static_cast<float>(dyn > 0 && std::isfinite(d) && d > 0 ? d : kDegenerateSceneScale);
-  }
-  // Objectives (packJGS2VertexObjectives, layout.ts:635-668); copied into
-  // the pinned mirrors once the device is set up.
-  std::vector<float4> initialForces(s->V), initialTargets(s->V);
-  s->pinned.assign(s->V, 0);
-  s->forceCount = s->targetCount = 0;
-  for (uint32_t v = 0; v < s->V; ++v) {
-    const float* f = in->external_forces ? &in->external_forces[3ull * v] : nullptr;
-    initialForces[v] = f ? make_float4(f[0], f[1], f[2], 0.f) : make_float4(0.f, 0.f, 0.f, 0.f);
-    const float* tp = in->target_positions ? &in->target_positions[3ull * v] : &in->positions[4ull * v];
-    initialTargets[v] = make_float4(tp[0], tp[1], tp[2], in->target_stiffnesses ? in->target_stiffnesses[v] : 0.f);
-    if (forceActive(initialForces[v])) s->forceCount++;
-    if (initialTargets[v].w > 0) s->targetCount++;
-    s->pinned[v] = in->vertex_info[4ull * v + 2] != 0;
-  }
-  refreshObjectiveFlags(s.get());
-  // Colour lists and per-colour frame lists.
-  std::vector<uint32_t> byColor(s->V);
-  s->colorOffsets.assign(colorCount + 1, 0);
-  for (uint32_t v = 0; v < s->V; ++v) s->colorOffsets[colors[v] + 1]++;
-  for (uint32_t c = 0; c < colorCount; ++c) s->colorOffsets[c + 1] += s->colorOffsets[c];
-  {
-    std::vector<uint32_t> cur(s->colorOffsets.begin(), s->colorOffsets.end() - 1);
-    for (uint32_t v = 0; v < s->V; ++v) byColor[cur[colors[v]]++] = v;
-  }
-  std::vector<uint32_t> need;
-  s->needOffsets.assign(colorCount + 1, 0);
-  {
-    std::vector<uint32_t> mark(s->V, 0xffffffffu);
-    for (uint32_t c = 0; c < colorCount; ++c) {
-      std::vector<uint32_t> list;
-      auto add = [&](uint32_t u) {
-        if (mark[u] != c) { mark[u] = c; list.push_back(u); }
-      };
-      for (uint32_t i = s->colorOffsets[c]; i < s->colorOffsets[c + 1]; ++i) {
-        const uint32_t v = byColor[i];
-        add(v);
-        for (uint32_t k = 0; k < s->K; ++k) {
-          const size_t r = static_cast<size_t>(v) * s->K + k;
-          const uint32_t t = in->cubature_tet_ids[r];
-          if (t == kEmptyTet || t >= s->T || !(in->cubature_weights[r] > 0)) continue;
-          for (int l = 0; l < 4; ++l) add(in->tet_indices[4ull * t + l]);
-        }
-      }
-      std::sort(list.begin(), list.end());
-      need.insert(need.end(), list.begin(), list.end());
-      s->needOffsets[c + 1] = static_cast<uint32_t>(need.size());
-    }
-  }
-  // Device packing.
-  jgs2_solver* sp = s.get();
-  cudaError_t ce = cudaSetDevice(device);
-  if (ce != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, format("cudaSetDevice: %s", cudaGetErrorString(ce)));
-  if (jgs2::solveGroupsPerBlock(in->cubature_k) == 0)
-    return fail(nullptr, JGS2_UNSUPPORTED,
-                format("cubatureK %u is too large for the shared-memory record cache of one vertex.",
-                       in->cubature_k));
-  ce = cudaStreamCreateWithFlags(&sp->stream, cudaStreamNonBlocking);
-  if (ce != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, format("cudaStreamCreate: %s", cudaGetErrorString(ce)));
-  auto bail = [&](jgs2_status st) {
-    gGlobalError = sp->error;
-    releaseDevice(sp);
-    return st;
-  };
-  const uint32_t V = s->V, T = s->T, K = s->K;
-  std::vector<float4> pos(V), rest(V);
-  std::vector<uint4> info(V);
-  for (uint32_t v = 0; v < V; ++v) {
-    pos[v] = make_float4(in->positions[4ull * v], in->positions[4ull * v + 1], in->positions[4ull * v + 2], 1.f);
-    rest[v] = make_float4(in->vertex_rest[4ull * v], in->vertex_rest[4ull * v + 1], in->vertex_rest[4ull * v + 2],
-                          in->vertex_rest[4ull * v + 3]);
-    info[v] = make_uint4(in->vertex_info[4ull * v], in->vertex_info[4ull * v + 1], in->vertex_info[4ull * v + 2],
-                         in->vertex_info[4ull * v + 3]);
-  }
-  std::vector<float4> vel(V, make_float4(0, 0, 0, 0));
-  if (in->velocities)
-    for (uint32_t v = 0; v < V; ++v)
-      vel[v] = make_float4(in->velocities[4ull * v], in->velocities[4ull * v + 1], in->velocities[4ull * v + 2], 0.f);
-  // Tet record: rows of inverse Dm (shape gradients g1..g3) with volume,
-  // lambda, mu in w, then the four indices.
-  std::vector<float4> tets(4ull * T);
-  for (uint32_t t = 0; t < T; ++t) {
-    const float* m = &in->tet_inverse_dm[12ull * t];
-    const float* meta = &in->tet_meta[4ull * t];
-    tets[4ull * t] = make_float4(m[0], m[4], m[8], meta[0]);
-    tets[4ull * t + 1] = make_float4(m[1], m[5], m[9], meta[1]);
-    tets[4ull * t + 2] = make_float4(m[2], m[6], m[10], meta[2]);
-    uint4 q = make_uint4(in->tet_indices[4ull * t], in->tet_indices[4ull * t + 1], in->tet_indices[4ull * t + 2],
-                         in->tet_indices[4ull * t + 3]);
-    std::memcpy(&tets[4ull * t + 3], &q, sizeof(q));
-  }
-  std::vector<uint32_t> adjacency(in->adjacency_length);
-  for (uint32_t v = 0; v < V; ++v) {
-    const uint32_t start = in->vertex_info[4ull * v], count = in->vertex_info[4ull * v + 1];
-    for (uint32_t a = 0; a < count; ++a) {
-      const uint32_t t = in->adjacency[start + a];
-      uint32_t slot = 0;
-      for (uint32_t l = 0; l < 4; ++l)
-        if (in->tet_indices[4ull * t + l] == v) { slot = l; break; }
-      adjacency[start + a] = t * 4u + slot;
-    }
-  }
-  const size_t R = static_cast<size_t>(V) * K;
-  std::vector<uint32_t> cubTet(in->cubature_tet_ids, in->cubature_tet_ids + R);
-  std::vector<float> cubW(in->cubature_weights, in->cubature_weights + R);
-  jgs2_status st = JGS2_OK;
-  Buffers& b = sp->b;
-#define STEP(x) do { st = (x); if (st != JGS2_OK) return bail(st); } while (0)
-  STEP(upload(sp, &b.pos[0], pos.data(), V));
-  STEP(upload(sp, &b.pos[1], pos.data(), V));
-  STEP(upload(sp, &b.predicted, pos.data(), V));
-  STEP(upload(sp, &b.old, pos.data(), V));
-  STEP(upload(sp, &b.velocity, vel.data(), V));
-  std::vector<float4> identity(3ull * V);
-  for (uint32_t v = 0; v < V; ++v) {
-    identity[3ull * v] = make_float4(1, 0, 0, 0);
-    identity[3ull * v + 1] = make_float4(0, 1, 0, 0);
-    identity[3ull * v + 2] = make_float4(0, 0, 1, 0);
-  }
-  STEP(upload(sp, &b.vertexRot, identity.data(), 3ull * V));
-  b.tetRot = nullptr;
-  STEP(deviceAlloc(sp, &b.finalUpdate, V));
-  STEP(deviceAlloc(sp, &b.local, 4ull * V));
-  STEP(deviceAlloc(sp, &b.incident, 3ull * V));
-  CUDA_TRY(sp, cudaMemsetAsync(b.finalUpdate, 0, sizeof(float) * V, sp->stream));
-  CUDA_TRY(sp, cudaMemsetAsync(b.local, 0, sizeof(float4) * 4ull * V, sp->stream));
-  CUDA_TRY(sp, cudaMemsetAsync(b.incident, 0, sizeof(float4) * 3ull * V, sp->stream));
-  STEP(deviceAlloc(sp, &b.frame, 1));
-  {
-    FrameState fs;
-    std::memset(&fs, 0, sizeof(fs));
-    fs.gateMinSource = fs.gateMinCandidate = 0xffffffffu;  // encodes the largest float
-    fs.gateBits = 0xffffffffu;
-    fs.localNumericsValid = 1;
-    fs.convValid = 1;
-    // Encode +3e38 exactly as the kernels do.
-    uint32_t u;
-    const float big = 3.0e38f;
-    std::memcpy(&u, &big, 4);
-    fs.gateMinSource = fs.gateMinCandidate = u | 0x80000000u;
-    CUDA_TRY(sp, cudaMemcpyAsync(b.frame, &fs, sizeof(fs), cudaMemcpyHostToDevice, sp->stream));
-    CUDA_TRY(sp, cudaStreamSynchronize(sp->stream));
-  }
-  b.gateBlocks = jgs2::gateBlockCount(V, T);
-  b.convBlocks = jgs2::convBlockCount(V);
-  {
-    double* gp = nullptr;
-    double* cp = nullptr;
-    STEP(deviceAlloc(sp, &gp, jgs2::kGatePartialBytes / sizeof(double) * b.gateBlocks));
-    STEP(deviceAlloc(sp, &cp, jgs2::kConvPartialBytes / sizeof(double) * b.convBlocks));
-    b.gatePartials = gp;
-    b.convPartials = cp;
-  }
-  STEP(deviceAlloc(sp, &b.bodyAccum, 6ull * sp->bodies));
-  {
-    float4* p = nullptr;
-    STEP(upload(sp, &p, rest.data(), V));
-    b.restMass = p;
-    uint4* q = nullptr;
-    STEP(upload(sp, &q, info.data(), V));
-    b.vinfo = q;
-    float4* tt = nullptr;
-    STEP(upload(sp, &tt, tets.data(), 4ull * T));
-    b.tets = tt;
-    uint32_t* a = nullptr;
-    STEP(upload(sp, &a, adjacency.data(), adjacency.size()));
-    b.adjacency = a;
-    // Record headers: tet id and weight, then the tet's vertex indices, so a
-    // record's vertex data can be fetched without waiting for its tet.
-    std::vector<uint4> head(2 * R);
-    for (size_t rec = 0; rec < R; ++rec) {
-      const uint32_t t = cubTet[rec];
-      uint32_t wbits;
-      std::memcpy(&wbits, &cubW[rec], 4);
-      head[2 * rec] = make_uint4(t, wbits, 0u, 0u);
-      head[2 * rec + 1] = t < T ? make_uint4(in->tet_indices[4ull * t], in->tet_indices[4ull * t + 1],
-                                             in->tet_indices[4ull * t + 2], in->tet_indices[4ull * t + 3])
-                                : make_uint4(0u, 0u, 0u, 0u);
-    }
-    uint4* ch = nullptr;
-    STEP(upload(sp, &ch, head.data(), 2 * R));
-    b.cubHead = ch;
-    float4* cb = nullptr;
-    STEP(deviceAlloc(sp, &cb, 9 * R));
-    if (R) CUDA_TRY(sp, cudaMemcpyAsync(cb, in->cubature_basis, sizeof(float) * 36 * R, cudaMemcpyHostToDevice,
-                                        sp->stream));
-    b.cubBasis = cb;
-    b.stiffness = nullptr;
-    float4* df = nullptr;
-    float4* dt = nullptr;
-    STEP(deviceAlloc(sp, &df, V));
-    STEP(deviceAlloc(sp, &dt, V));
-    b.forces = df;
-    b.targets = dt;
-    CUDA_TRY(sp, cudaMallocHost(reinterpret_cast<void**>(&sp->hForces), sizeof(float4) * std::max<size_t>(1, V)));
-    CUDA_TRY(sp, cudaMallocHost(reinterpret_cast<void**>(&sp->hTargets), sizeof(float4) * std::max<size_t>(1, V)));
-    CUDA_TRY(sp, cudaEventCreateWithFlags(&sp->objectiveUpload, cudaEventDisableTiming));
-    std::memcpy(sp->hForces, initialForces.data(), sizeof(float4) * V);
-    std::memcpy(sp->hTargets, initialTargets.data(), sizeof(float4) * V);
-    CUDA_TRY(sp, cudaMemcpyAsync(df, sp->hForces, sizeof(float4) * V, cudaMemcpyHostToDevice, sp->stream));
-    CUDA_TRY(sp, cudaMemcpyAsync(dt, sp->hTargets, sizeof(float4) * V, cudaMemcpyHostToDevice, sp->stream));
-    CUDA_TRY(sp, cudaEventRecord(sp->objectiveUpload, sp->stream));
-    sp->objectiveUploadPending = true;
-    uint32_t* cl = nullptr;
-    STEP(upload(sp, &cl, colors.data(), V));
-    b.colors = cl;
-    STEP(upload(sp, &sp->dColorVertices, byColor.data(), byColor.size()));
-    STEP(upload(sp, &sp->dNeedVertices, need.data(), need.size()));
-    STEP(deviceAlloc(sp, &sp->dParams, 1));
-  }
-#undef STEP
-  // GPU preflight of the uploaded pose (validateGpuInitialStableSource,
-  // jgs2-solver.ts:820-893): the gate on (posA, posA) must accept.
-  if (glob) {
-    DevParams p = makeParams(sp, resolved, false);
-    CUDA_TRY(sp, cudaMemcpyAsync(sp->dParams, &p, sizeof(p), cudaMemcpyHostToDevice, sp->stream));
-    jgs2::launchGate(b, sp->dParams, b.pos[0], b.pos[0], V, T, sp->stream);
-    sp->launches += 1;
-    float4 control[4];
-    CUDA_TRY(sp, cudaMemcpyAsync(control, b.frame->control, sizeof(control), cudaMemcpyDeviceToHost, sp->stream));
-    ce = cudaStreamSynchronize(sp->stream);
-    if (ce != cudaSuccess) { cudaFail(sp, ce, "preflight"); return bail(JGS2_DEVICE_ERROR); }
-    const uint32_t required = 1u | 2u | 4u;
-    const float vb = control[0].w;
-    const bool ok = std::isfinite(control[0].x) && std::isfinite(control[0].y) && std::isfinite(control[0].z) &&
-                    control[0].x > kDeterminantFloor && control[0].y > kDeterminantFloor &&
-                    control[0].z > kDeterminantFloor && vb == std::floor(vb) &&
-                    ((static_cast<uint32_t>(vb) & required) == required);
-    if (!ok) {
-      sp->error = format("The uploaded stable Neo-Hookean source pose is not feasible under the production GPU f32 "
-                         "determinant calculation; source J=%g, candidate J=%g, accepted J=%g.",
-                         control[0].x, control[0].y, control[0].z);
-      return bail(JGS2_INFEASIBLE_INPUT);
-    }
-  }
+  st = buildEngine(s.get(), prep, device);
+  if (st != JGS2_OK) return st;
   *out = s.release();
   return JGS2_OK;
 }
@@ -1113,34 +1292,14 @@ jgs2_status jgs2_get_info(jgs2_solver* s, jgs2_info* out) {
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
   if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
-  std::memset(out, 0, sizeof(*out));
-  out->vertex_count = s->V;
-  out->tet_count = s->T;
-  out->cubature_k = s->K;
-  out->body_count = s->bodies;
-  out->schedule_color_count = s->colorCount;
-  out->globalization_enabled = s->glob ? 1 : 0;
-  out->objective_flags = s->objectiveFlags;
-  out->external_force_vertex_count = s->forceCount;
-  out->quadratic_target_vertex_count = s->targetCount;
-  out->objective_revision = s->objectiveRevision;
-  out->last_submitted_iterations = s->submittedIterations;
-  out->scene_scale = s->sceneScale;
-  out->preprocessing_timestep = s->preprocessingTimestep;
-  out->current_position_buffer = 0;
-  if (s->recordsAvailable) {
-    float4 c1;
-    if (readRegion(s, &s->b.frame->control[1], sizeof(c1), &c1) == JGS2_OK)
-      out->history_count = static_cast<uint32_t>(c1.w);
-  }
-  return JGS2_OK;
+  return sceneInfo(s, 0, out);
 }
 
 jgs2_status jgs2_get_default_settings(jgs2_solver* s, jgs2_settings* out) {
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
   if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
-  *out = s->defaults;
+  *out = s->scenes[0].defaults;
   return JGS2_OK;
 }
 
@@ -1148,7 +1307,7 @@ jgs2_status jgs2_get_last_submitted_settings(jgs2_solver* s, jgs2_settings* out)
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
   if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
-  *out = s->submitted;
+  *out = s->scenes[0].submitted;
   return JGS2_OK;
 }
 
@@ -1210,11 +1369,12 @@ jgs2_status jgs2_set_external_force(jgs2_solver* s, uint32_t vertex, const float
     return fail(s, JGS2_INVALID_ARGUMENT, format("Pinned vertex %u cannot have a nonzero external force.", vertex));
   st = waitObjectiveMirror(s);
   if (st != JGS2_OK) return st;
+  SceneHost& sc = s->scenes[0];
   float4& f = s->hForces[vertex];
-  s->forceCount -= forceActive(f) ? 1u : 0u;
+  sc.forceCount -= forceActive(f) ? 1u : 0u;
   f = make_float4(force[0], force[1], force[2], 0.f);
-  s->forceCount += forceActive(f) ? 1u : 0u;
-  return writeObjectives(s, vertex, 1, true, false);
+  sc.forceCount += forceActive(f) ? 1u : 0u;
+  return writeObjectives(s, 0, vertex, 1, true, false);
 }
 
 jgs2_status jgs2_replace_external_forces(jgs2_solver* s, const float* forces) {
@@ -1240,8 +1400,8 @@ jgs2_status jgs2_replace_external_forces(jgs2_solver* s, const float* forces) {
     s->hForces[v] = f;
     count += forceActive(f) ? 1u : 0u;
   }
-  s->forceCount = count;
-  return writeObjectives(s, 0, s->V, true, false);
+  s->scenes[0].forceCount = count;
+  return writeObjectives(s, 0, 0, s->V, true, false);
 }
 
 jgs2_status jgs2_clear_external_forces(jgs2_solver* s) {
@@ -1271,11 +1431,12 @@ jgs2_status jgs2_set_quadratic_target(jgs2_solver* s, uint32_t vertex, const flo
                 format("Pinned vertex %u cannot have a nonzero quadratic-target stiffness.", vertex));
   st = waitObjectiveMirror(s);
   if (st != JGS2_OK) return st;
+  SceneHost& sc = s->scenes[0];
   float4& t = s->hTargets[vertex];
-  s->targetCount -= t.w > 0 ? 1u : 0u;
+  sc.targetCount -= t.w > 0 ? 1u : 0u;
   t = make_float4(target[0], target[1], target[2], stiffness);
-  s->targetCount += t.w > 0 ? 1u : 0u;
-  return writeObjectives(s, vertex, 1, false, true);
+  sc.targetCount += t.w > 0 ? 1u : 0u;
+  return writeObjectives(s, 0, vertex, 1, false, true);
 }
 
 jgs2_status jgs2_replace_quadratic_targets(jgs2_solver* s, const float* positions, const float* stiffnesses) {
@@ -1304,8 +1465,8 @@ jgs2_status jgs2_replace_quadratic_targets(jgs2_solver* s, const float* position
     s->hTargets[v] = make_float4(positions[3ull * v], positions[3ull * v + 1], positions[3ull * v + 2], stiffnesses[v]);
     count += stiffnesses[v] > 0 ? 1u : 0u;
   }
-  s->targetCount = count;
-  return writeObjectives(s, 0, s->V, false, true);
+  s->scenes[0].targetCount = count;
+  return writeObjectives(s, 0, 0, s->V, false, true);
 }
 
 jgs2_status jgs2_release_quadratic_target(jgs2_solver* s, uint32_t vertex) {
@@ -1314,9 +1475,9 @@ jgs2_status jgs2_release_quadratic_target(jgs2_solver* s, uint32_t vertex) {
   if (vertex >= s->V) return fail(s, JGS2_INVALID_ARGUMENT, format("vertex %u is out of range.", vertex));
   st = waitObjectiveMirror(s);
   if (st != JGS2_OK) return st;
-  s->targetCount -= s->hTargets[vertex].w > 0 ? 1u : 0u;
+  s->scenes[0].targetCount -= s->hTargets[vertex].w > 0 ? 1u : 0u;
   s->hTargets[vertex].w = 0.f;
-  return writeObjectives(s, vertex, 1, false, true);
+  return writeObjectives(s, 0, vertex, 1, false, true);
 }
 
 jgs2_status jgs2_release_all_quadratic_targets(jgs2_solver* s) {
@@ -1325,31 +1486,23 @@ jgs2_status jgs2_release_all_quadratic_targets(jgs2_solver* s) {
   st = waitObjectiveMirror(s);
   if (st != JGS2_OK) return st;
   for (uint32_t v = 0; v < s->V; ++v) s->hTargets[v].w = 0.f;
-  s->targetCount = 0;
-  return writeObjectives(s, 0, s->V, false, true);
-}
-
-static jgs2_status readVec4(jgs2_solver* s, const float4* dev, float* out, size_t floats, size_t perVertex) {
-  jgs2_status st = usable(s);
-  if (st != JGS2_OK) return st;
-  if (!out || floats < perVertex * s->V)
-    return fail(s, JGS2_INVALID_ARGUMENT, format("output needs %zu floats.", perVertex * s->V));
-  return readRegion(s, dev, sizeof(float) * perVertex * s->V, out);
+  s->scenes[0].targetCount = 0;
+  return writeObjectives(s, 0, 0, s->V, false, true);
 }
 
 jgs2_status jgs2_read_positions(jgs2_solver* s, float* out, size_t floats) {
   if (usable(s) != JGS2_OK) return usable(s);
-  return readVec4(s, s->b.pos[0], out, floats, 4);
+  return readSceneVec4(s, 0, s->b.pos[0], out, floats, 4);
 }
 
 jgs2_status jgs2_read_velocities(jgs2_solver* s, float* out, size_t floats) {
   if (usable(s) != JGS2_OK) return usable(s);
-  return readVec4(s, s->b.velocity, out, floats, 4);
+  return readSceneVec4(s, 0, s->b.velocity, out, floats, 4);
 }
 
 jgs2_status jgs2_read_predicted_positions(jgs2_solver* s, float* out, size_t floats) {
   if (usable(s) != JGS2_OK) return usable(s);
-  const jgs2_status st = readVec4(s, s->b.predicted, out, floats, 4);
+  const jgs2_status st = readSceneVec4(s, 0, s->b.predicted, out, floats, 4);
   if (st != JGS2_OK) return st;
   // The device copy keeps the distributed inertia weight in w.
   for (uint32_t v = 0; v < s->V; ++v) out[4ull * v + 3] = 1.0f;
@@ -1363,7 +1516,7 @@ jgs2_status jgs2_read_final_iteration_updates(jgs2_solver* s, float* out, size_t
   std::vector<float> u(s->V);
   st = readRegion(s, s->b.finalUpdate, sizeof(float) * s->V, u.data());
   if (st != JGS2_OK) return st;
-  const float w = s->submittedIterations > 0 ? 1.f : 0.f;
+  const float w = s->scenes[0].submittedIterations > 0 ? 1.f : 0.f;
   for (uint32_t v = 0; v < s->V; ++v) {
     out[4ull * v] = u[v];
     out[4ull * v + 1] = 0.f;
@@ -1375,7 +1528,7 @@ jgs2_status jgs2_read_final_iteration_updates(jgs2_solver* s, float* out, size_t
 
 jgs2_status jgs2_read_vertex_rotations(jgs2_solver* s, float* out, size_t floats) {
   if (usable(s) != JGS2_OK) return usable(s);
-  return readVec4(s, s->b.vertexRot, out, floats, 12);
+  return readSceneVec4(s, 0, s->b.vertexRot, out, floats, 12);
 }
 
 jgs2_status jgs2_read_globalization(jgs2_solver* s, float* local, size_t localFloats, float* control,
@@ -1385,30 +1538,7 @@ jgs2_status jgs2_read_globalization(jgs2_solver* s, float* local, size_t localFl
   if (!s->glob)
     return fail(s, JGS2_UNSUPPORTED,
                 "Globalization diagnostics are available only for stable Neo-Hookean production solves.");
-  if (!s->recordsAvailable)
-    return fail(s, JGS2_NOT_READY,
-                "Globalization diagnostics are unavailable until a stable nonlinear iteration or diagnostic test "
-                "kernel has produced records.");
-  if (local) {
-    if (localFloats < 16ull * s->V) return fail(s, JGS2_INVALID_ARGUMENT, "local output too small.");
-    st = readRegion(s, s->b.local, sizeof(float) * 16ull * s->V, local);
-    if (st != JGS2_OK) return st;
-  }
-  float4 ctl[4];
-  st = readRegion(s, s->b.frame->control, sizeof(ctl), ctl);
-  if (st != JGS2_OK) return st;
-  if (control) std::memcpy(control, ctl, sizeof(ctl));
-  const float raw = ctl[1].w;
-  if (!(raw >= 0 && raw <= float(JGS2_HISTORY_CAPACITY) && raw == std::floor(raw)))
-    return fail(s, JGS2_DEVICE_ERROR, format("GPU returned invalid globalization history count %g.", raw));
-  const uint32_t count = static_cast<uint32_t>(raw);
-  if (historyCount) *historyCount = count;
-  if (history) {
-    if (historyFloats < 32ull * JGS2_HISTORY_CAPACITY) return fail(s, JGS2_INVALID_ARGUMENT, "history output too small.");
-    st = readRegion(s, s->b.frame->history, sizeof(float) * 32ull * JGS2_HISTORY_CAPACITY, history);
-    if (st != JGS2_OK) return st;
-  }
-  return JGS2_OK;
+  return readSceneGlobalization(s, 0, local, localFloats, control, history, historyFloats, historyCount);
 }
 
 jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* s, const float* source, const float* candidate,
@@ -1426,42 +1556,44 @@ jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* s, const float* sourc
   }
   jgs2_settings settings;
   std::string err;
-  if (!resolve(s->defaults, o, mask, &settings, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
-  const DevParams p = makeParams(s, settings, false);
+  if (!resolve(s->scenes[0].defaults, o, mask, &settings, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
+  s->hParams[0] = makeParams(s, 0, settings, false);
   const Buffers& b = s->b;
+  FrameState* fs = &b.frames[0];
   CUDA_TRY(s, cudaSetDevice(s->device));
-  CUDA_TRY(s, cudaMemcpyAsync(s->dParams, &p, sizeof(p), cudaMemcpyHostToDevice, s->stream));
+  CUDA_TRY(s, cudaMemcpyAsync(s->dParams, &s->hParams[0], sizeof(DevParams), cudaMemcpyHostToDevice, s->stream));
   // posB = source, posA = candidate, predicted = source; local records and
   // the control record cleared (jgs2-solver.ts:2644-2679).
   CUDA_TRY(s, cudaMemcpyAsync(b.pos[1], source, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(s, cudaMemcpyAsync(b.pos[0], candidate, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(s, cudaMemcpyAsync(b.predicted, source, sizeof(float) * n, cudaMemcpyHostToDevice, s->stream));
   CUDA_TRY(s, cudaMemsetAsync(b.local, 0, sizeof(float4) * 4ull * s->V, s->stream));
-  CUDA_TRY(s, cudaMemsetAsync(b.frame->control, 0, sizeof(float4) * 4, s->stream));
+  CUDA_TRY(s, cudaMemsetAsync(fs->control, 0, sizeof(float4) * 4, s->stream));
   // The sweep aggregates the gate reads, as a cleared record per vertex
   // gives them: status 0 (accepted) with no backtracks and no evaluations,
   // i.e. one skipped trial per vertex and valid numerics.
   const uint32_t aggregates[6] = {0u, 0u, s->V, 0u, 0u, 1u};
   static_assert(offsetof(FrameState, localNumericsValid) - offsetof(FrameState, localFailures) == 20,
                 "sweep aggregates are six consecutive words");
-  CUDA_TRY(s, cudaMemcpyAsync(&b.frame->localFailures, aggregates, sizeof(aggregates), cudaMemcpyHostToDevice,
+  CUDA_TRY(s, cudaMemcpyAsync(&fs->localFailures, aggregates, sizeof(aggregates), cudaMemcpyHostToDevice,
                               s->stream));
-  s->launches += jgs2::launchGate(b, s->dParams, b.pos[1], b.pos[0], s->V, s->T, s->stream);
-  s->launches += jgs2::launchConvergence(b, s->dParams, b.pos[1], b.pos[0], s->V, false, s->stream);
+  s->launches += jgs2::launchGate(b, s->dParams, b.pos[1], b.pos[0], s->stream);
+  s->launches += jgs2::launchConvergence(b, s->dParams, b.pos[1], b.pos[0], false, s->stream);
   CUDA_TRY(s, cudaGetLastError());
-  s->recordsAvailable = true;
-  s->submitted = settings;
-  s->submittedIterations = 1;
+  SceneHost& sc = s->scenes[0];
+  sc.recordsAvailable = true;
+  sc.submitted = settings;
+  sc.submittedIterations = 1;
   if (positionsOut) {
     st = readRegion(s, b.pos[0], sizeof(float) * n, positionsOut);
     if (st != JGS2_OK) return st;
   }
   if (controlOut) {
-    st = readRegion(s, b.frame->control, sizeof(float4) * 4, controlOut);
+    st = readRegion(s, fs->control, sizeof(float4) * 4, controlOut);
     if (st != JGS2_OK) return st;
   }
   if (historyOut) {
-    st = readRegion(s, b.frame->history, sizeof(float4) * 8, historyOut);
+    st = readRegion(s, fs->history, sizeof(float4) * 8, historyOut);
     if (st != JGS2_OK) return st;
   }
   return jgs2_sync(s);
@@ -1498,8 +1630,8 @@ jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* s, const float* source, co
                                             kMaxScratchDevices));
   jgs2_settings settings;
   std::string err;
-  if (!resolve(s->defaults, o, mask, &settings, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
-  const DevParams p = makeParams(s, settings, false);
+  if (!resolve(s->scenes[0].defaults, o, mask, &settings, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
+  const DevParams p = makeParams(s, 0, settings, false);
   CUDA_TRY(s, cudaSetDevice(s->device));
   void* scratch = nullptr;
   {
@@ -1533,5 +1665,125 @@ jgs2_status jgs2_device_positions(jgs2_solver* s, void** ptr, void** stream) {
 }
 
 uint64_t jgs2_kernel_launch_count(const jgs2_solver* s) { return s ? s->launches : 0; }
+
+// ---- batches -------------------------------------------------------------------
+
+jgs2_status jgs2_batch_create(const jgs2_input* const* inputs, uint32_t scene_count, const jgs2_settings* settings,
+                              const uint32_t* masks, int device, jgs2_batch** out) {
+  if (!out) return fail(nullptr, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  *out = nullptr;
+  if (!inputs || scene_count == 0) return fail(nullptr, JGS2_INVALID_ARGUMENT, "A batch needs at least one scene.");
+  std::vector<PreparedScene> prep(scene_count);
+  for (uint32_t i = 0; i < scene_count; ++i) {
+    const jgs2_status st =
+        prepareScene(inputs[i], settings ? &settings[i] : nullptr, masks ? masks[i] : 0u, &prep[i]);
+    if (st != JGS2_OK) {
+      gGlobalError = format("scene %u: %s", i, gGlobalError.c_str());
+      return st;
+    }
+  }
+  std::unique_ptr<jgs2_batch> s(new jgs2_batch());
+  const jgs2_status st = buildEngine(s.get(), prep, device);
+  if (st != JGS2_OK) return st;
+  *out = s.release();
+  return JGS2_OK;
+}
+
+void jgs2_batch_destroy(jgs2_batch* s) {
+  if (!s) return;
+  if (!s->destroyed) {
+    cudaSetDevice(s->device);
+    releaseDevice(s);
+    s->destroyed = true;
+  }
+  delete s;
+}
+
+const char* jgs2_batch_last_error(const jgs2_batch* s) { return s ? s->error.c_str() : gGlobalError.c_str(); }
+
+uint32_t jgs2_batch_scene_count(const jgs2_batch* s) { return s ? static_cast<uint32_t>(s->scenes.size()) : 0u; }
+
+jgs2_status jgs2_batch_step_frames(jgs2_batch* s, uint32_t frames, uint32_t exact_iterations,
+                                   const jgs2_settings* overrides, const uint32_t* masks) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (frames < 1 || frames > JGS2_MAX_BATCH_FRAMES)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("frameCount must be a positive safe integer no greater than %u; got %u.",
+                       JGS2_MAX_BATCH_FRAMES, frames));
+  const uint32_t S = static_cast<uint32_t>(s->scenes.size());
+  std::vector<jgs2_settings> resolved(S);
+  uint32_t iterations = exact_iterations;
+  for (uint32_t i = 0; i < S; ++i) {
+    st = resolveStep(s, i, overrides ? &overrides[i] : nullptr, masks ? masks[i] : 0u, &resolved[i]);
+    if (st != JGS2_OK) {
+      s->error = format("scene %u: %s", i, s->error.c_str());
+      return st;
+    }
+    if (exact_iterations == 0) {
+      // Production stepping: every scene's normalised odd count must agree.
+      const uint32_t it = normalizeOdd(resolved[i].iterations);
+      if (i == 0) iterations = it;
+      else if (it != iterations)
+        return fail(s, JGS2_INVALID_ARGUMENT,
+                    format("All scenes of one batched production step must run the same number of iterations; "
+                           "scene 0 runs %u, scene %u runs %u.", iterations, i, it));
+    }
+  }
+  return runFrames(s, resolved, frames, iterations, exact_iterations == 0);
+}
+
+jgs2_status jgs2_batch_sync(jgs2_batch* s) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_batch_get_info(jgs2_batch* s, uint32_t scene, jgs2_info* out) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (scene >= s->scenes.size()) return fail(s, JGS2_INVALID_ARGUMENT, format("scene %u is out of range.", scene));
+  if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  return sceneInfo(s, scene, out);
+}
+
+jgs2_status jgs2_batch_read_positions(jgs2_batch* s, uint32_t scene, float* out, size_t floats) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (scene >= s->scenes.size()) return fail(s, JGS2_INVALID_ARGUMENT, format("scene %u is out of range.", scene));
+  return readSceneVec4(s, scene, s->b.pos[0], out, floats, 4);
+}
+
+jgs2_status jgs2_batch_read_velocities(jgs2_batch* s, uint32_t scene, float* out, size_t floats) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (scene >= s->scenes.size()) return fail(s, JGS2_INVALID_ARGUMENT, format("scene %u is out of range.", scene));
+  return readSceneVec4(s, scene, s->b.velocity, out, floats, 4);
+}
+
+jgs2_status jgs2_batch_read_globalization(jgs2_batch* s, uint32_t scene, float* local, size_t local_floats,
+                                          float* control, float* history, size_t history_floats,
+                                          uint32_t* history_count) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (scene >= s->scenes.size()) return fail(s, JGS2_INVALID_ARGUMENT, format("scene %u is out of range.", scene));
+  return readSceneGlobalization(s, scene, local, local_floats, control, history, history_floats, history_count);
+}
+
+jgs2_status jgs2_batch_read_all_positions(jgs2_batch* s, float* out, size_t floats) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out || floats < 4ull * s->V)
+    return fail(s, JGS2_INVALID_ARGUMENT, format("output needs %llu floats.", 4ull * s->V));
+  return readRegion(s, s->b.pos[0], sizeof(float4) * s->V, out);
+}
+
+uint64_t jgs2_batch_kernel_launch_count(const jgs2_batch* s) { return s ? s->launches : 0; }
+
+uint32_t jgs2_batch_vertex_count(const jgs2_batch* s) { return s ? s->V : 0u; }
+
+void* jgs2_batch_stream(const jgs2_batch* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
 
 }  // extern "C"

@@ -211,6 +211,29 @@ def step_lib() -> ctypes.CDLL:
                                                           POINTER(c_float), POINTER(c_float), POINTER(c_float)]
         lib.jgs2_kernel_launch_count.argtypes = [vp]
         lib.jgs2_kernel_launch_count.restype = c_uint64
+        lib.jgs2_batch_create.argtypes = [POINTER(POINTER(Input)), c_uint32, S, POINTER(c_uint32), c_int,
+                                          POINTER(vp)]
+        lib.jgs2_batch_destroy.argtypes = [vp]
+        lib.jgs2_batch_destroy.restype = None
+        lib.jgs2_batch_last_error.argtypes = [vp]
+        lib.jgs2_batch_last_error.restype = c_char_p
+        lib.jgs2_batch_scene_count.argtypes = [vp]
+        lib.jgs2_batch_scene_count.restype = c_uint32
+        lib.jgs2_batch_vertex_count.argtypes = [vp]
+        lib.jgs2_batch_vertex_count.restype = c_uint32
+        lib.jgs2_batch_step_frames.argtypes = [vp, c_uint32, c_uint32, S, POINTER(c_uint32)]
+        lib.jgs2_batch_sync.argtypes = [vp]
+        lib.jgs2_batch_get_info.argtypes = [vp, c_uint32, POINTER(Info)]
+        for name in ("jgs2_batch_read_positions", "jgs2_batch_read_velocities"):
+            getattr(lib, name).argtypes = [vp, c_uint32, POINTER(c_float), c_size_t]
+        lib.jgs2_batch_read_globalization.argtypes = [vp, c_uint32, POINTER(c_float), c_size_t,
+                                                      POINTER(c_float), POINTER(c_float), c_size_t,
+                                                      POINTER(c_uint32)]
+        lib.jgs2_batch_read_all_positions.argtypes = [vp, POINTER(c_float), c_size_t]
+        lib.jgs2_batch_kernel_launch_count.argtypes = [vp]
+        lib.jgs2_batch_kernel_launch_count.restype = c_uint64
+        lib.jgs2_batch_stream.argtypes = [vp]
+        lib.jgs2_batch_stream.restype = c_void_p
         _step_lib = lib
     return _step_lib
 

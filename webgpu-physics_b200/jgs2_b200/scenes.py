@@ -128,6 +128,61 @@ class SceneInput:
     def active_vertex_count(self) -> int:
         return int(np.count_nonzero(self.vertex_info.reshape(-1, 4)[:, 2] == 0))
 
+    def split_bodies(self) -> list:
+        """One SceneInput per body.  Bodies are disjoint meshes whose vertices
+        and tets are contiguous (as the scene builder lays them out), so each
+        body's slice, re-indexed to start at zero, is a complete scene with
+        the same rest data and cubature records it had in the whole."""
+        info = self.vertex_info.reshape(-1, 4)
+        tets = self.tet_indices.reshape(-1, 4)
+        body_of_vertex = info[:, 3]
+        bodies = np.unique(body_of_vertex)
+        body_of_tet = body_of_vertex[tets[:, 0]] if self.tet_count else np.zeros(0, np.uint32)
+        K = self.cubature_k
+        out = []
+        for b in bodies:
+            vs = np.flatnonzero(body_of_vertex == b)
+            ts = np.flatnonzero(body_of_tet == b)
+            v0, v1 = int(vs[0]), int(vs[-1]) + 1
+            t0, t1 = (int(ts[0]), int(ts[-1]) + 1) if ts.size else (0, 0)
+            if v1 - v0 != vs.size or t1 - t0 != ts.size:
+                raise ValueError(f"body {b} is not contiguous")
+            bi = info[v0:v1].copy()
+            a0 = int(bi[:, 0].min()) if bi[:, 1].any() else 0
+            a1 = int((bi[:, 0] + bi[:, 1]).max())
+            bi[:, 0] -= a0
+            bi[:, 3] = 0
+            adj = self.adjacency[a0:a1].astype(np.int64) - t0
+            if adj.size and (adj.min() < 0 or adj.max() >= t1 - t0):
+                raise ValueError(f"body {b} has adjacency outside its tets")
+            cub = self.cubature_tet_ids[v0 * K:v1 * K].astype(np.int64)
+            empty = cub == 0xFFFFFFFF
+            cub = np.where(empty, cub, cub - t0)
+            if (~empty).any() and (cub[~empty].min() < 0 or cub[~empty].max() >= t1 - t0):
+                raise ValueError(f"body {b} has cubature records outside its tets")
+
+            def vs4(a, per):
+                return None if a is None else a[v0 * per:v1 * per].copy()
+
+            out.append(SceneInput(
+                vertex_count=v1 - v0, tet_count=t1 - t0, cubature_k=K,
+                positions=vs4(self.positions, 4), vertex_rest=vs4(self.vertex_rest, 4),
+                vertex_info=bi.reshape(-1).astype(np.uint32),
+                tet_indices=(tets[t0:t1].astype(np.int64) - v0).astype(np.uint32).reshape(-1),
+                tet_inverse_dm=self.tet_inverse_dm[t0 * 12:t1 * 12].copy(),
+                tet_meta=self.tet_meta[t0 * 4:t1 * 4].copy(),
+                adjacency=adj.astype(np.uint32),
+                cubature_tet_ids=cub.astype(np.uint32),
+                cubature_weights=self.cubature_weights[v0 * K:v1 * K].copy(),
+                cubature_basis=self.cubature_basis[v0 * K * 36:v1 * K * 36].copy(),
+                velocities=vs4(self.velocities, 4), vertex_colors=vs4(self.vertex_colors, 4),
+                tet_rest_stiffness=(None if self.tet_rest_stiffness is None
+                                    else self.tet_rest_stiffness[t0 * 144:t1 * 144].copy()),
+                external_forces=vs4(self.external_forces, 3), target_positions=vs4(self.target_positions, 3),
+                target_stiffnesses=vs4(self.target_stiffnesses, 1),
+                rest_positions=None if self.rest_positions is None else self.rest_positions[v0:v1].copy()))
+        return out
+
 
 class Scene:
     """Owner of a native jgs2_scene handle (include/jgs2_scene.h)."""
@@ -285,6 +340,12 @@ def single_tetrahedron(timestep=1 / 60, cubature_k=4) -> SceneInput:
     sc.add_mesh([0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1], [0, 1, 2, 3], m, pinned=[1, 0, 0, 0])
     sc.precompute(timestep=timestep, cubature_k=cubature_k)
     return sc.pack()
+
+
+def batched_scenes(count=256, **kwargs) -> list:
+    """The batched uneven bodies of `batched_bodies`, one independent scene
+    per body (their cubature training is shared across identical patches)."""
+    return batched_bodies(count=count, **kwargs).split_bodies()
 
 
 def cantilever_target(inp: SceneInput, frame: int, lift=0.15, stiffness=1000.0):

@@ -359,3 +359,132 @@ class JGS2GpuSolver:
         n = int(count.value)
         return {"local": local.reshape(-1, 16), "control": control,
                 "history": history.reshape(64, 32)[:n], "historyCount": n}
+
+
+class JGS2Batch:
+    """Many independent scenes stepped together (include/jgs2.h, batched form).
+
+    Each scene keeps the solver's semantics (own settings, own assembled gate,
+    convergence history and stop latch); `stepFrames` advances all of them with
+    one launch sequence.  Per-scene reads mirror JGS2GpuSolver's."""
+
+    def __init__(self, handle, lib, vertex_counts):
+        self._h = handle
+        self._L = lib
+        self.vertexCounts = list(vertex_counts)
+        self._destroyed = False
+
+    @classmethod
+    def create(cls, scene_inputs, settings=None, device: int = 0) -> "JGS2Batch":
+        """settings: None, one dict for every scene, or a list of dicts."""
+        L = _ffi.step_lib()
+        n = len(scene_inputs)
+        if n == 0:
+            raise JGS2RangeError(1, "A batch needs at least one scene.")
+        recs = [inp.as_ctypes() for inp in scene_inputs]
+        ptrs = (ctypes.POINTER(_ffi.Input) * n)(*[ctypes.pointer(r) for r in recs])
+        per = settings if isinstance(settings, (list, tuple)) else [settings] * n
+        structs = (_ffi.Settings * n)()
+        masks = (c_uint32 * n)()
+        for i, o in enumerate(per):
+            s, m = settings_struct(o)
+            structs[i] = s
+            masks[i] = m
+        h = c_void_p()
+        st = L.jgs2_batch_create(ptrs, n, structs, masks, int(device), byref(h))
+        if st != 0:
+            _raise(st, L.jgs2_global_last_error().decode())
+        return cls(h, L, [inp.vertex_count for inp in scene_inputs])
+
+    def destroy(self):
+        if not self._destroyed and self._h:
+            self._L.jgs2_batch_destroy(self._h)
+        self._destroyed = True
+        self._h = None
+
+    def __del__(self):
+        try:
+            self.destroy()
+        except Exception:
+            pass
+
+    def _check(self, st):
+        if st != 0:
+            msg = self._L.jgs2_batch_last_error(self._h).decode() if self._h else "destroyed"
+            _raise(st, msg)
+
+    def _usable(self):
+        if self._destroyed:
+            raise JGS2RangeError(6, "JGS2 batch has been destroyed.")
+
+    @property
+    def sceneCount(self) -> int:
+        return len(self.vertexCounts)
+
+    def kernelLaunchCount(self) -> int:
+        return int(self._L.jgs2_batch_kernel_launch_count(self._h)) if self._h else 0
+
+    def stream(self) -> int:
+        """The batch's cudaStream_t as an integer handle."""
+        self._usable()
+        return int(self._L.jgs2_batch_stream(self._h) or 0)
+
+    def stepFrames(self, frameCount: int = 1, exactIterations: int = 0, overrides=None):
+        """exactIterations 0: production step; overrides: None, a dict for
+        every scene, or a list of dicts."""
+        self._usable()
+        n = self.sceneCount
+        per = overrides if isinstance(overrides, (list, tuple)) else [overrides] * n
+        structs = (_ffi.Settings * n)()
+        masks = (c_uint32 * n)()
+        for i, o in enumerate(per):
+            s, m = settings_struct(o)
+            structs[i] = s
+            masks[i] = m
+        self._check(self._L.jgs2_batch_step_frames(self._h, int(frameCount), int(exactIterations), structs, masks))
+
+    def awaitIdle(self):
+        self._usable()
+        self._check(self._L.jgs2_batch_sync(self._h))
+
+    def info(self, scene: int) -> dict:
+        self._usable()
+        out = _ffi.Info()
+        self._check(self._L.jgs2_batch_get_info(self._h, int(scene), byref(out)))
+        return {name: getattr(out, name) for name, _t in _ffi.Info._fields_}
+
+    def _read(self, fn, scene, per_vertex):
+        self._usable()
+        out = np.empty(per_vertex * self.vertexCounts[scene], dtype=np.float32)
+        self._check(fn(self._h, int(scene), _ffi.fptr(out), out.size))
+        return out
+
+    def readPositions(self, scene: int) -> np.ndarray:
+        return self._read(self._L.jgs2_batch_read_positions, scene, 4)
+
+    def readVelocities(self, scene: int) -> np.ndarray:
+        return self._read(self._L.jgs2_batch_read_velocities, scene, 4)
+
+    def readAllPositions(self, out: Optional[np.ndarray] = None) -> np.ndarray:
+        self._usable()
+        total = 4 * sum(self.vertexCounts)
+        if out is None:
+            out = np.empty(total, dtype=np.float32)
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size < total:
+            raise JGS2RangeError(1, "out must be a contiguous float32 array with 4 floats per vertex.")
+        self._check(self._L.jgs2_batch_read_all_positions(self._h, _ffi.fptr(out), out.size))
+        return out
+
+    def readGlobalizationDiagnostics(self, scene: int) -> dict:
+        self._usable()
+        V = self.vertexCounts[scene]
+        local = np.empty(16 * V, dtype=np.float32)
+        control = np.empty(16, dtype=np.float32)
+        history = np.empty(32 * 64, dtype=np.float32)
+        count = c_uint32(0)
+        self._check(self._L.jgs2_batch_read_globalization(self._h, int(scene), _ffi.fptr(local), local.size,
+                                                          _ffi.fptr(control), _ffi.fptr(history), history.size,
+                                                          byref(count)))
+        n = int(count.value)
+        return {"local": local.reshape(-1, 16), "control": control,
+                "history": history.reshape(64, 32)[:n], "historyCount": n}
