@@ -385,7 +385,9 @@ uint32_t jgs2_batch_vertex_count(const jgs2_batch* batch);
  * that many iterations per frame (stepFramesExactIterations); 0 runs the
  * production step (odd-normalised iteration count with the stop latch), and
  * then every scene's normalised count must agree.  overrides / masks: NULL or
- * one per scene.  All scenes must use the same schedule. */
+ * one per scene.  All scenes must use the same schedule; a batch steps with the
+ * graph-coloured schedule only if one of its scenes had that schedule at
+ * creation (the colouring is built then). */
 jgs2_status jgs2_batch_step_frames(jgs2_batch* batch, uint32_t frames, uint32_t exact_iterations,
                                    const jgs2_settings* overrides, const uint32_t* masks);
 jgs2_status jgs2_batch_sync(jgs2_batch* batch);
@@ -401,6 +403,11 @@ jgs2_status jgs2_batch_read_all_positions(jgs2_batch* batch, float* out, size_t 
 uint64_t jgs2_batch_kernel_launch_count(const jgs2_batch* batch);
 /* The batch's CUDA stream (a cudaStream_t), for event timing and ordering. */
 void* jgs2_batch_stream(const jgs2_batch* batch);
+/* An inactive scene sits every following frame out: its state stays as it
+ * is until it is made active again (used to retire finished requests). */
+jgs2_status jgs2_batch_set_scene_active(jgs2_batch* batch, uint32_t scene, uint32_t active);
+/* Device bytes a scene occupies once packed (the serving admission estimate). */
+uint64_t jgs2_estimate_device_bytes(const jgs2_input* input);
 
 #ifdef __cplusplus
 }

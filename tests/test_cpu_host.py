@@ -19,7 +19,8 @@ def _declared(header):
     return sorted(set(re.findall(r"\b(jgs2_[a-z0-9_]+)\s*\(", text)))
 
 
-@pytest.mark.parametrize("header,lib", [("jgs2.h", "libjgs2.so"), ("jgs2_scene.h", "libjgs2_scene.so")])
+@pytest.mark.parametrize("header,lib", [("jgs2.h", "libjgs2.so"), ("jgs2_server.h", "libjgs2.so"),
+                                        ("jgs2_scene.h", "libjgs2_scene.so")])
 def test_library_exports_every_declared_symbol(header, lib):
     cdll = ctypes.CDLL(os.path.join(_ffi.LIB_DIR, lib))
     missing = [name for name in _declared(header) if not hasattr(cdll, name)]

@@ -281,14 +281,15 @@ __global__ void __launch_bounds__(kBlock) vertexPolarKernel(Buffers b, const Dev
   const uint32_t v = list ? list[i] : i;
   const uint32_t scene = b.vertexScene[v];
   const DevParams& p = pp[scene];
-  if (latched(p, &b.frames[scene])) return;
+  if (!p.active || latched(p, &b.frames[scene])) return;
   storeRot(b.vertexRot, v, vertexFrame(b, x, v, p.rotationEpsilon));
 }
 
-__global__ void __launch_bounds__(kBlock) copyKernel(const float4* __restrict__ src, float4* __restrict__ dst,
+__global__ void __launch_bounds__(kBlock) copyKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                     const float4* __restrict__ src, float4* __restrict__ dst,
                                                      uint32_t V) {
   const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
-  if (i < V) {
+  if (i < V && pp[b.vertexScene[i]].active) {
     const float4 s = src[i];
     dst[i] = make_float4(s.x, s.y, s.z, 1.0f);
   }
@@ -344,7 +345,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
   uint32_t status = kNonfinite, backtracks = 0, evals = 0;
   float shiftN = 0.0f;
   bool localValid = true, haveRecord = false;
-  if (haveVertex) {
+  if (haveVertex && pp[scene].active) {
     const DevParams p = pp[scene];
     FrameState* fs = &b.frames[scene];
     const bool isLatched = latched(p, fs);
@@ -815,6 +816,7 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
   const RedBlock rb = b.gateTable[blockIdx.x];
   const SceneRange sr = b.scenes[rb.scene];
   const DevParams p = pp[rb.scene];
+  if (!p.active) return;  // uniform across the scene's blocks
   FrameState* fs = &b.frames[rb.scene];
   GatePartial acc = gateIdentity();
   for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
@@ -883,7 +885,7 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
   const SceneRange sr = b.scenes[rb.scene];
   const DevParams p = pp[rb.scene];
   FrameState* fs = &b.frames[rb.scene];
-  if (latched(p, fs)) return;  // uniform across the scene's blocks
+  if (!p.active || latched(p, fs)) return;  // uniform across the scene's blocks
   GatePartial acc = gateIdentity();
   for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
     if (k < sr.T) {
@@ -954,7 +956,7 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
   const SceneRange sr = b.scenes[rb.scene];
   const DevParams p = pp[rb.scene];
   FrameState* fs = &b.frames[rb.scene];
-  if (latched(p, fs)) return;  // uniform across the scene's blocks
+  if (!p.active || latched(p, fs)) return;  // uniform across the scene's blocks
   const bool accepted = fs->control[1].x == 1.0f;
   const float4* __restrict__ acc = accepted ? tgt : src;
   const uint32_t V = sr.V;
@@ -1089,10 +1091,10 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
 // ---------------------------------------------------------------------------
 // Epilogue: even-count copy (copyPosition, :4488-4496), optional body
 // correction (:4498-4551), finalize (:4553-4589).
-__global__ void __launch_bounds__(kBlock) bodyAccumulateKernel(Buffers b, const float4* __restrict__ finalPos,
-                                                               uint32_t V) {
+__global__ void __launch_bounds__(kBlock) bodyAccumulateKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                               const float4* __restrict__ finalPos, uint32_t V) {
   const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
-  if (v >= V) return;
+  if (v >= V || !pp[b.vertexScene[v]].active) return;
   float4 x = finalPos[v];
   if (finalPos != b.pos[0]) b.pos[0][v] = make_float4(x.x, x.y, x.z, 1.0f);
   const uint4 info = b.vinfo[v];
@@ -1117,6 +1119,7 @@ __global__ void __launch_bounds__(kBlock) finalizeKernel(Buffers b, const DevPar
   const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
   if (v >= V) return;
   const DevParams& p = pp[b.vertexScene[v]];
+  if (!p.active) return;
   const uint4 info = b.vinfo[v];
   float4 x = accumulated ? b.pos[0][v] : finalPos[v];
   if (isPinned(info)) {
@@ -1261,8 +1264,8 @@ uint32_t solveGroupsPerBlock(uint32_t K) {
   return groups;
 }
 
-int launchCopy(const float4* src, float4* dst, uint32_t V, cudaStream_t s) {
-  copyKernel<<<blocksFor(V), kBlock, 0, s>>>(src, dst, V);
+int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* dst, uint32_t V, cudaStream_t s) {
+  copyKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, src, dst, V);
   return 1;
 }
 
@@ -1282,7 +1285,7 @@ int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos,
   int n = 0;
   if (bodyCorrection) {
     cudaMemsetAsync(b.bodyAccum, 0, sizeof(double) * 6ull * bodies, s);
-    bodyAccumulateKernel<<<blocksFor(V), kBlock, 0, s>>>(b, finalPos, V);
+    bodyAccumulateKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, finalPos, V);
     ++n;
   }
   finalizeKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, finalPos, V, bodyCorrection ? 1 : 0);

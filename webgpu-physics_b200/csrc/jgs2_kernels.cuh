@@ -24,7 +24,8 @@ struct DevParams {
   uint32_t historyCapacity;
   uint32_t vertexCount, tetCount, cubatureK, bodyCount;
   uint32_t bodyCorrection;  // horizontal body correction in the epilogue
-  uint32_t pad[3];
+  uint32_t active;          // 0: the scene sits this frame out (no state changes)
+  uint32_t pad[2];
 };
 
 // One scene of a batch: its slices of the concatenated vertex and tet arrays
@@ -107,7 +108,7 @@ int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, c
 // gathering them.
 int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
                 uint32_t count, uint32_t K, bool cachedIncident, cudaStream_t s);
-int launchCopy(const float4* src, float4* dst, uint32_t V, cudaStream_t s);
+int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* dst, uint32_t V, cudaStream_t s);
 int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s);
 int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt,
                       bool computeNextRotations, cudaStream_t s);

@@ -18,6 +18,8 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <atomic>
+#include <thread>
 #include <string>
 #include <tuple>
 #include <vector>
@@ -432,6 +434,7 @@ struct SceneHost {
   uint32_t colorCount = 1;
   std::vector<uint32_t> colors;  // scene-local colouring
   uint32_t objectiveFlags = 0, forceCount = 0, targetCount = 0, objectiveRevision = 0;
+  bool active = true;  // an inactive scene sits every frame out
 };
 
 }  // namespace
@@ -446,6 +449,7 @@ struct Engine {
   std::vector<SceneHost> scenes;
   // Colour lists over all scenes: colour c holds every scene's colour-c vertices.
   uint32_t colorCount = 1;
+  bool coloringBuilt = true;  // batches colour their scenes only when a scene asks for GGS2
   std::vector<uint32_t> colorOffsets;  // colorCount + 1 into colorVertices
   std::vector<uint32_t> needOffsets;   // colorCount + 1 into needVertices
   // Objectives: pinned host mirrors of the device force and target arrays
@@ -489,6 +493,24 @@ jgs2_status cudaFail(Engine* s, cudaError_t e, const char* what) {
     cudaError_t _e = (call);                            \
     if (_e != cudaSuccess) return cudaFail((s), _e, #call); \
   } while (0)
+
+// Runs fn(i) for i in [0, n) on up to hardware-concurrency threads (host-side
+// scene preparation and packing; every i writes its own outputs).
+template <class F>
+void parallelFor(uint32_t n, F&& fn) {
+  const uint32_t workers = std::min<uint32_t>(n, std::max(1u, std::thread::hardware_concurrency()));
+  if (workers <= 1) {
+    for (uint32_t i = 0; i < n; ++i) fn(i);
+    return;
+  }
+  std::atomic<uint32_t> next{0};
+  std::vector<std::thread> pool;
+  for (uint32_t w = 0; w < workers; ++w)
+    pool.emplace_back([&] {
+      for (uint32_t i = next++; i < n; i = next++) fn(i);
+    });
+  for (auto& t : pool) t.join();
+}
 
 template <class T>
 jgs2_status deviceAlloc(Engine* s, T** out, size_t count) {
@@ -561,6 +583,7 @@ DevParams makeParams(const Engine* s, uint32_t scene, const jgs2_settings& st, b
   p.cubatureK = sc.K;
   p.bodyCount = sc.bodies;
   p.bodyCorrection = st.horizontal_body_correction ? 1u : 0u;
+  p.active = sc.active ? 1u : 0u;
   return p;
 }
 
@@ -614,7 +637,7 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
     float4* tgt = (it % 2 == 0) ? b.pos[0] : b.pos[1];
     const bool last = it + 1 == iterations;
     if (colored) {
-      n += timed(P::kCopy, [&] { return jgs2::launchCopy(src, tgt, s->V, st); });
+      n += timed(P::kCopy, [&] { return jgs2::launchCopy(b, s->dParams, src, tgt, s->V, st); });
       for (uint32_t c = 0; c < s->colorCount; ++c) {
         const uint32_t nb = s->needOffsets[c], ne = s->needOffsets[c + 1];
         n += timed(P::kVertexFrames, [&] {
@@ -658,6 +681,10 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
       return fail(s, JGS2_INVALID_ARGUMENT, "All scenes of one batched step must use the same schedule.");
     body = body || st[i].horizontal_body_correction != 0;
   }
+  if (schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL && !s->coloringBuilt)
+    return fail(s, JGS2_UNSUPPORTED,
+                "This batch was created without graph colouring: give one of its scenes the graph-coloured "
+                "schedule when the batch is created to step it with that schedule.");
   const uint32_t sub = schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL ? s->colorCount : 1u;
   if (static_cast<uint64_t>(iterations) * sub > JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION / frames)
     return fail(s, JGS2_INVALID_ARGUMENT,
@@ -782,9 +809,12 @@ struct PreparedScene {
   jgs2_settings resolved{};
   uint32_t colorCount = 0;
   std::vector<uint32_t> colors;
+  bool colored = false;
+  std::string error;  // message of a failed preparation (thread-safe copy)
 };
 
-jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, uint32_t mask, PreparedScene* out) {
+jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, uint32_t mask, bool colour,
+                         PreparedScene* out) {
   std::string err;
   if (!validateInput(in, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
   // inferJGS2MaterialMode (layout.ts:509-522).
@@ -799,7 +829,8 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
                 "The co-rotated regression material path is not built into this library; use stable Neo-Hookean "
                 "tetrahedra.");
   out->in = in;
-  out->colors = colorInput(in, &out->colorCount);
+  out->colored = colour;
+  if (colour) out->colors = colorInput(in, &out->colorCount);
   if (out->colorCount > JGS2_MAX_SCHEDULE_COLORS)
     return fail(nullptr, JGS2_INVALID_ARGUMENT,
                 format("Colored Gauss-Seidel supports at most %u colors; the small-scene conflict graph needs %u.",
@@ -859,7 +890,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     sc.submitted = prep[i].resolved;
     sc.preprocessingTimestep = prep[i].resolved.timestep;
     sc.colors = prep[i].colors;
-    sc.colorCount = prep[i].colorCount;
+    sc.colorCount = prep[i].colored ? prep[i].colorCount : 0u;
     sc.sceneScale = initialSceneScale(in);
     V += sc.V;
     T += sc.T;
@@ -873,13 +904,16 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   sp->T = static_cast<uint32_t>(T);
   sp->K = K;
   sp->bodies = static_cast<uint32_t>(bodies);
+  sp->coloringBuilt = true;
+  for (const PreparedScene& p : prep) sp->coloringBuilt = sp->coloringBuilt && p.colored;
+  if (!sp->coloringBuilt) colorCount = 0;
   sp->colorCount = colorCount;
   const uint32_t nV = sp->V, nT = sp->T;
 
   // Objectives (packJGS2VertexObjectives, layout.ts:635-668).
   std::vector<float4> initialForces(nV), initialTargets(nV);
   sp->pinned.assign(nV, 0);
-  for (uint32_t i = 0; i < S; ++i) {
+  parallelFor(S, [&](uint32_t i) {
     const jgs2_input* in = prep[i].in;
     SceneHost& sc = sp->scenes[i];
     sc.forceCount = sc.targetCount = 0;
@@ -894,14 +928,14 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       sp->pinned[g] = in->vertex_info[4ull * v + 2] != 0;
     }
     refreshObjectiveFlags(sc);
-  }
+  });
 
   // Colour lists (union over scenes) and per-colour frame lists.
   std::vector<uint32_t> byColor;
   std::vector<uint32_t> need;
   sp->colorOffsets.assign(colorCount + 1, 0);
   sp->needOffsets.assign(colorCount + 1, 0);
-  {
+  if (sp->coloringBuilt) {
     std::vector<uint32_t> mark(nV, 0xffffffffu);
     for (uint32_t c = 0; c < colorCount; ++c) {
       std::vector<uint32_t> needList;
@@ -949,7 +983,10 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   // Tet record: rows of inverse Dm (shape gradients g1..g3) with volume,
   // lambda, mu in w, then the four (global) indices.
   std::vector<float4> tets(4ull * nT);
-  std::vector<uint32_t> adjacency;
+  std::vector<uint32_t> adjacencyOffsets(S + 1, 0);
+  for (uint32_t i = 0; i < S; ++i)
+    adjacencyOffsets[i + 1] = adjacencyOffsets[i] + static_cast<uint32_t>(prep[i].in->adjacency_length);
+  std::vector<uint32_t> adjacency(adjacencyOffsets[S]);
   const size_t R = static_cast<size_t>(nV) * K;
   // Record headers: tet id and weight, then the tet's vertex indices, so a
   // record's vertex data can be fetched without waiting for its tet.  Scenes
@@ -957,10 +994,10 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   std::vector<uint4> head(2 * R, make_uint4(kEmptyTet, 0u, 0u, 0u));
   for (size_t r = 0; r < R; ++r) head[2 * r + 1] = make_uint4(0u, 0u, 0u, 0u);
   std::vector<float> basis(36 * R, 0.f);
-  for (uint32_t i = 0; i < S; ++i) {
+  parallelFor(S, [&](uint32_t i) {
     const jgs2_input* in = prep[i].in;
     const SceneHost& sc = sp->scenes[i];
-    const uint32_t adjOff = static_cast<uint32_t>(adjacency.size());
+    const uint32_t adjOff = adjacencyOffsets[i];
     for (uint32_t v = 0; v < sc.V; ++v) {
       const uint32_t g = sc.vOff + v;
       pos[g] = make_float4(in->positions[4ull * v], in->positions[4ull * v + 1], in->positions[4ull * v + 2], 1.f);
@@ -971,7 +1008,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       if (in->velocities)
         vel[g] = make_float4(in->velocities[4ull * v], in->velocities[4ull * v + 1], in->velocities[4ull * v + 2], 0.f);
       vertexScene[g] = i;
-      colors[g] = sc.colors[v];
+      colors[g] = sc.colors.empty() ? 0u : sc.colors[v];
     }
     for (uint32_t t = 0; t < sc.T; ++t) {
       const float* m = &in->tet_inverse_dm[12ull * t];
@@ -984,7 +1021,6 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
                                  sc.vOff + in->tet_indices[4ull * t + 2], sc.vOff + in->tet_indices[4ull * t + 3]);
       std::memcpy(&tets[4 * g + 3], &q, sizeof(q));
     }
-    adjacency.resize(adjOff + in->adjacency_length);
     for (uint32_t v = 0; v < sc.V; ++v) {
       const uint32_t start = in->vertex_info[4ull * v], count = in->vertex_info[4ull * v + 1];
       for (uint32_t a = 0; a < count; ++a) {
@@ -1011,7 +1047,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
         std::memcpy(&basis[36 * dst], &in->cubature_basis[36 * src], sizeof(float) * 36);
       }
     }
-  }
+  });
   // Segmented reduction tables: each scene's elements in fixed chunks.
   std::vector<jgs2::SceneRange> ranges(S);
   std::vector<jgs2::RedBlock> gateTable, convTable;
@@ -1267,7 +1303,7 @@ jgs2_status jgs2_create(const jgs2_input* in, const jgs2_settings* settings, uin
   if (!out) return fail(nullptr, JGS2_INVALID_ARGUMENT, "out is NULL.");
   *out = nullptr;
   std::vector<PreparedScene> prep(1);
-  jgs2_status st = prepareScene(in, settings, mask, &prep[0]);
+  jgs2_status st = prepareScene(in, settings, mask, true, &prep[0]);
   if (st != JGS2_OK) return st;
   std::unique_ptr<jgs2_solver> s(new jgs2_solver());
   st = buildEngine(s.get(), prep, device);
@@ -1673,13 +1709,26 @@ jgs2_status jgs2_batch_create(const jgs2_input* const* inputs, uint32_t scene_co
   if (!out) return fail(nullptr, JGS2_INVALID_ARGUMENT, "out is NULL.");
   *out = nullptr;
   if (!inputs || scene_count == 0) return fail(nullptr, JGS2_INVALID_ARGUMENT, "A batch needs at least one scene.");
-  std::vector<PreparedScene> prep(scene_count);
+  // Graph colouring is built only when some scene's default schedule needs it.
+  bool colour = false;
   for (uint32_t i = 0; i < scene_count; ++i) {
-    const jgs2_status st =
-        prepareScene(inputs[i], settings ? &settings[i] : nullptr, masks ? masks[i] : 0u, &prep[i]);
-    if (st != JGS2_OK) {
-      gGlobalError = format("scene %u: %s", i, gGlobalError.c_str());
-      return st;
+    jgs2_settings base, resolved;
+    defaults(&base);
+    std::string err;
+    if (resolve(base, settings ? &settings[i] : nullptr, masks ? masks[i] : 0u, &resolved, &err) &&
+        resolved.schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL)
+      colour = true;
+  }
+  std::vector<PreparedScene> prep(scene_count);
+  std::vector<jgs2_status> status(scene_count, JGS2_OK);
+  parallelFor(scene_count, [&](uint32_t i) {
+    status[i] = prepareScene(inputs[i], settings ? &settings[i] : nullptr, masks ? masks[i] : 0u, colour, &prep[i]);
+    if (status[i] != JGS2_OK) prep[i].error = gGlobalError;  // this worker's thread-local message
+  });
+  for (uint32_t i = 0; i < scene_count; ++i) {
+    if (status[i] != JGS2_OK) {
+      gGlobalError = format("scene %u: %s", i, prep[i].error.c_str());
+      return status[i];
     }
   }
   std::unique_ptr<jgs2_batch> s(new jgs2_batch());
@@ -1785,5 +1834,24 @@ uint64_t jgs2_batch_kernel_launch_count(const jgs2_batch* s) { return s ? s->lau
 uint32_t jgs2_batch_vertex_count(const jgs2_batch* s) { return s ? s->V : 0u; }
 
 void* jgs2_batch_stream(const jgs2_batch* s) { return s ? static_cast<void*>(s->stream) : nullptr; }
+
+jgs2_status jgs2_batch_set_scene_active(jgs2_batch* s, uint32_t scene, uint32_t active) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (scene >= s->scenes.size()) return fail(s, JGS2_INVALID_ARGUMENT, format("scene %u is out of range.", scene));
+  s->scenes[scene].active = active != 0;
+  return JGS2_OK;
+}
+
+uint64_t jgs2_estimate_device_bytes(const jgs2_input* in) {
+  if (!in) return 0;
+  const uint64_t V = in->vertex_count, T = in->tet_count, K = in->cubature_k;
+  // Per vertex: two position buffers, predicted, velocity, old, frame (3),
+  // local records (4), incident system (3), rest/mass, info, force, target
+  // (16 bytes each), final update, colour, scene id; per record a 32-byte
+  // header and 144 bytes of basis; per tet a 64-byte record, four adjacency
+  // entries and a share of the reduction partials.
+  return V * (16 * 20 + 12) + V * K * (32 + 144) + T * (64 + 16 + 1) + (1u << 16);
+}
 
 }  // extern "C"

@@ -93,6 +93,28 @@ class KernelProfile(Structure):
     ]
 
 
+class ServerOptions(Structure):
+    _fields_ = [("device", c_int), ("memory_budget_bytes", c_uint64), ("max_scenes_per_wave", c_uint32),
+                ("max_waves", c_uint32)]
+
+
+class RequestResult(Structure):
+    _fields_ = [
+        ("id", c_uint64), ("status", c_int), ("frames", c_uint32), ("vertex_count", c_uint32),
+        ("wave_scenes", c_uint32), ("submit_seconds", c_double), ("admit_seconds", c_double),
+        ("finish_seconds", c_double), ("mean_frame_ms", c_double), ("max_frame_ms", c_double),
+    ]
+
+
+class ServerStats(Structure):
+    _fields_ = [
+        ("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64),
+        ("waves_created", c_uint64), ("rounds", c_uint64),
+        ("resident_bytes", c_uint64), ("peak_resident_bytes", c_uint64),
+        ("waves_in_flight", c_uint32), ("queued", c_uint32), ("busy_seconds", c_double),
+    ]
+
+
 class PrecomputeOptions(Structure):
     _fields_ = [
         ("timestep", c_double), ("cubature_k", c_uint32), ("method", c_uint32),
@@ -234,6 +256,19 @@ def step_lib() -> ctypes.CDLL:
         lib.jgs2_batch_kernel_launch_count.restype = c_uint64
         lib.jgs2_batch_stream.argtypes = [vp]
         lib.jgs2_batch_stream.restype = c_void_p
+        lib.jgs2_batch_set_scene_active.argtypes = [vp, c_uint32, c_uint32]
+        lib.jgs2_estimate_device_bytes.argtypes = [POINTER(Input)]
+        lib.jgs2_estimate_device_bytes.restype = c_uint64
+        lib.jgs2_server_create.argtypes = [POINTER(ServerOptions), POINTER(vp)]
+        lib.jgs2_server_destroy.argtypes = [vp]
+        lib.jgs2_server_destroy.restype = None
+        lib.jgs2_server_last_error.argtypes = [vp]
+        lib.jgs2_server_last_error.restype = c_char_p
+        lib.jgs2_server_submit.argtypes = [vp, POINTER(Input), S, c_uint32, c_uint32, c_uint32, POINTER(c_uint64)]
+        lib.jgs2_server_wait.argtypes = [vp, c_uint64, POINTER(c_float), c_size_t, POINTER(c_float), c_size_t,
+                                         POINTER(RequestResult)]
+        lib.jgs2_server_drain.argtypes = [vp]
+        lib.jgs2_server_get_stats.argtypes = [vp, POINTER(ServerStats)]
         _step_lib = lib
     return _step_lib
 

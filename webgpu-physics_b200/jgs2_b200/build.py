@@ -56,23 +56,23 @@ def _stale(target, sources) -> bool:
 def build_step_library(force=False, verbose=False) -> str:
     os.makedirs(LIB, exist_ok=True)
     target = os.path.join(LIB, "libjgs2.so")
-    sources = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cu", "jgs2_runtime.cpp")]
+    sources = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cu", "jgs2_runtime.cpp", "jgs2_server.cpp")]
     headers = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cuh", "jgs2_device.cuh")] + [
-        os.path.join(INCLUDE, "jgs2.h")]
+        os.path.join(INCLUDE, f) for f in ("jgs2.h", "jgs2_server.h")]
     if not force and not _stale(target, sources + headers):
         return target
     nvcc = _nvcc()
     objs = []
     for src in sources:
         obj = os.path.join(LIB, os.path.basename(src) + ".o")
-        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-I", INCLUDE, "-I", CSRC,
-               "-c", src, "-o", obj]
+        cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-pthread", "-I", INCLUDE,
+               "-I", CSRC, "-c", src, "-o", obj]
         if src.endswith(".cpp"):
             cmd.insert(1, "-x")
             cmd.insert(2, "cu")
         _run(cmd, verbose)
         objs.append(obj)
-    _run([nvcc, *ARCH, "-shared", "-o", target, *objs, "-lcudart"], verbose)
+    _run([nvcc, *ARCH, "-shared", "-o", target, *objs, "-lcudart", "-Xcompiler", "-pthread"], verbose)
     for obj in objs:
         os.remove(obj)
     return target
