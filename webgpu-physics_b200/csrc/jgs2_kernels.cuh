@@ -43,7 +43,7 @@ struct RedBlock {
   uint32_t scene, begin, end, slot;
 };
 constexpr uint32_t kGateChunk = 2048;  // tets / vertices per prologue or gate block
-constexpr uint32_t kConvChunk = 1024;  // vertices per convergence block
+constexpr uint32_t kConvChunk = 256;   // vertices per convergence block
 
 // Reduction scratch and the GPU-resident control/history records
 // (dynamic arena regions globalizationControl/globalizationHistory,
