@@ -285,6 +285,216 @@ __global__ void __launch_bounds__(kBlock) vertexPolarKernel(Buffers b, const Dev
   storeRot(b.vertexRot, v, vertexFrame(b, x, v, p.rotationEpsilon));
 }
 
+// ---------------------------------------------------------------------------
+// Co-rotated linear path (the reference's legacy co-rotated branches of
+// jgs2Solve and tetPolarRotation, jgs2-shader.ts:2931-2957, 2991-3263,
+// 2479-2512).  No globalization: each vertex takes a regularised Newton step
+// clamped to maxStep, and no gate or convergence pass follows.
+
+// Tet frames: polar of each co-rotated tet's deformation gradient.
+__global__ void __launch_bounds__(kBlock) tetPolarKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                         const float4* __restrict__ x, uint32_t T) {
+  const uint32_t t = blockIdx.x * kBlock + threadIdx.x;
+  if (t >= T) return;
+  const DevParams& p = pp[b.tetScene[t]];
+  if (!p.active) return;
+  const TetRec r = loadTet(b.tets, t);
+  storeRot(b.tetRot, t, polarRotation(deformationAt(r, x), p.rotationEpsilon));
+}
+
+// Block (rv, cv) of a tet's 12 x 12 row-major rest stiffness, as columns.
+__device__ __forceinline__ M3 stiffnessBlock(const float* __restrict__ k, uint32_t rv, uint32_t cv) {
+  const float* r0 = k + (3 * rv) * 12 + 3 * cv;
+  const float* r1 = r0 + 12;
+  const float* r2 = r1 + 12;
+  return {f3(r0[0], r1[0], r2[0]), f3(r0[1], r1[1], r2[1]), f3(r0[2], r1[2], r2[2])};
+}
+
+// Element gradient of a co-rotated tet at pose x (tetGradient):
+// R K (R^T (x_l - centroid) - (X_l - rest centroid)) per vertex slot.
+__device__ __forceinline__ void corotatedGradient(const Buffers& b, const float4* __restrict__ x, uint32_t t,
+                                                  const uint4& q, const M3& R, float3 out[4]) {
+  float3 cur[4], rest[4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    const uint32_t v = idxAt(q, l);
+    cur[l] = xyz(x[v]);
+    rest[l] = xyz(b.restMass[v]);
+  }
+  const float3 cc = 0.25f * (cur[0] + cur[1] + cur[2] + cur[3]);
+  const float3 rc = 0.25f * (rest[0] + rest[1] + rest[2] + rest[3]);
+  const M3 Rt = mtrans(R);
+  float3 disp[4];
+#pragma unroll
+  for (int l = 0; l < 4; ++l) disp[l] = mv(Rt, cur[l] - cc) - (rest[l] - rc);
+  const float* k = b.stiffness + 144ull * t;
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    float3 lg = f3(0, 0, 0);
+#pragma unroll
+    for (int c = 0; c < 4; ++c) lg = lg + mv(stiffnessBlock(k, r, c), disp[c]);
+    out[r] = mv(R, lg);
+  }
+}
+
+// Reduced Hessian of a co-rotated record (cubatureHessian):
+// column c = sum_l B_l^T R K_l. R^T B_.[:, c].
+__device__ __forceinline__ M3 corotatedRecordHessian(const Buffers& b, uint32_t t, const M3& R, const M3 basis[4]) {
+  const M3 Rt = mtrans(R);
+  const float* k = b.stiffness + 144ull * t;
+  M3 out;
+#pragma unroll
+  for (int c = 0; c < 3; ++c) {
+    float3 ld[4], wp[4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) ld[l] = mv(Rt, c == 0 ? basis[l].c0 : (c == 1 ? basis[l].c1 : basis[l].c2));
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      float3 lp = f3(0, 0, 0);
+#pragma unroll
+      for (int cv = 0; cv < 4; ++cv) lp = lp + mv(stiffnessBlock(k, r, cv), ld[cv]);
+      wp[r] = mv(R, lp);
+    }
+    float3 col;
+    col.x = dot3(basis[0].c0, wp[0]) + dot3(basis[1].c0, wp[1]) + dot3(basis[2].c0, wp[2]) + dot3(basis[3].c0, wp[3]);
+    col.y = dot3(basis[0].c1, wp[0]) + dot3(basis[1].c1, wp[1]) + dot3(basis[2].c1, wp[2]) + dot3(basis[3].c1, wp[3]);
+    col.z = dot3(basis[0].c2, wp[0]) + dot3(basis[1].c2, wp[1]) + dot3(basis[2].c2, wp[2]) + dot3(basis[3].c2, wp[3]);
+    if (c == 0) out.c0 = col;
+    else if (c == 1) out.c1 = col;
+    else out.c2 = col;
+  }
+  return out;
+}
+
+// Distributed objective gradient / target stiffness of a record vertex.
+__device__ __forceinline__ float3 distributedObjective(const DevParams& p, const Buffers& b, uint32_t q, float3 x,
+                                                     const uint4& qi) {
+  if (isPinned(qi)) return f3(0, 0, 0);
+  return objectiveGradient(p, b, q, x) * (1.0f / float(qi.y > 1u ? qi.y : 1u));
+}
+
+// One thread per vertex: the exact co-rotated gather, the cubature
+// complement and the regularised solve (regularizedSolve, :2479-2512).
+__global__ void __launch_bounds__(kBlock) corotatedSolveKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                               const float4* __restrict__ src, float4* tgt,
+                                                               const uint32_t* __restrict__ list, uint32_t count,
+                                                               uint32_t K) {
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= count) return;
+  const uint32_t v = list ? list[i] : i;
+  const DevParams& p = pp[b.vertexScene[v]];
+  if (!p.active) return;
+  const uint4 info = b.vinfo[v];
+  const float4 rm = b.restMass[v];
+  if (isPinned(info)) {
+    tgt[v] = make_float4(rm.x, rm.y, rm.z, 1.0f);
+    b.finalUpdate[v] = 0.0f;
+    return;
+  }
+  const float3 position = xyz(src[v]);
+  const float4 pv = b.predicted[v];
+  const float inertia = rm.w * p.invDt2;
+  const bool objActive = p.objectiveFlags != 0u;
+  float3 grad = inertia * (position - xyz(pv));
+  M3 hess = inertia * midentity();
+  if (objActive) grad = grad + objectiveGradient(p, b, v, position);
+  if (p.objectiveFlags & 2u) hess = hess + targetStiffness(p, b, v) * midentity();
+  for (uint32_t a = 0; a < info.y; ++a) {
+    const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
+    const uint32_t t = entry >> 2, slot = entry & 3u;
+    const TetRec r = loadTet(b.tets, t);
+    const M3 R = loadRot(b.tetRot, t);
+    float3 tg[4];
+    corotatedGradient(b, src, t, r.idx, R, tg);
+    grad = grad + tg[slot];
+    hess = hess + mm(mm(R, stiffnessBlock(b.stiffness + 144ull * t, slot, slot)), mtrans(R));
+  }
+  if (p.floorStiffness > 0.0f && position.y < p.floorHeight) {
+    grad.y += p.floorStiffness * (position.y - p.floorHeight);
+    hess.c1.y += p.floorStiffness;
+  }
+  const M3 RsT = mtrans(loadRot(b.vertexRot, v));
+  const float dWs = pv.w;
+  for (uint32_t s = 0; s < K; ++s) {
+    const size_t rec = static_cast<size_t>(v) * K + s;
+    const uint4 head = __ldg(&b.cubHead[2 * rec]);
+    const float w = __uint_as_float(head.y);
+    if (head.x == kEmptyTet || !(w > 0.0f)) continue;
+    const uint32_t t = head.x;
+    const uint4 q = __ldg(&b.cubHead[2 * rec + 1]);
+    const float4* U = b.cubBasis + 9ull * rec;
+    M3 basis[4];
+#pragma unroll
+    for (int l = 0; l < 4; ++l) basis[l] = mm(mm(loadRot(b.vertexRot, idxAt(q, l)), loadBlockVec(U, l)), RsT);
+    const M3 R = loadRot(b.tetRot, t);
+    float3 tg[4];
+    corotatedGradient(b, src, t, q, R, tg);
+    float3 pg = f3(0, 0, 0);
+    M3 ih = mzero();
+    uint32_t ss = 4;
+#pragma unroll
+    for (int l = 0; l < 4; ++l) {
+      const uint32_t qv = idxAt(q, l);
+      if (qv == v) ss = l;
+      const float4 pq = b.predicted[qv];
+      const float3 xq = xyz(src[qv]);
+      pg = pg + mtv(basis[l], tg[l] + pq.w * (xq - xyz(pq)));
+      ih = ih + pq.w * mm(mtrans(basis[l]), basis[l]);
+    }
+    if (objActive) {
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const uint32_t qv = idxAt(q, l);
+        pg = pg + mtv(basis[l], distributedObjective(p, b, qv, xyz(src[qv]), b.vinfo[qv]));
+      }
+    }
+    M3 ph = corotatedRecordHessian(b, t, R, basis) + ih;
+    if (p.objectiveFlags & 2u) {
+      M3 oh = mzero();
+#pragma unroll
+      for (int l = 0; l < 4; ++l) {
+        const uint32_t qv = idxAt(q, l);
+        const uint4 qi = b.vinfo[qv];
+        const float kt = isPinned(qi) ? 0.0f : targetStiffness(p, b, qv) / float(qi.y > 1u ? qi.y : 1u);
+        oh = oh + kt * mm(mtrans(basis[l]), basis[l]);
+      }
+      ph = ph + oh;
+    }
+    if (ss < 4) {
+      pg = pg - (tg[ss] + dWs * (position - xyz(pv)));
+      if (objActive) pg = pg - distributedObjective(p, b, v, position, info);
+      ph = ph - (mm(mm(R, stiffnessBlock(b.stiffness + 144ull * t, ss, ss)), mtrans(R)) + dWs * midentity());
+      if (p.objectiveFlags & 2u)
+        ph = ph - (targetStiffness(p, b, v) / float(info.y > 1u ? info.y : 1u)) * midentity();
+    }
+    grad = grad + w * pg;
+    hess = hess + w * ph;
+  }
+  // Regularised Cholesky solve with the shift max(regularization * scale, 1e-9).
+  const float ds = fmaxf(1.0f, fmaxf(fabsf(hess.c0.x), fmaxf(fabsf(hess.c1.y), fabsf(hess.c2.z))));
+  const float shift = fmaxf(p.regularization * ds, 1.0e-9f);
+  const float a00 = hess.c0.x + shift, a11 = hess.c1.y + shift, a22 = hess.c2.z + shift;
+  const float a01 = 0.5f * (hess.c0.y + hess.c1.x);
+  const float a02 = 0.5f * (hess.c0.z + hess.c2.x);
+  const float a12 = 0.5f * (hess.c1.z + hess.c2.y);
+  const float3 rhs = -grad;
+  const float l00 = sqrtf(fmaxf(a00, shift));
+  const float l10 = a01 / l00, l20 = a02 / l00;
+  const float l11 = sqrtf(fmaxf(a11 - l10 * l10, shift));
+  const float l21 = (a12 - l20 * l10) / l11;
+  const float l22 = sqrtf(fmaxf(a22 - l20 * l20 - l21 * l21, shift));
+  const float y0 = rhs.x / l00, y1 = (rhs.y - l10 * y0) / l11, y2 = (rhs.z - l20 * y0 - l21 * y1) / l22;
+  const float x2 = y2 / l22, x1 = (y1 - l21 * x2) / l11, x0 = (y0 - l10 * x1 - l20 * x2) / l00;
+  float3 delta = f3(x0, x1, x2);
+  const float sq = dot3(delta, delta);
+  if (!(sq >= 0.0f && sq < 1.0e30f)) delta = f3(0, 0, 0);
+  const float dls = dot3(delta, delta);
+  if (p.maxStep > 0.0f && dls > p.maxStep * p.maxStep) delta = delta * (p.maxStep * (1.0f / sqrtf(dls)));
+  const float3 np = position + delta;
+  tgt[v] = make_float4(np.x, np.y, np.z, 1.0f);
+  b.finalUpdate[v] = sqrtf(dot3(delta, delta));
+}
+
 __global__ void __launch_bounds__(kBlock) copyKernel(Buffers b, const DevParams* __restrict__ pp,
                                                      const float4* __restrict__ src, float4* __restrict__ dst,
                                                      uint32_t V) {
@@ -834,9 +1044,14 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
         b.velocity[i] = make_float4(0, 0, 0, 0);
       }
       b.predicted[i] = make_float4(pred.x, pred.y, pred.z, distributedInertiaWeight(rm, info, p.invDt2));
+      b.finalUpdate[i] = 0.0f;
+      if (!p.globalization) {
+        // Co-rotated path: the iteration source is the inertial prediction.
+        b.pos[1][i] = make_float4(pred.x, pred.y, pred.z, 1.0f);
+        continue;
+      }
       // The stable iteration source is the accepted pose.
       b.pos[1][i] = make_float4(o.x, o.y, o.z, 1.0f);
-      b.finalUpdate[i] = 0.0f;
       // Iteration-0 frames (and, for free vertices, the incident system).
       if (isPinned(info)) storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
       else frameAndIncident(b, b.pos[0], i, info, p.rotationEpsilon);
@@ -844,12 +1059,13 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
       if (finiteS(e)) { acc.e0 += e; acc.e1 += e; }
       else acc.bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
     }
-    if (k < sr.T) {
+    if (p.globalization && k < sr.T) {
       const TetRec r = loadTet(b.tets, sr.tOff + k);
       const M3 F = deformationAt(r, b.pos[0]);
       accumulateTet(acc, r, F, F);
     }
   }
+  if (!p.globalization) return;  // no preflight on the co-rotated path (uniform)
   const GatePartial blk = blockFold(acc, smem, gateCombine);
   GatePartial* partials = reinterpret_cast<GatePartial*>(b.gatePartials);
   if (!publishPartial(blk, partials, rb.slot, sr.gateBlocks, &fs->prologueTicket, &isLast)) return;
@@ -1123,6 +1339,10 @@ __global__ void __launch_bounds__(kBlock) finalizeKernel(Buffers b, const DevPar
   const uint4 info = b.vinfo[v];
   float4 x = accumulated ? b.pos[0][v] : finalPos[v];
   if (isPinned(info)) {
+    if (!p.globalization) {
+      const float4 rm = b.restMass[v];
+      x = make_float4(rm.x, rm.y, rm.z, 1.0f);
+    }
     b.pos[0][v] = make_float4(x.x, x.y, x.z, 1.0f);
     b.velocity[v] = make_float4(0, 0, 0, 0);
     return;
@@ -1222,6 +1442,19 @@ uint32_t smCount() {
 
 int launchPrologue(const Buffers& b, const DevParams* p, cudaStream_t s) {
   prologueKernel<<<b.gateBlocks, kBlock, 0, s>>>(b, p);
+  return 1;
+}
+
+int launchTetPolar(const Buffers& b, const DevParams* p, const float4* src, uint32_t T, cudaStream_t s) {
+  if (T == 0) return 0;
+  tetPolarKernel<<<blocksFor(T), kBlock, 0, s>>>(b, p, src, T);
+  return 1;
+}
+
+int launchCorotatedSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
+                         uint32_t count, uint32_t K, cudaStream_t s) {
+  if (count == 0) return 0;
+  corotatedSolveKernel<<<blocksFor(count), kBlock, 0, s>>>(b, p, src, tgt, list, count, K);
   return 1;
 }
 

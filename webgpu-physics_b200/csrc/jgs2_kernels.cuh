@@ -92,6 +92,7 @@ struct Buffers {
   float4* targets;            // quadratic target xyz, stiffness per vertex
   const uint32_t* colors;     // per vertex colour
   const uint32_t* vertexScene;  // scene of each vertex
+  const uint32_t* tetScene;     // scene of each tet (co-rotated engines only)
   const SceneRange* scenes;
   const RedBlock* gateTable;    // prologue / gate blocks
   const RedBlock* convTable;    // convergence blocks
@@ -108,6 +109,10 @@ int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, c
 // gathering them.
 int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
                 uint32_t count, uint32_t K, bool cachedIncident, cudaStream_t s);
+// Co-rotated path: tet frames and the regularised per-vertex solve.
+int launchTetPolar(const Buffers& b, const DevParams* p, const float4* src, uint32_t T, cudaStream_t s);
+int launchCorotatedSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
+                         uint32_t count, uint32_t K, cudaStream_t s);
 int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* dst, uint32_t V, cudaStream_t s);
 int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s);
 int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt,

@@ -632,6 +632,36 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
   int n = 0;
   n += timed(P::kPrologue, [&] { return jgs2::launchPrologue(b, s->dParams, st); });
   const bool colored = schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL;
+  if (!s->glob) {
+    // Co-rotated path (legacy frames of jgs2-solver.ts:2207-2494): tet and
+    // vertex frames from the current pose, then the regularised solve; no gate.
+    for (uint32_t it = 0; it < iterations; ++it) {
+      float4* src = (it % 2 == 0) ? b.pos[1] : b.pos[0];
+      float4* tgt = (it % 2 == 0) ? b.pos[0] : b.pos[1];
+      if (colored) {
+        n += timed(P::kCopy, [&] { return jgs2::launchCopy(b, s->dParams, src, tgt, s->V, st); });
+        for (uint32_t c = 0; c < s->colorCount; ++c) {
+          n += timed(P::kTetFrames, [&] { return jgs2::launchTetPolar(b, s->dParams, tgt, s->T, st); });
+          const uint32_t nb = s->needOffsets[c], ne = s->needOffsets[c + 1];
+          n += timed(P::kVertexFrames, [&] {
+            return jgs2::launchVertexPolar(b, s->dParams, tgt, s->dNeedVertices + nb, ne - nb, st);
+          });
+          const uint32_t cb = s->colorOffsets[c], ce = s->colorOffsets[c + 1];
+          n += timed(P::kSolve, [&] {
+            return jgs2::launchCorotatedSolve(b, s->dParams, tgt, tgt, s->dColorVertices + cb, ce - cb, s->K, st);
+          });
+        }
+      } else {
+        n += timed(P::kTetFrames, [&] { return jgs2::launchTetPolar(b, s->dParams, src, s->T, st); });
+        n += timed(P::kVertexFrames, [&] { return jgs2::launchVertexPolar(b, s->dParams, src, nullptr, s->V, st); });
+        n += timed(P::kSolve, [&] { return jgs2::launchCorotatedSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, st); });
+      }
+    }
+    const float4* finalPos = (iterations % 2 == 0) ? b.pos[1] : b.pos[0];
+    n += timed(P::kEpilogue,
+               [&] { return jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, bodyCorrection, s->bodies, st); });
+    return n;
+  }
   for (uint32_t it = 0; it < iterations; ++it) {
     float4* src = (it % 2 == 0) ? b.pos[1] : b.pos[0];
     float4* tgt = (it % 2 == 0) ? b.pos[0] : b.pos[1];
@@ -670,7 +700,7 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
 // resolved settings (one per scene; the schedule must agree).
 jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t frames, uint32_t iterations,
                       bool stop, KernelProfiler* prof = nullptr) {
-  if (iterations > JGS2_HISTORY_CAPACITY)
+  if (s->glob && iterations > JGS2_HISTORY_CAPACITY)
     return fail(s, JGS2_INVALID_ARGUMENT,
                 format("Stable JGS2 records at most %u nonlinear iterations per frame; got %u.",
                        JGS2_HISTORY_CAPACITY, iterations));
@@ -686,7 +716,7 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
                 "This batch was created without graph colouring: give one of its scenes the graph-coloured "
                 "schedule when the batch is created to step it with that schedule.");
   const uint32_t sub = schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL ? s->colorCount : 1u;
-  if (static_cast<uint64_t>(iterations) * sub > JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION / frames)
+  if (s->glob && static_cast<uint64_t>(iterations) * sub > JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION / frames)
     return fail(s, JGS2_INVALID_ARGUMENT,
                 format("Stable JGS2 may encode at most %u total nonlinear iterations per submission; got %u "
                        "frames * %u iterations.",
@@ -721,7 +751,7 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
   for (uint32_t i = 0; i < s->scenes.size(); ++i) {
     s->scenes[i].submitted = st[i];
     s->scenes[i].submittedIterations = iterations;
-    s->scenes[i].recordsAvailable = true;
+    if (s->glob) s->scenes[i].recordsAvailable = true;
   }
   return JGS2_OK;
 }
@@ -810,6 +840,7 @@ struct PreparedScene {
   uint32_t colorCount = 0;
   std::vector<uint32_t> colors;
   bool colored = false;
+  bool stable = true;  // stable Neo-Hookean (else co-rotated linear)
   std::string error;  // message of a failed preparation (thread-safe copy)
 };
 
@@ -824,11 +855,8 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
     return fail(nullptr, JGS2_INVALID_ARGUMENT,
                 "A production JGS2 solve cannot mix stable Neo-Hookean and co-rotated regression tetrahedra in one "
                 "precomputation.");
-  if (stable != in->tet_count)
-    return fail(nullptr, JGS2_UNSUPPORTED,
-                "The co-rotated regression material path is not built into this library; use stable Neo-Hookean "
-                "tetrahedra.");
   out->in = in;
+  out->stable = stable == in->tet_count;
   out->colored = colour;
   if (colour) out->colors = colorInput(in, &out->colorCount);
   if (out->colorCount > JGS2_MAX_SCHEDULE_COLORS)
@@ -838,7 +866,7 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
   jgs2_settings base;
   defaults(&base);
   if (!resolve(base, settings, mask, &out->resolved, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
-  const double m = minimumInputDeterminant(in);
+  const double m = out->stable ? minimumInputDeterminant(in) : 1.0;
   if (!std::isfinite(m) || !(m > kDeterminantFloor))
     return fail(nullptr, JGS2_INFEASIBLE_INPUT,
                 format("A stable Neo-Hookean production solve requires an initially feasible pose with minimum J "
@@ -870,7 +898,11 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   sp->device = device;
   // JGS2_NO_GRAPHS=1 launches each frame's kernels directly (debugging).
   sp->useGraphs = std::getenv("JGS2_NO_GRAPHS") == nullptr;
-  sp->glob = true;
+  sp->glob = prep[0].stable;
+  for (const PreparedScene& p : prep)
+    if (p.stable != sp->glob)
+      return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                  "A batch cannot mix stable Neo-Hookean scenes with co-rotated linear scenes.");
   sp->scenes.resize(S);
   uint64_t V = 0, T = 0, bodies = 0;
   uint32_t K = 0, colorCount = 1;
@@ -1163,11 +1195,33 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     STEP(upload(sp, &sp->dNeedVertices, need.data(), need.size()));
     STEP(deviceAlloc(sp, &sp->dParams, S));
     sp->hParams.resize(S);
+    if (!sp->glob) {
+      // Co-rotated path: tet frames, the 144-float rest stiffness of each tet
+      // and each tet's scene.
+      STEP(deviceAlloc(sp, &b.tetRot, 3ull * nT));
+      std::vector<float> stiff(144ull * nT);
+      std::vector<uint32_t> tetScene(nT);
+      parallelFor(S, [&](uint32_t i) {
+        const SceneHost& sc = sp->scenes[i];
+        std::memcpy(&stiff[144ull * sc.tOff], prep[i].in->tet_rest_stiffness, sizeof(float) * 144ull * sc.T);
+        std::fill(tetScene.begin() + sc.tOff, tetScene.begin() + sc.tOff + sc.T, i);
+      });
+      float* k = nullptr;
+      STEP(upload(sp, &k, stiff.data(), stiff.size()));
+      b.stiffness = k;
+      uint32_t* ts = nullptr;
+      STEP(upload(sp, &ts, tetScene.data(), tetScene.size()));
+      b.tetScene = ts;
+    }
   }
 #undef STEP
+  for (uint32_t i = 0; i < S; ++i) sp->hParams[i] = makeParams(sp, i, sp->scenes[i].defaults, false);
+  if (!sp->glob) {
+    CUDA_TRY(sp, cudaStreamSynchronize(sp->stream));
+    return JGS2_OK;
+  }
   // GPU preflight of the uploaded pose (validateGpuInitialStableSource,
   // jgs2-solver.ts:820-893): the gate on (posA, posA) must accept in every scene.
-  for (uint32_t i = 0; i < S; ++i) sp->hParams[i] = makeParams(sp, i, sp->scenes[i].defaults, false);
   CUDA_TRY(sp, cudaMemcpyAsync(sp->dParams, sp->hParams.data(), sizeof(DevParams) * S, cudaMemcpyHostToDevice,
                                sp->stream));
   jgs2::launchGate(b, sp->dParams, b.pos[0], b.pos[0], sp->stream);

@@ -1049,8 +1049,9 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
   }
   jgs2_precompute_stats st{};
   std::vector<double> residuals(V, -1.0);
-  if (anyCorotated) {
-    // Co-rotated scenes run the exact local gather only (no cubature records).
+  if (anyCorotated && !opt.exact_complement) {
+    // Co-rotated scenes run the exact local gather only (no cubature records)
+    // unless the exact complement is asked for.
     st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
     if (stats) *stats = st;
     return true;
