@@ -67,6 +67,30 @@ typedef enum jgs2_status {
 #define JGS2_CONTROL_RECORD_FLOATS 16u
 
 /*
+ * Triangle cloth: JGS2GpuClothInput (src/simulation/gpu/cloth-layout.ts:88-104).
+ * St. Venant-Kirchhoff membrane triangles in plane stress and quadratic
+ * dihedral hinges over vertices of the same scene.  Hinges are oriented: the
+ * hinge (i0, i1, i2, i3) joins triangles (i0, i1, i2) and (i1, i0, i3).  Cloth
+ * requires the stable Neo-Hookean path (jgs2-solver.ts:998-1002).
+ */
+typedef struct jgs2_cloth_input {
+  uint32_t vertex_count;                    /* must equal the scene's vertex_count */
+  uint32_t triangle_count;
+  uint32_t hinge_count;
+  uint32_t reserved0;
+  const uint32_t* triangle_indices;         /* 3 * triangles */
+  const float* triangle_inverse_rest_bases; /* 4 * triangles, row-major 2x2 */
+  const float* triangle_rest_areas;         /* triangles, positive */
+  const uint32_t* hinge_indices;            /* 4 * hinges */
+  const float* hinge_rest_angles;           /* hinges */
+  const float* hinge_rest_edge_lengths;     /* hinges, positive */
+  float young_modulus;                      /* > 0 */
+  float poisson_ratio;                      /* [0, 0.5) */
+  float thickness;                          /* > 0 */
+  float bending_stiffness;                  /* >= 0 */
+} jgs2_cloth_input;
+
+/*
  * Input record: JGS2GpuInput (src/simulation/gpu/layout.ts:41-90).
  * Optional arrays may be NULL.  tet_rest_stiffness may be NULL when every
  * tetrahedron is stable Neo-Hookean (the stable path never reads it).
@@ -93,6 +117,7 @@ typedef struct jgs2_input {
   const uint32_t* cubature_tet_ids;  /* V * K; 0xffffffff = empty slot */
   const float* cubature_weights;     /* V * K */
   const float* cubature_basis;       /* V * K * 36: four row-major Ubar blocks */
+  const jgs2_cloth_input* cloth;     /* NULL: no cloth (input.cloth, layout.ts:62) */
 } jgs2_input;
 
 /*
@@ -172,7 +197,7 @@ typedef struct jgs2_info {
   float scene_scale;               /* initial dynamic AABB diagonal */
   float preprocessing_timestep;
   uint32_t current_position_buffer;/* 0 = A, reported for zero-copy consumers */
-  uint32_t reserved;
+  uint32_t cloth_triangle_count;   /* clothTriangleCount (:911) */
 } jgs2_info;
 
 /* ---- library ---------------------------------------------------------- */
@@ -336,8 +361,9 @@ jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* solver, const float* 
  *
  * It allocates no device memory: its reduction scratch is a fixed static
  * device array of 262,400 bytes (8192 block partials of 32 bytes after a
- * 256-byte header).  So max(vertex_count, tet_count) may be at most
- * 1,048,576 (8192 blocks of 128); larger solvers get JGS2_INVALID_ARGUMENT.
+ * 256-byte header).  So the largest of vertex_count, tet_count and the cloth
+ * triangle and hinge counts may be at most 1,048,576 (8192 blocks of 128);
+ * larger solvers get JGS2_INVALID_ARGUMENT.
  * The first call on each device looks up the scratch address there (this may
  * load the kernel module onto the device), so make one call before any stream
  * capture begins.  The scratch's ticket word must start at zero: module load

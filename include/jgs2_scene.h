@@ -103,6 +103,20 @@ int64_t jgs2_scene_add_mesh(jgs2_scene* scene, uint32_t vertex_count,
                             uint32_t material, const uint8_t* pinned,
                             uint32_t body);
 
+/* Triangle cloth appended as one body: SceneDefinition.cloth
+ * (src/scenes/index.ts:632-720) with its areal masses density * thickness *
+ * area / 3 per triangle vertex (validateAndAddClothMasses,
+ * src/simulation/cpu/precompute.ts:44-95).  triangles index the new vertices
+ * (0 .. vertex_count - 1); pinned may be NULL.  A scene holds one cloth
+ * material.  The packer derives the rest bases, rest areas, hinges and rest
+ * dihedrals (buildJGS2GpuClothInput, src/scenes/index.ts:881-973) and points
+ * jgs2_input.cloth at them.  Returns the first vertex id or -1. */
+int64_t jgs2_scene_add_cloth(jgs2_scene* scene, uint32_t vertex_count, const double* positions,
+                             uint32_t triangle_count, const uint32_t* triangles, const uint8_t* pinned,
+                             uint32_t body, double density, double young_modulus, double poisson_ratio,
+                             double thickness, double bending_stiffness);
+uint32_t jgs2_scene_cloth_triangle_count(const jgs2_scene* scene);
+
 /* Replace the pin flags of every vertex (V bytes, nonzero = pinned); the
  * reference's cuboid generator takes an arbitrary predicate (mesh.ts:142). */
 jgs2_status jgs2_scene_set_pinned(jgs2_scene* scene, const uint8_t* pinned);

@@ -548,6 +548,203 @@ struct Oracle {
     return objectiveDelta(v, base, d) / T(incidentCount(v));
   }
 
+  // ---- triangle cloth (jgs2-shader.ts:1225-1844; cloth-layout.ts:88-452) ----
+  uint32_t C = 0, H = 0;
+  std::vector<uint32_t> clothTri;            // 3C
+  std::vector<V4<T>> clothInv;               // C: row-major inverse rest basis (x y / z w)
+  std::vector<T> clothArea;                  // C
+  std::vector<uint32_t> hingeIdx;            // 4H
+  std::vector<T> hingeAngle, hingeLength;    // H
+  T clothLambda = 0, clothMu = 0, clothThickness = 0, clothBending = 0;
+  // Vertex-to-element CSR in ascending element order (buildIncidentElementCsr,
+  // cloth-layout.ts:198-223).
+  std::vector<uint32_t> triRows, triElems, hingeRows, hingeElems;
+
+  static V3<T> clothAt(const std::vector<V3<T>>& x, uint32_t q, uint32_t ov, V3<T> op) {
+    return q == ov ? op : x[q];
+  }
+  static uint32_t triSlot(const uint32_t* q, uint32_t v) {
+    if (q[0] == v) return 0;
+    if (q[1] == v) return 1;
+    if (q[2] == v) return 2;
+    return 3;
+  }
+  // clothTriangleShapeGradient (jgs2-shader.ts:1536-1547).
+  static void triShapeGradient(const V4<T>& inv, uint32_t l, T* gx, T* gy) {
+    if (l == 1) { *gx = inv.x; *gy = inv.y; return; }
+    if (l == 2) { *gx = inv.z; *gy = inv.w; return; }
+    *gx = -inv.x - inv.z;
+    *gy = -inv.y - inv.w;
+  }
+  struct Membrane {
+    T energy;
+    V3<T> d0, d1;
+    T s0, s1, s2;
+    V3<T> g[3];
+  };
+  // clothMembraneEvaluationAt (jgs2-shader.ts:1549-1608).
+  Membrane membraneAt(uint32_t c, const std::vector<V3<T>>& x, uint32_t ov, V3<T> op) const {
+    const uint32_t* q = &clothTri[3ull * c];
+    const V3<T> x0 = clothAt(x, q[0], ov, op);
+    const V3<T> e01 = clothAt(x, q[1], ov, op) - x0;
+    const V3<T> e02 = clothAt(x, q[2], ov, op) - x0;
+    const V4<T> inv = clothInv[c];
+    Membrane m;
+    m.d0 = e01 * inv.x + e02 * inv.z;
+    m.d1 = e01 * inv.y + e02 * inv.w;
+    const T e00 = T(0.5) * (dot(m.d0, m.d0) - T(1));
+    const T e01s = T(0.5) * dot(m.d0, m.d1);
+    const T e11 = T(0.5) * (dot(m.d1, m.d1) - T(1));
+    const T trace = e00 + e11;
+    m.s0 = T(2) * clothMu * e00 + clothLambda * trace;
+    m.s1 = T(2) * clothMu * e01s;
+    m.s2 = T(2) * clothMu * e11 + clothLambda * trace;
+    const V3<T> p0 = m.d0 * m.s0 + m.d1 * m.s1;
+    const V3<T> p1 = m.d0 * m.s1 + m.d1 * m.s2;
+    const T aw = clothArea[c] * clothThickness;
+    for (uint32_t l = 0; l < 3; ++l) {
+      T gx, gy;
+      triShapeGradient(inv, l, &gx, &gy);
+      m.g[l] = aw * (p0 * gx + p1 * gy);
+    }
+    const T density = clothMu * (e00 * e00 + T(2) * e01s * e01s + e11 * e11) + T(0.5) * clothLambda * trace * trace;
+    m.energy = aw * density;
+    return m;
+  }
+  // clothMembraneLocalHessian (jgs2-shader.ts:1610-1660) at the source pose.
+  M3<T> membraneLocalHessian(uint32_t c, uint32_t slot) const {
+    const Membrane ev = membraneAt(c, *src, 0xffffffffu, v3<T>(0, 0, 0));
+    T gx, gy;
+    triShapeGradient(clothInv[c], slot, &gx, &gy);
+    const T aw = clothArea[c] * clothThickness;
+    M3<T> r;
+    for (int k = 0; k < 3; ++k) {
+      V3<T> axis = v3<T>(0, 0, 0);
+      setComp(axis, k, T(1));
+      const V3<T> f0 = axis * gx, f1 = axis * gy;
+      const T de00 = gx * comp(ev.d0, k);
+      const T de01 = T(0.5) * (gx * comp(ev.d1, k) + gy * comp(ev.d0, k));
+      const T de11 = gy * comp(ev.d1, k);
+      const T dtr = de00 + de11;
+      const T ds0 = T(2) * clothMu * de00 + clothLambda * dtr;
+      const T ds1 = T(2) * clothMu * de01;
+      const T ds2 = T(2) * clothMu * de11 + clothLambda * dtr;
+      const V3<T> dp0 = f0 * ev.s0 + f1 * ev.s1 + ev.d0 * ds0 + ev.d1 * ds1;
+      const V3<T> dp1 = f0 * ev.s1 + f1 * ev.s2 + ev.d0 * ds1 + ev.d1 * ds2;
+      r.c[k] = aw * (dp0 * gx + dp1 * gy);
+    }
+    return T(0.5) * (r + transpose(r));
+  }
+  // clothTriangleRawNormalAt (jgs2-shader.ts:1662-1690).
+  V3<T> triangleNormalAt(uint32_t c, const std::vector<V3<T>>& x, uint32_t ov, V3<T> op) const {
+    const uint32_t* q = &clothTri[3ull * c];
+    const V3<T> x0 = clothAt(x, q[0], ov, op);
+    return cross(clothAt(x, q[1], ov, op) - x0, clothAt(x, q[2], ov, op) - x0);
+  }
+  struct Dihedral {
+    T angle;
+    bool valid;
+    V3<T> g[4];
+  };
+  static T length3(V3<T> v) { return std::sqrt(dot(v, v)); }
+  static V3<T> normalizedDifferential(V3<T> unit, T len, V3<T> d) { return (d - unit * dot(unit, d)) / len; }
+  // clothDihedralEvaluationAt (jgs2-shader.ts:1702-1813): atan2 of
+  // (t . (n0 x n1), n0 . n1) and its analytic differential per coordinate.
+  Dihedral dihedralAt(uint32_t h, const std::vector<V3<T>>& x, uint32_t ov, V3<T> op) const {
+    const uint32_t* q = &hingeIdx[4ull * h];
+    V3<T> p[4];
+    for (int l = 0; l < 4; ++l) p[l] = clothAt(x, q[l], ov, op);
+    Dihedral out{0, false, {}};
+    for (auto& g : out.g) g = v3<T>(0, 0, 0);
+    const V3<T> edge = p[1] - p[0];
+    const T edgeLength = length3(edge);
+    const V3<T> to2 = p[2] - p[0];
+    const V3<T> rev = -edge;
+    const V3<T> to3 = p[3] - p[1];
+    const V3<T> n0r = cross(edge, to2), n1r = cross(rev, to3);
+    const T nl0 = length3(n0r), nl1 = length3(n1r);
+    const T es0 = std::max(edgeLength, std::max(length3(to2), length3(to2 - edge)));
+    const T es1 = std::max(edgeLength, std::max(length3(to3), length3(to3 - rev)));
+    const bool geometryValid = finiteS(edgeLength) && edgeLength > T(0) && finiteS(nl0) && finiteS(nl1) &&
+                               nl0 > T(1.0e-12) * es0 * es0 && nl1 > T(1.0e-12) * es1 * es1;
+    if (!geometryValid) return out;
+    const V3<T> t = edge / edgeLength;
+    const V3<T> n0 = n0r / nl0, n1 = n1r / nl1;
+    const V3<T> nc = cross(n0, n1);
+    const T sine = dot(t, nc), cosine = dot(n0, n1);
+    const T den = sine * sine + cosine * cosine;
+    if (!finiteS(den) || !(den > T(0))) return out;
+    for (int coord = 0; coord < 12; ++coord) {
+      const int dv = coord / 3, axis = coord % 3;
+      V3<T> deltas[4];
+      for (auto& d : deltas) d = v3<T>(0, 0, 0);
+      setComp(deltas[dv], axis, T(1));
+      const V3<T> dEdge = deltas[1] - deltas[0];
+      const V3<T> dt = normalizedDifferential(t, edgeLength, dEdge);
+      const V3<T> dTo2 = deltas[2] - deltas[0];
+      const V3<T> dTo3 = deltas[3] - deltas[1];
+      const V3<T> dn0r = cross(dEdge, to2) + cross(edge, dTo2);
+      const V3<T> dn1r = cross(-dEdge, to3) + cross(rev, dTo3);
+      const V3<T> dn0 = normalizedDifferential(n0, nl0, dn0r);
+      const V3<T> dn1 = normalizedDifferential(n1, nl1, dn1r);
+      const T dcos = dot(dn0, n1) + dot(n0, dn1);
+      const T dsin = dot(dt, nc) + dot(t, cross(dn0, n1) + cross(n0, dn1));
+      setComp(out.g[dv], axis, (cosine * dsin - sine * dcos) / den);
+    }
+    const T angle = std::atan2(sine, cosine);
+    bool fin = finiteS(angle);
+    for (auto& g : out.g) fin = fin && finiteV(g);
+    if (!fin) {
+      for (auto& g : out.g) g = v3<T>(0, 0, 0);
+      return out;
+    }
+    out.angle = angle;
+    out.valid = true;
+    return out;
+  }
+  // clothWrappedAngleDifference (jgs2-shader.ts:1815-1818).
+  static T wrappedAngleDifference(T angle, T reference) {
+    const T d = angle - reference;
+    return std::atan2(std::sin(d), std::cos(d));
+  }
+  // clothBendingEnergyAt (jgs2-shader.ts:1820-1836).
+  T bendingEnergyAt(uint32_t h, const std::vector<V3<T>>& x, uint32_t ov, V3<T> op) const {
+    const Dihedral e = dihedralAt(h, x, ov, op);
+    if (!e.valid) return static_cast<T>(kF32Max);
+    const T diff = wrappedAngleDifference(e.angle, hingeAngle[h]);
+    const T ws = clothBending * hingeLength[h];
+    return T(0.5) * ws * diff * diff;
+  }
+  // Membrane and bending gradient (and, with hess, the local Hessian) of
+  // vertex v at the source pose: the cloth loops of jgs2Solve
+  // (jgs2-shader.ts:3113-3186).
+  void clothLocal(uint32_t v, const std::vector<V3<T>>& x, V3<T>* grad, M3<T>* hess) const {
+    if (C == 0) return;
+    for (uint32_t k = triRows[v]; k < triRows[v + 1]; ++k) {
+      const uint32_t c = triElems[k];
+      const uint32_t slot = triSlot(&clothTri[3ull * c], v);
+      if (slot >= 3) continue;
+      *grad = *grad + membraneAt(c, x, 0xffffffffu, v3<T>(0, 0, 0)).g[slot];
+      if (hess) *hess = *hess + membraneLocalHessian(c, slot);
+    }
+    for (uint32_t k = hingeRows[v]; k < hingeRows[v + 1]; ++k) {
+      const uint32_t h = hingeElems[k];
+      const uint32_t slot = slotOf(&hingeIdx[4ull * h], v);
+      if (slot >= 4) continue;
+      const Dihedral d = dihedralAt(h, x, 0xffffffffu, v3<T>(0, 0, 0));
+      if (!d.valid) {
+        const T m = static_cast<T>(kF32Max);
+        *grad = *grad + v3<T>(m, m, m);
+        continue;
+      }
+      const T diff = wrappedAngleDifference(d.angle, hingeAngle[h]);
+      const T ws = clothBending * hingeLength[h];
+      const V3<T> ag = d.g[slot];
+      *grad = *grad + ws * diff * ag;
+      if (hess) *hess = *hess + ws * outerColumns(ag, ag);
+    }
+  }
+
   struct Geometry { T minimum; bool valid; };
   Geometry restrictedMinimumDeterminant(uint32_t v, V3<T> d) const {
     T minimum = static_cast<T>(kF32Max);
@@ -572,6 +769,23 @@ struct Oracle {
       if (!finiteS(j)) return {0, false};
       minimum = std::min(minimum, j);
     }
+    // Cloth: signed relative area stretch of each incident triangle at the
+    // source and the trial pose (jgs2-shader.ts:2067-2116).
+    if (C != 0) {
+      const V3<T> trial = (*src)[v] + d;
+      for (uint32_t k = triRows[v]; k < triRows[v + 1]; ++k) {
+        const uint32_t c = triElems[k];
+        if (triSlot(&clothTri[3ull * c], v) >= 3) continue;
+        const V3<T> sn = triangleNormalAt(c, *src, 0xffffffffu, v3<T>(0, 0, 0));
+        const V3<T> tn = triangleNormalAt(c, *src, v, trial);
+        const T twice = T(2) * clothArea[c];
+        const T ss = length3(sn) / twice;
+        const T tm = length3(tn) / twice;
+        const T ts = dot(sn, tn) > T(0) ? tm : -tm;
+        if (!(twice > T(0)) || !finiteS(ss) || !finiteS(ts)) return {0, false};
+        minimum = std::min(minimum, std::min(ss, ts));
+      }
+    }
     return {minimum, true};
   }
   T restrictedEnergyDelta(uint32_t v, V3<T> d) const {
@@ -583,6 +797,21 @@ struct Oracle {
     for (uint32_t a = 0; a < count; ++a) {
       const uint32_t t = adjacency[start + a];
       result += materialDelta(t, deformationAt(t, *src), exactTrialF(t, v, d));
+    }
+    // Cloth membrane and bending deltas of the incident elements
+    // (jgs2-shader.ts:2207-2263).
+    if (C != 0) {
+      const V3<T> trial = sp + d;
+      for (uint32_t k = triRows[v]; k < triRows[v + 1]; ++k) {
+        const uint32_t c = triElems[k];
+        if (triSlot(&clothTri[3ull * c], v) >= 3) continue;
+        result += membraneAt(c, *src, v, trial).energy - membraneAt(c, *src, 0xffffffffu, v3<T>(0, 0, 0)).energy;
+      }
+      for (uint32_t k = hingeRows[v]; k < hingeRows[v + 1]; ++k) {
+        const uint32_t h = hingeElems[k];
+        if (slotOf(&hingeIdx[4ull * h], v) >= 4) continue;
+        result += bendingEnergyAt(h, *src, v, trial) - bendingEnergyAt(h, *src, 0xffffffffu, v3<T>(0, 0, 0));
+      }
     }
     for (uint32_t s = 0; s < K; ++s) {
       const size_t rec = static_cast<size_t>(v) * K + s;
@@ -675,6 +904,25 @@ struct Oracle {
     if (!pin && st.floorStiffness > 0) {
       const T pen = std::min(T(0), p.y - static_cast<T>(st.floorHeight));
       e += T(0.5) * static_cast<T>(st.floorStiffness) * pen * pen;
+    }
+    // Each cloth element's energy is owned by its lowest vertex index, pinned
+    // or not (jgs2-shader.ts:2585-2642).
+    if (C != 0) {
+      for (uint32_t k = triRows[v]; k < triRows[v + 1]; ++k) {
+        const uint32_t c = triElems[k];
+        const uint32_t* q = &clothTri[3ull * c];
+        if (v != std::min(q[0], std::min(q[1], q[2]))) continue;
+        const T twice = T(2) * clothArea[c];
+        const T stretch = length3(triangleNormalAt(c, x, 0xffffffffu, v3<T>(0, 0, 0))) / twice;
+        if (!(twice > T(0)) || !finiteS(stretch) || !(stretch > T(kDeterminantFloor))) return static_cast<T>(kF32Max);
+        e += membraneAt(c, x, 0xffffffffu, v3<T>(0, 0, 0)).energy;
+      }
+      for (uint32_t k = hingeRows[v]; k < hingeRows[v + 1]; ++k) {
+        const uint32_t h = hingeElems[k];
+        const uint32_t* q = &hingeIdx[4ull * h];
+        if (v != std::min(std::min(q[0], q[1]), std::min(q[2], q[3]))) continue;
+        e += bendingEnergyAt(h, x, 0xffffffffu, v3<T>(0, 0, 0));
+      }
     }
     return e;
   }
@@ -774,6 +1022,7 @@ struct Oracle {
       if (stableTet(t)) hessian = hessian + stableLocalHessian(t, slot);
       else hessian = hessian + tetRot[t] * stiffnessBlock(t, slot, slot) * transpose(tetRot[t]);
     }
+    clothLocal(v, *src, &gradient, &hessian);
     if (st.floorStiffness > 0 && position.y < static_cast<T>(st.floorHeight)) {
       gradient.y += static_cast<T>(st.floorStiffness) * (position.y - static_cast<T>(st.floorHeight));
       hessian.c[1].y += static_cast<T>(st.floorStiffness);
@@ -922,6 +1171,23 @@ struct Oracle {
       tetGlob[2 * t] = {sgv ? sj : T(0), cgv ? cj : T(0), sgv ? T(1) : T(0), cgv ? T(1) : T(0)};
       tetGlob[2 * t + 1] = {sev ? se : T(0), cev ? ce : T(0), sev ? T(1) : T(0), cev ? T(1) : T(0)};
     }
+    // Cloth triangles follow the tets: signed area stretch as geometry, and
+    // neutral energy lanes (jgs2-shader.ts:3507-3549).
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < C; ++i) {
+      const uint32_t c = static_cast<uint32_t>(i);
+      const V3<T> sn = triangleNormalAt(c, *src, 0xffffffffu, v3<T>(0, 0, 0));
+      const V3<T> cn = triangleNormalAt(c, *tgt, 0xffffffffu, v3<T>(0, 0, 0));
+      const T twice = T(2) * clothArea[c];
+      const T ss = length3(sn) / twice;
+      const T cm = length3(cn) / twice;
+      const T cs = dot(sn, cn) > T(0) ? cm : -cm;
+      const bool sgv = twice > T(0) && finiteV(sn) && finiteS(ss);
+      const bool cgv = twice > T(0) && finiteV(cn) && finiteS(cs);
+      const size_t e = static_cast<size_t>(Tn) + c;
+      tetGlob[2 * e] = {sgv ? ss : T(0), cgv ? cs : T(0), sgv ? T(1) : T(0), cgv ? T(1) : T(0)};
+      tetGlob[2 * e + 1] = {0, 0, 1, 1};
+    }
   }
   static bool localFailure(uint32_t s) {
     return s == kStatusShiftLimit || s == kStatusNonDescent || s == kStatusLineSearchFailed ||
@@ -947,7 +1213,7 @@ struct Oracle {
     std::vector<CandLane> lanes(kWorkgroup);
     for (uint32_t lane = 0; lane < kWorkgroup; ++lane) {
       CandLane r{{T(kF32Max), T(kF32Max)}, {0, 0}, 0, 0, 0, 0, 0, kReductionMask};
-      for (uint32_t t = lane; t < Tn; t += kWorkgroup) {
+      for (uint32_t t = lane; t < Tn + C; t += kWorkgroup) {
         const V4<T> g = tetGlob[2 * t], e = tetGlob[2 * t + 1];
         const bool sgv = g.z == T(1) && finiteS(g.x), cgv = g.w == T(1) && finiteS(g.y);
         if (sgv) r.minDet[0] = std::min(r.minDet[0], g.x); else r.bits &= ~kSourceGeometryValid;
@@ -1072,6 +1338,7 @@ struct Oracle {
           material = material + g[slot];
         }
       }
+      clothLocal(v, *tgt, &material, nullptr);
       V3<T> contact = v3<T>(0, 0, 0);
       if (st.floorStiffness > 0 && p.y < static_cast<T>(st.floorHeight))
         contact.y = static_cast<T>(st.floorStiffness) * (p.y - static_cast<T>(st.floorHeight));
@@ -1308,7 +1575,7 @@ struct Oracle {
 
 // buildGreedyVertexColoring (src/simulation/cpu/vertex-coloring.ts:20-110)
 // over the conflict groups of buildJGS2InputVertexColoring
-// (src/simulation/gpu/jgs2-solver.ts:308-367), IPC/cloth groups absent.
+// (src/simulation/gpu/jgs2-solver.ts:308-367), IPC groups absent.
 std::vector<uint32_t> greedyColoring(const jgs2_input* in, uint32_t* countOut) {
   const uint32_t V = in->vertex_count;
   std::vector<std::vector<uint32_t>> adj(V);
@@ -1336,6 +1603,10 @@ std::vector<uint32_t> greedyColoring(const jgs2_input* in, uint32_t* countOut) {
                        in->tet_indices[4ull * t + 3]};
       addGroup(g, 5);
     }
+  if (in->cloth) {
+    for (uint32_t c = 0; c < in->cloth->triangle_count; ++c) addGroup(&in->cloth->triangle_indices[3ull * c], 3);
+    for (uint32_t h = 0; h < in->cloth->hinge_count; ++h) addGroup(&in->cloth->hinge_indices[4ull * h], 4);
+  }
   std::vector<uint32_t> colors(V, 0xffffffffu), stamp(V + 1, 0);
   uint32_t count = 0, st = 0;
   for (uint32_t v = 0; v < V; ++v) {
@@ -1435,7 +1706,45 @@ void initOracle(Oracle<T>& o, const jgs2_input* in) {
   o.tetRot.assign(Tn, identityM<T>());
   o.finalUpdate.assign(V, {0, 0, 0, 0});
   o.local.assign(4ull * V, {0, 0, 0, 0});
-  o.tetGlob.assign(2ull * Tn, {0, 0, 0, 0});
+  if (const jgs2_cloth_input* cl = in->cloth) {
+    // packJGS2GpuClothArena (cloth-layout.ts:335-452): plane-stress Lame
+    // parameters formed in double and stored as f32, incidence CSR rows.
+    o.C = cl->triangle_count;
+    o.H = cl->hinge_count;
+    o.clothTri.assign(cl->triangle_indices, cl->triangle_indices + 3ull * o.C);
+    o.clothInv.resize(o.C);
+    o.clothArea.resize(o.C);
+    for (uint32_t c = 0; c < o.C; ++c) {
+      const float* b = &cl->triangle_inverse_rest_bases[4ull * c];
+      o.clothInv[c] = {b[0], b[1], b[2], b[3]};
+      o.clothArea[c] = cl->triangle_rest_areas[c];
+    }
+    o.hingeIdx.assign(cl->hinge_indices, cl->hinge_indices + 4ull * o.H);
+    o.hingeAngle.resize(o.H);
+    o.hingeLength.resize(o.H);
+    for (uint32_t h = 0; h < o.H; ++h) {
+      o.hingeAngle[h] = cl->hinge_rest_angles[h];
+      o.hingeLength[h] = cl->hinge_rest_edge_lengths[h];
+    }
+    const double E = cl->young_modulus, nu = cl->poisson_ratio;
+    o.clothLambda = static_cast<T>(static_cast<float>(E * nu / (1 - nu * nu)));
+    o.clothMu = static_cast<T>(static_cast<float>(E / (2 * (1 + nu))));
+    o.clothThickness = cl->thickness;
+    o.clothBending = cl->bending_stiffness;
+    auto csr = [&](const std::vector<uint32_t>& idx, uint32_t width, std::vector<uint32_t>& rows,
+                   std::vector<uint32_t>& elems) {
+      rows.assign(V + 1, 0);
+      for (uint32_t q : idx) rows[q + 1] += 1;
+      for (uint32_t v = 0; v < V; ++v) rows[v + 1] += rows[v];
+      elems.assign(idx.size(), 0);
+      std::vector<uint32_t> cursor(rows.begin(), rows.end() - 1);
+      for (size_t e = 0; e < idx.size() / width; ++e)
+        for (uint32_t l = 0; l < width; ++l) elems[cursor[idx[e * width + l]]++] = static_cast<uint32_t>(e);
+    };
+    csr(o.clothTri, 3, o.triRows, o.triElems);
+    csr(o.hingeIdx, 4, o.hingeRows, o.hingeElems);
+  }
+  o.tetGlob.assign(2ull * (Tn + o.C), {0, 0, 0, 0});
   o.vertexEnergy.assign(V, {0, 0, 0, 0});
   o.conv.assign(5ull * V, {0, 0, 0, 0});
   for (auto& c : o.control) c = {0, 0, 0, 0};
@@ -1611,6 +1920,7 @@ int jgs2_oracle_local_system(void* handle, const jgs2_settings* settings, uint32
       gradient = gradient + tg[slot];
       hessian = hessian + o.stableLocalHessian(t, slot);
     }
+    o.clothLocal(v, *o.src, &gradient, &hessian);
     for (uint32_t s = 0; s < o.K; ++s) {
       const size_t rec = static_cast<size_t>(v) * o.K + s;
       const uint32_t t = o.cubTet[rec];
@@ -1640,6 +1950,68 @@ int jgs2_oracle_local_system(void* handle, const jgs2_settings* settings, uint32
     out[13] = o.restrictedMinimumDeterminant(v, dd).minimum;
   };
   if (h->dbl) body(h->d, 0.0); else body(h->f, 0.0f);
+  return 0;
+}
+
+// Single cloth elements, for the closed-form and finite-difference checks of
+// the reference's cloth tests (src/simulation/cpu/cloth.test.ts).
+// Membrane: positions 9, row-major inverse rest basis 4; out = energy, 9
+// gradient entries.  Bending: positions 12; out = energy, 12 gradient
+// entries (k L (theta - theta0) dtheta/dx), valid flag.
+}  // extern "C"
+namespace {
+template <class T>
+void clothMembraneElement(const double* x, const double* inverse, double area, double young, double poisson,
+                          double thickness, double* out) {
+  Oracle<T> o;
+  o.C = 1;
+  o.clothTri = {0, 1, 2};
+  o.clothInv = {{static_cast<T>(inverse[0]), static_cast<T>(inverse[1]), static_cast<T>(inverse[2]),
+                 static_cast<T>(inverse[3])}};
+  o.clothArea = {static_cast<T>(area)};
+  o.clothLambda = static_cast<T>(young * poisson / (1 - poisson * poisson));
+  o.clothMu = static_cast<T>(young / (2 * (1 + poisson)));
+  o.clothThickness = static_cast<T>(thickness);
+  std::vector<V3<T>> p(3);
+  for (int l = 0; l < 3; ++l) p[l] = v3<T>(x[3 * l], x[3 * l + 1], x[3 * l + 2]);
+  const auto m = o.membraneAt(0, p, 0xffffffffu, v3<T>(0, 0, 0));
+  out[0] = m.energy;
+  for (int l = 0; l < 3; ++l) { out[1 + 3 * l] = m.g[l].x; out[2 + 3 * l] = m.g[l].y; out[3 + 3 * l] = m.g[l].z; }
+}
+template <class T>
+void clothBendingElement(const double* x, double restAngle, double restLength, double stiffness, double* out) {
+  Oracle<T> o;
+  o.H = 1;
+  o.hingeIdx = {0, 1, 2, 3};
+  o.hingeAngle = {static_cast<T>(restAngle)};
+  o.hingeLength = {static_cast<T>(restLength)};
+  o.clothBending = static_cast<T>(stiffness);
+  std::vector<V3<T>> p(4);
+  for (int l = 0; l < 4; ++l) p[l] = v3<T>(x[3 * l], x[3 * l + 1], x[3 * l + 2]);
+  const auto d = o.dihedralAt(0, p, 0xffffffffu, v3<T>(0, 0, 0));
+  out[0] = o.bendingEnergyAt(0, p, 0xffffffffu, v3<T>(0, 0, 0));
+  const T diff = d.valid ? Oracle<T>::wrappedAngleDifference(d.angle, o.hingeAngle[0]) : T(0);
+  const T ws = o.clothBending * o.hingeLength[0];
+  for (int l = 0; l < 4; ++l) {
+    const V3<T> g = ws * diff * d.g[l];
+    out[1 + 3 * l] = g.x; out[2 + 3 * l] = g.y; out[3 + 3 * l] = g.z;
+  }
+  out[13] = d.valid ? 1.0 : 0.0;
+}
+}  // namespace
+extern "C" {
+
+int jgs2_oracle_cloth_membrane(const double* positions, const double* inverse, double area, double young,
+                               double poisson, double thickness, int precision, double* out) {
+  if (precision == 64) clothMembraneElement<double>(positions, inverse, area, young, poisson, thickness, out);
+  else clothMembraneElement<float>(positions, inverse, area, young, poisson, thickness, out);
+  return 0;
+}
+
+int jgs2_oracle_cloth_bending(const double* positions, double rest_angle, double rest_length, double stiffness,
+                              int precision, double* out) {
+  if (precision == 64) clothBendingElement<double>(positions, rest_angle, rest_length, stiffness, out);
+  else clothBendingElement<float>(positions, rest_angle, rest_length, stiffness, out);
   return 0;
 }
 

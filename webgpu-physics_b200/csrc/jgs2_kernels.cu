@@ -24,6 +24,7 @@
 
 #include <algorithm>
 
+#include "jgs2_cloth.cuh"
 #include "jgs2_device.cuh"
 #include "jgs2_kernels.cuh"
 
@@ -114,6 +115,10 @@ __device__ __forceinline__ bool finiteNonnegInt(float v, float maximum) {
 }
 
 __device__ __forceinline__ bool isPinned(const uint4& info) { return info.z != 0u; }
+
+__device__ __forceinline__ ClothMaterial clothMaterial(const DevParams& p) {
+  return {p.clothLambda, p.clothMu, p.clothThickness, p.clothBending};
+}
 
 __device__ __forceinline__ float distributedInertiaWeight(const float4& rm, const uint4& info, float invDt2) {
   if (isPinned(info)) return 0.0f;
@@ -232,9 +237,10 @@ __device__ __forceinline__ void storeIncident(float4* __restrict__ inc, uint32_t
 // Vertex frame and incident system of a free vertex at pose x in one pass
 // over its incident tets: the frame is the polar of the volume-weighted
 // average F (vertexPolarRotation, jgs2-shader.ts:2959-2989), the system the
-// incident material gradient sum vol P(F) g and Hessian blocks.
-__device__ __forceinline__ void frameAndIncident(const Buffers& b, const float4* __restrict__ x, uint32_t v,
-                                                 const uint4& info, float eps) {
+// incident material gradient sum vol P(F) g and Hessian blocks, plus the
+// cloth membrane and bending terms of the vertex's incident elements.
+__device__ __forceinline__ void frameAndIncident(const Buffers& b, const DevParams& p, const float4* __restrict__ x,
+                                                 uint32_t v, const uint4& info, float eps) {
   M3 avg = mzero();
   float total = 0.0f;
   float3 grad = f3(0, 0, 0);
@@ -250,6 +256,9 @@ __device__ __forceinline__ void frameAndIncident(const Buffers& b, const float4*
     avg = avg + r.vol * F;
     total += r.vol;
   }
+  if (p.cloth)
+    clothLocalSystem<true>(b.clothTris, b.clothHinges, b.clothIncidence, b.clothRange[v], x, clothMaterial(p), 0u, 1u,
+                           grad, hess);
   const M3 favg = total > 0.0f ? (1.0f / total) * avg : midentity();
   storeRot(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, eps));
   storeIncident(b.incident, v, grad, hess);
@@ -721,6 +730,10 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             grad = grad + r.vol * mv(piola(F, pt), g);
             addIncidentBlock(hess, r, F, pt, g);
           }
+          // ---- cloth membrane and bending (jgs2-shader.ts:3113-3186) ----
+          if (p.cloth)
+            clothLocalSystem<true>(b.clothTris, b.clothHinges, b.clothIncidence, b.clothRange[v], src,
+                                   clothMaterial(p), lane, W, grad, hess);
         }
         // Group reduction of the gather.
         grad.x = groupSum<W>(grad.x, mask);
@@ -772,6 +785,8 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
           const float dl = scaledLength(dr.direction);
           if (p.maxStep > 0.0f && dl > p.maxStep) ta = p.maxStep / dl;
           const float controlMin = c0.z;  // accepted-source minimum (finite here)
+          const uint4 cr = p.cloth ? b.clothRange[v] : make_uint4(0u, 0u, 0u, 0u);
+          const ClothMaterial cmat = clothMaterial(p);
           for (uint32_t bt = 0; bt <= kMaxBacktracks; ++bt) {
             const float3 tp = position + ta * dr.direction;
             const float3 td = tp - position;
@@ -819,6 +834,38 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
               de += r.vol * snhEnergyDelta(F, I0, J0, outer(td, shapeGradient(r, entry & 3u)), r.lambda, r.mu, &J);
               if (!finiteS(J)) geomFinite = false;
               jmin = fminf(jmin, J);
+            }
+            // Cloth: signed area stretch at the source and the trial pose
+            // (jgs2-shader.ts:2067-2116) and the membrane / bending energy
+            // deltas (:2207-2263) of the incident elements.
+            const float3 trialPos = position + td;
+            for (uint32_t a = lane; a < cr.y; a += W) {
+              const uint32_t entry = __ldg(&b.clothIncidence[cr.x + a]);
+              const uint32_t slot = entry & 3u;
+              const ClothTri ct = loadClothTri(b.clothTris, entry >> 2);
+              const float3 x0 = xyz(src[ct.i0]), x1 = xyz(src[ct.i1]), x2 = xyz(src[ct.i2]);
+              const float3 y0 = slot == 0u ? trialPos : x0;
+              const float3 y1 = slot == 1u ? trialPos : x1;
+              const float3 y2 = slot == 2u ? trialPos : x2;
+              const float3 sn = clothRawNormal(x0, x1, x2), tn = clothRawNormal(y0, y1, y2);
+              const float twice = 2.0f * ct.area;
+              const float ss = length3(sn) / twice, tm = length3(tn) / twice;
+              const float ts = dot3(sn, tn) > 0.0f ? tm : -tm;
+              if (!(twice > 0.0f) || !finiteS(ss) || !finiteS(ts)) geomFinite = false;
+              jmin = fminf(jmin, fminf(ss, ts));
+              de += clothMembraneEnergy(ct, y0, y1, y2, cmat) - clothMembraneEnergy(ct, x0, x1, x2, cmat);
+            }
+            for (uint32_t a = lane; a < cr.w; a += W) {
+              const uint32_t entry = __ldg(&b.clothIncidence[cr.z + a]);
+              const uint32_t slot = entry & 3u, h = entry >> 2;
+              const uint4 q = hingeIndices(b.clothHinges, h);
+              const float4 rest = __ldg(&b.clothHinges[2ull * h + 1]);
+              const float3 x0 = xyz(src[q.x]), x1 = xyz(src[q.y]), x2 = xyz(src[q.z]), x3 = xyz(src[q.w]);
+              const float es = clothBendingEnergy(x0, x1, x2, x3, rest, cmat.bending);
+              const float et = clothBendingEnergy(slot == 0u ? trialPos : x0, slot == 1u ? trialPos : x1,
+                                                  slot == 2u ? trialPos : x2, slot == 3u ? trialPos : x3, rest,
+                                                  cmat.bending);
+              de += et - es;
             }
             jmin = groupMin<W>(jmin, mask);
             const bool allFinite = __all_sync(mask, geomFinite);
@@ -1016,6 +1063,45 @@ __device__ __forceinline__ void accumulateTet(GatePartial& acc, const TetRec& r,
   if (!cev) acc.bits &= ~kCandidateEnergyValid;
 }
 
+// A cloth triangle as a gate element: its signed area stretch at the source
+// and the candidate (candidateTetrahedron, jgs2-shader.ts:3507-3549), and its
+// membrane energy, which the reference adds to the energy of the triangle's
+// lowest vertex when that vertex's area stretch is above the floor and
+// replaces the vertex energy by kF32Max otherwise (:2585-2621).
+__device__ __forceinline__ void accumulateClothTri(GatePartial& acc, const ClothTri& t, const float4* __restrict__ s,
+                                                   const float4* __restrict__ c, const ClothMaterial& m) {
+  const float3 s0 = xyz(s[t.i0]), s1 = xyz(s[t.i1]), s2 = xyz(s[t.i2]);
+  const float3 c0 = xyz(c[t.i0]), c1 = xyz(c[t.i1]), c2 = xyz(c[t.i2]);
+  const float3 sn = clothRawNormal(s0, s1, s2), cn = clothRawNormal(c0, c1, c2);
+  const float twice = 2.0f * t.area;
+  const float ss = length3(sn) / twice;
+  const float cm = length3(cn) / twice;
+  const float cs = dot3(sn, cn) > 0.0f ? cm : -cm;
+  const bool sgv = twice > 0.0f && finiteV(sn) && finiteS(ss);
+  const bool cgv = twice > 0.0f && finiteV(cn) && finiteS(cs);
+  if (sgv) acc.minS = fminf(acc.minS, ss); else acc.bits &= ~kSourceGeometryValid;
+  if (cgv) acc.minC = fminf(acc.minC, cs); else acc.bits &= ~kCandidateGeometryValid;
+  const float es = (twice > 0.0f && finiteS(ss) && ss > kDeterminantFloor) ? clothMembraneEnergy(t, s0, s1, s2, m)
+                                                                            : kF32Max;
+  const float ec = (twice > 0.0f && finiteS(cm) && cm > kDeterminantFloor) ? clothMembraneEnergy(t, c0, c1, c2, m)
+                                                                            : kF32Max;
+  if (finiteS(es)) acc.e0 += es; else acc.bits &= ~kSourceEnergyValid;
+  if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
+}
+
+// A hinge's bending energy at the source and the candidate (owned by its
+// lowest vertex in the reference, :2623-2642).
+__device__ __forceinline__ void accumulateHinge(GatePartial& acc, const float4* __restrict__ hinges, uint32_t h,
+                                                const float4* __restrict__ s, const float4* __restrict__ c,
+                                                float bending) {
+  const uint4 q = hingeIndices(hinges, h);
+  const float4 rest = __ldg(&hinges[2ull * h + 1]);
+  const float es = clothBendingEnergy(xyz(s[q.x]), xyz(s[q.y]), xyz(s[q.z]), xyz(s[q.w]), rest, bending);
+  const float ec = clothBendingEnergy(xyz(c[q.x]), xyz(c[q.y]), xyz(c[q.z]), xyz(c[q.w]), rest, bending);
+  if (finiteS(es)) acc.e0 += es; else acc.bits &= ~kSourceEnergyValid;
+  if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
+}
+
 // ---------------------------------------------------------------------------
 // Prologue: predict (jgs2-shader.ts:2660-2692), iteration-0 vertex frames and
 // the source feasibility preflight (candidateTetrahedron + reduceCandidate on
@@ -1054,7 +1140,7 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
       b.pos[1][i] = make_float4(o.x, o.y, o.z, 1.0f);
       // Iteration-0 frames (and, for free vertices, the incident system).
       if (isPinned(info)) storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
-      else frameAndIncident(b, b.pos[0], i, info, p.rotationEpsilon);
+      else frameAndIncident(b, p, b.pos[0], i, info, p.rotationEpsilon);
       const float e = implicitEnergy(p, b, i, xyz(o), info);
       if (finiteS(e)) { acc.e0 += e; acc.e1 += e; }
       else acc.bits &= ~(kSourceEnergyValid | kCandidateEnergyValid);
@@ -1063,6 +1149,10 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
       const TetRec r = loadTet(b.tets, sr.tOff + k);
       const M3 F = deformationAt(r, b.pos[0]);
       accumulateTet(acc, r, F, F);
+    }
+    if (p.cloth) {
+      if (k < sr.C) accumulateClothTri(acc, loadClothTri(b.clothTris, sr.cOff + k), b.pos[0], b.pos[0], clothMaterial(p));
+      if (k < sr.H) accumulateHinge(acc, b.clothHinges, sr.hOff + k, b.pos[0], b.pos[0], p.clothBending);
     }
   }
   if (!p.globalization) return;  // no preflight on the co-rotated path (uniform)
@@ -1115,6 +1205,10 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
       const float ec = implicitEnergy(p, b, i, xyz(tgt[i]), info);
       if (finiteS(es)) acc.e0 += es; else acc.bits &= ~kSourceEnergyValid;
       if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
+    }
+    if (p.cloth) {
+      if (k < sr.C) accumulateClothTri(acc, loadClothTri(b.clothTris, sr.cOff + k), src, tgt, clothMaterial(p));
+      if (k < sr.H) accumulateHinge(acc, b.clothHinges, sr.hOff + k, src, tgt, p.clothBending);
     }
   }
   const GatePartial blk = blockFold(acc, smem, gateCombine);
@@ -1206,6 +1300,15 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
         if (nextRotations) addIncidentBlock(hess, r, F, pt, g);
         avg = avg + r.vol * F;
         total += r.vol;
+      }
+      if (p.cloth) {
+        const uint4 cr = b.clothRange[v];
+        if (nextRotations)
+          clothLocalSystem<true>(b.clothTris, b.clothHinges, b.clothIncidence, cr, acc, clothMaterial(p), 0u, 1u,
+                                 material, hess);
+        else
+          clothLocalSystem<false>(b.clothTris, b.clothHinges, b.clothIncidence, cr, acc, clothMaterial(p), 0u, 1u,
+                                  material, hess);
       }
       comps[1] = material;
       comps[2] = f3(0, 0, 0);
@@ -1381,7 +1484,7 @@ static __device__ __align__(256) unsigned char gGateScratch[kGateScratchBytes];
 // failures, valid numerics, history slot 0, one skipped trial per vertex.
 __global__ void __launch_bounds__(kBlock) gateScratchKernel(Buffers b, DevParams p, const float4* __restrict__ src,
                                                             const float4* __restrict__ tgt, uint32_t V, uint32_t T,
-                                                            float4* __restrict__ control,
+                                                            uint32_t C, uint32_t H, float4* __restrict__ control,
                                                             unsigned char* __restrict__ scratch) {
   __shared__ GatePartial smem[kBlock];
   __shared__ bool isLast;
@@ -1400,6 +1503,8 @@ __global__ void __launch_bounds__(kBlock) gateScratchKernel(Buffers b, DevParams
     if (finiteS(es)) acc.e0 += es; else acc.bits &= ~kSourceEnergyValid;
     if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
   }
+  if (i < C) accumulateClothTri(acc, loadClothTri(b.clothTris, i), src, tgt, clothMaterial(p));
+  if (i < H) accumulateHinge(acc, b.clothHinges, i, src, tgt, p.clothBending);
   const GatePartial blk = blockFold(acc, smem, gateCombine);
   if (!publishPartial(blk, partials, blockIdx.x, gridDim.x, ticket, &isLast)) return;
   const GatePartial tot = foldPartials(partials, gridDim.x, smem, gateIdentity, gateCombine);
@@ -1530,12 +1635,13 @@ cudaError_t gateScratchAddress(void** out) { return cudaGetSymbolAddress(out, gG
 uint32_t gateScratchMaxElements() { return kGateScratchMaxBlocks * static_cast<uint32_t>(kBlock); }
 
 int launchGateScratch(const Buffers& b, const DevParams& p, const float4* predicted, const float4* src,
-                      const float4* tgt, uint32_t V, uint32_t T, float4* control, void* scratch, cudaStream_t s) {
-  const uint32_t n = T > V ? T : V;
+                      const float4* tgt, uint32_t V, uint32_t T, uint32_t C, uint32_t H, float4* control,
+                      void* scratch, cudaStream_t s) {
+  const uint32_t n = std::max(std::max(T, V), std::max(C, H));
   if (n == 0 || n > gateScratchMaxElements()) return 0;
   Buffers view = b;
   view.predicted = const_cast<float4*>(predicted);
-  gateScratchKernel<<<blocksFor(n), kBlock, 0, s>>>(view, p, src, tgt, V, T, control,
+  gateScratchKernel<<<blocksFor(n), kBlock, 0, s>>>(view, p, src, tgt, V, T, C, H, control,
                                                    static_cast<unsigned char*>(scratch));
   return 1;
 }

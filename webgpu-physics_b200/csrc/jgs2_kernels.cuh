@@ -25,7 +25,9 @@ struct DevParams {
   uint32_t vertexCount, tetCount, cubatureK, bodyCount;
   uint32_t bodyCorrection;  // horizontal body correction in the epilogue
   uint32_t active;          // 0: the scene sits this frame out (no state changes)
-  uint32_t pad[2];
+  uint32_t cloth;           // the scene has cloth triangles
+  // Cloth material (the cloth arena's second global vec4, cloth-layout.ts:45-50).
+  float clothLambda, clothMu, clothThickness, clothBending;
 };
 
 // One scene of a batch: its slices of the concatenated vertex and tet arrays
@@ -35,6 +37,7 @@ struct SceneRange {
   uint32_t vOff, V, tOff, T;
   uint32_t gateBase, gateBlocks;  // prologue / gate partials of this scene
   uint32_t convBase, convBlocks;  // convergence partials of this scene
+  uint32_t cOff, C, hOff, H;      // cloth triangles and hinges of this scene
 };
 
 // One block of a segmented reduction: elements [begin, end) of `scene`,
@@ -96,6 +99,15 @@ struct Buffers {
   const SceneRange* scenes;
   const RedBlock* gateTable;    // prologue / gate blocks
   const RedBlock* convTable;    // convergence blocks
+  // Triangle cloth (all null when no scene has cloth): two float4 per
+  // triangle (indices as uint + rest area, inverse rest basis), two per hinge
+  // (indices as uint, rest angle and edge length), per vertex the incidence
+  // ranges (triangle begin, count, hinge begin, count) into `clothIncidence`
+  // (element * 4 + local slot).
+  const float4* clothTris;
+  const float4* clothHinges;
+  const uint4* clothRange;
+  const uint32_t* clothIncidence;
   uint32_t gateBlocks, convBlocks, sceneCount, pad;
 };
 
@@ -136,8 +148,10 @@ cudaError_t gateScratchAddress(void** out);
 uint32_t gateScratchMaxElements();
 // Launches the gate over caller device arrays with `scratch` (the address of
 // the static array on the current device); writes 4 float4 to `control`.
-// Returns 0 without launching when max(V, T) is 0 or over the limit.
+// C / H: cloth triangles and hinges.  Returns 0 without launching when
+// max(V, T, C, H) is 0 or over the limit.
 int launchGateScratch(const Buffers& b, const DevParams& p, const float4* predicted, const float4* src,
-                      const float4* tgt, uint32_t V, uint32_t T, float4* control, void* scratch, cudaStream_t s);
+                      const float4* tgt, uint32_t V, uint32_t T, uint32_t C, uint32_t H, float4* control,
+                      void* scratch, cudaStream_t s);
 
 }  // namespace jgs2

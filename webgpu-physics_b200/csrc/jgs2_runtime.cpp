@@ -342,6 +342,75 @@ bool validateInput(const jgs2_input* in, std::string* err) {
       return false;
     }
   }
+  if (in->cloth) {
+    // validateJGS2GpuClothInput (cloth-layout.ts:225-332) and the vertex
+    // count agreement of validateJGS2GpuInput (layout.ts:247-253).
+    const jgs2_cloth_input& c = *in->cloth;
+    if (c.vertex_count != V) {
+      *err = format("Cloth vertexCount %u must equal solver vertexCount %u.", c.vertex_count, V);
+      return false;
+    }
+    const uint32_t C = c.triangle_count, H = c.hinge_count;
+    if ((C > 0 && (!c.triangle_indices || !c.triangle_inverse_rest_bases || !c.triangle_rest_areas)) ||
+        (H > 0 && (!c.hinge_indices || !c.hinge_rest_angles || !c.hinge_rest_edge_lengths))) {
+      *err = "A required cloth array is NULL.";
+      return false;
+    }
+    if (C >= (1u << 29) || H >= (1u << 29)) { *err = "Cloth element counts must be below 2^29."; return false; }
+    auto distinct = [&](const uint32_t* q, int n, const char* label, uint32_t e) {
+      for (int a = 0; a < n; ++a) {
+        if (q[a] >= V) {
+          *err = format("%s %u index %u is outside vertexCount %u.", label, e, q[a], V);
+          return false;
+        }
+        for (int b = 0; b < a; ++b)
+          if (q[a] == q[b]) {
+            *err = format("%s %u must reference %d distinct vertices.", label, e, n);
+            return false;
+          }
+      }
+      return true;
+    };
+    for (uint32_t t = 0; t < C; ++t)
+      if (!distinct(&c.triangle_indices[3ull * t], 3, "Triangle", t)) return false;
+    for (uint32_t h = 0; h < H; ++h)
+      if (!distinct(&c.hinge_indices[4ull * h], 4, "Hinge", h)) return false;
+    if (!finiteArray(c.triangle_inverse_rest_bases, 4ull * C, "triangleInverseRestBases") ||
+        !finiteArray(c.triangle_rest_areas, C, "triangleRestAreas") ||
+        !finiteArray(c.hinge_rest_angles, H, "hingeRestAngles") ||
+        !finiteArray(c.hinge_rest_edge_lengths, H, "hingeRestEdgeLengths"))
+      return false;
+    for (uint32_t t = 0; t < C; ++t) {
+      if (!(c.triangle_rest_areas[t] > 0)) { *err = format("triangleRestAreas[%u] must be positive.", t); return false; }
+      const float* b = &c.triangle_inverse_rest_bases[4ull * t];
+      const float d = b[0] * b[3] - b[1] * b[2];
+      if (d == 0 || !std::isfinite(d)) {
+        *err = format("triangleInverseRestBases for triangle %u must be invertible.", t);
+        return false;
+      }
+    }
+    for (uint32_t h = 0; h < H; ++h)
+      if (!(c.hinge_rest_edge_lengths[h] > 0)) {
+        *err = format("hingeRestEdgeLengths[%u] must be positive.", h);
+        return false;
+      }
+    if (!(c.young_modulus > 0) || !std::isfinite(c.young_modulus)) {
+      *err = "Cloth Young's modulus must be finite and positive.";
+      return false;
+    }
+    if (!(c.poisson_ratio >= 0 && c.poisson_ratio < 0.5f)) {
+      *err = "Cloth Poisson ratio must be finite and in [0, 0.5).";
+      return false;
+    }
+    if (!(c.thickness > 0) || !std::isfinite(c.thickness)) {
+      *err = "Cloth thickness must be finite and positive.";
+      return false;
+    }
+    if (!(c.bending_stiffness >= 0) || !std::isfinite(c.bending_stiffness)) {
+      *err = "Cloth bending stiffness must be finite and nonnegative.";
+      return false;
+    }
+  }
   return true;
 }
 
@@ -374,6 +443,10 @@ std::vector<uint32_t> colorInput(const jgs2_input* in, uint32_t* count) {
                              in->tet_indices[4ull * t + 2], in->tet_indices[4ull * t + 3]};
       group(g, 5);
     }
+  if (in->cloth) {
+    for (uint32_t c = 0; c < in->cloth->triangle_count; ++c) group(&in->cloth->triangle_indices[3ull * c], 3);
+    for (uint32_t h = 0; h < in->cloth->hinge_count; ++h) group(&in->cloth->hinge_indices[4ull * h], 4);
+  }
   std::vector<uint32_t> colors(V, 0xffffffffu), stamp(V + 1, 0);
   uint32_t n = 0, st = 0;
   for (uint32_t v = 0; v < V; ++v) {
@@ -425,6 +498,8 @@ namespace {
 // Host state of one scene.
 struct SceneHost {
   uint32_t V = 0, T = 0, K = 0, vOff = 0, tOff = 0, bodyOff = 0, bodies = 1;
+  uint32_t C = 0, H = 0, cOff = 0, hOff = 0;  // cloth triangles / hinges and their offsets
+  float clothLambda = 0.f, clothMu = 0.f, clothThickness = 0.f, clothBending = 0.f;
   float sceneScale = 1.f;
   float preprocessingTimestep = 0.f;
   jgs2_settings defaults{};
@@ -445,6 +520,7 @@ struct Engine {
   bool destroyed = false;
   std::string error;
   uint32_t V = 0, T = 0, K = 0, bodies = 1;  // totals over the scenes; K = widest record count
+  uint32_t C = 0, H = 0;                     // cloth triangles and hinges over the scenes
   bool glob = true;
   std::vector<SceneHost> scenes;
   // Colour lists over all scenes: colour c holds every scene's colour-c vertices.
@@ -584,6 +660,11 @@ DevParams makeParams(const Engine* s, uint32_t scene, const jgs2_settings& st, b
   p.bodyCount = sc.bodies;
   p.bodyCorrection = st.horizontal_body_correction ? 1u : 0u;
   p.active = sc.active ? 1u : 0u;
+  p.cloth = (sc.C > 0 || sc.H > 0) ? 1u : 0u;
+  p.clothLambda = sc.clothLambda;
+  p.clothMu = sc.clothMu;
+  p.clothThickness = sc.clothThickness;
+  p.clothBending = sc.clothBending;
   return p;
 }
 
@@ -857,6 +938,8 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
                 "precomputation.");
   out->in = in;
   out->stable = stable == in->tet_count;
+  if (in->cloth && in->cloth->triangle_count > 0 && !out->stable)
+    return fail(nullptr, JGS2_INVALID_ARGUMENT, "Triangle cloth requires the stable Neo-Hookean production path.");
   out->colored = colour;
   if (colour) out->colors = colorInput(in, &out->colorCount);
   if (out->colorCount > JGS2_MAX_SCHEDULE_COLORS)
@@ -904,7 +987,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       return fail(nullptr, JGS2_INVALID_ARGUMENT,
                   "A batch cannot mix stable Neo-Hookean scenes with co-rotated linear scenes.");
   sp->scenes.resize(S);
-  uint64_t V = 0, T = 0, bodies = 0;
+  uint64_t V = 0, T = 0, bodies = 0, C = 0, H = 0;
   uint32_t K = 0, colorCount = 1;
   for (uint32_t i = 0; i < S; ++i) {
     const jgs2_input* in = prep[i].in;
@@ -915,6 +998,21 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     sc.vOff = static_cast<uint32_t>(V);
     sc.tOff = static_cast<uint32_t>(T);
     sc.bodyOff = static_cast<uint32_t>(bodies);
+    sc.cOff = static_cast<uint32_t>(C);
+    sc.hOff = static_cast<uint32_t>(H);
+    if (const jgs2_cloth_input* cl = in->cloth) {
+      sc.C = cl->triangle_count;
+      sc.H = cl->hinge_count;
+      // packJGS2GpuClothArena (cloth-layout.ts:358-372): plane-stress Lame
+      // parameters formed in double, stored as f32.
+      const double E = cl->young_modulus, nu = cl->poisson_ratio;
+      sc.clothLambda = static_cast<float>(E * nu / (1 - nu * nu));
+      sc.clothMu = static_cast<float>(E / (2 * (1 + nu)));
+      sc.clothThickness = cl->thickness;
+      sc.clothBending = cl->bending_stiffness;
+      C += sc.C;
+      H += sc.H;
+    }
     uint32_t maxBody = 0;
     for (uint32_t v = 0; v < sc.V; ++v) maxBody = std::max(maxBody, in->vertex_info[4ull * v + 3]);
     sc.bodies = maxBody + 1;
@@ -930,10 +1028,12 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     K = std::max(K, sc.K);
     colorCount = std::max(colorCount, sc.colorCount);
   }
-  if (V > 0xffffffffull / 16 || T > 0xffffffffull / 16)
+  if (V > 0xffffffffull / 16 || T > 0xffffffffull / 16 || C > 0xffffffffull / 16 || H > 0xffffffffull / 16)
     return fail(nullptr, JGS2_INVALID_ARGUMENT, "The scenes together exceed the engine's index range.");
   sp->V = static_cast<uint32_t>(V);
   sp->T = static_cast<uint32_t>(T);
+  sp->C = static_cast<uint32_t>(C);
+  sp->H = static_cast<uint32_t>(H);
   sp->K = K;
   sp->bodies = static_cast<uint32_t>(bodies);
   sp->coloringBuilt = true;
@@ -1080,6 +1180,55 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       }
     }
   });
+  // Cloth (packJGS2GpuClothArena, cloth-layout.ts:335-452, in this engine's
+  // layout): triangles and hinges with global indices, and per vertex its
+  // incident triangles then hinges in ascending element order, each entry
+  // element * 4 + the vertex's local slot.
+  const uint32_t nC = sp->C, nH = sp->H;
+  const bool anyCloth = nC + nH > 0;
+  std::vector<float4> clothTris(2ull * nC), clothHinges(2ull * nH);
+  std::vector<uint4> clothRange(anyCloth ? nV : 0, make_uint4(0u, 0u, 0u, 0u));
+  std::vector<uint32_t> incidence(3ull * nC + 4ull * nH);
+  if (anyCloth) parallelFor(S, [&](uint32_t i) {
+    const jgs2_cloth_input* cl = prep[i].in->cloth;
+    const SceneHost& sc = sp->scenes[i];
+    if (!cl || sc.C + sc.H == 0) return;
+    auto bits = [](uint32_t u) { float f; std::memcpy(&f, &u, 4); return f; };
+    std::vector<uint32_t> tRows(sc.V + 1, 0), hRows(sc.V + 1, 0);
+    for (uint32_t c = 0; c < sc.C; ++c) {
+      const uint32_t* q = &cl->triangle_indices[3ull * c];
+      const float* inv = &cl->triangle_inverse_rest_bases[4ull * c];
+      const size_t g = sc.cOff + c;
+      clothTris[2 * g] = make_float4(bits(sc.vOff + q[0]), bits(sc.vOff + q[1]), bits(sc.vOff + q[2]),
+                                     cl->triangle_rest_areas[c]);
+      clothTris[2 * g + 1] = make_float4(inv[0], inv[1], inv[2], inv[3]);
+      for (int l = 0; l < 3; ++l) tRows[q[l] + 1]++;
+    }
+    for (uint32_t h = 0; h < sc.H; ++h) {
+      const uint32_t* q = &cl->hinge_indices[4ull * h];
+      const size_t g = sc.hOff + h;
+      clothHinges[2 * g] = make_float4(bits(sc.vOff + q[0]), bits(sc.vOff + q[1]), bits(sc.vOff + q[2]),
+                                       bits(sc.vOff + q[3]));
+      clothHinges[2 * g + 1] = make_float4(cl->hinge_rest_angles[h], cl->hinge_rest_edge_lengths[h], 0.f, 0.f);
+      for (int l = 0; l < 4; ++l) hRows[q[l] + 1]++;
+    }
+    for (uint32_t v = 0; v < sc.V; ++v) {
+      tRows[v + 1] += tRows[v];
+      hRows[v + 1] += hRows[v];
+    }
+    const uint32_t triBase = 3u * sc.cOff, hingeBase = 3u * nC + 4u * sc.hOff;
+    for (uint32_t v = 0; v < sc.V; ++v)
+      clothRange[sc.vOff + v] = make_uint4(triBase + tRows[v], tRows[v + 1] - tRows[v], hingeBase + hRows[v],
+                                           hRows[v + 1] - hRows[v]);
+    std::vector<uint32_t> cursor(tRows.begin(), tRows.end() - 1);
+    for (uint32_t c = 0; c < sc.C; ++c)
+      for (uint32_t l = 0; l < 3; ++l)
+        incidence[triBase + cursor[cl->triangle_indices[3ull * c + l]]++] = (sc.cOff + c) * 4u + l;
+    cursor.assign(hRows.begin(), hRows.end() - 1);
+    for (uint32_t h = 0; h < sc.H; ++h)
+      for (uint32_t l = 0; l < 4; ++l)
+        incidence[hingeBase + cursor[cl->hinge_indices[4ull * h + l]]++] = (sc.hOff + h) * 4u + l;
+  });
   // Segmented reduction tables: each scene's elements in fixed chunks.
   std::vector<jgs2::SceneRange> ranges(S);
   std::vector<jgs2::RedBlock> gateTable, convTable;
@@ -1087,7 +1236,8 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     const SceneHost& sc = sp->scenes[i];
     jgs2::SceneRange& r = ranges[i];
     r.vOff = sc.vOff; r.V = sc.V; r.tOff = sc.tOff; r.T = sc.T;
-    const uint32_t n = std::max(sc.V, sc.T);
+    r.cOff = sc.cOff; r.C = sc.C; r.hOff = sc.hOff; r.H = sc.H;
+    const uint32_t n = std::max(std::max(sc.V, sc.T), std::max(sc.C, sc.H));
     r.gateBase = static_cast<uint32_t>(gateTable.size());
     for (uint32_t b0 = 0; b0 < std::max(n, 1u); b0 += jgs2::kGateChunk)
       gateTable.push_back({i, b0, std::min(n, b0 + jgs2::kGateChunk), static_cast<uint32_t>(gateTable.size())});
@@ -1191,6 +1341,23 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     uint32_t* cl = nullptr;
     STEP(upload(sp, &cl, colors.data(), nV));
     b.colors = cl;
+    b.clothTris = b.clothHinges = nullptr;
+    b.clothRange = nullptr;
+    b.clothIncidence = nullptr;
+    if (anyCloth) {
+      float4* ct = nullptr;
+      float4* ch = nullptr;
+      uint4* cr = nullptr;
+      uint32_t* ci = nullptr;
+      STEP(upload(sp, &ct, clothTris.data(), clothTris.size()));
+      STEP(upload(sp, &ch, clothHinges.data(), clothHinges.size()));
+      STEP(upload(sp, &cr, clothRange.data(), clothRange.size()));
+      STEP(upload(sp, &ci, incidence.data(), incidence.size()));
+      b.clothTris = ct;
+      b.clothHinges = ch;
+      b.clothRange = cr;
+      b.clothIncidence = ci;
+    }
     STEP(upload(sp, &sp->dColorVertices, byColor.data(), byColor.size()));
     STEP(upload(sp, &sp->dNeedVertices, need.data(), need.size()));
     STEP(deviceAlloc(sp, &sp->dParams, S));
@@ -1303,6 +1470,7 @@ jgs2_status sceneInfo(Engine* s, uint32_t scene, jgs2_info* out) {
   out->scene_scale = sc.sceneScale;
   out->preprocessing_timestep = sc.preprocessingTimestep;
   out->current_position_buffer = 0;
+  out->cloth_triangle_count = sc.C;
   if (sc.recordsAvailable) {
     float4 c1;
     if (readRegion(s, &s->b.frames[scene].control[1], sizeof(c1), &c1) == JGS2_OK)
@@ -1710,11 +1878,12 @@ jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* s, const float* source, co
     if (reinterpret_cast<uintptr_t>(p) % 16 != 0)
       return fail(s, JGS2_INVALID_ARGUMENT, "The no-allocation gate's device arrays must be 16-byte aligned.");
   const uint32_t limit = jgs2::gateScratchMaxElements();
-  if (std::max(s->V, s->T) > limit)
+  if (std::max(std::max(s->V, s->T), std::max(s->C, s->H)) > limit)
     return fail(s, JGS2_INVALID_ARGUMENT,
-                format("The no-allocation gate handles at most %u vertices and %u tetrahedra (its static scratch "
-                       "holds %u block partials); this solver has %u vertices and %u tetrahedra.",
-                       limit, limit, jgs2::kGateScratchMaxBlocks, s->V, s->T));
+                format("The no-allocation gate handles at most %u vertices, tetrahedra, cloth triangles and hinges "
+                       "(its static scratch holds %u block partials); this solver has %u vertices, %u tetrahedra, "
+                       "%u triangles and %u hinges.",
+                       limit, jgs2::kGateScratchMaxBlocks, s->V, s->T, s->C, s->H));
   if (s->device < 0 || s->device >= kMaxScratchDevices)
     return fail(s, JGS2_UNSUPPORTED, format("The no-allocation gate supports device ordinals below %d.",
                                             kMaxScratchDevices));
@@ -1738,8 +1907,8 @@ jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* s, const float* source, co
   cudaStream_t launchStream = stream ? static_cast<cudaStream_t>(stream) : s->stream;
   const int launched = jgs2::launchGateScratch(
       s->b, p, reinterpret_cast<const float4*>(predicted), reinterpret_cast<const float4*>(source),
-      reinterpret_cast<const float4*>(candidate), s->V, s->T, reinterpret_cast<float4*>(control), scratch,
-      launchStream);
+      reinterpret_cast<const float4*>(candidate), s->V, s->T, s->C, s->H, reinterpret_cast<float4*>(control),
+      scratch, launchStream);
   if (launched == 0) return fail(s, JGS2_INVALID_ARGUMENT, "The no-allocation gate was given an empty mesh.");
   CUDA_TRY(s, cudaGetLastError());
   s->launches += static_cast<uint64_t>(launched);
@@ -1904,8 +2073,12 @@ uint64_t jgs2_estimate_device_bytes(const jgs2_input* in) {
   // local records (4), incident system (3), rest/mass, info, force, target
   // (16 bytes each), final update, colour, scene id; per record a 32-byte
   // header and 144 bytes of basis; per tet a 64-byte record, four adjacency
-  // entries and a share of the reduction partials.
-  return V * (16 * 20 + 12) + V * K * (32 + 144) + T * (64 + 16 + 1) + (1u << 16);
+  // entries and a share of the reduction partials; per cloth triangle and
+  // hinge a 32-byte record and one incidence entry per vertex, plus a
+  // 16-byte incidence range per vertex.
+  const uint64_t C = in->cloth ? in->cloth->triangle_count : 0, H = in->cloth ? in->cloth->hinge_count : 0;
+  const uint64_t cloth = (C + H) ? V * 16 + C * (32 + 12) + H * (32 + 16) : 0;
+  return V * (16 * 20 + 12) + V * K * (32 + 144) + T * (64 + 16 + 1) + cloth + (1u << 16);
 }
 
 }  // extern "C"

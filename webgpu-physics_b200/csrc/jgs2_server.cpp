@@ -33,6 +33,9 @@ struct OwnedInput {
   std::vector<float> positions, velocities, rest, colors, forces, targets, stiff, invDm, meta, restStiffness;
   std::vector<float> cubW, cubBasis;
   std::vector<uint32_t> info, tets, adjacency, cubTet;
+  jgs2_cloth_input cloth{};
+  std::vector<uint32_t> clothTris, hinges;
+  std::vector<float> clothInv, clothAreas, hingeAngles, hingeLengths;
 
   template <class T>
   static const T* take(std::vector<T>& dst, const T* src, size_t n) {
@@ -60,6 +63,18 @@ struct OwnedInput {
     view.cubature_tet_ids = take(cubTet, in.cubature_tet_ids, V * K);
     view.cubature_weights = take(cubW, in.cubature_weights, V * K);
     view.cubature_basis = take(cubBasis, in.cubature_basis, 36 * V * K);
+    if (in.cloth) {
+      const jgs2_cloth_input& c = *in.cloth;
+      const size_t C = c.triangle_count, H = c.hinge_count;
+      cloth = c;
+      cloth.triangle_indices = take(clothTris, c.triangle_indices, 3 * C);
+      cloth.triangle_inverse_rest_bases = take(clothInv, c.triangle_inverse_rest_bases, 4 * C);
+      cloth.triangle_rest_areas = take(clothAreas, c.triangle_rest_areas, C);
+      cloth.hinge_indices = take(hinges, c.hinge_indices, 4 * H);
+      cloth.hinge_rest_angles = take(hingeAngles, c.hinge_rest_angles, H);
+      cloth.hinge_rest_edge_lengths = take(hingeLengths, c.hinge_rest_edge_lengths, H);
+      view.cloth = &cloth;
+    }
   }
 };
 

@@ -4,6 +4,7 @@
 #include <algorithm>
 #include <cstring>
 #include <stdexcept>
+#include <unordered_map>
 
 #include "scene_internal.hpp"
 
@@ -246,7 +247,127 @@ bool computeRest(Scene& s) {
     const double vm = s.materialTable[s.mesh.materials[t]].density * vol / 4.0;
     for (int l = 0; l < 4; ++l) s.masses[q[l]] += vm;
   }
+  // validateAndAddClothMasses (src/simulation/cpu/precompute.ts:44-95): each
+  // cloth triangle adds density * thickness * area / 3 to its vertices.
+  if (s.cloth.present) {
+    const size_t C = s.cloth.triangles.size() / 3;
+    for (size_t c = 0; c < C; ++c) {
+      const uint32_t* q = &s.cloth.triangles[3 * c];
+      double e1[3], e2[3], n[3];
+      for (int k = 0; k < 3; ++k) {
+        e1[k] = p[3ull * q[1] + k] - p[3ull * q[0] + k];
+        e2[k] = p[3ull * q[2] + k] - p[3ull * q[0] + k];
+      }
+      n[0] = e1[1] * e2[2] - e1[2] * e2[1];
+      n[1] = e1[2] * e2[0] - e1[0] * e2[2];
+      n[2] = e1[0] * e2[1] - e1[1] * e2[0];
+      const double area = 0.5 * std::sqrt(n[0] * n[0] + n[1] * n[1] + n[2] * n[2]);
+      if (!(area > 1e-12) || !std::isfinite(area)) {
+        s.error = "Cloth triangle " + std::to_string(c) + " must be nondegenerate.";
+        return false;
+      }
+      const double vm = s.cloth.density * s.cloth.thickness * area / 3.0;
+      for (int l = 0; l < 3; ++l) s.masses[q[l]] += vm;
+    }
+  }
   s.restValid = true;
+  return true;
+}
+
+// ---- cloth rest data (src/simulation/cpu/cloth.ts:107-140, 237-334) --------
+
+double norm3(const double* v) { return std::sqrt(v[0] * v[0] + v[1] * v[1] + v[2] * v[2]); }
+
+// assertNondegenerateTriangle (cloth.ts:90-104): twice the area, or -1.
+double nondegenerateTwiceArea(const double* e0, const double* e1) {
+  double c[3];
+  cross3(e0, e1, c);
+  const double twiceArea = norm3(c);
+  const double d[3] = {e1[0] - e0[0], e1[1] - e0[1], e1[2] - e0[2]};
+  const double scale = std::max(norm3(e0), std::max(norm3(e1), norm3(d)));
+  if (!(scale > 0) || !(twiceArea > 1e-12 * scale * scale)) return -1.0;
+  return twiceArea;
+}
+
+// precomputeStVKTriangleRest (cloth.ts:111-140): the intrinsic 2D basis has
+// its first axis along rest edge (0, 1); returns the row-major inverse of
+// Dm = [[|e01|, x], [0, y]] and the rest area.
+bool clothTriangleRest(const double* x0, const double* x1, const double* x2, double inverse[4], double* area) {
+  const double e01[3] = {x1[0] - x0[0], x1[1] - x0[1], x1[2] - x0[2]};
+  const double e02[3] = {x2[0] - x0[0], x2[1] - x0[1], x2[2] - x0[2]};
+  const double twiceArea = nondegenerateTwiceArea(e01, e02);
+  if (twiceArea < 0) return false;
+  const double length = norm3(e01);
+  const double tangent[3] = {e01[0] / length, e01[1] / length, e01[2] / length};
+  double normal[3];
+  cross3(e01, e02, normal);
+  for (double& c : normal) c /= twiceArea;
+  double bitangent[3];
+  cross3(normal, tangent, bitangent);
+  const double mx = e02[0] * tangent[0] + e02[1] * tangent[1] + e02[2] * tangent[2];
+  const double my = e02[0] * bitangent[0] + e02[1] * bitangent[1] + e02[2] * bitangent[2];
+  inverse[0] = 1.0 / length;
+  inverse[1] = -mx / (length * my);
+  inverse[2] = 0.0;
+  inverse[3] = 1.0 / my;
+  *area = 0.5 * twiceArea;
+  return true;
+}
+
+// precomputeQuadraticDihedralRest (cloth.ts:316-321) through the angle of
+// evaluateSignedDihedral (cloth.ts:237-312) for the oriented hinge
+// (0, 1, 2) / (1, 0, 3).
+bool clothHingeRest(const double* x0, const double* x1, const double* x2, const double* x3, double* angle,
+                    double* edgeLength) {
+  const double edge[3] = {x1[0] - x0[0], x1[1] - x0[1], x1[2] - x0[2]};
+  const double length = norm3(edge);
+  if (!(length > 0)) return false;
+  const double to2[3] = {x2[0] - x0[0], x2[1] - x0[1], x2[2] - x0[2]};
+  const double reverse[3] = {-edge[0], -edge[1], -edge[2]};
+  const double to3[3] = {x3[0] - x1[0], x3[1] - x1[1], x3[2] - x1[2]};
+  const double l0 = nondegenerateTwiceArea(edge, to2);
+  const double l1 = nondegenerateTwiceArea(reverse, to3);
+  if (l0 < 0 || l1 < 0) return false;
+  double n0[3], n1[3], nc[3];
+  cross3(edge, to2, n0);
+  cross3(reverse, to3, n1);
+  for (int k = 0; k < 3; ++k) { n0[k] /= l0; n1[k] /= l1; }
+  cross3(n0, n1, nc);
+  const double sine = (edge[0] * nc[0] + edge[1] * nc[1] + edge[2] * nc[2]) / length;
+  const double cosine = n0[0] * n1[0] + n0[1] * n1[1] + n0[2] * n1[2];
+  *angle = std::atan2(sine, cosine);
+  *edgeLength = length;
+  return true;
+}
+
+// Hinges of buildJGS2GpuClothInput (src/scenes/index.ts:893-933): every
+// interior edge shared by two consistently oriented triangles gives one
+// hinge (first, second, opposite of the first triangle, opposite of the
+// second); an edge with three triangles or opposite windings is an error.
+bool buildHinges(const std::vector<uint32_t>& triangles, std::vector<uint32_t>* hinges, std::string* err) {
+  struct HalfEdge { uint32_t first, second, opposite; };
+  std::unordered_map<uint64_t, HalfEdge> open;
+  std::unordered_map<uint64_t, bool> closed;
+  auto add = [&](uint32_t a, uint32_t b, uint32_t o) {
+    const uint64_t key = (static_cast<uint64_t>(std::min(a, b)) << 32) | std::max(a, b);
+    const std::string name = std::to_string(std::min(a, b)) + ":" + std::to_string(std::max(a, b));
+    if (closed.count(key)) { *err = "Cloth edge " + name + " is non-manifold."; return false; }
+    auto it = open.find(key);
+    if (it == open.end()) { open.emplace(key, HalfEdge{a, b, o}); return true; }
+    const HalfEdge prev = it->second;
+    if (prev.first != b || prev.second != a) {
+      *err = "Cloth triangles sharing edge " + name + " must have consistent orientation.";
+      return false;
+    }
+    hinges->insert(hinges->end(), {prev.first, prev.second, prev.opposite, o});
+    open.erase(it);
+    closed.emplace(key, true);
+    return true;
+  };
+  for (size_t c = 0; c < triangles.size() / 3; ++c) {
+    const uint32_t i0 = triangles[3 * c], i1 = triangles[3 * c + 1], i2 = triangles[3 * c + 2];
+    if (!add(i0, i1, i2) || !add(i1, i2, i0) || !add(i2, i0, i1)) return false;
+  }
   return true;
 }
 
@@ -395,6 +516,56 @@ int64_t jgs2_scene_add_mesh(jgs2_scene* s, uint32_t vertex_count, const double* 
   return static_cast<int64_t>(base);
 }
 
+int64_t jgs2_scene_add_cloth(jgs2_scene* s, uint32_t vertex_count, const double* positions,
+                             uint32_t triangle_count, const uint32_t* triangles, const uint8_t* pinned,
+                             uint32_t body, double density, double young_modulus, double poisson_ratio,
+                             double thickness, double bending_stiffness) {
+  if (!s || !positions || !triangles || vertex_count == 0 || triangle_count == 0) return -1;
+  // validateAndAddClothMasses (src/simulation/cpu/precompute.ts:44-78).
+  if (!(density > 0) || !std::isfinite(density)) return fail(s, "Cloth density must be finite and positive."), -1;
+  if (!(young_modulus > 0) || !std::isfinite(young_modulus))
+    return fail(s, "Cloth youngModulus must be finite and positive."), -1;
+  if (!(thickness > 0) || !std::isfinite(thickness))
+    return fail(s, "Cloth thickness must be finite and positive."), -1;
+  if (!std::isfinite(poisson_ratio) || poisson_ratio < 0 || poisson_ratio >= 0.5)
+    return fail(s, "Cloth poissonRatio must be in [0, 0.5)."), -1;
+  if (!std::isfinite(bending_stiffness) || bending_stiffness < 0)
+    return fail(s, "Cloth bendingStiffness must be finite and nonnegative."), -1;
+  Cloth& c = s->cloth;
+  if (c.present && (c.density != density || c.young != young_modulus || c.poisson != poisson_ratio ||
+                    c.thickness != thickness || c.bending != bending_stiffness))
+    return fail(s, "A scene holds one cloth material; a second sheet must use the same one."), -1;
+  const uint64_t base = s->mesh.vertexCount();
+  if (base + vertex_count > 0xfffffff0ull) return fail(s, "Scene exceeds 32-bit index space."), -1;
+  std::vector<double> pos(positions, positions + 3ull * vertex_count);
+  for (double v : pos)
+    if (!std::isfinite(v)) return fail(s, "Cloth positions must be finite."), -1;
+  std::vector<uint32_t> tri(triangles, triangles + 3ull * triangle_count);
+  for (uint32_t t = 0; t < triangle_count; ++t) {
+    const uint32_t a = tri[3ull * t], b = tri[3ull * t + 1], d = tri[3ull * t + 2];
+    if (a >= vertex_count || b >= vertex_count || d >= vertex_count || a == b || a == d || b == d)
+      return fail(s, "Cloth triangle " + std::to_string(t) + " has invalid vertex indices."), -1;
+  }
+  auto& m = s->mesh;
+  m.positions.insert(m.positions.end(), pos.begin(), pos.end());
+  for (uint32_t v = 0; v < vertex_count; ++v) m.fixed.push_back(pinned ? (pinned[v] ? 1 : 0) : 0);
+  m.bodies.insert(m.bodies.end(), vertex_count, body);
+  for (auto& v : tri) v += static_cast<uint32_t>(base);
+  c.triangles.insert(c.triangles.end(), tri.begin(), tri.end());
+  c.present = true;
+  c.density = density;
+  c.young = young_modulus;
+  c.poisson = poisson_ratio;
+  c.thickness = thickness;
+  c.bending = bending_stiffness;
+  invalidate(*s);
+  return static_cast<int64_t>(base);
+}
+
+uint32_t jgs2_scene_cloth_triangle_count(const jgs2_scene* s) {
+  return s ? static_cast<uint32_t>(s->cloth.triangles.size() / 3) : 0;
+}
+
 jgs2_status jgs2_scene_set_pinned(jgs2_scene* s, const uint8_t* pinned) {
   if (!s || !pinned) return JGS2_INVALID_ARGUMENT;
   for (uint32_t v = 0; v < s->mesh.vertexCount(); ++v) s->mesh.fixed[v] = pinned[v] ? 1 : 0;
@@ -536,7 +707,56 @@ jgs2_status jgs2_scene_pack(jgs2_scene* s, jgs2_input* out) {
   } else {
     s->packStiffness.clear();
   }
+  // buildJGS2GpuClothInput (src/scenes/index.ts:881-973): rest bases, areas,
+  // hinges and rest dihedrals in double, stored as f32.
+  const bool cloth = s->cloth.present;
+  if (cloth) {
+    const auto& tri = s->cloth.triangles;
+    const size_t C = tri.size() / 3;
+    s->packClothTriangles = tri;
+    s->packClothInverse.assign(4 * C, 0.f);
+    s->packClothAreas.assign(C, 0.f);
+    const auto& p = m.positions;
+    for (size_t c = 0; c < C; ++c) {
+      double inv[4], area;
+      if (!clothTriangleRest(&p[3ull * tri[3 * c]], &p[3ull * tri[3 * c + 1]], &p[3ull * tri[3 * c + 2]], inv, &area))
+        return fail(s, "Rest triangle must be nondegenerate."), JGS2_INVALID_ARGUMENT;
+      for (int k = 0; k < 4; ++k) s->packClothInverse[4 * c + k] = static_cast<float>(inv[k]);
+      s->packClothAreas[c] = static_cast<float>(area);
+    }
+    std::vector<uint32_t> hinges;
+    std::string err;
+    if (!buildHinges(tri, &hinges, &err)) return fail(s, err), JGS2_INVALID_ARGUMENT;
+    const size_t H = hinges.size() / 4;
+    s->packHinges = hinges;
+    s->packHingeAngles.assign(H, 0.f);
+    s->packHingeLengths.assign(H, 0.f);
+    for (size_t h = 0; h < H; ++h) {
+      const uint32_t* q = &hinges[4 * h];
+      double angle, length;
+      if (!clothHingeRest(&p[3ull * q[0]], &p[3ull * q[1]], &p[3ull * q[2]], &p[3ull * q[3]], &angle, &length))
+        return fail(s, "First hinge triangle must be nondegenerate."), JGS2_INVALID_ARGUMENT;
+      s->packHingeAngles[h] = static_cast<float>(angle);
+      s->packHingeLengths[h] = static_cast<float>(length);
+    }
+    jgs2_cloth_input& ci = s->packCloth;
+    std::memset(&ci, 0, sizeof(ci));
+    ci.vertex_count = V;
+    ci.triangle_count = static_cast<uint32_t>(C);
+    ci.hinge_count = static_cast<uint32_t>(H);
+    ci.triangle_indices = s->packClothTriangles.data();
+    ci.triangle_inverse_rest_bases = s->packClothInverse.data();
+    ci.triangle_rest_areas = s->packClothAreas.data();
+    ci.hinge_indices = H ? s->packHinges.data() : nullptr;
+    ci.hinge_rest_angles = H ? s->packHingeAngles.data() : nullptr;
+    ci.hinge_rest_edge_lengths = H ? s->packHingeLengths.data() : nullptr;
+    ci.young_modulus = static_cast<float>(s->cloth.young);
+    ci.poisson_ratio = static_cast<float>(s->cloth.poisson);
+    ci.thickness = static_cast<float>(s->cloth.thickness);
+    ci.bending_stiffness = static_cast<float>(s->cloth.bending);
+  }
   std::memset(out, 0, sizeof(*out));
+  out->cloth = cloth ? &s->packCloth : nullptr;
   out->vertex_count = V;
   out->tet_count = T;
   out->cubature_k = K;

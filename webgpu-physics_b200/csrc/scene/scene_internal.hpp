@@ -44,10 +44,19 @@ struct CubatureRecord {
   std::array<double, 36> basis{};  // four row-major 3x3 blocks
 };
 
+// Triangle cloth of a scene (SceneDefinition.cloth, src/scenes/index.ts:688-696):
+// triangles over scene vertices and one membrane / bending material.
+struct Cloth {
+  bool present = false;
+  std::vector<uint32_t> triangles;  // 3 per triangle, scene vertex ids
+  double density = 0, young = 0, poisson = 0, thickness = 0, bending = 0;
+};
+
 struct Scene {
   std::string error;
   std::vector<Material> materialTable;
   Mesh mesh;
+  Cloth cloth;
   RestData rest;
   bool restValid = false;
   std::vector<double> masses;  // lumped, V
@@ -69,6 +78,9 @@ struct Scene {
   std::vector<float> packPositions, packVelocities, packRest, packColors;
   std::vector<uint32_t> packInfo, packTetIndices, packAdjacency;
   std::vector<float> packInverseDm, packMeta, packStiffness;
+  std::vector<uint32_t> packClothTriangles, packHinges;
+  std::vector<float> packClothInverse, packClothAreas, packHingeAngles, packHingeLengths;
+  jgs2_cloth_input packCloth{};
 };
 
 // ---- small dense helpers (row-major 3x3) ---------------------------------

@@ -27,6 +27,21 @@ class JGS2Error(RuntimeError):
         self.message = message
 
 
+class ClothInput(Structure):
+    _fields_ = [
+        ("vertex_count", c_uint32), ("triangle_count", c_uint32),
+        ("hinge_count", c_uint32), ("reserved0", c_uint32),
+        ("triangle_indices", POINTER(c_uint32)),
+        ("triangle_inverse_rest_bases", POINTER(c_float)),
+        ("triangle_rest_areas", POINTER(c_float)),
+        ("hinge_indices", POINTER(c_uint32)),
+        ("hinge_rest_angles", POINTER(c_float)),
+        ("hinge_rest_edge_lengths", POINTER(c_float)),
+        ("young_modulus", c_float), ("poisson_ratio", c_float),
+        ("thickness", c_float), ("bending_stiffness", c_float),
+    ]
+
+
 class Input(Structure):
     _fields_ = [
         ("vertex_count", c_uint32), ("tet_count", c_uint32),
@@ -43,6 +58,7 @@ class Input(Structure):
         ("cubature_tet_ids", POINTER(c_uint32)),
         ("cubature_weights", POINTER(c_float)),
         ("cubature_basis", POINTER(c_float)),
+        ("cloth", POINTER(ClothInput)),
     ]
 
 
@@ -79,7 +95,7 @@ class Info(Structure):
         ("objective_revision", c_uint32),
         ("last_submitted_iterations", c_uint32), ("history_count", c_uint32),
         ("scene_scale", c_float), ("preprocessing_timestep", c_float),
-        ("current_position_buffer", c_uint32), ("reserved", c_uint32),
+        ("current_position_buffer", c_uint32), ("cloth_triangle_count", c_uint32),
     ]
 
 
@@ -167,6 +183,12 @@ def scene_lib() -> ctypes.CDLL:
                                             POINTER(c_uint32), POINTER(c_uint32), c_uint32,
                                             POINTER(c_uint8), c_uint32]
         lib.jgs2_scene_add_mesh.restype = c_int64
+        lib.jgs2_scene_add_cloth.argtypes = [c_void_p, c_uint32, POINTER(c_double), c_uint32,
+                                             POINTER(c_uint32), POINTER(c_uint8), c_uint32, c_double,
+                                             c_double, c_double, c_double, c_double]
+        lib.jgs2_scene_add_cloth.restype = c_int64
+        lib.jgs2_scene_cloth_triangle_count.argtypes = [c_void_p]
+        lib.jgs2_scene_cloth_triangle_count.restype = c_uint32
         lib.jgs2_scene_set_pinned.argtypes = [c_void_p, POINTER(c_uint8)]
         lib.jgs2_scene_vertex_count.argtypes = [c_void_p]
         lib.jgs2_scene_vertex_count.restype = c_uint32

@@ -70,7 +70,41 @@ class SceneInput:
     target_positions: Optional[np.ndarray] = None
     target_stiffnesses: Optional[np.ndarray] = None
     rest_positions: Optional[np.ndarray] = None  # float64 FEM rest shape
+    # Triangle cloth (JGS2GpuClothInput, src/simulation/gpu/cloth-layout.ts:88-104).
+    cloth_triangles: Optional[np.ndarray] = None       # uint32, 3 per triangle
+    cloth_inverse_rest: Optional[np.ndarray] = None    # float32, 4 per triangle
+    cloth_rest_areas: Optional[np.ndarray] = None      # float32, 1 per triangle
+    hinge_indices: Optional[np.ndarray] = None         # uint32, 4 per hinge
+    hinge_rest_angles: Optional[np.ndarray] = None     # float32
+    hinge_rest_edge_lengths: Optional[np.ndarray] = None  # float32
+    cloth_material: Optional[np.ndarray] = None        # float32 (E, nu, thickness, bending)
     stats: Optional[dict] = None
+
+    @property
+    def cloth_triangle_count(self) -> int:
+        return 0 if self.cloth_triangles is None else self.cloth_triangles.size // 3
+
+    @property
+    def hinge_count(self) -> int:
+        return 0 if self.hinge_indices is None else self.hinge_indices.size // 4
+
+    def cloth_ctypes(self):
+        """The jgs2_cloth_input record, or None without cloth."""
+        if self.cloth_triangles is None:
+            return None
+        c = _ffi.ClothInput()
+        c.vertex_count = self.vertex_count
+        c.triangle_count = self.cloth_triangle_count
+        c.hinge_count = self.hinge_count
+        c.triangle_indices = _ffi.uptr(self.cloth_triangles)
+        c.triangle_inverse_rest_bases = _ffi.fptr(self.cloth_inverse_rest)
+        c.triangle_rest_areas = _ffi.fptr(self.cloth_rest_areas)
+        c.hinge_indices = _ffi.uptr(self.hinge_indices)
+        c.hinge_rest_angles = _ffi.fptr(self.hinge_rest_angles)
+        c.hinge_rest_edge_lengths = _ffi.fptr(self.hinge_rest_edge_lengths)
+        (c.young_modulus, c.poisson_ratio, c.thickness,
+         c.bending_stiffness) = (float(x) for x in self.cloth_material)
+        return c
 
     def as_ctypes(self) -> _ffi.Input:
         rec = _ffi.Input()
@@ -94,8 +128,11 @@ class SceneInput:
         rec.cubature_tet_ids = _ffi.uptr(self.cubature_tet_ids)
         rec.cubature_weights = _ffi.fptr(self.cubature_weights)
         rec.cubature_basis = _ffi.fptr(self.cubature_basis)
-        # Keep the arrays alive as long as the record.
-        rec._owner = self  # type: ignore[attr-defined]
+        cloth = self.cloth_ctypes()
+        if cloth is not None:
+            rec.cloth = ctypes.pointer(cloth)
+        # Keep the arrays (and the cloth record) alive as long as the record.
+        rec._owner = (self, cloth)  # type: ignore[attr-defined]
         return rec
 
     def copy(self) -> "SceneInput":
@@ -133,6 +170,8 @@ class SceneInput:
         and tets are contiguous (as the scene builder lays them out), so each
         body's slice, re-indexed to start at zero, is a complete scene with
         the same rest data and cubature records it had in the whole."""
+        if self.cloth_triangles is not None:
+            raise ValueError("split_bodies takes tetrahedral scenes only")
         info = self.vertex_info.reshape(-1, 4)
         tets = self.tet_indices.reshape(-1, 4)
         body_of_vertex = info[:, 3]
@@ -230,6 +269,21 @@ class Scene:
             raise ValueError(self._error())
         return base
 
+    def add_cloth(self, positions, triangles, pinned=None, body=0, density=480.0, young=9000.0,
+                  poisson=0.3, thickness=0.012, bending=0.045) -> int:
+        """Triangle cloth sheet as one body (defaults: the reference's pinned
+        cloth drape material, src/scenes/index.ts:688-696)."""
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
+        tri = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1)
+        pin = None if pinned is None else np.ascontiguousarray(pinned, dtype=np.uint8)
+        base = self._lib.jgs2_scene_add_cloth(
+            self._h, pos.size // 3, _ffi.dptr(pos), tri.size // 3, _ffi.uptr(tri),
+            None if pin is None else pin.ctypes.data_as(ctypes.POINTER(ctypes.c_uint8)), body,
+            density, young, poisson, thickness, bending)
+        if base < 0:
+            raise ValueError(self._error())
+        return base
+
     def set_pinned(self, pinned):
         pin = np.ascontiguousarray(pinned, dtype=np.uint8)
         if pin.size != self.vertex_count:
@@ -296,7 +350,21 @@ class Scene:
                 return None
             return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
 
+        cloth = {}
+        if rec.cloth:
+            c = rec.cloth.contents
+            C, H = c.triangle_count, c.hinge_count
+            cloth = dict(
+                cloth_triangles=f(c.triangle_indices, 3 * C),
+                cloth_inverse_rest=f(c.triangle_inverse_rest_bases, 4 * C),
+                cloth_rest_areas=f(c.triangle_rest_areas, C),
+                hinge_indices=f(c.hinge_indices, 4 * H) if H else np.zeros(0, np.uint32),
+                hinge_rest_angles=f(c.hinge_rest_angles, H) if H else np.zeros(0, np.float32),
+                hinge_rest_edge_lengths=f(c.hinge_rest_edge_lengths, H) if H else np.zeros(0, np.float32),
+                cloth_material=np.array([c.young_modulus, c.poisson_ratio, c.thickness, c.bending_stiffness],
+                                        dtype=np.float32))
         return SceneInput(
+            **cloth,
             vertex_count=V, tet_count=T, cubature_k=K,
             positions=f(rec.positions, 4 * V), vertex_rest=f(rec.vertex_rest, 4 * V),
             vertex_info=f(rec.vertex_info, 4 * V), tet_indices=f(rec.tet_indices, 4 * T),
@@ -340,6 +408,58 @@ def single_tetrahedron(timestep=1 / 60, cubature_k=4) -> SceneInput:
     sc.add_mesh([0, 0, 0, 1, 0, 0, 0, 1, 0, 0, 0, 1], [0, 1, 2, 3], m, pinned=[1, 0, 0, 0])
     sc.precompute(timestep=timestep, cubature_k=cubature_k)
     return sc.pack()
+
+
+def cloth_grid(cells, prefold=False):
+    """Vertices and triangles of a (cells+1)^2 sheet in the xz plane spanning
+    [-0.8, 0.8]^2 at y = 1.15, two triangles per cell wound (i00, i01, i10),
+    (i10, i01, i11) (clothDefinition, src/scenes/index.ts:632-681).  With
+    `prefold` the columns x >= 3 are folded back over the sheet at y = 1.229,
+    as the reference's 4-cell demo is."""
+    n = cells + 1
+    pos = np.zeros((n * n, 3))
+    for z in range(n):
+        for x in range(n):
+            folded = prefold and x >= 3
+            wx = (0.8 - 0.4 * x) if folded else (-0.8 + 1.6 * x / cells)
+            pos[x + z * n] = (wx, 1.229 if folded else 1.15, -0.8 + 1.6 * z / cells)
+    tri = []
+    for z in range(cells):
+        for x in range(cells):
+            i00, i10 = x + z * n, x + 1 + z * n
+            i01, i11 = x + (z + 1) * n, x + 1 + (z + 1) * n
+            tri += [i00, i01, i10, i10, i01, i11]
+    return pos, np.array(tri, dtype=np.uint32)
+
+
+def cloth_drape(cells=4, prefold=True, pinned_columns=(0, 2), young=9000.0, poisson=0.3, thickness=0.012,
+                bending=0.045, density=480.0, timestep=1 / 120, cubature_k=4) -> SceneInput:
+    """Pinned cloth drape (clothDefinition, src/scenes/index.ts:632-720): a
+    fully pinned stable Neo-Hookean box collider (E=1.1e5, nu=0.34) and a
+    StVK sheet whose z = 0 row is pinned at the given columns.  Without IPC
+    the sheet does not touch the collider; the collider keeps the scene on the
+    stable Neo-Hookean path that cloth requires."""
+    sc = Scene()
+    m = sc.add_material(1000.0, 110000.0, 0.34, MATERIAL_STABLE_NEO_HOOKEAN)
+    sc.add_cuboid((1, 1, 1), (-0.65, 0.0, -0.45), (0.9, 0.5, 0.9), m, 0, 63)
+    pos, tri = cloth_grid(cells, prefold)
+    n = cells + 1
+    pin = np.zeros(n * n, dtype=np.uint8)
+    for x in pinned_columns:
+        pin[x] = 1
+    sc.add_cloth(pos, tri, pin, 1, density, young, poisson, thickness, bending)
+    stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=PRECOMPUTE_PATCH)
+    inp = sc.pack()
+    inp.stats = stats
+    return inp
+
+
+def cloth_sheet(cells=127, young=1e4, bending=1e-3, **kwargs) -> SceneInput:
+    """The serving mix's cloth request: a (cells+1)^2-vertex StVK sheet
+    (16,384 vertices and 32,258 triangles at 127 cells) with its two z = 0
+    corners pinned, over a pinned box collider."""
+    return cloth_drape(cells=cells, prefold=False, pinned_columns=(0, cells), young=young, bending=bending,
+                       **kwargs)
 
 
 def batched_scenes(count=256, **kwargs) -> list:

@@ -180,6 +180,16 @@ class JGS2GpuSolver:
         return bool(self.info()["globalization_enabled"])
 
     @property
+    def clothTriangleCount(self) -> int:
+        return self.info()["cloth_triangle_count"]
+
+    @property
+    def globalizationElementCount(self) -> int:
+        """Tets plus cloth triangles (jgs2-solver.ts:959)."""
+        i = self.info()
+        return i["tet_count"] + i["cloth_triangle_count"]
+
+    @property
     def objectiveActivity(self) -> dict:
         i = self.info()
         return {"flags": i["objective_flags"], "externalForces": bool(i["objective_flags"] & 1),
