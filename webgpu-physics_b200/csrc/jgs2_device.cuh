@@ -113,6 +113,15 @@ __device__ __forceinline__ float3 smv(const S3& a, float3 v) {
             a.xz * v.x + a.yz * v.y + a.zz * v.z);
 }
 // B^T B for a 3x3 B (columns).
+// R S R^T of a symmetric S.
+__device__ __forceinline__ S3 srotate(const M3& r, const S3& s) {
+  const M3 rs = {mv(r, f3(s.xx, s.xy, s.xz)), mv(r, f3(s.xy, s.yy, s.yz)), mv(r, f3(s.xz, s.yz, s.zz))};
+  // (R S R^T)_ij = row i of R S . row j of R
+  const float3 a0 = f3(rs.c0.x, rs.c1.x, rs.c2.x), a1 = f3(rs.c0.y, rs.c1.y, rs.c2.y);
+  const float3 a2 = f3(rs.c0.z, rs.c1.z, rs.c2.z);
+  const float3 r0 = f3(r.c0.x, r.c1.x, r.c2.x), r1 = f3(r.c0.y, r.c1.y, r.c2.y), r2 = f3(r.c0.z, r.c1.z, r.c2.z);
+  return {dot3(a0, r0), dot3(a1, r1), dot3(a2, r2), dot3(a0, r1), dot3(a0, r2), dot3(a1, r2)};
+}
 __device__ __forceinline__ S3 gramColumns(const M3& b) {
   return {dot3(b.c0, b.c0), dot3(b.c1, b.c1), dot3(b.c2, b.c2), dot3(b.c0, b.c1), dot3(b.c0, b.c2), dot3(b.c1, b.c2)};
 }

@@ -537,7 +537,9 @@ static_assert(sizeof(CubState) <= kRecFloats * 4, "cubature cache record too sma
 #define JGS2_SOLVE_MIN_BLOCKS 4
 #endif
 
-template <int W>
+// kCloth: some scene of the engine has cloth (the cloth gathers and line
+// search terms are compiled out otherwise).
+template <int W, bool kCloth>
 __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
                                                       const float4* __restrict__ src, float4* tgt,
                                                       const uint32_t* __restrict__ list, uint32_t count,
@@ -609,7 +611,13 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
         const float ktS = targetStiffness(p, b, v);
         float3 grad = f3(0, 0, 0);
         S3 hess = szero();
-        const M3 RsT = mtrans(loadRot(b.vertexRot, v));
+        // Record terms are formed in the source vertex's frame: with
+        // B_l = R_l Ubar_l R_s^T = B'_l R_s^T, a record's projected gradient
+        // and Hessian are R_s g' and R_s H' R_s^T of the same expressions over
+        // B'_l = R_l Ubar_l, so R_s is applied once per record instead of once
+        // per basis block.  The exact source block subtracted for a record at
+        // the vertex's own slot is formed in the world frame.
+        const M3 Rs = loadRot(b.vertexRot, v);
         CubState* myCache = cache + static_cast<size_t>(group) * K;
         // Cubature records first, then (unless cached) the incident tets, in
         // separate loops so the two kinds of item never share a divergent pass.
@@ -627,9 +635,10 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             if (t != kEmptyTet && w > 0.0f) {
               const TetRec r = loadTet(b.tets, t);
               const float4* U = b.cubBasis + 9ull * rec;
-              // One basis block B_l = R_l Ubar_l R_s^T at a time: accumulate F,
-              // the projected directions dF_c = sum_l B_l[:,c] g_l^T and the
-              // inertia / objective quadratic (gQ, HQ) of the record.
+              // One basis block B'_l = R_l Ubar_l at a time: accumulate F,
+              // the projected directions dF_c = sum_l B'_l[:,c] g_l^T and the
+              // inertia / objective quadratic (gQ, HQ) of the record, all in
+              // the source frame.
               M3 F = mzero(), dF0 = mzero(), dF1 = mzero(), dF2 = mzero();
               float3 gQ = f3(0, 0, 0);
               S3 HQ = szero();
@@ -640,7 +649,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                 const uint32_t q = idxAt(idx, l);
                 if (q == v) slot = l;
                 const float3 gl = shapeGradient(r, l);
-                const M3 B = mm(mm(loadRot(b.vertexRot, q), loadBlockVec(U, l)), RsT);
+                const M3 B = mm(loadRot(b.vertexRot, q), loadBlockVec(U, l));
                 const float3 xl = l == 0 ? x0 : xyz(src[q]);
                 if (l > 0) F = F + outer(xl - x0, gl);
                 dF0 = dF0 + outer(B.c0, gl);
@@ -689,22 +698,23 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
               ph.yz += pt.a * frob(dF1, dF2) + pt.c1 * p1 * p2 + r.lambda * q1 * q2;
               ph.xx *= r.vol; ph.yy *= r.vol; ph.zz *= r.vol; ph.xy *= r.vol; ph.xz *= r.vol; ph.yz *= r.vol;
               sadd(ph, HQ);
+              grad = grad + w * mv(Rs, pg);
+              saddScaled(hess, w, srotate(Rs, ph));
               float3 gs = f3(0, 0, 0);
               if (slot < 4) {
                 // Remove the exact source block already in the local gather.
                 gs = shapeGradient(r, slot);
-                pg = pg - (r.vol * mv(P, gs) + dWs * (position - predV));
-                if (objActive) pg = pg - objS * (1.0f / nS);
+                float3 ps = r.vol * mv(P, gs) + dWs * (position - predV);
+                if (objActive) ps = ps + objS * (1.0f / nS);
                 const float3 u1 = mv(F, gs), w1 = mv(pt.cof, gs);
                 S3 blk = szero();
                 saddDiag(blk, pt.a * dot3(gs, gs));
                 saddOuter(blk, pt.c1, u1);
                 saddOuter(blk, r.lambda, w1);
-                saddScaled(ph, -r.vol, blk);
-                saddDiag(ph, -(dWs + ktS / nS));
+                grad = grad - w * ps;
+                saddScaled(hess, -w * r.vol, blk);
+                saddDiag(hess, -w * (dWs + ktS / nS));
               }
-              grad = grad + w * pg;
-              saddScaled(hess, w, ph);
               st.F = F;
               st.I0 = pt.I1;
               st.J0 = pt.J;
@@ -731,7 +741,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             addIncidentBlock(hess, r, F, pt, g);
           }
           // ---- cloth membrane and bending (jgs2-shader.ts:3113-3186) ----
-          if (p.cloth)
+          if (kCloth && p.cloth)
             clothLocalSystem<true>(b.clothTris, b.clothHinges, b.clothIncidence, b.clothRange[v], src,
                                    clothMaterial(p), lane, W, grad, hess);
         }
@@ -785,7 +795,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
           const float dl = scaledLength(dr.direction);
           if (p.maxStep > 0.0f && dl > p.maxStep) ta = p.maxStep / dl;
           const float controlMin = c0.z;  // accepted-source minimum (finite here)
-          const uint4 cr = p.cloth ? b.clothRange[v] : make_uint4(0u, 0u, 0u, 0u);
+          const uint4 cr = (kCloth && p.cloth) ? b.clothRange[v] : make_uint4(0u, 0u, 0u, 0u);
           const ClothMaterial cmat = clothMaterial(p);
           for (uint32_t bt = 0; bt <= kMaxBacktracks; ++bt) {
             const float3 tp = position + ta * dr.direction;
@@ -802,6 +812,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             // restrictedEnergyDelta :2120-2337); the energy is used only
             // when the geometry is feasible, as in the reference order.
             float jmin = kF32Max, de = 0.0f;
+            const float3 ts = mtv(Rs, td);
             bool geomFinite = true;
             // A lane's items in order: its cached cubature records, then its
             // incident tets (the same per-lane order as one merged loop).
@@ -809,9 +820,10 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
               const CubState& st = myCache[u];
               if (!(st.w > 0.0f)) continue;
               float J = 0.0f;
-              const M3 D = td.x * st.dF0 + td.y * st.dF1 + td.z * st.dF2;
+              // Record state is in the source frame: the trial step there is R_s^T td.
+              const M3 D = ts.x * st.dF0 + ts.y * st.dF1 + ts.z * st.dF2;
               const float dm = st.vol * snhEnergyDelta(st.F, st.I0, st.J0, D, st.lambda, st.mu, &J);
-              float comp = dm + dot3(td, st.gQ) + 0.5f * dot3(td, smv(st.HQ, td));
+              float comp = dm + dot3(ts, st.gQ) + 0.5f * dot3(ts, smv(st.HQ, ts));
               if (st.slot < 4) {
                 float Js;
                 comp -= st.vol * snhEnergyDelta(st.F, st.I0, st.J0, outer(td, st.gs), st.lambda, st.mu, &Js);
@@ -1579,8 +1591,12 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   // One vertex per lane group: the line search makes per-vertex work uneven,
   // and the block scheduler balances it better than a fixed grid stride.
   const uint32_t blocks = std::max(1u, (count + groups - 1) / groups);
-  solveKernel<kGroup><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
-                                                               cachedIncident ? 1 : 0);
+  if (b.clothRange)
+    solveKernel<kGroup, true><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
+                                                                    cachedIncident ? 1 : 0);
+  else
+    solveKernel<kGroup, false><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
+                                                                     cachedIncident ? 1 : 0);
   return 1;
 }
 
@@ -1594,7 +1610,8 @@ uint32_t solveGroupsPerBlock(uint32_t K) {
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) optin = 48 * 1024;
     optin -= 1024;  // static shared memory of the kernel
-    cudaFuncSetAttribute(solveKernel<kGroup>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(solveKernel<kGroup, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(solveKernel<kGroup, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   }
   const uint32_t perVertex = static_cast<uint32_t>(K * sizeof(CubState));
   uint32_t groups = kBlock / kGroup;
