@@ -48,9 +48,11 @@ def parse_args():
                     help="iterations per frame (default 20 for the cube, 10 for the batched bodies)")
     ap.add_argument("--schedule", default="jacobi", choices=["jacobi", "graph-colored-gauss-seidel"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cube", choices=["cube", "batched", "serving"],
+    ap.add_argument("--workload", default="cube", choices=["cube", "batched", "serving", "trough", "cloth"],
                     help="cube: one large body (headline); batched: independent uneven bodies in one batch; "
-                         "serving: a Poisson stream of step requests through the continuous-batching loop")
+                         "serving: a Poisson stream of step requests through the continuous-batching loop; "
+                         "trough: the reference's IPC box trough; cloth: the 128x128 StVK sheet")
+    ap.add_argument("--boxes", type=int, default=10, help="boxes of the trough workload")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serving workload")
     ap.add_argument("--bodies", type=int, default=256, help="scenes of the batched workload")
     args = ap.parse_args()
@@ -657,6 +659,114 @@ def ours_arm(args):
     return 0
 
 
+# Published GPU simulation time of the reference's 10-box trough after a
+# 96-frame pre-roll (docs/ROADMAP.md:319-321 of the reference): 11.831 ms per
+# frame of 3 iterations over 80 active vertices, i.e. 2.03e4 vertex-updates/s.
+TROUGH_REFERENCE_MS = 11.831
+
+
+def scene_arm(args):
+    """One small scene stepped with the production settings of the reference
+    app: the IPC box trough (troughDefinition + the app's IPC settings) or the
+    128x128 StVK cloth sheet of the serving mix.  Frames are timed with CUDA
+    events on the solver's stream after a pre-roll (96 frames for the trough,
+    as the reference's published measurement)."""
+    import numpy as np
+    import torch
+
+    from jgs2_b200 import scenes, solver
+
+    world, rank, local = dist_env()
+    dist = init_dist(world, "nccl")
+    torch.cuda.set_device(local)
+    device = local
+    t0 = time.perf_counter()
+    if args.workload == "trough":
+        inp = scenes.trough(args.boxes)
+        settings = dict(scenes.TROUGH_SETTINGS)
+        preroll = 96
+        what = (f"IPC box trough: {args.boxes} one-cell stable Neo-Hookean boxes falling into a pinned V-trough "
+                f"({inp.vertex_count} vertices, {inp.tet_count} tets, {inp.contact_candidate_count} static "
+                f"VT/EE candidates), the reference app's IPC settings (dHat 0.08, dMin 0.003, kappa 1e5, "
+                f"mu 0.45, maxStep 0.075), production step of 3 iterations at dt=1/60, after a 96-frame pre-roll")
+    else:
+        inp = scenes.cloth_sheet()
+        settings = dict(timestep=1 / 120, gravity=(0.0, -9.81, 0.0), floorStiffness=0.0, iterations=5,
+                        velocityDamping=0.997, contactTangentialDamping=0.0, horizontalBodyCorrection=False,
+                        maxStep=0.01)
+        preroll = args.warmup
+        what = (f"StVK cloth sheet 128x128 ({inp.vertex_count} vertices, {inp.cloth_triangle_count} triangles, "
+                f"{inp.hinge_count} hinges; E=1e4, bending 1e-3, two corners pinned) over a pinned box collider, "
+                f"production step of 5 iterations at dt=1/120")
+    build_s = time.perf_counter() - t0
+    s = solver.JGS2GpuSolver.create(inp, settings, device=device)
+    _ptr, stream_ptr = s.devicePositions()
+    stream = torch.cuda.ExternalStream(stream_ptr, device=device)
+    for _ in range(max(preroll, args.warmup)):
+        s.step()
+    s.awaitIdle()
+    iters = s.lastSubmittedIterationCount
+    active = inp.active_vertex_count()
+    launches0 = s.kernelLaunchCount()
+    start_ev = torch.cuda.Event(enable_timing=True)
+    end_ev = torch.cuda.Event(enable_timing=True)
+    if dist is not None:
+        dist.barrier()
+    torch.cuda.synchronize(device)
+    with ClockSampler(device) as clocks:
+        start_ev.record(stream)
+        for _ in range(args.steps):
+            s.step()
+        end_ev.record(stream)
+        end_ev.synchronize()
+    ms = max_over_ranks(dist, start_ev.elapsed_time(end_ev), f"cuda:{device}")
+    launches = s.kernelLaunchCount() - launches0
+    value = whole_job_rate(world, active * iters * args.steps, ms / 1e3)
+    prof = s.stepWithGpuTimestamps(max(1, min(args.steps, 5)), iters)
+    # End to end: each frame's external-force upload and position read.
+    V = inp.vertex_count
+    f_np = torch.zeros(3 * V, dtype=torch.float32).pin_memory().numpy()
+    p_np = torch.empty(4 * V, dtype=torch.float32).pin_memory().numpy()
+    e2e_steps = max(1, min(args.steps, 20))
+    t_e2e = time.perf_counter()
+    for _ in range(e2e_steps):
+        s.replaceExternalForces(f_np)
+        s.step()
+        s.readPositions(out=p_np)
+    e2e_total = max_over_ranks(dist, time.perf_counter() - t_e2e, f"cuda:{device}")
+    s.destroy()
+    if rank == 0:
+        ref = None
+        if args.workload == "trough" and args.boxes == 10:
+            ref = {"ms_per_frame": TROUGH_REFERENCE_MS, "vertex_updates_per_s": active * 3 / (TROUGH_REFERENCE_MS / 1e3),
+                   "source": "reference docs/ROADMAP.md:319-321 (Chrome WebGPU, unnamed NVIDIA adapter)"}
+        line = {
+            "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": max(preroll, args.warmup), "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": (value / ref["vertex_updates_per_s"]) if ref else None,
+            "dtype": "f32", "data": "synthetic (the reference's scene generator restated)",
+            "config": {"workload": what, "vertices": V, "active_vertices": active, "tets": inp.tet_count,
+                       "iterations": iters, "step": "one production frame",
+                       "l2": "no flush: the scene fits in L2; the number is per-frame latency bound",
+                       "precompute": {"seconds": round(build_s, 2)},
+                       "parallelism": "replicas" if world > 1 else "single GPU"},
+            "frames_per_s": world * 1e3 * args.steps / ms,
+            "reference_published": ref,
+            "gpu_launches": int(launches),
+            "kernel_ms_per_frame": {k: v[1] / max(1, min(args.steps, 5)) for k, v in prof.items() if v[0]},
+            "roofline": None,
+            "cpu_baseline": None,
+            "e2e": {"value": whole_job_rate(world, active * iters * e2e_steps, e2e_total), "unit": UNIT,
+                    "h2d_bytes_per_step": int(12 * V), "d2h_bytes_per_step": int(16 * V), "steps": e2e_steps},
+            "clocks": clocks.summary(),
+        }
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+    return 0
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -665,6 +775,8 @@ def main():
         return batched_arm(args)
     if args.workload == "serving":
         return serving_arm(args)
+    if args.workload in ("trough", "cloth"):
+        return scene_arm(args)
     return ours_arm(args)
 
 

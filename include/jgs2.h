@@ -118,6 +118,15 @@ typedef struct jgs2_input {
   const float* cubature_weights;     /* V * K */
   const float* cubature_basis;       /* V * K * 36: four row-major Ubar blocks */
   const jgs2_cloth_input* cloth;     /* NULL: no cloth (input.cloth, layout.ts:62) */
+  /* Static IPC contact candidates (input.contactCandidates, layout.ts:63;
+   * StaticIpcContactCandidates, src/simulation/cpu/ipc-contact.ts:28-38):
+   * four vertex indices per candidate, the vertex-triangle candidates
+   * (point, t0, t1, t2) first, then the edge-edge candidates (a0, a1, b0, b1).
+   * NULL with zero counts: no contact.  Contact requires the stable
+   * Neo-Hookean path (jgs2-solver.ts:1014-1018). */
+  const uint32_t* contact_indices;
+  uint32_t contact_vertex_triangle_count;
+  uint32_t contact_edge_edge_count;
 } jgs2_input;
 
 /*
@@ -198,6 +207,8 @@ typedef struct jgs2_info {
   float preprocessing_timestep;
   uint32_t current_position_buffer;/* 0 = A, reported for zero-copy consumers */
   uint32_t cloth_triangle_count;   /* clothTriangleCount (:911) */
+  uint32_t contact_candidate_count;/* contactCandidateCount */
+  uint32_t reserved1;
 } jgs2_info;
 
 /* ---- library ---------------------------------------------------------- */
@@ -281,7 +292,7 @@ jgs2_status jgs2_sync(jgs2_solver* solver);
  * jgs2_step_frames_exact_iterations but without graph replay, with a CUDA
  * event pair around every kernel on the solver stream; the call waits for the
  * frames and fills one entry per kernel kind. */
-#define JGS2_PROFILE_KINDS 8
+#define JGS2_PROFILE_KINDS 9
 typedef struct jgs2_kernel_profile {
   uint32_t kinds;
   uint32_t launches[JGS2_PROFILE_KINDS];

@@ -117,6 +117,26 @@ int64_t jgs2_scene_add_cloth(jgs2_scene* scene, uint32_t vertex_count, const dou
                              double thickness, double bending_stiffness);
 uint32_t jgs2_scene_cloth_triangle_count(const jgs2_scene* scene);
 
+/* Replace the rest positions of every vertex (3 * V doubles) and re-orient the
+ * tetrahedra, as transformTetrahedralMesh does (src/simulation/cpu/mesh.ts:
+ * 237-280) for rotated, warped or translated bodies. */
+jgs2_status jgs2_scene_set_rest_positions(jgs2_scene* scene, const double* positions);
+
+/* Nonzero: the packer enumerates the static IPC contact candidates of the
+ * scene's surface (the tet boundary plus the cloth triangles;
+ * buildStaticIpcContactCandidates, src/simulation/cpu/ipc-contact.ts:591-665)
+ * into jgs2_input.contact_indices.  The enumeration is quadratic in the
+ * surface size, like the reference's static superset. */
+jgs2_status jgs2_scene_set_contact(jgs2_scene* scene, uint32_t enabled);
+
+/* buildStaticIpcContactCandidates (src/simulation/cpu/ipc-contact.ts:591-665)
+ * for an arbitrary triangle surface: returns the candidate count (-1 on
+ * invalid input) and, when out holds at least that many candidates (4 u32
+ * each), writes them, vertex-triangle first. */
+int64_t jgs2_build_static_contact_candidates(uint32_t vertex_count, const uint32_t* triangles,
+                                             uint32_t triangle_count, uint32_t* out, uint64_t capacity,
+                                             uint32_t* vertex_triangle_count, uint32_t* edge_edge_count);
+
 /* Replace the pin flags of every vertex (V bytes, nonzero = pinned); the
  * reference's cuboid generator takes an arbitrary predicate (mesh.ts:142). */
 jgs2_status jgs2_scene_set_pinned(jgs2_scene* scene, const uint8_t* pinned);

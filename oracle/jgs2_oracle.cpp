@@ -296,13 +296,220 @@ template <class T> T snhEnergyDelta(const M3<T>& i, const M3<T>& f, T lambda, T 
   return T(0.5) * mu * id - T(0.75) * mu * detd + T(0.5) * lambda * detd * (j1 + j0 - T(2)) - T(0.5) * mu * lr;
 }
 
+// ---- IPC contact library (ipc-contact-wgsl.ts:19-472) ----
+constexpr float kIpcLengthSquaredFloor = 1.0e-20f;
+constexpr float kIpcParallelRelativeEpsilon = 1.0e-6f;
+constexpr uint32_t kIpcVertexTriangle = 0, kIpcEdgeEdge = 1;
+
+template <class T>
+struct Contact {
+  V3<T> pa;
+  T distance;
+  V3<T> pb;
+  T squared;
+  V3<T> normal;
+  bool valid;
+  V4<T> weights;
+};
+
+template <class T> V3<T> ipcSafeUnit(V3<T> v, V3<T> fallback) {
+  const T l2 = dot(v, v);
+  if (finiteS(l2) && l2 > T(kIpcLengthSquaredFloor)) return v * (T(1) / std::sqrt(l2));
+  const T f2 = dot(fallback, fallback);
+  if (finiteS(f2) && f2 > T(kIpcLengthSquaredFloor)) return fallback * (T(1) / std::sqrt(f2));
+  return v3<T>(1, 0, 0);
+}
+template <class T> V3<T> ipcOrthogonalUnit(V3<T> d) {
+  const V3<T> a = v3(std::fabs(d.x), std::fabs(d.y), std::fabs(d.z));
+  V3<T> axis = v3<T>(1, 0, 0);
+  if (a.y <= a.x && a.y <= a.z) axis = v3<T>(0, 1, 0);
+  else if (a.z <= a.x && a.z <= a.y) axis = v3<T>(0, 0, 1);
+  return ipcSafeUnit(cross(d, axis), v3<T>(1, 0, 0));
+}
+template <class T> Contact<T> ipcInvalidContact() {
+  return {v3<T>(0, 0, 0), T(0), v3<T>(0, 0, 0), T(0), v3<T>(1, 0, 0), false, {0, 0, 0, 0}};
+}
+template <class T> bool finite4v(V4<T> v) { return finiteS(v.x) && finiteS(v.y) && finiteS(v.z) && finiteS(v.w); }
+template <class T> Contact<T> ipcMakeContact(V3<T> pa, V3<T> pb, V4<T> w, V3<T> fallback) {
+  if (!finiteV(pa) || !finiteV(pb) || !finite4v(w)) return ipcInvalidContact<T>();
+  const V3<T> gap = pa - pb;
+  const T sq = dot(gap, gap);
+  if (!finiteS(sq) || sq < T(0)) return ipcInvalidContact<T>();
+  return {pa, std::sqrt(sq), pb, sq, ipcSafeUnit(gap, fallback), true, w};
+}
+template <class T> T clamp01(T v) { return std::min(std::max(v, T(0)), T(1)); }
+template <class T>
+struct SegmentPoint { V3<T> point; T parameter; T squared; };
+template <class T> SegmentPoint<T> ipcClosestOnSegment(V3<T> q, V3<T> s, V3<T> e) {
+  const V3<T> edge = e - s;
+  const T l2 = dot(edge, edge);
+  T t = 0;
+  if (finiteS(l2) && l2 > T(kIpcLengthSquaredFloor)) t = clamp01(dot(q - s, edge) / l2);
+  const V3<T> p = s + t * edge;
+  const V3<T> d = q - p;
+  return {p, t, dot(d, d)};
+}
+template <class T> Contact<T> ipcPointTriangle(V3<T> p, V3<T> t0, V3<T> t1, V3<T> t2) {
+  const V3<T> e01 = t1 - t0, e02 = t2 - t0, e12 = t2 - t1;
+  const T s01 = dot(e01, e01), s02 = dot(e02, e02), s12 = dot(e12, e12);
+  const T largest = std::max(s01, std::max(s02, s12));
+  const V3<T> an = cross(e01, e02);
+  const T a2 = dot(an, an);
+  const T threshold = std::max(T(kIpcLengthSquaredFloor) * T(kIpcLengthSquaredFloor),
+                               T(kIpcParallelRelativeEpsilon) * largest * largest);
+  V3<T> longest = e01;
+  if (s02 > s01 && s02 >= s12) longest = e02;
+  else if (s12 > s01 && s12 > s02) longest = e12;
+  const V3<T> fallback = ipcSafeUnit(an, ipcOrthogonalUnit(longest));
+  if (finiteS(a2) && a2 > threshold) {
+    const T d00 = s01, d01 = dot(e01, e02), d11 = s02;
+    const V3<T> po = p - t0;
+    const T d20 = dot(po, e01), d21 = dot(po, e02);
+    const T den = d00 * d11 - d01 * d01;
+    const T b1 = (d11 * d20 - d01 * d21) / den;
+    const T b2 = (d00 * d21 - d01 * d20) / den;
+    const T b0 = T(1) - b1 - b2;
+    if (b0 >= T(0) && b1 >= T(0) && b2 >= T(0)) {
+      const V3<T> closest = b0 * t0 + b1 * t1 + b2 * t2;
+      return ipcMakeContact(p, closest, V4<T>{T(1), -b0, -b1, -b2}, fallback);
+    }
+  }
+  const SegmentPoint<T> c01 = ipcClosestOnSegment(p, t0, t1);
+  const SegmentPoint<T> c12 = ipcClosestOnSegment(p, t1, t2);
+  const SegmentPoint<T> c20 = ipcClosestOnSegment(p, t2, t0);
+  SegmentPoint<T> best = c01;
+  V3<T> bary = v3<T>(T(1) - c01.parameter, c01.parameter, T(0));
+  if (c12.squared < best.squared) { best = c12; bary = v3<T>(T(0), T(1) - c12.parameter, c12.parameter); }
+  if (c20.squared < best.squared) { best = c20; bary = v3<T>(c20.parameter, T(0), T(1) - c20.parameter); }
+  return ipcMakeContact(p, best.point, V4<T>{T(1), -bary.x, -bary.y, -bary.z}, fallback);
+}
+template <class T> Contact<T> ipcEdgeEdge(V3<T> a0, V3<T> a1, V3<T> b0, V3<T> b1) {
+  const V3<T> da = a1 - a0, db = b1 - b0, off = a0 - b0;
+  const T la = dot(da, da), lb = dot(db, db);
+  const T scale = std::max(la, lb);
+  const T degenerate = std::max(T(kIpcLengthSquaredFloor), T(kIpcParallelRelativeEpsilon) * scale);
+  const bool aDeg = !(la > degenerate), bDeg = !(lb > degenerate);
+  T pa = 0, pb = 0;
+  if (aDeg && !bDeg) {
+    pb = clamp01(dot(db, off) / lb);
+  } else if (!aDeg) {
+    const T projA = dot(da, off);
+    if (bDeg) {
+      pa = clamp01(-projA / la);
+    } else {
+      const T coupling = dot(da, db);
+      const T projB = dot(db, off);
+      const T den = la * lb - coupling * coupling;
+      const T parallel = T(kIpcParallelRelativeEpsilon) * la * lb;
+      if (den > parallel) pa = clamp01((coupling * projB - projA * lb) / den);
+      const T pbu = (coupling * pa + projB) / lb;
+      if (pbu < T(0)) {
+        pb = 0;
+        pa = clamp01(-projA / la);
+      } else if (pbu > T(1)) {
+        pb = 1;
+        pa = clamp01((coupling - projA) / la);
+      } else {
+        pb = pbu;
+      }
+    }
+  }
+  const V3<T> pointA = a0 + pa * da, pointB = b0 + pb * db;
+  const V3<T> longest = lb > la ? db : da;
+  const V3<T> fallback = ipcSafeUnit(cross(da, db), ipcOrthogonalUnit(longest));
+  return ipcMakeContact(pointA, pointB, V4<T>{T(1) - pa, pa, -(T(1) - pb), -pb}, fallback);
+}
+template <class T> bool ipcBarrierActive(T d, T dHat) {
+  return finiteS(d) && finiteS(dHat) && d > T(0) && d < dHat;
+}
+template <class T> T ipcBarrier(T d, T dHat) {
+  if (!ipcBarrierActive(d, dHat)) return 0;
+  const T o = d - dHat;
+  const T lr = std::log(d) - std::log(dHat);
+  return -(o * o) * lr;
+}
+template <class T> T ipcBarrier1(T d, T dHat) {
+  if (!ipcBarrierActive(d, dHat)) return 0;
+  const T o = d - dHat;
+  const T lr = std::log(d) - std::log(dHat);
+  return T(-2) * o * lr - o * o / d;
+}
+template <class T> T ipcBarrier2(T d, T dHat) {
+  if (!ipcBarrierActive(d, dHat)) return 0;
+  const T o = d - dHat;
+  const T lr = std::log(d) - std::log(dHat);
+  return T(-2) * lr - T(4) * o / d + o * o / (d * d);
+}
+template <class T> T ipcNormalGradientScalar(T w, T kappa, T b1) {
+  if (!finiteS(w) || !finiteS(kappa) || !finiteS(b1) || kappa < T(0)) return 0;
+  return w * kappa * b1;
+}
+template <class T> T ipcPsdScalar(T w, T kappa, T b2) {
+  if (!finiteS(w) || !finiteS(kappa) || !finiteS(b2) || kappa <= T(0) || w == T(0) || b2 <= T(0)) return 0;
+  const T s = kappa * w * w * b2;
+  if (!finiteS(s)) return static_cast<T>(kF32Max);
+  return s;
+}
+template <class T> M3<T> ipcPsdNormalHessian(V3<T> n, T s) {
+  const V3<T> u = ipcSafeUnit(n, v3<T>(1, 0, 0));
+  const T k = std::max(s, T(0));
+  return {{k * u.x * u, k * u.y * u, k * u.z * u}};
+}
+template <class T> T ipcSafeStepCap(T src, T dMin, T L, T safety) {
+  if (!finiteS(src) || !finiteS(dMin) || !finiteS(L) || !finiteS(safety) || dMin < T(0) || src <= dMin ||
+      L < T(0))
+    return 0;
+  if (L == T(0)) return 1;
+  return clamp01(clamp01(safety) * (src - dMin) / L);
+}
+template <class T> T ipcFrictionF1(T s, T eps) {
+  const T n = std::max(s, T(0));
+  if (!(eps > T(0)) || n >= eps) return n > T(0) ? T(1) : T(0);
+  const T u = n / eps;
+  return u * (T(2) - u);
+}
+template <class T> T ipcFrictionDissipation(T slip, T eps, T mu, T lambda) {
+  if (!finiteS(slip) || !finiteS(eps) || !finiteS(mu) || !finiteS(lambda)) return 0;
+  const T n = std::max(slip, T(0));
+  const T scale = std::max(mu, T(0)) * std::max(lambda, T(0));
+  if (!(eps > T(0))) return scale * n;
+  if (n < eps) {
+    const T u = n / eps;
+    return scale * eps * u * u * (T(1) - u / T(3));
+  }
+  return scale * (n - eps / T(3));
+}
+// ipcAabbDistanceLowerBound (jgs2-shader.ts:520-548).
+template <class T> T ipcAabbLowerBound(uint32_t type, V3<T> p0, V3<T> p1, V3<T> p2, V3<T> p3) {
+  auto vmin = [](V3<T> a, V3<T> b) { return v3(std::min(a.x, b.x), std::min(a.y, b.y), std::min(a.z, b.z)); };
+  auto vmax = [](V3<T> a, V3<T> b) { return v3(std::max(a.x, b.x), std::max(a.y, b.y), std::max(a.z, b.z)); };
+  V3<T> gap = v3<T>(0, 0, 0);
+  if (type == kIpcVertexTriangle) {
+    const V3<T> lo = vmin(p1, vmin(p2, p3)), hi = vmax(p1, vmax(p2, p3));
+    gap = vmax(vmax(lo - p0, p0 - hi), v3<T>(0, 0, 0));
+  } else {
+    const V3<T> lo0 = vmin(p0, p1), hi0 = vmax(p0, p1), lo1 = vmin(p2, p3), hi1 = vmax(p2, p3);
+    gap = vmax(vmax(lo1 - hi0, lo0 - hi1), v3<T>(0, 0, 0));
+  }
+  return std::sqrt(dot(gap, gap));
+}
+// ipcContactFromPositions (jgs2-shader.ts:564-592): a separated contact at
+// the AABB lower bound when that bound reaches the threshold.
+template <class T>
+Contact<T> ipcContactFromPositions(uint32_t type, V3<T> p0, V3<T> p1, V3<T> p2, V3<T> p3, T threshold) {
+  const T lb = ipcAabbLowerBound(type, p0, p1, p2, p3);
+  if (finiteS(lb) && lb >= threshold) return {v3<T>(0, 0, 0), lb, v3<T>(0, 0, 0), lb * lb, v3<T>(1, 0, 0), true, {0, 0, 0, 0}};
+  if (type == kIpcVertexTriangle) return ipcPointTriangle(p0, p1, p2, p3);
+  return ipcEdgeEdge(p0, p1, p2, p3);
+}
+
 // ---- the oracle solver ----------------------------------------------------
 
 struct Settings {
   uint32_t schedule, iterations;
   float timestep, gravity[3], floorHeight, floorStiffness, velocityDamping, regularization,
       rotationEpsilon, maxStep, residualTolerance, normalizedUpdateTolerance,
-      contactTangentialDamping, contactMargin;
+      contactTangentialDamping, contactMargin, ipcActivation, ipcStiffness;
   bool horizontalBodyCorrection;
 };
 
@@ -745,12 +952,275 @@ struct Oracle {
     }
   }
 
+  // ---- IPC contact (jgs2-shader.ts:233-874, 2694-2929) ----
+  uint32_t NC = 0, NVT = 0;
+  std::vector<uint32_t> cIdx;                  // 4 per candidate
+  std::vector<uint32_t> cRows, cIds;           // vertex -> incident candidates (CSR)
+  std::vector<uint32_t> activeCount, activeIds;  // per-iteration active rows (capacity of cIds)
+  std::vector<V4<T>> srcC, srcW, tgtC, tgtW, lagN, lagW, scratch;
+  T contactAlpha = 1;
+  bool contactFixed = false;
+  T ipcMinDistance = 0, ipcFriction = 0, ipcEpsilon = 0, ipcSafety = 0;  // fixed at create
+
+  uint32_t cType(uint32_t c) const { return c < NVT ? kIpcVertexTriangle : kIpcEdgeEdge; }
+  T dHat() const { return static_cast<T>(st.ipcActivation); }
+  T kappa() const { return static_cast<T>(st.ipcStiffness); }
+  // ipcEnabled (jgs2-shader.ts:458-464).
+  bool ipcEnabled() const { return glob && NC > 0 && kappa() > T(0) && dHat() > ipcMinDistance; }
+  // ipcContactRoundingReach / ipcBarrierBroadPhaseThreshold / ipcActiveContactReach (:505-518).
+  T roundingReach() const {
+    return std::max(std::max(sceneScale, dHat()), T(1.0e-12)) * T(kUnitRoundoff) * T(kPositionResolutionMultiplier);
+  }
+  T broadPhaseThreshold() const { return dHat() + roundingReach(); }
+  T activeReach() const { return dHat() + T(2) * (std::max(static_cast<T>(st.maxStep), T(0)) + roundingReach()); }
+
+  Contact<T> contactAt(uint32_t c, const std::vector<V3<T>>& x, T threshold, uint32_t ov = 0xffffffffu,
+                       V3<T> op = v3<T>(0, 0, 0)) const {
+    const uint32_t* q = &cIdx[4ull * c];
+    return ipcContactFromPositions(cType(c), clothAt(x, q[0], ov, op), clothAt(x, q[1], ov, op),
+                                   clothAt(x, q[2], ov, op), clothAt(x, q[3], ov, op), threshold);
+  }
+  static void storeCache(std::vector<V4<T>>& cc, std::vector<V4<T>>& cw, uint32_t c, const Contact<T>& k) {
+    const bool valid = k.valid && finiteS(k.distance) && k.distance >= T(0) && finiteV(k.normal) && finite4v(k.weights);
+    cc[c] = valid ? V4<T>{k.normal.x, k.normal.y, k.normal.z, k.distance} : V4<T>{0, 0, 0, T(-1)};
+    cw[c] = valid ? k.weights : V4<T>{0, 0, 0, 0};
+  }
+  // ipcCachedContact (:408-437).
+  static Contact<T> cached(const V4<T>& nd, const V4<T>& w) {
+    const bool valid = nd.w >= T(0) && finite4v(nd) && finite4v(w);
+    const T d = valid ? nd.w : T(0);
+    return {v3<T>(0, 0, 0), d, v3<T>(0, 0, 0), d * d, valid ? v3(nd.x, nd.y, nd.z) : v3<T>(1, 0, 0), valid,
+            valid ? w : V4<T>{0, 0, 0, 0}};
+  }
+  Contact<T> sourceCache(uint32_t c) const { return cached(srcC[c], srcW[c]); }
+  Contact<T> targetCache(uint32_t c) const { return cached(tgtC[c], tgtW[c]); }
+  static T weightFor(const uint32_t* q, V4<T> w, uint32_t v) {
+    T r = 0;
+    if (q[0] == v) r += w.x;
+    if (q[1] == v) r += w.y;
+    if (q[2] == v) r += w.z;
+    if (q[3] == v) r += w.w;
+    return r;
+  }
+  // ipcWeightedDisplacement (:686-708): displacement since the frame start.
+  V3<T> weightedDisplacement(uint32_t c, V4<T> w, const std::vector<V3<T>>& x, uint32_t ov, V3<T> op) const {
+    const uint32_t* q = &cIdx[4ull * c];
+    V3<T> r = v3<T>(0, 0, 0);
+    r = r + w.x * (clothAt(x, q[0], ov, op) - old[q[0]]);
+    r = r + w.y * (clothAt(x, q[1], ov, op) - old[q[1]]);
+    r = r + w.z * (clothAt(x, q[2], ov, op) - old[q[2]]);
+    r = r + w.w * (clothAt(x, q[3], ov, op) - old[q[3]]);
+    return r;
+  }
+  // ipcCandidateEnergyFromContact (:710-741).
+  T candidateEnergy(uint32_t c, const Contact<T>& k, const std::vector<V3<T>>& x, uint32_t ov, V3<T> op) const {
+    if (!k.valid || !(k.distance > ipcMinDistance)) return static_cast<T>(kF32Max);
+    T e = kappa() * ipcBarrier(k.distance, dHat());
+    const V4<T> lag = lagN[c];
+    if (ipcFriction > T(0) && lag.w > T(0)) {
+      const V3<T> n = ipcSafeUnit(v3(lag.x, lag.y, lag.z), k.normal);
+      const V3<T> rel = weightedDisplacement(c, lagW[c], x, ov, op);
+      const V3<T> tang = rel - n * dot(n, rel);
+      const T slipVelocity = std::sqrt(dot(tang, tang)) * invDt;
+      e += dt * ipcFrictionDissipation(slipVelocity, ipcEpsilon, ipcFriction, lag.w);
+    }
+    return e;
+  }
+  uint32_t energyOwner(const uint32_t* q) const {
+    for (int l = 0; l < 4; ++l)
+      if (!pinned(q[l])) return q[l];
+    return q[0];
+  }
+  // ipcOwnedEnergy (:751-781); useTarget selects the target contact cache
+  // (ipcCachedContactAt, :439-449).
+  T ownedEnergy(uint32_t v, const std::vector<V3<T>>& x, bool useTarget) const {
+    if (!ipcEnabled()) return 0;
+    T r = 0;
+    for (uint32_t k = 0; k < activeCount[v]; ++k) {
+      const uint32_t c = activeIds[cRows[v] + k];
+      const Contact<T> contact = useTarget ? targetCache(c) : sourceCache(c);
+      if (!contact.valid) return static_cast<T>(kF32Max);
+      const bool barrier = ipcBarrierActive(contact.distance, dHat());
+      const bool friction = ipcFriction > T(0) && lagN[c].w > T(0);
+      if (!barrier && !friction) continue;
+      if (energyOwner(&cIdx[4ull * c]) != v) continue;
+      const T e = candidateEnergy(c, contact, x, 0xffffffffu, v3<T>(0, 0, 0));
+      if (!finiteS(e)) return static_cast<T>(kF32Max);
+      r += e;
+    }
+    return r;
+  }
+  // ipcLocalContribution (:788-869): barrier gradient and PSD normal block,
+  // lagged friction gradient and tangential block.
+  void contactLocal(uint32_t v, const std::vector<V3<T>>& x, bool fresh, V3<T>* grad, M3<T>* hess) const {
+    if (!ipcEnabled()) return;
+    for (uint32_t k = 0; k < activeCount[v]; ++k) {
+      const uint32_t c = activeIds[cRows[v] + k];
+      const uint32_t* q = &cIdx[4ull * c];
+      const Contact<T> contact = fresh ? contactAt(c, x, dHat()) : sourceCache(c);
+      if (!contact.valid) continue;
+      const bool barrier = ipcBarrierActive(contact.distance, dHat());
+      const V4<T> lag = lagN[c];
+      const bool friction = ipcFriction > T(0) && lag.w > T(0);
+      if (!barrier && !friction) continue;
+      if (weightFor(q, V4<T>{1, 1, 1, 1}, v) == T(0)) continue;
+      const T w = weightFor(q, contact.weights, v);
+      if (w != T(0) && barrier) {
+        const T b1 = ipcBarrier1(contact.distance, dHat()), b2 = ipcBarrier2(contact.distance, dHat());
+        *grad = *grad + ipcNormalGradientScalar(w, kappa(), b1) * contact.normal;
+        if (hess) *hess = *hess + ipcPsdNormalHessian(contact.normal, ipcPsdScalar(w, kappa(), b2));
+      }
+      const T lw = weightFor(q, lagW[c], v);
+      if (friction && lw != T(0)) {
+        const V3<T> n = ipcSafeUnit(v3(lag.x, lag.y, lag.z), contact.normal);
+        const V3<T> rel = weightedDisplacement(c, lagW[c], x, 0xffffffffu, v3<T>(0, 0, 0));
+        const V3<T> tang = rel - n * dot(n, rel);
+        const T slip = std::sqrt(dot(tang, tang));
+        const T slipVelocity = slip * invDt;
+        const T scale = ipcFriction * lag.w;
+        V3<T> dir = v3<T>(0, 0, 0);
+        if (slip > T(1.0e-12)) dir = tang / slip;
+        const T f1 = ipcFrictionF1(slipVelocity, ipcEpsilon);
+        *grad = *grad + lw * scale * f1 * dir;
+        if (hess) {
+          const M3<T> projector = identityM<T>() - ipcPsdNormalHessian(n, T(1));
+          T curvature = T(2) * scale / std::max(ipcEpsilon * dt, T(1.0e-12));
+          if (slip > T(1.0e-12)) curvature = scale * f1 / slip;
+          *hess = *hess + (lw * lw * std::max(curvature, T(0))) * projector;
+        }
+      }
+    }
+  }
+  bool pinnedMotionExceeds(uint32_t c, T bound) const {
+    const uint32_t* q = &cIdx[4ull * c];
+    for (int l = 0; l < 4; ++l) {
+      if (!pinned(q[l])) continue;
+      const V3<T> d = v3(restMass[q[l]].x, restMass[q[l]].y, restMass[q[l]].z) - (*src)[q[l]];
+      const T len = std::sqrt(dot(d, d));
+      if (!finiteV(d) || !finiteS(len) || len > bound) return true;
+    }
+    return false;
+  }
+  // lagContact (:2712-2740), at the accepted pose.
+  void lagContact() {
+    for (uint32_t c = 0; c < NC; ++c) {
+      const Contact<T> k = contactAt(c, posA, broadPhaseThreshold());
+      storeCache(srcC, srcW, c, k);
+      V4<T> force{0, 0, 0, 0}, w{0, 0, 0, 0};
+      if (k.valid && k.distance > ipcMinDistance) {
+        const T f = std::max(T(0), -kappa() * ipcBarrier1(k.distance, dHat()));
+        if (finiteS(f)) { force = {k.normal.x, k.normal.y, k.normal.z, f}; w = k.weights; }
+      }
+      lagN[c] = force;
+      lagW[c] = w;
+      scratch[c] = {1, 0, 0, 0};
+    }
+    contactAlpha = 1;
+  }
+  // buildActiveContactRows (:2742-2782).
+  void buildActiveRows() {
+    const bool bounded = st.maxStep > 0;
+    const T reach = activeReach();
+    for (uint32_t v = 0; v < V; ++v) {
+      uint32_t n = 0;
+      for (uint32_t k = cRows[v]; k < cRows[v + 1]; ++k) {
+        const uint32_t c = cIds[k];
+        const Contact<T> contact = sourceCache(c);
+        const bool friction = ipcFriction > T(0) && lagN[c].w > T(0);
+        const bool pinnedMotion = pinnedMotionExceeds(c, std::max(static_cast<T>(st.maxStep), T(0)));
+        if (!contact.valid || !bounded || contact.distance <= reach || friction || pinnedMotion)
+          activeIds[cRows[v] + n++] = c;
+      }
+      activeCount[v] = n;
+    }
+  }
+  // candidateContactStep (:2784-2847) + reduceContactStep (:2870-2907).
+  void contactStepAndReduce() {
+    if (latched()) {
+      for (uint32_t c = 0; c < NC; ++c) scratch[c] = {1, 0, 0, 1};
+    } else {
+      for (uint32_t c = 0; c < NC; ++c) {
+        const uint32_t* q = &cIdx[4ull * c];
+        V3<T> d[4];
+        for (int l = 0; l < 4; ++l) d[l] = (*tgt)[q[l]] - (*src)[q[l]];
+        T L = 0;
+        if (cType(c) == kIpcVertexTriangle)
+          L = length3(d[0]) + std::max(length3(d[1]), std::max(length3(d[2]), length3(d[3])));
+        else
+          L = std::max(length3(d[0]), length3(d[1])) + std::max(length3(d[2]), length3(d[3]));
+        Contact<T> source = sourceCache(c);
+        bool fullStepSafe = source.valid && finiteS(L) && source.distance - L > ipcMinDistance;
+        if (!fullStepSafe) {
+          source = contactAt(c, *src, static_cast<T>(kF32Max));
+          fullStepSafe = source.valid && finiteS(L) && source.distance - L > ipcMinDistance;
+        }
+        const bool trialValid = finiteV(d[0]) && finiteV(d[1]) && finiteV(d[2]) && finiteV(d[3]);
+        const bool valid = source.valid && trialValid && source.distance > ipcMinDistance && finiteS(L);
+        T alpha = 0;
+        if (valid) alpha = fullStepSafe ? T(1) : ipcSafeStepCap(source.distance, ipcMinDistance, L, ipcSafety);
+        scratch[c] = {alpha, source.valid ? source.distance : T(0), trialValid ? source.distance : T(0),
+                      valid ? T(1) : T(0)};
+      }
+    }
+    reduceContactStep();
+  }
+  void reduceContactStep() {
+    T minimum = 1;
+    bool all = true;
+    for (uint32_t c = 0; c < NC; ++c) {
+      const V4<T> s = scratch[c];
+      const bool valid = s.w == T(1) && finiteS(s.x) && finiteS(s.y) && finiteS(s.z);
+      minimum = std::min(minimum, valid ? s.x : T(0));
+      all = all && valid;
+    }
+    contactAlpha = all ? clamp01(minimum) : T(0);
+  }
+  // applyContactStep (:2909-2917).
+  void applyContactStep() {
+    if (latched()) return;
+    const T a = clamp01(contactAlpha);
+    for (uint32_t v = 0; v < V; ++v) (*tgt)[v] = (*src)[v] + a * ((*tgt)[v] - (*src)[v]);
+  }
+  // validateContactStep (:2849-2868).
+  void validateContactStep() {
+    for (uint32_t c = 0; c < NC; ++c) {
+      const Contact<T> k = contactAt(c, *tgt, broadPhaseThreshold());
+      storeCache(tgtC, tgtW, c, k);
+      const bool valid = k.valid && finiteS(k.distance) && k.distance > ipcMinDistance;
+      const T d = valid ? k.distance : T(0);
+      scratch[c] = {1, d, d, valid ? T(1) : T(0)};
+    }
+    reduceContactStep();
+  }
+  // promoteAcceptedContactCache (:2694-2710).
+  void promoteContacts() {
+    if (!(control[1].x == T(1) && finiteS(contactAlpha) && contactAlpha > T(0))) return;
+    srcC = tgtC;
+    srcW = tgtW;
+  }
+
   struct Geometry { T minimum; bool valid; };
   Geometry restrictedMinimumDeterminant(uint32_t v, V3<T> d) const {
     T minimum = static_cast<T>(kF32Max);
     const V4<T> pre = control[0];
     const uint32_t bits = validityBits(pre.w);
     if ((bits & kAcceptedMinimumValid) != 0 && finiteS(pre.z)) minimum = pre.z;
+    // IPC: a trial that brings an active candidate within the minimum
+    // distance is infeasible (jgs2-shader.ts:1997-2038).
+    if (ipcEnabled()) {
+      const V3<T> trial = (*src)[v] + d;
+      const T dl = length3(d);
+      for (uint32_t k = 0; k < activeCount[v]; ++k) {
+        const uint32_t c = activeIds[cRows[v] + k];
+        const Contact<T> source = activeColor >= 0 ? contactAt(c, *src, dHat()) : sourceCache(c);
+        if (!source.valid) return {0, false};
+        if (source.distance - dl > ipcMinDistance) continue;
+        if (weightFor(&cIdx[4ull * c], V4<T>{1, 1, 1, 1}, v) == T(0)) continue;
+        const Contact<T> trialContact = contactAt(c, *src, dHat(), v, trial);
+        if (!trialContact.valid) return {0, false};
+        if (!(trialContact.distance > ipcMinDistance)) return {0, true};
+      }
+    }
     const uint32_t start = info[4 * v], count = info[4 * v + 1];
     for (uint32_t a = 0; a < count; ++a) {
       const uint32_t t = adjacency[start + a];
@@ -793,6 +1263,26 @@ struct Oracle {
     const T inertia = restMass[v].w * invDt2;
     T result = quadraticDelta(sp, predicted[v], d, inertia) + floorDelta(sp.y, d.y);
     if (objectiveFlags != 0) result += objectiveDelta(v, sp, d);
+    // IPC barrier and lagged friction deltas (jgs2-shader.ts:2137-2196).
+    if (ipcEnabled()) {
+      const V3<T> trial = sp + d;
+      const T dl = length3(d);
+      for (uint32_t k = 0; k < activeCount[v]; ++k) {
+        const uint32_t c = activeIds[cRows[v] + k];
+        const Contact<T> source = activeColor >= 0 ? contactAt(c, *src, dHat()) : sourceCache(c);
+        if (!source.valid) return static_cast<T>(kF32Max);
+        const bool friction = ipcFriction > T(0) && lagN[c].w > T(0);
+        const bool barrierMayChange = source.distance - dl < dHat();
+        if (!barrierMayChange && !friction) continue;
+        if (weightFor(&cIdx[4ull * c], V4<T>{1, 1, 1, 1}, v) == T(0)) continue;
+        Contact<T> trialContact = {v3<T>(0, 0, 0), dHat(), v3<T>(0, 0, 0), dHat() * dHat(), v3<T>(1, 0, 0), true,
+                                   {0, 0, 0, 0}};
+        if (barrierMayChange) trialContact = contactAt(c, *src, dHat(), v, trial);
+        const T se = candidateEnergy(c, source, *src, 0xffffffffu, v3<T>(0, 0, 0));
+        const T te = candidateEnergy(c, trialContact, *src, v, trial);
+        result += te - se;
+      }
+    }
     const uint32_t start = info[4 * v], count = info[4 * v + 1];
     for (uint32_t a = 0; a < count; ++a) {
       const uint32_t t = adjacency[start + a];
@@ -882,7 +1372,7 @@ struct Oracle {
     local[4 * v + 2] = {dE, bound, gdd, res};
     local[4 * v + 3] = {minDet, T(back), T(evals), T(status)};
   }
-  T implicitEnergyAt(const std::vector<V3<T>>& x, uint32_t v) const {
+  T implicitEnergyAt(const std::vector<V3<T>>& x, uint32_t v, bool useTargetCache = false) const {
     const bool pin = pinned(v);
     const V3<T> p = x[v];
     T e = 0;
@@ -924,10 +1414,14 @@ struct Oracle {
         e += bendingEnergyAt(h, x, 0xffffffffu, v3<T>(0, 0, 0));
       }
     }
+    e += ownedEnergy(v, x, useTargetCache);
     return e;
   }
   void storeAssembledVertexEnergy(uint32_t v) {
-    const T se = implicitEnergyAt(*src, v), ce = implicitEnergyAt(*tgt, v);
+    // The candidate pose reads the target contact cache unless the contact
+    // step collapsed to zero (ipcCachedContactAt, jgs2-shader.ts:439-449).
+    const bool target = src != tgt && contactAlpha != T(0);
+    const T se = implicitEnergyAt(*src, v, false), ce = implicitEnergyAt(*tgt, v, target);
     const bool sv = finiteS(se), cv = finiteS(ce);
     vertexEnergy[v] = {sv ? se : T(0), cv ? ce : T(0), sv ? T(1) : T(0), cv ? T(1) : T(0)};
   }
@@ -1027,6 +1521,7 @@ struct Oracle {
       gradient.y += static_cast<T>(st.floorStiffness) * (position.y - static_cast<T>(st.floorHeight));
       hessian.c[1].y += static_cast<T>(st.floorStiffness);
     }
+    contactLocal(v, *src, activeColor >= 0, &gradient, &hessian);
     for (uint32_t s = 0; s < K; ++s) {
       const size_t rec = static_cast<size_t>(v) * K + s;
       const uint32_t t = cubTet[rec];
@@ -1342,6 +1837,7 @@ struct Oracle {
       V3<T> contact = v3<T>(0, 0, 0);
       if (st.floorStiffness > 0 && p.y < static_cast<T>(st.floorHeight))
         contact.y = static_cast<T>(st.floorStiffness) * (p.y - static_cast<T>(st.floorHeight));
+      contactLocal(v, *tgt, false, &contact, nullptr);
       base[0] = {inertia.x, inertia.y, inertia.z, 0};
       base[1] = {material.x, material.y, material.z, 0};
       base[2] = {ef.x, ef.y, ef.z, 0};
@@ -1527,8 +2023,11 @@ struct Oracle {
 
   // encodeFrame (src/simulation/gpu/jgs2-solver.ts:2207-2494), IPC/cloth off.
   void frame(uint32_t iterations) {
+    // contactEnabled (jgs2-solver.ts:2213-2214).
+    const bool contact = ipcEnabled();
     bind(&posA, &posA, -1);
     predict();
+    if (contact) lagContact();
     if (glob) {
       candidateTetrahedron();
       reduceCandidate();
@@ -1537,6 +2036,7 @@ struct Oracle {
       std::vector<V3<T>>* s = (it % 2 == 0) ? &posB : &posA;
       std::vector<V3<T>>* t = (it % 2 == 0) ? &posA : &posB;
       bind(s, t, -1);
+      if (contact) buildActiveRows();
       if (st.schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL) {
         copyPosition();
         for (uint32_t c = 0; c < colorCount; ++c) {
@@ -1546,16 +2046,27 @@ struct Oracle {
           solveAll();
         }
         bind(s, t, -1);
-        if (glob) assembledVertexEnergyAll();
+        if (glob && !contact) assembledVertexEnergyAll();
       } else {
         tetPolarRotation();
         vertexPolarRotation();
         solveAll();
       }
+      if (contact) {
+        // Safe-step scaling of the candidate, exact validation of the scaled
+        // pose (a failure restores the source), then the assembled energies
+        // of the final pair (jgs2-solver.ts:2340-2393).
+        contactStepAndReduce();
+        applyContactStep();
+        validateContactStep();
+        applyContactStep();
+        assembledVertexEnergyAll();
+      }
       if (glob) {
         candidateTetrahedron();
         reduceCandidate();
         applyCandidate();
+        if (contact) promoteContacts();
         convergenceGradient();
         reduceConvergence();
       }
@@ -1575,7 +2086,7 @@ struct Oracle {
 
 // buildGreedyVertexColoring (src/simulation/cpu/vertex-coloring.ts:20-110)
 // over the conflict groups of buildJGS2InputVertexColoring
-// (src/simulation/gpu/jgs2-solver.ts:308-367), IPC groups absent.
+// (src/simulation/gpu/jgs2-solver.ts:308-367).
 std::vector<uint32_t> greedyColoring(const jgs2_input* in, uint32_t* countOut) {
   const uint32_t V = in->vertex_count;
   std::vector<std::vector<uint32_t>> adj(V);
@@ -1606,6 +2117,10 @@ std::vector<uint32_t> greedyColoring(const jgs2_input* in, uint32_t* countOut) {
   if (in->cloth) {
     for (uint32_t c = 0; c < in->cloth->triangle_count; ++c) addGroup(&in->cloth->triangle_indices[3ull * c], 3);
     for (uint32_t h = 0; h < in->cloth->hinge_count; ++h) addGroup(&in->cloth->hinge_indices[4ull * h], 4);
+  }
+  if (in->contact_indices) {
+    const uint64_t nc = uint64_t(in->contact_vertex_triangle_count) + in->contact_edge_edge_count;
+    for (uint64_t c = 0; c < nc; ++c) addGroup(&in->contact_indices[4 * c], 4);
   }
   std::vector<uint32_t> colors(V, 0xffffffffu), stamp(V + 1, 0);
   uint32_t count = 0, st = 0;
@@ -1744,6 +2259,30 @@ void initOracle(Oracle<T>& o, const jgs2_input* in) {
     csr(o.clothTri, 3, o.triRows, o.triElems);
     csr(o.hingeIdx, 4, o.hingeRows, o.hingeElems);
   }
+  // Static IPC candidates (packIpcContactBuffer and
+  // packIpcIncidentCandidateAdjacency, ipc-contact-layout.ts:190-342):
+  // empty contact caches, zero lagged records, incidence CSR.
+  o.NVT = in->contact_indices ? in->contact_vertex_triangle_count : 0;
+  o.NC = in->contact_indices ? in->contact_vertex_triangle_count + in->contact_edge_edge_count : 0;
+  o.cIdx.assign(in->contact_indices, in->contact_indices + 4ull * o.NC);
+  o.cRows.assign(V + 1, 0);
+  for (uint32_t q : o.cIdx) o.cRows[q + 1] += 1;
+  for (uint32_t v = 0; v < V; ++v) o.cRows[v + 1] += o.cRows[v];
+  o.cIds.assign(o.cIdx.size(), 0);
+  {
+    std::vector<uint32_t> cursor(o.cRows.begin(), o.cRows.end() - 1);
+    for (uint32_t c = 0; c < o.NC; ++c)
+      for (int l = 0; l < 4; ++l) o.cIds[cursor[o.cIdx[4ull * c + l]]++] = c;
+  }
+  o.activeCount.assign(V, 0);
+  o.activeIds.assign(o.cIds.size(), 0);
+  o.srcC.assign(o.NC, {0, 0, 0, T(-1)});
+  o.tgtC.assign(o.NC, {0, 0, 0, T(-1)});
+  o.srcW.assign(o.NC, {0, 0, 0, 0});
+  o.tgtW.assign(o.NC, {0, 0, 0, 0});
+  o.lagN.assign(o.NC, {0, 0, 0, 0});
+  o.lagW.assign(o.NC, {0, 0, 0, 0});
+  o.scratch.assign(o.NC, {1, 0, 0, 0});
   o.tetGlob.assign(2ull * (Tn + o.C), {0, 0, 0, 0});
   o.vertexEnergy.assign(V, {0, 0, 0, 0});
   o.conv.assign(5ull * V, {0, 0, 0, 0});
@@ -1769,6 +2308,12 @@ void applySettings(Oracle<T>& o, const jgs2_settings* s, bool stop) {
   o.st.contactTangentialDamping = s->contact_tangential_damping;
   o.st.contactMargin = s->contact_margin;
   o.st.horizontalBodyCorrection = s->horizontal_body_correction != 0;
+  o.st.ipcActivation = s->ipc_activation_distance;
+  o.st.ipcStiffness = s->ipc_barrier_stiffness;
+  // resolveStepSettings (jgs2-solver.ts:1999-2009): body correction is off
+  // while objectives or mesh contacts act on the stable path.
+  if (o.glob && (o.objectiveFlags != 0 || (o.NC > 0 && s->ipc_barrier_stiffness > 0)))
+    o.st.horizontalBodyCorrection = false;
   // packUniforms (src/simulation/gpu/jgs2-solver.ts:604-730): the time vec4
   // is (dt, 1/dt, 1/dt^2, maxStep), formed in double and stored as f32.
   const double dt = s->timestep;
@@ -1842,6 +2387,23 @@ void* jgs2_oracle_create(const jgs2_input* input, int precision) {
 }
 
 void jgs2_oracle_destroy(void* handle) { delete static_cast<Handle*>(handle); }
+
+// The create-time IPC parameters (minimum distance, friction coefficient,
+// friction velocity smoothing, step safety), which the reference writes into
+// the contact buffer once at create (jgs2-solver.ts:1096-1105).
+int jgs2_oracle_fix_contact(void* handle, const jgs2_settings* s) {
+  Handle* h = static_cast<Handle*>(handle);
+  auto body = [&](auto& o) {
+    using T = std::remove_reference_t<decltype(o.dt)>;
+    o.ipcMinDistance = static_cast<T>(s->ipc_minimum_distance);
+    o.ipcFriction = static_cast<T>(s->ipc_friction_coefficient);
+    o.ipcEpsilon = static_cast<T>(s->ipc_friction_velocity_epsilon);
+    o.ipcSafety = static_cast<T>(s->ipc_step_safety);
+    o.contactFixed = true;
+  };
+  if (h->dbl) body(h->d); else body(h->f);
+  return 0;
+}
 
 void jgs2_oracle_set_threads(int threads) {
   if (threads > 0) omp_set_num_threads(threads);
@@ -2000,6 +2562,52 @@ void clothBendingElement(const double* x, double restAngle, double restLength, d
 }
 }  // namespace
 extern "C" {
+
+// IPC scalar kernels and contact features for the reference's contact tests
+// (src/simulation/cpu/ipc-contact.test.ts).  barrier: out = B, B', B''.
+// friction: out = f1 and the lagged dissipation for (mu, lambda) = (1, 1).
+// contact: type 0 = point-triangle (p, t0, t1, t2), 1 = edge-edge; out =
+// distance, normal xyz, weights xyzw, valid.
+int jgs2_oracle_ipc_barrier(double d, double dHat, int precision, double* out) {
+  if (precision == 64) {
+    out[0] = ipcBarrier(d, dHat); out[1] = ipcBarrier1(d, dHat); out[2] = ipcBarrier2(d, dHat);
+  } else {
+    const float a = static_cast<float>(d), b = static_cast<float>(dHat);
+    out[0] = ipcBarrier(a, b); out[1] = ipcBarrier1(a, b); out[2] = ipcBarrier2(a, b);
+  }
+  return 0;
+}
+
+int jgs2_oracle_ipc_friction(double slip, double eps, double* out) {
+  out[0] = ipcFrictionF1(slip, eps);
+  out[1] = ipcFrictionDissipation(slip, eps, 1.0, 1.0);
+  return 0;
+}
+
+int jgs2_oracle_ipc_contact(uint32_t type, const double* x, double* out) {
+  V3<double> p[4];
+  for (int l = 0; l < 4; ++l) p[l] = v3(x[3 * l], x[3 * l + 1], x[3 * l + 2]);
+  const Contact<double> k = type == 0 ? ipcPointTriangle(p[0], p[1], p[2], p[3]) : ipcEdgeEdge(p[0], p[1], p[2], p[3]);
+  out[0] = k.distance;
+  out[1] = k.normal.x; out[2] = k.normal.y; out[3] = k.normal.z;
+  out[4] = k.weights.x; out[5] = k.weights.y; out[6] = k.weights.z; out[7] = k.weights.w;
+  out[8] = k.valid ? 1.0 : 0.0;
+  return 0;
+}
+
+// Minimum exact contact distance over the candidates at the current pose.
+double jgs2_oracle_min_contact_distance(void* handle) {
+  Handle* h = static_cast<Handle*>(handle);
+  auto body = [&](auto& o) {
+    double m = 3.0e38;
+    for (uint32_t c = 0; c < o.NC; ++c) {
+      const auto k = o.contactAt(c, o.posA, static_cast<decltype(o.dt)>(kF32Max));
+      if (k.valid) m = std::min(m, static_cast<double>(k.distance));
+    }
+    return m;
+  };
+  return h->dbl ? body(h->d) : body(h->f);
+}
 
 int jgs2_oracle_cloth_membrane(const double* positions, const double* inverse, double area, double young,
                                double poisson, double thickness, int precision, double* out) {

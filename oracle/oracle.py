@@ -80,6 +80,7 @@ def lib():
         L.jgs2_oracle_set_objectives.argtypes = [c_void_p, POINTER(c_float), POINTER(c_float),
                                                  POINTER(c_float)]
         L.jgs2_oracle_evaluate_candidate.argtypes = [c_void_p, c_void_p, POINTER(c_float), POINTER(c_float)]
+        L.jgs2_oracle_fix_contact.argtypes = [c_void_p, c_void_p]
         _lib = L
     return _lib
 
@@ -112,6 +113,8 @@ class OracleSolver:
             raise RuntimeError("oracle create failed")
         self.vertex_count = scene_input.vertex_count
         self.defaults = resolve_settings(None, **(settings or {}))
+        # The IPC parameters the reference fixes at create.
+        self._L.jgs2_oracle_fix_contact(self._h, ctypes.byref(_settings_struct(self.defaults)))
 
     def __del__(self):
         h = getattr(self, "_h", None)

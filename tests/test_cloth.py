@@ -373,6 +373,13 @@ def test_cloth_batch_matches_alone():
     for a in alone:
         a.stepFramesExactIterations(4, 5)
     for i, a in enumerate(alone):
-        np.testing.assert_array_equal(batch.readPositions(i), a.readPositions(), err_msg=f"scene {i}")
+        if parts[i].cloth_triangles is not None:
+            # The same kernels alone and in the batch: bitwise.
+            np.testing.assert_array_equal(batch.readPositions(i), a.readPositions(), err_msg=f"scene {i}")
+        else:
+            # Alone, a tet-only scene runs the kernel variant without cloth
+            # terms, whose floating-point contractions may differ.
+            err = np.abs(batch.readPositions(i) - a.readPositions()).max() / parts[i].bbox_diagonal()
+            assert err <= TOL, f"scene {i}: {err}"
         a.destroy()
     batch.destroy()

@@ -25,6 +25,7 @@
 #include <algorithm>
 
 #include "jgs2_cloth.cuh"
+#include "jgs2_contact.cuh"
 #include "jgs2_device.cuh"
 #include "jgs2_kernels.cuh"
 
@@ -515,6 +516,302 @@ __global__ void __launch_bounds__(kBlock) copyKernel(Buffers b, const DevParams*
 }
 
 // ---------------------------------------------------------------------------
+// IPC contact (jgs2-shader.ts:233-874, 2694-2917).
+
+__device__ __forceinline__ uint4 contactIndices(const Buffers& b, uint32_t c, uint32_t* type) {
+  uint4 q = __ldg(&b.contactIdx[c]);
+  *type = q.w >> 31;
+  q.w &= 0x7fffffffu;
+  return q;
+}
+
+__device__ __forceinline__ float3 posOverride(const float4* __restrict__ x, uint32_t q, uint32_t ov, float3 op) {
+  return q == ov ? op : xyz(x[q]);
+}
+
+// ipcContactAtThreshold / ipcContactAtOverride (:594-668).
+__device__ __forceinline__ ContactData contactAt(const Buffers& b, uint32_t c, const float4* __restrict__ x,
+                                                 float threshold, uint32_t ov = 0xffffffffu,
+                                                 float3 op = make_float3(0.f, 0.f, 0.f)) {
+  uint32_t type;
+  const uint4 q = contactIndices(b, c, &type);
+  return ipcContactFromPositions(type, posOverride(x, q.x, ov, op), posOverride(x, q.y, ov, op),
+                                 posOverride(x, q.z, ov, op), posOverride(x, q.w, ov, op), threshold);
+}
+
+// ipcContactRoundingReach (:505-509).
+__device__ __forceinline__ float contactRoundingReach(const DevParams& p) {
+  return fmaxf(fmaxf(p.sceneScale, p.ipcActivation), 1.0e-12f) * kUnitRoundoff * kPositionResolutionMultiplier;
+}
+
+// ipcCandidatePinnedMotionExceedsBound (:476-503).
+__device__ __forceinline__ bool contactPinnedMotion(const Buffers& b, uint4 q, const float4* __restrict__ src,
+                                                    float bound) {
+  const uint32_t vs[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    if (!isPinned(b.vinfo[vs[l]])) continue;
+    const float3 d = xyz(b.restMass[vs[l]]) - xyz(src[vs[l]]);
+    const float len = length3(d);
+    if (!finiteV(d) || !finiteS(len) || len > bound) return true;
+  }
+  return false;
+}
+
+// includeCandidate of buildActiveContactRows (:2742-2782): a candidate stays
+// active unless its source cache is valid, beyond the reach a bounded step can
+// cross, frictionless and free of unbounded pinned motion.  The decision
+// depends on the candidate only, so every incident vertex agrees.
+__device__ __forceinline__ bool contactIncluded(const Buffers& b, const DevParams& p, uint32_t c,
+                                                const float4* __restrict__ src) {
+  const float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+  const ContactData k = ipcCached(st[kContactSource], st[kContactSourceWeights]);
+  const bool friction = p.ipcFriction > 0.0f && st[kContactLagged].w > 0.0f;
+  const bool bounded = p.maxStep > 0.0f;
+  const float reach = p.ipcActivation + 2.0f * (fmaxf(p.maxStep, 0.0f) + contactRoundingReach(p));
+  uint32_t type;
+  const uint4 q = contactIndices(b, c, &type);
+  const bool pinnedMotion = contactPinnedMotion(b, q, src, fmaxf(p.maxStep, 0.0f));
+  return !k.valid || !bounded || k.distance <= reach || friction || pinnedMotion;
+}
+
+// Displacement since the frame start weighted by the lagged weights
+// (ipcWeightedDisplacement, :686-708).
+__device__ __forceinline__ float3 contactRelative(const Buffers& b, uint4 q, float4 w, const float4* __restrict__ x,
+                                                  uint32_t ov, float3 op) {
+  float3 r = w.x * (posOverride(x, q.x, ov, op) - xyz(b.old[q.x]));
+  r = r + w.y * (posOverride(x, q.y, ov, op) - xyz(b.old[q.y]));
+  r = r + w.z * (posOverride(x, q.z, ov, op) - xyz(b.old[q.z]));
+  r = r + w.w * (posOverride(x, q.w, ov, op) - xyz(b.old[q.w]));
+  return r;
+}
+
+// ipcCandidateEnergyFromContact (:710-741).
+__device__ __forceinline__ float contactEnergy(const Buffers& b, const DevParams& p, uint32_t c, const ContactData& k,
+                                               const float4* __restrict__ x, uint32_t ov, float3 op) {
+  if (!k.valid || !(k.distance > p.ipcMinDistance)) return kF32Max;
+  float e = p.ipcStiffness * ipcBarrier(k.distance, p.ipcActivation);
+  const float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+  const float4 lag = st[kContactLagged];
+  if (p.ipcFriction > 0.0f && lag.w > 0.0f) {
+    const float3 n = ipcSafeUnit(xyz(lag), k.normal);
+    uint32_t type;
+    const uint4 q = contactIndices(b, c, &type);
+    const float3 rel = contactRelative(b, q, st[kContactLaggedWeights], x, ov, op);
+    const float3 tang = rel - n * dot3(n, rel);
+    e += p.dt * ipcFrictionDissipation(length3(tang) * p.invDt, p.ipcEpsilon, p.ipcFriction, lag.w);
+  }
+  return e;
+}
+
+// ipcLocalContribution (:788-869) over the vertex's active candidates
+// [first, count) step `stride`: barrier gradient and PSD normal block, lagged
+// friction gradient and tangential block.  `fresh` evaluates the contact at x
+// (the coloured schedule), otherwise the cache at `slot` is used.
+template <bool kHessian>
+__device__ __forceinline__ void contactLocal(const Buffers& b, const DevParams& p, uint32_t v,
+                                             const float4* __restrict__ x, bool fresh, int slot, uint32_t first,
+                                             uint32_t stride, float3& grad, S3& hess) {
+  const uint2 range = b.contactRange[v];
+  const uint32_t n = b.activeCount[v];
+  for (uint32_t a = first; a < n; a += stride) {
+    const uint32_t c = b.activeIds[range.x + a];
+    const float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+    const ContactData k = fresh ? contactAt(b, c, x, p.ipcActivation) : ipcCached(st[slot], st[slot + 1]);
+    if (!k.valid) continue;
+    const bool barrier = ipcBarrierActive(k.distance, p.ipcActivation);
+    const float4 lag = st[kContactLagged];
+    const bool friction = p.ipcFriction > 0.0f && lag.w > 0.0f;
+    if (!barrier && !friction) continue;
+    uint32_t type;
+    const uint4 q = contactIndices(b, c, &type);
+    if (ipcWeightFor(q, make_float4(1.f, 1.f, 1.f, 1.f), v) == 0.0f) continue;
+    const float w = ipcWeightFor(q, k.weights, v);
+    if (w != 0.0f && barrier) {
+      grad = grad + ipcNormalGradientScalar(w, p.ipcStiffness, ipcBarrier1(k.distance, p.ipcActivation)) * k.normal;
+      if (kHessian) {
+        const float s = ipcPsdScalar(w, p.ipcStiffness, ipcBarrier2(k.distance, p.ipcActivation));
+        saddOuter(hess, fmaxf(s, 0.0f), ipcSafeUnit(k.normal, f3(1, 0, 0)));
+      }
+    }
+    const float4 lagW = st[kContactLaggedWeights];
+    const float lw = ipcWeightFor(q, lagW, v);
+    if (friction && lw != 0.0f) {
+      const float3 nrm = ipcSafeUnit(xyz(lag), k.normal);
+      const float3 rel = contactRelative(b, q, lagW, x, 0xffffffffu, f3(0, 0, 0));
+      const float3 tang = rel - nrm * dot3(nrm, rel);
+      const float slip = length3(tang);
+      const float scale = p.ipcFriction * lag.w;
+      const float3 dir = slip > 1.0e-12f ? tang * (1.0f / slip) : f3(0, 0, 0);
+      const float f1 = ipcFrictionF1(slip * p.invDt, p.ipcEpsilon);
+      grad = grad + (lw * scale * f1) * dir;
+      if (kHessian) {
+        float curvature = 2.0f * scale / fmaxf(p.ipcEpsilon * p.dt, 1.0e-12f);
+        if (slip > 1.0e-12f) curvature = scale * f1 / slip;
+        const float c2 = lw * lw * fmaxf(curvature, 0.0f);
+        saddDiag(hess, c2);
+        saddOuter(hess, -c2, ipcSafeUnit(nrm, f3(1, 0, 0)));
+      }
+    }
+  }
+}
+
+// lagContact (:2712-2740): source cache and lagged normal force at the
+// accepted pose, once per frame.
+__global__ void __launch_bounds__(kBlock) contactLagKernel(Buffers b, const DevParams* __restrict__ pp) {
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= b.contactCount) return;
+  const uint32_t scene = b.contactScene[c];
+  const DevParams& p = pp[scene];
+  if (!p.active || !p.ipc) return;
+  const ContactData k = contactAt(b, c, b.pos[0], p.ipcActivation + contactRoundingReach(p));
+  float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+  ipcStoreCached(st, kContactSource, k);
+  float4 force = make_float4(0, 0, 0, 0), w = make_float4(0, 0, 0, 0);
+  if (k.valid && k.distance > p.ipcMinDistance) {
+    const float f = fmaxf(0.0f, -p.ipcStiffness * ipcBarrier1(k.distance, p.ipcActivation));
+    if (finiteS(f)) {
+      force = make_float4(k.normal.x, k.normal.y, k.normal.z, f);
+      w = k.weights;
+    }
+  }
+  st[kContactLagged] = force;
+  st[kContactLaggedWeights] = w;
+  st[kContactScratch] = make_float4(1, 0, 0, 0);
+  if (c == b.scenes[scene].kOff) b.frames[scene].contactAlpha = 1.0f;
+}
+
+// buildActiveContactRows (:2742-2782), and the reset of the iteration's
+// safe-step reductions.
+__global__ void __launch_bounds__(kBlock) contactRowsKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                            const float4* __restrict__ src, uint32_t V) {
+  const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
+  if (v >= V) return;
+  const uint32_t scene = b.vertexScene[v];
+  const DevParams& p = pp[scene];
+  if (!p.active || !p.ipc) return;
+  if (v == b.scenes[scene].vOff) {
+    FrameState* fs = &b.frames[scene];
+    fs->stepAlphaBits = __float_as_uint(1.0f);
+    fs->stepValid = 1u;
+    fs->checkAlphaBits = __float_as_uint(1.0f);
+    fs->checkValid = 1u;
+  }
+  const uint2 r = b.contactRange[v];
+  uint32_t n = 0;
+  for (uint32_t k = 0; k < r.y; ++k) {
+    const uint32_t c = b.contactIds[r.x + k];
+    if (contactIncluded(b, p, c, src)) b.activeIds[r.x + n++] = c;
+  }
+  b.activeCount[v] = n;
+}
+
+__device__ __forceinline__ uint32_t alphaBits(float a) { return a > 0.0f ? __float_as_uint(a) : 0u; }
+
+// candidateContactStep (:2784-2847) with the min / all-valid reduction of
+// reduceContactStep folded in as order-free atomics.
+__global__ void __launch_bounds__(kBlock) contactStepKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                            const float4* __restrict__ src,
+                                                            const float4* __restrict__ tgt) {
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= b.contactCount) return;
+  const uint32_t scene = b.contactScene[c];
+  const DevParams& p = pp[scene];
+  if (!p.active || !p.ipc) return;
+  FrameState* fs = &b.frames[scene];
+  float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+  if (latched(p, fs)) {
+    st[kContactScratch] = make_float4(1, 0, 0, 1);
+    return;  // alpha one, valid: the reduction's identity
+  }
+  uint32_t type;
+  const uint4 q = contactIndices(b, c, &type);
+  const float3 d0 = xyz(tgt[q.x]) - xyz(src[q.x]), d1 = xyz(tgt[q.y]) - xyz(src[q.y]);
+  const float3 d2 = xyz(tgt[q.z]) - xyz(src[q.z]), d3 = xyz(tgt[q.w]) - xyz(src[q.w]);
+  float L = 0.0f;
+  if (type == kIpcVertexTriangle) L = length3(d0) + fmaxf(length3(d1), fmaxf(length3(d2), length3(d3)));
+  else L = fmaxf(length3(d0), length3(d1)) + fmaxf(length3(d2), length3(d3));
+  ContactData source = ipcCached(st[kContactSource], st[kContactSourceWeights]);
+  bool fullStepSafe = source.valid && finiteS(L) && source.distance - L > p.ipcMinDistance;
+  if (!fullStepSafe) {
+    source = contactAt(b, c, src, kF32Max);
+    fullStepSafe = source.valid && finiteS(L) && source.distance - L > p.ipcMinDistance;
+  }
+  const bool trialValid = finiteV(d0) && finiteV(d1) && finiteV(d2) && finiteV(d3);
+  const bool valid = source.valid && trialValid && source.distance > p.ipcMinDistance && finiteS(L);
+  float alpha = 0.0f;
+  if (valid) alpha = fullStepSafe ? 1.0f : ipcSafeStepCap(source.distance, p.ipcMinDistance, L, p.ipcSafety);
+  st[kContactScratch] = make_float4(alpha, source.valid ? source.distance : 0.0f,
+                                    trialValid ? source.distance : 0.0f, valid ? 1.0f : 0.0f);
+  if (valid && finiteS(alpha)) {
+    if (alpha < 1.0f) atomicMin(&fs->stepAlphaBits, alphaBits(alpha));
+  } else {
+    atomicMin(&fs->stepAlphaBits, 0u);
+    atomicAnd(&fs->stepValid, 0u);
+  }
+}
+
+// applyContactStep (:2909-2917): candidate = source + alpha (candidate -
+// source) with the safe-step alpha, or after validation with 1 (kept) or 0
+// (restored); the validated alpha becomes the iteration's contact alpha.
+__global__ void __launch_bounds__(kBlock) contactApplyKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                             const float4* __restrict__ src, float4* tgt,
+                                                             uint32_t V, int validated) {
+  const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
+  if (v >= V) return;
+  const uint32_t scene = b.vertexScene[v];
+  const DevParams& p = pp[scene];
+  if (!p.active || !p.ipc) return;
+  FrameState* fs = &b.frames[scene];
+  const uint32_t bits = validated ? fs->checkAlphaBits : fs->stepAlphaBits;
+  const uint32_t ok = validated ? fs->checkValid : fs->stepValid;
+  const float alpha = ok ? clamp01f(__uint_as_float(bits)) : 0.0f;
+  if (validated && v == b.scenes[scene].vOff) fs->contactAlpha = alpha;
+  if (latched(p, fs)) return;
+  const float3 s = xyz(src[v]);
+  const float3 t = s + alpha * (xyz(tgt[v]) - s);
+  tgt[v] = make_float4(t.x, t.y, t.z, 1.0f);
+}
+
+// validateContactStep (:2849-2868): exact contacts of the scaled candidate
+// (the target cache) and the all-valid reduction.
+__global__ void __launch_bounds__(kBlock) contactValidateKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                                const float4* __restrict__ tgt) {
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= b.contactCount) return;
+  const uint32_t scene = b.contactScene[c];
+  const DevParams& p = pp[scene];
+  if (!p.active || !p.ipc) return;
+  FrameState* fs = &b.frames[scene];
+  const ContactData k = contactAt(b, c, tgt, p.ipcActivation + contactRoundingReach(p));
+  float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+  ipcStoreCached(st, kContactTarget, k);
+  const bool valid = k.valid && finiteS(k.distance) && k.distance > p.ipcMinDistance;
+  const float d = valid ? k.distance : 0.0f;
+  st[kContactScratch] = make_float4(1.0f, d, d, valid ? 1.0f : 0.0f);
+  if (!valid) {
+    atomicMin(&fs->checkAlphaBits, 0u);
+    atomicAnd(&fs->checkValid, 0u);
+  }
+}
+
+// promoteAcceptedContactCache (:2694-2710).
+__global__ void __launch_bounds__(kBlock) contactPromoteKernel(Buffers b, const DevParams* __restrict__ pp) {
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= b.contactCount) return;
+  const uint32_t scene = b.contactScene[c];
+  const DevParams& p = pp[scene];
+  if (!p.active || !p.ipc) return;
+  const FrameState* fs = &b.frames[scene];
+  const float alpha = fs->contactAlpha;
+  if (fs->control[1].x == 1.0f && finiteS(alpha) && alpha > 0.0f) {
+    float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+    st[kContactSource] = st[kContactTarget];
+    st[kContactSourceWeights] = st[kContactTargetWeights];
+  }
+}
+
+// ---------------------------------------------------------------------------
 // The per-vertex JGS2 local solve, stable Neo-Hookean path
 // (jgs2Solve, jgs2-shader.ts:2991-3473).  W lanes cooperate on one vertex:
 // item u < K is cubature record u, item u >= K is incident tet u - K; lane j
@@ -537,9 +834,9 @@ static_assert(sizeof(CubState) <= kRecFloats * 4, "cubature cache record too sma
 #define JGS2_SOLVE_MIN_BLOCKS 4
 #endif
 
-// kCloth: some scene of the engine has cloth (the cloth gathers and line
-// search terms are compiled out otherwise).
-template <int W, bool kCloth>
+// kExt: some scene of the engine has cloth or contact candidates (their
+// gathers and line search terms are compiled out otherwise).
+template <int W, bool kExt>
 __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
                                                       const float4* __restrict__ src, float4* tgt,
                                                       const uint32_t* __restrict__ list, uint32_t count,
@@ -741,10 +1038,14 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             addIncidentBlock(hess, r, F, pt, g);
           }
           // ---- cloth membrane and bending (jgs2-shader.ts:3113-3186) ----
-          if (kCloth && p.cloth)
+          if (kExt && p.cloth)
             clothLocalSystem<true>(b.clothTris, b.clothHinges, b.clothIncidence, b.clothRange[v], src,
                                    clothMaterial(p), lane, W, grad, hess);
         }
+        // ---- IPC contact (jgs2-shader.ts:3193-3195): the cached source
+        // contacts, or fresh ones under the coloured schedule ----
+        if (kExt && p.ipc)
+          contactLocal<true>(b, p, v, src, !cachedIncident, kContactSource, lane, W, grad, hess);
         // Group reduction of the gather.
         grad.x = groupSum<W>(grad.x, mask);
         grad.y = groupSum<W>(grad.y, mask);
@@ -795,7 +1096,9 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
           const float dl = scaledLength(dr.direction);
           if (p.maxStep > 0.0f && dl > p.maxStep) ta = p.maxStep / dl;
           const float controlMin = c0.z;  // accepted-source minimum (finite here)
-          const uint4 cr = (kCloth && p.cloth) ? b.clothRange[v] : make_uint4(0u, 0u, 0u, 0u);
+          const uint4 cr = (kExt && p.cloth) ? b.clothRange[v] : make_uint4(0u, 0u, 0u, 0u);
+          const uint32_t contactFirst = (kExt && p.ipc) ? b.contactRange[v].x : 0u;
+          const uint32_t contactActive = (kExt && p.ipc) ? b.activeCount[v] : 0u;
           const ClothMaterial cmat = clothMaterial(p);
           for (uint32_t bt = 0; bt <= kMaxBacktracks; ++bt) {
             const float3 tp = position + ta * dr.direction;
@@ -878,6 +1181,37 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                                                   slot == 2u ? trialPos : x2, slot == 3u ? trialPos : x3, rest,
                                                   cmat.bending);
               de += et - es;
+            }
+            // IPC: a trial within the minimum distance of an active candidate
+            // is infeasible (jgs2-shader.ts:1997-2038); barrier and lagged
+            // friction energy deltas (:2137-2196).
+            if (kExt && contactActive) {
+              const float dl = length3(td);
+              for (uint32_t a = lane; a < contactActive; a += W) {
+                const uint32_t c = b.activeIds[contactFirst + a];
+                const float4* cst = b.contactState + kContactStateWords * static_cast<size_t>(c);
+                const ContactData source = cachedIncident ? ipcCached(cst[kContactSource], cst[kContactSourceWeights])
+                                                          : contactAt(b, c, src, p.ipcActivation);
+                if (!source.valid) {
+                  geomFinite = false;
+                  continue;
+                }
+                uint32_t ctype;
+                const uint4 cq = contactIndices(b, c, &ctype);
+                if (ipcWeightFor(cq, make_float4(1.f, 1.f, 1.f, 1.f), v) == 0.0f) continue;
+                const bool nearMinimum = !(source.distance - dl > p.ipcMinDistance);
+                const bool mayChange = source.distance - dl < p.ipcActivation;
+                const bool friction = p.ipcFriction > 0.0f && cst[kContactLagged].w > 0.0f;
+                ContactData trial = {p.ipcActivation, f3(1, 0, 0), make_float4(0, 0, 0, 0), true};
+                if (nearMinimum || mayChange) trial = contactAt(b, c, src, p.ipcActivation, v, trialPos);
+                if (nearMinimum) {
+                  if (!trial.valid) geomFinite = false;
+                  else if (!(trial.distance > p.ipcMinDistance)) jmin = fminf(jmin, 0.0f);
+                }
+                if (mayChange || friction)
+                  de += contactEnergy(b, p, c, trial, src, v, trialPos) -
+                        contactEnergy(b, p, c, source, src, 0xffffffffu, f3(0, 0, 0));
+              }
             }
             jmin = groupMin<W>(jmin, mask);
             const bool allFinite = __all_sync(mask, geomFinite);
@@ -1101,6 +1435,30 @@ __device__ __forceinline__ void accumulateClothTri(GatePartial& acc, const Cloth
   if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
 }
 
+// An active IPC candidate's barrier and friction energy at the source
+// (source contact cache) and the candidate (target cache, or the source cache
+// when the contact step collapsed to zero): ipcOwnedEnergy (:751-781), which
+// the reference adds to the energy of the candidate's first unpinned vertex,
+// and which becomes kF32Max for an invalid contact.
+__device__ __forceinline__ void accumulateContact(GatePartial& acc, const Buffers& b, const DevParams& p,
+                                                  float contactAlpha, uint32_t c, const float4* __restrict__ src,
+                                                  const float4* __restrict__ tgt) {
+  if (!contactIncluded(b, p, c, src)) return;
+  const float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+  const ContactData ks = ipcCached(st[kContactSource], st[kContactSourceWeights]);
+  const ContactData kc = contactAlpha != 0.0f ? ipcCached(st[kContactTarget], st[kContactTargetWeights]) : ks;
+  const bool friction = p.ipcFriction > 0.0f && st[kContactLagged].w > 0.0f;
+  auto energy = [&](const ContactData& k, const float4* __restrict__ x) {
+    if (!k.valid) return kF32Max;
+    if (!ipcBarrierActive(k.distance, p.ipcActivation) && !friction) return 0.0f;
+    const float e = contactEnergy(b, p, c, k, x, 0xffffffffu, f3(0, 0, 0));
+    return finiteS(e) ? e : kF32Max;
+  };
+  const float es = energy(ks, src), ec = energy(kc, tgt);
+  if (finiteS(es)) acc.e0 += es; else acc.bits &= ~kSourceEnergyValid;
+  if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
+}
+
 // A hinge's bending energy at the source and the candidate (owned by its
 // lowest vertex in the reference, :2623-2642).
 __device__ __forceinline__ void accumulateHinge(GatePartial& acc, const float4* __restrict__ hinges, uint32_t h,
@@ -1222,6 +1580,7 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
       if (k < sr.C) accumulateClothTri(acc, loadClothTri(b.clothTris, sr.cOff + k), src, tgt, clothMaterial(p));
       if (k < sr.H) accumulateHinge(acc, b.clothHinges, sr.hOff + k, src, tgt, p.clothBending);
     }
+    if (p.ipc && k < sr.KC) accumulateContact(acc, b, p, fs->contactAlpha, sr.kOff + k, src, tgt);
   }
   const GatePartial blk = blockFold(acc, smem, gateCombine);
   GatePartial* partials = reinterpret_cast<GatePartial*>(b.gatePartials);
@@ -1334,6 +1693,14 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
       }
       comps[4] = f3(0, 0, 0);
       if (p.floorStiffness > 0.0f && x.y < p.floorHeight) comps[4].y = p.floorStiffness * (x.y - p.floorHeight);
+      if (p.ipc) {
+        // IPC gradient at the accepted pose from the contacts the promotion
+        // pass makes the next source cache (convergenceGradient, :4088).
+        const float alpha = fs->contactAlpha;
+        const int slot = (accepted && finiteS(alpha) && alpha > 0.0f) ? kContactTarget : kContactSource;
+        S3 unused = szero();
+        contactLocal<false>(b, p, v, acc, false, slot, 0u, 1u, comps[4], unused);
+      }
       float3 totalG = f3(0, 0, 0);
       bool tv = true;
 #pragma unroll
@@ -1591,7 +1958,7 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   // One vertex per lane group: the line search makes per-vertex work uneven,
   // and the block scheduler balances it better than a fixed grid stride.
   const uint32_t blocks = std::max(1u, (count + groups - 1) / groups);
-  if (b.clothRange)
+  if (b.clothRange || b.contactIdx)
     solveKernel<kGroup, true><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
                                                                     cachedIncident ? 1 : 0);
   else
@@ -1617,6 +1984,43 @@ uint32_t solveGroupsPerBlock(uint32_t K) {
   uint32_t groups = kBlock / kGroup;
   if (perVertex > 0) groups = std::min<uint32_t>(groups, static_cast<uint32_t>(optin) / perVertex);
   return groups;
+}
+
+int launchContactLag(const Buffers& b, const DevParams* p, cudaStream_t s) {
+  if (b.contactCount == 0) return 0;
+  contactLagKernel<<<blocksFor(b.contactCount), kBlock, 0, s>>>(b, p);
+  return 1;
+}
+
+int launchContactRows(const Buffers& b, const DevParams* p, const float4* src, uint32_t V, cudaStream_t s) {
+  if (b.contactCount == 0) return 0;
+  contactRowsKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, src, V);
+  return 1;
+}
+
+int launchContactStep(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s) {
+  if (b.contactCount == 0) return 0;
+  contactStepKernel<<<blocksFor(b.contactCount), kBlock, 0, s>>>(b, p, src, tgt);
+  return 1;
+}
+
+int launchContactApply(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, uint32_t V,
+                       bool validated, cudaStream_t s) {
+  if (b.contactCount == 0) return 0;
+  contactApplyKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, src, tgt, V, validated ? 1 : 0);
+  return 1;
+}
+
+int launchContactValidate(const Buffers& b, const DevParams* p, const float4* tgt, cudaStream_t s) {
+  if (b.contactCount == 0) return 0;
+  contactValidateKernel<<<blocksFor(b.contactCount), kBlock, 0, s>>>(b, p, tgt);
+  return 1;
+}
+
+int launchContactPromote(const Buffers& b, const DevParams* p, cudaStream_t s) {
+  if (b.contactCount == 0) return 0;
+  contactPromoteKernel<<<blocksFor(b.contactCount), kBlock, 0, s>>>(b, p);
+  return 1;
 }
 
 int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* dst, uint32_t V, cudaStream_t s) {

@@ -28,6 +28,14 @@ struct DevParams {
   uint32_t cloth;           // the scene has cloth triangles
   // Cloth material (the cloth arena's second global vec4, cloth-layout.ts:45-50).
   float clothLambda, clothMu, clothThickness, clothBending;
+  // IPC contact: enabled this frame (candidates, stable path, barrier
+  // stiffness > 0, activation above the minimum distance), the per-step
+  // activation distance and stiffness (the uniform's contact vec4) and the
+  // create-time minimum distance, friction, friction smoothing and step
+  // safety (the contact buffer's parameter vec4, jgs2-solver.ts:1096-1105).
+  uint32_t ipc;
+  float ipcActivation, ipcStiffness, ipcMinDistance, ipcFriction, ipcEpsilon, ipcSafety;
+  uint32_t pad2;
 };
 
 // One scene of a batch: its slices of the concatenated vertex and tet arrays
@@ -38,6 +46,7 @@ struct SceneRange {
   uint32_t gateBase, gateBlocks;  // prologue / gate partials of this scene
   uint32_t convBase, convBlocks;  // convergence partials of this scene
   uint32_t cOff, C, hOff, H;      // cloth triangles and hinges of this scene
+  uint32_t kOff, KC, pad[2];      // IPC candidates of this scene
 };
 
 // One block of a segmented reduction: elements [begin, end) of `scene`,
@@ -61,7 +70,13 @@ struct FrameState {
   uint32_t localFailures, localMaxBacktracks, localSkipped, localEvaluations;
   uint32_t localMaxShift;  // float bits of a non-negative value
   uint32_t localNumericsValid;
-  uint32_t pad[7];
+  // IPC safe-step reductions (reduceContactStep, jgs2-shader.ts:2870-2907):
+  // minimum candidate alpha (float bits) and the all-valid flag of the
+  // safe-step pass and of the validation pass, and the resulting contact
+  // alpha of the iteration.
+  uint32_t stepAlphaBits, stepValid, checkAlphaBits, checkValid;
+  float contactAlpha;
+  uint32_t pad[2];
 };
 
 // All device arrays of one solver.
@@ -108,7 +123,19 @@ struct Buffers {
   const float4* clothHinges;
   const uint4* clothRange;
   const uint32_t* clothIncidence;
-  uint32_t gateBlocks, convBlocks, sceneCount, pad;
+  // IPC contact (all null without candidates): per candidate its global
+  // vertex indices with the type (1 = edge-edge) in bit 31 of the fourth, its
+  // scene and 7 float4 of state (jgs2_contact.cuh); per vertex the range
+  // (first, count) of its incident candidates in `contactIds` and the count
+  // of active ones, listed at the same offsets in `activeIds`.
+  const uint4* contactIdx;
+  const uint32_t* contactScene;
+  float4* contactState;
+  const uint2* contactRange;
+  const uint32_t* contactIds;
+  uint32_t* activeCount;
+  uint32_t* activeIds;
+  uint32_t gateBlocks, convBlocks, sceneCount, contactCount;
 };
 
 // Kernel launch entry points (jgs2_kernels.cu).  `p` points at one DevParams
@@ -129,6 +156,19 @@ int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* 
 int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s);
 int launchConvergence(const Buffers& b, const DevParams* p, const float4* src, float4* tgt,
                       bool computeNextRotations, cudaStream_t s);
+// IPC contact passes (jgs2-shader.ts:2694-2917): lagContact at the frame
+// start; per iteration the active rows before the solve, then the safe-step
+// pass, its application, the validation of the scaled pose, its application
+// (a failure restores the source), and after the convergence pass the
+// promotion of the accepted target contacts.  Each launcher returns the
+// number of kernels launched (0 without candidates).
+int launchContactLag(const Buffers& b, const DevParams* p, cudaStream_t s);
+int launchContactRows(const Buffers& b, const DevParams* p, const float4* src, uint32_t V, cudaStream_t s);
+int launchContactStep(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s);
+int launchContactApply(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, uint32_t V,
+                       bool validated, cudaStream_t s);
+int launchContactValidate(const Buffers& b, const DevParams* p, const float4* tgt, cudaStream_t s);
+int launchContactPromote(const Buffers& b, const DevParams* p, cudaStream_t s);
 // bodyCorrection: some scene of the batch corrects its bodies this frame.
 int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool bodyCorrection,
                    uint32_t bodies, cudaStream_t s);

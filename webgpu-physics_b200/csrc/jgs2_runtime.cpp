@@ -15,6 +15,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -411,7 +412,120 @@ bool validateInput(const jgs2_input* in, std::string* err) {
       return false;
     }
   }
+  // validateIpcContactCandidatesForGpu (ipc-contact-layout.ts:119-176).
+  const uint64_t nc = uint64_t(in->contact_vertex_triangle_count) + in->contact_edge_edge_count;
+  if (nc > 0 && !in->contact_indices) {
+    *err = "IPC contact candidate indices are NULL.";
+    return false;
+  }
+  if (nc >= (1ull << 29)) {
+    *err = "Total IPC candidate count must be below 2^29.";
+    return false;
+  }
+  for (uint64_t c = 0; c < nc; ++c) {
+    const uint32_t* q = &in->contact_indices[4 * c];
+    const char* type = c < in->contact_vertex_triangle_count ? "VT" : "EE";
+    for (int a = 0; a < 4; ++a) {
+      if (q[a] >= V) {
+        *err = format("IPC candidate references vertex %u, but vertexCount is %u.", q[a], V);
+        return false;
+      }
+      for (int b = 0; b < a; ++b)
+        if (q[a] == q[b]) {
+          *err = format("%s candidate %llu must reference four distinct vertices.", type,
+                        static_cast<unsigned long long>(c));
+          return false;
+        }
+    }
+  }
   return true;
+}
+
+// evaluateIpcVertexTriangleDistance / evaluateIpcEdgeEdgeDistance /
+// minimumStaticIpcContactDistance (src/simulation/cpu/ipc-contact.ts:192-385)
+// in double on the f32 input positions.
+double staticContactDistance(const jgs2_input* in) {
+  struct P { double x, y, z; };
+  auto at = [&](uint32_t v) {
+    return P{in->positions[4ull * v], in->positions[4ull * v + 1], in->positions[4ull * v + 2]};
+  };
+  auto sub = [](P a, P b) { return P{a.x - b.x, a.y - b.y, a.z - b.z}; };
+  auto dot = [](P a, P b) { return a.x * b.x + a.y * b.y + a.z * b.z; };
+  auto cross = [](P a, P b) { return P{a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x}; };
+  auto clamp01 = [](double v) { return !(v > 0) ? 0.0 : (v >= 1 ? 1.0 : v); };
+  auto dist = [](P a, P b) {
+    const double d = std::hypot(a.x - b.x, a.y - b.y, a.z - b.z);
+    return std::isfinite(d) ? d : std::numeric_limits<double>::max();
+  };
+  auto lerp = [](P s, P e, double t) { return P{s.x + t * (e.x - s.x), s.y + t * (e.y - s.y), s.z + t * (e.z - s.z)}; };
+  auto segment = [&](P q, P s, P e, double* t) {
+    const P edge = sub(e, s);
+    const double l2 = dot(edge, edge);
+    *t = 0;
+    if (std::isfinite(l2) && l2 > 1e-20) *t = clamp01(dot(sub(q, s), edge) / l2);
+    return dist(q, lerp(s, e, *t));
+  };
+  double minimum = std::numeric_limits<double>::max();
+  const uint64_t nvt = in->contact_vertex_triangle_count;
+  const uint64_t nc = nvt + in->contact_edge_edge_count;
+  for (uint64_t c = 0; c < nc; ++c) {
+    const uint32_t* q = &in->contact_indices[4 * c];
+    const P p0 = at(q[0]), p1 = at(q[1]), p2 = at(q[2]), p3 = at(q[3]);
+    double d;
+    if (c < nvt) {
+      const P e01 = sub(p2, p1), e02 = sub(p3, p1), e12 = sub(p3, p2);
+      const double s01 = dot(e01, e01), s02 = dot(e02, e02), s12 = dot(e12, e12);
+      const double largest = std::max(s01, std::max(s02, s12));
+      const P an = cross(e01, e02);
+      const double a2 = dot(an, an);
+      const double threshold = std::max(1e-40, 1e-6 * largest * largest);
+      d = -1;
+      if (std::isfinite(a2) && a2 > threshold) {
+        const double d01 = dot(e01, e02);
+        const P po = sub(p0, p1);
+        const double d20 = dot(po, e01), d21 = dot(po, e02);
+        const double den = s01 * s02 - d01 * d01;
+        const double b1 = (s02 * d20 - d01 * d21) / den, b2 = (s01 * d21 - d01 * d20) / den;
+        const double b0 = 1 - b1 - b2;
+        if (std::isfinite(b0) && std::isfinite(b1) && std::isfinite(b2) && b0 >= 0 && b1 >= 0 && b2 >= 0) {
+          const P cp{b0 * p1.x + b1 * p2.x + b2 * p3.x, b0 * p1.y + b1 * p2.y + b2 * p3.y,
+                     b0 * p1.z + b1 * p2.z + b2 * p3.z};
+          if (std::isfinite(cp.x) && std::isfinite(cp.y) && std::isfinite(cp.z)) d = dist(p0, cp);
+        }
+      }
+      if (d < 0) {
+        double t;
+        d = segment(p0, p1, p2, &t);
+        d = std::min(d, segment(p0, p2, p3, &t));
+        d = std::min(d, segment(p0, p3, p1, &t));
+      }
+    } else {
+      const P da = sub(p1, p0), db = sub(p3, p2), off = sub(p0, p2);
+      const double la = dot(da, da), lb = dot(db, db);
+      const double degenerate = std::max(1e-20, 1e-6 * std::max(la, lb));
+      const bool aDeg = !(la > degenerate), bDeg = !(lb > degenerate);
+      double pa = 0, pb = 0;
+      if (aDeg && !bDeg) {
+        pb = clamp01(dot(db, off) / lb);
+      } else if (!aDeg) {
+        const double projA = dot(da, off);
+        if (bDeg) {
+          pa = clamp01(-projA / la);
+        } else {
+          const double coupling = dot(da, db), projB = dot(db, off);
+          const double den = la * lb - coupling * coupling;
+          if (den > 1e-6 * la * lb) pa = clamp01((coupling * projB - projA * lb) / den);
+          const double pbu = (coupling * pa + projB) / lb;
+          if (pbu < 0) { pb = 0; pa = clamp01(-projA / la); }
+          else if (pbu > 1) { pb = 1; pa = clamp01((coupling - projA) / la); }
+          else pb = clamp01(pbu);
+        }
+      }
+      d = dist(lerp(p0, p1, pa), lerp(p2, p3, pb));
+    }
+    minimum = std::min(minimum, d);
+  }
+  return minimum;
 }
 
 // buildJGS2InputVertexColoring + buildGreedyVertexColoring.
@@ -446,6 +560,10 @@ std::vector<uint32_t> colorInput(const jgs2_input* in, uint32_t* count) {
   if (in->cloth) {
     for (uint32_t c = 0; c < in->cloth->triangle_count; ++c) group(&in->cloth->triangle_indices[3ull * c], 3);
     for (uint32_t h = 0; h < in->cloth->hinge_count; ++h) group(&in->cloth->hinge_indices[4ull * h], 4);
+  }
+  if (in->contact_indices) {
+    const uint64_t nc = uint64_t(in->contact_vertex_triangle_count) + in->contact_edge_edge_count;
+    for (uint64_t c = 0; c < nc; ++c) group(&in->contact_indices[4 * c], 4);
   }
   std::vector<uint32_t> colors(V, 0xffffffffu), stamp(V + 1, 0);
   uint32_t n = 0, st = 0;
@@ -500,6 +618,9 @@ struct SceneHost {
   uint32_t V = 0, T = 0, K = 0, vOff = 0, tOff = 0, bodyOff = 0, bodies = 1;
   uint32_t C = 0, H = 0, cOff = 0, hOff = 0;  // cloth triangles / hinges and their offsets
   float clothLambda = 0.f, clothMu = 0.f, clothThickness = 0.f, clothBending = 0.f;
+  uint32_t KC = 0, kOff = 0;  // IPC candidates and their offset
+  // IPC parameters fixed at create (jgs2-solver.ts:1096-1105).
+  float ipcMinDistance = 0.f, ipcFriction = 0.f, ipcEpsilon = 0.f, ipcSafety = 0.f;
   float sceneScale = 1.f;
   float preprocessingTimestep = 0.f;
   jgs2_settings defaults{};
@@ -521,6 +642,7 @@ struct Engine {
   std::string error;
   uint32_t V = 0, T = 0, K = 0, bodies = 1;  // totals over the scenes; K = widest record count
   uint32_t C = 0, H = 0;                     // cloth triangles and hinges over the scenes
+  uint32_t KC = 0;                           // IPC candidates over the scenes
   bool glob = true;
   std::vector<SceneHost> scenes;
   // Colour lists over all scenes: colour c holds every scene's colour-c vertices.
@@ -543,8 +665,8 @@ struct Engine {
   uint32_t* dNeedVertices = nullptr;
   std::vector<void*> allocations;
   uint64_t launches = 0;
-  // graphs: (iterations, schedule, bodyCorrection) -> exec, launches per replay
-  std::map<std::tuple<uint32_t, uint32_t, bool>, std::pair<cudaGraphExec_t, int>> graphs;
+  // graphs: (iterations, schedule, bodyCorrection, contact) -> exec, launches per replay
+  std::map<std::tuple<uint32_t, uint32_t, bool, bool>, std::pair<cudaGraphExec_t, int>> graphs;
   bool useGraphs = true;
 };
 
@@ -665,14 +787,25 @@ DevParams makeParams(const Engine* s, uint32_t scene, const jgs2_settings& st, b
   p.clothMu = sc.clothMu;
   p.clothThickness = sc.clothThickness;
   p.clothBending = sc.clothBending;
+  // contactEnabled (jgs2-solver.ts:2213-2214) and ipcEnabled
+  // (jgs2-shader.ts:458-464).
+  p.ipcActivation = st.ipc_activation_distance;
+  p.ipcStiffness = st.ipc_barrier_stiffness;
+  p.ipcMinDistance = sc.ipcMinDistance;
+  p.ipcFriction = sc.ipcFriction;
+  p.ipcEpsilon = sc.ipcEpsilon;
+  p.ipcSafety = sc.ipcSafety;
+  p.ipc = (s->glob && sc.KC > 0 && st.ipc_barrier_stiffness > 0 && st.ipc_activation_distance > sc.ipcMinDistance)
+              ? 1u : 0u;
   return p;
 }
 
 // Optional per-kernel CUDA event timing of an encoded frame.
 struct KernelProfiler {
-  static constexpr const char* kNames[JGS2_PROFILE_KINDS] = {"prologue", "vertex_frames", "tet_frames", "solve",
-                                                              "gate", "convergence", "copy", "epilogue"};
-  enum Kind { kPrologue = 0, kVertexFrames, kTetFrames, kSolve, kGate, kConvergence, kCopy, kEpilogue };
+  static constexpr const char* kNames[JGS2_PROFILE_KINDS] = {"prologue", "vertex_frames", "tet_frames",
+                                                              "solve",    "gate",          "convergence",
+                                                              "copy",     "epilogue",      "contact"};
+  enum Kind { kPrologue = 0, kVertexFrames, kTetFrames, kSolve, kGate, kConvergence, kCopy, kEpilogue, kContact };
   std::vector<std::pair<cudaEvent_t, cudaEvent_t>> pool;
   std::vector<int> kinds;
   size_t used = 0;
@@ -696,8 +829,9 @@ struct KernelProfiler {
 };
 
 // encodeFrame (src/simulation/gpu/jgs2-solver.ts:2207-2494) on the stream,
-// for every scene of the engine at once.
-int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorrection,
+// for every scene of the engine at once.  contact: some scene has IPC
+// contact this frame.
+int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorrection, bool contact,
                 KernelProfiler* prof = nullptr) {
   const Buffers& b = s->b;
   cudaStream_t st = s->stream;
@@ -743,10 +877,12 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
                [&] { return jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, bodyCorrection, s->bodies, st); });
     return n;
   }
+  if (contact) n += timed(P::kContact, [&] { return jgs2::launchContactLag(b, s->dParams, st); });
   for (uint32_t it = 0; it < iterations; ++it) {
     float4* src = (it % 2 == 0) ? b.pos[1] : b.pos[0];
     float4* tgt = (it % 2 == 0) ? b.pos[0] : b.pos[1];
     const bool last = it + 1 == iterations;
+    if (contact) n += timed(P::kContact, [&] { return jgs2::launchContactRows(b, s->dParams, src, s->V, st); });
     if (colored) {
       n += timed(P::kCopy, [&] { return jgs2::launchCopy(b, s->dParams, src, tgt, s->V, st); });
       for (uint32_t c = 0; c < s->colorCount; ++c) {
@@ -767,9 +903,21 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
       // convergence pass leave the source pose's incident system in b.incident.
       n += timed(P::kSolve, [&] { return jgs2::launchSolve(b, s->dParams, src, tgt, nullptr, s->V, s->K, true, st); });
     }
+    if (contact) {
+      // Safe-step scaling, exact validation of the scaled pose (a failure
+      // restores the source), before the assembled gate (jgs2-solver.ts:2340-2393).
+      n += timed(P::kContact, [&] {
+        int k = jgs2::launchContactStep(b, s->dParams, src, tgt, st);
+        k += jgs2::launchContactApply(b, s->dParams, src, tgt, s->V, false, st);
+        k += jgs2::launchContactValidate(b, s->dParams, tgt, st);
+        k += jgs2::launchContactApply(b, s->dParams, src, tgt, s->V, true, st);
+        return k;
+      });
+    }
     n += timed(P::kGate, [&] { return jgs2::launchGate(b, s->dParams, src, tgt, st); });
     n += timed(P::kConvergence,
                [&] { return jgs2::launchConvergence(b, s->dParams, src, tgt, !colored && !last, st); });
+    if (contact) n += timed(P::kContact, [&] { return jgs2::launchContactPromote(b, s->dParams, st); });
   }
   const float4* finalPos = (iterations % 2 == 0) ? b.pos[1] : b.pos[0];
   n += timed(P::kEpilogue,
@@ -802,17 +950,21 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
                 format("Stable JGS2 may encode at most %u total nonlinear iterations per submission; got %u "
                        "frames * %u iterations.",
                        JGS2_MAX_GLOBALIZED_ITERATIONS_PER_SUBMISSION, frames, iterations * sub));
-  for (uint32_t i = 0; i < s->scenes.size(); ++i) s->hParams[i] = makeParams(s, i, st[i], stop);
+  bool contact = false;
+  for (uint32_t i = 0; i < s->scenes.size(); ++i) {
+    s->hParams[i] = makeParams(s, i, st[i], stop);
+    contact = contact || s->hParams[i].ipc != 0;
+  }
   CUDA_TRY(s, cudaSetDevice(s->device));
   CUDA_TRY(s, cudaMemcpyAsync(s->dParams, s->hParams.data(), sizeof(DevParams) * s->hParams.size(),
                               cudaMemcpyHostToDevice, s->stream));
-  const auto key = std::make_tuple(iterations, schedule, body);
+  const auto key = std::make_tuple(iterations, schedule, body, contact);
   if (s->useGraphs && !prof) {
     auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
       cudaGraph_t graph = nullptr;
       CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
-      const int n = encodeFrame(s, iterations, schedule, body);
+      const int n = encodeFrame(s, iterations, schedule, body, contact);
       cudaError_t e = cudaStreamEndCapture(s->stream, &graph);
       if (e != cudaSuccess) return cudaFail(s, e, "cudaStreamEndCapture");
       cudaGraphExec_t exec = nullptr;
@@ -826,7 +978,7 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
       s->launches += static_cast<uint64_t>(it->second.second);
     }
   } else {
-    for (uint32_t f = 0; f < frames; ++f) s->launches += encodeFrame(s, iterations, schedule, body, prof);
+    for (uint32_t f = 0; f < frames; ++f) s->launches += encodeFrame(s, iterations, schedule, body, contact, prof);
   }
   CUDA_TRY(s, cudaGetLastError());
   for (uint32_t i = 0; i < s->scenes.size(); ++i) {
@@ -856,9 +1008,16 @@ jgs2_status resolveStep(Engine* s, uint32_t scene, const jgs2_settings* o, uint3
                 format("JGS2 was precomputed for timestep %g, but the step requested %g. Regenerate the "
                        "precomputation before changing timestep.",
                        sc.preprocessingTimestep, o->timestep));
+  if (sc.KC > 0 && o && (mask & JGS2_SET_IPC_MINIMUM_DISTANCE) && o->ipc_minimum_distance != sc.ipcMinDistance)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                "ipcMinimumDistance is fixed when an IPC solver is created; recreate the solver before changing it.");
   std::string err;
   if (!resolve(sc.defaults, o, mask, out, &err)) return fail(s, JGS2_INVALID_ARGUMENT, err);
-  if (s->glob && sc.objectiveFlags != 0 && out->horizontal_body_correction) out->horizontal_body_correction = 0;
+  // Objectives and mesh contacts are not translation invariant per body, so
+  // they keep their solved centre-of-mass motion (jgs2-solver.ts:1999-2009).
+  if (s->glob && (sc.objectiveFlags != 0 || (sc.KC > 0 && out->ipc_barrier_stiffness > 0)) &&
+      out->horizontal_body_correction)
+    out->horizontal_body_correction = 0;
   return JGS2_OK;
 }
 
@@ -940,6 +1099,10 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
   out->stable = stable == in->tet_count;
   if (in->cloth && in->cloth->triangle_count > 0 && !out->stable)
     return fail(nullptr, JGS2_INVALID_ARGUMENT, "Triangle cloth requires the stable Neo-Hookean production path.");
+  const uint64_t contacts = uint64_t(in->contact_vertex_triangle_count) + in->contact_edge_edge_count;
+  if (contacts > 0 && !out->stable)
+    return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                "IPC contact candidates require the stable Neo-Hookean production path.");
   out->colored = colour;
   if (colour) out->colors = colorInput(in, &out->colorCount);
   if (out->colorCount > JGS2_MAX_SCHEDULE_COLORS)
@@ -949,6 +1112,18 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
   jgs2_settings base;
   defaults(&base);
   if (!resolve(base, settings, mask, &out->resolved, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  if (contacts > 0) {
+    // The source pose must clear the minimum distance by an f32 rounding
+    // margin (jgs2-solver.ts:1040-1070).
+    const double minimum = staticContactDistance(in);
+    const double margin = 8.0 * std::ldexp(1.0, -24) *
+                          std::max(1.0, std::max(double(out->resolved.ipc_activation_distance), std::fabs(minimum)));
+    const double required = double(out->resolved.ipc_minimum_distance) + margin;
+    if (!std::isfinite(minimum) || !(minimum > required))
+      return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                  format("IPC candidates require an initially feasible source pose with distance greater than %g "
+                         "(minimum plus an f32 safety margin); got %g.", required, minimum));
+  }
   const double m = out->stable ? minimumInputDeterminant(in) : 1.0;
   if (!std::isfinite(m) || !(m > kDeterminantFloor))
     return fail(nullptr, JGS2_INFEASIBLE_INPUT,
@@ -987,7 +1162,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       return fail(nullptr, JGS2_INVALID_ARGUMENT,
                   "A batch cannot mix stable Neo-Hookean scenes with co-rotated linear scenes.");
   sp->scenes.resize(S);
-  uint64_t V = 0, T = 0, bodies = 0, C = 0, H = 0;
+  uint64_t V = 0, T = 0, bodies = 0, C = 0, H = 0, KC = 0;
   uint32_t K = 0, colorCount = 1;
   for (uint32_t i = 0; i < S; ++i) {
     const jgs2_input* in = prep[i].in;
@@ -1013,6 +1188,13 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       C += sc.C;
       H += sc.H;
     }
+    sc.kOff = static_cast<uint32_t>(KC);
+    sc.KC = in->contact_indices ? in->contact_vertex_triangle_count + in->contact_edge_edge_count : 0u;
+    sc.ipcMinDistance = prep[i].resolved.ipc_minimum_distance;
+    sc.ipcFriction = prep[i].resolved.ipc_friction_coefficient;
+    sc.ipcEpsilon = prep[i].resolved.ipc_friction_velocity_epsilon;
+    sc.ipcSafety = prep[i].resolved.ipc_step_safety;
+    KC += sc.KC;
     uint32_t maxBody = 0;
     for (uint32_t v = 0; v < sc.V; ++v) maxBody = std::max(maxBody, in->vertex_info[4ull * v + 3]);
     sc.bodies = maxBody + 1;
@@ -1028,12 +1210,14 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     K = std::max(K, sc.K);
     colorCount = std::max(colorCount, sc.colorCount);
   }
-  if (V > 0xffffffffull / 16 || T > 0xffffffffull / 16 || C > 0xffffffffull / 16 || H > 0xffffffffull / 16)
+  if (V > 0xffffffffull / 16 || T > 0xffffffffull / 16 || C > 0xffffffffull / 16 || H > 0xffffffffull / 16 ||
+      KC > 0xffffffffull / 16)
     return fail(nullptr, JGS2_INVALID_ARGUMENT, "The scenes together exceed the engine's index range.");
   sp->V = static_cast<uint32_t>(V);
   sp->T = static_cast<uint32_t>(T);
   sp->C = static_cast<uint32_t>(C);
   sp->H = static_cast<uint32_t>(H);
+  sp->KC = static_cast<uint32_t>(KC);
   sp->K = K;
   sp->bodies = static_cast<uint32_t>(bodies);
   sp->coloringBuilt = true;
@@ -1229,6 +1413,35 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       for (uint32_t l = 0; l < 4; ++l)
         incidence[hingeBase + cursor[cl->hinge_indices[4ull * h + l]]++] = (sc.hOff + h) * 4u + l;
   });
+  // IPC candidates (packIpcContactBuffer and packIpcIncidentCandidateAdjacency,
+  // ipc-contact-layout.ts:190-342, in this engine's layout): global vertex
+  // indices with the edge-edge type in bit 31 of the fourth, the scene of each
+  // candidate, and per vertex its incident candidates in ascending order.
+  const uint32_t nK = sp->KC;
+  std::vector<uint4> contactIdx(nK);
+  std::vector<uint32_t> contactScene(nK);
+  std::vector<uint2> contactRange(nK ? nV : 0, make_uint2(0u, 0u));
+  std::vector<uint32_t> contactIds(4ull * nK);
+  if (nK) parallelFor(S, [&](uint32_t i) {
+    const jgs2_input* in = prep[i].in;
+    const SceneHost& sc = sp->scenes[i];
+    if (sc.KC == 0) return;
+    const uint32_t nvt = in->contact_vertex_triangle_count;
+    std::vector<uint32_t> rows(sc.V + 1, 0);
+    for (uint32_t c = 0; c < sc.KC; ++c) {
+      const uint32_t* q = &in->contact_indices[4ull * c];
+      contactIdx[sc.kOff + c] = make_uint4(sc.vOff + q[0], sc.vOff + q[1], sc.vOff + q[2],
+                                           (sc.vOff + q[3]) | (c < nvt ? 0u : 0x80000000u));
+      contactScene[sc.kOff + c] = i;
+      for (int l = 0; l < 4; ++l) rows[q[l] + 1]++;
+    }
+    for (uint32_t v = 0; v < sc.V; ++v) rows[v + 1] += rows[v];
+    const uint32_t base = 4u * sc.kOff;
+    for (uint32_t v = 0; v < sc.V; ++v) contactRange[sc.vOff + v] = make_uint2(base + rows[v], rows[v + 1] - rows[v]);
+    std::vector<uint32_t> cursor(rows.begin(), rows.end() - 1);
+    for (uint32_t c = 0; c < sc.KC; ++c)
+      for (int l = 0; l < 4; ++l) contactIds[base + cursor[in->contact_indices[4ull * c + l]]++] = sc.kOff + c;
+  });
   // Segmented reduction tables: each scene's elements in fixed chunks.
   std::vector<jgs2::SceneRange> ranges(S);
   std::vector<jgs2::RedBlock> gateTable, convTable;
@@ -1237,7 +1450,8 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     jgs2::SceneRange& r = ranges[i];
     r.vOff = sc.vOff; r.V = sc.V; r.tOff = sc.tOff; r.T = sc.T;
     r.cOff = sc.cOff; r.C = sc.C; r.hOff = sc.hOff; r.H = sc.H;
-    const uint32_t n = std::max(std::max(sc.V, sc.T), std::max(sc.C, sc.H));
+    r.kOff = sc.kOff; r.KC = sc.KC;
+    const uint32_t n = std::max(std::max(std::max(sc.V, sc.T), std::max(sc.C, sc.H)), sc.KC);
     r.gateBase = static_cast<uint32_t>(gateTable.size());
     for (uint32_t b0 = 0; b0 < std::max(n, 1u); b0 += jgs2::kGateChunk)
       gateTable.push_back({i, b0, std::min(n, b0 + jgs2::kGateChunk), static_cast<uint32_t>(gateTable.size())});
@@ -1358,6 +1572,40 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       b.clothRange = cr;
       b.clothIncidence = ci;
     }
+    b.contactIdx = nullptr;
+    b.contactScene = nullptr;
+    b.contactState = nullptr;
+    b.contactRange = nullptr;
+    b.contactIds = nullptr;
+    b.activeCount = nullptr;
+    b.activeIds = nullptr;
+    b.contactCount = nK;
+    if (nK) {
+      uint4* ki = nullptr;
+      uint32_t* ks = nullptr;
+      uint2* kr = nullptr;
+      uint32_t* kd = nullptr;
+      STEP(upload(sp, &ki, contactIdx.data(), nK));
+      STEP(upload(sp, &ks, contactScene.data(), nK));
+      STEP(upload(sp, &kr, contactRange.data(), nV));
+      STEP(upload(sp, &kd, contactIds.data(), contactIds.size()));
+      // Empty contact caches (distance -1), zero lagged records, neutral
+      // scratch (packIpcContactBuffer, ipc-contact-layout.ts:290-340).
+      std::vector<float4> state(7ull * nK, make_float4(0.f, 0.f, 0.f, 0.f));
+      for (size_t c = 0; c < nK; ++c) {
+        state[7 * c + 0] = make_float4(0.f, 0.f, 0.f, -1.f);
+        state[7 * c + 2] = make_float4(0.f, 0.f, 0.f, -1.f);
+        state[7 * c + 6] = make_float4(1.f, 0.f, 0.f, 0.f);
+      }
+      STEP(upload(sp, &b.contactState, state.data(), state.size()));
+      STEP(deviceAlloc(sp, &b.activeCount, nV));
+      STEP(deviceAlloc(sp, &b.activeIds, contactIds.size()));
+      CUDA_TRY(sp, cudaMemsetAsync(b.activeCount, 0, sizeof(uint32_t) * nV, sp->stream));
+      b.contactIdx = ki;
+      b.contactScene = ks;
+      b.contactRange = kr;
+      b.contactIds = kd;
+    }
     STEP(upload(sp, &sp->dColorVertices, byColor.data(), byColor.size()));
     STEP(upload(sp, &sp->dNeedVertices, need.data(), need.size()));
     STEP(deviceAlloc(sp, &sp->dParams, S));
@@ -1471,6 +1719,7 @@ jgs2_status sceneInfo(Engine* s, uint32_t scene, jgs2_info* out) {
   out->preprocessing_timestep = sc.preprocessingTimestep;
   out->current_position_buffer = 0;
   out->cloth_triangle_count = sc.C;
+  out->contact_candidate_count = sc.KC;
   if (sc.recordsAvailable) {
     float4 c1;
     if (readRegion(s, &s->b.frames[scene].control[1], sizeof(c1), &c1) == JGS2_OK)
@@ -1871,6 +2120,10 @@ jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* s, const float* source, co
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
   if (!s->glob) return fail(s, JGS2_UNSUPPORTED, "The assembled gate requires stable globalization.");
+  if (s->KC > 0)
+    return fail(s, JGS2_UNSUPPORTED,
+                "The no-allocation gate does not evaluate IPC contact energies; use "
+                "jgs2_evaluate_assembled_candidate for solvers with contact candidates.");
   if (!source || !candidate || !predicted || !control)
     return fail(s, JGS2_INVALID_ARGUMENT, "The no-allocation gate's device arrays must not be NULL.");
   for (const void* p : {static_cast<const void*>(source), static_cast<const void*>(candidate),
@@ -2078,7 +2331,11 @@ uint64_t jgs2_estimate_device_bytes(const jgs2_input* in) {
   // 16-byte incidence range per vertex.
   const uint64_t C = in->cloth ? in->cloth->triangle_count : 0, H = in->cloth ? in->cloth->hinge_count : 0;
   const uint64_t cloth = (C + H) ? V * 16 + C * (32 + 12) + H * (32 + 16) : 0;
-  return V * (16 * 20 + 12) + V * K * (32 + 144) + T * (64 + 16 + 1) + cloth + (1u << 16);
+  // IPC: per candidate its indices, scene, 7 float4 of state and four
+  // incidence and four active entries; per vertex a range and an active count.
+  const uint64_t KC = uint64_t(in->contact_vertex_triangle_count) + in->contact_edge_edge_count;
+  const uint64_t contact = KC ? KC * (16 + 4 + 112 + 32) + V * 12 : 0;
+  return V * (16 * 20 + 12) + V * K * (32 + 144) + T * (64 + 16 + 1) + cloth + contact + (1u << 16);
 }
 
 }  // extern "C"

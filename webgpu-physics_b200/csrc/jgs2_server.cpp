@@ -34,7 +34,7 @@ struct OwnedInput {
   std::vector<float> cubW, cubBasis;
   std::vector<uint32_t> info, tets, adjacency, cubTet;
   jgs2_cloth_input cloth{};
-  std::vector<uint32_t> clothTris, hinges;
+  std::vector<uint32_t> clothTris, hinges, contacts;
   std::vector<float> clothInv, clothAreas, hingeAngles, hingeLengths;
 
   template <class T>
@@ -75,6 +75,8 @@ struct OwnedInput {
       cloth.hinge_rest_edge_lengths = take(hingeLengths, c.hinge_rest_edge_lengths, H);
       view.cloth = &cloth;
     }
+    view.contact_indices = take(contacts, in.contact_indices,
+                                4 * (size_t(in.contact_vertex_triangle_count) + in.contact_edge_edge_count));
   }
 };
 

@@ -340,6 +340,86 @@ bool clothHingeRest(const double* x0, const double* x1, const double* x2, const 
   return true;
 }
 
+// extractBoundarySurface (src/simulation/cpu/mesh.ts:364-420): the faces that
+// belong to exactly one tetrahedron, each as its sorted vertex triple (the
+// candidate enumeration below only needs the vertex sets).
+bool boundaryTriangles(const Mesh& m, std::vector<std::array<uint32_t, 3>>* out, std::string* err) {
+  std::unordered_map<uint64_t, std::pair<std::array<uint32_t, 3>, int>> faces;
+  faces.reserve(m.tets.size());
+  for (size_t t = 0; t < m.tets.size() / 4; ++t) {
+    const uint32_t* q = &m.tets[4 * t];
+    const uint32_t local[4][3] = {{q[1], q[2], q[3]}, {q[0], q[3], q[2]}, {q[0], q[1], q[3]}, {q[0], q[2], q[1]}};
+    for (const auto& f : local) {
+      std::array<uint32_t, 3> s = {f[0], f[1], f[2]};
+      std::sort(s.begin(), s.end());
+      // 21 bits per index is enough for the contact scenes (the enumeration
+      // is quadratic); larger meshes are rejected.
+      if (s[2] >= (1u << 21)) {
+        *err = "Contact candidate enumeration takes meshes below 2^21 vertices.";
+        return false;
+      }
+      const uint64_t key = (static_cast<uint64_t>(s[0]) << 42) | (static_cast<uint64_t>(s[1]) << 21) | s[2];
+      auto it = faces.find(key);
+      if (it == faces.end()) {
+        faces.emplace(key, std::make_pair(s, 1));
+      } else if (++it->second.second > 2) {
+        *err = "Non-manifold face belongs to over two tets.";
+        return false;
+      }
+    }
+  }
+  for (const auto& kv : faces)
+    if (kv.second.second == 1) out->push_back(kv.second.first);
+  return true;
+}
+
+// buildStaticIpcContactCandidates (src/simulation/cpu/ipc-contact.ts:591-665):
+// canonical (sorted, deduplicated) surface triangles and edges; every vertex
+// paired with every triangle none of whose vertices is in the vertex's closed
+// surface one-ring, then every edge pair (lexicographic order, i < j) whose
+// vertices are pairwise outside each other's closed one-rings.  Four indices
+// per candidate, vertex-triangle candidates first.
+void staticContactCandidates(uint32_t V, std::vector<std::array<uint32_t, 3>> triangles, std::vector<uint32_t>* out,
+                             uint32_t* vtCount, uint32_t* eeCount) {
+  std::sort(triangles.begin(), triangles.end());
+  triangles.erase(std::unique(triangles.begin(), triangles.end()), triangles.end());
+  std::vector<std::array<uint32_t, 2>> edges;
+  for (const auto& t : triangles) {
+    const uint32_t pairs[3][2] = {{t[0], t[1]}, {t[1], t[2]}, {t[2], t[0]}};
+    for (const auto& p : pairs) edges.push_back({std::min(p[0], p[1]), std::max(p[0], p[1])});
+  }
+  std::sort(edges.begin(), edges.end());
+  edges.erase(std::unique(edges.begin(), edges.end()), edges.end());
+  std::vector<std::vector<uint32_t>> ring(V);
+  for (const auto& e : edges) {
+    ring[e[0]].push_back(e[1]);
+    ring[e[1]].push_back(e[0]);
+  }
+  for (auto& r : ring) std::sort(r.begin(), r.end());
+  auto closed = [&](uint32_t a, uint32_t b) {
+    return a == b || std::binary_search(ring[a].begin(), ring[a].end(), b);
+  };
+  out->clear();
+  uint32_t vt = 0;
+  for (uint32_t v = 0; v < V; ++v)
+    for (const auto& t : triangles) {
+      if (closed(v, t[0]) || closed(v, t[1]) || closed(v, t[2])) continue;
+      out->insert(out->end(), {v, t[0], t[1], t[2]});
+      vt++;
+    }
+  uint32_t ee = 0;
+  for (size_t i = 0; i < edges.size(); ++i)
+    for (size_t j = i + 1; j < edges.size(); ++j) {
+      const auto& a = edges[i];
+      const auto& b = edges[j];
+      if (closed(a[0], b[0]) || closed(a[0], b[1]) || closed(a[1], b[0]) || closed(a[1], b[1])) continue;
+      out->insert(out->end(), {a[0], a[1], b[0], b[1]});
+      ee++;
+    }
+  *vtCount = vt;
+  *eeCount = ee;
+}
+
 // Hinges of buildJGS2GpuClothInput (src/scenes/index.ts:893-933): every
 // interior edge shared by two consistently oriented triangles gives one
 // hinge (first, second, opposite of the first triangle, opposite of the
@@ -562,6 +642,46 @@ int64_t jgs2_scene_add_cloth(jgs2_scene* s, uint32_t vertex_count, const double*
   return static_cast<int64_t>(base);
 }
 
+jgs2_status jgs2_scene_set_rest_positions(jgs2_scene* s, const double* positions) {
+  if (!s || !positions) return JGS2_INVALID_ARGUMENT;
+  const size_t n = 3ull * s->mesh.vertexCount();
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(positions[i])) return fail(s, "Rest positions must be finite."), JGS2_INVALID_ARGUMENT;
+  std::vector<double> pos(positions, positions + n);
+  std::vector<uint32_t> tets = s->mesh.tets;
+  std::string err;
+  // transformTetrahedralMesh re-orients the tetrahedra (mesh.ts:272-273).
+  if (!orientTets(pos, tets.data(), tets.size() / 4, &err)) return fail(s, err), JGS2_INVALID_ARGUMENT;
+  s->mesh.positions = std::move(pos);
+  s->mesh.tets = std::move(tets);
+  invalidate(*s);
+  return JGS2_OK;
+}
+
+int64_t jgs2_build_static_contact_candidates(uint32_t vertex_count, const uint32_t* triangles,
+                                             uint32_t triangle_count, uint32_t* out, uint64_t capacity,
+                                             uint32_t* vertex_triangle_count, uint32_t* edge_edge_count) {
+  if ((!triangles && triangle_count) || !vertex_triangle_count || !edge_edge_count) return -1;
+  std::vector<std::array<uint32_t, 3>> tri(triangle_count);
+  for (uint32_t t = 0; t < triangle_count; ++t) {
+    std::array<uint32_t, 3> s = {triangles[3ull * t], triangles[3ull * t + 1], triangles[3ull * t + 2]};
+    std::sort(s.begin(), s.end());
+    if (s[2] >= vertex_count || s[0] == s[1] || s[1] == s[2]) return -1;
+    tri[t] = s;
+  }
+  std::vector<uint32_t> packed;
+  staticContactCandidates(vertex_count, std::move(tri), &packed, vertex_triangle_count, edge_edge_count);
+  const uint64_t n = packed.size() / 4;
+  if (out && capacity >= n) std::memcpy(out, packed.data(), packed.size() * sizeof(uint32_t));
+  return static_cast<int64_t>(n);
+}
+
+jgs2_status jgs2_scene_set_contact(jgs2_scene* s, uint32_t enabled) {
+  if (!s) return JGS2_INVALID_ARGUMENT;
+  s->contact = enabled != 0;
+  return JGS2_OK;
+}
+
 uint32_t jgs2_scene_cloth_triangle_count(const jgs2_scene* s) {
   return s ? static_cast<uint32_t>(s->cloth.triangles.size() / 3) : 0;
 }
@@ -755,8 +875,28 @@ jgs2_status jgs2_scene_pack(jgs2_scene* s, jgs2_input* out) {
     ci.thickness = static_cast<float>(s->cloth.thickness);
     ci.bending_stiffness = static_cast<float>(s->cloth.bending);
   }
+  // Static IPC candidates over the tet boundary and the cloth triangles
+  // (surfaceWithCloth, precompute.ts:98-140; buildStaticIpcContactCandidates).
+  s->packContact.clear();
+  s->packContactVT = s->packContactEE = 0;
+  if (s->contact) {
+    std::vector<std::array<uint32_t, 3>> surface;
+    std::string err;
+    if (!boundaryTriangles(m, &surface, &err)) return fail(s, err), JGS2_INVALID_ARGUMENT;
+    if (cloth)
+      for (size_t c = 0; c < s->cloth.triangles.size() / 3; ++c) {
+        std::array<uint32_t, 3> t = {s->cloth.triangles[3 * c], s->cloth.triangles[3 * c + 1],
+                                     s->cloth.triangles[3 * c + 2]};
+        std::sort(t.begin(), t.end());
+        surface.push_back(t);
+      }
+    staticContactCandidates(V, std::move(surface), &s->packContact, &s->packContactVT, &s->packContactEE);
+  }
   std::memset(out, 0, sizeof(*out));
   out->cloth = cloth ? &s->packCloth : nullptr;
+  out->contact_indices = s->packContact.empty() ? nullptr : s->packContact.data();
+  out->contact_vertex_triangle_count = s->packContactVT;
+  out->contact_edge_edge_count = s->packContactEE;
   out->vertex_count = V;
   out->tet_count = T;
   out->cubature_k = K;

@@ -81,6 +81,10 @@ struct Scene {
   std::vector<uint32_t> packClothTriangles, packHinges;
   std::vector<float> packClothInverse, packClothAreas, packHingeAngles, packHingeLengths;
   jgs2_cloth_input packCloth{};
+  // Static IPC candidates over the boundary surface (tets) and the cloth.
+  bool contact = false;
+  std::vector<uint32_t> packContact;
+  uint32_t packContactVT = 0, packContactEE = 0;
 };
 
 // ---- small dense helpers (row-major 3x3) ---------------------------------

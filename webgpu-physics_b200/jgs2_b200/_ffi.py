@@ -59,6 +59,9 @@ class Input(Structure):
         ("cubature_weights", POINTER(c_float)),
         ("cubature_basis", POINTER(c_float)),
         ("cloth", POINTER(ClothInput)),
+        ("contact_indices", POINTER(c_uint32)),
+        ("contact_vertex_triangle_count", c_uint32),
+        ("contact_edge_edge_count", c_uint32),
     ]
 
 
@@ -96,10 +99,11 @@ class Info(Structure):
         ("last_submitted_iterations", c_uint32), ("history_count", c_uint32),
         ("scene_scale", c_float), ("preprocessing_timestep", c_float),
         ("current_position_buffer", c_uint32), ("cloth_triangle_count", c_uint32),
+        ("contact_candidate_count", c_uint32), ("reserved1", c_uint32),
     ]
 
 
-PROFILE_KINDS = 8
+PROFILE_KINDS = 9
 
 
 class KernelProfile(Structure):
@@ -189,6 +193,12 @@ def scene_lib() -> ctypes.CDLL:
         lib.jgs2_scene_add_cloth.restype = c_int64
         lib.jgs2_scene_cloth_triangle_count.argtypes = [c_void_p]
         lib.jgs2_scene_cloth_triangle_count.restype = c_uint32
+        lib.jgs2_scene_set_rest_positions.argtypes = [c_void_p, POINTER(c_double)]
+        lib.jgs2_scene_set_contact.argtypes = [c_void_p, c_uint32]
+        lib.jgs2_build_static_contact_candidates.argtypes = [c_uint32, POINTER(c_uint32), c_uint32,
+                                                             POINTER(c_uint32), c_uint64, POINTER(c_uint32),
+                                                             POINTER(c_uint32)]
+        lib.jgs2_build_static_contact_candidates.restype = c_int64
         lib.jgs2_scene_set_pinned.argtypes = [c_void_p, POINTER(c_uint8)]
         lib.jgs2_scene_vertex_count.argtypes = [c_void_p]
         lib.jgs2_scene_vertex_count.restype = c_uint32

@@ -57,7 +57,8 @@ def build_step_library(force=False, verbose=False) -> str:
     os.makedirs(LIB, exist_ok=True)
     target = os.path.join(LIB, "libjgs2.so")
     sources = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cu", "jgs2_runtime.cpp", "jgs2_server.cpp")]
-    headers = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cuh", "jgs2_device.cuh", "jgs2_cloth.cuh")] + [
+    headers = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cuh", "jgs2_device.cuh", "jgs2_cloth.cuh",
+                                                "jgs2_contact.cuh")] + [
         os.path.join(INCLUDE, f) for f in ("jgs2.h", "jgs2_server.h")]
     if not force and not _stale(target, sources + headers):
         return target

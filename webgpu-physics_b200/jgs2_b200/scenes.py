@@ -78,7 +78,15 @@ class SceneInput:
     hinge_rest_angles: Optional[np.ndarray] = None     # float32
     hinge_rest_edge_lengths: Optional[np.ndarray] = None  # float32
     cloth_material: Optional[np.ndarray] = None        # float32 (E, nu, thickness, bending)
+    # Static IPC contact candidates: 4 indices each, vertex-triangle first,
+    # and their counts (vertex-triangle, edge-edge).
+    contact_indices: Optional[np.ndarray] = None       # uint32
+    contact_counts: Optional[np.ndarray] = None        # uint32 (vt, ee)
     stats: Optional[dict] = None
+
+    @property
+    def contact_candidate_count(self) -> int:
+        return 0 if self.contact_counts is None else int(self.contact_counts.sum())
 
     @property
     def cloth_triangle_count(self) -> int:
@@ -131,6 +139,10 @@ class SceneInput:
         cloth = self.cloth_ctypes()
         if cloth is not None:
             rec.cloth = ctypes.pointer(cloth)
+        if self.contact_counts is not None and self.contact_candidate_count > 0:
+            rec.contact_indices = _ffi.uptr(self.contact_indices)
+            rec.contact_vertex_triangle_count = int(self.contact_counts[0])
+            rec.contact_edge_edge_count = int(self.contact_counts[1])
         # Keep the arrays (and the cloth record) alive as long as the record.
         rec._owner = (self, cloth)  # type: ignore[attr-defined]
         return rec
@@ -284,6 +296,17 @@ class Scene:
             raise ValueError(self._error())
         return base
 
+    def set_rest_positions(self, positions):
+        pos = np.ascontiguousarray(positions, dtype=np.float64).reshape(-1)
+        if pos.size != 3 * self.vertex_count:
+            raise ValueError("positions must hold 3 values per vertex")
+        status = self._lib.jgs2_scene_set_rest_positions(self._h, _ffi.dptr(pos))
+        if status != 0:
+            raise _ffi.JGS2Error(status, self._error())
+
+    def set_contact(self, enabled=True):
+        self._lib.jgs2_scene_set_contact(self._h, 1 if enabled else 0)
+
     def set_pinned(self, pinned):
         pin = np.ascontiguousarray(pinned, dtype=np.uint8)
         if pin.size != self.vertex_count:
@@ -363,8 +386,14 @@ class Scene:
                 hinge_rest_edge_lengths=f(c.hinge_rest_edge_lengths, H) if H else np.zeros(0, np.float32),
                 cloth_material=np.array([c.young_modulus, c.poisson_ratio, c.thickness, c.bending_stiffness],
                                         dtype=np.float32))
+        contact = {}
+        nc = rec.contact_vertex_triangle_count + rec.contact_edge_edge_count
+        if nc:
+            contact = dict(contact_indices=f(rec.contact_indices, 4 * nc),
+                           contact_counts=np.array([rec.contact_vertex_triangle_count,
+                                                    rec.contact_edge_edge_count], dtype=np.uint32))
         return SceneInput(
-            **cloth,
+            **cloth, **contact,
             vertex_count=V, tet_count=T, cubature_k=K,
             positions=f(rec.positions, 4 * V), vertex_rest=f(rec.vertex_rest, 4 * V),
             vertex_info=f(rec.vertex_info, 4 * V), tet_indices=f(rec.tet_indices, 4 * T),
@@ -460,6 +489,68 @@ def cloth_sheet(cells=127, young=1e4, bending=1e-3, **kwargs) -> SceneInput:
     corners pinned, over a pinned box collider."""
     return cloth_drape(cells=cells, prefold=False, pinned_columns=(0, cells), young=young, bending=bending,
                        **kwargs)
+
+
+def static_contact_candidates(vertex_count, triangles):
+    """buildStaticIpcContactCandidates: (indices uint32[4n], vt count, ee count)."""
+    lib = _ffi.scene_lib()
+    tri = np.ascontiguousarray(triangles, dtype=np.uint32).reshape(-1)
+    vt, ee = c_uint32(0), c_uint32(0)
+    n = lib.jgs2_build_static_contact_candidates(vertex_count, _ffi.uptr(tri), tri.size // 3, None, 0,
+                                                 ctypes.byref(vt), ctypes.byref(ee))
+    if n < 0:
+        raise ValueError("invalid surface triangles")
+    out = np.zeros(4 * n, dtype=np.uint32)
+    lib.jgs2_build_static_contact_candidates(vertex_count, _ffi.uptr(tri), tri.size // 3, _ffi.uptr(out), n,
+                                             ctypes.byref(vt), ctypes.byref(ee))
+    return out, vt.value, ee.value
+
+
+def rotate_euler_xyz(p, rx, ry, rz):
+    """rotateEulerXyz (src/simulation/cpu/mesh.ts:210-235): x, then y, then z."""
+    cx, sx, cy, sy, cz, sz = math.cos(rx), math.sin(rx), math.cos(ry), math.sin(ry), math.cos(rz), math.sin(rz)
+    x, y, z = p[:, 0], p[:, 1] * cx - p[:, 2] * sx, p[:, 1] * sx + p[:, 2] * cx
+    x, z = cy * x + sy * z, -sy * x + cy * z
+    x, y = cz * x - sz * y, sz * x + cz * y
+    return np.stack([x, y, z], axis=1)
+
+
+# Trough settings of the reference app for its IPC scenes (src/App.tsx:529-575).
+TROUGH_SETTINGS = dict(timestep=1 / 60, gravity=(0.0, -9.81, 0.0), floorHeight=-0.18, floorStiffness=0.0,
+                       iterations=3, velocityDamping=0.997, contactTangentialDamping=0.0, contactMargin=0.01,
+                       horizontalBodyCorrection=False, ipcActivationDistance=0.08, ipcMinimumDistance=0.003,
+                       ipcBarrierStiffness=1e5, ipcFrictionCoefficient=0.45, ipcFrictionVelocityEpsilon=0.05,
+                       ipcStepSafety=0.9, regularization=1e-6, rotationEpsilon=1e-7, maxStep=0.075)
+
+
+def trough(boxes=10, cubature_k=6, timestep=1 / 60, method=PRECOMPUTE_EXACT) -> SceneInput:
+    """IPC box trough (troughDefinition, src/scenes/index.ts:551-630): a
+    pinned two-cell solid warped into a V (y = 0.05 + 0.65|x| - 0.18(1 - layer))
+    and `boxes` one-cell stable Neo-Hookean boxes (0.46 m) stacked four per
+    layer above it, each slightly rotated; static IPC candidates over the
+    whole boundary surface."""
+    sc = Scene()
+    m_trough = sc.add_material(1000.0, 120000.0, 0.34, MATERIAL_STABLE_NEO_HOOKEAN)
+    m_box = [sc.add_material(850.0, 70000.0, 0.35, MATERIAL_STABLE_NEO_HOOKEAN) for _ in range(2)]
+    sc.add_cuboid((2, 1, 1), (-2.2, 0.0, -1.5), (4.4, 1.0, 3.0), m_trough, 0, 63)
+    starts = []
+    for i in range(boxes):
+        starts.append(sc.add_cuboid((1, 1, 1), (-0.23, -0.23, -0.23), (0.46, 0.46, 0.46), m_box[i % 2], i + 1, 0))
+    p = sc.rest_positions()
+    x, layer = p[:12, 0].copy(), p[:12, 1].copy()
+    p[:12, 1] = 0.05 + 0.65 * np.abs(x) - 0.18 * (1 - layer)
+    for i, s in enumerate(starts):
+        slot, lay = i % 4, i // 4
+        rot = (((i % 3) - 1) * 0.04, ((i % 5) - 2) * 0.035, (-1 if i % 2 == 0 else 1) * 0.055)
+        q = rotate_euler_xyz(p[s:s + 8], *rot)
+        q += np.array([-0.37 if slot % 2 == 0 else 0.37, 2.15 + 0.72 * lay, -0.38 if slot < 2 else 0.38])
+        p[s:s + 8] = q
+    sc.set_rest_positions(p)
+    sc.set_contact(True)
+    stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=method)
+    inp = sc.pack()
+    inp.stats = stats
+    return inp
 
 
 def batched_scenes(count=256, **kwargs) -> list:
