@@ -681,29 +681,72 @@ __global__ void __launch_bounds__(kBlock) contactLagKernel(Buffers b, const DevP
   if (c == b.scenes[scene].kOff) b.frames[scene].contactAlpha = 1.0f;
 }
 
-// buildActiveContactRows (:2742-2782), and the reset of the iteration's
-// safe-step reductions.
-__global__ void __launch_bounds__(kBlock) contactRowsKernel(Buffers b, const DevParams* __restrict__ pp,
-                                                            const float4* __restrict__ src, uint32_t V) {
-  const uint32_t v = blockIdx.x * kBlock + threadIdx.x;
-  if (v >= V) return;
-  const uint32_t scene = b.vertexScene[v];
+// buildActiveContactRows (:2742-2782) in two passes: the candidate's
+// inclusion (a property of the candidate alone), with the reset of the
+// iteration's safe-step reductions...
+__global__ void __launch_bounds__(kBlock) contactFlagKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                            const float4* __restrict__ src) {
+  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
+  if (c >= b.contactCount) return;
+  const uint32_t scene = b.contactScene[c];
   const DevParams& p = pp[scene];
   if (!p.active || !p.ipc) return;
-  if (v == b.scenes[scene].vOff) {
+  if (c == b.scenes[scene].kOff) {
     FrameState* fs = &b.frames[scene];
     fs->stepAlphaBits = __float_as_uint(1.0f);
     fs->stepValid = 1u;
     fs->checkAlphaBits = __float_as_uint(1.0f);
     fs->checkValid = 1u;
   }
+  b.contactFlag[c] = contactIncluded(b, p, c, src) ? 1u : 0u;
+}
+
+// ...then, one warp per vertex, the ordered compaction of its included
+// incident candidates into its active row.
+__global__ void __launch_bounds__(kBlock) contactRowsKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                            uint32_t V) {
+  const uint32_t v = blockIdx.x * (kBlock / 32) + threadIdx.x / 32;
+  const uint32_t lane = threadIdx.x & 31u;
+  if (v >= V) return;  // uniform across the warp
+  const DevParams& p = pp[b.vertexScene[v]];
+  if (!p.active || !p.ipc) return;
   const uint2 r = b.contactRange[v];
   uint32_t n = 0;
-  for (uint32_t k = 0; k < r.y; ++k) {
-    const uint32_t c = b.contactIds[r.x + k];
-    if (contactIncluded(b, p, c, src)) b.activeIds[r.x + n++] = c;
+  for (uint32_t k0 = 0; k0 < r.y; k0 += 32) {
+    const uint32_t k = k0 + lane;
+    const uint32_t c = k < r.y ? b.contactIds[r.x + k] : 0u;
+    const bool keep = k < r.y && b.contactFlag[c] != 0u;
+    const unsigned ballot = __ballot_sync(0xffffffffu, keep);
+    if (keep) b.activeIds[r.x + n + __popc(ballot & ((1u << lane) - 1u))] = c;
+    n += __popc(ballot);
   }
-  b.activeCount[v] = n;
+  if (lane == 0) b.activeCount[v] = n;
+}
+
+// The IPC part of convergenceGradient's contact component (:4086-4088) at
+// the accepted pose, one warp per vertex, from the contacts the promotion
+// pass makes the next source cache.
+__global__ void __launch_bounds__(kBlock) contactGradientKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                                const float4* __restrict__ src,
+                                                                const float4* __restrict__ tgt, uint32_t V) {
+  const uint32_t v = blockIdx.x * (kBlock / 32) + threadIdx.x / 32;
+  const uint32_t lane = threadIdx.x & 31u;
+  if (v >= V) return;  // uniform across the warp
+  const uint32_t scene = b.vertexScene[v];
+  const DevParams& p = pp[scene];
+  const FrameState* fs = &b.frames[scene];
+  if (!p.active || !p.ipc || latched(p, fs)) return;
+  if (isPinned(b.vinfo[v])) return;
+  const bool accepted = fs->control[1].x == 1.0f;
+  const float alpha = fs->contactAlpha;
+  const int slot = (accepted && finiteS(alpha) && alpha > 0.0f) ? kContactTarget : kContactSource;
+  float3 g = f3(0, 0, 0);
+  S3 unused = szero();
+  contactLocal<false>(b, p, v, accepted ? tgt : src, false, slot, lane, 32u, g, unused);
+  g.x = groupSum<32>(g.x, 0xffffffffu);
+  g.y = groupSum<32>(g.y, 0xffffffffu);
+  g.z = groupSum<32>(g.z, 0xffffffffu);
+  if (lane == 0) b.contactGrad[v] = make_float4(g.x, g.y, g.z, 0.0f);
 }
 
 __device__ __forceinline__ uint32_t alphaBits(float a) { return a > 0.0f ? __float_as_uint(a) : 0u; }
@@ -1443,7 +1486,7 @@ __device__ __forceinline__ void accumulateClothTri(GatePartial& acc, const Cloth
 __device__ __forceinline__ void accumulateContact(GatePartial& acc, const Buffers& b, const DevParams& p,
                                                   float contactAlpha, uint32_t c, const float4* __restrict__ src,
                                                   const float4* __restrict__ tgt) {
-  if (!contactIncluded(b, p, c, src)) return;
+  if (!b.contactFlag[c]) return;  // not in the active rows of this iteration
   const float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
   const ContactData ks = ipcCached(st[kContactSource], st[kContactSourceWeights]);
   const ContactData kc = contactAlpha != 0.0f ? ipcCached(st[kContactTarget], st[kContactTargetWeights]) : ks;
@@ -1693,14 +1736,7 @@ __global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const Dev
       }
       comps[4] = f3(0, 0, 0);
       if (p.floorStiffness > 0.0f && x.y < p.floorHeight) comps[4].y = p.floorStiffness * (x.y - p.floorHeight);
-      if (p.ipc) {
-        // IPC gradient at the accepted pose from the contacts the promotion
-        // pass makes the next source cache (convergenceGradient, :4088).
-        const float alpha = fs->contactAlpha;
-        const int slot = (accepted && finiteS(alpha) && alpha > 0.0f) ? kContactTarget : kContactSource;
-        S3 unused = szero();
-        contactLocal<false>(b, p, v, acc, false, slot, 0u, 1u, comps[4], unused);
-      }
+      if (p.ipc) comps[4] = comps[4] + xyz(b.contactGrad[v]);  // contactGradientKernel
       float3 totalG = f3(0, 0, 0);
       bool tv = true;
 #pragma unroll
@@ -1958,12 +1994,20 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   // One vertex per lane group: the line search makes per-vertex work uneven,
   // and the block scheduler balances it better than a fixed grid stride.
   const uint32_t blocks = std::max(1u, (count + groups - 1) / groups);
-  if (b.clothRange || b.contactIdx)
+  if (b.contactIdx && uint64_t(b.contactCount) * 4u > uint64_t(64) * count) {
+    // Contact-heavy engines (more than 64 candidate incidences per solved
+    // vertex on average): a whole warp per vertex over its active candidates.
+    const uint32_t wg = std::max(1u, std::min(groups * kGroup / 32u, kBlock / 32u));
+    const size_t wsmem = static_cast<size_t>(wg) * K * sizeof(CubState);
+    solveKernel<32, true><<<std::max(1u, (count + wg - 1) / wg), wg * 32, wsmem, s>>>(
+        b, p, src, tgt, list, count, K, cachedIncident ? 1 : 0);
+  } else if (b.clothRange || b.contactIdx) {
     solveKernel<kGroup, true><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
                                                                     cachedIncident ? 1 : 0);
-  else
+  } else {
     solveKernel<kGroup, false><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
                                                                      cachedIncident ? 1 : 0);
+  }
   return 1;
 }
 
@@ -1979,6 +2023,7 @@ uint32_t solveGroupsPerBlock(uint32_t K) {
     optin -= 1024;  // static shared memory of the kernel
     cudaFuncSetAttribute(solveKernel<kGroup, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     cudaFuncSetAttribute(solveKernel<kGroup, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(solveKernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   }
   const uint32_t perVertex = static_cast<uint32_t>(K * sizeof(CubState));
   uint32_t groups = kBlock / kGroup;
@@ -1994,7 +2039,15 @@ int launchContactLag(const Buffers& b, const DevParams* p, cudaStream_t s) {
 
 int launchContactRows(const Buffers& b, const DevParams* p, const float4* src, uint32_t V, cudaStream_t s) {
   if (b.contactCount == 0) return 0;
-  contactRowsKernel<<<blocksFor(V), kBlock, 0, s>>>(b, p, src, V);
+  contactFlagKernel<<<blocksFor(b.contactCount), kBlock, 0, s>>>(b, p, src);
+  contactRowsKernel<<<(V + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, s>>>(b, p, V);
+  return 2;
+}
+
+int launchContactGradient(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V,
+                          cudaStream_t s) {
+  if (b.contactCount == 0) return 0;
+  contactGradientKernel<<<(V + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, s>>>(b, p, src, tgt, V);
   return 1;
 }
 

@@ -135,6 +135,8 @@ struct Buffers {
   const uint32_t* contactIds;
   uint32_t* activeCount;
   uint32_t* activeIds;
+  uint32_t* contactFlag;   // per candidate: active this iteration
+  float4* contactGrad;     // per vertex: IPC gradient at the accepted pose
   uint32_t gateBlocks, convBlocks, sceneCount, contactCount;
 };
 
@@ -169,6 +171,10 @@ int launchContactApply(const Buffers& b, const DevParams* p, const float4* src, 
                        bool validated, cudaStream_t s);
 int launchContactValidate(const Buffers& b, const DevParams* p, const float4* tgt, cudaStream_t s);
 int launchContactPromote(const Buffers& b, const DevParams* p, cudaStream_t s);
+// The IPC component of the convergence gradient at the accepted pose, before
+// the convergence pass.
+int launchContactGradient(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V,
+                          cudaStream_t s);
 // bodyCorrection: some scene of the batch corrects its bodies this frame.
 int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool bodyCorrection,
                    uint32_t bodies, cudaStream_t s);

@@ -915,6 +915,8 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
       });
     }
     n += timed(P::kGate, [&] { return jgs2::launchGate(b, s->dParams, src, tgt, st); });
+    if (contact)
+      n += timed(P::kContact, [&] { return jgs2::launchContactGradient(b, s->dParams, src, tgt, s->V, st); });
     n += timed(P::kConvergence,
                [&] { return jgs2::launchConvergence(b, s->dParams, src, tgt, !colored && !last, st); });
     if (contact) n += timed(P::kContact, [&] { return jgs2::launchContactPromote(b, s->dParams, st); });
@@ -1579,6 +1581,8 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     b.contactIds = nullptr;
     b.activeCount = nullptr;
     b.activeIds = nullptr;
+    b.contactFlag = nullptr;
+    b.contactGrad = nullptr;
     b.contactCount = nK;
     if (nK) {
       uint4* ki = nullptr;
@@ -1600,7 +1604,11 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       STEP(upload(sp, &b.contactState, state.data(), state.size()));
       STEP(deviceAlloc(sp, &b.activeCount, nV));
       STEP(deviceAlloc(sp, &b.activeIds, contactIds.size()));
+      STEP(deviceAlloc(sp, &b.contactFlag, nK));
+      STEP(deviceAlloc(sp, &b.contactGrad, nV));
       CUDA_TRY(sp, cudaMemsetAsync(b.activeCount, 0, sizeof(uint32_t) * nV, sp->stream));
+      CUDA_TRY(sp, cudaMemsetAsync(b.contactFlag, 0, sizeof(uint32_t) * nK, sp->stream));
+      CUDA_TRY(sp, cudaMemsetAsync(b.contactGrad, 0, sizeof(float4) * nV, sp->stream));
       b.contactIdx = ki;
       b.contactScene = ks;
       b.contactRange = kr;
