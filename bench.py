@@ -415,12 +415,15 @@ def batched_arm(args):
 
 
 def serving_arm(args):
-    """A seeded Poisson stream (mean 2000 requests/s) of step requests, each a
-    cantilever (the 20x4x4 bar) at 1-4x resolution for 1-60 frames of 10
-    exact Jacobi iterations, served by the native continuous-batching loop
-    against a 150 GB device-memory budget; the plain per-request path (create
-    a solver, step, read, destroy, one request after another in arrival
-    order) runs the same stream beside it."""
+    """A seeded Poisson stream (mean 2000 requests/s) of step requests drawn
+    from the serving mix: a cantilever (the 20x4x4 bar) at 1-4x resolution
+    for 10 exact Jacobi iterations per frame, an IPC trough of 1-20 boxes with
+    the reference app's contact settings (3 iterations per frame), or the
+    128x128 StVK cloth sheet (5 iterations per frame at dt=1/120), each for
+    1-60 frames, served by the native continuous-batching loop against a
+    150 GB device-memory budget; the plain per-request path (create a solver,
+    step, read, destroy, one request after another in arrival order) runs the
+    same stream beside it."""
     import threading
 
     import numpy as np
@@ -433,37 +436,50 @@ def serving_arm(args):
     torch.cuda.set_device(local)
     device = local
     t0 = time.perf_counter()
-    bars = {}
-    for r in (1, 2, 3, 4):
-        path = os.path.join(cache_dir(), f"cantilever_x{r}_k6_v1.npz")
-        inp = None
+
+    def cached(name, build):
+        path = os.path.join(cache_dir(), name)
         if os.path.exists(path):
             try:
-                inp = scenes.SceneInput.load(path)
+                return scenes.SceneInput.load(path)
             except Exception:
                 os.remove(path)
-        if inp is None:
-            inp = scenes.cantilever(cells=(20 * r, 4 * r, 4 * r), method=scenes.PRECOMPUTE_PATCH)
-            try:
-                inp.save(path)
-            except OSError:
-                pass
-        bars[r] = inp
+        inp = build()
+        try:
+            inp.save(path)
+        except OSError:
+            pass
+        return inp
+
+    bar_settings = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floorStiffness=0.0, parityMode=True)
+    cloth_settings = dict(timestep=1 / 120, gravity=(0.0, -9.81, 0.0), floorStiffness=0.0, velocityDamping=0.997,
+                          contactTangentialDamping=0.0, horizontalBodyCorrection=False, maxStep=0.01)
+    kinds = {}  # key -> (input, settings, iterations per frame)
+    for r in (1, 2, 3, 4):
+        kinds[("bar", r)] = (cached(f"cantilever_x{r}_k6_v1.npz", lambda r=r: scenes.cantilever(
+            cells=(20 * r, 4 * r, 4 * r), method=scenes.PRECOMPUTE_PATCH)), bar_settings, 10)
+    for n_boxes in range(1, 21):
+        kinds[("trough", n_boxes)] = (cached(f"trough_{n_boxes}_k6_v1.npz", lambda n_boxes=n_boxes: scenes.trough(
+            n_boxes)), dict(scenes.TROUGH_SETTINGS), 3)
+    kinds[("cloth", 0)] = (cached("cloth_sheet_127_v1.npz", scenes.cloth_sheet), cloth_settings, 5)
     build_s = time.perf_counter() - t0
     rng = np.random.default_rng(2000 + rank)
     n = args.requests
     arrivals = np.cumsum(rng.exponential(1.0 / 2000.0, size=n))
-    sizes = rng.integers(1, 5, size=n)
     frames = rng.integers(1, 61, size=n)
-    iters = 10
-    settings = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floorStiffness=0.0, parityMode=True)
-    work = sum(bars[int(s)].active_vertex_count() * iters * int(f) for s, f in zip(sizes, frames))
+    kind_draw = rng.integers(0, 3, size=n)
+    size_draw = rng.integers(1, 5, size=n)
+    box_draw = rng.integers(1, 21, size=n)
+    keys = [("bar", int(size_draw[i])) if kind_draw[i] == 0 else
+            ("trough", int(box_draw[i])) if kind_draw[i] == 1 else ("cloth", 0) for i in range(n)]
+    work = sum(kinds[k][0].active_vertex_count() * kinds[k][2] * int(f) for k, f in zip(keys, frames))
     budget = 150 * 10**9
 
     if args.warmup > 0:  # module load and first graph captures, outside the measurement
         srv = server.JGS2Server(memoryBudgetBytes=budget, device=device)
-        for r in (1, 2, 3, 4):
-            srv.wait(srv.submit(bars[r], settings, frames=2, exactIterations=iters))
+        for k in (("bar", 1), ("bar", 4), ("trough", 1), ("trough", 20), ("cloth", 0)):
+            inp, st, it = kinds[k]
+            srv.wait(srv.submit(inp, st, frames=2, exactIterations=it))
         srv.destroy()
     srv = server.JGS2Server(memoryBudgetBytes=budget, device=device)
     ids = [None] * n
@@ -474,7 +490,8 @@ def serving_arm(args):
             delay = start + arrivals[i] - time.perf_counter()
             if delay > 0:
                 time.sleep(delay)
-            ids[i] = srv.submit(bars[int(sizes[i])], settings, frames=int(frames[i]), exactIterations=iters)
+            inp, st, it = kinds[keys[i]]
+            ids[i] = srv.submit(inp, st, frames=int(frames[i]), exactIterations=it)
 
     th = threading.Thread(target=submitter)
     with ClockSampler(device) as clocks:
@@ -493,8 +510,9 @@ def serving_arm(args):
         delay = start + arrivals[i] - time.perf_counter()
         if delay > 0:
             time.sleep(delay)
-        s = solver.JGS2GpuSolver.create(bars[int(sizes[i])], settings, device=device)
-        s.stepFramesExactIterations(int(frames[i]), iters)
+        inp, st, it = kinds[keys[i]]
+        s = solver.JGS2GpuSolver.create(inp, st, device=device)
+        s.stepFramesExactIterations(int(frames[i]), it)
         s.readPositions()
         s.destroy()
         plain_lat.append((time.perf_counter() - start - arrivals[i]) * 1e3)
@@ -502,18 +520,20 @@ def serving_arm(args):
     plain_lat = np.array(plain_lat)
     total_frames = int(frames.sum())
     value = whole_job_rate(world, work, makespan)
+    mix = {name: int(sum(1 for k in keys if k[0] == name)) for name in ("bar", "trough", "cloth")}
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": n, "warmup": args.warmup,
             "ms_per_step": 1e3 * makespan / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded)",
             "config": {
-                "workload": (f"serving stream: {n} requests, Poisson arrivals at a mean 2000/s (seed 2000), each a "
-                             "20x4x4-hex cantilever at 1-4x resolution (stable Neo-Hookean E=1e5 nu=0.4, K=6 "
-                             "patch-trained cubature) for 1-60 frames of 10 exact Jacobi iterations; 150 GB "
-                             "device-memory admission budget; trough and cloth requests are not served (no "
-                             "IPC or cloth in this build)"),
-                "requests": n, "frames": total_frames, "step": "one request",
+                "workload": (f"serving stream: {n} requests, Poisson arrivals at a mean 2000/s (seed 2000), drawn "
+                             "uniformly from a 20x4x4-hex cantilever at 1-4x resolution (stable Neo-Hookean E=1e5 "
+                             "nu=0.4, K=6 patch-trained cubature, 10 exact Jacobi iterations per frame), an IPC box "
+                             "trough of 1-20 boxes (the reference app's contact settings, 3 iterations per frame) "
+                             "and the 128x128 StVK cloth sheet (5 iterations per frame), each for 1-60 frames; "
+                             "150 GB device-memory admission budget"),
+                "requests": n, "mix": mix, "frames": total_frames, "step": "one request",
                 "l2": "no flush: requests stream through different resident scenes",
                 "precompute": {"seconds": round(build_s, 1)},
                 "parallelism": "replicas" if world > 1 else "single GPU"},
