@@ -127,7 +127,31 @@ typedef struct jgs2_input {
   const uint32_t* contact_indices;
   uint32_t contact_vertex_triangle_count;
   uint32_t contact_edge_edge_count;
+  /* Contact surface for the device broad phase (NULL: none); excludes
+   * contact_indices.  No counterpart in the reference, whose candidates are
+   * the static superset above. */
+  const struct jgs2_contact_surface* contact_surface;
 } jgs2_input;
+
+/*
+ * Device broad phase over the static candidate superset.  The superset of a
+ * surface grows with (surface vertices x triangles + edges^2), so instead of
+ * listing it the solver enumerates, every iteration on the device, the
+ * superset's candidates whose boxes, widened by each vertex's largest
+ * possible motion in the iteration (maxStep for free vertices, the snap to
+ * rest for pinned ones), come within the activation distance plus the f32
+ * rounding reach; candidates that carry lagged friction stay listed for the
+ * frame.  Every candidate left out contributes nothing to the reference's
+ * step (no active row, a full safe step, a valid check, zero energy), so
+ * the step is the one the static superset gives, in the superset's
+ * canonical order.  Requires the Jacobi schedule and maxStep > 0.
+ */
+typedef struct jgs2_contact_surface {
+  uint32_t triangle_count;
+  uint32_t reserved0;
+  const uint32_t* triangles;     /* 3 * triangle_count vertex indices; any order, duplicates merged */
+  uint64_t candidate_capacity;   /* candidates one iteration may list; 0 = 64 x (vertices + edges) */
+} jgs2_contact_surface;
 
 /*
  * Step settings: JGS2StepSettings (src/simulation/gpu/jgs2-solver.ts:64-100),
@@ -207,8 +231,9 @@ typedef struct jgs2_info {
   float preprocessing_timestep;
   uint32_t current_position_buffer;/* 0 = A, reported for zero-copy consumers */
   uint32_t cloth_triangle_count;   /* clothTriangleCount (:911) */
-  uint32_t contact_candidate_count;/* contactCandidateCount */
-  uint32_t reserved1;
+  uint32_t contact_candidate_count;/* contactCandidateCount; with a contact surface, the
+                                      candidates of the last iteration */
+  uint32_t contact_candidate_capacity; /* broad-phase capacity (0 for static candidates) */
 } jgs2_info;
 
 /* ---- library ---------------------------------------------------------- */
@@ -230,6 +255,13 @@ jgs2_status jgs2_resolve_settings(const jgs2_settings* defaults,
 
 /* validateJGS2GpuInput (src/simulation/gpu/layout.ts:223-416). */
 jgs2_status jgs2_validate_input(const jgs2_input* input);
+
+/* minimumStaticIpcContactDistance (src/simulation/cpu/ipc-contact.ts:385) in
+ * double at input->positions: over the static candidates, or over the
+ * superset of input->contact_surface restricted to pairs whose boxes come
+ * within `cutoff` (+infinity when none does).  The exact intersection check
+ * of a contact run: feed it the positions read back after each frame. */
+jgs2_status jgs2_minimum_contact_distance(const jgs2_input* input, double cutoff, double* distance);
 
 /* buildJGS2InputVertexColoring + buildGreedyVertexColoring
  * (src/simulation/gpu/jgs2-solver.ts:308-367;
@@ -348,6 +380,15 @@ jgs2_status jgs2_read_globalization(jgs2_solver* solver, float* local,
                                     size_t local_floats, float* control,
                                     float* history, size_t history_floats,
                                     uint32_t* history_count);
+
+/* The IPC candidates of the last iteration (4 u32 each: VT point, t0, t1,
+ * t2 or EE a0, a1, b0, b1 with bit 31 of the fourth set, canonical order).
+ * *count receives the number
+ * listed; out (may be NULL) holds `capacity` candidates.  Static candidates
+ * are listed as given.  With a contact surface, a broad-phase list that did
+ * not fit its capacity fails the step and this read with JGS2_DEVICE_ERROR. */
+jgs2_status jgs2_read_contact_candidates(jgs2_solver* solver, uint32_t* out,
+                                         uint64_t capacity, uint64_t* count);
 
 /* evaluateAssembledCandidateForTest(source, candidate, overrides)
  * (:2611-2726): run the production assembled gate (vertex energies,

@@ -122,12 +122,20 @@ uint32_t jgs2_scene_cloth_triangle_count(const jgs2_scene* scene);
  * 237-280) for rotated, warped or translated bodies. */
 jgs2_status jgs2_scene_set_rest_positions(jgs2_scene* scene, const double* positions);
 
-/* Nonzero: the packer enumerates the static IPC contact candidates of the
- * scene's surface (the tet boundary plus the cloth triangles;
- * buildStaticIpcContactCandidates, src/simulation/cpu/ipc-contact.ts:591-665)
- * into jgs2_input.contact_indices.  The enumeration is quadratic in the
- * surface size, like the reference's static superset. */
-jgs2_status jgs2_scene_set_contact(jgs2_scene* scene, uint32_t enabled);
+/* IPC contact over the scene's surface (the tet boundary plus the cloth
+ * triangles).  JGS2_SCENE_CONTACT_STATIC: the packer enumerates the static
+ * candidates (buildStaticIpcContactCandidates,
+ * src/simulation/cpu/ipc-contact.ts:591-665) into jgs2_input.contact_indices;
+ * the enumeration is quadratic in the surface size, like the reference's
+ * static superset.  JGS2_SCENE_CONTACT_SURFACE: the packer hands the surface
+ * to the device broad phase (jgs2_input.contact_surface) with
+ * `candidate_capacity` (0: the default).  JGS2_SCENE_CONTACT_NONE: no
+ * contact. */
+#define JGS2_SCENE_CONTACT_NONE 0u
+#define JGS2_SCENE_CONTACT_STATIC 1u
+#define JGS2_SCENE_CONTACT_SURFACE 2u
+jgs2_status jgs2_scene_set_contact(jgs2_scene* scene, uint32_t mode);
+jgs2_status jgs2_scene_set_contact_capacity(jgs2_scene* scene, uint64_t candidate_capacity);
 
 /* buildStaticIpcContactCandidates (src/simulation/cpu/ipc-contact.ts:591-665)
  * for an arbitrary triangle surface: returns the candidate count (-1 on

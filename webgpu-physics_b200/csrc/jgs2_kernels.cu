@@ -518,6 +518,12 @@ __global__ void __launch_bounds__(kBlock) copyKernel(Buffers b, const DevParams*
 // ---------------------------------------------------------------------------
 // IPC contact (jgs2-shader.ts:233-874, 2694-2917).
 
+// Candidates listed this iteration: the broad phase's count with a contact
+// surface, else the static total.  Candidate kernels stride over it.
+__device__ __forceinline__ uint32_t contactListed(const Buffers& b) {
+  return b.contactDynamic ? __ldcg(b.bpStatus) : b.contactCount;
+}
+
 __device__ __forceinline__ uint4 contactIndices(const Buffers& b, uint32_t c, uint32_t* type) {
   uint4 q = __ldg(&b.contactIdx[c]);
   *type = q.w >> 31;
@@ -751,13 +757,10 @@ __global__ void __launch_bounds__(kBlock) contactGradientKernel(Buffers b, const
 
 __device__ __forceinline__ uint32_t alphaBits(float a) { return a > 0.0f ? __float_as_uint(a) : 0u; }
 
-// candidateContactStep (:2784-2847) with the min / all-valid reduction of
-// reduceContactStep folded in as order-free atomics.
-__global__ void __launch_bounds__(kBlock) contactStepKernel(Buffers b, const DevParams* __restrict__ pp,
-                                                            const float4* __restrict__ src,
-                                                            const float4* __restrict__ tgt) {
-  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c >= b.contactCount) return;
+// candidateContactStep of one candidate.
+__device__ __forceinline__ void contactStepOne(const Buffers& b, const DevParams* __restrict__ pp,
+                                               const float4* __restrict__ src, const float4* __restrict__ tgt,
+                                               uint32_t c) {
   const uint32_t scene = b.contactScene[c];
   const DevParams& p = pp[scene];
   if (!p.active || !p.ipc) return;
@@ -794,6 +797,16 @@ __global__ void __launch_bounds__(kBlock) contactStepKernel(Buffers b, const Dev
   }
 }
 
+// candidateContactStep (:2784-2847) with the min / all-valid reduction of
+// reduceContactStep folded in as order-free atomics.
+__global__ void __launch_bounds__(kBlock) contactStepKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                            const float4* __restrict__ src,
+                                                            const float4* __restrict__ tgt) {
+  const uint32_t n = contactListed(b);
+  for (uint32_t c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock)
+    contactStepOne(b, pp, src, tgt, c);
+}
+
 // applyContactStep (:2909-2917): candidate = source + alpha (candidate -
 // source) with the safe-step alpha, or after validation with 1 (kept) or 0
 // (restored); the validated alpha becomes the iteration's contact alpha.
@@ -820,37 +833,511 @@ __global__ void __launch_bounds__(kBlock) contactApplyKernel(Buffers b, const De
 // (the target cache) and the all-valid reduction.
 __global__ void __launch_bounds__(kBlock) contactValidateKernel(Buffers b, const DevParams* __restrict__ pp,
                                                                 const float4* __restrict__ tgt) {
-  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c >= b.contactCount) return;
-  const uint32_t scene = b.contactScene[c];
-  const DevParams& p = pp[scene];
-  if (!p.active || !p.ipc) return;
-  FrameState* fs = &b.frames[scene];
-  const ContactData k = contactAt(b, c, tgt, p.ipcActivation + contactRoundingReach(p));
-  float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
-  ipcStoreCached(st, kContactTarget, k);
-  const bool valid = k.valid && finiteS(k.distance) && k.distance > p.ipcMinDistance;
-  const float d = valid ? k.distance : 0.0f;
-  st[kContactScratch] = make_float4(1.0f, d, d, valid ? 1.0f : 0.0f);
-  if (!valid) {
-    atomicMin(&fs->checkAlphaBits, 0u);
-    atomicAnd(&fs->checkValid, 0u);
+  const uint32_t n = contactListed(b);
+  for (uint32_t c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock) {
+    const uint32_t scene = b.contactScene[c];
+    const DevParams& p = pp[scene];
+    if (!p.active || !p.ipc) continue;
+    FrameState* fs = &b.frames[scene];
+    const ContactData k = contactAt(b, c, tgt, p.ipcActivation + contactRoundingReach(p));
+    float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+    ipcStoreCached(st, kContactTarget, k);
+    const bool valid = k.valid && finiteS(k.distance) && k.distance > p.ipcMinDistance;
+    const float d = valid ? k.distance : 0.0f;
+    st[kContactScratch] = make_float4(1.0f, d, d, valid ? 1.0f : 0.0f);
+    if (!valid) {
+      atomicMin(&fs->checkAlphaBits, 0u);
+      atomicAnd(&fs->checkValid, 0u);
+    }
   }
 }
 
 // promoteAcceptedContactCache (:2694-2710).
 __global__ void __launch_bounds__(kBlock) contactPromoteKernel(Buffers b, const DevParams* __restrict__ pp) {
-  const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
-  if (c >= b.contactCount) return;
-  const uint32_t scene = b.contactScene[c];
+  const uint32_t n = contactListed(b);
+  for (uint32_t c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock) {
+    const uint32_t scene = b.contactScene[c];
+    const DevParams& p = pp[scene];
+    if (!p.active || !p.ipc) continue;
+    const FrameState* fs = &b.frames[scene];
+    const float alpha = fs->contactAlpha;
+    if (fs->control[1].x == 1.0f && finiteS(alpha) && alpha > 0.0f) {
+      float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+      st[kContactSource] = st[kContactTarget];
+      st[kContactSourceWeights] = st[kContactTargetWeights];
+    }
+  }
+}
+
+// ---------------------------------------------------------------------------
+// IPC broad phase over the static candidate superset (contact surfaces).
+//
+// The superset (buildStaticIpcContactCandidates, ipc-contact.ts:591-665) is
+// never listed.  Every iteration one warp per row (a vertex against its
+// scene's surface triangles, or a surface edge against the later edges)
+// walks the row's columns in canonical order, 32-primitive chunk boxes
+// first, and lists the pairs whose boxes, each widened by the largest motion
+// its vertices can make this iteration, are not separated by more than the
+// activation distance plus the rounding reach; pairs of the previous list
+// that carry lagged friction stay listed for the frame.  A pair left out is
+// farther than that from every pose the iteration can produce, so the
+// reference's passes give it no active row, a full safe step, a valid check
+// and no energy: it does not act.  A listed pair's state is carried from the
+// previous list (the promoted source cache, the lagged friction) or formed
+// from the source pose as lagContact does.  The per-vertex active rows come
+// from a stable radix sort of the active candidates' vertex entries, so each
+// row keeps ascending candidate order, as the static rows do.
+
+constexpr uint32_t kBpChunk = 32;
+constexpr float kBpInf = __builtin_huge_valf();
+
+struct BpBox {
+  float3 lo, hi;
+  float m;  // largest motion of the primitive's vertices this iteration
+};
+
+// A vertex's largest displacement in one iteration: maxStep for a free
+// vertex (the line search caps each local step at maxStep, :3322-3445) and
+// the snap to rest for a pinned one, widened by a relative 2^-12 and 16 ulps
+// of the coordinates for the rounding of the committed positions.
+__device__ __forceinline__ float bpMotion(const Buffers& b, const DevParams& p, uint32_t v, float3 x) {
+  float m = fmaxf(p.maxStep, 0.0f);
+  if (isPinned(b.vinfo[v])) m = fmaxf(m, length3(xyz(b.restMass[v]) - x));
+  const float ax = fmaxf(fabsf(x.x), fmaxf(fabsf(x.y), fabsf(x.z)));
+  const float r = m * (1.0f + 0x1p-12f) + ax * 0x1p-19f;
+  return finiteS(r) ? r : kBpInf;
+}
+
+__device__ __forceinline__ BpBox bpEmpty() { return {f3(kBpInf, kBpInf, kBpInf), f3(-kBpInf, -kBpInf, -kBpInf), 0.0f}; }
+__device__ __forceinline__ BpBox bpEverything() {
+  return {f3(-kBpInf, -kBpInf, -kBpInf), f3(kBpInf, kBpInf, kBpInf), kBpInf};
+}
+
+// Bounds and largest motion of a primitive at x; non-finite data widens it
+// to everything (such a pair is always listed, as the static path keeps it).
+template <int N>
+__device__ __forceinline__ BpBox bpPrimitive(const Buffers& b, const DevParams& p, const float4* __restrict__ x,
+                                             const uint32_t (&vs)[N]) {
+  BpBox q = bpEmpty();
+  bool ok = true;
+#pragma unroll
+  for (int l = 0; l < N; ++l) {
+    const float3 y = xyz(x[vs[l]]);
+    ok = ok && finiteV(y);
+    q.lo = fmin3(q.lo, y);
+    q.hi = fmax3(q.hi, y);
+    q.m = fmaxf(q.m, bpMotion(b, p, vs[l], y));
+  }
+  return (ok && finiteS(q.m)) ? q : bpEverything();
+}
+
+__device__ __forceinline__ void bpStore(float4* boxes, uint32_t i, const BpBox& q) {
+  boxes[2ull * i] = make_float4(q.lo.x, q.lo.y, q.lo.z, q.m);
+  boxes[2ull * i + 1] = make_float4(q.hi.x, q.hi.y, q.hi.z, 0.0f);
+}
+__device__ __forceinline__ BpBox bpLoad(const float4* __restrict__ boxes, uint32_t i) {
+  const float4 a = boxes[2ull * i], c = boxes[2ull * i + 1];
+  return {f3(a.x, a.y, a.z), f3(c.x, c.y, c.z), a.w};
+}
+
+// Separated by more than `reach` once both boxes are widened by their
+// motions: the per-axis gaps less the motions, as a Euclidean length.  Each
+// step is monotone in the boxes, so a chunk box that contains a primitive's
+// box (and its motion) separates no more than the primitive's does.
+__device__ __forceinline__ bool bpSeparated(const BpBox& a, const BpBox& c, float reach) {
+  const float m = a.m + c.m;
+  const float3 g = fmax3(fmax3(c.lo - a.hi, a.lo - c.hi), f3(0, 0, 0));
+  const float3 h = fmax3(g - f3(m, m, m), f3(0, 0, 0));
+  return dot3(h, h) > reach * reach;
+}
+
+// The activation distance and twice the rounding reach
+// (ipcActiveContactReach less its step terms, which the motions carry),
+// widened by 2^-10.
+__device__ __forceinline__ float bpReach(const DevParams& p) {
+  return (p.ipcActivation + 2.0f * contactRoundingReach(p)) * (1.0f + 0x1p-10f);
+}
+
+// closed(a, v) of the enumeration: a == v or v in a's surface one-ring.
+__device__ __forceinline__ bool bpClosed(const Buffers& b, uint32_t a, uint32_t v) {
+  if (a == v) return true;
+  const uint2 r = b.bpRing[a];
+  for (uint32_t i = 0; i < r.y; ++i)
+    if (b.bpRingIds[r.x + i] == v) return true;
+  return false;
+}
+
+// The superset leaves out a vertex and a triangle of its closed one-ring,
+// and two edges with an endpoint of one in the other's closed one-rings.
+__device__ __forceinline__ bool bpPairClosed(const Buffers& b, bool edgeRow, const uint32_t (&rv)[2], uint32_t col) {
+  if (!edgeRow) {
+    const uint4 t = b.bpTris[col];
+    return bpClosed(b, rv[0], t.x) || bpClosed(b, rv[0], t.y) || bpClosed(b, rv[0], t.z);
+  }
+  const uint2 e = b.bpEdges[col];
+  return bpClosed(b, rv[0], e.x) || bpClosed(b, rv[0], e.y) || bpClosed(b, rv[1], e.x) || bpClosed(b, rv[1], e.y);
+}
+
+// Primitive and chunk boxes at the iteration's source pose (a warp's 32
+// primitives form one chunk), and the reset of every vertex's active row.
+__global__ void __launch_bounds__(kBlock) bpBoxesKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                        const float4* __restrict__ src, uint32_t triBlocks,
+                                                        uint32_t edgeBlocks, uint32_t V) {
+  const uint32_t blk = blockIdx.x;
+  if (blk < triBlocks + edgeBlocks) {
+    const bool edges = blk >= triBlocks;
+    const uint32_t i = (edges ? blk - triBlocks : blk) * kBlock + threadIdx.x;
+    const uint32_t n = edges ? b.bpEdgeTotal : b.bpTriTotal;
+    BpBox q = bpEmpty();
+    if (i < n) {
+      if (edges) {
+        const uint2 e = b.bpEdges[i];
+        const uint32_t vs[2] = {e.x, e.y};
+        q = bpPrimitive(b, pp[b.vertexScene[e.x]], src, vs);
+        bpStore(b.bpEdgeBox, i, q);
+      } else {
+        const uint4 t = b.bpTris[i];
+        const uint32_t vs[3] = {t.x, t.y, t.z};
+        q = bpPrimitive(b, pp[t.w], src, vs);
+        bpStore(b.bpTriBox, i, q);
+      }
+    }
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      q.lo.x = fminf(q.lo.x, __shfl_xor_sync(0xffffffffu, q.lo.x, o));
+      q.lo.y = fminf(q.lo.y, __shfl_xor_sync(0xffffffffu, q.lo.y, o));
+      q.lo.z = fminf(q.lo.z, __shfl_xor_sync(0xffffffffu, q.lo.z, o));
+      q.hi.x = fmaxf(q.hi.x, __shfl_xor_sync(0xffffffffu, q.hi.x, o));
+      q.hi.y = fmaxf(q.hi.y, __shfl_xor_sync(0xffffffffu, q.hi.y, o));
+      q.hi.z = fmaxf(q.hi.z, __shfl_xor_sync(0xffffffffu, q.hi.z, o));
+      q.m = fmaxf(q.m, __shfl_xor_sync(0xffffffffu, q.m, o));
+    }
+    if ((threadIdx.x & 31u) == 0u && i < n) bpStore(edges ? b.bpEdgeChunk : b.bpTriChunk, i / kBpChunk, q);
+    return;
+  }
+  const uint32_t v = (blk - triBlocks - edgeBlocks) * kBlock + threadIdx.x;
+  if (v < V) b.activeCount[v] = 0u;
+}
+
+// A listed pair at `pos`: indices, scene, column, state (carried from the
+// previous list, or the source contact and, at the frame's first iteration,
+// its lagged force as lagContact :2712-2740 forms them), activity
+// (contactIncluded) and the pair's four sort entries (vertex, candidate),
+// whose key is the sentinel when the pair is inactive.
+__device__ __forceinline__ void bpWriteCandidate(const Buffers& b, const DevParams& p, const float4* __restrict__ src,
+                                                 int first, uint32_t scene, bool edgeRow, const uint32_t (&rv)[2],
+                                                 uint32_t col, uint32_t pos, uint32_t prevBegin, uint32_t prevEnd) {
+  uint4 q;
+  if (edgeRow) {
+    const uint2 e = b.bpEdges[col];
+    q = make_uint4(rv[0], rv[1], e.x, e.y);
+  } else {
+    const uint4 t = b.bpTris[col];
+    q = make_uint4(rv[0], t.x, t.y, t.z);
+  }
+  b.contactIdx[pos] = make_uint4(q.x, q.y, q.z, q.w | (edgeRow ? 0x80000000u : 0u));
+  b.contactScene[pos] = scene;
+  b.bpCols[pos] = col;
+  float4* st = b.contactState + kContactStateWords * static_cast<size_t>(pos);
+  float4 lagF = make_float4(0, 0, 0, 0), lagW = make_float4(0, 0, 0, 0);
+  bool carried = false;
+  if (!first) {
+    uint32_t lo = prevBegin, hi = prevEnd;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (b.bpPrevCols[mid] < col) lo = mid + 1;
+      else hi = mid;
+    }
+    if (lo < prevEnd && b.bpPrevCols[lo] == col) {
+      const float4* ps = b.bpPrevState + kContactStateWords * static_cast<size_t>(lo);
+      st[kContactSource] = ps[kContactSource];
+      st[kContactSourceWeights] = ps[kContactSourceWeights];
+      lagF = ps[kContactLagged];
+      lagW = ps[kContactLaggedWeights];
+      carried = true;
+    }
+  }
+  if (!carried) {
+    const ContactData k = ipcContactFromPositions(edgeRow ? kIpcEdgeEdge : kIpcVertexTriangle, xyz(src[q.x]),
+                                                  xyz(src[q.y]), xyz(src[q.z]), xyz(src[q.w]),
+                                                  p.ipcActivation + contactRoundingReach(p));
+    ipcStoreCached(st, kContactSource, k);
+    if (first && k.valid && k.distance > p.ipcMinDistance) {
+      const float f = fmaxf(0.0f, -p.ipcStiffness * ipcBarrier1(k.distance, p.ipcActivation));
+      if (finiteS(f)) {
+        lagF = make_float4(k.normal.x, k.normal.y, k.normal.z, f);
+        lagW = k.weights;
+      }
+    }
+  }
+  st[kContactLagged] = lagF;
+  st[kContactLaggedWeights] = lagW;
+  st[kContactScratch] = make_float4(1, 0, 0, 0);
+  // contactIncluded on the state just written.
+  const ContactData k = ipcCached(st[kContactSource], st[kContactSourceWeights]);
+  const bool friction = p.ipcFriction > 0.0f && lagF.w > 0.0f;
+  const bool bounded = p.maxStep > 0.0f;
+  const float reach = p.ipcActivation + 2.0f * (fmaxf(p.maxStep, 0.0f) + contactRoundingReach(p));
+  const bool active =
+      !k.valid || !bounded || k.distance <= reach || friction || contactPinnedMotion(b, q, src, fmaxf(p.maxStep, 0.0f));
+  b.contactFlag[pos] = active ? 1u : 0u;
+  const uint32_t vs[4] = {q.x, q.y, q.z, q.w};
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    b.bpKeys[0][4ull * pos + l] = active ? vs[l] : b.bpSentinel;
+    b.bpVals[0][4ull * pos + l] = pos;
+  }
+}
+
+// One warp per row: the row's pairs in column order, counted (kWrite false,
+// into bpRowOff[row]) or written at the row's offset (kWrite true).
+template <bool kWrite>
+__global__ void __launch_bounds__(kBlock) bpRowsKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                       const float4* __restrict__ src, int first) {
+  __shared__ uint32_t carried[kBlock / 32][32];
+  const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x & 31u;
+  const uint32_t r = blockIdx.x * (kBlock / 32) + warp;
+  if (r >= b.bpRowTotal) return;                   // uniform across the warp
+  if (kWrite && __ldcg(&b.bpStatus[3])) return;   // over capacity: nothing listed this iteration
+  const uint4 row = b.bpRows[r];
+  const uint32_t scene = row.y & 0x7fffffffu;
+  const bool edgeRow = (row.y >> 31) != 0u;
   const DevParams& p = pp[scene];
-  if (!p.active || !p.ipc) return;
-  const FrameState* fs = &b.frames[scene];
-  const float alpha = fs->contactAlpha;
-  if (fs->control[1].x == 1.0f && finiteS(alpha) && alpha > 0.0f) {
-    float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
-    st[kContactSource] = st[kContactTarget];
-    st[kContactSourceWeights] = st[kContactTargetWeights];
+  uint32_t count = 0;
+  if (p.active && p.ipc && row.z < row.w) {
+    const float reach = bpReach(p);
+    uint32_t rv[2];
+    BpBox P;
+    if (edgeRow) {
+      const uint2 e = b.bpEdges[row.x];
+      rv[0] = e.x;
+      rv[1] = e.y;
+      P = bpLoad(b.bpEdgeBox, row.x);
+    } else {
+      rv[0] = rv[1] = row.x;
+      const uint32_t vs[1] = {row.x};
+      P = bpPrimitive(b, p, src, vs);
+    }
+    const uint32_t base = kWrite ? b.bpRowOff[r] : 0u;
+    uint32_t pc = 0, pe = 0;  // this row's entries of the previous list
+    if (!first) {
+      pc = b.bpPrevRowOff[r];
+      pe = b.bpPrevRowOff[r + 1];
+    }
+    const uint32_t prevBegin = pc;
+    const uint32_t chunkLo = row.z / kBpChunk, chunkHi = (row.w - 1) / kBpChunk;
+    const float4* chunkBoxes = edgeRow ? b.bpEdgeChunk : b.bpTriChunk;
+    const float4* primBoxes = edgeRow ? b.bpEdgeBox : b.bpTriBox;
+    for (uint32_t c0 = chunkLo; c0 <= chunkHi; c0 += 32) {
+      const uint32_t windowEnd = (c0 + 32) * kBpChunk;
+      carried[warp][lane] = 0u;
+      __syncwarp();
+      // Previous pairs of this window that carry lagged friction and that the
+      // box test leaves out stay listed.
+      while (pc < pe) {
+        const uint32_t i = pc + lane;
+        const uint32_t col = i < pe ? b.bpPrevCols[i] : 0xffffffffu;
+        const bool in = i < pe && col < windowEnd;
+        if (in && p.ipcFriction > 0.0f &&
+            b.bpPrevState[kContactStateWords * static_cast<size_t>(i) + kContactLagged].w > 0.0f &&
+            bpSeparated(P, bpLoad(primBoxes, col), reach))
+          atomicOr(&carried[warp][col / kBpChunk - c0], 1u << (col % kBpChunk));
+        const unsigned inMask = __ballot_sync(0xffffffffu, in);
+        pc += __popc(inMask);
+        if (inMask != 0xffffffffu) break;
+      }
+      __syncwarp();
+      const uint32_t chunk = c0 + lane;
+      const bool look = chunk <= chunkHi &&
+                        (carried[warp][lane] != 0u || !bpSeparated(P, bpLoad(chunkBoxes, chunk), reach));
+      unsigned todo = __ballot_sync(0xffffffffu, look);
+      while (todo) {
+        const uint32_t j = __ffs(todo) - 1;
+        todo &= todo - 1;
+        const uint32_t col = (c0 + j) * kBpChunk + lane;
+        bool hit = false;
+        if (col >= row.z && col < row.w) {
+          hit = ((carried[warp][j] >> lane) & 1u) != 0u;
+          if (!hit && !bpSeparated(P, bpLoad(primBoxes, col), reach)) hit = !bpPairClosed(b, edgeRow, rv, col);
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, hit);
+        if (kWrite && hit)
+          bpWriteCandidate(b, p, src, first, scene, edgeRow, rv, col, base + count + __popc(m & ((1u << lane) - 1u)),
+                           prevBegin, pe);
+        count += __popc(m);
+      }
+      __syncwarp();  // carried[] is rewritten by the next window
+    }
+  }
+  if (!kWrite && lane == 0) b.bpRowOff[r] = count;
+}
+
+constexpr int kScanThreads = 1024;
+
+// Exclusive scan of data[0, n) in place by one block of kScanThreads threads
+// (a contiguous run per thread); returns the total.  With the total above
+// `limit` every entry becomes zero.
+__device__ uint64_t blockScan(uint32_t* data, uint32_t n, uint64_t limit) {
+  __shared__ uint64_t part[kScanThreads];
+  const uint32_t per = (n + kScanThreads - 1) / kScanThreads;
+  const uint32_t lo = min(n, threadIdx.x * per), hi = min(n, lo + per);
+  uint64_t s = 0;
+  for (uint32_t i = lo; i < hi; ++i) s += data[i];
+  part[threadIdx.x] = s;
+  __syncthreads();
+  for (uint32_t o = 1; o < kScanThreads; o <<= 1) {
+    const uint64_t add = threadIdx.x >= o ? part[threadIdx.x - o] : 0ull;
+    __syncthreads();
+    part[threadIdx.x] += add;
+    __syncthreads();
+  }
+  const uint64_t total = part[kScanThreads - 1];
+  const bool over = total > limit;
+  uint64_t run = part[threadIdx.x] - s;
+  for (uint32_t i = lo; i < hi; ++i) {
+    const uint32_t c = data[i];
+    data[i] = over ? 0u : static_cast<uint32_t>(run);
+    run += c;
+  }
+  __syncthreads();
+  return total;
+}
+
+// Row offsets, the list's size (zero, with the overflow flags set, when it
+// exceeds the capacity), each scene's span of the list, and the resets the
+// static path makes in its flag and lag passes: the safe-step reductions
+// every iteration, the contact alpha at the frame's first.
+__global__ void __launch_bounds__(kScanThreads) bpScanKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                             int first) {
+  const uint32_t R = b.bpRowTotal;
+  const uint64_t total = blockScan(b.bpRowOff, R, b.contactCount);
+  const bool over = total > b.contactCount;
+  if (threadIdx.x == 0) {
+    b.bpRowOff[R] = over ? 0u : static_cast<uint32_t>(total);
+    b.bpStatus[0] = over ? 0u : static_cast<uint32_t>(total);
+    b.bpStatus[3] = over ? 1u : 0u;
+    if (over) {
+      b.bpStatus[1] = 1u;
+      b.bpStatus[2] = max(b.bpStatus[2], static_cast<uint32_t>(total > 0xffffffffull ? 0xffffffffull : total));
+    }
+  }
+  __syncthreads();
+  for (uint32_t s = threadIdx.x; s < b.sceneCount; s += blockDim.x) {
+    const SceneRange sr = b.scenes[s];
+    uint2 span = make_uint2(0u, 0u);
+    if (sr.rowCount) {
+      const uint32_t a = b.bpRowOff[sr.rowOff], e = b.bpRowOff[sr.rowOff + sr.rowCount];
+      span = make_uint2(a, e - a);
+    }
+    b.bpSpan[s] = span;
+    const DevParams& p = pp[s];
+    if (!p.active || !p.ipc) continue;
+    FrameState* fs = &b.frames[s];
+    fs->stepAlphaBits = __float_as_uint(1.0f);
+    fs->stepValid = 1u;
+    fs->checkAlphaBits = __float_as_uint(1.0f);
+    fs->checkValid = 1u;
+    if (first) fs->contactAlpha = 1.0f;
+  }
+}
+
+// Stable LSD radix sort of the (vertex, candidate) entries, 8 bits a pass:
+// per 4096-entry tile a digit histogram, one scan of the histograms in
+// digit-major order, then a scatter in which each warp ranks its entries in
+// input order (match_any peers) so equal digits keep their order.
+constexpr uint32_t kSortThreads = 256, kSortItems = 16, kSortTile = kSortThreads * kSortItems;
+
+__device__ __forceinline__ uint32_t sortTiles(const uint32_t* status) {
+  return (4u * __ldcg(status) + kSortTile - 1) / kSortTile;
+}
+
+__global__ void __launch_bounds__(kSortThreads) bpSortHistKernel(const uint32_t* __restrict__ keys,
+                                                                 const uint32_t* status, uint32_t shift,
+                                                                 uint32_t* __restrict__ hist) {
+  __shared__ uint32_t h[256];
+  const uint32_t M = 4u * __ldcg(status), tiles = sortTiles(status);
+  if (blockIdx.x >= tiles) return;
+  h[threadIdx.x] = 0u;
+  __syncthreads();
+#pragma unroll
+  for (uint32_t j = 0; j < kSortItems; ++j) {
+    const uint32_t i = blockIdx.x * kSortTile + j * kSortThreads + threadIdx.x;
+    if (i < M) atomicAdd(&h[(keys[i] >> shift) & 255u], 1u);
+  }
+  __syncthreads();
+  hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
+}
+
+__global__ void __launch_bounds__(kScanThreads) bpSortScanKernel(const uint32_t* status, uint32_t* hist) {
+  blockScan(hist, 256u * sortTiles(status), ~0ull);
+}
+
+__global__ void __launch_bounds__(kSortThreads) bpSortScatterKernel(const uint32_t* __restrict__ kin,
+                                                                    const uint32_t* __restrict__ vin,
+                                                                    uint32_t* __restrict__ kout,
+                                                                    uint32_t* __restrict__ vout,
+                                                                    const uint32_t* status, uint32_t shift,
+                                                                    const uint32_t* __restrict__ hist) {
+  __shared__ uint32_t wh[kSortThreads / 32][256];
+  const uint32_t M = 4u * __ldcg(status), tiles = sortTiles(status);
+  const uint32_t tile = blockIdx.x;
+  if (tile >= tiles) return;
+  const uint32_t w = threadIdx.x / 32, lane = threadIdx.x & 31u;
+  for (uint32_t d = threadIdx.x; d < 256u * (kSortThreads / 32); d += kSortThreads) (&wh[0][0])[d] = 0u;
+  __syncthreads();
+  const uint32_t base = tile * kSortTile + w * (kSortItems * 32);
+  uint32_t dig[kSortItems], pos[kSortItems];
+#pragma unroll
+  for (uint32_t j = 0; j < kSortItems; ++j) {
+    const uint32_t i = base + j * 32 + lane;
+    const bool valid = i < M;
+    const uint32_t d = valid ? (kin[i] >> shift) & 255u : 256u;
+    const unsigned peers = __match_any_sync(0xffffffffu, d);
+    const uint32_t rank = __popc(peers & ((1u << lane) - 1u));
+    const uint32_t before = valid ? wh[w][d] : 0u;
+    __syncwarp();
+    if (valid && rank == 0) wh[w][d] = before + __popc(peers);
+    __syncwarp();
+    dig[j] = d;
+    pos[j] = before + rank;
+  }
+  __syncthreads();
+  {
+    const uint32_t d = threadIdx.x;  // one digit per thread
+    uint32_t run = 0;
+#pragma unroll
+    for (uint32_t ww = 0; ww < kSortThreads / 32; ++ww) {
+      const uint32_t t = wh[ww][d];
+      wh[ww][d] = run;
+      run += t;
+    }
+  }
+  __syncthreads();
+#pragma unroll
+  for (uint32_t j = 0; j < kSortItems; ++j) {
+    if (dig[j] < 256u) {
+      const uint32_t i = base + j * 32 + lane;
+      const uint32_t o = hist[dig[j] * tiles + tile] + wh[w][dig[j]] + pos[j];
+      kout[o] = kin[i];
+      vout[o] = vin[i];
+    }
+  }
+}
+
+// Each vertex's run of the sorted keys is its active row.
+__global__ void __launch_bounds__(kBlock) bpSegmentsKernel(Buffers b, const uint32_t* __restrict__ keys) {
+  const uint32_t M = 4u * __ldcg(b.bpStatus);
+  for (uint32_t i = blockIdx.x * kBlock + threadIdx.x; i < M; i += gridDim.x * kBlock) {
+    const uint32_t k = keys[i];
+    if (k >= b.bpSentinel || (i > 0 && keys[i - 1] == k)) continue;
+    uint32_t lo = i + 1, hi = M;
+    while (lo < hi) {
+      const uint32_t mid = (lo + hi) >> 1;
+      if (keys[mid] <= k) lo = mid + 1;
+      else hi = mid;
+    }
+    b.contactRange[k] = make_uint2(i, 0u);
+    b.activeCount[k] = lo - i;
   }
 }
 
@@ -1606,6 +2093,10 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
   FrameState* fs = &b.frames[rb.scene];
   if (!p.active || latched(p, fs)) return;  // uniform across the scene's blocks
   GatePartial acc = gateIdentity();
+  // Contacts: element k takes candidates k, k + span, ... of the scene's
+  // list (a single pass for static candidates, which the table covers).
+  const uint32_t span = max(max(max(sr.V, sr.T), max(sr.C, sr.H)), max(sr.KC, 1u));
+  const uint2 contacts = b.contactDynamic ? b.bpSpan[rb.scene] : make_uint2(sr.kOff, sr.KC);
   for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
     if (k < sr.T) {
       const TetRec r = loadTet(b.tets, sr.tOff + k);
@@ -1623,7 +2114,9 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
       if (k < sr.C) accumulateClothTri(acc, loadClothTri(b.clothTris, sr.cOff + k), src, tgt, clothMaterial(p));
       if (k < sr.H) accumulateHinge(acc, b.clothHinges, sr.hOff + k, src, tgt, p.clothBending);
     }
-    if (p.ipc && k < sr.KC) accumulateContact(acc, b, p, fs->contactAlpha, sr.kOff + k, src, tgt);
+    if (p.ipc)
+      for (uint32_t c = k; c < contacts.y; c += span)
+        accumulateContact(acc, b, p, fs->contactAlpha, contacts.x + c, src, tgt);
   }
   const GatePartial blk = blockFold(acc, smem, gateCombine);
   GatePartial* partials = reinterpret_cast<GatePartial*>(b.gatePartials);
@@ -1994,9 +2487,13 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   // One vertex per lane group: the line search makes per-vertex work uneven,
   // and the block scheduler balances it better than a fixed grid stride.
   const uint32_t blocks = std::max(1u, (count + groups - 1) / groups);
-  if (b.contactIdx && uint64_t(b.contactCount) * 4u > uint64_t(64) * count) {
-    // Contact-heavy engines (more than 64 candidate incidences per solved
-    // vertex on average): a whole warp per vertex over its active candidates.
+  // Contact-heavy engines (more than 64 static candidate incidences per
+  // solved vertex on average, or a broad phase over cloth, whose sheets lie
+  // within the barrier reach of many of their own triangles): a whole warp
+  // per vertex over its active candidates.
+  const bool heavy = b.contactDynamic ? b.clothRange != nullptr
+                                      : uint64_t(b.contactCount) * 4u > uint64_t(64) * count;
+  if (b.contactIdx && heavy) {
     const uint32_t wg = std::max(1u, std::min(groups * kGroup / 32u, kBlock / 32u));
     const size_t wsmem = static_cast<size_t>(wg) * K * sizeof(CubState);
     solveKernel<32, true><<<std::max(1u, (count + wg - 1) / wg), wg * 32, wsmem, s>>>(
@@ -2051,9 +2548,16 @@ int launchContactGradient(const Buffers& b, const DevParams* p, const float4* sr
   return 1;
 }
 
+// Candidate kernels: one thread per static candidate, or a grid that strides
+// over the broad phase's list (its count is on the device).
+uint32_t candidateBlocks(const Buffers& b) {
+  const uint32_t n = blocksFor(b.contactCount);
+  return b.contactDynamic ? std::min(n, smCount() * 16u) : n;
+}
+
 int launchContactStep(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s) {
   if (b.contactCount == 0) return 0;
-  contactStepKernel<<<blocksFor(b.contactCount), kBlock, 0, s>>>(b, p, src, tgt);
+  contactStepKernel<<<candidateBlocks(b), kBlock, 0, s>>>(b, p, src, tgt);
   return 1;
 }
 
@@ -2066,14 +2570,43 @@ int launchContactApply(const Buffers& b, const DevParams* p, const float4* src, 
 
 int launchContactValidate(const Buffers& b, const DevParams* p, const float4* tgt, cudaStream_t s) {
   if (b.contactCount == 0) return 0;
-  contactValidateKernel<<<blocksFor(b.contactCount), kBlock, 0, s>>>(b, p, tgt);
+  contactValidateKernel<<<candidateBlocks(b), kBlock, 0, s>>>(b, p, tgt);
   return 1;
 }
 
 int launchContactPromote(const Buffers& b, const DevParams* p, cudaStream_t s) {
   if (b.contactCount == 0) return 0;
-  contactPromoteKernel<<<blocksFor(b.contactCount), kBlock, 0, s>>>(b, p);
+  contactPromoteKernel<<<candidateBlocks(b), kBlock, 0, s>>>(b, p);
   return 1;
+}
+
+uint32_t broadPhaseSortPasses(uint32_t V) {
+  uint32_t bits = 1;
+  while (bits < 32 && (V >> bits) != 0u) ++bits;  // keys 0..V, the sentinel V included
+  return (bits + 7) / 8;
+}
+
+int launchBroadPhase(const Buffers& b, const DevParams* p, const float4* src, uint32_t V, bool first,
+                     cudaStream_t s) {
+  if (!b.contactDynamic || b.contactCount == 0) return 0;
+  const uint32_t triBlocks = blocksFor(b.bpTriTotal), edgeBlocks = blocksFor(b.bpEdgeTotal);
+  bpBoxesKernel<<<triBlocks + edgeBlocks + blocksFor(V), kBlock, 0, s>>>(b, p, src, triBlocks, edgeBlocks, V);
+  const uint32_t rowBlocks = (b.bpRowTotal + kBlock / 32 - 1) / (kBlock / 32);
+  const int f = first ? 1 : 0;
+  bpRowsKernel<false><<<rowBlocks, kBlock, 0, s>>>(b, p, src, f);
+  bpScanKernel<<<1, kScanThreads, 0, s>>>(b, p, f);
+  bpRowsKernel<true><<<rowBlocks, kBlock, 0, s>>>(b, p, src, f);
+  const uint32_t tiles = static_cast<uint32_t>((4ull * b.contactCount + kSortTile - 1) / kSortTile);
+  for (uint32_t pass = 0; pass < b.bpSortPasses; ++pass) {
+    const uint32_t in = pass & 1u, out = in ^ 1u;
+    bpSortHistKernel<<<tiles, kSortThreads, 0, s>>>(b.bpKeys[in], b.bpStatus, 8u * pass, b.bpHist);
+    bpSortScanKernel<<<1, kScanThreads, 0, s>>>(b.bpStatus, b.bpHist);
+    bpSortScatterKernel<<<tiles, kSortThreads, 0, s>>>(b.bpKeys[in], b.bpVals[in], b.bpKeys[out], b.bpVals[out],
+                                                       b.bpStatus, 8u * pass, b.bpHist);
+  }
+  const uint32_t segBlocks = std::min(blocksFor(4u * b.contactCount), smCount() * 8u);
+  bpSegmentsKernel<<<segBlocks, kBlock, 0, s>>>(b, b.bpKeys[b.bpSortPasses & 1u]);
+  return 5 + 3 * static_cast<int>(b.bpSortPasses);
 }
 
 int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* dst, uint32_t V, cudaStream_t s) {

@@ -46,7 +46,8 @@ struct SceneRange {
   uint32_t gateBase, gateBlocks;  // prologue / gate partials of this scene
   uint32_t convBase, convBlocks;  // convergence partials of this scene
   uint32_t cOff, C, hOff, H;      // cloth triangles and hinges of this scene
-  uint32_t kOff, KC, pad[2];      // IPC candidates of this scene
+  uint32_t kOff, KC;              // static IPC candidates of this scene
+  uint32_t rowOff, rowCount;      // broad-phase rows of this scene (contact surface)
 };
 
 // One block of a segmented reduction: elements [begin, end) of `scene`,
@@ -128,16 +129,51 @@ struct Buffers {
   // scene and 7 float4 of state (jgs2_contact.cuh); per vertex the range
   // (first, count) of its incident candidates in `contactIds` and the count
   // of active ones, listed at the same offsets in `activeIds`.
-  const uint4* contactIdx;
-  const uint32_t* contactScene;
+  uint4* contactIdx;
+  uint32_t* contactScene;
   float4* contactState;
-  const uint2* contactRange;
+  uint2* contactRange;
   const uint32_t* contactIds;
   uint32_t* activeCount;
   uint32_t* activeIds;
   uint32_t* contactFlag;   // per candidate: active this iteration
   float4* contactGrad;     // per vertex: IPC gradient at the accepted pose
   uint32_t gateBlocks, convBlocks, sceneCount, contactCount;
+  // IPC broad phase (contact surfaces; all null for static candidates, and
+  // contactCount is then the candidate capacity of one iteration).  Rows:
+  // one per vertex of a contact scene (vertex-triangle rows) and one per
+  // surface edge (edge-edge rows), each (primitive, scene | edge-edge bit 31,
+  // first column, end column) over the global surface triangle or edge
+  // index; a row's columns are its candidates in the superset's canonical
+  // order.  Surface triangles (vertex indices, scene), edges, each vertex's
+  // closed surface one-ring; per iteration the primitive and 32-primitive
+  // chunk boxes ((lo, motion), (hi, 0)); the current list (row offsets,
+  // columns) and the previous iteration's (row offsets, columns, state) for
+  // carried caches and lagged friction; per scene its span of the current
+  // list; status words (listed candidates, sticky overflow flag, largest
+  // count asked for, this iteration's overflow); the sort's key / value
+  // ping-pong buffers and tile histograms.
+  uint32_t contactDynamic;
+  uint32_t bpRowTotal, bpTriTotal, bpEdgeTotal, bpSentinel, bpSortPasses, bpPad[2];
+  const uint4* bpRows;
+  const uint4* bpTris;
+  const uint2* bpEdges;
+  const uint2* bpRing;
+  const uint32_t* bpRingIds;
+  float4* bpTriBox;
+  float4* bpEdgeBox;
+  float4* bpTriChunk;
+  float4* bpEdgeChunk;
+  uint32_t* bpRowOff;
+  const uint32_t* bpPrevRowOff;
+  uint32_t* bpCols;
+  const uint32_t* bpPrevCols;
+  const float4* bpPrevState;
+  uint2* bpSpan;
+  uint32_t* bpStatus;
+  uint32_t* bpKeys[2];
+  uint32_t* bpVals[2];
+  uint32_t* bpHist;
 };
 
 // Kernel launch entry points (jgs2_kernels.cu).  `p` points at one DevParams
@@ -171,6 +207,15 @@ int launchContactApply(const Buffers& b, const DevParams* p, const float4* src, 
                        bool validated, cudaStream_t s);
 int launchContactValidate(const Buffers& b, const DevParams* p, const float4* tgt, cudaStream_t s);
 int launchContactPromote(const Buffers& b, const DevParams* p, cudaStream_t s);
+// The device broad phase of one iteration (contact surfaces): primitive and
+// chunk boxes, row counts, their scan, the rows' candidates with their
+// carried or fresh state and activity, and the per-vertex active rows (a
+// stable sort of the active candidates' vertex entries).  `first`: the
+// frame's first iteration, which also lags the contacts.
+int launchBroadPhase(const Buffers& b, const DevParams* p, const float4* src, uint32_t V, bool first,
+                     cudaStream_t s);
+// Sort passes of launchBroadPhase for `V` vertex keys (the sentinel included).
+uint32_t broadPhaseSortPasses(uint32_t V);
 // The IPC component of the convergence gradient at the accepted pose, before
 // the convergence pass.
 int launchContactGradient(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V,

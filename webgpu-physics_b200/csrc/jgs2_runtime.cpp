@@ -11,6 +11,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -23,6 +24,7 @@
 #include <thread>
 #include <string>
 #include <tuple>
+#include <unordered_map>
 #include <vector>
 
 #include "jgs2.h"
@@ -422,6 +424,33 @@ bool validateInput(const jgs2_input* in, std::string* err) {
     *err = "Total IPC candidate count must be below 2^29.";
     return false;
   }
+  if (const jgs2_contact_surface* cs = in->contact_surface) {
+    if (nc > 0) {
+      *err = "Give either static IPC candidates or a contact surface, not both.";
+      return false;
+    }
+    if (cs->triangle_count > 0 && !cs->triangles) {
+      *err = "Contact surface triangles are NULL.";
+      return false;
+    }
+    if (cs->candidate_capacity >= (1ull << 28)) {
+      *err = "The contact candidate capacity must be below 2^28.";
+      return false;
+    }
+    for (uint64_t t = 0; t < cs->triangle_count; ++t) {
+      const uint32_t* q = &cs->triangles[3 * t];
+      if (q[0] >= V || q[1] >= V || q[2] >= V) {
+        *err = format("Contact surface triangle %llu references a vertex outside vertexCount %u.",
+                      static_cast<unsigned long long>(t), V);
+        return false;
+      }
+      if (q[0] == q[1] || q[1] == q[2] || q[0] == q[2]) {
+        *err = format("Contact surface triangle %llu must reference three distinct vertices.",
+                      static_cast<unsigned long long>(t));
+        return false;
+      }
+    }
+  }
   for (uint64_t c = 0; c < nc; ++c) {
     const uint32_t* q = &in->contact_indices[4 * c];
     const char* type = c < in->contact_vertex_triangle_count ? "VT" : "EE";
@@ -441,10 +470,10 @@ bool validateInput(const jgs2_input* in, std::string* err) {
   return true;
 }
 
-// evaluateIpcVertexTriangleDistance / evaluateIpcEdgeEdgeDistance /
-// minimumStaticIpcContactDistance (src/simulation/cpu/ipc-contact.ts:192-385)
-// in double on the f32 input positions.
-double staticContactDistance(const jgs2_input* in) {
+// evaluateIpcVertexTriangleDistance / evaluateIpcEdgeEdgeDistance
+// (src/simulation/cpu/ipc-contact.ts:192-385) in double on the f32 input
+// positions: candidate q (vertex-triangle when vt, else edge-edge).
+double candidateDistance(const jgs2_input* in, const uint32_t* q, bool vt) {
   struct P { double x, y, z; };
   auto at = [&](uint32_t v) {
     return P{in->positions[4ull * v], in->positions[4ull * v + 1], in->positions[4ull * v + 2]};
@@ -465,14 +494,10 @@ double staticContactDistance(const jgs2_input* in) {
     if (std::isfinite(l2) && l2 > 1e-20) *t = clamp01(dot(sub(q, s), edge) / l2);
     return dist(q, lerp(s, e, *t));
   };
-  double minimum = std::numeric_limits<double>::max();
-  const uint64_t nvt = in->contact_vertex_triangle_count;
-  const uint64_t nc = nvt + in->contact_edge_edge_count;
-  for (uint64_t c = 0; c < nc; ++c) {
-    const uint32_t* q = &in->contact_indices[4 * c];
+  {
     const P p0 = at(q[0]), p1 = at(q[1]), p2 = at(q[2]), p3 = at(q[3]);
     double d;
-    if (c < nvt) {
+    if (vt) {
       const P e01 = sub(p2, p1), e02 = sub(p3, p1), e12 = sub(p3, p2);
       const double s01 = dot(e01, e01), s02 = dot(e02, e02), s12 = dot(e12, e12);
       const double largest = std::max(s01, std::max(s02, s12));
@@ -523,7 +548,162 @@ double staticContactDistance(const jgs2_input* in) {
       }
       d = dist(lerp(p0, p1, pa), lerp(p2, p3, pb));
     }
-    minimum = std::min(minimum, d);
+    return d;
+  }
+}
+
+// minimumStaticIpcContactDistance (src/simulation/cpu/ipc-contact.ts:385).
+double staticContactDistance(const jgs2_input* in) {
+  double minimum = std::numeric_limits<double>::max();
+  const uint64_t nvt = in->contact_vertex_triangle_count;
+  const uint64_t nc = nvt + in->contact_edge_edge_count;
+  for (uint64_t c = 0; c < nc; ++c) minimum = std::min(minimum, candidateDistance(in, &in->contact_indices[4 * c], c < nvt));
+  return minimum;
+}
+
+// A contact surface for the device broad phase: canonical triangles (sorted
+// vertices, sorted, unique), their edges (sorted, unique) and each vertex's
+// surface one-ring (sorted), the order and exclusions of the static superset
+// (buildStaticIpcContactCandidates, src/simulation/cpu/ipc-contact.ts:591-665).
+struct ContactSurface {
+  std::vector<std::array<uint32_t, 3>> tris;
+  std::vector<std::array<uint32_t, 2>> edges;
+  std::vector<uint32_t> ringStart;  // V + 1
+  std::vector<uint32_t> ring;
+  uint64_t capacity = 0;            // candidates one iteration may list
+};
+
+void buildContactSurface(const jgs2_input* in, ContactSurface* out) {
+  const jgs2_contact_surface* cs = in->contact_surface;
+  out->tris.resize(cs->triangle_count);
+  for (uint32_t t = 0; t < cs->triangle_count; ++t) {
+    std::array<uint32_t, 3> a = {cs->triangles[3ull * t], cs->triangles[3ull * t + 1], cs->triangles[3ull * t + 2]};
+    std::sort(a.begin(), a.end());
+    out->tris[t] = a;
+  }
+  std::sort(out->tris.begin(), out->tris.end());
+  out->tris.erase(std::unique(out->tris.begin(), out->tris.end()), out->tris.end());
+  for (const auto& t : out->tris) {
+    out->edges.push_back({t[0], t[1]});
+    out->edges.push_back({t[1], t[2]});
+    out->edges.push_back({t[0], t[2]});
+  }
+  std::sort(out->edges.begin(), out->edges.end());
+  out->edges.erase(std::unique(out->edges.begin(), out->edges.end()), out->edges.end());
+  const uint32_t V = in->vertex_count;
+  out->ringStart.assign(V + 1, 0);
+  for (const auto& e : out->edges) {
+    out->ringStart[e[0] + 1]++;
+    out->ringStart[e[1] + 1]++;
+  }
+  for (uint32_t v = 0; v < V; ++v) out->ringStart[v + 1] += out->ringStart[v];
+  out->ring.resize(out->ringStart[V]);
+  std::vector<uint32_t> cursor(out->ringStart.begin(), out->ringStart.end() - 1);
+  for (const auto& e : out->edges) {
+    out->ring[cursor[e[0]]++] = e[1];
+    out->ring[cursor[e[1]]++] = e[0];
+  }
+  for (uint32_t v = 0; v < V; ++v) std::sort(out->ring.begin() + out->ringStart[v], out->ring.begin() + out->ringStart[v + 1]);
+  out->capacity = cs->candidate_capacity
+                      ? cs->candidate_capacity
+                      : std::max<uint64_t>(4096, 64ull * (uint64_t(V) + out->edges.size()));
+}
+
+// The smallest distance over the superset's candidates whose boxes come
+// within `cutoff` (a hashed grid over the primitive boxes); +infinity when
+// no candidate does.  Pairs farther apart cannot decide the create-time
+// feasibility check.
+double surfaceContactDistance(const jgs2_input* in, const ContactSurface& cs, double cutoff) {
+  struct Box { double lo[3], hi[3]; };
+  const float* x = in->positions;
+  auto boxOf = [&](const uint32_t* v, int n) {
+    Box b;
+    for (int k = 0; k < 3; ++k) {
+      b.lo[k] = b.hi[k] = x[4ull * v[0] + k];
+      for (int l = 1; l < n; ++l) {
+        b.lo[k] = std::min(b.lo[k], double(x[4ull * v[l] + k]));
+        b.hi[k] = std::max(b.hi[k], double(x[4ull * v[l] + k]));
+      }
+    }
+    return b;
+  };
+  const size_t nT = cs.tris.size(), nE = cs.edges.size();
+  std::vector<Box> tb(nT), eb(nE);
+  double extent = 0;
+  for (size_t t = 0; t < nT; ++t) {
+    tb[t] = boxOf(cs.tris[t].data(), 3);
+    for (int k = 0; k < 3; ++k) extent = std::max(extent, tb[t].hi[k] - tb[t].lo[k]);
+  }
+  for (size_t e = 0; e < nE; ++e) eb[e] = boxOf(cs.edges[e].data(), 2);
+  for (int k = 0; k < 3; ++k)
+    for (size_t t = 0; t < nT; ++t)
+      if (!std::isfinite(tb[t].lo[k]) || !std::isfinite(tb[t].hi[k])) return -1.0;  // non-finite pose
+  const double cell = std::max(cutoff, extent / 4 + cutoff);
+  auto key = [](int64_t i, int64_t j, int64_t k) {
+    return (uint64_t(i & 0x1fffff) << 42) | (uint64_t(j & 0x1fffff) << 21) | uint64_t(k & 0x1fffff);
+  };
+  auto cellOf = [&](double v) { return static_cast<int64_t>(std::floor(v / cell)); };
+  auto closed = [&](uint32_t a, uint32_t b) {
+    return a == b || std::binary_search(cs.ring.begin() + cs.ringStart[a], cs.ring.begin() + cs.ringStart[a + 1], b);
+  };
+  auto gridOf = [&](const std::vector<Box>& boxes) {
+    std::unordered_map<uint64_t, std::vector<uint32_t>> g;
+    for (size_t i = 0; i < boxes.size(); ++i) {
+      const Box& b = boxes[i];
+      for (int64_t a = cellOf(b.lo[0] - cutoff); a <= cellOf(b.hi[0] + cutoff); ++a)
+        for (int64_t c = cellOf(b.lo[1] - cutoff); c <= cellOf(b.hi[1] + cutoff); ++c)
+          for (int64_t d = cellOf(b.lo[2] - cutoff); d <= cellOf(b.hi[2] + cutoff); ++d)
+            g[key(a, c, d)].push_back(static_cast<uint32_t>(i));
+    }
+    return g;
+  };
+  auto gap = [](const Box& a, const Box& b) {
+    double s = 0;
+    for (int k = 0; k < 3; ++k) {
+      const double g = std::max(0.0, std::max(b.lo[k] - a.hi[k], a.lo[k] - b.hi[k]));
+      s += g * g;
+    }
+    return std::sqrt(s);
+  };
+  double minimum = INFINITY;
+  {
+    const auto g = gridOf(tb);
+    for (uint32_t v = 0; v < in->vertex_count; ++v) {
+      const uint32_t vv[1] = {v};
+      const Box p = boxOf(vv, 1);
+      auto it = g.find(key(cellOf(p.lo[0]), cellOf(p.lo[1]), cellOf(p.lo[2])));
+      if (it == g.end()) continue;
+      for (uint32_t t : it->second) {
+        const auto& tri = cs.tris[t];
+        if (closed(v, tri[0]) || closed(v, tri[1]) || closed(v, tri[2]) || gap(p, tb[t]) > cutoff) continue;
+        const uint32_t q[4] = {v, tri[0], tri[1], tri[2]};
+        minimum = std::min(minimum, candidateDistance(in, q, true));
+      }
+    }
+  }
+  {
+    const auto g = gridOf(eb);
+    std::vector<uint32_t> stamp(nE, 0xffffffffu);
+    for (uint32_t i = 0; i < nE; ++i) {
+      const Box& b = eb[i];
+      for (int64_t a = cellOf(b.lo[0]); a <= cellOf(b.hi[0]); ++a)
+        for (int64_t c = cellOf(b.lo[1]); c <= cellOf(b.hi[1]); ++c)
+          for (int64_t d = cellOf(b.lo[2]); d <= cellOf(b.hi[2]); ++d) {
+            auto it = g.find(key(a, c, d));
+            if (it == g.end()) continue;
+            for (uint32_t j : it->second) {
+              if (j <= i || stamp[j] == i) continue;
+              stamp[j] = i;
+              const auto& ea = cs.edges[i];
+              const auto& eb2 = cs.edges[j];
+              if (closed(ea[0], eb2[0]) || closed(ea[0], eb2[1]) || closed(ea[1], eb2[0]) || closed(ea[1], eb2[1]) ||
+                  gap(b, eb[j]) > cutoff)
+                continue;
+              const uint32_t q[4] = {ea[0], ea[1], eb2[0], eb2[1]};
+              minimum = std::min(minimum, candidateDistance(in, q, false));
+            }
+          }
+    }
   }
   return minimum;
 }
@@ -619,6 +799,11 @@ struct SceneHost {
   uint32_t C = 0, H = 0, cOff = 0, hOff = 0;  // cloth triangles / hinges and their offsets
   float clothLambda = 0.f, clothMu = 0.f, clothThickness = 0.f, clothBending = 0.f;
   uint32_t KC = 0, kOff = 0;  // IPC candidates and their offset
+  // Contact surface (device broad phase): surface triangles and edges, their
+  // offsets, the scene's rows and its share of the list capacity.
+  bool dynamic = false;
+  uint32_t bpTris = 0, bpEdges = 0, bpTriOff = 0, bpEdgeOff = 0, bpRowOff = 0, bpRows = 0;
+  uint64_t bpCapacity = 0;
   // IPC parameters fixed at create (jgs2-solver.ts:1096-1105).
   float ipcMinDistance = 0.f, ipcFriction = 0.f, ipcEpsilon = 0.f, ipcSafety = 0.f;
   float sceneScale = 1.f;
@@ -643,6 +828,16 @@ struct Engine {
   uint32_t V = 0, T = 0, K = 0, bodies = 1;  // totals over the scenes; K = widest record count
   uint32_t C = 0, H = 0;                     // cloth triangles and hinges over the scenes
   uint32_t KC = 0;                           // IPC candidates over the scenes
+  // Device broad phase: the two candidate lists (current and previous
+  // iteration, alternating by iteration) and the sort's buffers.
+  bool dynamic = false;
+  uint64_t bpCapacity = 0;
+  uint4* dynIdx[2] = {nullptr, nullptr};
+  uint32_t* dynScene[2] = {nullptr, nullptr};
+  float4* dynState[2] = {nullptr, nullptr};
+  uint32_t* dynFlag[2] = {nullptr, nullptr};
+  uint32_t* dynCols[2] = {nullptr, nullptr};
+  uint32_t* dynRowOff[2] = {nullptr, nullptr};
   bool glob = true;
   std::vector<SceneHost> scenes;
   // Colour lists over all scenes: colour c holds every scene's colour-c vertices.
@@ -795,7 +990,8 @@ DevParams makeParams(const Engine* s, uint32_t scene, const jgs2_settings& st, b
   p.ipcFriction = sc.ipcFriction;
   p.ipcEpsilon = sc.ipcEpsilon;
   p.ipcSafety = sc.ipcSafety;
-  p.ipc = (s->glob && sc.KC > 0 && st.ipc_barrier_stiffness > 0 && st.ipc_activation_distance > sc.ipcMinDistance)
+  p.ipc = (s->glob && (sc.KC > 0 || sc.dynamic) && st.ipc_barrier_stiffness > 0 &&
+           st.ipc_activation_distance > sc.ipcMinDistance)
               ? 1u : 0u;
   return p;
 }
@@ -877,12 +1073,30 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
                [&] { return jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, bodyCorrection, s->bodies, st); });
     return n;
   }
-  if (contact) n += timed(P::kContact, [&] { return jgs2::launchContactLag(b, s->dParams, st); });
+  const bool dynamic = contact && b.contactDynamic;
+  if (contact && !dynamic) n += timed(P::kContact, [&] { return jgs2::launchContactLag(s->b, s->dParams, st); });
   for (uint32_t it = 0; it < iterations; ++it) {
-    float4* src = (it % 2 == 0) ? b.pos[1] : b.pos[0];
-    float4* tgt = (it % 2 == 0) ? b.pos[0] : b.pos[1];
+    float4* src = (it % 2 == 0) ? s->b.pos[1] : s->b.pos[0];
+    float4* tgt = (it % 2 == 0) ? s->b.pos[0] : s->b.pos[1];
     const bool last = it + 1 == iterations;
-    if (contact) n += timed(P::kContact, [&] { return jgs2::launchContactRows(b, s->dParams, src, s->V, st); });
+    // With a contact surface the iterations alternate between two candidate
+    // lists: this iteration's and the previous one's (carried state).
+    Buffers b = s->b;
+    if (dynamic) {
+      const int cur = static_cast<int>(it & 1u), prev = cur ^ 1;
+      b.contactIdx = s->dynIdx[cur];
+      b.contactScene = s->dynScene[cur];
+      b.contactState = s->dynState[cur];
+      b.contactFlag = s->dynFlag[cur];
+      b.bpCols = s->dynCols[cur];
+      b.bpRowOff = s->dynRowOff[cur];
+      b.bpPrevRowOff = s->dynRowOff[prev];
+      b.bpPrevCols = s->dynCols[prev];
+      b.bpPrevState = s->dynState[prev];
+      n += timed(P::kContact, [&] { return jgs2::launchBroadPhase(b, s->dParams, src, s->V, it == 0, st); });
+    } else if (contact) {
+      n += timed(P::kContact, [&] { return jgs2::launchContactRows(b, s->dParams, src, s->V, st); });
+    }
     if (colored) {
       n += timed(P::kCopy, [&] { return jgs2::launchCopy(b, s->dParams, src, tgt, s->V, st); });
       for (uint32_t c = 0; c < s->colorCount; ++c) {
@@ -921,9 +1135,9 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
                [&] { return jgs2::launchConvergence(b, s->dParams, src, tgt, !colored && !last, st); });
     if (contact) n += timed(P::kContact, [&] { return jgs2::launchContactPromote(b, s->dParams, st); });
   }
-  const float4* finalPos = (iterations % 2 == 0) ? b.pos[1] : b.pos[0];
+  const float4* finalPos = (iterations % 2 == 0) ? s->b.pos[1] : s->b.pos[0];
   n += timed(P::kEpilogue,
-             [&] { return jgs2::launchEpilogue(b, s->dParams, finalPos, s->V, bodyCorrection, s->bodies, st); });
+             [&] { return jgs2::launchEpilogue(s->b, s->dParams, finalPos, s->V, bodyCorrection, s->bodies, st); });
   return n;
 }
 
@@ -956,6 +1170,14 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
   for (uint32_t i = 0; i < s->scenes.size(); ++i) {
     s->hParams[i] = makeParams(s, i, st[i], stop);
     contact = contact || s->hParams[i].ipc != 0;
+  }
+  if (s->dynamic && contact) {
+    if (schedule != JGS2_SCHEDULE_JACOBI)
+      return fail(s, JGS2_INVALID_ARGUMENT, "The IPC broad phase steps the Jacobi schedule only.");
+    for (uint32_t i = 0; i < s->scenes.size(); ++i)
+      if (s->hParams[i].ipc && !(s->hParams[i].maxStep > 0.0f))
+        return fail(s, JGS2_INVALID_ARGUMENT,
+                    "The IPC broad phase bounds each iteration's motion by maxStep; maxStep must be positive.");
   }
   CUDA_TRY(s, cudaSetDevice(s->device));
   CUDA_TRY(s, cudaMemcpyAsync(s->dParams, s->hParams.data(), sizeof(DevParams) * s->hParams.size(),
@@ -1040,11 +1262,24 @@ jgs2_status stepCommon(jgs2_solver* s, uint32_t frames, int exactIterations, con
   return runFrames(s, st, frames, iterations, production, prof);
 }
 
+// After a synchronisation: a broad-phase list that did not fit its capacity
+// (the iteration then listed nothing) fails the call.
+jgs2_status checkBroadPhase(Engine* s) {
+  if (!s->dynamic) return JGS2_OK;
+  uint32_t status[4];
+  CUDA_TRY(s, cudaMemcpy(status, s->b.bpStatus, sizeof(status), cudaMemcpyDeviceToHost));
+  if (status[1] == 0u) return JGS2_OK;
+  return fail(s, JGS2_DEVICE_ERROR,
+              format("The IPC broad phase needed %u candidates in one iteration, above its capacity of %llu; "
+                     "raise contact_surface.candidate_capacity.",
+                     status[2], static_cast<unsigned long long>(s->bpCapacity)));
+}
+
 jgs2_status readRegion(Engine* s, const void* dev, size_t bytes, void* host) {
   CUDA_TRY(s, cudaSetDevice(s->device));
   CUDA_TRY(s, cudaMemcpyAsync(host, dev, bytes, cudaMemcpyDeviceToHost, s->stream));
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));
-  return JGS2_OK;
+  return checkBroadPhase(s);
 }
 
 // The host mirrors may change only after the previous upload from them has
@@ -1083,6 +1318,8 @@ struct PreparedScene {
   std::vector<uint32_t> colors;
   bool colored = false;
   bool stable = true;  // stable Neo-Hookean (else co-rotated linear)
+  bool dynamic = false;        // contact surface for the device broad phase
+  ContactSurface surface;
   std::string error;  // message of a failed preparation (thread-safe copy)
 };
 
@@ -1105,6 +1342,16 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
   if (contacts > 0 && !out->stable)
     return fail(nullptr, JGS2_INVALID_ARGUMENT,
                 "IPC contact candidates require the stable Neo-Hookean production path.");
+  if (in->contact_surface) {
+    if (!out->stable)
+      return fail(nullptr, JGS2_INVALID_ARGUMENT, "IPC contact requires the stable Neo-Hookean production path.");
+    if (colour)
+      return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                  "The IPC broad phase steps the Jacobi schedule; create a contact-surface scene without the "
+                  "graph-coloured schedule.");
+    out->dynamic = true;
+    buildContactSurface(in, &out->surface);
+  }
   out->colored = colour;
   if (colour) out->colors = colorInput(in, &out->colorCount);
   if (out->colorCount > JGS2_MAX_SCHEDULE_COLORS)
@@ -1125,6 +1372,24 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
       return fail(nullptr, JGS2_INVALID_ARGUMENT,
                   format("IPC candidates require an initially feasible source pose with distance greater than %g "
                          "(minimum plus an f32 safety margin); got %g.", required, minimum));
+  }
+  if (out->dynamic) {
+    // The same check over the superset of the contact surface; candidates
+    // farther than the cutoff cannot fail it.
+    const double dMin = out->resolved.ipc_minimum_distance;
+    const double cutoff =
+        2.0 * (dMin + 8.0 * std::ldexp(1.0, -24) * std::max(1.0, double(out->resolved.ipc_activation_distance))) +
+        1e-9;
+    const double minimum = surfaceContactDistance(in, out->surface, cutoff);
+    if (minimum != INFINITY) {
+      const double margin = 8.0 * std::ldexp(1.0, -24) *
+                            std::max(1.0, std::max(double(out->resolved.ipc_activation_distance), std::fabs(minimum)));
+      const double required = dMin + margin;
+      if (!std::isfinite(minimum) || !(minimum > required))
+        return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                    format("IPC candidates require an initially feasible source pose with distance greater than %g "
+                           "(minimum plus an f32 safety margin); got %g.", required, minimum));
+    }
   }
   const double m = out->stable ? minimumInputDeterminant(in) : 1.0;
   if (!std::isfinite(m) || !(m > kDeterminantFloor))
@@ -1197,6 +1462,12 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     sc.ipcEpsilon = prep[i].resolved.ipc_friction_velocity_epsilon;
     sc.ipcSafety = prep[i].resolved.ipc_step_safety;
     KC += sc.KC;
+    if (prep[i].dynamic) {
+      sc.dynamic = true;
+      sc.bpTris = static_cast<uint32_t>(prep[i].surface.tris.size());
+      sc.bpEdges = static_cast<uint32_t>(prep[i].surface.edges.size());
+      sc.bpCapacity = prep[i].surface.capacity;
+    }
     uint32_t maxBody = 0;
     for (uint32_t v = 0; v < sc.V; ++v) maxBody = std::max(maxBody, in->vertex_info[4ull * v + 3]);
     sc.bodies = maxBody + 1;
@@ -1227,6 +1498,26 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   if (!sp->coloringBuilt) colorCount = 0;
   sp->colorCount = colorCount;
   const uint32_t nV = sp->V, nT = sp->T;
+  // Contact surfaces: rows, triangles and edges of each scene in order.
+  uint64_t bpT = 0, bpE = 0, bpR = 0, bpCap = 0;
+  for (SceneHost& sc : sp->scenes) {
+    if (!sc.dynamic) continue;
+    sp->dynamic = true;
+    sc.bpTriOff = static_cast<uint32_t>(bpT);
+    sc.bpEdgeOff = static_cast<uint32_t>(bpE);
+    sc.bpRowOff = static_cast<uint32_t>(bpR);
+    sc.bpRows = sc.V + sc.bpEdges;
+    bpT += sc.bpTris;
+    bpE += sc.bpEdges;
+    bpR += sc.bpRows;
+    bpCap += sc.bpCapacity;
+  }
+  if (sp->dynamic && sp->KC > 0)
+    return fail(nullptr, JGS2_INVALID_ARGUMENT, "A batch cannot mix static IPC candidates with contact surfaces.");
+  if (bpCap >= (1ull << 28) || bpR >= (1ull << 31) || bpT >= (1ull << 31) || bpE >= (1ull << 31))
+    return fail(nullptr, JGS2_INVALID_ARGUMENT,
+                "The contact surfaces of one batch must stay below 2^28 candidates and 2^31 rows or primitives.");
+  sp->bpCapacity = bpCap;
 
   // Objectives (packJGS2VertexObjectives, layout.ts:635-668).
   std::vector<float4> initialForces(nV), initialTargets(nV);
@@ -1444,6 +1735,33 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     for (uint32_t c = 0; c < sc.KC; ++c)
       for (int l = 0; l < 4; ++l) contactIds[base + cursor[in->contact_indices[4ull * c + l]]++] = sc.kOff + c;
   });
+  // Contact surfaces: triangles (global vertices, scene) and edges in each
+  // scene's canonical order, per vertex its one-ring, and the rows: per
+  // vertex of the scene against its triangles, per edge against its later
+  // edges, in the superset's order.
+  std::vector<uint4> bpRowsH(bpR), bpTrisH(bpT);
+  std::vector<uint2> bpEdgesH(bpE), bpRingH(sp->dynamic ? nV : 0, make_uint2(0u, 0u));
+  std::vector<uint32_t> ringBase(S + 1, 0);
+  for (uint32_t i = 0; i < S; ++i)
+    ringBase[i + 1] = ringBase[i] + (prep[i].dynamic ? static_cast<uint32_t>(prep[i].surface.ring.size()) : 0u);
+  std::vector<uint32_t> bpRingIdsH(ringBase[S]);
+  if (sp->dynamic) parallelFor(S, [&](uint32_t i) {
+    const SceneHost& sc = sp->scenes[i];
+    if (!sc.dynamic) return;
+    const ContactSurface& cs = prep[i].surface;
+    for (uint32_t t = 0; t < sc.bpTris; ++t)
+      bpTrisH[sc.bpTriOff + t] = make_uint4(sc.vOff + cs.tris[t][0], sc.vOff + cs.tris[t][1], sc.vOff + cs.tris[t][2], i);
+    for (uint32_t e = 0; e < sc.bpEdges; ++e)
+      bpEdgesH[sc.bpEdgeOff + e] = make_uint2(sc.vOff + cs.edges[e][0], sc.vOff + cs.edges[e][1]);
+    for (uint32_t v = 0; v < sc.V; ++v) {
+      bpRingH[sc.vOff + v] = make_uint2(ringBase[i] + cs.ringStart[v], cs.ringStart[v + 1] - cs.ringStart[v]);
+      bpRowsH[sc.bpRowOff + v] = make_uint4(sc.vOff + v, i, sc.bpTriOff, sc.bpTriOff + sc.bpTris);
+    }
+    for (size_t k = 0; k < cs.ring.size(); ++k) bpRingIdsH[ringBase[i] + k] = sc.vOff + cs.ring[k];
+    for (uint32_t e = 0; e < sc.bpEdges; ++e)
+      bpRowsH[sc.bpRowOff + sc.V + e] =
+          make_uint4(sc.bpEdgeOff + e, i | 0x80000000u, sc.bpEdgeOff + e + 1, sc.bpEdgeOff + sc.bpEdges);
+  });
   // Segmented reduction tables: each scene's elements in fixed chunks.
   std::vector<jgs2::SceneRange> ranges(S);
   std::vector<jgs2::RedBlock> gateTable, convTable;
@@ -1453,6 +1771,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     r.vOff = sc.vOff; r.V = sc.V; r.tOff = sc.tOff; r.T = sc.T;
     r.cOff = sc.cOff; r.C = sc.C; r.hOff = sc.hOff; r.H = sc.H;
     r.kOff = sc.kOff; r.KC = sc.KC;
+    r.rowOff = sc.bpRowOff; r.rowCount = sc.dynamic ? sc.bpRows : 0u;
     const uint32_t n = std::max(std::max(std::max(sc.V, sc.T), std::max(sc.C, sc.H)), sc.KC);
     r.gateBase = static_cast<uint32_t>(gateTable.size());
     for (uint32_t b0 = 0; b0 < std::max(n, 1u); b0 += jgs2::kGateChunk)
@@ -1614,6 +1933,66 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       b.contactRange = kr;
       b.contactIds = kd;
     }
+    b.contactDynamic = sp->dynamic ? 1u : 0u;
+    if (sp->dynamic) {
+      // Device broad phase: static surface data, per-iteration boxes, two
+      // candidate lists, the sort's buffers and the status words.
+      const uint64_t cap = sp->bpCapacity;
+      b.contactCount = static_cast<uint32_t>(cap);
+      b.bpRowTotal = static_cast<uint32_t>(bpR);
+      b.bpTriTotal = static_cast<uint32_t>(bpT);
+      b.bpEdgeTotal = static_cast<uint32_t>(bpE);
+      b.bpSentinel = nV;
+      b.bpSortPasses = jgs2::broadPhaseSortPasses(nV);
+      uint4* rows = nullptr;
+      uint4* tris = nullptr;
+      uint2* edges = nullptr;
+      uint2* ring = nullptr;
+      uint32_t* ringIds = nullptr;
+      STEP(upload(sp, &rows, bpRowsH.data(), bpRowsH.size()));
+      STEP(upload(sp, &tris, bpTrisH.data(), bpTrisH.size()));
+      STEP(upload(sp, &edges, bpEdgesH.data(), bpEdgesH.size()));
+      STEP(upload(sp, &ring, bpRingH.data(), bpRingH.size()));
+      STEP(upload(sp, &ringIds, bpRingIdsH.data(), bpRingIdsH.size()));
+      b.bpRows = rows;
+      b.bpTris = tris;
+      b.bpEdges = edges;
+      b.bpRing = ring;
+      b.bpRingIds = ringIds;
+      STEP(deviceAlloc(sp, &b.bpTriBox, 2 * bpT));
+      STEP(deviceAlloc(sp, &b.bpEdgeBox, 2 * bpE));
+      STEP(deviceAlloc(sp, &b.bpTriChunk, 2 * ((bpT + 31) / 32)));
+      STEP(deviceAlloc(sp, &b.bpEdgeChunk, 2 * ((bpE + 31) / 32)));
+      for (int l = 0; l < 2; ++l) {
+        STEP(deviceAlloc(sp, &sp->dynIdx[l], cap));
+        STEP(deviceAlloc(sp, &sp->dynScene[l], cap));
+        STEP(deviceAlloc(sp, &sp->dynState[l], 7 * cap));
+        STEP(deviceAlloc(sp, &sp->dynFlag[l], cap));
+        STEP(deviceAlloc(sp, &sp->dynCols[l], cap));
+        STEP(deviceAlloc(sp, &sp->dynRowOff[l], bpR + 1));
+        CUDA_TRY(sp, cudaMemsetAsync(sp->dynRowOff[l], 0, sizeof(uint32_t) * (bpR + 1), sp->stream));
+        STEP(deviceAlloc(sp, &b.bpKeys[l], 4 * cap));
+        STEP(deviceAlloc(sp, &b.bpVals[l], 4 * cap));
+      }
+      STEP(deviceAlloc(sp, &b.bpHist, 256 * ((4 * cap + 4095) / 4096) + 1));
+      STEP(deviceAlloc(sp, &b.bpSpan, S));
+      STEP(deviceAlloc(sp, &b.bpStatus, 4));
+      CUDA_TRY(sp, cudaMemsetAsync(b.bpStatus, 0, sizeof(uint32_t) * 4, sp->stream));
+      CUDA_TRY(sp, cudaMemsetAsync(b.bpSpan, 0, sizeof(uint2) * S, sp->stream));
+      STEP(deviceAlloc(sp, &b.contactRange, nV));
+      STEP(deviceAlloc(sp, &b.activeCount, nV));
+      STEP(deviceAlloc(sp, &b.contactGrad, nV));
+      CUDA_TRY(sp, cudaMemsetAsync(b.activeCount, 0, sizeof(uint32_t) * nV, sp->stream));
+      CUDA_TRY(sp, cudaMemsetAsync(b.contactGrad, 0, sizeof(float4) * nV, sp->stream));
+      // The first list view; encodeFrame points each iteration at its own.
+      b.contactIdx = sp->dynIdx[0];
+      b.contactScene = sp->dynScene[0];
+      b.contactState = sp->dynState[0];
+      b.contactFlag = sp->dynFlag[0];
+      b.bpCols = sp->dynCols[0];
+      b.bpRowOff = sp->dynRowOff[0];
+      b.activeIds = b.bpVals[b.bpSortPasses & 1u];
+    }
     STEP(upload(sp, &sp->dColorVertices, byColor.data(), byColor.size()));
     STEP(upload(sp, &sp->dNeedVertices, need.data(), need.size()));
     STEP(deviceAlloc(sp, &sp->dParams, S));
@@ -1728,6 +2107,14 @@ jgs2_status sceneInfo(Engine* s, uint32_t scene, jgs2_info* out) {
   out->current_position_buffer = 0;
   out->cloth_triangle_count = sc.C;
   out->contact_candidate_count = sc.KC;
+  out->contact_candidate_capacity = 0;
+  if (sc.dynamic) {
+    // The scene's span of the last iteration's list.
+    out->contact_candidate_capacity = static_cast<uint32_t>(sc.bpCapacity);
+    uint2 span = make_uint2(0u, 0u);
+    if (sc.submittedIterations && readRegion(s, s->b.bpSpan + scene, sizeof(span), &span) == JGS2_OK)
+      out->contact_candidate_count = span.y;
+  }
   if (sc.recordsAvailable) {
     float4 c1;
     if (readRegion(s, &s->b.frames[scene].control[1], sizeof(c1), &c1) == JGS2_OK)
@@ -1765,6 +2152,22 @@ jgs2_status jgs2_resolve_settings(const jgs2_settings* base, const jgs2_settings
 jgs2_status jgs2_validate_input(const jgs2_input* input) {
   std::string err;
   if (!validateInput(input, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_minimum_contact_distance(const jgs2_input* input, double cutoff, double* distance) {
+  std::string err;
+  if (!validateInput(input, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  if (!distance) return fail(nullptr, JGS2_INVALID_ARGUMENT, "distance is NULL.");
+  if (!(cutoff >= 0)) return fail(nullptr, JGS2_INVALID_ARGUMENT, "cutoff must be nonnegative.");
+  if (input->contact_surface) {
+    ContactSurface cs;
+    buildContactSurface(input, &cs);
+    *distance = surfaceContactDistance(input, cs, cutoff);
+  } else {
+    const uint64_t nc = uint64_t(input->contact_vertex_triangle_count) + input->contact_edge_edge_count;
+    *distance = nc ? staticContactDistance(input) : INFINITY;
+  }
   return JGS2_OK;
 }
 
@@ -1868,6 +2271,41 @@ jgs2_status jgs2_sync(jgs2_solver* s) {
   if (st != JGS2_OK) return st;
   CUDA_TRY(s, cudaSetDevice(s->device));
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return checkBroadPhase(s);
+}
+
+jgs2_status jgs2_read_contact_candidates(jgs2_solver* s, uint32_t* out, uint64_t capacity, uint64_t* count) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!count) return fail(s, JGS2_INVALID_ARGUMENT, "count is NULL.");
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  st = checkBroadPhase(s);
+  if (st != JGS2_OK) return st;
+  const SceneHost& sc = s->scenes[0];
+  const uint4* list = s->b.contactIdx;
+  uint64_t n = sc.KC;
+  uint64_t first = sc.kOff;
+  if (s->dynamic) {
+    // The last iteration's list: the one its iteration count's parity picks.
+    const uint32_t it = sc.submittedIterations;
+    list = s->dynIdx[it ? static_cast<int>((it - 1) & 1u) : 0];
+    uint32_t total = 0;
+    CUDA_TRY(s, cudaMemcpy(&total, s->b.bpStatus, sizeof(total), cudaMemcpyDeviceToHost));
+    n = sc.submittedIterations ? total : 0u;
+    first = 0;
+  }
+  *count = n;
+  if (!out || n == 0) return JGS2_OK;
+  if (capacity < n) return fail(s, JGS2_INVALID_ARGUMENT, "out holds fewer candidates than were listed.");
+  std::vector<uint4> host(n);
+  CUDA_TRY(s, cudaMemcpy(host.data(), list + first, sizeof(uint4) * n, cudaMemcpyDeviceToHost));
+  for (uint64_t c = 0; c < n; ++c) {
+    out[4 * c] = host[c].x - sc.vOff;
+    out[4 * c + 1] = host[c].y - sc.vOff;
+    out[4 * c + 2] = host[c].z - sc.vOff;
+    out[4 * c + 3] = ((host[c].w & 0x7fffffffu) - sc.vOff) | (host[c].w & 0x80000000u);
+  }
   return JGS2_OK;
 }
 
@@ -2128,7 +2566,7 @@ jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* s, const float* source, co
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
   if (!s->glob) return fail(s, JGS2_UNSUPPORTED, "The assembled gate requires stable globalization.");
-  if (s->KC > 0)
+  if (s->KC > 0 || s->dynamic)
     return fail(s, JGS2_UNSUPPORTED,
                 "The no-allocation gate does not evaluate IPC contact energies; use "
                 "jgs2_evaluate_assembled_candidate for solvers with contact candidates.");
@@ -2342,7 +2780,16 @@ uint64_t jgs2_estimate_device_bytes(const jgs2_input* in) {
   // IPC: per candidate its indices, scene, 7 float4 of state and four
   // incidence and four active entries; per vertex a range and an active count.
   const uint64_t KC = uint64_t(in->contact_vertex_triangle_count) + in->contact_edge_edge_count;
-  const uint64_t contact = KC ? KC * (16 + 4 + 112 + 32) + V * 12 : 0;
+  uint64_t contact = KC ? KC * (16 + 4 + 112 + 32) + V * 12 : 0;
+  if (const jgs2_contact_surface* cs = in->contact_surface) {
+    // Broad phase: two lists of capacity candidates (indices, scene, state,
+    // flag, column) and the sort's four entry buffers; surface data, boxes
+    // and rows per triangle and edge (at most three edges per triangle).
+    const uint64_t E = 3ull * cs->triangle_count;
+    const uint64_t cap = cs->candidate_capacity ? cs->candidate_capacity : std::max<uint64_t>(4096, 64 * (V + E));
+    contact = 2 * cap * (16 + 4 + 112 + 4 + 4) + 4 * cap * 16 + cs->triangle_count * (16 + 32) + E * (8 + 32 + 32) +
+              V * (8 + 16 + 8 + 8 + 4 + 16) + (4 * cap / 4096 + 1) * 1024;
+  }
   return V * (16 * 20 + 12) + V * K * (32 + 144) + T * (64 + 16 + 1) + cloth + contact + (1u << 16);
 }
 

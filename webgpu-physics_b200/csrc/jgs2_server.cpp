@@ -34,7 +34,8 @@ struct OwnedInput {
   std::vector<float> cubW, cubBasis;
   std::vector<uint32_t> info, tets, adjacency, cubTet;
   jgs2_cloth_input cloth{};
-  std::vector<uint32_t> clothTris, hinges, contacts;
+  std::vector<uint32_t> clothTris, hinges, contacts, surfaceTris;
+  jgs2_contact_surface surface{};
   std::vector<float> clothInv, clothAreas, hingeAngles, hingeLengths;
 
   template <class T>
@@ -77,6 +78,11 @@ struct OwnedInput {
     }
     view.contact_indices = take(contacts, in.contact_indices,
                                 4 * (size_t(in.contact_vertex_triangle_count) + in.contact_edge_edge_count));
+    if (in.contact_surface) {
+      surface = *in.contact_surface;
+      surface.triangles = take(surfaceTris, surface.triangles, 3 * size_t(surface.triangle_count));
+      view.contact_surface = &surface;
+    }
   }
 };
 

@@ -676,9 +676,16 @@ int64_t jgs2_build_static_contact_candidates(uint32_t vertex_count, const uint32
   return static_cast<int64_t>(n);
 }
 
-jgs2_status jgs2_scene_set_contact(jgs2_scene* s, uint32_t enabled) {
+jgs2_status jgs2_scene_set_contact(jgs2_scene* s, uint32_t mode) {
   if (!s) return JGS2_INVALID_ARGUMENT;
-  s->contact = enabled != 0;
+  if (mode > JGS2_SCENE_CONTACT_SURFACE) return fail(s, "Unknown contact mode."), JGS2_INVALID_ARGUMENT;
+  s->contact = mode;
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_scene_set_contact_capacity(jgs2_scene* s, uint64_t capacity) {
+  if (!s) return JGS2_INVALID_ARGUMENT;
+  s->contactCapacity = capacity;
   return JGS2_OK;
 }
 
@@ -879,7 +886,8 @@ jgs2_status jgs2_scene_pack(jgs2_scene* s, jgs2_input* out) {
   // (surfaceWithCloth, precompute.ts:98-140; buildStaticIpcContactCandidates).
   s->packContact.clear();
   s->packContactVT = s->packContactEE = 0;
-  if (s->contact) {
+  s->packSurface.clear();
+  if (s->contact != JGS2_SCENE_CONTACT_NONE) {
     std::vector<std::array<uint32_t, 3>> surface;
     std::string err;
     if (!boundaryTriangles(m, &surface, &err)) return fail(s, err), JGS2_INVALID_ARGUMENT;
@@ -890,13 +898,24 @@ jgs2_status jgs2_scene_pack(jgs2_scene* s, jgs2_input* out) {
         std::sort(t.begin(), t.end());
         surface.push_back(t);
       }
-    staticContactCandidates(V, std::move(surface), &s->packContact, &s->packContactVT, &s->packContactEE);
+    if (s->contact == JGS2_SCENE_CONTACT_STATIC) {
+      staticContactCandidates(V, std::move(surface), &s->packContact, &s->packContactVT, &s->packContactEE);
+    } else {
+      std::sort(surface.begin(), surface.end());
+      surface.erase(std::unique(surface.begin(), surface.end()), surface.end());
+      for (const auto& t : surface) s->packSurface.insert(s->packSurface.end(), t.begin(), t.end());
+      s->packSurfaceRec = jgs2_contact_surface{};
+      s->packSurfaceRec.triangle_count = static_cast<uint32_t>(surface.size());
+      s->packSurfaceRec.triangles = s->packSurface.data();
+      s->packSurfaceRec.candidate_capacity = s->contactCapacity;
+    }
   }
   std::memset(out, 0, sizeof(*out));
   out->cloth = cloth ? &s->packCloth : nullptr;
   out->contact_indices = s->packContact.empty() ? nullptr : s->packContact.data();
   out->contact_vertex_triangle_count = s->packContactVT;
   out->contact_edge_edge_count = s->packContactEE;
+  out->contact_surface = s->contact == JGS2_SCENE_CONTACT_SURFACE ? &s->packSurfaceRec : nullptr;
   out->vertex_count = V;
   out->tet_count = T;
   out->cubature_k = K;

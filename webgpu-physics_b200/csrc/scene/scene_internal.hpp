@@ -82,9 +82,12 @@ struct Scene {
   std::vector<float> packClothInverse, packClothAreas, packHingeAngles, packHingeLengths;
   jgs2_cloth_input packCloth{};
   // Static IPC candidates over the boundary surface (tets) and the cloth.
-  bool contact = false;
+  uint32_t contact = 0;  // JGS2_SCENE_CONTACT_*
+  uint64_t contactCapacity = 0;
   std::vector<uint32_t> packContact;
   uint32_t packContactVT = 0, packContactEE = 0;
+  std::vector<uint32_t> packSurface;
+  jgs2_contact_surface packSurfaceRec{};
 };
 
 // ---- small dense helpers (row-major 3x3) ---------------------------------

@@ -42,6 +42,13 @@ class ClothInput(Structure):
     ]
 
 
+class ContactSurface(Structure):
+    _fields_ = [
+        ("triangle_count", c_uint32), ("reserved0", c_uint32),
+        ("triangles", POINTER(c_uint32)), ("candidate_capacity", c_uint64),
+    ]
+
+
 class Input(Structure):
     _fields_ = [
         ("vertex_count", c_uint32), ("tet_count", c_uint32),
@@ -62,6 +69,7 @@ class Input(Structure):
         ("contact_indices", POINTER(c_uint32)),
         ("contact_vertex_triangle_count", c_uint32),
         ("contact_edge_edge_count", c_uint32),
+        ("contact_surface", POINTER(ContactSurface)),
     ]
 
 
@@ -99,7 +107,7 @@ class Info(Structure):
         ("last_submitted_iterations", c_uint32), ("history_count", c_uint32),
         ("scene_scale", c_float), ("preprocessing_timestep", c_float),
         ("current_position_buffer", c_uint32), ("cloth_triangle_count", c_uint32),
-        ("contact_candidate_count", c_uint32), ("reserved1", c_uint32),
+        ("contact_candidate_count", c_uint32), ("contact_candidate_capacity", c_uint32),
     ]
 
 
@@ -195,6 +203,7 @@ def scene_lib() -> ctypes.CDLL:
         lib.jgs2_scene_cloth_triangle_count.restype = c_uint32
         lib.jgs2_scene_set_rest_positions.argtypes = [c_void_p, POINTER(c_double)]
         lib.jgs2_scene_set_contact.argtypes = [c_void_p, c_uint32]
+        lib.jgs2_scene_set_contact_capacity.argtypes = [c_void_p, c_uint64]
         lib.jgs2_build_static_contact_candidates.argtypes = [c_uint32, POINTER(c_uint32), c_uint32,
                                                              POINTER(c_uint32), c_uint64, POINTER(c_uint32),
                                                              POINTER(c_uint32)]
@@ -261,6 +270,8 @@ def step_lib() -> ctypes.CDLL:
                                                 POINTER(c_float), POINTER(c_float),
                                                 c_size_t, POINTER(c_uint32)]
         lib.jgs2_device_positions.argtypes = [vp, POINTER(c_void_p), POINTER(c_void_p)]
+        lib.jgs2_read_contact_candidates.argtypes = [vp, POINTER(c_uint32), c_uint64, POINTER(c_uint64)]
+        lib.jgs2_minimum_contact_distance.argtypes = [POINTER(Input), c_double, POINTER(c_double)]
         lib.jgs2_evaluate_assembled_candidate.argtypes = [vp, POINTER(c_float), POINTER(c_float), S, c_uint32,
                                                           POINTER(c_float), POINTER(c_float), POINTER(c_float)]
         lib.jgs2_kernel_launch_count.argtypes = [vp]

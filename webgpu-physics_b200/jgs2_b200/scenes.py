@@ -23,6 +23,7 @@ MATERIAL_COROTATED_LINEAR = 0
 MATERIAL_STABLE_NEO_HOOKEAN = 1
 PRECOMPUTE_EXACT = 0
 PRECOMPUTE_PATCH = 1
+CONTACT_NONE, CONTACT_STATIC, CONTACT_SURFACE = 0, 1, 2
 FACE_X_MIN, FACE_X_MAX, FACE_Y_MIN, FACE_Y_MAX, FACE_Z_MIN, FACE_Z_MAX = (
     1, 2, 4, 8, 16, 32)
 EMPTY_TET = 0xFFFFFFFF
@@ -82,6 +83,10 @@ class SceneInput:
     # and their counts (vertex-triangle, edge-edge).
     contact_indices: Optional[np.ndarray] = None       # uint32
     contact_counts: Optional[np.ndarray] = None        # uint32 (vt, ee)
+    # Contact surface for the device broad phase instead (3 indices per
+    # triangle) and its per-iteration candidate capacity (0: the default).
+    contact_surface: Optional[np.ndarray] = None       # uint32
+    contact_capacity: int = 0
     stats: Optional[dict] = None
 
     @property
@@ -143,8 +148,15 @@ class SceneInput:
             rec.contact_indices = _ffi.uptr(self.contact_indices)
             rec.contact_vertex_triangle_count = int(self.contact_counts[0])
             rec.contact_edge_edge_count = int(self.contact_counts[1])
-        # Keep the arrays (and the cloth record) alive as long as the record.
-        rec._owner = (self, cloth)  # type: ignore[attr-defined]
+        surface = None
+        if self.contact_surface is not None:
+            surface = _ffi.ContactSurface()
+            surface.triangle_count = self.contact_surface.size // 3
+            surface.triangles = _ffi.uptr(self.contact_surface)
+            surface.candidate_capacity = int(self.contact_capacity)
+            rec.contact_surface = ctypes.pointer(surface)
+        # Keep the arrays (and the cloth / surface records) alive as long as the record.
+        rec._owner = (self, cloth, surface)  # type: ignore[attr-defined]
         return rec
 
     def copy(self) -> "SceneInput":
@@ -304,8 +316,13 @@ class Scene:
         if status != 0:
             raise _ffi.JGS2Error(status, self._error())
 
-    def set_contact(self, enabled=True):
-        self._lib.jgs2_scene_set_contact(self._h, 1 if enabled else 0)
+    def set_contact(self, enabled=True, capacity=0):
+        """True (or CONTACT_STATIC): static candidates; CONTACT_SURFACE: the
+        surface for the device broad phase, listing at most `capacity`
+        candidates an iteration (0: the default); False: no contact."""
+        mode = CONTACT_STATIC if enabled is True else (CONTACT_NONE if enabled is False else int(enabled))
+        self._lib.jgs2_scene_set_contact(self._h, mode)
+        self._lib.jgs2_scene_set_contact_capacity(self._h, int(capacity))
 
     def set_pinned(self, pinned):
         pin = np.ascontiguousarray(pinned, dtype=np.uint8)
@@ -392,6 +409,10 @@ class Scene:
             contact = dict(contact_indices=f(rec.contact_indices, 4 * nc),
                            contact_counts=np.array([rec.contact_vertex_triangle_count,
                                                     rec.contact_edge_edge_count], dtype=np.uint32))
+        if rec.contact_surface:
+            cs = rec.contact_surface.contents
+            contact = dict(contact_surface=f(cs.triangles, 3 * cs.triangle_count),
+                           contact_capacity=int(cs.candidate_capacity))
         return SceneInput(
             **cloth, **contact,
             vertex_count=V, tet_count=T, cubature_k=K,
@@ -523,7 +544,8 @@ TROUGH_SETTINGS = dict(timestep=1 / 60, gravity=(0.0, -9.81, 0.0), floorHeight=-
                        ipcStepSafety=0.9, regularization=1e-6, rotationEpsilon=1e-7, maxStep=0.075)
 
 
-def trough(boxes=10, cubature_k=6, timestep=1 / 60, method=PRECOMPUTE_EXACT) -> SceneInput:
+def trough(boxes=10, cubature_k=6, timestep=1 / 60, method=PRECOMPUTE_EXACT, contact=CONTACT_STATIC,
+           capacity=0) -> SceneInput:
     """IPC box trough (troughDefinition, src/scenes/index.ts:551-630): a
     pinned two-cell solid warped into a V (y = 0.05 + 0.65|x| - 0.18(1 - layer))
     and `boxes` one-cell stable Neo-Hookean boxes (0.46 m) stacked four per
@@ -546,9 +568,76 @@ def trough(boxes=10, cubature_k=6, timestep=1 / 60, method=PRECOMPUTE_EXACT) -> 
         q += np.array([-0.37 if slot % 2 == 0 else 0.37, 2.15 + 0.72 * lay, -0.38 if slot < 2 else 0.38])
         p[s:s + 8] = q
     sc.set_rest_positions(p)
-    sc.set_contact(True)
+    sc.set_contact(contact, capacity)
     stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=method)
     inp = sc.pack()
+    inp.stats = stats
+    return inp
+
+
+# Settings of the box trough: the trough's contact parameters with the
+# activation distance 1e-3 m, friction 0.3 and 15 iterations; the minimum
+# distance (1e-4 m, below the activation distance) and the per-iteration step
+# bound (0.02 m, room for 9 m/s at 15 iterations per 1/60 s frame) are this
+# workload's choices.
+BOX_TROUGH_SETTINGS = dict(TROUGH_SETTINGS, iterations=15, ipcActivationDistance=1e-3, ipcMinimumDistance=1e-4,
+                           ipcFrictionCoefficient=0.3, maxStep=0.02)
+
+
+def box_trough(boxes=20, cells=8, box_size=0.3, heights=(1.0, 3.0), seed=3003, young=2e5, poisson=0.4,
+               density=1000.0, plate_cells=(16, 4), plate_thickness=0.04, cubature_k=6, timestep=1 / 60,
+               method=PRECOMPUTE_PATCH, contact=CONTACT_SURFACE, capacity=0, threads=0) -> SceneInput:
+    """IPC box trough: `boxes` stable Neo-Hookean boxes of cells^3 hexes x6
+    tets (edge `box_size`), dropped from seeded heights U[heights] and yaws
+    U[0, 2 pi) into a pinned V-trough of two 4 x 1 m plates at +-45 degrees
+    (plate_cells along the trough and down the slope, one cell thick, inner
+    edges 1 cm apart at the apex).  Placement (Mulberry32): x U[-0.25, 0.25],
+    z within the trough, redrawn until the boxes' bounding spheres are 1 cm
+    apart.  Contact over the whole boundary surface."""
+    sc = Scene()
+    m_plate = sc.add_material(1000.0, 1.2e5, 0.34, MATERIAL_STABLE_NEO_HOOKEAN)
+    m_box = sc.add_material(density, young, poisson, MATERIAL_STABLE_NEO_HOOKEAN)
+    t = plate_thickness
+    plates = [sc.add_cuboid((plate_cells[1], 1, plate_cells[0]), (0.0, 0.0, -2.0), (1.0, t, 4.0), m_plate, 0, 63)
+              for _ in range(2)]
+    starts = [sc.add_cuboid((cells, cells, cells), (-box_size / 2,) * 3, (box_size,) * 3, m_box, i + 1, 0)
+              for i in range(boxes)]
+    p = sc.rest_positions()
+    n_plate = plates[1] - plates[0]
+    c = s_ = math.sqrt(0.5)
+    gap = 0.005
+    for side, base in ((1.0, plates[0]), (-1.0, plates[1])):
+        q = p[base:base + n_plate].copy()
+        # Top face (local y = t) on the line from (side * gap, 0) at 45 degrees;
+        # the plate's thickness lies outside the trough.
+        ux, uy, nx, ny = side * c, s_, -side * s_, c
+        x, y = q[:, 0], q[:, 1] - t
+        p[base:base + n_plate, 0] = side * gap + x * ux + y * nx
+        p[base:base + n_plate, 1] = x * uy + y * ny
+    rand = mulberry32(seed)
+    radius = box_size * math.sqrt(3.0) / 2
+    centres = []
+    n_box = cells + 1
+    for i, start in enumerate(starts):
+        for _attempt in range(10000):
+            yaw = 2 * math.pi * rand()
+            height = heights[0] + (heights[1] - heights[0]) * rand()
+            x = -0.25 + 0.5 * rand()
+            z = -2.0 + radius + (4.0 - 2 * radius) * rand()
+            ctr = np.array([x, height, z])
+            clear = (height - abs(x)) / math.sqrt(2.0) > radius + 0.01
+            if clear and all(np.linalg.norm(ctr - o) > 2 * radius + 0.01 for o in centres):
+                break
+        else:
+            raise ValueError("box_trough could not place the boxes apart; lower the count or widen the heights")
+        centres.append(ctr)
+        q = rotate_euler_xyz(p[start:start + n_box ** 3], 0.0, yaw, 0.0)
+        p[start:start + n_box ** 3] = q + ctr
+    sc.set_rest_positions(p)
+    sc.set_contact(contact, capacity)
+    stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=method, threads=threads)
+    inp = sc.pack()
+    stats["centres"] = [c_.tolist() for c_ in centres]
     inp.stats = stats
     return inp
 

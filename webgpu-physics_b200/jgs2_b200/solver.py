@@ -12,6 +12,7 @@ the reference throws RangeError/TypeError this raises `JGS2RangeError`
 from __future__ import annotations
 
 import ctypes
+import dataclasses
 from ctypes import byref, c_float, c_uint32, c_void_p
 from typing import Optional
 
@@ -112,6 +113,22 @@ def build_vertex_coloring(scene_input):
     if st != 0:
         _raise(st, L.jgs2_global_last_error().decode())
     return colors, int(count.value)
+
+
+def minimum_contact_distance(scene_input, positions=None, cutoff=1.0) -> float:
+    """The exact (double) minimum distance over the scene's IPC candidates at
+    `positions` (4 floats per vertex; default the input's), restricted for a
+    contact surface to pairs whose boxes come within `cutoff` (inf if none)."""
+    L = _ffi.step_lib()
+    inp = scene_input
+    if positions is not None:
+        inp = dataclasses.replace(scene_input, positions=np.ascontiguousarray(positions, dtype=np.float32).reshape(-1))
+    rec = inp.as_ctypes()
+    out = ctypes.c_double(0.0)
+    st = L.jgs2_minimum_contact_distance(byref(rec), float(cutoff), byref(out))
+    if st != 0:
+        _raise(st, L.jgs2_global_last_error().decode())
+    return float(out.value)
 
 
 def validate_input(scene_input):
@@ -314,6 +331,21 @@ class JGS2GpuSolver:
         out = np.empty(per_vertex * self.vertexCount, dtype=np.float32)
         self._check(fn(self._h, _ffi.fptr(out), out.size))
         return out
+
+    @property
+    def contactCandidateCount(self) -> int:
+        """Static candidates, or the broad phase's listing of the last iteration."""
+        return self.info()["contact_candidate_count"]
+
+    def readContactCandidates(self) -> np.ndarray:
+        """The IPC candidates of the last iteration, (n, 4) uint32 in
+        canonical order (vertex-triangle rows first)."""
+        self._usable()
+        n = ctypes.c_uint64(0)
+        self._check(self._L.jgs2_read_contact_candidates(self._h, None, 0, ctypes.byref(n)))
+        out = np.zeros(4 * max(n.value, 1), dtype=np.uint32)
+        self._check(self._L.jgs2_read_contact_candidates(self._h, _ffi.uptr(out), n.value, ctypes.byref(n)))
+        return out[:4 * n.value].reshape(-1, 4)
 
     def readPositions(self, out: Optional[np.ndarray] = None) -> np.ndarray:
         """Positions (4 floats per vertex); `out` may be a caller-owned
