@@ -48,12 +48,15 @@ def parse_args():
                     help="iterations per frame (default 20 for the cube, 10 for the batched bodies)")
     ap.add_argument("--schedule", default="jacobi", choices=["jacobi", "graph-colored-gauss-seidel"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cube", choices=["cube", "batched", "serving", "trough", "cloth"],
+    ap.add_argument("--workload", default="cube", choices=["cube", "batched", "serving", "trough", "boxes", "cloth"],
                     help="cube: one large body (headline); batched: independent uneven bodies in one batch; "
                          "serving: a Poisson stream of step requests through the continuous-batching loop; "
-                         "trough: the reference's IPC box trough; cloth: the 128x128 StVK sheet")
-    ap.add_argument("--boxes", type=int, default=10, help="boxes of the trough workload")
+                         "trough: the reference's IPC box trough; boxes: twenty 8^3-hex boxes in the V-trough "
+                         "through the device broad phase; cloth: the 128x128 StVK sheet")
+    ap.add_argument("--boxes", type=int, default=None, help="boxes of the trough (10) or boxes (20) workload")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serving workload")
+    ap.add_argument("--preroll", type=int, default=None,
+                    help="untimed frames before the timed ones (trough 96, boxes 60, cloth the warm-up)")
     ap.add_argument("--bodies", type=int, default=256, help="scenes of the batched workload")
     args = ap.parse_args()
     if args.iterations is None:
@@ -701,7 +704,10 @@ def scene_arm(args):
     torch.cuda.set_device(local)
     device = local
     t0 = time.perf_counter()
+    exact = None  # iterations per frame when the workload fixes them
+    check = None  # exact contact distances of the run (intersection check)
     if args.workload == "trough":
+        args.boxes = 10 if args.boxes is None else args.boxes
         inp = scenes.trough(args.boxes)
         settings = dict(scenes.TROUGH_SETTINGS)
         preroll = 96
@@ -709,6 +715,20 @@ def scene_arm(args):
                 f"({inp.vertex_count} vertices, {inp.tet_count} tets, {inp.contact_candidate_count} static "
                 f"VT/EE candidates), the reference app's IPC settings (dHat 0.08, dMin 0.003, kappa 1e5, "
                 f"mu 0.45, maxStep 0.075), production step of 3 iterations at dt=1/60, after a 96-frame pre-roll")
+    elif args.workload == "boxes":
+        args.boxes = 20 if args.boxes is None else args.boxes
+        inp = scenes.box_trough(boxes=args.boxes)
+        settings = dict(scenes.BOX_TROUGH_SETTINGS)
+        exact = settings["iterations"]
+        preroll = 60 if args.preroll is None else args.preroll
+        check = []
+        what = (f"IPC box trough: {args.boxes} stable Neo-Hookean boxes of 8^3 hexes x6 tets (0.46 m, E=2e5, "
+                f"nu=0.4, rho=7800), seeded heights U[1,3] m and yaws, dropped into a pinned V-trough of two "
+                f"4x1 m plates at +-45 degrees ({inp.vertex_count} vertices, {inp.tet_count} tets, K="
+                f"{inp.cubature_k} exact-complement records); IPC over the boundary surface through the device "
+                f"broad phase (static superset {solver.contact_superset_size(inp)} candidates never listed), "
+                f"dHat 1e-3, dMin 1e-4, kappa 1e5, mu 0.3, maxStep 0.02; {exact} exact Jacobi iterations per "
+                f"frame at dt=1/60, timed after a {preroll}-frame pre-roll (the first boxes reach the trough)")
     else:
         inp = scenes.cloth_sheet()
         settings = dict(timestep=1 / 120, gravity=(0.0, -9.81, 0.0), floorStiffness=0.0, iterations=5,
@@ -718,12 +738,22 @@ def scene_arm(args):
         what = (f"StVK cloth sheet 128x128 ({inp.vertex_count} vertices, {inp.cloth_triangle_count} triangles, "
                 f"{inp.hinge_count} hinges; E=1e4, bending 1e-3, two corners pinned) over a pinned box collider, "
                 f"production step of 5 iterations at dt=1/120")
+    if args.preroll is not None:
+        preroll = args.preroll
     build_s = time.perf_counter() - t0
     s = solver.JGS2GpuSolver.create(inp, settings, device=device)
     _ptr, stream_ptr = s.devicePositions()
     stream = torch.cuda.ExternalStream(stream_ptr, device=device)
-    for _ in range(max(preroll, args.warmup)):
-        s.step()
+    def frame():
+        if exact is None:
+            s.step()
+        else:
+            s.stepExactIterations(exact)
+
+    for f in range(max(preroll, args.warmup)):
+        frame()
+        if check is not None and (f + 1) % 40 == 0:
+            check.append(solver.minimum_contact_distance(inp, s.readPositions(), cutoff=0.05))
     s.awaitIdle()
     iters = s.lastSubmittedIterationCount
     active = inp.active_vertex_count()
@@ -736,7 +766,7 @@ def scene_arm(args):
     with ClockSampler(device) as clocks:
         start_ev.record(stream)
         for _ in range(args.steps):
-            s.step()
+            frame()
         end_ev.record(stream)
         end_ev.synchronize()
     ms = max_over_ranks(dist, start_ev.elapsed_time(end_ev), f"cuda:{device}")
@@ -751,9 +781,12 @@ def scene_arm(args):
     t_e2e = time.perf_counter()
     for _ in range(e2e_steps):
         s.replaceExternalForces(f_np)
-        s.step()
+        frame()
         s.readPositions(out=p_np)
     e2e_total = max_over_ranks(dist, time.perf_counter() - t_e2e, f"cuda:{device}")
+    listed = s.contactCandidateCount if (inp.contact_surface is not None) else None
+    if check is not None:
+        check.append(solver.minimum_contact_distance(inp, s.readPositions(), cutoff=0.05))
     s.destroy()
     if rank == 0:
         ref = None
@@ -774,6 +807,11 @@ def scene_arm(args):
             "reference_published": ref,
             "gpu_launches": int(launches),
             "kernel_ms_per_frame": {k: v[1] / max(1, min(args.steps, 5)) for k, v in prof.items() if v[0]},
+            "contact": None if check is None else {
+                "listed_candidates_last_iteration": listed,
+                "minimum_distance_every_40_frames": check,
+                "intersection_free": bool(min(check) > settings["ipcMinimumDistance"]),
+                "frames": max(preroll, args.warmup) + args.steps + e2e_steps},
             "roofline": None,
             "cpu_baseline": None,
             "e2e": {"value": whole_job_rate(world, active * iters * e2e_steps, e2e_total), "unit": UNIT,
@@ -795,7 +833,7 @@ def main():
         return batched_arm(args)
     if args.workload == "serving":
         return serving_arm(args)
-    if args.workload in ("trough", "cloth"):
+    if args.workload in ("trough", "boxes", "cloth"):
         return scene_arm(args)
     return ours_arm(args)
 

@@ -263,6 +263,10 @@ jgs2_status jgs2_validate_input(const jgs2_input* input);
  * of a contact run: feed it the positions read back after each frame. */
 jgs2_status jgs2_minimum_contact_distance(const jgs2_input* input, double cutoff, double* distance);
 
+/* Candidates of the static superset of input->contact_surface (what
+ * buildStaticIpcContactCandidates would list), counted without listing. */
+jgs2_status jgs2_contact_superset_size(const jgs2_input* input, uint64_t* count);
+
 /* buildJGS2InputVertexColoring + buildGreedyVertexColoring
  * (src/simulation/gpu/jgs2-solver.ts:308-367;
  *  src/simulation/cpu/vertex-coloring.ts:20-110).  colors has V entries. */

@@ -25,7 +25,7 @@ D_HAT = 0.08
 
 
 def _small(contact, **kw):
-    args = dict(boxes=3, cells=3, heights=(0.8, 1.0), plate_cells=(8, 2), method=scenes.PRECOMPUTE_PATCH)
+    args = dict(boxes=3, cells=3, heights=(1.0, 1.3), plate_cells=(8, 2), method=scenes.PRECOMPUTE_PATCH)
     args.update(kw)
     return scenes.box_trough(contact=contact, **args)
 
@@ -63,6 +63,9 @@ def test_packed_surface_gives_the_reference_superset():
     cand, vt, ee = scenes.static_contact_candidates(b.vertex_count, b.contact_surface)
     assert (vt, ee) == tuple(int(x) for x in a.contact_counts) and vt + ee == 31801
     np.testing.assert_array_equal(cand, a.contact_indices)
+    assert solver.contact_superset_size(b) == 31801
+    small = _small(scenes.CONTACT_STATIC)
+    assert solver.contact_superset_size(_small(scenes.CONTACT_SURFACE)) == small.contact_candidate_count
 
 
 def test_surface_input_checks():
@@ -152,17 +155,20 @@ def _distance(lib, kind, x):
 
 @pytest.mark.gpu
 def test_box_trough_surface_run_is_the_static_run():
+    # The static superset of this pile needs more than the 256 colours a
+    # solver's create-time colouring allows, so both run as one-scene batches
+    # (which colour only for the coloured schedule).
     static = _small(scenes.CONTACT_STATIC)
     surface = _small(scenes.CONTACT_SURFACE)
     s = scenes.BOX_TROUGH_SETTINGS
-    a = solver.JGS2GpuSolver.create(static, s)
-    b = solver.JGS2GpuSolver.create(surface, s)
+    a = solver.JGS2Batch.create([static], [s])
+    b = solver.JGS2Batch.create([surface], [s])
     for _ in range(4):
-        a.stepFramesExactIterations(10, 15)
-        b.stepFramesExactIterations(10, 15)
-        np.testing.assert_array_equal(b.readPositions(), a.readPositions())
-    assert b.contactCandidateCount > 0
-    d = solver.minimum_contact_distance(surface, b.readPositions(), cutoff=1.0)
+        a.stepFrames(10, exactIterations=15)
+        b.stepFrames(10, exactIterations=15)
+        np.testing.assert_array_equal(b.readPositions(0), a.readPositions(0))
+    assert b.info(0)["contact_candidate_count"] > 0
+    d = solver.minimum_contact_distance(surface, b.readPositions(0), cutoff=1.0)
     assert d > s["ipcMinimumDistance"], d
     a.destroy()
     b.destroy()
@@ -170,7 +176,7 @@ def test_box_trough_surface_run_is_the_static_run():
 
 @pytest.mark.gpu
 def test_box_pile_stays_intersection_free():
-    inp = scenes.box_trough(boxes=6, cells=4, heights=(0.9, 1.6), method=scenes.PRECOMPUTE_PATCH)
+    inp = scenes.box_trough(boxes=6, cells=4, heights=(1.0, 1.6), method=scenes.PRECOMPUTE_PATCH)
     s = scenes.BOX_TROUGH_SETTINGS
     gpu = solver.JGS2GpuSolver.create(inp, s)
     p0 = gpu.readPositions().reshape(-1, 4)[:, :3].copy()
@@ -203,9 +209,9 @@ def test_capacity_overflow_fails_the_step_without_faulting():
 @pytest.mark.gpu
 def test_surface_settings_checks():
     inp = scenes.trough(1, contact=scenes.CONTACT_SURFACE)
-    with pytest.raises(solver.JGS2RangeError, match="Jacobi"):
-        solver.JGS2GpuSolver.create(inp, dict(scenes.TROUGH_SETTINGS, schedule="graph-colored-gauss-seidel"))
     gpu = solver.JGS2GpuSolver.create(inp, scenes.TROUGH_SETTINGS)
+    with pytest.raises(solver.JGS2RangeError, match="Jacobi schedule only"):
+        gpu.step({"schedule": "graph-colored-gauss-seidel"})
     with pytest.raises(solver.JGS2RangeError, match="maxStep must be positive"):
         gpu.step({"maxStep": 0.0})
     gpu.step()

@@ -2095,7 +2095,7 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
   GatePartial acc = gateIdentity();
   // Contacts: element k takes candidates k, k + span, ... of the scene's
   // list (a single pass for static candidates, which the table covers).
-  const uint32_t span = max(max(max(sr.V, sr.T), max(sr.C, sr.H)), max(sr.KC, 1u));
+  const uint32_t span = max(sr.gateSpan, 1u);
   const uint2 contacts = b.contactDynamic ? b.bpSpan[rb.scene] : make_uint2(sr.kOff, sr.KC);
   for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
     if (k < sr.T) {
@@ -2487,13 +2487,12 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   // One vertex per lane group: the line search makes per-vertex work uneven,
   // and the block scheduler balances it better than a fixed grid stride.
   const uint32_t blocks = std::max(1u, (count + groups - 1) / groups);
-  // Contact-heavy engines (more than 64 static candidate incidences per
-  // solved vertex on average, or a broad phase over cloth, whose sheets lie
-  // within the barrier reach of many of their own triangles): a whole warp
-  // per vertex over its active candidates.
-  const bool heavy = b.contactDynamic ? b.clothRange != nullptr
-                                      : uint64_t(b.contactCount) * 4u > uint64_t(64) * count;
-  if (b.contactIdx && heavy) {
+  // Contact-heavy engines (more than 64 candidate incidences of the static
+  // superset per solved vertex on average, listed or not): a whole warp per
+  // vertex over its active candidates.  A broad-phase engine decides on the
+  // superset too, so it runs the variant its static twin runs.
+  const uint64_t superset = b.contactDynamic ? b.bpSuperset : b.contactCount;
+  if (b.contactIdx && superset * 4u > uint64_t(64) * count) {
     const uint32_t wg = std::max(1u, std::min(groups * kGroup / 32u, kBlock / 32u));
     const size_t wsmem = static_cast<size_t>(wg) * K * sizeof(CubState);
     solveKernel<32, true><<<std::max(1u, (count + wg - 1) / wg), wg * 32, wsmem, s>>>(

@@ -48,6 +48,9 @@ struct SceneRange {
   uint32_t cOff, C, hOff, H;      // cloth triangles and hinges of this scene
   uint32_t kOff, KC;              // static IPC candidates of this scene
   uint32_t rowOff, rowCount;      // broad-phase rows of this scene (contact surface)
+  // Elements one pass of the scene's gate blocks covers (the table's range);
+  // broad-phase candidates beyond it stride over the same blocks.
+  uint32_t gateSpan, pad[3];
 };
 
 // One block of a segmented reduction: elements [begin, end) of `scene`,
@@ -154,7 +157,9 @@ struct Buffers {
   // count asked for, this iteration's overflow); the sort's key / value
   // ping-pong buffers and tile histograms.
   uint32_t contactDynamic;
-  uint32_t bpRowTotal, bpTriTotal, bpEdgeTotal, bpSentinel, bpSortPasses, bpPad[2];
+  uint32_t bpRowTotal, bpTriTotal, bpEdgeTotal, bpSentinel, bpSortPasses;
+  uint32_t bpSuperset;  // candidates of the static superset (clamped to 2^32 - 1)
+  uint32_t bpPad;
   const uint4* bpRows;
   const uint4* bpTris;
   const uint2* bpEdges;

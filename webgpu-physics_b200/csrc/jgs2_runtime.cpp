@@ -571,6 +571,7 @@ struct ContactSurface {
   std::vector<uint32_t> ringStart;  // V + 1
   std::vector<uint32_t> ring;
   uint64_t capacity = 0;            // candidates one iteration may list
+  uint64_t superset = 0;            // candidates of the static superset
 };
 
 void buildContactSurface(const jgs2_input* in, ContactSurface* out) {
@@ -607,6 +608,39 @@ void buildContactSurface(const jgs2_input* in, ContactSurface* out) {
   out->capacity = cs->candidate_capacity
                       ? cs->candidate_capacity
                       : std::max<uint64_t>(4096, 64ull * (uint64_t(V) + out->edges.size()));
+  // Size of the superset: per vertex the triangles outside its closed
+  // one-ring, per edge pair those whose endpoints avoid each other's closed
+  // one-rings.
+  const size_t nT = out->tris.size(), nE = out->edges.size();
+  std::vector<std::vector<uint32_t>> vTris(V), vEdges(V);
+  for (uint32_t t = 0; t < nT; ++t)
+    for (uint32_t v : out->tris[t]) vTris[v].push_back(t);
+  for (uint32_t e = 0; e < nE; ++e)
+    for (uint32_t v : out->edges[e]) vEdges[v].push_back(e);
+  std::vector<uint32_t> stamp(std::max(nT, nE), 0xffffffffu);
+  uint64_t vt = 0, closedEdges = 0;
+  auto closedSet = [&](uint32_t v, auto&& visit) {
+    visit(v);
+    for (uint32_t i = out->ringStart[v]; i < out->ringStart[v + 1]; ++i) visit(out->ring[i]);
+  };
+  for (uint32_t v = 0; v < V; ++v) {
+    uint64_t touching = 0;
+    closedSet(v, [&](uint32_t u) {
+      for (uint32_t t : vTris[u])
+        if (stamp[t] != v) { stamp[t] = v; ++touching; }
+    });
+    vt += nT - touching;
+  }
+  std::fill(stamp.begin(), stamp.end(), 0xffffffffu);
+  for (uint32_t e = 0; e < nE; ++e) {
+    auto visit = [&](uint32_t u) {
+      for (uint32_t f : vEdges[u])
+        if (f != e && stamp[f] != e) { stamp[f] = e; ++closedEdges; }
+    };
+    closedSet(out->edges[e][0], visit);
+    closedSet(out->edges[e][1], visit);
+  }
+  out->superset = vt + (uint64_t(nE) * (nE - (nE ? 1 : 0)) / 2 - closedEdges / 2);
 }
 
 // The smallest distance over the superset's candidates whose boxes come
@@ -803,7 +837,7 @@ struct SceneHost {
   // offsets, the scene's rows and its share of the list capacity.
   bool dynamic = false;
   uint32_t bpTris = 0, bpEdges = 0, bpTriOff = 0, bpEdgeOff = 0, bpRowOff = 0, bpRows = 0;
-  uint64_t bpCapacity = 0;
+  uint64_t bpCapacity = 0, bpSuperset = 0;
   // IPC parameters fixed at create (jgs2-solver.ts:1096-1105).
   float ipcMinDistance = 0.f, ipcFriction = 0.f, ipcEpsilon = 0.f, ipcSafety = 0.f;
   float sceneScale = 1.f;
@@ -1156,6 +1190,8 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
       return fail(s, JGS2_INVALID_ARGUMENT, "All scenes of one batched step must use the same schedule.");
     body = body || st[i].horizontal_body_correction != 0;
   }
+  if (s->dynamic && schedule != JGS2_SCHEDULE_JACOBI)
+    return fail(s, JGS2_INVALID_ARGUMENT, "The IPC broad phase steps the Jacobi schedule only.");
   if (schedule == JGS2_SCHEDULE_GRAPH_COLORED_GAUSS_SEIDEL && !s->coloringBuilt)
     return fail(s, JGS2_UNSUPPORTED,
                 "This batch was created without graph colouring: give one of its scenes the graph-coloured "
@@ -1172,8 +1208,6 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
     contact = contact || s->hParams[i].ipc != 0;
   }
   if (s->dynamic && contact) {
-    if (schedule != JGS2_SCHEDULE_JACOBI)
-      return fail(s, JGS2_INVALID_ARGUMENT, "The IPC broad phase steps the Jacobi schedule only.");
     for (uint32_t i = 0; i < s->scenes.size(); ++i)
       if (s->hParams[i].ipc && !(s->hParams[i].maxStep > 0.0f))
         return fail(s, JGS2_INVALID_ARGUMENT,
@@ -1345,10 +1379,8 @@ jgs2_status prepareScene(const jgs2_input* in, const jgs2_settings* settings, ui
   if (in->contact_surface) {
     if (!out->stable)
       return fail(nullptr, JGS2_INVALID_ARGUMENT, "IPC contact requires the stable Neo-Hookean production path.");
-    if (colour)
-      return fail(nullptr, JGS2_INVALID_ARGUMENT,
-                  "The IPC broad phase steps the Jacobi schedule; create a contact-surface scene without the "
-                  "graph-coloured schedule.");
+    // The broad phase steps the Jacobi schedule only: no colouring.
+    colour = false;
     out->dynamic = true;
     buildContactSurface(in, &out->surface);
   }
@@ -1467,6 +1499,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       sc.bpTris = static_cast<uint32_t>(prep[i].surface.tris.size());
       sc.bpEdges = static_cast<uint32_t>(prep[i].surface.edges.size());
       sc.bpCapacity = prep[i].surface.capacity;
+      sc.bpSuperset = prep[i].surface.superset;
     }
     uint32_t maxBody = 0;
     for (uint32_t v = 0; v < sc.V; ++v) maxBody = std::max(maxBody, in->vertex_info[4ull * v + 3]);
@@ -1772,7 +1805,11 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     r.cOff = sc.cOff; r.C = sc.C; r.hOff = sc.hOff; r.H = sc.H;
     r.kOff = sc.kOff; r.KC = sc.KC;
     r.rowOff = sc.bpRowOff; r.rowCount = sc.dynamic ? sc.bpRows : 0u;
-    const uint32_t n = std::max(std::max(std::max(sc.V, sc.T), std::max(sc.C, sc.H)), sc.KC);
+    // A contact-surface scene's gate also takes its listed candidates: the
+    // table covers an eighth of the list capacity, more stride over it.
+    const uint32_t listed = sc.dynamic ? static_cast<uint32_t>(sc.bpCapacity / 8) : 0u;
+    const uint32_t n = std::max(std::max(std::max(sc.V, sc.T), std::max(sc.C, sc.H)), std::max(sc.KC, listed));
+    r.gateSpan = std::max(n, 1u);
     r.gateBase = static_cast<uint32_t>(gateTable.size());
     for (uint32_t b0 = 0; b0 < std::max(n, 1u); b0 += jgs2::kGateChunk)
       gateTable.push_back({i, b0, std::min(n, b0 + jgs2::kGateChunk), static_cast<uint32_t>(gateTable.size())});
@@ -1944,6 +1981,9 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       b.bpEdgeTotal = static_cast<uint32_t>(bpE);
       b.bpSentinel = nV;
       b.bpSortPasses = jgs2::broadPhaseSortPasses(nV);
+      uint64_t superset = 0;
+      for (const SceneHost& sc : sp->scenes) superset += sc.bpSuperset;
+      b.bpSuperset = static_cast<uint32_t>(std::min<uint64_t>(superset, 0xffffffffull));
       uint4* rows = nullptr;
       uint4* tris = nullptr;
       uint2* edges = nullptr;
@@ -2168,6 +2208,17 @@ jgs2_status jgs2_minimum_contact_distance(const jgs2_input* input, double cutoff
     const uint64_t nc = uint64_t(input->contact_vertex_triangle_count) + input->contact_edge_edge_count;
     *distance = nc ? staticContactDistance(input) : INFINITY;
   }
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_contact_superset_size(const jgs2_input* input, uint64_t* count) {
+  std::string err;
+  if (!validateInput(input, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
+  if (!count) return fail(nullptr, JGS2_INVALID_ARGUMENT, "count is NULL.");
+  if (!input->contact_surface) return fail(nullptr, JGS2_INVALID_ARGUMENT, "The input has no contact surface.");
+  ContactSurface cs;
+  buildContactSurface(input, &cs);
+  *count = cs.superset;
   return JGS2_OK;
 }
 

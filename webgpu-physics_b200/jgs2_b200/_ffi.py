@@ -272,6 +272,7 @@ def step_lib() -> ctypes.CDLL:
         lib.jgs2_device_positions.argtypes = [vp, POINTER(c_void_p), POINTER(c_void_p)]
         lib.jgs2_read_contact_candidates.argtypes = [vp, POINTER(c_uint32), c_uint64, POINTER(c_uint64)]
         lib.jgs2_minimum_contact_distance.argtypes = [POINTER(Input), c_double, POINTER(c_double)]
+        lib.jgs2_contact_superset_size.argtypes = [POINTER(Input), POINTER(c_uint64)]
         lib.jgs2_evaluate_assembled_candidate.argtypes = [vp, POINTER(c_float), POINTER(c_float), S, c_uint32,
                                                           POINTER(c_float), POINTER(c_float), POINTER(c_float)]
         lib.jgs2_kernel_launch_count.argtypes = [vp]

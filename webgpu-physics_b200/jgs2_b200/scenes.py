@@ -584,16 +584,27 @@ BOX_TROUGH_SETTINGS = dict(TROUGH_SETTINGS, iterations=15, ipcActivationDistance
                            ipcFrictionCoefficient=0.3, maxStep=0.02)
 
 
-def box_trough(boxes=20, cells=8, box_size=0.3, heights=(1.0, 3.0), seed=3003, young=2e5, poisson=0.4,
-               density=1000.0, plate_cells=(16, 4), plate_thickness=0.04, cubature_k=6, timestep=1 / 60,
-               method=PRECOMPUTE_PATCH, contact=CONTACT_SURFACE, capacity=0, threads=0) -> SceneInput:
+def box_trough(boxes=20, cells=8, box_size=0.46, heights=(1.0, 3.0), seed=3003, young=2e5, poisson=0.4,
+               density=7800.0, plate_cells=(16, 4), plate_thickness=0.04, cubature_k=6, timestep=1 / 60,
+               method=PRECOMPUTE_PATCH, contact=CONTACT_SURFACE, capacity=0, threads=0,
+               exact_complement=True, patch_radius=1) -> SceneInput:
     """IPC box trough: `boxes` stable Neo-Hookean boxes of cells^3 hexes x6
-    tets (edge `box_size`), dropped from seeded heights U[heights] and yaws
-    U[0, 2 pi) into a pinned V-trough of two 4 x 1 m plates at +-45 degrees
-    (plate_cells along the trough and down the slope, one cell thick, inner
-    edges 1 cm apart at the apex).  Placement (Mulberry32): x U[-0.25, 0.25],
-    z within the trough, redrawn until the boxes' bounding spheres are 1 cm
-    apart.  Contact over the whole boundary surface."""
+    tets (edge `box_size`, the reference trough's box), dropped from seeded
+    heights U[heights] and yaws U[0, 2 pi) into a pinned V-trough of two
+    4 x 1 m plates at +-45 degrees (plate_cells along the trough and down the
+    slope, one cell thick, inner edges 1 cm apart at the apex).  Placement
+    (Mulberry32): x U[-0.3, 0.3], z within the trough, redrawn until every
+    pair of boxes is 2 cm apart horizontally (footprint radius edge / sqrt 2)
+    or vertically, and each box clears the plates.  Contact over the whole
+    boundary surface.
+
+    Cubature: by default the patch method's exact complement (every
+    candidate tet within `patch_radius` rings, weight one; K is the largest
+    candidate count).  The density (steel) keeps the step's elastic to
+    inertial ratio E h^2 / (rho cell^2) near 2: fine free bodies far above
+    that (1000 kg/m^3 gives 40 at 8^3 cells), or trained K = `cubature_k`
+    records (exact_complement False), deform in the Jacobi sweep until the
+    assembled gate reverts every pose and the pile stops."""
     sc = Scene()
     m_plate = sc.add_material(1000.0, 1.2e5, 0.34, MATERIAL_STABLE_NEO_HOOKEAN)
     m_box = sc.add_material(density, young, poisson, MATERIAL_STABLE_NEO_HOOKEAN)
@@ -615,18 +626,20 @@ def box_trough(boxes=20, cells=8, box_size=0.3, heights=(1.0, 3.0), seed=3003, y
         p[base:base + n_plate, 0] = side * gap + x * ux + y * nx
         p[base:base + n_plate, 1] = x * uy + y * ny
     rand = mulberry32(seed)
-    radius = box_size * math.sqrt(3.0) / 2
+    foot = box_size / math.sqrt(2.0)  # horizontal reach of a yawed box
     centres = []
     n_box = cells + 1
     for i, start in enumerate(starts):
         for _attempt in range(10000):
             yaw = 2 * math.pi * rand()
             height = heights[0] + (heights[1] - heights[0]) * rand()
-            x = -0.25 + 0.5 * rand()
-            z = -2.0 + radius + (4.0 - 2 * radius) * rand()
+            x = -0.3 + 0.6 * rand()
+            z = -2.0 + foot + (4.0 - 2 * foot) * rand()
             ctr = np.array([x, height, z])
-            clear = (height - abs(x)) / math.sqrt(2.0) > radius + 0.01
-            if clear and all(np.linalg.norm(ctr - o) > 2 * radius + 0.01 for o in centres):
+            clear = height - box_size / 2 > abs(x) + foot + 0.02
+            apart = all(math.hypot(x - o[0], z - o[2]) > 2 * foot + 0.02 or abs(height - o[1]) > box_size + 0.02
+                        for o in centres)
+            if clear and apart:
                 break
         else:
             raise ValueError("box_trough could not place the boxes apart; lower the count or widen the heights")
@@ -635,7 +648,13 @@ def box_trough(boxes=20, cells=8, box_size=0.3, heights=(1.0, 3.0), seed=3003, y
         p[start:start + n_box ** 3] = q + ctr
     sc.set_rest_positions(p)
     sc.set_contact(contact, capacity)
-    stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=method, threads=threads)
+    if exact_complement:
+        args = dict(timestep=timestep, method=method, threads=threads, patch_radius=patch_radius, exact_complement=1)
+        stats = sc.precompute(cubature_k=4096, **args)
+        stats = sc.precompute(cubature_k=max(1, stats["max_records_per_vertex"]), **args)
+    else:
+        stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=method, threads=threads,
+                              patch_radius=patch_radius)
     inp = sc.pack()
     stats["centres"] = [c_.tolist() for c_ in centres]
     inp.stats = stats

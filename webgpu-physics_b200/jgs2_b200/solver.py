@@ -131,6 +131,17 @@ def minimum_contact_distance(scene_input, positions=None, cutoff=1.0) -> float:
     return float(out.value)
 
 
+def contact_superset_size(scene_input) -> int:
+    """Candidates of the static superset of the input's contact surface."""
+    L = _ffi.step_lib()
+    rec = scene_input.as_ctypes()
+    out = ctypes.c_uint64(0)
+    st = L.jgs2_contact_superset_size(byref(rec), byref(out))
+    if st != 0:
+        _raise(st, L.jgs2_global_last_error().decode())
+    return int(out.value)
+
+
 def validate_input(scene_input):
     L = _ffi.step_lib()
     rec = scene_input.as_ctypes()
