@@ -730,14 +730,16 @@ def scene_arm(args):
                 f"dHat 1e-3, dMin 1e-4, kappa 1e5, mu 0.3, maxStep 0.02; {exact} exact Jacobi iterations per "
                 f"frame at dt=1/60, timed after a {preroll}-frame pre-roll (the first boxes reach the trough)")
     else:
-        inp = scenes.cloth_sheet()
-        settings = dict(timestep=1 / 120, gravity=(0.0, -9.81, 0.0), floorStiffness=0.0, iterations=5,
-                        velocityDamping=0.997, contactTangentialDamping=0.0, horizontalBodyCorrection=False,
-                        maxStep=0.01)
-        preroll = args.warmup
-        what = (f"StVK cloth sheet 128x128 ({inp.vertex_count} vertices, {inp.cloth_triangle_count} triangles, "
-                f"{inp.hinge_count} hinges; E=1e4, bending 1e-3, two corners pinned) over a pinned box collider, "
-                f"production step of 5 iterations at dt=1/120")
+        inp = scenes.cloth_sphere()
+        settings = dict(scenes.CLOTH_SETTINGS)
+        preroll = args.warmup if args.preroll is None else args.preroll
+        check = []
+        what = (f"StVK cloth sheet 128x128 ({inp.vertex_count} vertices with the sphere, "
+                f"{inp.cloth_triangle_count} triangles, {inp.hinge_count} hinges; E=1e4, bending 1e-3, two corners "
+                f"pinned) draping over a fixed sphere of radius 0.3 m, IPC self-contact and sphere contact through "
+                f"the device broad phase (static superset {solver.contact_superset_size(inp)} candidates never "
+                f"listed; dHat 0.01, dMin 0.003, kappa 1e5, mu 0.3, maxStep 0.01), production step of 5 "
+                f"iterations at dt=1/120")
     if args.preroll is not None:
         preroll = args.preroll
     build_s = time.perf_counter() - t0

@@ -889,6 +889,7 @@ __global__ void __launch_bounds__(kBlock) contactPromoteKernel(Buffers b, const 
 // row keeps ascending candidate order, as the static rows do.
 
 constexpr uint32_t kBpChunk = 32;
+constexpr uint32_t kBpClosedMax = 64;  // closed one-ring vertices a row keeps in shared memory
 constexpr float kBpInf = __builtin_huge_valf();
 
 struct BpBox {
@@ -1016,85 +1017,108 @@ __global__ void __launch_bounds__(kBlock) bpBoxesKernel(Buffers b, const DevPara
     return;
   }
   const uint32_t v = (blk - triBlocks - edgeBlocks) * kBlock + threadIdx.x;
-  if (v < V) b.activeCount[v] = 0u;
+  if (v >= V) return;
+  b.activeCount[v] = 0u;
+  // ipcCandidatePinnedMotionExceedsBound per vertex (contactPinnedMotion).
+  uint32_t move = 0u;
+  if (isPinned(b.vinfo[v])) {
+    const DevParams& p = pp[b.vertexScene[v]];
+    const float3 d = xyz(b.restMass[v]) - xyz(src[v]);
+    const float len = length3(d);
+    move = (!finiteV(d) || !finiteS(len) || len > fmaxf(p.maxStep, 0.0f)) ? 1u : 0u;
+  }
+  b.bpPinnedMove[v] = move;
 }
 
-// A listed pair at `pos`: indices, scene, column, state (carried from the
-// previous list, or the source contact and, at the frame's first iteration,
-// its lagged force as lagContact :2712-2740 forms them), activity
-// (contactIncluded) and the pair's four sort entries (vertex, candidate),
-// whose key is the sentinel when the pair is inactive.
-__device__ __forceinline__ void bpWriteCandidate(const Buffers& b, const DevParams& p, const float4* __restrict__ src,
-                                                 int first, uint32_t scene, bool edgeRow, const uint32_t (&rv)[2],
-                                                 uint32_t col, uint32_t pos, uint32_t prevBegin, uint32_t prevEnd) {
-  uint4 q;
-  if (edgeRow) {
-    const uint2 e = b.bpEdges[col];
-    q = make_uint4(rv[0], rv[1], e.x, e.y);
-  } else {
-    const uint4 t = b.bpTris[col];
-    q = make_uint4(rv[0], t.x, t.y, t.z);
+// Superchunk boxes: one warp per 32 chunks (the union of their boxes).
+__global__ void __launch_bounds__(kBlock) bpSuperKernel(Buffers b, uint32_t triSupers, uint32_t edgeSupers) {
+  const uint32_t w = blockIdx.x * (kBlock / 32) + threadIdx.x / 32, lane = threadIdx.x & 31u;
+  if (w >= triSupers + edgeSupers) return;  // uniform across the warp
+  const bool edges = w >= triSupers;
+  const uint32_t sc = edges ? w - triSupers : w;
+  const uint32_t chunks = ((edges ? b.bpEdgeTotal : b.bpTriTotal) + kBpChunk - 1) / kBpChunk;
+  const uint32_t chunk = sc * kBpChunk + lane;
+  BpBox q = chunk < chunks ? bpLoad(edges ? b.bpEdgeChunk : b.bpTriChunk, chunk) : bpEmpty();
+#pragma unroll
+  for (int o = 16; o > 0; o >>= 1) {
+    q.lo.x = fminf(q.lo.x, __shfl_xor_sync(0xffffffffu, q.lo.x, o));
+    q.lo.y = fminf(q.lo.y, __shfl_xor_sync(0xffffffffu, q.lo.y, o));
+    q.lo.z = fminf(q.lo.z, __shfl_xor_sync(0xffffffffu, q.lo.z, o));
+    q.hi.x = fmaxf(q.hi.x, __shfl_xor_sync(0xffffffffu, q.hi.x, o));
+    q.hi.y = fmaxf(q.hi.y, __shfl_xor_sync(0xffffffffu, q.hi.y, o));
+    q.hi.z = fmaxf(q.hi.z, __shfl_xor_sync(0xffffffffu, q.hi.z, o));
+    q.m = fmaxf(q.m, __shfl_xor_sync(0xffffffffu, q.m, o));
   }
-  b.contactIdx[pos] = make_uint4(q.x, q.y, q.z, q.w | (edgeRow ? 0x80000000u : 0u));
-  b.contactScene[pos] = scene;
-  b.bpCols[pos] = col;
-  float4* st = b.contactState + kContactStateWords * static_cast<size_t>(pos);
-  float4 lagF = make_float4(0, 0, 0, 0), lagW = make_float4(0, 0, 0, 0);
-  bool carried = false;
-  if (!first) {
-    uint32_t lo = prevBegin, hi = prevEnd;
-    while (lo < hi) {
-      const uint32_t mid = (lo + hi) >> 1;
-      if (b.bpPrevCols[mid] < col) lo = mid + 1;
-      else hi = mid;
-    }
-    if (lo < prevEnd && b.bpPrevCols[lo] == col) {
-      const float4* ps = b.bpPrevState + kContactStateWords * static_cast<size_t>(lo);
-      st[kContactSource] = ps[kContactSource];
-      st[kContactSourceWeights] = ps[kContactSourceWeights];
+  if (lane == 0) bpStore(edges ? b.bpEdgeSuper : b.bpTriSuper, sc, q);
+}
+
+// A listed pair's state: carried from the previous list (its entry
+// `bpPrev`), else the source contact and, at the frame's first iteration, its
+// lagged force as lagContact (:2712-2740) forms them; its activity
+// (contactIncluded) and its four sort entries (vertex, candidate), whose key
+// is the sentinel when the pair is inactive.  One thread per candidate.
+__global__ void __launch_bounds__(kBlock) bpInitKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                       const float4* __restrict__ src, int first) {
+  const uint32_t n = __ldcg(b.bpStatus);
+  for (uint32_t c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock) {
+    const DevParams& p = pp[b.contactScene[c]];
+    uint32_t type;
+    const uint4 q = contactIndices(b, c, &type);
+    float4* st = b.contactState + kContactStateWords * static_cast<size_t>(c);
+    float4 lagF = make_float4(0, 0, 0, 0), lagW = make_float4(0, 0, 0, 0);
+    const uint32_t prev = first ? 0xffffffffu : b.bpPrev[c];
+    float4 s0, s1;
+    if (prev != 0xffffffffu) {
+      const float4* ps = b.bpPrevState + kContactStateWords * static_cast<size_t>(prev);
+      s0 = ps[kContactSource];
+      s1 = ps[kContactSourceWeights];
       lagF = ps[kContactLagged];
       lagW = ps[kContactLaggedWeights];
-      carried = true;
-    }
-  }
-  if (!carried) {
-    const ContactData k = ipcContactFromPositions(edgeRow ? kIpcEdgeEdge : kIpcVertexTriangle, xyz(src[q.x]),
-                                                  xyz(src[q.y]), xyz(src[q.z]), xyz(src[q.w]),
-                                                  p.ipcActivation + contactRoundingReach(p));
-    ipcStoreCached(st, kContactSource, k);
-    if (first && k.valid && k.distance > p.ipcMinDistance) {
-      const float f = fmaxf(0.0f, -p.ipcStiffness * ipcBarrier1(k.distance, p.ipcActivation));
-      if (finiteS(f)) {
-        lagF = make_float4(k.normal.x, k.normal.y, k.normal.z, f);
-        lagW = k.weights;
+      st[kContactSource] = s0;
+      st[kContactSourceWeights] = s1;
+    } else {
+      const ContactData k = ipcContactFromPositions(type, xyz(src[q.x]), xyz(src[q.y]), xyz(src[q.z]), xyz(src[q.w]),
+                                                    p.ipcActivation + contactRoundingReach(p));
+      ipcStoreCached(st, kContactSource, k);
+      s0 = st[kContactSource];
+      s1 = st[kContactSourceWeights];
+      if (first && k.valid && k.distance > p.ipcMinDistance) {
+        const float f = fmaxf(0.0f, -p.ipcStiffness * ipcBarrier1(k.distance, p.ipcActivation));
+        if (finiteS(f)) {
+          lagF = make_float4(k.normal.x, k.normal.y, k.normal.z, f);
+          lagW = k.weights;
+        }
       }
     }
-  }
-  st[kContactLagged] = lagF;
-  st[kContactLaggedWeights] = lagW;
-  st[kContactScratch] = make_float4(1, 0, 0, 0);
-  // contactIncluded on the state just written.
-  const ContactData k = ipcCached(st[kContactSource], st[kContactSourceWeights]);
-  const bool friction = p.ipcFriction > 0.0f && lagF.w > 0.0f;
-  const bool bounded = p.maxStep > 0.0f;
-  const float reach = p.ipcActivation + 2.0f * (fmaxf(p.maxStep, 0.0f) + contactRoundingReach(p));
-  const bool active =
-      !k.valid || !bounded || k.distance <= reach || friction || contactPinnedMotion(b, q, src, fmaxf(p.maxStep, 0.0f));
-  b.contactFlag[pos] = active ? 1u : 0u;
-  const uint32_t vs[4] = {q.x, q.y, q.z, q.w};
-#pragma unroll
-  for (int l = 0; l < 4; ++l) {
-    b.bpKeys[0][4ull * pos + l] = active ? vs[l] : b.bpSentinel;
-    b.bpVals[0][4ull * pos + l] = pos;
+    st[kContactLagged] = lagF;
+    st[kContactLaggedWeights] = lagW;
+    st[kContactScratch] = make_float4(1, 0, 0, 0);
+    // contactIncluded on the state just written.
+    const ContactData k = ipcCached(s0, s1);
+    const bool friction = p.ipcFriction > 0.0f && lagF.w > 0.0f;
+    const bool bounded = p.maxStep > 0.0f;
+    const float reach = p.ipcActivation + 2.0f * (fmaxf(p.maxStep, 0.0f) + contactRoundingReach(p));
+    const bool pinnedMove =
+        (b.bpPinnedMove[q.x] | b.bpPinnedMove[q.y] | b.bpPinnedMove[q.z] | b.bpPinnedMove[q.w]) != 0u;
+    const bool active = !k.valid || !bounded || k.distance <= reach || friction || pinnedMove;
+    b.contactFlag[c] = active ? 1u : 0u;
+    const uint32_t key = b.bpSentinel;
+    reinterpret_cast<uint4*>(b.bpKeys[0])[c] =
+        active ? make_uint4(q.x, q.y, q.z, q.w) : make_uint4(key, key, key, key);
+    reinterpret_cast<uint4*>(b.bpVals[0])[c] = make_uint4(c, c, c, c);
   }
 }
 
 // One warp per row: the row's pairs in column order, counted (kWrite false,
-// into bpRowOff[row]) or written at the row's offset (kWrite true).
+// into bpRowOff[row]) or placed at the row's offset with their previous
+// entry (kWrite true).  The columns are walked 32 superchunks (of 32 chunks
+// of 32 primitives) at a time, then 32 chunks, then 32 primitives, each
+// level only inside the boxes the row's box does not clear.
 template <bool kWrite>
 __global__ void __launch_bounds__(kBlock) bpRowsKernel(Buffers b, const DevParams* __restrict__ pp,
                                                        const float4* __restrict__ src, int first) {
   __shared__ uint32_t carried[kBlock / 32][32];
+  __shared__ uint32_t closedSet[kBlock / 32][kBpClosedMax];
   const uint32_t warp = threadIdx.x / 32, lane = threadIdx.x & 31u;
   const uint32_t r = blockIdx.x * (kBlock / 32) + warp;
   if (r >= b.bpRowTotal) return;                   // uniform across the warp
@@ -1118,55 +1142,142 @@ __global__ void __launch_bounds__(kBlock) bpRowsKernel(Buffers b, const DevParam
       const uint32_t vs[1] = {row.x};
       P = bpPrimitive(b, p, src, vs);
     }
+    // The row's closed one-ring set: a pair whose other vertices meet it is
+    // not in the superset (more than kBpClosedMax vertices: the ring lists).
+    uint32_t nClosed = 0;
+    {
+      const uint2 r0 = b.bpRing[rv[0]];
+      const uint2 r1 = edgeRow ? b.bpRing[rv[1]] : make_uint2(0u, 0u);
+      nClosed = (edgeRow ? 2u : 1u) + r0.y + r1.y;
+      if (nClosed <= kBpClosedMax) {
+        for (uint32_t i = lane; i < nClosed; i += 32) {
+          uint32_t v;
+          if (i == 0) v = rv[0];
+          else if (i <= r0.y) v = b.bpRingIds[r0.x + i - 1];
+          else if (i == r0.y + 1) v = rv[1];
+          else v = b.bpRingIds[r1.x + i - r0.y - 2];
+          closedSet[warp][i] = v;
+        }
+      }
+      __syncwarp();
+    }
+    auto closed = [&](uint32_t col) {
+      if (nClosed > kBpClosedMax) return bpPairClosed(b, edgeRow, rv, col);
+      uint32_t q0, q1, q2;
+      if (edgeRow) {
+        const uint2 e = b.bpEdges[col];
+        q0 = e.x;
+        q1 = q2 = e.y;
+      } else {
+        const uint4 t = b.bpTris[col];
+        q0 = t.x;
+        q1 = t.y;
+        q2 = t.z;
+      }
+      for (uint32_t i = 0; i < nClosed; ++i) {
+        const uint32_t v = closedSet[warp][i];
+        if (v == q0 || v == q1 || v == q2) return true;
+      }
+      return false;
+    };
     const uint32_t base = kWrite ? b.bpRowOff[r] : 0u;
     uint32_t pc = 0, pe = 0;  // this row's entries of the previous list
     if (!first) {
       pc = b.bpPrevRowOff[r];
       pe = b.bpPrevRowOff[r + 1];
     }
-    const uint32_t prevBegin = pc;
+    uint32_t qc = pc;  // carry cursor: first previous entry at or past the current chunk
     const uint32_t chunkLo = row.z / kBpChunk, chunkHi = (row.w - 1) / kBpChunk;
+    const float4* superBoxes = edgeRow ? b.bpEdgeSuper : b.bpTriSuper;
     const float4* chunkBoxes = edgeRow ? b.bpEdgeChunk : b.bpTriChunk;
     const float4* primBoxes = edgeRow ? b.bpEdgeBox : b.bpTriBox;
-    for (uint32_t c0 = chunkLo; c0 <= chunkHi; c0 += 32) {
-      const uint32_t windowEnd = (c0 + 32) * kBpChunk;
-      carried[warp][lane] = 0u;
-      __syncwarp();
-      // Previous pairs of this window that carry lagged friction and that the
-      // box test leaves out stay listed.
-      while (pc < pe) {
-        const uint32_t i = pc + lane;
-        const uint32_t col = i < pe ? b.bpPrevCols[i] : 0xffffffffu;
-        const bool in = i < pe && col < windowEnd;
-        if (in && p.ipcFriction > 0.0f &&
-            b.bpPrevState[kContactStateWords * static_cast<size_t>(i) + kContactLagged].w > 0.0f &&
-            bpSeparated(P, bpLoad(primBoxes, col), reach))
-          atomicOr(&carried[warp][col / kBpChunk - c0], 1u << (col % kBpChunk));
-        const unsigned inMask = __ballot_sync(0xffffffffu, in);
-        pc += __popc(inMask);
-        if (inMask != 0xffffffffu) break;
+    // Rows whose previous entries carry no lagged friction skip whole
+    // superchunks whose box the row's box clears.
+    bool friction = false;
+    if (!first && p.ipcFriction > 0.0f)
+      for (uint32_t i0 = pc; i0 < pe && !friction; i0 += 32) {
+        const uint32_t i = i0 + lane;
+        friction = __any_sync(0xffffffffu,
+                              i < pe && b.bpPrevState[kContactStateWords * static_cast<size_t>(i) + kContactLagged].w >
+                                            0.0f);
       }
-      __syncwarp();
-      const uint32_t chunk = c0 + lane;
-      const bool look = chunk <= chunkHi &&
-                        (carried[warp][lane] != 0u || !bpSeparated(P, bpLoad(chunkBoxes, chunk), reach));
-      unsigned todo = __ballot_sync(0xffffffffu, look);
-      while (todo) {
-        const uint32_t j = __ffs(todo) - 1;
-        todo &= todo - 1;
-        const uint32_t col = (c0 + j) * kBpChunk + lane;
-        bool hit = false;
-        if (col >= row.z && col < row.w) {
-          hit = ((carried[warp][j] >> lane) & 1u) != 0u;
-          if (!hit && !bpSeparated(P, bpLoad(primBoxes, col), reach)) hit = !bpPairClosed(b, edgeRow, rv, col);
+    const uint32_t superLo = chunkLo / kBpChunk, superHi = chunkHi / kBpChunk;
+    for (uint32_t s0 = superLo; s0 <= superHi; s0 += 32) {
+      const uint32_t sc = s0 + lane;
+      unsigned superTodo = __ballot_sync(0xffffffffu, sc <= superHi && (friction || !bpSeparated(
+                                                                                     P, bpLoad(superBoxes, sc), reach)));
+      while (superTodo) {
+        const uint32_t c0 = (s0 + __ffs(superTodo) - 1) * kBpChunk;  // the superchunk's first chunk
+        superTodo &= superTodo - 1;
+        const uint32_t windowEnd = (c0 + 32) * kBpChunk;
+        carried[warp][lane] = 0u;
+        __syncwarp();
+        // Previous pairs of this window that carry lagged friction and that
+        // the box test leaves out stay listed.
+        while (friction && pc < pe) {
+          const uint32_t i = pc + lane;
+          const uint32_t col = i < pe ? b.bpPrevCols[i] : 0xffffffffu;
+          const bool in = i < pe && col < windowEnd;
+          if (in && b.bpPrevState[kContactStateWords * static_cast<size_t>(i) + kContactLagged].w > 0.0f &&
+              bpSeparated(P, bpLoad(primBoxes, col), reach))
+            atomicOr(&carried[warp][col / kBpChunk - c0], 1u << (col % kBpChunk));
+          const unsigned inMask = __ballot_sync(0xffffffffu, in);
+          pc += __popc(inMask);
+          if (inMask != 0xffffffffu) break;
         }
-        const unsigned m = __ballot_sync(0xffffffffu, hit);
-        if (kWrite && hit)
-          bpWriteCandidate(b, p, src, first, scene, edgeRow, rv, col, base + count + __popc(m & ((1u << lane) - 1u)),
-                           prevBegin, pe);
-        count += __popc(m);
+        __syncwarp();
+        const uint32_t chunk = c0 + lane;
+        const bool look = chunk >= chunkLo && chunk <= chunkHi &&
+                          (carried[warp][lane] != 0u || !bpSeparated(P, bpLoad(chunkBoxes, chunk), reach));
+        unsigned todo = __ballot_sync(0xffffffffu, look);
+        while (todo) {
+          const uint32_t j = __ffs(todo) - 1;
+          todo &= todo - 1;
+          const uint32_t col = (c0 + j) * kBpChunk + lane;
+          bool hit = false;
+          if (col >= row.z && col < row.w) {
+            hit = ((carried[warp][j] >> lane) & 1u) != 0u;
+            if (!hit && !bpSeparated(P, bpLoad(primBoxes, col), reach)) hit = !closed(col);
+          }
+          const unsigned m = __ballot_sync(0xffffffffu, hit);
+          if (kWrite && m) {
+            // The previous list's entries of this chunk (sorted, at most 32):
+            // a bit per column, so a listed pair finds its entry by rank.
+            uint32_t prev = 0xffffffffu;
+            if (!first) {
+              const uint32_t chunkStart = (c0 + j) * kBpChunk;
+              while (qc < pe) {
+                const uint32_t i = qc + lane;
+                const unsigned below = __ballot_sync(0xffffffffu, i < pe && b.bpPrevCols[i] < chunkStart);
+                qc += __popc(below);
+                if (below != 0xffffffffu) break;
+              }
+              const uint32_t i = qc + lane;
+              const uint32_t pcol = i < pe ? b.bpPrevCols[i] : 0xffffffffu;
+              const uint32_t off = pcol - chunkStart;
+              const unsigned have = __reduce_or_sync(0xffffffffu, off < kBpChunk ? (1u << off) : 0u);
+              if ((have >> lane) & 1u) prev = qc + __popc(have & ((1u << lane) - 1u));
+            }
+            if (hit) {
+              const uint32_t pos = base + count + __popc(m & ((1u << lane) - 1u));
+              uint4 q;
+              if (edgeRow) {
+                const uint2 e = b.bpEdges[col];
+                q = make_uint4(rv[0], rv[1], e.x, e.y | 0x80000000u);
+              } else {
+                const uint4 t = b.bpTris[col];
+                q = make_uint4(rv[0], t.x, t.y, t.z);
+              }
+              b.contactIdx[pos] = q;
+              b.contactScene[pos] = scene;
+              b.bpCols[pos] = col;
+              b.bpPrev[pos] = prev;
+            }
+          }
+          count += __popc(m);
+        }
+        __syncwarp();  // carried[] is rewritten by the next window
       }
-      __syncwarp();  // carried[] is rewritten by the next window
     }
   }
   if (!kWrite && lane == 0) b.bpRowOff[r] = count;
@@ -1268,8 +1379,12 @@ __global__ void __launch_bounds__(kSortThreads) bpSortHistKernel(const uint32_t*
   hist[threadIdx.x * tiles + blockIdx.x] = h[threadIdx.x];
 }
 
+// One block per digit: the exclusive scan of the digit's tile counts and the
+// digit's total (after the 256 x tiles histogram).
 __global__ void __launch_bounds__(kScanThreads) bpSortScanKernel(const uint32_t* status, uint32_t* hist) {
-  blockScan(hist, 256u * sortTiles(status), ~0ull);
+  const uint32_t tiles = sortTiles(status);
+  const uint64_t total = blockScan(hist + static_cast<size_t>(blockIdx.x) * tiles, tiles, ~0ull);
+  if (threadIdx.x == 0) hist[256u * tiles + blockIdx.x] = static_cast<uint32_t>(total);
 }
 
 __global__ void __launch_bounds__(kSortThreads) bpSortScatterKernel(const uint32_t* __restrict__ kin,
@@ -1279,11 +1394,24 @@ __global__ void __launch_bounds__(kSortThreads) bpSortScatterKernel(const uint32
                                                                     const uint32_t* status, uint32_t shift,
                                                                     const uint32_t* __restrict__ hist) {
   __shared__ uint32_t wh[kSortThreads / 32][256];
+  __shared__ uint32_t digitBase[256];
   const uint32_t M = 4u * __ldcg(status), tiles = sortTiles(status);
   const uint32_t tile = blockIdx.x;
   if (tile >= tiles) return;
   const uint32_t w = threadIdx.x / 32, lane = threadIdx.x & 31u;
   for (uint32_t d = threadIdx.x; d < 256u * (kSortThreads / 32); d += kSortThreads) (&wh[0][0])[d] = 0u;
+  // Exclusive prefix of the digit totals (one digit per thread).
+  digitBase[threadIdx.x] = hist[256u * tiles + threadIdx.x];
+  __syncthreads();
+  for (uint32_t o = 1; o < 256u; o <<= 1) {
+    const uint32_t add = threadIdx.x >= o ? digitBase[threadIdx.x - o] : 0u;
+    __syncthreads();
+    digitBase[threadIdx.x] += add;
+    __syncthreads();
+  }
+  const uint32_t mine = digitBase[threadIdx.x] - hist[256u * tiles + threadIdx.x];
+  __syncthreads();
+  digitBase[threadIdx.x] = mine;
   __syncthreads();
   const uint32_t base = tile * kSortTile + w * (kSortItems * 32);
   uint32_t dig[kSortItems], pos[kSortItems];
@@ -1317,7 +1445,7 @@ __global__ void __launch_bounds__(kSortThreads) bpSortScatterKernel(const uint32
   for (uint32_t j = 0; j < kSortItems; ++j) {
     if (dig[j] < 256u) {
       const uint32_t i = base + j * 32 + lane;
-      const uint32_t o = hist[dig[j] * tiles + tile] + wh[w][dig[j]] + pos[j];
+      const uint32_t o = digitBase[dig[j]] + hist[dig[j] * tiles + tile] + wh[w][dig[j]] + pos[j];
       kout[o] = kin[i];
       vout[o] = vin[i];
     }
@@ -2590,22 +2718,27 @@ int launchBroadPhase(const Buffers& b, const DevParams* p, const float4* src, ui
   if (!b.contactDynamic || b.contactCount == 0) return 0;
   const uint32_t triBlocks = blocksFor(b.bpTriTotal), edgeBlocks = blocksFor(b.bpEdgeTotal);
   bpBoxesKernel<<<triBlocks + edgeBlocks + blocksFor(V), kBlock, 0, s>>>(b, p, src, triBlocks, edgeBlocks, V);
+  const uint32_t triSupers = (b.bpTriTotal + kBpChunk * kBpChunk - 1) / (kBpChunk * kBpChunk);
+  const uint32_t edgeSupers = (b.bpEdgeTotal + kBpChunk * kBpChunk - 1) / (kBpChunk * kBpChunk);
+  bpSuperKernel<<<(triSupers + edgeSupers + kBlock / 32 - 1) / (kBlock / 32), kBlock, 0, s>>>(b, triSupers,
+                                                                                              edgeSupers);
   const uint32_t rowBlocks = (b.bpRowTotal + kBlock / 32 - 1) / (kBlock / 32);
   const int f = first ? 1 : 0;
   bpRowsKernel<false><<<rowBlocks, kBlock, 0, s>>>(b, p, src, f);
   bpScanKernel<<<1, kScanThreads, 0, s>>>(b, p, f);
   bpRowsKernel<true><<<rowBlocks, kBlock, 0, s>>>(b, p, src, f);
+  bpInitKernel<<<candidateBlocks(b), kBlock, 0, s>>>(b, p, src, f);
   const uint32_t tiles = static_cast<uint32_t>((4ull * b.contactCount + kSortTile - 1) / kSortTile);
   for (uint32_t pass = 0; pass < b.bpSortPasses; ++pass) {
     const uint32_t in = pass & 1u, out = in ^ 1u;
     bpSortHistKernel<<<tiles, kSortThreads, 0, s>>>(b.bpKeys[in], b.bpStatus, 8u * pass, b.bpHist);
-    bpSortScanKernel<<<1, kScanThreads, 0, s>>>(b.bpStatus, b.bpHist);
+    bpSortScanKernel<<<256, kScanThreads, 0, s>>>(b.bpStatus, b.bpHist);
     bpSortScatterKernel<<<tiles, kSortThreads, 0, s>>>(b.bpKeys[in], b.bpVals[in], b.bpKeys[out], b.bpVals[out],
                                                        b.bpStatus, 8u * pass, b.bpHist);
   }
   const uint32_t segBlocks = std::min(blocksFor(4u * b.contactCount), smCount() * 8u);
   bpSegmentsKernel<<<segBlocks, kBlock, 0, s>>>(b, b.bpKeys[b.bpSortPasses & 1u]);
-  return 5 + 3 * static_cast<int>(b.bpSortPasses);
+  return 7 + 3 * static_cast<int>(b.bpSortPasses);
 }
 
 int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* dst, uint32_t V, cudaStream_t s) {

@@ -169,6 +169,8 @@ struct Buffers {
   float4* bpEdgeBox;
   float4* bpTriChunk;
   float4* bpEdgeChunk;
+  float4* bpTriSuper;   // 2 per 32 chunks
+  float4* bpEdgeSuper;
   uint32_t* bpRowOff;
   const uint32_t* bpPrevRowOff;
   uint32_t* bpCols;
@@ -178,7 +180,9 @@ struct Buffers {
   uint32_t* bpStatus;
   uint32_t* bpKeys[2];
   uint32_t* bpVals[2];
-  uint32_t* bpHist;
+  uint32_t* bpHist;         // 256 digits x tiles, then the 256 digit totals
+  uint32_t* bpPinnedMove;   // per vertex: pinned and its snap to rest exceeds maxStep (or is not finite)
+  uint32_t* bpPrev;         // per listed candidate: its entry in the previous list, or ~0
 };
 
 // Kernel launch entry points (jgs2_kernels.cu).  `p` points at one DevParams

@@ -2003,6 +2003,8 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
       STEP(deviceAlloc(sp, &b.bpEdgeBox, 2 * bpE));
       STEP(deviceAlloc(sp, &b.bpTriChunk, 2 * ((bpT + 31) / 32)));
       STEP(deviceAlloc(sp, &b.bpEdgeChunk, 2 * ((bpE + 31) / 32)));
+      STEP(deviceAlloc(sp, &b.bpTriSuper, 2 * ((bpT + 1023) / 1024)));
+      STEP(deviceAlloc(sp, &b.bpEdgeSuper, 2 * ((bpE + 1023) / 1024)));
       for (int l = 0; l < 2; ++l) {
         STEP(deviceAlloc(sp, &sp->dynIdx[l], cap));
         STEP(deviceAlloc(sp, &sp->dynScene[l], cap));
@@ -2014,7 +2016,9 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
         STEP(deviceAlloc(sp, &b.bpKeys[l], 4 * cap));
         STEP(deviceAlloc(sp, &b.bpVals[l], 4 * cap));
       }
-      STEP(deviceAlloc(sp, &b.bpHist, 256 * ((4 * cap + 4095) / 4096) + 1));
+      STEP(deviceAlloc(sp, &b.bpHist, 256 * ((4 * cap + 4095) / 4096) + 256));
+      STEP(deviceAlloc(sp, &b.bpPinnedMove, nV));
+      STEP(deviceAlloc(sp, &b.bpPrev, cap));
       STEP(deviceAlloc(sp, &b.bpSpan, S));
       STEP(deviceAlloc(sp, &b.bpStatus, 4));
       CUDA_TRY(sp, cudaMemsetAsync(b.bpStatus, 0, sizeof(uint32_t) * 4, sp->stream));

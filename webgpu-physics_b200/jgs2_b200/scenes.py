@@ -512,6 +512,52 @@ def cloth_sheet(cells=127, young=1e4, bending=1e-3, **kwargs) -> SceneInput:
                        **kwargs)
 
 
+# Settings of the reference app's cloth scene (src/App.tsx:529-575: activation
+# distance 0.01, step bound 0.01, friction 0.3) at dt = 1/120 and 5 iterations.
+CLOTH_SETTINGS = dict(timestep=1 / 120, gravity=(0.0, -9.81, 0.0), floorHeight=-0.18, floorStiffness=0.0,
+                      iterations=5, velocityDamping=0.997, contactTangentialDamping=0.0, contactMargin=0.01,
+                      horizontalBodyCorrection=False, ipcActivationDistance=0.01, ipcMinimumDistance=0.003,
+                      ipcBarrierStiffness=1e5, ipcFrictionCoefficient=0.3, ipcFrictionVelocityEpsilon=0.05,
+                      ipcStepSafety=0.9, regularization=1e-6, rotationEpsilon=1e-7, maxStep=0.01)
+
+
+def spherify(p):
+    """Map points of the cube [-1, 1]^3 onto the unit ball (each axis scaled
+    by sqrt(1 - a^2/2 - b^2/2 + a^2 b^2 / 3) of the other two): the cube's
+    faces land on the sphere and a hex grid stays a valid mesh."""
+    x, y, z = p[:, 0], p[:, 1], p[:, 2]
+    x2, y2, z2 = x * x, y * y, z * z
+    return np.stack([x * np.sqrt(1 - y2 / 2 - z2 / 2 + y2 * z2 / 3),
+                     y * np.sqrt(1 - z2 / 2 - x2 / 2 + z2 * x2 / 3),
+                     z * np.sqrt(1 - x2 / 2 - y2 / 2 + x2 * y2 / 3)], axis=1)
+
+
+def cloth_sphere(cells=127, radius=0.3, centre=(0.0, 0.8, 0.0), sphere_cells=8, young=1e4, bending=1e-3,
+                 contact=CONTACT_SURFACE, capacity=8 << 20, timestep=1 / 120) -> SceneInput:
+    """The serving mix's cloth request: the (cells+1)^2-vertex StVK sheet of
+    `cloth_sheet` (E = 1e4, bending 1e-3, its two z = -0.8 corners pinned,
+    y = 1.15) draping over a fixed sphere of `radius` (a pinned hex grid of
+    sphere_cells^3 x6 tets mapped onto the ball) with IPC over the sheet and
+    the sphere's surface, the sheet's self-contact included."""
+    sc = Scene()
+    m = sc.add_material(1000.0, 110000.0, 0.34, MATERIAL_STABLE_NEO_HOOKEAN)
+    start = sc.add_cuboid((sphere_cells,) * 3, (-1.0,) * 3, (2.0,) * 3, m, 0, 63)
+    n_sphere = (sphere_cells + 1) ** 3
+    p = sc.rest_positions()
+    p[start:start + n_sphere] = spherify(p[start:start + n_sphere]) * radius + np.array(centre)
+    sc.set_rest_positions(p)
+    pos, tri = cloth_grid(cells)
+    n = cells + 1
+    pin = np.zeros(n * n, dtype=np.uint8)
+    pin[0] = pin[cells] = 1
+    sc.add_cloth(pos, tri, pin, 1, 480.0, young, 0.3, 0.012, bending)
+    sc.set_contact(contact, capacity)
+    stats = sc.precompute(timestep=timestep, cubature_k=4, method=PRECOMPUTE_PATCH)
+    inp = sc.pack()
+    inp.stats = stats
+    return inp
+
+
 def static_contact_candidates(vertex_count, triangles):
     """buildStaticIpcContactCandidates: (indices uint32[4n], vt count, ee count)."""
     lib = _ffi.scene_lib()
