@@ -420,10 +420,11 @@ def batched_arm(args):
 def serving_arm(args):
     """A seeded Poisson stream (mean 2000 requests/s) of step requests drawn
     from the serving mix: a cantilever (the 20x4x4 bar) at 1-4x resolution
-    for 10 exact Jacobi iterations per frame, an IPC trough of 1-20 boxes with
-    the reference app's contact settings (3 iterations per frame), or the
-    128x128 StVK cloth sheet (5 iterations per frame at dt=1/120), each for
-    1-60 frames, served by the native continuous-batching loop against a
+    for 10 exact Jacobi iterations per frame, the IPC box trough with 1-20
+    boxes of 8^3 hexes (15 iterations per frame, contact through the device
+    broad phase), or the 128x128 StVK cloth sheet draping over a sphere with
+    IPC self-contact (5 iterations per frame at dt=1/120), each for 1-60
+    frames, served by the native continuous-batching loop against a
     150 GB device-memory budget; the plain per-request path (create a solver,
     step, read, destroy, one request after another in arrival order) runs the
     same stream beside it."""
@@ -455,16 +456,14 @@ def serving_arm(args):
         return inp
 
     bar_settings = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floorStiffness=0.0, parityMode=True)
-    cloth_settings = dict(timestep=1 / 120, gravity=(0.0, -9.81, 0.0), floorStiffness=0.0, velocityDamping=0.997,
-                          contactTangentialDamping=0.0, horizontalBodyCorrection=False, maxStep=0.01)
     kinds = {}  # key -> (input, settings, iterations per frame)
     for r in (1, 2, 3, 4):
         kinds[("bar", r)] = (cached(f"cantilever_x{r}_k6_v1.npz", lambda r=r: scenes.cantilever(
             cells=(20 * r, 4 * r, 4 * r), method=scenes.PRECOMPUTE_PATCH)), bar_settings, 10)
     for n_boxes in range(1, 21):
-        kinds[("trough", n_boxes)] = (cached(f"trough_{n_boxes}_k6_v1.npz", lambda n_boxes=n_boxes: scenes.trough(
-            n_boxes)), dict(scenes.TROUGH_SETTINGS), 3)
-    kinds[("cloth", 0)] = (cached("cloth_sheet_127_v1.npz", scenes.cloth_sheet), cloth_settings, 5)
+        kinds[("trough", n_boxes)] = (cached(f"box_trough_{n_boxes}_v1.npz", lambda n_boxes=n_boxes: scenes.box_trough(
+            boxes=n_boxes)), dict(scenes.BOX_TROUGH_SETTINGS), 15)
+    kinds[("cloth", 0)] = (cached("cloth_sphere_127_v1.npz", scenes.cloth_sphere), dict(scenes.CLOTH_SETTINGS), 5)
     build_s = time.perf_counter() - t0
     rng = np.random.default_rng(2000 + rank)
     n = args.requests
@@ -532,10 +531,11 @@ def serving_arm(args):
             "config": {
                 "workload": (f"serving stream: {n} requests, Poisson arrivals at a mean 2000/s (seed 2000), drawn "
                              "uniformly from a 20x4x4-hex cantilever at 1-4x resolution (stable Neo-Hookean E=1e5 "
-                             "nu=0.4, K=6 patch-trained cubature, 10 exact Jacobi iterations per frame), an IPC box "
-                             "trough of 1-20 boxes (the reference app's contact settings, 3 iterations per frame) "
-                             "and the 128x128 StVK cloth sheet (5 iterations per frame), each for 1-60 frames; "
-                             "150 GB device-memory admission budget"),
+                             "nu=0.4, K=6 patch-trained cubature, 10 exact Jacobi iterations per frame), the IPC "
+                             "box trough with 1-20 boxes of 8^3 hexes (dHat 1e-3, 15 iterations per frame, device "
+                             "broad phase) and the 128x128 StVK cloth sheet draping over a 0.3 m sphere with IPC "
+                             "self-contact (5 iterations per frame), each for 1-60 frames; 150 GB device-memory "
+                             "admission budget"),
                 "requests": n, "mix": mix, "frames": total_frames, "step": "one request",
                 "l2": "no flush: requests stream through different resident scenes",
                 "precompute": {"seconds": round(build_s, 1)},

@@ -1806,8 +1806,9 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     r.kOff = sc.kOff; r.KC = sc.KC;
     r.rowOff = sc.bpRowOff; r.rowCount = sc.dynamic ? sc.bpRows : 0u;
     // A contact-surface scene's gate also takes its listed candidates: the
-    // table covers an eighth of the list capacity, more stride over it.
-    const uint32_t listed = sc.dynamic ? static_cast<uint32_t>(sc.bpCapacity / 8) : 0u;
+    // table covers half the list capacity (blocks past the listed count
+    // only join the reduction), more stride over it.
+    const uint32_t listed = sc.dynamic ? static_cast<uint32_t>(sc.bpCapacity / 2) : 0u;
     const uint32_t n = std::max(std::max(std::max(sc.V, sc.T), std::max(sc.C, sc.H)), std::max(sc.KC, listed));
     r.gateSpan = std::max(n, 1u);
     r.gateBase = static_cast<uint32_t>(gateTable.size());

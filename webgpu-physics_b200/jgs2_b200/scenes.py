@@ -696,7 +696,13 @@ def box_trough(boxes=20, cells=8, box_size=0.46, heights=(1.0, 3.0), seed=3003, 
     sc.set_contact(contact, capacity)
     if exact_complement:
         args = dict(timestep=timestep, method=method, threads=threads, patch_radius=patch_radius, exact_complement=1)
-        stats = sc.precompute(cubature_k=4096, **args)
+        # Probe with a bound on the patch's candidate tets (192 at one ring
+        # of a hex grid, 400 at two), then pack exactly the widest count.
+        probe = 256 * patch_radius
+        stats = sc.precompute(cubature_k=probe, **args)
+        while stats["max_records_per_vertex"] >= probe:
+            probe *= 2
+            stats = sc.precompute(cubature_k=probe, **args)
         stats = sc.precompute(cubature_k=max(1, stats["max_records_per_vertex"]), **args)
     else:
         stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=method, threads=threads,
