@@ -150,7 +150,7 @@ typedef struct jgs2_contact_surface {
   uint32_t triangle_count;
   uint32_t reserved0;
   const uint32_t* triangles;     /* 3 * triangle_count vertex indices; any order, duplicates merged */
-  uint64_t candidate_capacity;   /* candidates one iteration may list; 0 = 64 x (vertices + edges) */
+  uint64_t candidate_capacity;   /* candidates one iteration may list; 0 = 65536 + 16 x (vertices + edges) */
 } jgs2_contact_surface;
 
 /*

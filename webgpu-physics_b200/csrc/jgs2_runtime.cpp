@@ -607,7 +607,7 @@ void buildContactSurface(const jgs2_input* in, ContactSurface* out) {
   for (uint32_t v = 0; v < V; ++v) std::sort(out->ring.begin() + out->ringStart[v], out->ring.begin() + out->ringStart[v + 1]);
   out->capacity = cs->candidate_capacity
                       ? cs->candidate_capacity
-                      : std::max<uint64_t>(4096, 64ull * (uint64_t(V) + out->edges.size()));
+                      : 65536 + 16ull * (uint64_t(V) + out->edges.size());
   // Size of the superset: per vertex the triangles outside its closed
   // one-ring, per edge pair those whose endpoints avoid each other's closed
   // one-rings.
@@ -2842,7 +2842,7 @@ uint64_t jgs2_estimate_device_bytes(const jgs2_input* in) {
     // flag, column) and the sort's four entry buffers; surface data, boxes
     // and rows per triangle and edge (at most three edges per triangle).
     const uint64_t E = 3ull * cs->triangle_count;
-    const uint64_t cap = cs->candidate_capacity ? cs->candidate_capacity : std::max<uint64_t>(4096, 64 * (V + E));
+    const uint64_t cap = cs->candidate_capacity ? cs->candidate_capacity : 65536 + 16 * (V + E);
     contact = 2 * cap * (16 + 4 + 112 + 4 + 4) + 4 * cap * 16 + cs->triangle_count * (16 + 32) + E * (8 + 32 + 32) +
               V * (8 + 16 + 8 + 8 + 4 + 16) + (4 * cap / 4096 + 1) * 1024;
   }
