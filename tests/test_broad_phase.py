@@ -216,3 +216,25 @@ def test_surface_settings_checks():
         gpu.step({"maxStep": 0.0})
     gpu.step()
     gpu.destroy()
+
+
+@pytest.mark.gpu
+def test_surface_batch_matches_alone():
+    # The serving loop steps contact-surface requests as one batch: each
+    # scene's rows, list span, reductions and active rows stay its own, so a
+    # scene runs bitwise as it runs alone.
+    parts = [scenes.trough(2, contact=scenes.CONTACT_SURFACE), _small(scenes.CONTACT_SURFACE),
+             scenes.trough(1, contact=scenes.CONTACT_SURFACE)]
+    opts = [dict(scenes.TROUGH_SETTINGS), dict(scenes.BOX_TROUGH_SETTINGS), dict(scenes.TROUGH_SETTINGS)]
+    batch = solver.JGS2Batch.create(parts, opts)
+    alone = [solver.JGS2Batch.create([p], [o]) for p, o in zip(parts, opts)]
+    for frames in (10, 30):
+        batch.stepFrames(frames, exactIterations=3)
+        for a in alone:
+            a.stepFrames(frames, exactIterations=3)
+        for i, a in enumerate(alone):
+            np.testing.assert_array_equal(batch.readPositions(i), a.readPositions(0), err_msg=f"scene {i}")
+            assert batch.info(i)["contact_candidate_count"] == a.info(0)["contact_candidate_count"]
+    for a in alone:
+        a.destroy()
+    batch.destroy()
