@@ -391,6 +391,35 @@ jgs2_status jgs2_read_globalization(jgs2_solver* solver, float* local,
  * listed; out (may be NULL) holds `capacity` candidates.  Static candidates
  * are listed as given.  With a contact surface, a broad-phase list that did
  * not fit its capacity fails the step and this read with JGS2_DEVICE_ERROR. */
+/* readOracleDiagnostics (src/simulation/gpu/jgs2-solver.ts:2882-2907;
+ * JGS2GpuOracleDiagnostics, src/simulation/gpu/jgs2-diagnostics.ts:31-111):
+ * the exact, all-element frozen-frame implicit-Euler oracle at the current
+ * canonical pose against the last submitted inertial target and settings.
+ * Opt-in: the frame loop never runs it; its device records are allocated at
+ * the first call.  Fails with JGS2_UNSUPPORTED while IPC contact is enabled
+ * (the reference excludes contact energy); cloth terms are not included, as
+ * in the reference.  vertex_records (may be NULL) receive 36 floats per
+ * vertex in the reference's layout (gradient + active; the Hessian block's
+ * rows with inertia energy, floor energy and update magnitude beside them;
+ * squared gradient norm, finite, inertia weight, update valid; inertia,
+ * elasticity and floor squared norms, floor distance; floor active; external
+ * force gradient + energy; target gradient + energy); tet_records (may be
+ * NULL) 4 floats per tet (energy, determinant, finite, 0).  Sums in double. */
+typedef struct jgs2_oracle_diagnostics {
+  double energy;  /* the five components summed */
+  double inertia, elasticity, external_force, quadratic_target, floor_contact;
+  /* component gradient norms, in the production convergence order */
+  double inertia_gradient_norm, material_gradient_norm, external_force_gradient_norm, target_gradient_norm,
+      contact_gradient_norm;
+  double gradient_norm, gradient_squared_norm, residual_denominator, relative_residual;
+  double maximum_update, minimum_deformation_determinant, minimum_contact_distance;
+  uint32_t active_vertex_count, active_contact_count;
+  uint32_t relative_residual_valid, gradient_valid, maximum_update_valid, minimum_deformation_determinant_valid;
+  uint32_t minimum_contact_distance_valid, finite;
+} jgs2_oracle_diagnostics;
+jgs2_status jgs2_read_oracle_diagnostics(jgs2_solver* solver, jgs2_oracle_diagnostics* out, float* vertex_records,
+                                         size_t vertex_floats, float* tet_records, size_t tet_floats);
+
 jgs2_status jgs2_read_contact_candidates(jgs2_solver* solver, uint32_t* out,
                                          uint64_t capacity, uint64_t* count);
 

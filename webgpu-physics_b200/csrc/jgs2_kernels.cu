@@ -2569,6 +2569,229 @@ __global__ void __launch_bounds__(kBlock) gateScratchKernel(Buffers b, DevParams
 
 }  // namespace
 
+// ---------------------------------------------------------------------------
+// Exact all-element oracle diagnostics (JGS2GpuOracleEvaluator,
+// jgs2-diagnostics.ts:388-1146): per tet its frozen frame (the step's
+// seven-step polar), energy, determinant and finiteness; per vertex the exact
+// active-coordinate gradient, the diagonal block of the frozen global
+// Hessian, the inertia, objective and floor energies and norms; one
+// fixed-order reduction.  Opt-in; the frame loop never runs it.
+
+__device__ __forceinline__ float finiteOr0(float v) { return finiteS(v) ? v : 0.0f; }
+__device__ __forceinline__ float4 finite4(float3 v, float w) {
+  return make_float4(finiteOr0(v.x), finiteOr0(v.y), finiteOr0(v.z), w);
+}
+
+// Co-rotated displacement of a tet's vertices in its frame R:
+// R^T (x_l - centroid) - (X_l - rest centroid).
+__device__ __forceinline__ void oracleDisplacement(const Buffers& b, const float4* __restrict__ x, const uint4& q,
+                                                   const M3& R, float3 d[4], bool* finite) {
+  float3 cur[4], rest[4];
+  float3 cc = f3(0, 0, 0), rc = f3(0, 0, 0);
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    const uint32_t v = idxAt(q, l);
+    cur[l] = xyz(x[v]);
+    rest[l] = xyz(b.restMass[v]);
+    cc = cc + 0.25f * cur[l];
+    rc = rc + 0.25f * rest[l];
+  }
+  const M3 Rt = mtrans(R);
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    d[l] = mv(Rt, cur[l] - cc) - (rest[l] - rc);
+    *finite = *finite && finiteV(cur[l]) && finiteV(rest[l]) && finiteV(d[l]);
+  }
+}
+
+__global__ void __launch_bounds__(kBlock) oracleTetKernel(Buffers b, OracleParams q, const float4* __restrict__ x,
+                                                          float4* __restrict__ rot, float4* __restrict__ metric) {
+  const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
+  if (k >= q.T) return;
+  const uint32_t t = q.tOff + k;
+  const TetRec r = loadTet(b.tets, t);
+  const M3 F = deformationAt(r, x);
+  const float det = mdet(F);
+  const M3 R = polarRotation(F, q.rotationEpsilon);
+  bool finite = finiteM(F) && finiteS(det) && finiteM(R);
+  float energy = 0.0f;
+  if (q.corotated) {
+    float3 d[4];
+    oracleDisplacement(b, x, r.idx, R, d, &finite);
+    const float* K = b.stiffness + 144ull * t;
+#pragma unroll
+    for (int row = 0; row < 4; ++row) {
+      float3 lg = f3(0, 0, 0);
+#pragma unroll
+      for (int col = 0; col < 4; ++col) lg = lg + mv(stiffnessBlock(K, row, col), d[col]);
+      finite = finite && finiteV(lg);
+      energy += 0.5f * dot3(d[row], lg);
+    }
+  } else {
+    energy = r.vol * snhEnergy(F, r.lambda, r.mu);
+    const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
+    finite = finite && finiteM(piola(F, pt));
+  }
+  finite = finite && finiteS(energy);
+  rot[3ull * k] = finite4(R.c0, 0.0f);
+  rot[3ull * k + 1] = finite4(R.c1, 0.0f);
+  rot[3ull * k + 2] = finite4(R.c2, 0.0f);
+  metric[k] = make_float4(finiteOr0(energy), finiteOr0(det), finite ? 1.0f : 0.0f, 0.0f);
+}
+
+__global__ void __launch_bounds__(kBlock) oracleVertexKernel(Buffers b, OracleParams q, const float4* __restrict__ x,
+                                                             const float4* __restrict__ rot,
+                                                             float4* __restrict__ rec) {
+  const uint32_t k = blockIdx.x * kBlock + threadIdx.x;
+  if (k >= q.V) return;
+  const uint32_t v = q.vOff + k;
+  const uint4 info = b.vinfo[v];
+  const float4 rm = b.restMass[v];
+  const float3 cur = xyz(x[v]), pred = xyz(b.predicted[v]);
+  const float3 diff = cur - pred;
+  const float update = b.finalUpdate[v];
+  const float floorDistance = cur.y - q.floorHeight;
+  const bool active = !isPinned(info);
+  float3 grad = f3(0, 0, 0), gIn = f3(0, 0, 0), gEl = f3(0, 0, 0), gExt = f3(0, 0, 0), gTgt = f3(0, 0, 0);
+  float3 gFloor = f3(0, 0, 0);
+  M3 H = mzero();
+  float eIn = 0.0f, eExt = 0.0f, eTgt = 0.0f, eFloor = 0.0f, weight = 0.0f, mag = 0.0f;
+  bool updateValid = false, floorActive = false;
+  bool finite = finiteV(cur) && finiteV(pred) && finiteV(xyz(rm)) && finiteS(rm.w) && finiteS(update) &&
+                finiteS(floorDistance);
+  if (active) {
+    weight = rm.w * q.invDt2;
+    gIn = weight * diff;
+    grad = gIn;
+    H = weight * midentity();
+    eIn = 0.5f * weight * dot3(diff, diff);
+    mag = update;
+    updateValid = update >= 0.0f;
+    const float3 force = (q.objectiveFlags & 1u) ? xyz(b.forces[v]) : f3(0, 0, 0);
+    gExt = -1.0f * force;
+    eExt = -dot3(force, cur);
+    grad = grad + gExt;
+    const float4 target = (q.objectiveFlags & 2u) ? b.targets[v] : make_float4(0, 0, 0, 0);
+    finite = finite && finiteV(force) && finiteS(target.w) && target.w >= 0.0f;
+    if (target.w > 0.0f) {
+      finite = finite && finiteV(xyz(target));
+      const float3 res = cur - xyz(target);
+      gTgt = target.w * res;
+      eTgt = 0.5f * target.w * dot3(res, res);
+      grad = grad + gTgt;
+      H = H + target.w * midentity();
+    }
+    for (uint32_t a = 0; a < info.y; ++a) {
+      const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
+      const uint32_t t = entry >> 2, slot = entry & 3u;
+      const TetRec r = loadTet(b.tets, t);
+      if (q.corotated) {
+        const uint32_t kt = t - q.tOff;
+        const M3 R = {xyz(rot[3ull * kt]), xyz(rot[3ull * kt + 1]), xyz(rot[3ull * kt + 2])};
+        float3 d[4];
+        oracleDisplacement(b, x, r.idx, R, d, &finite);
+        const float* K = b.stiffness + 144ull * t;
+        float3 lg = f3(0, 0, 0);
+#pragma unroll
+        for (int col = 0; col < 4; ++col) lg = lg + mv(stiffnessBlock(K, slot, col), d[col]);
+        gEl = gEl + mv(R, lg);
+        H = H + mm(mm(R, stiffnessBlock(K, slot, slot)), mtrans(R));
+      } else {
+        const M3 F = deformationAt(r, x);
+        const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
+        const float3 g = shapeGradient(r, slot);
+        gEl = gEl + r.vol * mv(piola(F, pt), g);
+        S3 blk = szero();
+        addIncidentBlock(blk, r, F, pt, g);
+        H.c0 = H.c0 + f3(blk.xx, blk.xy, blk.xz);
+        H.c1 = H.c1 + f3(blk.xy, blk.yy, blk.yz);
+        H.c2 = H.c2 + f3(blk.xz, blk.yz, blk.zz);
+      }
+    }
+    grad = grad + gEl;
+    floorActive = q.floorStiffness > 0.0f && floorDistance < 0.0f;
+    if (floorActive) {
+      eFloor = 0.5f * q.floorStiffness * floorDistance * floorDistance;
+      gFloor.y = q.floorStiffness * floorDistance;
+      grad = grad + gFloor;
+      H.c1.y += q.floorStiffness;
+    }
+  }
+  const float gSq = dot3(grad, grad), inSq = dot3(gIn, gIn), elSq = dot3(gEl, gEl), flSq = dot3(gFloor, gFloor);
+  finite = finite && finiteS(weight) && finiteS(eIn) && finiteS(eExt) && finiteS(eTgt) && finiteS(eFloor) &&
+           finiteS(mag) && finiteV(grad) && finiteV(gIn) && finiteV(gEl) && finiteV(gExt) && finiteV(gTgt) &&
+           finiteV(gFloor) && finiteM(H) && finiteS(gSq) && finiteS(inSq) && finiteS(elSq) &&
+           finiteS(dot3(gExt, gExt)) && finiteS(dot3(gTgt, gTgt)) && finiteS(flSq);
+  float4* o = rec + 9ull * k;
+  o[0] = finite4(grad, active ? 1.0f : 0.0f);
+  // Rows of the (symmetric) block with the energies beside them.
+  o[1] = make_float4(finiteOr0(H.c0.x), finiteOr0(H.c1.x), finiteOr0(H.c2.x), finiteOr0(eIn));
+  o[2] = make_float4(finiteOr0(H.c0.y), finiteOr0(H.c1.y), finiteOr0(H.c2.y), finiteOr0(eFloor));
+  o[3] = make_float4(finiteOr0(H.c0.z), finiteOr0(H.c1.z), finiteOr0(H.c2.z), finiteOr0(mag));
+  o[4] = make_float4(finiteOr0(gSq), finite ? 1.0f : 0.0f, finiteOr0(weight), updateValid ? 1.0f : 0.0f);
+  o[5] = make_float4(finiteOr0(inSq), finiteOr0(elSq), finiteOr0(flSq), finiteOr0(floorDistance));
+  o[6] = make_float4(floorActive ? 1.0f : 0.0f, 0.0f, 0.0f, 0.0f);
+  o[7] = finite4(gExt, finiteOr0(eExt));
+  o[8] = finite4(gTgt, finiteOr0(eTgt));
+}
+
+// reduceDiagnostics in one block: each thread folds a fixed stride of the
+// records in double, then a fixed-order tree; deterministic.
+__global__ void __launch_bounds__(1024) oracleReduceKernel(OracleParams q, const float4* __restrict__ metric,
+                                                           const float4* __restrict__ rec, double* out) {
+  __shared__ double sh[1024];
+  double acc[kOracleSummaryWords];
+#pragma unroll
+  for (int i = 0; i < kOracleSummaryWords; ++i) acc[i] = 0.0;
+  acc[11] = 0.0;                 // largest update
+  acc[12] = 3.0e38;              // smallest determinant
+  acc[13] = 3.0e38;              // smallest floor distance
+  acc[16] = 1.0;                 // all active updates valid
+  acc[17] = 1.0;                 // all finite
+  for (uint32_t t = threadIdx.x; t < q.T; t += blockDim.x) {
+    const float4 m = metric[t];
+    acc[1] += m.x;
+    acc[12] = fmin(acc[12], double(m.y));
+    if (!(m.z >= 0.5f)) acc[17] = 0.0;
+  }
+  for (uint32_t v = threadIdx.x; v < q.V; v += blockDim.x) {
+    const float4* o = rec + 9ull * v;
+    const float4 g = o[0], r0 = o[1], r1 = o[2], r2 = o[3], m = o[4], c = o[5], fl = o[6], ext = o[7], tg = o[8];
+    const bool active = g.w >= 0.5f;
+    acc[0] += r0.w;
+    acc[2] += ext.w;
+    acc[3] += tg.w;
+    acc[4] += r1.w;
+    acc[5] += m.x;
+    acc[6] += c.x;
+    acc[7] += c.y;
+    acc[8] += double(ext.x) * ext.x + double(ext.y) * ext.y + double(ext.z) * ext.z;
+    acc[9] += double(tg.x) * tg.x + double(tg.y) * tg.y + double(tg.z) * tg.z;
+    acc[10] += c.z;
+    if (active) {
+      acc[11] = fmax(acc[11], double(r2.w));
+      acc[13] = fmin(acc[13], double(c.w));
+      acc[15] += fl.x >= 0.5f ? 1.0 : 0.0;
+      if (!(m.w >= 0.5f)) acc[16] = 0.0;
+      acc[14] += 1.0;
+    }
+    if (!(m.y >= 0.5f)) acc[17] = 0.0;
+  }
+  for (int i = 0; i < kOracleSummaryWords; ++i) {
+    sh[threadIdx.x] = acc[i];
+    __syncthreads();
+    for (uint32_t o = blockDim.x / 2; o > 0; o >>= 1) {
+      if (threadIdx.x < o) {
+        const double a = sh[threadIdx.x], c = sh[threadIdx.x + o];
+        sh[threadIdx.x] = (i == 11) ? fmax(a, c) : (i == 12 || i == 13 || i == 16 || i == 17) ? fmin(a, c) : a + c;
+      }
+      __syncthreads();
+    }
+    if (threadIdx.x == 0) out[i] = sh[0];
+    __syncthreads();
+  }
+}
+
 inline uint32_t blocksFor(uint32_t n) { return (n + kBlock - 1) / kBlock; }
 
 uint32_t smCount() {
@@ -2739,6 +2962,21 @@ int launchBroadPhase(const Buffers& b, const DevParams* p, const float4* src, ui
   const uint32_t segBlocks = std::min(blocksFor(4u * b.contactCount), smCount() * 8u);
   bpSegmentsKernel<<<segBlocks, kBlock, 0, s>>>(b, b.bpKeys[b.bpSortPasses & 1u]);
   return 7 + 3 * static_cast<int>(b.bpSortPasses);
+}
+
+int launchOracleDiagnostics(const Buffers& b, const OracleParams& q, float4* tetRot, float4* tetMetric,
+                            float4* vertexRecords, double* summary, cudaStream_t s) {
+  int n = 0;
+  if (q.T) {
+    oracleTetKernel<<<blocksFor(q.T), kBlock, 0, s>>>(b, q, b.pos[0], tetRot, tetMetric);
+    ++n;
+  }
+  if (q.V) {
+    oracleVertexKernel<<<blocksFor(q.V), kBlock, 0, s>>>(b, q, b.pos[0], tetRot, vertexRecords);
+    ++n;
+  }
+  oracleReduceKernel<<<1, 1024, 0, s>>>(q, tetMetric, vertexRecords, summary);
+  return n + 1;
 }
 
 int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* dst, uint32_t V, cudaStream_t s) {

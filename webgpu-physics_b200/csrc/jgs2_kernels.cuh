@@ -233,6 +233,25 @@ int launchContactGradient(const Buffers& b, const DevParams* p, const float4* sr
 int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool bodyCorrection,
                    uint32_t bodies, cudaStream_t s);
 
+// Exact all-element oracle diagnostics of one scene (an opt-in diagnostic,
+// not part of the step): at the canonical pose against the last inertial
+// target and settings.  invDt2 = 1 / h^2; objectiveFlags bit0 forces, bit1
+// targets; corotated selects the co-rotated element energy.
+struct OracleParams {
+  float invDt2, floorHeight, floorStiffness, rotationEpsilon;
+  uint32_t objectiveFlags, vOff, V, tOff, T, corotated, pad[2];
+};
+// Summary sums (doubles): energies (inertia, elasticity, external force,
+// target, floor), squared gradient norms (total, inertia, elasticity,
+// external force, target, floor), largest active update, smallest
+// determinant, smallest active floor distance, active vertices, active floor
+// contacts, all active updates valid, all finite.
+constexpr int kOracleSummaryWords = 18;
+// Tet records: 3 float4 frame columns + (energy, det, finite, 0); vertex
+// records: 9 float4 (gradient + active, Hessian rows with energies, metrics).
+int launchOracleDiagnostics(const Buffers& b, const OracleParams& q, float4* tetRot, float4* tetMetric,
+                            float4* vertexRecords, double* summary, cudaStream_t s);
+
 // Vertices per solve block for cubature width K (0: K too large to cache).
 uint32_t solveGroupsPerBlock(uint32_t K);
 constexpr size_t kGatePartialBytes = 32;

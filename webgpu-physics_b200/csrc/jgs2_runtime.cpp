@@ -896,6 +896,11 @@ struct Engine {
   uint64_t launches = 0;
   // graphs: (iterations, schedule, bodyCorrection, contact) -> exec, launches per replay
   std::map<std::tuple<uint32_t, uint32_t, bool, bool>, std::pair<cudaGraphExec_t, int>> graphs;
+  // Oracle diagnostics records, allocated at the first request.
+  float4* oracleTetRot = nullptr;
+  float4* oracleTetMetric = nullptr;
+  float4* oracleVertex = nullptr;
+  double* oracleSummary = nullptr;
   bool useGraphs = true;
 };
 
@@ -2328,6 +2333,93 @@ jgs2_status jgs2_sync(jgs2_solver* s) {
   CUDA_TRY(s, cudaSetDevice(s->device));
   CUDA_TRY(s, cudaStreamSynchronize(s->stream));
   return checkBroadPhase(s);
+}
+
+jgs2_status jgs2_read_oracle_diagnostics(jgs2_solver* s, jgs2_oracle_diagnostics* out, float* vertexRecords,
+                                         size_t vertexFloats, float* tetRecords, size_t tetFloats) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  const SceneHost& sc = s->scenes[0];
+  const jgs2_settings& set = sc.submitted;
+  if ((sc.KC > 0 || sc.dynamic) && set.ipc_barrier_stiffness > 0)
+    return fail(s, JGS2_UNSUPPORTED,
+                "Exact oracle diagnostics do not yet include IPC contact energy; disable IPC before requesting "
+                "this diagnostic.");
+  if (vertexRecords && vertexFloats < 36ull * sc.V)
+    return fail(s, JGS2_INVALID_ARGUMENT, "vertex_records holds fewer than 36 floats per vertex.");
+  if (tetRecords && tetFloats < 4ull * sc.T)
+    return fail(s, JGS2_INVALID_ARGUMENT, "tet_records holds fewer than 4 floats per tet.");
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  if (!s->oracleSummary) {
+    if ((st = deviceAlloc(s, &s->oracleTetRot, 3ull * std::max(1u, s->T))) != JGS2_OK) return st;
+    if ((st = deviceAlloc(s, &s->oracleTetMetric, std::max(1u, s->T))) != JGS2_OK) return st;
+    if ((st = deviceAlloc(s, &s->oracleVertex, 9ull * std::max(1u, s->V))) != JGS2_OK) return st;
+    if ((st = deviceAlloc(s, &s->oracleSummary, jgs2::kOracleSummaryWords)) != JGS2_OK) return st;
+  }
+  jgs2::OracleParams q{};
+  const double h = set.timestep;
+  q.invDt2 = static_cast<float>(1.0 / (h * h));
+  q.floorHeight = set.floor_height;
+  q.floorStiffness = set.floor_stiffness;
+  q.rotationEpsilon = set.rotation_epsilon;
+  q.objectiveFlags = sc.objectiveFlags;
+  q.vOff = sc.vOff;
+  q.V = sc.V;
+  q.tOff = sc.tOff;
+  q.T = sc.T;
+  q.corotated = s->glob ? 0u : 1u;
+  jgs2::launchOracleDiagnostics(s->b, q, s->oracleTetRot, s->oracleTetMetric, s->oracleVertex, s->oracleSummary,
+                                s->stream);
+  CUDA_TRY(s, cudaGetLastError());
+  double sum[jgs2::kOracleSummaryWords];
+  st = readRegion(s, s->oracleSummary, sizeof(sum), sum);
+  if (st != JGS2_OK) return st;
+  if (vertexRecords) {
+    st = readRegion(s, s->oracleVertex, sizeof(float) * 36ull * sc.V, vertexRecords);
+    if (st != JGS2_OK) return st;
+  }
+  if (tetRecords) {
+    st = readRegion(s, s->oracleTetMetric, sizeof(float) * 4ull * sc.T, tetRecords);
+    if (st != JGS2_OK) return st;
+  }
+  // reduceDiagnostics' closing arithmetic (jgs2-diagnostics.ts:1040-1090).
+  jgs2_oracle_diagnostics& d = *out;
+  d = jgs2_oracle_diagnostics{};
+  d.inertia = sum[0];
+  d.elasticity = sum[1];
+  d.external_force = sum[2];
+  d.quadratic_target = sum[3];
+  d.floor_contact = sum[4];
+  d.energy = sum[0] + sum[1] + sum[2] + sum[3] + sum[4];
+  d.gradient_squared_norm = sum[5];
+  d.gradient_norm = std::sqrt(std::max(sum[5], 0.0));
+  d.inertia_gradient_norm = std::sqrt(std::max(sum[6], 0.0));
+  d.material_gradient_norm = std::sqrt(std::max(sum[7], 0.0));
+  d.external_force_gradient_norm = std::sqrt(std::max(sum[8], 0.0));
+  d.target_gradient_norm = std::sqrt(std::max(sum[9], 0.0));
+  d.contact_gradient_norm = std::sqrt(std::max(sum[10], 0.0));
+  d.active_vertex_count = static_cast<uint32_t>(sum[14]);
+  d.gradient_valid = sum[14] > 0 ? 1u : 0u;
+  d.minimum_deformation_determinant_valid = sc.T > 0 ? 1u : 0u;
+  d.minimum_deformation_determinant = sc.T > 0 ? sum[12] : 0.0;
+  d.maximum_update = sum[11];
+  d.maximum_update_valid = (d.gradient_valid && sum[16] >= 0.5) ? 1u : 0u;
+  const bool floorValid = set.floor_stiffness > 0 && d.gradient_valid;
+  d.minimum_contact_distance_valid = floorValid ? 1u : 0u;
+  d.minimum_contact_distance = floorValid ? sum[13] : 0.0;
+  d.active_contact_count = floorValid ? static_cast<uint32_t>(sum[15]) : 0u;
+  d.residual_denominator = std::max(1.0, d.inertia_gradient_norm + d.material_gradient_norm +
+                                             d.external_force_gradient_norm + d.target_gradient_norm +
+                                             d.contact_gradient_norm);
+  d.relative_residual = d.gradient_norm / d.residual_denominator;
+  bool finite = sum[17] >= 0.5;
+  for (double v : {d.energy, d.gradient_norm, d.residual_denominator, d.relative_residual, d.maximum_update,
+                   d.minimum_deformation_determinant, d.minimum_contact_distance})
+    finite = finite && std::isfinite(v);
+  d.finite = finite ? 1u : 0u;
+  d.relative_residual_valid = (d.maximum_update_valid && finite) ? 1u : 0u;
+  return JGS2_OK;
 }
 
 jgs2_status jgs2_read_contact_candidates(jgs2_solver* s, uint32_t* out, uint64_t capacity, uint64_t* count) {

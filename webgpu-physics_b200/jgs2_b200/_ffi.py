@@ -49,6 +49,18 @@ class ContactSurface(Structure):
     ]
 
 
+class OracleDiagnostics(Structure):
+    _fields_ = [(name, c_double) for name in (
+        "energy", "inertia", "elasticity", "external_force", "quadratic_target", "floor_contact",
+        "inertia_gradient_norm", "material_gradient_norm", "external_force_gradient_norm", "target_gradient_norm",
+        "contact_gradient_norm", "gradient_norm", "gradient_squared_norm", "residual_denominator",
+        "relative_residual", "maximum_update", "minimum_deformation_determinant", "minimum_contact_distance")] + [
+        (name, c_uint32) for name in (
+            "active_vertex_count", "active_contact_count", "relative_residual_valid", "gradient_valid",
+            "maximum_update_valid", "minimum_deformation_determinant_valid", "minimum_contact_distance_valid",
+            "finite")]
+
+
 class Input(Structure):
     _fields_ = [
         ("vertex_count", c_uint32), ("tet_count", c_uint32),
@@ -271,6 +283,8 @@ def step_lib() -> ctypes.CDLL:
                                                 c_size_t, POINTER(c_uint32)]
         lib.jgs2_device_positions.argtypes = [vp, POINTER(c_void_p), POINTER(c_void_p)]
         lib.jgs2_read_contact_candidates.argtypes = [vp, POINTER(c_uint32), c_uint64, POINTER(c_uint64)]
+        lib.jgs2_read_oracle_diagnostics.argtypes = [vp, POINTER(OracleDiagnostics), POINTER(c_float), c_size_t,
+                                                     POINTER(c_float), c_size_t]
         lib.jgs2_minimum_contact_distance.argtypes = [POINTER(Input), c_double, POINTER(c_double)]
         lib.jgs2_contact_superset_size.argtypes = [POINTER(Input), POINTER(c_uint64)]
         lib.jgs2_evaluate_assembled_candidate.argtypes = [vp, POINTER(c_float), POINTER(c_float), S, c_uint32,

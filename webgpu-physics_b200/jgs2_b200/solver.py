@@ -343,6 +343,43 @@ class JGS2GpuSolver:
         self._check(fn(self._h, _ffi.fptr(out), out.size))
         return out
 
+    def readOracleDiagnostics(self) -> dict:
+        """readOracleDiagnostics: the exact all-element implicit-Euler oracle
+        at the current pose (summary in the reference's field names, plus
+        'vertexRecords' (V, 9, 4) and 'tetRecords' (T, 4) float32)."""
+        self._usable()
+        info = self.info()
+        V, T = info["vertex_count"], info["tet_count"]
+        out = _ffi.OracleDiagnostics()
+        vrec = np.zeros(36 * max(V, 1), dtype=np.float32)
+        trec = np.zeros(4 * max(T, 1), dtype=np.float32)
+        self._check(self._L.jgs2_read_oracle_diagnostics(self._h, byref(out), _ffi.fptr(vrec), vrec.size,
+                                                         _ffi.fptr(trec), trec.size))
+        d = {name: getattr(out, name) for name, _t in _ffi.OracleDiagnostics._fields_}
+        summary = {
+            "energy": d["energy"],
+            "components": {"inertia": d["inertia"], "elasticity": d["elasticity"],
+                           "externalForce": d["external_force"], "quadraticTarget": d["quadratic_target"],
+                           "floorContact": d["floor_contact"]},
+            "componentGradientNorms": {"inertia": d["inertia_gradient_norm"],
+                                       "material": d["material_gradient_norm"],
+                                       "externalForce": d["external_force_gradient_norm"],
+                                       "target": d["target_gradient_norm"], "contact": d["contact_gradient_norm"]},
+            "gradientNorm": d["gradient_norm"], "residualNumerator": d["gradient_norm"],
+            "relativeResidual": d["relative_residual"], "relativeResidualValid": bool(d["relative_residual_valid"]),
+            "residualDenominator": d["residual_denominator"], "gradientSquaredNorm": d["gradient_squared_norm"],
+            "gradientValid": bool(d["gradient_valid"]), "maximumUpdate": d["maximum_update"],
+            "maximumUpdateValid": bool(d["maximum_update_valid"]),
+            "minimumDeformationDeterminant": d["minimum_deformation_determinant"],
+            "minimumDeformationDeterminantValid": bool(d["minimum_deformation_determinant_valid"]),
+            "minimumContactDistance": d["minimum_contact_distance"],
+            "minimumContactDistanceValid": bool(d["minimum_contact_distance_valid"]),
+            "activeContactCount": d["active_contact_count"], "activeVertexCount": d["active_vertex_count"],
+            "finite": bool(d["finite"]),
+            "vertexRecords": vrec[:36 * V].reshape(V, 9, 4), "tetRecords": trec[:4 * T].reshape(T, 4),
+        }
+        return summary
+
     @property
     def contactCandidateCount(self) -> int:
         """Static candidates, or the broad phase's listing of the last iteration."""
