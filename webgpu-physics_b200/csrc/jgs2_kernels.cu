@@ -2292,7 +2292,15 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
 // reduceConvergence (:4105-4486), and the next iteration's vertex frames.
 // The five component norms are exact Euclidean norms accumulated in double;
 // the reference forms the same norms in f32 as scale * sqrt(sum((g/scale)^2)).
-__global__ void __launch_bounds__(kBlock) convergenceKernel(Buffers b, const DevParams* __restrict__ pp,
+// JGS2_CONV_MIN_BLOCKS: blocks per SM the convergence kernel's register
+// budget must allow (unset: the compiler's choice).
+#ifdef JGS2_CONV_MIN_BLOCKS
+#define JGS2_CONV_BOUNDS __launch_bounds__(kBlock, JGS2_CONV_MIN_BLOCKS)
+#else
+#define JGS2_CONV_BOUNDS __launch_bounds__(kBlock)
+#endif
+
+__global__ void JGS2_CONV_BOUNDS convergenceKernel(Buffers b, const DevParams* __restrict__ pp,
                                                             const float4* __restrict__ src, float4* tgt,
                                                             int nextRotations) {
   __shared__ ConvPartial smem[kBlock];

@@ -58,8 +58,14 @@ struct SceneRange {
 struct RedBlock {
   uint32_t scene, begin, end, slot;
 };
-constexpr uint32_t kGateChunk = 2048;  // tets / vertices per prologue or gate block
-constexpr uint32_t kConvChunk = 256;   // vertices per convergence block
+#ifndef JGS2_GATE_CHUNK
+#define JGS2_GATE_CHUNK 2048
+#endif
+constexpr uint32_t kGateChunk = JGS2_GATE_CHUNK;  // tets / vertices per prologue or gate block
+#ifndef JGS2_CONV_CHUNK
+#define JGS2_CONV_CHUNK 256
+#endif
+constexpr uint32_t kConvChunk = JGS2_CONV_CHUNK;  // vertices per convergence block
 
 // Reduction scratch and the GPU-resident control/history records
 // (dynamic arena regions globalizationControl/globalizationHistory,
