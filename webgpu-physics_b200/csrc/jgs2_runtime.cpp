@@ -2482,25 +2482,50 @@ jgs2_status jgs2_replace_external_forces(jgs2_solver* s, const float* forces) {
   jgs2_status st = usable(s);
   if (st != JGS2_OK) return st;
   if (!forces) return fail(s, JGS2_INVALID_ARGUMENT, "forces is NULL.");
-  for (uint32_t v = 0; v < s->V; ++v) {
-    bool nonzero = false;
-    for (int k = 0; k < 3; ++k) {
-      if (!std::isfinite(forces[3ull * v + k]))
-        return fail(s, JGS2_INVALID_ARGUMENT, format("External forces[%llu] must be finite after f32 conversion.",
-                                                     static_cast<unsigned long long>(3ull * v + k)));
-      nonzero |= forces[3ull * v + k] != 0;
+  // Checked and mirrored in chunks across host threads (a per-frame call on
+  // million-vertex solvers); the first failing entry in vertex order is
+  // reported, as a sequential pass would, and nothing is mirrored then.
+  constexpr uint32_t kChunk = 1u << 16;
+  const uint32_t chunks = (s->V + kChunk - 1) / kChunk;
+  std::vector<uint64_t> firstBad(chunks, UINT64_MAX);  // 3 v + k, or (V + v) << 2 for a pinned vertex
+  parallelFor(chunks, [&](uint32_t c) {
+    for (uint32_t v = c * kChunk; v < std::min(s->V, (c + 1) * kChunk); ++v) {
+      bool nonzero = false;
+      for (int k = 0; k < 3; ++k) {
+        if (!std::isfinite(forces[3ull * v + k])) {
+          firstBad[c] = 3ull * v + k;
+          return;
+        }
+        nonzero |= forces[3ull * v + k] != 0;
+      }
+      if (s->pinned[v] && nonzero) {
+        firstBad[c] = (uint64_t(s->V) * 3 + v) << 2;
+        return;
+      }
     }
-    if (s->pinned[v] && nonzero)
-      return fail(s, JGS2_INVALID_ARGUMENT, format("Pinned vertex %u cannot have a nonzero external force.", v));
+  });
+  for (uint32_t c = 0; c < chunks; ++c) {
+    if (firstBad[c] == UINT64_MAX) continue;
+    if (firstBad[c] < 3ull * s->V)
+      return fail(s, JGS2_INVALID_ARGUMENT, format("External forces[%llu] must be finite after f32 conversion.",
+                                                   static_cast<unsigned long long>(firstBad[c])));
+    const uint32_t v = static_cast<uint32_t>((firstBad[c] >> 2) - uint64_t(s->V) * 3);
+    return fail(s, JGS2_INVALID_ARGUMENT, format("Pinned vertex %u cannot have a nonzero external force.", v));
   }
   st = waitObjectiveMirror(s);
   if (st != JGS2_OK) return st;
+  std::vector<uint32_t> active(chunks, 0u);
+  parallelFor(chunks, [&](uint32_t c) {
+    uint32_t n = 0;
+    for (uint32_t v = c * kChunk; v < std::min(s->V, (c + 1) * kChunk); ++v) {
+      const float4 f = make_float4(forces[3ull * v], forces[3ull * v + 1], forces[3ull * v + 2], 0.f);
+      s->hForces[v] = f;
+      n += forceActive(f) ? 1u : 0u;
+    }
+    active[c] = n;
+  });
   uint32_t count = 0;
-  for (uint32_t v = 0; v < s->V; ++v) {
-    const float4 f = make_float4(forces[3ull * v], forces[3ull * v + 1], forces[3ull * v + 2], 0.f);
-    s->hForces[v] = f;
-    count += forceActive(f) ? 1u : 0u;
-  }
+  for (uint32_t n : active) count += n;
   s->scenes[0].forceCount = count;
   return writeObjectives(s, 0, 0, s->V, true, false);
 }
