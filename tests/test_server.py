@@ -83,3 +83,24 @@ def test_batch_without_colouring_refuses_graph_coloured_steps(bars):
     with pytest.raises(_ffi.JGS2Error, match="without graph colouring"):
         batch.stepFrames(1, exactIterations=2, overrides={"schedule": "graph-colored-gauss-seidel"})
     batch.destroy()
+
+
+@pytest.mark.gpu
+def test_served_contact_surface_requests_equal_results_alone():
+    # Trough requests through the device broad phase share waves; each keeps
+    # its own rows, list span and reductions, so it runs as it runs alone.
+    # (Alone here is a one-scene batch: the contact scenes' static twins
+    # would colour past 256 colours, and a batch does not colour.)
+    troughs = [scenes.trough(n, contact=scenes.CONTACT_SURFACE) for n in (1, 2, 3)]
+    st = dict(scenes.TROUGH_SETTINGS)
+    requests = [(troughs[0], 6), (troughs[1], 4), (troughs[2], 6), (troughs[1], 2)]
+    srv = server.JGS2Server(memoryBudgetBytes=1 << 32)
+    ids = [srv.submit(inp, st, frames=f, exactIterations=3) for inp, f in requests]
+    results = [srv.wait(i) for i in ids]
+    srv.destroy()
+    for (inp, f), r in zip(requests, results):
+        assert r["status"] == 0 and r["frames"] == f
+        alone = solver.JGS2Batch.create([inp], [st])
+        alone.stepFrames(f, exactIterations=3)
+        np.testing.assert_array_equal(r["positions"], alone.readPositions(0))
+        alone.destroy()
