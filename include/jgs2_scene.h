@@ -52,10 +52,12 @@ typedef struct jgs2_precompute_options {
   uint32_t method;          /* JGS2_PRECOMPUTE_* */
   uint32_t patch_radius;    /* free rings around the source vertex (patch method) */
   uint32_t threads;         /* 0 = all hardware threads */
-  uint32_t mode_count;      /* training modes, 8 (nonlinear-cubature.ts:13) */
-  uint32_t inverse_iterations; /* 24 (nonlinear-cubature.ts:15) */
+  uint32_t mode_count;      /* training modes, 8 (nonlinear-cubature.ts:13;
+                             * precompute.ts:20 for co-rotated scenes) */
+  uint32_t inverse_iterations; /* 24 (nonlinear-cubature.ts:15; precompute.ts:21) */
   double training_amplitude;   /* 0.12 (nonlinear-cubature.ts:16) */
-  uint32_t refinement_passes;  /* 12 (nonlinear-cubature-training.ts:737) */
+  uint32_t refinement_passes;  /* 12 (nonlinear-cubature-training.ts:737);
+                                * co-rotated scenes use 4 (cubature.ts:52) */
   /* Nonzero: skip training and write the exact complement instead — one
    * weight-1 record per candidate tetrahedron (the "exact-all remainder" of
    * assembleStableNeoHookeanJGS2LocalSystem, nonlinear-cubature-training.ts:

@@ -4,6 +4,7 @@
 //   src/simulation/cpu/precompute.ts:141-206     (computeExactVertexBasis)
 //   src/simulation/cpu/cubature.ts:55-297        (low-frequency modes)
 //   src/simulation/cpu/cubature.ts:371-690       (greedy NNLS selection)
+//   src/simulation/cpu/cubature.ts:312-369, 714-820 (co-rotated linear training)
 //   src/simulation/cpu/nonlinear-cubature.ts:140-620 (pose corpus)
 //   src/simulation/cpu/nonlinear-cubature-training.ts:189-843 (training)
 //
@@ -29,6 +30,7 @@ constexpr double kMinimumPoseDeterminant = 0.5;        // nonlinear-cubature.ts:
 constexpr uint32_t kValidationOnlyModes = 4;           // nonlinear-cubature.ts:14
 constexpr double kResidualTolerance = 0.01;            // nonlinear-cubature-training.ts:23
 constexpr double kMatrixEpsilon = 1e-14;               // math.ts:1
+constexpr int kLinearRefinementPasses = 4;             // cubature.ts:52
 
 // ---- dense linear algebra -------------------------------------------------
 
@@ -228,6 +230,11 @@ struct Context {
   int poses = 0;
   std::vector<std::vector<double>> frames, elemGrad;
   bool amplitudeReduced = false;
+  // Co-rotated linear training: low-frequency displacement poses (3 * Vp
+  // each) and the rest stiffness of every tetrahedron (144 * Tp).
+  bool linear = false;
+  std::vector<std::vector<double>> linearPoses;
+  std::vector<double> stiffness;
 };
 
 void deformationGradient(const Problem& pb, uint32_t t, const double* x, double* F) {
@@ -531,6 +538,25 @@ void buildCorpus(Context& ctx, const jgs2_precompute_options& opt) {
   }
 }
 
+// Training data of the co-rotated linear path (precompute.ts:261-268): the
+// low-frequency modes of the rest system as displacement poses, and each
+// tetrahedron's rest stiffness.
+void buildLinearPoses(Context& ctx, const jgs2_precompute_options& opt) {
+  const Problem& pb = *ctx.pb;
+  ctx.linear = true;
+  ctx.linearPoses = lowFrequencyModes(ctx, static_cast<int>(opt.mode_count),
+                                      static_cast<int>(opt.inverse_iterations));
+  ctx.stiffness.assign(144ull * pb.Tp, 0.0);
+  for (uint32_t t = 0; t < pb.Tp; ++t)
+    linearStiffness(&pb.invRest[9ull * t], pb.vol[t], *pb.mats[t], &ctx.stiffness[144ull * t]);
+}
+
+void prepareTraining(Context& ctx, const jgs2_precompute_options& opt, bool linear) {
+  if (opt.exact_complement) return;
+  if (linear) buildLinearPoses(ctx, opt);
+  else buildCorpus(ctx, opt);
+}
+
 // ---- nonnegative least squares over small column sets ---------------------
 
 struct Gram {
@@ -754,6 +780,15 @@ struct LocalRecord {
   std::array<double, 36> basis;
 };
 
+// selectCubatureSamples (src/simulation/cpu/cubature.ts:714-820): one column
+// per tetrahedron holding, at every training pose, its reduced gradient
+// (evaluateReducedTetGradient, cubature.ts:312-369: rest stiffness times the
+// pose plus the tetrahedron's share of the inertia, projected by the exact
+// basis, less the source slot's own row); per-pose normalisation by the norm
+// of the summed target; greedy nonnegative selection; positive weights kept.
+double trainLinear(const Context& ctx, uint32_t s, const std::vector<double>& ubar,
+                   const jgs2_precompute_options& opt, std::vector<LocalRecord>& records);
+
 // computeExactVertexBasis (precompute.ts:141-206) + the training for one
 // source vertex (selectStableNeoHookeanCubatureSamples,
 // nonlinear-cubature-training.ts:689-843).
@@ -802,6 +837,7 @@ double trainSource(const Context& ctx, uint32_t s, const jgs2_precompute_options
     }
     return 0.0;
   }
+  if (ctx.linear) return trainLinear(ctx, s, ubar, opt, records);
   // Stacked training system (buildStackedTrainingSystem,
   // nonlinear-cubature-training.ts:473-552) with per-pose normalisation.
   const int P = ctx.poses;
@@ -855,6 +891,78 @@ double trainSource(const Context& ctx, uint32_t s, const jgs2_precompute_options
   Selection sel = greedySelect(cols, target, static_cast<int>(opt.cubature_k),
                                static_cast<int>(opt.refinement_passes));
   subsetAudit(cols, target, static_cast<int>(opt.cubature_k), sel);
+  for (size_t i = 0; i < sel.tets.size(); ++i) {
+    if (!(sel.weights[i] > 1e-10)) continue;
+    LocalRecord rec;
+    rec.tet = sel.tets[i];
+    rec.weight = sel.weights[i];
+    for (int l = 0; l < 4; ++l) {
+      const uint32_t v = pb.tets[4ull * rec.tet + l];
+      for (int e = 0; e < 9; ++e) rec.basis[l * 9 + e] = ubar[9ull * v + e];
+    }
+    records.push_back(rec);
+  }
+  return sel.residual;
+}
+
+double trainLinear(const Context& ctx, uint32_t s, const std::vector<double>& ubar,
+                   const jgs2_precompute_options& opt, std::vector<LocalRecord>& records) {
+  const Problem& pb = *ctx.pb;
+  const int P = static_cast<int>(ctx.linearPoses.size());
+  const double invH2 = 1.0 / (ctx.h * ctx.h);
+  std::vector<std::vector<double>> cols(pb.Tp, std::vector<double>(3ull * P, 0.0));
+  std::vector<double> target(3ull * P, 0.0);
+  for (int p = 0; p < P; ++p) {
+    const double* pose = ctx.linearPoses[p].data();
+    double poseTarget[3] = {0, 0, 0}, scaleSq = 0;
+    for (uint32_t t = 0; t < pb.Tp; ++t) {
+      const uint32_t* q = &pb.tets[4ull * t];
+      const double* k = &ctx.stiffness[144ull * t];
+      double u[12], g[12];
+      for (int c = 0; c < 12; ++c) u[c] = pose[3ull * q[c / 3] + c % 3];
+      for (int r = 0; r < 12; ++r) {
+        double val = 0;
+        for (int c = 0; c < 12; ++c) val += k[r * 12 + c] * u[c];
+        const uint32_t v = q[r / 3];
+        g[r] = val + pb.mass[v] * invH2 * u[r] / pb.incident[v];
+      }
+      double red[3] = {0, 0, 0};
+      for (int l = 0; l < 4; ++l) {
+        const double* U = &ubar[9ull * q[l]];
+        for (int rc = 0; rc < 3; ++rc)
+          for (int c = 0; c < 3; ++c) red[c] += U[rc * 3 + c] * g[l * 3 + rc];
+      }
+      for (int l = 0; l < 4; ++l)
+        if (q[l] == s) {
+          for (int c = 0; c < 3; ++c) red[c] -= g[l * 3 + c];
+          break;
+        }
+      for (int c = 0; c < 3; ++c) {
+        cols[t][3ull * p + c] = red[c];
+        poseTarget[c] += red[c];
+        scaleSq += red[c] * red[c];
+      }
+    }
+    const double poseNorm = std::sqrt(poseTarget[0] * poseTarget[0] + poseTarget[1] * poseTarget[1] +
+                                      poseTarget[2] * poseTarget[2]);
+    // A target that cancels to below 1e-6 of its terms (seen on local
+    // patches) would scale its rows by up to 1e12 and swamp the fit, so such
+    // a pose is dropped; the reference normalises every pose above 1e-12.
+    if (poseNorm <= 1e-6 * std::sqrt(scaleSq)) {
+      for (uint32_t t = 0; t < pb.Tp; ++t)
+        for (int c = 0; c < 3; ++c) cols[t][3ull * p + c] = 0.0;
+      continue;
+    }
+    if (poseNorm > 1e-12)
+      for (int c = 0; c < 3; ++c) {
+        target[3ull * p + c] = poseTarget[c] / poseNorm;
+        for (uint32_t t = 0; t < pb.Tp; ++t) cols[t][3ull * p + c] /= poseNorm;
+      }
+  }
+  bool anyColumn = false;
+  for (const auto& col : cols) anyColumn |= dotv(col.data(), col.data(), col.size()) > 1e-18;
+  if (!(std::sqrt(dotv(target.data(), target.data(), target.size())) > 1e-12) || !anyColumn) return 0.0;
+  const Selection sel = greedySelect(cols, target, static_cast<int>(opt.cubature_k), kLinearRefinementPasses);
   for (size_t i = 0; i < sel.tets.size(); ++i) {
     if (!(sel.weights[i] > 1e-10)) continue;
     LocalRecord rec;
@@ -1049,13 +1157,6 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
   }
   jgs2_precompute_stats st{};
   std::vector<double> residuals(V, -1.0);
-  if (anyCorotated && !opt.exact_complement) {
-    // Co-rotated scenes run the exact local gather only (no cubature records)
-    // unless the exact complement is asked for.
-    st.seconds = std::chrono::duration<double>(std::chrono::steady_clock::now() - start).count();
-    if (stats) *stats = st;
-    return true;
-  }
   std::vector<uint32_t> incident(V, 0);
   for (uint32_t v : m.tets) incident[v]++;
   if (opt.method == JGS2_PRECOMPUTE_EXACT) {
@@ -1080,7 +1181,7 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
     ctx.pb = &pb;
     ctx.h = opt.timestep;
     if (!buildSystem(ctx)) { sc.error = "A simulation scene must have at least one movable vertex."; return false; }
-    if (!opt.exact_complement) buildCorpus(ctx, opt);
+    prepareTraining(ctx, opt, anyCorotated);
     st.training_classes = 1;
     st.reduced_amplitude_classes = ctx.amplitudeReduced ? 1 : 0;
     std::vector<uint32_t> sources;
@@ -1145,7 +1246,7 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
         ctx.pb = &pb;
         ctx.h = opt.timestep;
         if (!buildSystem(ctx)) continue;
-        if (!opt.exact_complement) buildCorpus(ctx, opt);
+        prepareTraining(ctx, opt, anyCorotated);
         classReduced[c] = ctx.amplitudeReduced ? 1 : 0;
         classResidual[c] = trainSource(ctx, sl, opt, classRecords[c]);
       } catch (const std::exception& e) {
@@ -1177,7 +1278,7 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
       ctx.pb = &pb;
       ctx.h = opt.timestep;
       if (!buildSystem(ctx)) continue;
-      if (!opt.exact_complement) buildCorpus(ctx, opt);
+      prepareTraining(ctx, opt, anyCorotated);
       std::vector<LocalRecord> recs;
       residuals[sources[i]] = trainSource(ctx, sl, opt, recs);
       writeRecords(sc, sources[i], pb, recs, K);
