@@ -71,12 +71,16 @@ def test_corotated_gpu_matches_oracle(schedule, exact_complement):
     cpu = O.OracleSolver(inp, s, precision=32)
     assert not gpu.globalizationEnabled
     # With trained cubature (K = 4 of 192 tets, weights up to ~12) the
-    # co-rotated Jacobi sweep diverges: the f32 and f64 oracles themselves
-    # part by 3e-6 of the box after 1 frame, 3e-3 after 2 and 0.4 after 3.
-    # It is compared over the first frame; with the exact complement over 20.
-    for _ in range(20 if exact_complement else 1):
-        gpu.stepExactIterations(4)
-        cpu.step_exact_iterations(4)
+    # co-rotated sweep diverges: under Jacobi the f32 and f64 oracles
+    # themselves part by 3e-6 of the box after 1 frame, 3e-3 after 2 and 0.4
+    # after 3; under GGS2 by 1e-6 after one iteration, 5e-3 after two and 0.2
+    # after three.  Trained runs are compared over one frame (one iteration
+    # under GGS2); with the exact complement over 20 frames.
+    frames = 20 if exact_complement else 1
+    iterations = 1 if not exact_complement and schedule == 1 else 4
+    for _ in range(frames):
+        gpu.stepExactIterations(iterations)
+        cpu.step_exact_iterations(iterations)
     _compare(inp, gpu, cpu)
     gpu.destroy()
 
