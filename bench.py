@@ -58,6 +58,8 @@ def parse_args():
     ap.add_argument("--preroll", type=int, default=None,
                     help="untimed frames before the timed ones (trough 96, boxes 60, cloth the warm-up)")
     ap.add_argument("--bodies", type=int, default=256, help="scenes of the batched workload")
+    ap.add_argument("--tune-rounds", type=int, default=2,
+                    help="cube and batched workloads: autotuner rounds (frames per launch shape) before the warm-up; 0 = off")
     args = ap.parse_args()
     if args.iterations is None:
         args.iterations = 10 if args.workload == "batched" else 20
@@ -330,6 +332,12 @@ def batched_arm(args):
     stream = torch.cuda.ExternalStream(batch.stream(), device=device)
     active = sum(p.active_vertex_count() for p in parts)
     V = sum(p.vertex_count for p in parts)
+    # Launch shapes from the autotuner: untimed frames, one shape per frame in
+    # turn, before the warm-up.
+    if args.tune_rounds > 0:
+        batch.autotune(args.tune_rounds)
+        batch.stepFrames(3 * args.tune_rounds, exactIterations=iters)
+    shape = batch.launchShape()
     for _ in range(args.warmup):
         batch.stepFrames(1, exactIterations=iters)
     batch.awaitIdle()
@@ -392,6 +400,9 @@ def batched_arm(args):
                 "l2": (f"no flush: one iteration touches {algorithmic / iters / 1e9:.2f} GB of resident state, "
                        "more than the 126 MB L2"),
                 "precompute": {"cached": cached, "seconds": round(build_s, 1)},
+                "launch_shape": {"autotuned": args.tune_rounds > 0, "shape": shape["shape"],
+                                 "solve_vertices_per_block": shape["solveVerticesPerBlock"],
+                                 "tuning_frame_ms": [round(m, 3) for m in shape["frameMs"]]},
                 "parallelism": "replicas" if world > 1 else "single GPU"},
             "frames_per_s": world * len(parts) * 1e3 * args.steps / ms,
             "gpu_launches": int(launches),
@@ -595,6 +606,12 @@ def ours_arm(args):
     iters = args.iterations
     active = inp.active_vertex_count()
 
+    # Launch shapes from the autotuner: untimed frames, one shape per frame in
+    # turn, before the warm-up.
+    if args.tune_rounds > 0:
+        s.autotune(args.tune_rounds)
+        s.stepFramesExactIterations(3 * args.tune_rounds, iters)
+    shape = s.launchShape()
     for _ in range(args.warmup):
         s.stepExactIterations(iters)
     s.awaitIdle()
@@ -665,6 +682,9 @@ def ours_arm(args):
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
             "config": workload_config(inp, args, {"cached": cached, "seconds": round(build_s, 1)}) | {
+                "launch_shape": {"autotuned": args.tune_rounds > 0, "shape": shape["shape"],
+                                 "solve_vertices_per_block": shape["solveVerticesPerBlock"],
+                                 "tuning_frame_ms": [round(m, 3) for m in shape["frameMs"]]},
                 "parallelism": "replicas" if world > 1 else "single GPU"},
             "frames_per_s": world * 1e3 / ms_per_step,
             "gpu_launches": int(launches),

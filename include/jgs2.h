@@ -471,6 +471,31 @@ jgs2_status jgs2_device_positions(jgs2_solver* solver, void** device_ptr,
  * library issues is counted, including graph replays). */
 uint64_t jgs2_kernel_launch_count(const jgs2_solver* solver);
 
+/* Launch shapes and their autotuner (no counterpart in the reference, whose
+ * workgroup sizes are fixed in its shaders).  A shape sets how many vertices
+ * one block of the local-solve kernel takes: the default (32 vertices of 4
+ * lanes, or 4 warps of the contact-heavy warp-per-vertex form, fewer when
+ * the cubature cache fills shared memory) shifted right by the shape, 0-2.
+ * Each vertex's arithmetic is the same in every shape, so results are
+ * bit-identical whichever shape runs.
+ *
+ * jgs2_autotune starts online tuning: the next rounds x JGS2_LAUNCH_SHAPES
+ * frames stepped (by any step call) take the shapes in turn, each timed with
+ * a CUDA event pair (the stream waits after each timed frame), and the shape
+ * with the smallest median frame time is then kept.  rounds must be 1-64.
+ * jgs2_set_launch_shape fixes a shape (a cached choice) and ends tuning. */
+#define JGS2_LAUNCH_SHAPES 3
+typedef struct jgs2_launch_shape {
+  uint32_t shape;                     /* the shape in use, 0-2 */
+  uint32_t solve_vertices_per_block;  /* of the 4-lane form, for this K */
+  uint32_t tuning;                    /* frames still to time, 0 when done */
+  uint32_t samples;                   /* fewest frames timed for one shape */
+  double frame_ms[JGS2_LAUNCH_SHAPES];/* median timed frame per shape, 0 = none */
+} jgs2_launch_shape;
+jgs2_status jgs2_autotune(jgs2_solver* solver, uint32_t rounds);
+jgs2_status jgs2_get_launch_shape(jgs2_solver* solver, jgs2_launch_shape* out);
+jgs2_status jgs2_set_launch_shape(jgs2_solver* solver, uint32_t shape);
+
 /* ---- batched form ---------------------------------------------------------
  * Many independent scenes stepped together by one launch sequence.  The
  * reference has no batched solver: each scene would be its own
@@ -512,6 +537,11 @@ jgs2_status jgs2_batch_read_globalization(jgs2_batch* batch, uint32_t scene, flo
 /* Positions of all scenes, concatenated in scene order (4 floats per vertex). */
 jgs2_status jgs2_batch_read_all_positions(jgs2_batch* batch, float* out, size_t floats);
 uint64_t jgs2_batch_kernel_launch_count(const jgs2_batch* batch);
+/* Launch shapes of a batch, as jgs2_autotune / jgs2_get_launch_shape /
+ * jgs2_set_launch_shape for a solver. */
+jgs2_status jgs2_batch_autotune(jgs2_batch* batch, uint32_t rounds);
+jgs2_status jgs2_batch_get_launch_shape(jgs2_batch* batch, jgs2_launch_shape* out);
+jgs2_status jgs2_batch_set_launch_shape(jgs2_batch* batch, uint32_t shape);
 /* The batch's CUDA stream (a cudaStream_t), for event timing and ordering. */
 void* jgs2_batch_stream(const jgs2_batch* batch);
 /* An inactive scene sits every following frame out: its state stays as it

@@ -2840,8 +2840,9 @@ int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, c
 int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
                 uint32_t count, uint32_t K, bool cachedIncident, cudaStream_t s) {
   if (count == 0) return 0;
-  const uint32_t groups = solveGroupsPerBlock(K);
-  if (groups == 0) return 0;
+  const uint32_t fit = solveGroupsPerBlock(K);
+  if (fit == 0) return 0;
+  const uint32_t groups = std::max(1u, fit >> std::min(b.solveShift, 2u));
   const size_t smem = static_cast<size_t>(groups) * K * sizeof(CubState);
   // One vertex per lane group: the line search makes per-vertex work uneven,
   // and the block scheduler balances it better than a fixed grid stride.

@@ -165,7 +165,9 @@ struct Buffers {
   uint32_t contactDynamic;
   uint32_t bpRowTotal, bpTriTotal, bpEdgeTotal, bpSentinel, bpSortPasses;
   uint32_t bpSuperset;  // candidates of the static superset (clamped to 2^32 - 1)
-  uint32_t bpPad;
+  // Host-side launch shape: the solve kernel takes its default vertices per
+  // block shifted right by this (0-2); scheduling only, never arithmetic.
+  uint32_t solveShift;
   const uint4* bpRows;
   const uint4* bpTris;
   const uint2* bpEdges;

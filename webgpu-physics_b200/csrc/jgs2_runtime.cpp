@@ -894,8 +894,14 @@ struct Engine {
   uint32_t* dNeedVertices = nullptr;
   std::vector<void*> allocations;
   uint64_t launches = 0;
-  // graphs: (iterations, schedule, bodyCorrection, contact) -> exec, launches per replay
-  std::map<std::tuple<uint32_t, uint32_t, bool, bool>, std::pair<cudaGraphExec_t, int>> graphs;
+  // graphs: (iterations, schedule, bodyCorrection, contact, launch shape) ->
+  // exec, launches per replay
+  std::map<std::tuple<uint32_t, uint32_t, bool, bool, uint32_t>, std::pair<cudaGraphExec_t, int>> graphs;
+  // Online launch-shape tuning: frames left to time, the next shape to time,
+  // per-shape frame times (ms) and the event pair around a timed frame.
+  uint32_t tuneLeft = 0, tuneNext = 0, tuneRounds = 0;
+  std::vector<float> tuneMs[JGS2_LAUNCH_SHAPES];
+  cudaEvent_t tuneEvents[2] = {nullptr, nullptr};
   // Oracle diagnostics records, allocated at the first request.
   float4* oracleTetRot = nullptr;
   float4* oracleTetMetric = nullptr;
@@ -972,6 +978,8 @@ void releaseDevice(Engine* s) {
   if (s->hForces) cudaFreeHost(s->hForces);
   if (s->hTargets) cudaFreeHost(s->hTargets);
   s->hForces = s->hTargets = nullptr;
+  for (cudaEvent_t& e : s->tuneEvents)
+    if (e) { cudaEventDestroy(e); e = nullptr; }
   if (s->objectiveUpload) cudaEventDestroy(s->objectiveUpload);
   s->objectiveUpload = nullptr;
   if (s->stream) cudaStreamDestroy(s->stream);
@@ -1180,6 +1188,13 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
   return n;
 }
 
+double medianMs(std::vector<float> v) {
+  if (v.empty()) return 0.0;
+  std::sort(v.begin(), v.end());
+  const size_t n = v.size();
+  return n % 2 ? v[n / 2] : 0.5 * (static_cast<double>(v[n / 2 - 1]) + v[n / 2]);
+}
+
 // Encodes `frames` frames of `iterations` iterations for every scene with its
 // resolved settings (one per scene; the schedule must agree).
 jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t frames, uint32_t iterations,
@@ -1221,8 +1236,14 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
   CUDA_TRY(s, cudaSetDevice(s->device));
   CUDA_TRY(s, cudaMemcpyAsync(s->dParams, s->hParams.data(), sizeof(DevParams) * s->hParams.size(),
                               cudaMemcpyHostToDevice, s->stream));
-  const auto key = std::make_tuple(iterations, schedule, body, contact);
-  if (s->useGraphs && !prof) {
+  // One frame in the engine's current launch shape: a graph replay (captured
+  // at the first use of the key) or, without graphs, direct launches.
+  auto frame = [&]() -> jgs2_status {
+    if (!s->useGraphs || prof) {
+      s->launches += encodeFrame(s, iterations, schedule, body, contact, prof);
+      return JGS2_OK;
+    }
+    const auto key = std::make_tuple(iterations, schedule, body, contact, s->b.solveShift);
     auto it = s->graphs.find(key);
     if (it == s->graphs.end()) {
       cudaGraph_t graph = nullptr;
@@ -1236,12 +1257,37 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
       if (e != cudaSuccess) return cudaFail(s, e, "cudaGraphInstantiate");
       it = s->graphs.emplace(key, std::make_pair(exec, n)).first;
     }
-    for (uint32_t f = 0; f < frames; ++f) {
-      CUDA_TRY(s, cudaGraphLaunch(it->second.first, s->stream));
-      s->launches += static_cast<uint64_t>(it->second.second);
+    CUDA_TRY(s, cudaGraphLaunch(it->second.first, s->stream));
+    s->launches += static_cast<uint64_t>(it->second.second);
+    return JGS2_OK;
+  };
+  for (uint32_t f = 0; f < frames; ++f) {
+    if (s->tuneLeft == 0 || prof) {
+      const jgs2_status st2 = frame();
+      if (st2 != JGS2_OK) return st2;
+      continue;
     }
-  } else {
-    for (uint32_t f = 0; f < frames; ++f) s->launches += encodeFrame(s, iterations, schedule, body, contact, prof);
+    // Tuned frame: the shapes take turns; each frame is timed on the stream.
+    const uint32_t shape = s->tuneNext;
+    s->b.solveShift = shape;
+    CUDA_TRY(s, cudaEventRecord(s->tuneEvents[0], s->stream));
+    const jgs2_status st2 = frame();
+    if (st2 != JGS2_OK) return st2;
+    CUDA_TRY(s, cudaEventRecord(s->tuneEvents[1], s->stream));
+    CUDA_TRY(s, cudaEventSynchronize(s->tuneEvents[1]));
+    float ms = 0.0f;
+    CUDA_TRY(s, cudaEventElapsedTime(&ms, s->tuneEvents[0], s->tuneEvents[1]));
+    s->tuneMs[shape].push_back(ms);
+    s->tuneNext = (shape + 1) % JGS2_LAUNCH_SHAPES;
+    if (--s->tuneLeft == 0) {
+      uint32_t best = 0;
+      double bestMs = 0;
+      for (uint32_t c = 0; c < JGS2_LAUNCH_SHAPES; ++c) {
+        const double m = medianMs(s->tuneMs[c]);
+        if (c == 0 || m < bestMs) { best = c; bestMs = m; }
+      }
+      s->b.solveShift = best;
+    }
   }
   CUDA_TRY(s, cudaGetLastError());
   for (uint32_t i = 0; i < s->scenes.size(); ++i) {
@@ -2797,6 +2843,60 @@ jgs2_status jgs2_device_positions(jgs2_solver* s, void** ptr, void** stream) {
 
 uint64_t jgs2_kernel_launch_count(const jgs2_solver* s) { return s ? s->launches : 0; }
 
+namespace {
+
+jgs2_status startTuning(Engine* s, uint32_t rounds) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (rounds < 1 || rounds > 64)
+    return fail(s, JGS2_INVALID_ARGUMENT, format("Autotuning rounds must be 1-64; got %u.", rounds));
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  for (cudaEvent_t& e : s->tuneEvents)
+    if (!e) CUDA_TRY(s, cudaEventCreate(&e));
+  for (auto& v : s->tuneMs) v.clear();
+  s->tuneRounds = rounds;
+  s->tuneLeft = rounds * JGS2_LAUNCH_SHAPES;
+  s->tuneNext = 0;
+  return JGS2_OK;
+}
+
+jgs2_status readShape(Engine* s, jgs2_launch_shape* out) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out) return fail(s, JGS2_INVALID_ARGUMENT, "out is NULL.");
+  *out = jgs2_launch_shape{};
+  out->shape = s->b.solveShift;
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  const uint32_t fit = jgs2::solveGroupsPerBlock(s->K);
+  const uint32_t groups = std::max(1u, fit >> s->b.solveShift);
+  out->solve_vertices_per_block = fit == 0 ? 0 : groups;
+  out->tuning = s->tuneLeft;
+  uint32_t fewest = ~0u;
+  for (uint32_t c = 0; c < JGS2_LAUNCH_SHAPES; ++c) {
+    out->frame_ms[c] = medianMs(s->tuneMs[c]);
+    fewest = std::min<uint32_t>(fewest, static_cast<uint32_t>(s->tuneMs[c].size()));
+  }
+  out->samples = fewest;
+  return JGS2_OK;
+}
+
+jgs2_status fixShape(Engine* s, uint32_t shape) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (shape >= JGS2_LAUNCH_SHAPES)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("Launch shape must be below %u; got %u.", JGS2_LAUNCH_SHAPES, shape));
+  s->b.solveShift = shape;
+  s->tuneLeft = 0;
+  return JGS2_OK;
+}
+
+}  // namespace
+
+jgs2_status jgs2_autotune(jgs2_solver* s, uint32_t rounds) { return startTuning(s, rounds); }
+jgs2_status jgs2_get_launch_shape(jgs2_solver* s, jgs2_launch_shape* out) { return readShape(s, out); }
+jgs2_status jgs2_set_launch_shape(jgs2_solver* s, uint32_t shape) { return fixShape(s, shape); }
+
 // ---- batches -------------------------------------------------------------------
 
 jgs2_status jgs2_batch_create(const jgs2_input* const* inputs, uint32_t scene_count, const jgs2_settings* settings,
@@ -2925,6 +3025,9 @@ jgs2_status jgs2_batch_read_all_positions(jgs2_batch* s, float* out, size_t floa
 }
 
 uint64_t jgs2_batch_kernel_launch_count(const jgs2_batch* s) { return s ? s->launches : 0; }
+jgs2_status jgs2_batch_autotune(jgs2_batch* s, uint32_t rounds) { return startTuning(s, rounds); }
+jgs2_status jgs2_batch_get_launch_shape(jgs2_batch* s, jgs2_launch_shape* out) { return readShape(s, out); }
+jgs2_status jgs2_batch_set_launch_shape(jgs2_batch* s, uint32_t shape) { return fixShape(s, shape); }
 
 uint32_t jgs2_batch_vertex_count(const jgs2_batch* s) { return s ? s->V : 0u; }
 

@@ -49,6 +49,14 @@ class ContactSurface(Structure):
     ]
 
 
+LAUNCH_SHAPES = 3
+
+
+class LaunchShape(Structure):
+    _fields_ = [("shape", c_uint32), ("solve_vertices_per_block", c_uint32), ("tuning", c_uint32),
+                ("samples", c_uint32), ("frame_ms", c_double * LAUNCH_SHAPES)]
+
+
 class OracleDiagnostics(Structure):
     _fields_ = [(name, c_double) for name in (
         "energy", "inertia", "elasticity", "external_force", "quadratic_target", "floor_contact",
@@ -291,6 +299,10 @@ def step_lib() -> ctypes.CDLL:
                                                           POINTER(c_float), POINTER(c_float), POINTER(c_float)]
         lib.jgs2_kernel_launch_count.argtypes = [vp]
         lib.jgs2_kernel_launch_count.restype = c_uint64
+        for prefix in ("jgs2_", "jgs2_batch_"):
+            getattr(lib, prefix + "autotune").argtypes = [vp, c_uint32]
+            getattr(lib, prefix + "get_launch_shape").argtypes = [vp, POINTER(LaunchShape)]
+            getattr(lib, prefix + "set_launch_shape").argtypes = [vp, c_uint32]
         lib.jgs2_batch_create.argtypes = [POINTER(POINTER(Input)), c_uint32, S, POINTER(c_uint32), c_int,
                                           POINTER(vp)]
         lib.jgs2_batch_destroy.argtypes = [vp]

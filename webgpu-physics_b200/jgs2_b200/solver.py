@@ -246,6 +246,25 @@ class JGS2GpuSolver:
     def kernelLaunchCount(self) -> int:
         return int(self._L.jgs2_kernel_launch_count(self._h)) if self._h else 0
 
+    # Launch shapes (include/jgs2.h): vertices per block of the local-solve
+    # kernel; every shape gives bit-identical results.
+    def autotune(self, rounds: int = 3):
+        """Time the next rounds x 3 frames stepped, one shape per frame in
+        turn, then keep the fastest shape."""
+        self._usable()
+        self._check(getattr(self._L, "jgs2_" + "autotune")(self._h, int(rounds)))
+
+    def launchShape(self) -> dict:
+        self._usable()
+        out = _ffi.LaunchShape()
+        self._check(getattr(self._L, "jgs2_" + "get_launch_shape")(self._h, byref(out)))
+        return dict(shape=int(out.shape), solveVerticesPerBlock=int(out.solve_vertices_per_block),
+                    tuning=int(out.tuning), samples=int(out.samples), frameMs=list(out.frame_ms))
+
+    def setLaunchShape(self, shape: int):
+        self._usable()
+        self._check(getattr(self._L, "jgs2_" + "set_launch_shape")(self._h, int(shape)))
+
     def devicePositions(self):
         """(device pointer, cudaStream_t) of the canonical position array."""
         self._usable()
@@ -513,6 +532,25 @@ class JGS2Batch:
 
     def kernelLaunchCount(self) -> int:
         return int(self._L.jgs2_batch_kernel_launch_count(self._h)) if self._h else 0
+
+    # Launch shapes (include/jgs2.h): vertices per block of the local-solve
+    # kernel; every shape gives bit-identical results.
+    def autotune(self, rounds: int = 3):
+        """Time the next rounds x 3 frames stepped, one shape per frame in
+        turn, then keep the fastest shape."""
+        self._usable()
+        self._check(getattr(self._L, "jgs2_batch_" + "autotune")(self._h, int(rounds)))
+
+    def launchShape(self) -> dict:
+        self._usable()
+        out = _ffi.LaunchShape()
+        self._check(getattr(self._L, "jgs2_batch_" + "get_launch_shape")(self._h, byref(out)))
+        return dict(shape=int(out.shape), solveVerticesPerBlock=int(out.solve_vertices_per_block),
+                    tuning=int(out.tuning), samples=int(out.samples), frameMs=list(out.frame_ms))
+
+    def setLaunchShape(self, shape: int):
+        self._usable()
+        self._check(getattr(self._L, "jgs2_batch_" + "set_launch_shape")(self._h, int(shape)))
 
     def stream(self) -> int:
         """The batch's cudaStream_t as an integer handle."""
