@@ -1236,15 +1236,13 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
   CUDA_TRY(s, cudaSetDevice(s->device));
   CUDA_TRY(s, cudaMemcpyAsync(s->dParams, s->hParams.data(), sizeof(DevParams) * s->hParams.size(),
                               cudaMemcpyHostToDevice, s->stream));
-  // One frame in the engine's current launch shape: a graph replay (captured
-  // at the first use of the key) or, without graphs, direct launches.
-  auto frame = [&]() -> jgs2_status {
-    if (!s->useGraphs || prof) {
-      s->launches += encodeFrame(s, iterations, schedule, body, contact, prof);
-      return JGS2_OK;
-    }
+  // The graph of a frame in the engine's current launch shape, captured at
+  // the first use of its key.
+  using GraphMap = decltype(s->graphs);
+  GraphMap::iterator it = s->graphs.end();
+  auto graphFor = [&]() -> jgs2_status {
     const auto key = std::make_tuple(iterations, schedule, body, contact, s->b.solveShift);
-    auto it = s->graphs.find(key);
+    it = s->graphs.find(key);
     if (it == s->graphs.end()) {
       cudaGraph_t graph = nullptr;
       CUDA_TRY(s, cudaStreamBeginCapture(s->stream, cudaStreamCaptureModeThreadLocal));
@@ -1257,19 +1255,37 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
       if (e != cudaSuccess) return cudaFail(s, e, "cudaGraphInstantiate");
       it = s->graphs.emplace(key, std::make_pair(exec, n)).first;
     }
+    return JGS2_OK;
+  };
+  const bool graphs = s->useGraphs && !prof;
+  // One frame: a graph replay or, without graphs, direct launches.
+  auto frame = [&]() -> jgs2_status {
+    if (!graphs) {
+      s->launches += encodeFrame(s, iterations, schedule, body, contact, prof);
+      return JGS2_OK;
+    }
     CUDA_TRY(s, cudaGraphLaunch(it->second.first, s->stream));
     s->launches += static_cast<uint64_t>(it->second.second);
     return JGS2_OK;
   };
+  if (graphs) {
+    const jgs2_status st2 = graphFor();
+    if (st2 != JGS2_OK) return st2;
+  }
   for (uint32_t f = 0; f < frames; ++f) {
     if (s->tuneLeft == 0 || prof) {
       const jgs2_status st2 = frame();
       if (st2 != JGS2_OK) return st2;
       continue;
     }
-    // Tuned frame: the shapes take turns; each frame is timed on the stream.
+    // Tuned frame: the shapes take turns; each frame is timed on the stream,
+    // its graph captured before the first event.
     const uint32_t shape = s->tuneNext;
     s->b.solveShift = shape;
+    if (graphs) {
+      const jgs2_status st3 = graphFor();
+      if (st3 != JGS2_OK) return st3;
+    }
     CUDA_TRY(s, cudaEventRecord(s->tuneEvents[0], s->stream));
     const jgs2_status st2 = frame();
     if (st2 != JGS2_OK) return st2;
@@ -1287,6 +1303,10 @@ jgs2_status runFrames(Engine* s, const std::vector<jgs2_settings>& st, uint32_t 
         if (c == 0 || m < bestMs) { best = c; bestMs = m; }
       }
       s->b.solveShift = best;
+      if (graphs) {
+        const jgs2_status st3 = graphFor();
+        if (st3 != JGS2_OK) return st3;
+      }
     }
   }
   CUDA_TRY(s, cudaGetLastError());
