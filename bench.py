@@ -234,6 +234,33 @@ def run_cpu_baseline(inp, args, threads=None):
             "sample": f"1 frame x {iters} iterations of the full {args.cells}^3 cube ({dt:.2f} s)"}, o
 
 
+def fp64_error(inp, args, first_frame):
+    """The cpu_baseline leg's check of the GPU's first frame: the oracle's FP64
+    run of the same method over the same frame (`args.iterations` exact
+    iterations from the initial state), max position error over the bounding
+    box diagonal, and both runs' accepted iterations."""
+    import numpy as np
+
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+
+    sched = 1 if args.schedule != "jacobi" else 0
+    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, schedule=sched)
+    t0 = time.perf_counter()
+    o = O.OracleSolver(inp, s, precision=64)
+    o.step_exact_iterations(args.iterations)
+    dt = time.perf_counter() - t0
+    ref = o.read("positions").reshape(-1, 4)[:, :3].astype(np.float64)
+    gpu = np.asarray(first_frame["positions"], dtype=np.float64).reshape(-1, 4)[:, :3]
+    hist = o.read("history").reshape(64, 32)[:args.iterations]
+    return {"value": float(np.abs(gpu - ref).max() / inp.bbox_diagonal()), "bound": 1e-4,
+            "unit": "max position error / bbox diagonal",
+            "frames": 1, "iterations": args.iterations,
+            "accepted_iterations_gpu": int(first_frame["accepted"]),
+            "accepted_iterations_fp64": int(hist[:, 4].sum()),
+            "oracle": f"FP64 run of the same method on {O.max_threads()} host threads ({dt:.1f} s)"}
+
+
 def dist_env():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -612,6 +639,14 @@ def ours_arm(args):
         s.autotune(args.tune_rounds)
         s.stepFramesExactIterations(3 * args.tune_rounds, iters)
     shape = s.launchShape()
+    first_frame = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        # The first frame from the initial state, kept for the FP64 check.
+        f = solver.JGS2GpuSolver.create(inp, settings, device=device)
+        f.stepExactIterations(iters)
+        first_frame = {"positions": f.readPositions(),
+                       "accepted": float(f.readGlobalizationDiagnostics()["history"][:, 4].sum())}
+        f.destroy()
     for _ in range(args.warmup):
         s.stepExactIterations(iters)
     s.awaitIdle()
@@ -632,6 +667,7 @@ def ours_arm(args):
     ms = start_ev.elapsed_time(end_ev)
     launches = s.kernelLaunchCount() - launches0
     torch.cuda.synchronize(device)
+    accepted_timed = int(s.readGlobalizationDiagnostics()["history"][:, 4].sum())
     ms = max_over_ranks(dist, ms, f"cuda:{device}")
     ms_per_step = ms / args.steps
     value = whole_job_rate(world, active * iters * args.steps, ms / 1e3)
@@ -673,9 +709,12 @@ def ours_arm(args):
     e2e_value = whole_job_rate(world, active * iters * e2e_steps, e2e_total)
 
     cpu = None
+    err64 = None
+    s.destroy()
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         cpu, _o = run_cpu_baseline(inp, args)
-    s.destroy()
+        del _o
+        err64 = fp64_error(inp, args, first_frame)
     if rank == 0:
         line = {
             "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
@@ -685,8 +724,10 @@ def ours_arm(args):
                 "launch_shape": {"autotuned": args.tune_rounds > 0, "shape": shape["shape"],
                                  "solve_vertices_per_block": shape["solveVerticesPerBlock"],
                                  "tuning_frame_ms": [round(m, 3) for m in shape["frameMs"]]},
-                "parallelism": "replicas" if world > 1 else "single GPU"},
+                "parallelism": "replicas" if world > 1 else "single GPU",
+                "accepted_iterations_per_timed_frame": accepted_timed},
             "frames_per_s": world * 1e3 / ms_per_step,
+            "error_vs_fp64": err64,
             "gpu_launches": int(launches),
             "roofline": roofline,
             "cpu_baseline": cpu,

@@ -441,8 +441,9 @@ jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* solver, const float* 
  * predicted positions (4 * V floats each, 16-byte aligned), and writes the
  * 16-float control record (minimum determinants and validity bits, accept /
  * revert flags, energies, sweep aggregates; history slot 0) to the device
- * array control_out.  It reads the solver's static mesh data and changes no
- * solver state.
+ * array control_out.  It reads the solver's mesh data and also its mutable
+ * external-force, quadratic-target and rest-mass arrays, and changes no
+ * solver state.  Solvers with IPC contact candidates get JGS2_UNSUPPORTED.
  *
  * It allocates no device memory: its reduction scratch is a fixed static
  * device array of 262,400 bytes (8192 block partials of 32 bytes after a
@@ -455,7 +456,13 @@ jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* solver, const float* 
  * zeroes it and every launch leaves it zero.  Calls whose launches overlap in
  * time on one device (different streams, threads or solvers) share the
  * scratch and race; order them.  stream is a cudaStream_t, or NULL for the
- * solver's stream; the call is asynchronous on it. */
+ * solver's stream; the call is asynchronous on it.  A non-NULL stream must be
+ * ordered after the solver's stream (for example by an event wait), or the
+ * solver's objectives must not change while the call is in flight: the read
+ * of the force and target arrays is otherwise unordered against a step or an
+ * objective upload on the solver's stream.  The looked-up scratch address is
+ * kept for the life of the process: a device reset (cudaDeviceReset) or an
+ * unload and reload of this library in the same process is not supported. */
 jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* solver, const float* device_source,
                                          const float* device_candidate, const float* device_predicted,
                                          const jgs2_settings* overrides, uint32_t override_mask,

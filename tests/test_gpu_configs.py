@@ -1,0 +1,226 @@
+"""GPU parity on the benchmark configurations, through the C-ABI against the
+CPU oracle (f32 mirror) and with the error stated against the oracle's FP64
+run of the same method.
+
+- config 0 as specified: the 20x4x4-hex cantilever (525 V, 1 920 T, K = 6
+  trained records), 10 exact Jacobi iterations per frame, 300 frames, with
+  the scripted soft target on the free tip over frames 60-180;
+- config 1: the 100^3-hex unit cube (1 030 301 V, 6 000 000 T, K = 6), one
+  frame of 20 exact Jacobi iterations;
+- the 30^3 cube under the graph-coloured schedule;
+- the reference's schedule comparison (tests/e2e/colored-schedule.spec.ts:
+  56-137) on its minimal scene: Jacobi and GGS2 production frames agree;
+- the production finalize (velocity damping, floor tangential damping,
+  horizontal body correction) against the oracle.
+
+Tolerances: positions and velocities within 1e-4 of the bounding-box
+diagonal; accept / revert decisions equal per iteration; residual history
+within 5 % where it is above the f32 noise floor.
+"""
+import numpy as np
+import pytest
+
+from jgs2_b200 import scenes, solver
+from oracle import oracle as O
+
+pytestmark = pytest.mark.gpu
+
+POSITION_TOL = 1e-4  # of the bounding-box diagonal
+RESIDUAL_RTOL = 5e-2
+
+
+def _camel(s):
+    inv = {v: k for k, v in solver.CAMEL.items()}
+    return {inv.get(k, k): (bool(v) if k in ("parity_mode", "horizontal_body_correction") else v)
+            for k, v in s.items()}
+
+
+def _positions(x):
+    return np.asarray(x, dtype=np.float64).reshape(-1, 4)[:, :3]
+
+
+def _error(inp, a, b):
+    return float(np.abs(_positions(a) - _positions(b)).max()) / inp.bbox_diagonal()
+
+
+def _accepted(history, n):
+    return np.asarray(history, dtype=np.float32).reshape(-1, 32)[:n, 4].copy()
+
+
+def _apply_target(inp, frame, gpu, cpu, state):
+    """Scripted cantilever target: upload on keyframe changes only (as the
+    reference's app does), to both the GPU solver and the oracle."""
+    vertex, target, stiffness = scenes.cantilever_target(inp, frame)
+    key = (tuple(target.tolist()), stiffness)
+    if state.get("key") == key:
+        return
+    state["key"] = key
+    if stiffness > 0.0:
+        gpu.setQuadraticTarget(vertex, target, stiffness)
+    else:
+        gpu.releaseQuadraticTarget(vertex)
+    targets = inp.rest_positions.astype(np.float32).reshape(-1).copy()
+    stiff = np.zeros(inp.vertex_count, dtype=np.float32)
+    targets[3 * vertex:3 * vertex + 3] = target
+    stiff[vertex] = stiffness
+    cpu.set_objectives(None, targets, stiff)
+
+
+def test_config0_as_specified():
+    inp = scenes.cantilever()
+    assert (inp.vertex_count, inp.tet_count, inp.cubature_k) == (525, 1920, 6)
+    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=10)
+    gpu = solver.JGS2GpuSolver.create(inp, _camel(s))
+    cpu = O.OracleSolver(inp, s, precision=32)
+    f64 = O.OracleSolver(inp, s, precision=64)
+    gstate, fstate = {}, {}
+    for frame in range(300):
+        _apply_target(inp, frame, gpu, cpu, gstate)
+        vertex, target, stiffness = scenes.cantilever_target(inp, frame)
+        if fstate.get("key") != (tuple(target.tolist()), stiffness):
+            fstate["key"] = (tuple(target.tolist()), stiffness)
+            t = inp.rest_positions.astype(np.float32).reshape(-1).copy()
+            k = np.zeros(inp.vertex_count, dtype=np.float32)
+            t[3 * vertex:3 * vertex + 3] = target
+            k[vertex] = stiffness
+            f64.set_objectives(None, t, k)
+        gpu.stepExactIterations(10)
+        cpu.step_exact_iterations(10)
+        f64.step_exact_iterations(10)
+        # The accept / revert decision of every iteration equals the oracle's.
+        np.testing.assert_array_equal(_accepted(gpu.readGlobalizationDiagnostics()["history"], 10),
+                                      _accepted(cpu.read("history"), 10), err_msg=f"frame {frame}")
+        if frame in (0, 59, 119, 179, 299):
+            assert _error(inp, gpu.readPositions(), cpu.read("positions")) <= POSITION_TOL, frame
+    pe = _error(inp, gpu.readPositions(), cpu.read("positions"))
+    fe = _error(inp, gpu.readPositions(), f64.read("positions"))
+    ve = float(np.abs(_positions(gpu.readVelocities()) - _positions(cpu.read("velocities"))).max()) / 60 / \
+        inp.bbox_diagonal()
+    print(f"config 0, 300 frames: GPU vs f32 oracle {pe:.2e}, vs FP64 oracle {fe:.2e} of the bbox diagonal")
+    assert pe <= POSITION_TOL and ve <= POSITION_TOL
+    assert fe <= POSITION_TOL
+    gpu.destroy()
+
+
+@pytest.fixture(scope="module")
+def cube100():
+    return scenes.unit_cube(cells=100)
+
+
+def test_config1_first_frame(cube100):
+    inp = cube100
+    assert (inp.vertex_count, inp.tet_count, inp.cubature_k) == (1030301, 6000000, 6)
+    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=20)
+    gpu = solver.JGS2GpuSolver.create(inp, _camel(s))
+    gpu.stepExactIterations(20)
+    g_hist = gpu.readGlobalizationDiagnostics()
+    g_pos, g_vel = gpu.readPositions(), gpu.readVelocities()
+    gpu.destroy()
+    cpu = O.OracleSolver(inp, s, precision=32)
+    cpu.step_exact_iterations(20)
+    c_hist = cpu.read("history").reshape(64, 32)
+    assert g_hist["historyCount"] == 20
+    np.testing.assert_array_equal(g_hist["history"][:, 4], c_hist[:20, 4])  # accepted flags
+    np.testing.assert_array_equal(g_hist["history"][:, 5], c_hist[:20, 5])  # reverted flags
+    assert c_hist[:20, 4].sum() > 0
+    big = c_hist[:20, 19] > 1e-2
+    np.testing.assert_allclose(g_hist["history"][big, 19], c_hist[:20][big, 19], rtol=RESIDUAL_RTOL)
+    pe = _error(inp, g_pos, cpu.read("positions"))
+    ve = float(np.abs(_positions(g_vel) - _positions(cpu.read("velocities"))).max()) / 60 / inp.bbox_diagonal()
+    del cpu
+    f64 = O.OracleSolver(inp, s, precision=64)
+    f64.step_exact_iterations(20)
+    fe = _error(inp, g_pos, f64.read("positions"))
+    print(f"config 1, one frame: {int(c_hist[:20, 4].sum())} of 20 iterations accepted; GPU vs f32 oracle "
+          f"{pe:.2e}, vs FP64 oracle {fe:.2e} of the bbox diagonal")
+    assert pe <= POSITION_TOL and ve <= POSITION_TOL
+    assert fe <= POSITION_TOL
+
+
+def test_cube30_graph_colored():
+    inp = scenes.unit_cube(cells=30)
+    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=20,
+             schedule=1)
+    gpu = solver.JGS2GpuSolver.create(inp, _camel(s))
+    cpu = O.OracleSolver(inp, s, precision=32)
+    assert gpu.scheduleColorCount == cpu.color_count
+    for frame in range(2):
+        gpu.stepExactIterations(20)
+        cpu.step_exact_iterations(20)
+        np.testing.assert_array_equal(_accepted(gpu.readGlobalizationDiagnostics()["history"], 20),
+                                      _accepted(cpu.read("history"), 20), err_msg=f"frame {frame}")
+        assert _error(inp, gpu.readPositions(), cpu.read("positions")) <= POSITION_TOL
+    gpu.destroy()
+
+
+def _minimal_scene():
+    """The reference's public minimal cantilever (minimalDefinition,
+    src/scenes/index.ts:330-364): one hex of 2 x 0.8 x 0.8 m at
+    (-1, 1.35, -0.4), its x = min face pinned, soft stable Neo-Hookean rubber
+    (850 kg/m^3, E 35 000, nu 0.35), h = 1/30, six cubature samples."""
+    sc = scenes.Scene()
+    m = sc.add_material(850.0, 35000.0, 0.35)
+    sc.add_cuboid((1, 1, 1), (-1.0, 1.35, -0.4), (2.0, 0.8, 0.8), m, 0, scenes.FACE_X_MIN)
+    sc.precompute(timestep=1 / 30, cubature_k=6)
+    return sc.pack()
+
+
+# The app's production settings for the minimal scene (src/App.tsx:520-575).
+MINIMAL_SETTINGS = dict(timestep=1 / 30, gravity=(0.0, -9.81, 0.0), iterations=7, floor_height=0.0,
+                        floor_stiffness=250000.0, velocity_damping=0.997, contact_tangential_damping=12.0,
+                        contact_margin=0.01, horizontal_body_correction=1, parity_mode=0, regularization=1e-6,
+                        rotation_epsilon=1e-7, max_step=0.075)
+
+
+def test_minimal_scene_schedules_agree():
+    # Restates the reference's Jacobi-vs-GGS2 comparison: 12 production
+    # frames of each schedule from the same start settle to comparable poses.
+    inp = _minimal_scene()
+    runs = {}
+    for schedule in (0, 1):
+        gpu = solver.JGS2GpuSolver.create(inp, _camel(dict(MINIMAL_SETTINGS, schedule=schedule)))
+        if schedule == 1:
+            assert gpu.scheduleColorCount > 1
+        start = gpu.readPositions()
+        gpu.stepFrames(12)
+        end = gpu.readPositions()
+        assert float(np.abs(_positions(end) - _positions(start)).max()) > 1e-4  # the state advanced
+        runs[schedule] = end
+        gpu.destroy()
+    scale = inp.bbox_diagonal()
+    diff = _positions(runs[0]) - _positions(runs[1])
+    rms = float(np.sqrt((diff ** 2).sum(axis=1).mean()))
+    assert rms / scale < 5e-4
+    assert float(np.linalg.norm(diff, axis=1).max()) / scale < 1e-3
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_production_finalize_matches_oracle(schedule):
+    # Production frames (odd iteration count, stop latch, velocity damping
+    # 0.997, horizontal body correction) of the minimal scene and of a box
+    # dropped onto the penalty floor (floor tangential damping), GPU vs oracle.
+    inp = _minimal_scene()
+    s = dict(MINIMAL_SETTINGS, schedule=schedule)
+    gpu = solver.JGS2GpuSolver.create(inp, _camel(s))
+    cpu = O.OracleSolver(inp, s, precision=32)
+    for _ in range(12):
+        gpu.step()
+        cpu.step()
+    assert _error(inp, gpu.readPositions(), cpu.read("positions")) <= POSITION_TOL
+    gpu.destroy()
+
+    sc = scenes.Scene()
+    m = sc.add_material(850.0, 35000.0, 0.35)
+    sc.add_cuboid((2, 2, 2), (-0.3, 0.05, -0.3), (0.6, 0.6, 0.6), m, 0, 0)
+    sc.precompute(timestep=1 / 30, cubature_k=48, exact_complement=1)
+    drop = sc.pack()
+    gpu = solver.JGS2GpuSolver.create(drop, _camel(s))
+    cpu = O.OracleSolver(drop, s, precision=32)
+    for frame in range(40):
+        gpu.step()
+        cpu.step()
+    err = _error(drop, gpu.readPositions(), cpu.read("positions"))
+    assert err <= POSITION_TOL, err
+    low = _positions(cpu.read("positions"))[:, 1].min()
+    assert low < 0.02  # the box reached the floor, so the floor terms acted
+    gpu.destroy()

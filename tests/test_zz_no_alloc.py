@@ -56,14 +56,36 @@ def _poses(inp):
     return src.reshape(-1), [("accepted", accepted.reshape(-1)), ("rejected", rejected.reshape(-1))]
 
 
+def _cloth_poses(inp):
+    """An accepted small perturbation of the sheet and a rejected one that
+    mirrors a free cloth vertex through the opposite edge of its triangle
+    (the triangle's signed area stretch turns negative)."""
+    rng = np.random.default_rng(20240612)
+    info = inp.vertex_info.reshape(-1, 4)
+    src = inp.positions.astype(np.float32).reshape(-1, 4).copy()
+    free = info[:, 2] == 0
+    accepted = src.copy()
+    accepted[free, :3] += rng.normal(0.0, 1e-4, size=(int(free.sum()), 3)).astype(np.float32)
+    tris = inp.cloth_triangles.reshape(-1, 3).astype(np.int64)
+    rejected = src.copy()
+    for t in tris[::-1]:
+        if all(info[int(q), 2] == 0 for q in t):
+            v, a, c = (int(q) for q in t)
+            mid = 0.5 * (src[a, :3] + src[c, :3])
+            rejected[v, :3] = mid + (mid - src[v, :3])
+            break
+    else:
+        raise AssertionError("no free cloth triangle")
+    return src.reshape(-1), [("accepted", accepted.reshape(-1)), ("rejected", rejected.reshape(-1))]
+
+
 def _to_device(a):
     return torch.from_numpy(np.ascontiguousarray(a, dtype=np.float32)).to("cuda")
 
 
-def test_no_alloc_gate_matches_assembled_candidate(bar):
+def _check_against_existing_entry(inp, settings, src, cases):
     gate = _entry()
-    gpu = solver.JGS2GpuSolver.create(bar, SETTINGS)
-    src, cases = _poses(bar)
+    gpu = solver.JGS2GpuSolver.create(inp, settings)
     # The existing entry point, once per candidate.
     refs = [gpu.evaluateAssembledCandidateForTest(src, cand) for _name, cand in cases]
     assert refs[0]["history"][4] == 1.0 and refs[1]["history"][5] == 1.0  # one accepted, one reverted
@@ -92,6 +114,34 @@ def test_no_alloc_gate_matches_assembled_candidate(bar):
     # The gate changed no solver state: the canonical pose is still the one
     # the last existing-entry call left.
     np.testing.assert_array_equal(gpu.readPositions(), refs[1]["positions"])
+    gpu.destroy()
+
+
+def test_no_alloc_gate_matches_assembled_candidate(bar):
+    src, cases = _poses(bar)
+    _check_against_existing_entry(bar, SETTINGS, src, cases)
+
+
+def test_no_alloc_gate_matches_on_cloth():
+    # A tet collider and a 6x6-cell StVK sheet: the membrane and hinge terms
+    # of the allocation-free kernel against the existing entry point.
+    inp = scenes.cloth_drape(cells=6, prefold=False, pinned_columns=(0, 6))
+    assert inp.cloth_triangle_count > 0 and inp.hinge_count > 0
+    src, cases = _cloth_poses(inp)
+    _check_against_existing_entry(inp, dict(SETTINGS, timestep=1 / 120), src, cases)
+
+
+def test_no_alloc_gate_refuses_contact_solvers():
+    inp = scenes.trough(boxes=2)
+    assert inp.contact_candidate_count > 0
+    gate = _entry()
+    gpu = solver.JGS2GpuSolver.create(inp, scenes.TROUGH_SETTINGS)
+    d = torch.zeros(4 * inp.vertex_count, dtype=torch.float32, device="cuda")
+    ctl = torch.zeros(16, dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    status = gate(gpu._h, d.data_ptr(), d.data_ptr(), d.data_ptr(), None, 0, ctl.data_ptr(), None)
+    assert status == 7  # JGS2_UNSUPPORTED
+    assert b"contact" in _ffi.step_lib().jgs2_last_error(gpu._h)
     gpu.destroy()
 
 

@@ -207,17 +207,17 @@ __device__ __forceinline__ uint4 hingeIndices(const float4* __restrict__ hinges,
 // k L0 (dtheta/dx)(dtheta/dx)^T: the cloth loops of jgs2Solve
 // (jgs2-shader.ts:3113-3186).  Entries [first, first + count) step `stride`
 // of the vertex's incidence range (lane-split gathers pass their lane).
-template <bool kHessian>
+template <bool kHessian, class G>
 __device__ __forceinline__ void clothLocalSystem(const float4* __restrict__ tris, const float4* __restrict__ hinges,
                                                  const uint32_t* __restrict__ incidence, const uint4& range,
                                                  const float4* __restrict__ x, const ClothMaterial& m,
-                                                 uint32_t first, uint32_t stride, float3& grad, S3& hess) {
+                                                 uint32_t first, uint32_t stride, G& grad, S3& hess) {
   for (uint32_t a = first; a < range.y; a += stride) {
     const uint32_t entry = __ldg(&incidence[range.x + a]);
     const uint32_t slot = entry & 3u;
     const ClothTri t = loadClothTri(tris, entry >> 2);
     const Membrane e = clothMembrane(t, xyz(x[t.i0]), xyz(x[t.i1]), xyz(x[t.i2]), m);
-    grad = grad + clothMembraneGradient(t, e, slot, m);
+    gadd(grad, clothMembraneGradient(t, e, slot, m));
     if (kHessian) clothMembraneHessian(hess, t, e, slot, m);
   }
   for (uint32_t a = first; a < range.w; a += stride) {
@@ -229,12 +229,12 @@ __device__ __forceinline__ void clothLocalSystem(const float4* __restrict__ tris
     const float angle = f.valid ? atan2f(f.sine, f.cosine) : 0.0f;
     const float3 ag = f.valid ? clothDihedralGradient(f, slot) : f3(0, 0, 0);
     if (!f.valid || !finiteS(angle) || !finiteV(ag)) {
-      grad = grad + f3(kF32Max, kF32Max, kF32Max);
+      gadd(grad, f3(kF32Max, kF32Max, kF32Max));
       continue;
     }
     const float4 rest = __ldg(&hinges[2ull * h + 1]);
     const float ws = m.bending * rest.y;
-    grad = grad + (ws * clothWrappedAngle(angle, rest.x)) * ag;
+    gadd(grad, (ws * clothWrappedAngle(angle, rest.x)) * ag);
     if (kHessian) saddOuter(hess, ws, ag);
   }
 }

@@ -126,6 +126,52 @@ __device__ __forceinline__ S3 gramColumns(const M3& b) {
   return {dot3(b.c0, b.c0), dot3(b.c1, b.c1), dot3(b.c2, b.c2), dot3(b.c0, b.c1), dot3(b.c0, b.c2), dot3(b.c1, b.c2)};
 }
 
+// ---- compensated summation of the per-vertex gradient gathers --------------
+// Knuth's TwoSum: t = fl(a + b) and the exact rounding error e with
+// a + b = t + e, from six round-to-nearest operations.  The intrinsics keep
+// the compiler from contracting or reassociating them.  The error is unique,
+// so TwoSum(a, b) and TwoSum(b, a) give the same pair.
+__device__ __forceinline__ float twoSum(float a, float b, float* e) {
+  const float t = __fadd_rn(a, b);
+  const float bp = __fsub_rn(t, a);
+  *e = __fadd_rn(__fsub_rn(a, __fsub_rn(t, bp)), __fsub_rn(b, bp));
+  return t;
+}
+// A float3 sum carried as value + compensation (Kahan-Babuska summation in
+// Neumaier's form): each addend's rounding error is kept in `c`, and the
+// result is rounded once at the end.  The error of a gather of n terms is
+// then about one rounding of the result plus n u^2 of the terms, instead of
+// n u of the terms for a plain f32 sum.
+struct Comp3 {
+  float3 s, c;
+};
+__device__ __forceinline__ Comp3 czero() { return {f3(0, 0, 0), f3(0, 0, 0)}; }
+__device__ __forceinline__ void cadd(Comp3& a, float3 x) {
+  float ex, ey, ez;
+  a.s.x = twoSum(a.s.x, x.x, &ex);
+  a.s.y = twoSum(a.s.y, x.y, &ey);
+  a.s.z = twoSum(a.s.z, x.z, &ez);
+  a.c.x = __fadd_rn(a.c.x, ex);
+  a.c.y = __fadd_rn(a.c.y, ey);
+  a.c.z = __fadd_rn(a.c.z, ez);
+}
+// Merge two compensated sums (symmetric in its arguments).
+__device__ __forceinline__ void cmerge(Comp3& a, const Comp3& b) {
+  float ex, ey, ez;
+  a.s.x = twoSum(a.s.x, b.s.x, &ex);
+  a.s.y = twoSum(a.s.y, b.s.y, &ey);
+  a.s.z = twoSum(a.s.z, b.s.z, &ez);
+  a.c.x = __fadd_rn(__fadd_rn(a.c.x, b.c.x), ex);
+  a.c.y = __fadd_rn(__fadd_rn(a.c.y, b.c.y), ey);
+  a.c.z = __fadd_rn(__fadd_rn(a.c.z, b.c.z), ez);
+}
+__device__ __forceinline__ float3 cvalue(const Comp3& a) {
+  return f3(__fadd_rn(a.s.x, a.c.x), __fadd_rn(a.s.y, a.c.y), __fadd_rn(a.s.z, a.c.z));
+}
+// Gradient accumulation into a plain or a compensated sum.
+__device__ __forceinline__ void gadd(float3& g, float3 x) { g = g + x; }
+__device__ __forceinline__ void gadd(Comp3& g, float3 x) { cadd(g, x); }
+
 // ---- stable Neo-Hookean (stable-neo-hookean-wgsl.ts:44-94) -------------------
 __device__ __forceinline__ float snhEnergy(const M3& f, float lambda, float mu) {
   const float I1 = frob(f, f);

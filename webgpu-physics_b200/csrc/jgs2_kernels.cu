@@ -190,6 +190,22 @@ __device__ __forceinline__ float groupSum(float v, unsigned mask) {
   for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, W);
   return v;
 }
+// Merge of the lanes' compensated sums over a lane group (xor butterfly;
+// every lane ends with the same pair because the merge is symmetric).
+template <int W>
+__device__ __forceinline__ void groupMerge(Comp3& a, unsigned mask) {
+#pragma unroll
+  for (int o = W / 2; o > 0; o >>= 1) {
+    Comp3 t;
+    t.s.x = __shfl_xor_sync(mask, a.s.x, o, W);
+    t.s.y = __shfl_xor_sync(mask, a.s.y, o, W);
+    t.s.z = __shfl_xor_sync(mask, a.s.z, o, W);
+    t.c.x = __shfl_xor_sync(mask, a.c.x, o, W);
+    t.c.y = __shfl_xor_sync(mask, a.c.y, o, W);
+    t.c.z = __shfl_xor_sync(mask, a.c.z, o, W);
+    cmerge(a, t);
+  }
+}
 template <int W>
 __device__ __forceinline__ float groupMin(float v, unsigned mask) {
 #pragma unroll
@@ -244,7 +260,7 @@ __device__ __forceinline__ void frameAndIncident(const Buffers& b, const DevPara
                                                  uint32_t v, const uint4& info, float eps) {
   M3 avg = mzero();
   float total = 0.0f;
-  float3 grad = f3(0, 0, 0);
+  Comp3 grad = czero();  // compensated gradient gather
   S3 hess = szero();
   for (uint32_t a = 0; a < info.y; ++a) {
     const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
@@ -252,7 +268,7 @@ __device__ __forceinline__ void frameAndIncident(const Buffers& b, const DevPara
     const M3 F = deformationAt(r, x);
     const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
     const float3 g = shapeGradient(r, entry & 3u);
-    grad = grad + r.vol * mv(piola(F, pt), g);
+    cadd(grad, r.vol * mv(piola(F, pt), g));
     addIncidentBlock(hess, r, F, pt, g);
     avg = avg + r.vol * F;
     total += r.vol;
@@ -262,7 +278,7 @@ __device__ __forceinline__ void frameAndIncident(const Buffers& b, const DevPara
                            grad, hess);
   const M3 favg = total > 0.0f ? (1.0f / total) * avg : midentity();
   storeRot(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, eps));
-  storeIncident(b.incident, v, grad, hess);
+  storeIncident(b.incident, v, cvalue(grad), hess);
 }
 
 // Vertex frame: polar of the volume-weighted average F over incident tets
@@ -405,9 +421,10 @@ __global__ void __launch_bounds__(kBlock) corotatedSolveKernel(Buffers b, const 
   const float4 pv = b.predicted[v];
   const float inertia = rm.w * p.invDt2;
   const bool objActive = p.objectiveFlags != 0u;
-  float3 grad = inertia * (position - xyz(pv));
+  Comp3 gsum = czero();  // compensated gradient gather
+  cadd(gsum, inertia * (position - xyz(pv)));
   M3 hess = inertia * midentity();
-  if (objActive) grad = grad + objectiveGradient(p, b, v, position);
+  if (objActive) cadd(gsum, objectiveGradient(p, b, v, position));
   if (p.objectiveFlags & 2u) hess = hess + targetStiffness(p, b, v) * midentity();
   for (uint32_t a = 0; a < info.y; ++a) {
     const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
@@ -416,11 +433,11 @@ __global__ void __launch_bounds__(kBlock) corotatedSolveKernel(Buffers b, const 
     const M3 R = loadRot(b.tetRot, t);
     float3 tg[4];
     corotatedGradient(b, src, t, r.idx, R, tg);
-    grad = grad + tg[slot];
+    cadd(gsum, tg[slot]);
     hess = hess + mm(mm(R, stiffnessBlock(b.stiffness + 144ull * t, slot, slot)), mtrans(R));
   }
   if (p.floorStiffness > 0.0f && position.y < p.floorHeight) {
-    grad.y += p.floorStiffness * (position.y - p.floorHeight);
+    cadd(gsum, f3(0.0f, p.floorStiffness * (position.y - p.floorHeight), 0.0f));
     hess.c1.y += p.floorStiffness;
   }
   const M3 RsT = mtrans(loadRot(b.vertexRot, v));
@@ -477,7 +494,7 @@ __global__ void __launch_bounds__(kBlock) corotatedSolveKernel(Buffers b, const 
       if (p.objectiveFlags & 2u)
         ph = ph - (targetStiffness(p, b, v) / float(info.y > 1u ? info.y : 1u)) * midentity();
     }
-    grad = grad + w * pg;
+    cadd(gsum, w * pg);
     hess = hess + w * ph;
   }
   // Regularised Cholesky solve with the shift max(regularization * scale, 1e-9).
@@ -487,7 +504,7 @@ __global__ void __launch_bounds__(kBlock) corotatedSolveKernel(Buffers b, const 
   const float a01 = 0.5f * (hess.c0.y + hess.c1.x);
   const float a02 = 0.5f * (hess.c0.z + hess.c2.x);
   const float a12 = 0.5f * (hess.c1.z + hess.c2.y);
-  const float3 rhs = -grad;
+  const float3 rhs = -cvalue(gsum);
   const float l00 = sqrtf(fmaxf(a00, shift));
   const float l10 = a01 / l00, l20 = a02 / l00;
   const float l11 = sqrtf(fmaxf(a11 - l10 * l10, shift));
@@ -614,10 +631,10 @@ __device__ __forceinline__ float contactEnergy(const Buffers& b, const DevParams
 // [first, count) step `stride`: barrier gradient and PSD normal block, lagged
 // friction gradient and tangential block.  `fresh` evaluates the contact at x
 // (the coloured schedule), otherwise the cache at `slot` is used.
-template <bool kHessian>
+template <bool kHessian, class G>
 __device__ __forceinline__ void contactLocal(const Buffers& b, const DevParams& p, uint32_t v,
                                              const float4* __restrict__ x, bool fresh, int slot, uint32_t first,
-                                             uint32_t stride, float3& grad, S3& hess) {
+                                             uint32_t stride, G& grad, S3& hess) {
   const uint2 range = b.contactRange[v];
   const uint32_t n = b.activeCount[v];
   for (uint32_t a = first; a < n; a += stride) {
@@ -634,7 +651,7 @@ __device__ __forceinline__ void contactLocal(const Buffers& b, const DevParams& 
     if (ipcWeightFor(q, make_float4(1.f, 1.f, 1.f, 1.f), v) == 0.0f) continue;
     const float w = ipcWeightFor(q, k.weights, v);
     if (w != 0.0f && barrier) {
-      grad = grad + ipcNormalGradientScalar(w, p.ipcStiffness, ipcBarrier1(k.distance, p.ipcActivation)) * k.normal;
+      gadd(grad, ipcNormalGradientScalar(w, p.ipcStiffness, ipcBarrier1(k.distance, p.ipcActivation)) * k.normal);
       if (kHessian) {
         const float s = ipcPsdScalar(w, p.ipcStiffness, ipcBarrier2(k.distance, p.ipcActivation));
         saddOuter(hess, fmaxf(s, 0.0f), ipcSafeUnit(k.normal, f3(1, 0, 0)));
@@ -650,7 +667,7 @@ __device__ __forceinline__ void contactLocal(const Buffers& b, const DevParams& 
       const float scale = p.ipcFriction * lag.w;
       const float3 dir = slip > 1.0e-12f ? tang * (1.0f / slip) : f3(0, 0, 0);
       const float f1 = ipcFrictionF1(slip * p.invDt, p.ipcEpsilon);
-      grad = grad + (lw * scale * f1) * dir;
+      gadd(grad, (lw * scale * f1) * dir);
       if (kHessian) {
         float curvature = 2.0f * scale / fmaxf(p.ipcEpsilon * p.dt, 1.0e-12f);
         if (slip > 1.0e-12f) curvature = scale * f1 / slip;
@@ -1564,7 +1581,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
         const bool objActive = p.objectiveFlags != 0u;
         const float3 objS = objActive ? objectiveGradient(p, b, v, position) : f3(0, 0, 0);
         const float ktS = targetStiffness(p, b, v);
-        float3 grad = f3(0, 0, 0);
+        Comp3 gsum = czero();  // compensated gradient gather
         S3 hess = szero();
         // Record terms are formed in the source vertex's frame: with
         // B_l = R_l Ubar_l R_s^T = B'_l R_s^T, a record's projected gradient
@@ -1653,7 +1670,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
               ph.yz += pt.a * frob(dF1, dF2) + pt.c1 * p1 * p2 + r.lambda * q1 * q2;
               ph.xx *= r.vol; ph.yy *= r.vol; ph.zz *= r.vol; ph.xy *= r.vol; ph.xz *= r.vol; ph.yz *= r.vol;
               sadd(ph, HQ);
-              grad = grad + w * mv(Rs, pg);
+              cadd(gsum, w * mv(Rs, pg));
               saddScaled(hess, w, srotate(Rs, ph));
               float3 gs = f3(0, 0, 0);
               if (slot < 4) {
@@ -1666,7 +1683,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                 saddDiag(blk, pt.a * dot3(gs, gs));
                 saddOuter(blk, pt.c1, u1);
                 saddOuter(blk, r.lambda, w1);
-                grad = grad - w * ps;
+                cadd(gsum, (-w) * ps);
                 saddScaled(hess, -w * r.vol, blk);
                 saddDiag(hess, -w * (dWs + ktS / nS));
               }
@@ -1692,22 +1709,20 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             const M3 F = deformationAt(r, src);
             const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
             const float3 g = shapeGradient(r, entry & 3u);
-            grad = grad + r.vol * mv(piola(F, pt), g);
+            cadd(gsum, r.vol * mv(piola(F, pt), g));
             addIncidentBlock(hess, r, F, pt, g);
           }
           // ---- cloth membrane and bending (jgs2-shader.ts:3113-3186) ----
           if (kExt && p.cloth)
             clothLocalSystem<true>(b.clothTris, b.clothHinges, b.clothIncidence, b.clothRange[v], src,
-                                   clothMaterial(p), lane, W, grad, hess);
+                                   clothMaterial(p), lane, W, gsum, hess);
         }
         // ---- IPC contact (jgs2-shader.ts:3193-3195): the cached source
         // contacts, or fresh ones under the coloured schedule ----
         if (kExt && p.ipc)
-          contactLocal<true>(b, p, v, src, !cachedIncident, kContactSource, lane, W, grad, hess);
+          contactLocal<true>(b, p, v, src, !cachedIncident, kContactSource, lane, W, gsum, hess);
         // Group reduction of the gather.
-        grad.x = groupSum<W>(grad.x, mask);
-        grad.y = groupSum<W>(grad.y, mask);
-        grad.z = groupSum<W>(grad.z, mask);
+        groupMerge<W>(gsum, mask);
         hess.xx = groupSum<W>(hess.xx, mask);
         hess.yy = groupSum<W>(hess.yy, mask);
         hess.zz = groupSum<W>(hess.zz, mask);
@@ -1716,7 +1731,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
         hess.yz = groupSum<W>(hess.yz, mask);
         if (cachedIncident) {
           const float4 i0 = b.incident[3ull * v], i1 = b.incident[3ull * v + 1], i2 = b.incident[3ull * v + 2];
-          grad = grad + f3(i0.x, i0.y, i0.z);
+          cadd(gsum, f3(i0.x, i0.y, i0.z));
           hess.xx += i0.w;
           hess.yy += i1.x;
           hess.zz += i1.y;
@@ -1725,14 +1740,15 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
           hess.yz += i2.x;
         }
         // Own terms: inertia, objectives, floor (jgs2-shader.ts:3083-3092, 3188-3191).
-        grad = grad + inertia * (position - predV);
+        cadd(gsum, inertia * (position - predV));
         saddDiag(hess, inertia);
-        if (objActive) grad = grad + objS;
+        if (objActive) cadd(gsum, objS);
         if (p.objectiveFlags & 2u) saddDiag(hess, ktS);
         if (p.floorStiffness > 0.0f && position.y < p.floorHeight) {
-          grad.y += p.floorStiffness * (position.y - p.floorHeight);
+          cadd(gsum, f3(0.0f, p.floorStiffness * (position.y - p.floorHeight), 0.0f));
           hess.yy += p.floorStiffness;
         }
+        const float3 grad = cvalue(gsum);
         // ---- globalization and line search (jgs2-shader.ts:3265-3473) ----
         const SolveResult dr = globalizationSolve(hess, grad, inertia);
         status = kNonfinite;
@@ -2329,7 +2345,7 @@ __global__ void JGS2_CONV_BOUNDS convergenceKernel(Buffers b, const DevParams* _
       const float3 x = xyz(acc[v]);
       float3 comps[5];
       comps[0] = (b.restMass[v].w * p.invDt2) * (x - xyz(b.predicted[v]));
-      float3 material = f3(0, 0, 0);
+      Comp3 material = czero();  // compensated gradient gather
       M3 avg = mzero();
       float total = 0.0f;
       S3 hess = szero();
@@ -2339,7 +2355,7 @@ __global__ void JGS2_CONV_BOUNDS convergenceKernel(Buffers b, const DevParams* _
         const M3 F = deformationAt(r, acc);
         const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
         const float3 g = shapeGradient(r, entry & 3u);
-        material = material + r.vol * mv(piola(F, pt), g);
+        cadd(material, r.vol * mv(piola(F, pt), g));
         if (nextRotations) addIncidentBlock(hess, r, F, pt, g);
         avg = avg + r.vol * F;
         total += r.vol;
@@ -2353,7 +2369,7 @@ __global__ void JGS2_CONV_BOUNDS convergenceKernel(Buffers b, const DevParams* _
           clothLocalSystem<false>(b.clothTris, b.clothHinges, b.clothIncidence, cr, acc, clothMaterial(p), 0u, 1u,
                                   material, hess);
       }
-      comps[1] = material;
+      comps[1] = cvalue(material);
       comps[2] = f3(0, 0, 0);
       comps[3] = f3(0, 0, 0);
       if (p.objectiveFlags != 0u) {
@@ -2389,7 +2405,7 @@ __global__ void JGS2_CONV_BOUNDS convergenceKernel(Buffers b, const DevParams* _
       if (nextRotations) {
         const M3 favg = total > 0.0f ? (1.0f / total) * avg : midentity();
         storeRot(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, p.rotationEpsilon));
-        storeIncident(b.incident, v, material, hess);
+        storeIncident(b.incident, v, comps[1], hess);
       }
     } else if (nextRotations) {
       storeRot(b.vertexRot, v, vertexFrame(b, acc, v, p.rotationEpsilon));

@@ -2795,7 +2795,10 @@ jgs2_status jgs2_evaluate_assembled_candidate(jgs2_solver* s, const float* sourc
 // give the library a fixed device-memory budget up front, and per-frame loops
 // where a device allocation would synchronise the device and stall the frame.
 // The gate's scratch is a static device array whose address is looked up once
-// per device; nothing here calls cudaMalloc or cudaFree.
+// per device; nothing here calls cudaMalloc or cudaFree.  The address cache
+// below lives for the whole process and is keyed by device ordinal only: a
+// device reset or a reload of this library in the same process would leave it
+// stale, so neither is supported (the header says so).
 jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* s, const float* source, const float* candidate,
                                          const float* predicted, const jgs2_settings* o, uint32_t mask,
                                          float* control, void* stream) {

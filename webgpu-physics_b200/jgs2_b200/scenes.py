@@ -721,21 +721,47 @@ def batched_scenes(count=256, **kwargs) -> list:
     return batched_bodies(count=count, **kwargs).split_bodies()
 
 
-def cantilever_target(inp: SceneInput, frame: int, lift=0.15, stiffness=1000.0):
-    """Soft target on the free-end (x = max) vertices for frames 60-180: the
-    rest position raised by `lift` along a smoothstep over frames 60-120, held
-    until 180, released afterwards.  Returns (positions 3V, stiffnesses V)."""
+# The cantilever's scripted soft target, restating the reference's public
+# demo target (minimalScriptedTargetAtFrame, src/scenes/index.ts:252-328) on
+# the frame window of the 300-frame cantilever workload: one free-tip vertex
+# (the x = max, y = min, z = min corner, as vertex 1 is on the reference's
+# one-cell beam), stiffness 30 000, a smoothstep pull on keyframes every 3
+# frames from frame 60 to frame 120, held until frame 180 and then released
+# (stiffness 0).  The pull offset is the reference's (0.45, 0.65, 0.25) m on
+# its 2 m beam, scaled by the bar's length.
+CANTILEVER_TARGET_PULL_START = 60
+CANTILEVER_TARGET_PULL_END = 120
+CANTILEVER_TARGET_RELEASE = 180
+CANTILEVER_TARGET_KEYFRAME_INTERVAL = 3
+CANTILEVER_TARGET_STIFFNESS = 30000.0
+CANTILEVER_TARGET_OFFSET = (0.45, 0.65, 0.25)  # per 2 m of beam
+
+
+def cantilever_tip_vertex(inp: SceneInput) -> int:
+    """The free tip the scripted target pulls: the x = max, y = min, z = min
+    corner of the bar."""
     rest = inp.rest_positions
-    xmax = rest[:, 0].max()
-    tip = np.isclose(rest[:, 0], xmax)
-    targets = rest.astype(np.float32).copy()
-    stiff = np.zeros(inp.vertex_count, dtype=np.float32)
-    if 60 <= frame < 180:
-        u = min(1.0, (frame - 60) / 60.0)
-        progress = u * u * (3 - 2 * u)
-        targets[tip, 1] += np.float32(lift * progress)
-        stiff[tip] = stiffness
-    return targets.reshape(-1), stiff
+    key = np.lexsort((rest[:, 2], rest[:, 1], -rest[:, 0]))
+    return int(key[0])
+
+
+def cantilever_target(inp: SceneInput, frame: int):
+    """Scripted target of `frame`: (vertex, target position (3,), stiffness).
+    Stiffness is 0 before the pull starts and after the release."""
+    if frame < 0:
+        raise ValueError("cantilever target frame must be nonnegative")
+    vertex = cantilever_tip_vertex(inp)
+    rest = inp.rest_positions[vertex].astype(np.float64)
+    length = float(np.ptp(inp.rest_positions[:, 0]))
+    start, end = CANTILEVER_TARGET_PULL_START, CANTILEVER_TARGET_PULL_END
+    step = CANTILEVER_TARGET_KEYFRAME_INTERVAL
+    pull = min(frame, end)
+    key = min(end, start + ((pull - start) // step) * step) if frame >= start else start
+    u = (key - start) / (end - start)
+    progress = u * u * (3 - 2 * u)
+    target = rest + np.array(CANTILEVER_TARGET_OFFSET) * (length / 2.0) * progress
+    active = start <= frame < CANTILEVER_TARGET_RELEASE
+    return vertex, target.astype(np.float32), (CANTILEVER_TARGET_STIFFNESS if active else 0.0)
 
 
 def unit_cube(cells=100, young=1e6, poisson=0.45, density=1000.0, timestep=1 / 60,
