@@ -263,6 +263,21 @@ jgs2_status jgs2_validate_input(const jgs2_input* input);
  * of a contact run: feed it the positions read back after each frame. */
 jgs2_status jgs2_minimum_contact_distance(const jgs2_input* input, double cutoff, double* distance);
 
+/* The device closest-feature routine of the IPC passes on caller pairs
+ * (a diagnostic): the GPU counterpart of evaluateIpcVertexTriangleDistance
+ * and evaluateIpcEdgeEdgeDistance (src/simulation/cpu/ipc-contact.ts:194,
+ * 277), i.e. jgs2_ipc_point_triangle_contact / jgs2_ipc_edge_edge_contact
+ * (src/simulation/gpu/ipc-contact-wgsl.ts:151, 228) as every contact pass of
+ * this library evaluates them: f32, with near-degenerate pairs (sliver
+ * triangles, near-parallel edges, near-touching features) recomputed in FP64
+ * and rounded once.  points: 12 floats per pair (type 0: point, triangle;
+ * type 1: edge a, edge b); types: 0 or 1 per pair; out: 9 floats per pair
+ * (distance, normal xyz, weights xyzw with sum w_i x_i = a - b, valid);
+ * fp64_used (may be NULL): 1 where the FP64 run was taken.  Host arrays; the
+ * call allocates and frees its own device buffers on `device`. */
+jgs2_status jgs2_evaluate_contact_features(const float* points, const uint32_t* types, uint32_t count,
+                                           float* out, uint32_t* fp64_used, int device);
+
 /* Candidates of the static superset of input->contact_surface (what
  * buildStaticIpcContactCandidates would list), counted without listing. */
 jgs2_status jgs2_contact_superset_size(const jgs2_input* input, uint64_t* count);

@@ -2595,6 +2595,20 @@ int jgs2_oracle_ipc_contact(uint32_t type, const double* x, double* out) {
   return 0;
 }
 
+// The same contact features in the f32 mirror (inputs rounded to float,
+// computed in float): the plain-f32 error against the FP64 run.
+int jgs2_oracle_ipc_contact_f32(uint32_t type, const double* x, double* out) {
+  V3<float> p[4];
+  for (int l = 0; l < 4; ++l)
+    p[l] = v3(static_cast<float>(x[3 * l]), static_cast<float>(x[3 * l + 1]), static_cast<float>(x[3 * l + 2]));
+  const Contact<float> k = type == 0 ? ipcPointTriangle(p[0], p[1], p[2], p[3]) : ipcEdgeEdge(p[0], p[1], p[2], p[3]);
+  out[0] = k.distance;
+  out[1] = k.normal.x; out[2] = k.normal.y; out[3] = k.normal.z;
+  out[4] = k.weights.x; out[5] = k.weights.y; out[6] = k.weights.z; out[7] = k.weights.w;
+  out[8] = k.valid ? 1.0 : 0.0;
+  return 0;
+}
+
 // Minimum exact contact distance over the candidates at the current pose.
 double jgs2_oracle_min_contact_distance(void* handle) {
   Handle* h = static_cast<Handle*>(handle);

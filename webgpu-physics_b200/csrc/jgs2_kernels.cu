@@ -869,6 +869,29 @@ __global__ void __launch_bounds__(kBlock) contactValidateKernel(Buffers b, const
   }
 }
 
+// Closest features of caller-given pairs (a diagnostic, not part of the
+// step): the device routine every contact pass uses, f32 with the FP64 run
+// for near-degenerate pairs; 9 floats per pair out (distance, normal,
+// weights, valid) and whether the FP64 run was taken.
+__global__ void __launch_bounds__(kBlock) contactFeatureKernel(const float* __restrict__ points,
+                                                               const uint32_t* __restrict__ types, uint32_t n,
+                                                               float* __restrict__ out, uint32_t* __restrict__ wide) {
+  const uint32_t i = blockIdx.x * kBlock + threadIdx.x;
+  if (i >= n) return;
+  const float* x = points + 12ull * i;
+  const float3 p0 = f3(x[0], x[1], x[2]), p1 = f3(x[3], x[4], x[5]);
+  const float3 p2 = f3(x[6], x[7], x[8]), p3 = f3(x[9], x[10], x[11]);
+  bool w = false;
+  const ContactData k = types[i] == kIpcVertexTriangle ? ipcPointTriangle(p0, p1, p2, p3, &w)
+                                                       : ipcEdgeEdge(p0, p1, p2, p3, &w);
+  float* o = out + 9ull * i;
+  o[0] = k.distance;
+  o[1] = k.normal.x; o[2] = k.normal.y; o[3] = k.normal.z;
+  o[4] = k.weights.x; o[5] = k.weights.y; o[6] = k.weights.z; o[7] = k.weights.w;
+  o[8] = k.valid ? 1.0f : 0.0f;
+  wide[i] = w ? 1u : 0u;
+}
+
 // promoteAcceptedContactCache (:2694-2710).
 __global__ void __launch_bounds__(kBlock) contactPromoteKernel(Buffers b, const DevParams* __restrict__ pp) {
   const uint32_t n = contactListed(b);
@@ -2946,6 +2969,13 @@ int launchContactApply(const Buffers& b, const DevParams* p, const float4* src, 
 int launchContactValidate(const Buffers& b, const DevParams* p, const float4* tgt, cudaStream_t s) {
   if (b.contactCount == 0) return 0;
   contactValidateKernel<<<candidateBlocks(b), kBlock, 0, s>>>(b, p, tgt);
+  return 1;
+}
+
+int launchContactFeatures(const float* points, const uint32_t* types, uint32_t n, float* out, uint32_t* wide,
+                          cudaStream_t s) {
+  if (n == 0) return 0;
+  contactFeatureKernel<<<(n + kBlock - 1) / kBlock, kBlock, 0, s>>>(points, types, n, out, wide);
   return 1;
 }
 

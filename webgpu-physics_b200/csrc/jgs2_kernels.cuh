@@ -237,6 +237,10 @@ uint32_t broadPhaseSortPasses(uint32_t V);
 // the convergence pass.
 int launchContactGradient(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, uint32_t V,
                           cudaStream_t s);
+// Closest features of n caller pairs (12 floats each: four points) by the
+// step's device contact routine: 9 floats per pair out and the FP64 flag.
+int launchContactFeatures(const float* points, const uint32_t* types, uint32_t n, float* out, uint32_t* wide,
+                          cudaStream_t s);
 // bodyCorrection: some scene of the batch corrects its bodies this frame.
 int launchEpilogue(const Buffers& b, const DevParams* p, const float4* finalPos, uint32_t V, bool bodyCorrection,
                    uint32_t bodies, cudaStream_t s);

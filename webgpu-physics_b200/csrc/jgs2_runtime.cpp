@@ -2287,6 +2287,38 @@ jgs2_status jgs2_minimum_contact_distance(const jgs2_input* input, double cutoff
   return JGS2_OK;
 }
 
+jgs2_status jgs2_evaluate_contact_features(const float* points, const uint32_t* types, uint32_t count, float* out,
+                                           uint32_t* fp64_used, int device) {
+  if (count == 0) return JGS2_OK;
+  if (!points || !types || !out) return fail(nullptr, JGS2_INVALID_ARGUMENT, "points, types and out must not be NULL.");
+  for (uint32_t i = 0; i < count; ++i)
+    if (types[i] > 1u) return fail(nullptr, JGS2_INVALID_ARGUMENT, format("types[%u] must be 0 or 1.", i));
+  if (cudaSetDevice(device) != cudaSuccess) return fail(nullptr, JGS2_DEVICE_ERROR, "cudaSetDevice failed.");
+  float* dPoints = nullptr;
+  float* dOut = nullptr;
+  uint32_t* dTypes = nullptr;
+  uint32_t* dWide = nullptr;
+  cudaError_t e = cudaMalloc(&dPoints, sizeof(float) * 12ull * count);
+  if (e == cudaSuccess) e = cudaMalloc(&dOut, sizeof(float) * 9ull * count);
+  if (e == cudaSuccess) e = cudaMalloc(&dTypes, sizeof(uint32_t) * count);
+  if (e == cudaSuccess) e = cudaMalloc(&dWide, sizeof(uint32_t) * count);
+  if (e == cudaSuccess) e = cudaMemcpy(dPoints, points, sizeof(float) * 12ull * count, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dTypes, types, sizeof(uint32_t) * count, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    jgs2::launchContactFeatures(dPoints, dTypes, count, dOut, dWide, nullptr);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpy(out, dOut, sizeof(float) * 9ull * count, cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && fp64_used) e = cudaMemcpy(fp64_used, dWide, sizeof(uint32_t) * count, cudaMemcpyDeviceToHost);
+  cudaFree(dPoints);
+  cudaFree(dOut);
+  cudaFree(dTypes);
+  cudaFree(dWide);
+  if (e != cudaSuccess)
+    return fail(nullptr, JGS2_DEVICE_ERROR, format("contact feature evaluation: %s", cudaGetErrorString(e)));
+  return JGS2_OK;
+}
+
 jgs2_status jgs2_contact_superset_size(const jgs2_input* input, uint64_t* count) {
   std::string err;
   if (!validateInput(input, &err)) return fail(nullptr, JGS2_INVALID_ARGUMENT, err);
