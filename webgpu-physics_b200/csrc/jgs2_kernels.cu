@@ -33,7 +33,12 @@ namespace jgs2 {
 namespace {
 
 constexpr int kBlock = 128;
-constexpr int kGroup = 4;  // lanes per vertex in the solve kernel
+#ifndef JGS2_SOLVE_LANES
+#define JGS2_SOLVE_LANES 4
+#endif
+// Lanes per vertex in the solve kernel.  A warp holds 32 / kGroup lane groups;
+// a width that does not divide 32 leaves the warp's last lanes idle.
+constexpr int kGroup = JGS2_SOLVE_LANES;
 constexpr int kRecFloats = 56;  // cached cubature record state
 
 struct TetRec {
@@ -184,33 +189,75 @@ __device__ __forceinline__ float implicitEnergy(const DevParams& p, const Buffer
   return e;
 }
 
+// Reductions over a lane group of W lanes inside one warp.  A power-of-two
+// width folds with an xor butterfly; another width gathers the group's values
+// in lane order on every lane, so all lanes hold the same, order-fixed result.
+template <int W>
+__device__ __forceinline__ uint32_t groupBase() {
+  return ((threadIdx.x & 31u) / W) * W;
+}
 template <int W>
 __device__ __forceinline__ float groupSum(float v, unsigned mask) {
+  if constexpr ((W & (W - 1)) == 0) {
 #pragma unroll
-  for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, W);
-  return v;
+    for (int o = W / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, W);
+    return v;
+  } else {
+    const uint32_t base = groupBase<W>();
+    float s = __shfl_sync(mask, v, base);
+#pragma unroll
+    for (int j = 1; j < W; ++j) s += __shfl_sync(mask, v, base + j);
+    return s;
+  }
 }
 // Merge of the lanes' compensated sums over a lane group (xor butterfly;
 // every lane ends with the same pair because the merge is symmetric).
 template <int W>
+__device__ __forceinline__ Comp3 shflComp(const Comp3& a, unsigned mask, uint32_t src) {
+  Comp3 t;
+  t.s.x = __shfl_sync(mask, a.s.x, src);
+  t.s.y = __shfl_sync(mask, a.s.y, src);
+  t.s.z = __shfl_sync(mask, a.s.z, src);
+  t.c.x = __shfl_sync(mask, a.c.x, src);
+  t.c.y = __shfl_sync(mask, a.c.y, src);
+  t.c.z = __shfl_sync(mask, a.c.z, src);
+  return t;
+}
+template <int W>
 __device__ __forceinline__ void groupMerge(Comp3& a, unsigned mask) {
+  if constexpr ((W & (W - 1)) == 0) {
 #pragma unroll
-  for (int o = W / 2; o > 0; o >>= 1) {
-    Comp3 t;
-    t.s.x = __shfl_xor_sync(mask, a.s.x, o, W);
-    t.s.y = __shfl_xor_sync(mask, a.s.y, o, W);
-    t.s.z = __shfl_xor_sync(mask, a.s.z, o, W);
-    t.c.x = __shfl_xor_sync(mask, a.c.x, o, W);
-    t.c.y = __shfl_xor_sync(mask, a.c.y, o, W);
-    t.c.z = __shfl_xor_sync(mask, a.c.z, o, W);
-    cmerge(a, t);
+    for (int o = W / 2; o > 0; o >>= 1) {
+      Comp3 t;
+      t.s.x = __shfl_xor_sync(mask, a.s.x, o, W);
+      t.s.y = __shfl_xor_sync(mask, a.s.y, o, W);
+      t.s.z = __shfl_xor_sync(mask, a.s.z, o, W);
+      t.c.x = __shfl_xor_sync(mask, a.c.x, o, W);
+      t.c.y = __shfl_xor_sync(mask, a.c.y, o, W);
+      t.c.z = __shfl_xor_sync(mask, a.c.z, o, W);
+      cmerge(a, t);
+    }
+  } else {
+    const uint32_t base = groupBase<W>();
+    Comp3 r = shflComp<W>(a, mask, base);
+#pragma unroll
+    for (int j = 1; j < W; ++j) cmerge(r, shflComp<W>(a, mask, base + j));
+    a = r;
   }
 }
 template <int W>
 __device__ __forceinline__ float groupMin(float v, unsigned mask) {
+  if constexpr ((W & (W - 1)) == 0) {
 #pragma unroll
-  for (int o = W / 2; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(mask, v, o, W));
-  return v;
+    for (int o = W / 2; o > 0; o >>= 1) v = fminf(v, __shfl_xor_sync(mask, v, o, W));
+    return v;
+  } else {
+    const uint32_t base = groupBase<W>();
+    float m = __shfl_sync(mask, v, base);
+#pragma unroll
+    for (int j = 1; j < W; ++j) m = fminf(m, __shfl_sync(mask, v, base + j));
+    return m;
+  }
 }
 
 // Deterministic block sum of doubles (fixed tree order).
@@ -1528,6 +1575,9 @@ struct CubState {
 };
 static_assert(sizeof(CubState) <= kRecFloats * 4, "cubature cache record too small");
 
+#ifndef JGS2_SOLVE_PREFETCH
+#define JGS2_SOLVE_PREFETCH 0
+#endif
 #ifndef JGS2_SOLVE_MIN_BLOCKS
 #define JGS2_SOLVE_MIN_BLOCKS 4
 #endif
@@ -1538,23 +1588,40 @@ template <int W, bool kExt>
 __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
                                                       const float4* __restrict__ src, float4* tgt,
                                                       const uint32_t* __restrict__ list, uint32_t count,
-                                                      uint32_t K, int cachedIncident) {
+                                                      uint32_t K, int cachedIncident, uint32_t groupsPerBlock) {
   extern __shared__ float4 cache4[];
   CubState* cache = reinterpret_cast<CubState*>(cache4);
   __shared__ uint32_t sFail, sMaxBack, sSkip, sEvals, sMaxShift, sValid, sScene;
-  const uint32_t lane = threadIdx.x % W;
-  const uint32_t group = threadIdx.x / W;
-  const uint32_t groupsPerBlock = blockDim.x / W;
-  const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << ((threadIdx.x & 31u) / W * W));
+  // Lane groups never straddle a warp: warp w holds groups w * (32 / W) ...;
+  // lanes past the warp's last whole group, or past groupsPerBlock, are idle.
+  constexpr uint32_t kGroupsPerWarp = 32 / W;
+  const uint32_t lane = (threadIdx.x & 31u) % W;
+  const uint32_t groupInWarp = (threadIdx.x & 31u) / W;
+  const uint32_t group = (threadIdx.x >> 5) * kGroupsPerWarp + groupInWarp;
+  const bool groupLane = groupInWarp < kGroupsPerWarp && group < groupsPerBlock;
+  const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << (groupInWarp * W));
   if (threadIdx.x == 0) {
     sFail = 0; sMaxBack = 0; sSkip = 0; sEvals = 0; sMaxShift = 0; sValid = 1;
     const uint32_t first = blockIdx.x * groupsPerBlock;
     sScene = b.vertexScene[list ? list[first] : first];
+#if JGS2_SOLVE_PREFETCH > 0
+    // Whole sweeps: bring the record headers and basis blocks of the block
+    // JGS2_SOLVE_PREFETCH launches ahead into L2 (one bulk prefetch each),
+    // so that block finds them there.  In-bounds by construction.
+    const uint64_t ahead = uint64_t(blockIdx.x + JGS2_SOLVE_PREFETCH) * groupsPerBlock;
+    if (!list && ahead < count) {
+      const uint64_t n = min(uint64_t(groupsPerBlock), uint64_t(count) - ahead) * K;
+      const uint4* h = b.cubHead + 2ull * ahead * K;
+      const float4* u = b.cubBasis + 9ull * ahead * K;
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(h), "r"(uint32_t(n * 32ull)) : "memory");
+      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(u), "r"(uint32_t(n * 144ull)) : "memory");
+    }
+#endif
   }
   __syncthreads();
   // One vertex per lane group; its scene selects the settings and records.
   const uint32_t item = blockIdx.x * groupsPerBlock + group;
-  const bool haveVertex = item < count;
+  const bool haveVertex = groupLane && item < count;
   const uint32_t v = haveVertex ? (list ? list[item] : item) : 0u;
   const uint32_t scene = haveVertex ? b.vertexScene[v] : sScene;
   // Per-vertex outputs owned by lane 0.
@@ -2881,8 +2948,11 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   if (count == 0) return 0;
   const uint32_t fit = solveGroupsPerBlock(K);
   if (fit == 0) return 0;
-  const uint32_t groups = std::max(1u, fit >> std::min(b.solveShift, 2u));
+  const uint32_t shift = std::min(b.solveShift, 2u);
+  const uint32_t groups = std::max(1u, fit >> shift);
   const size_t smem = static_cast<size_t>(groups) * K * sizeof(CubState);
+  constexpr uint32_t perWarp = 32u / kGroup;
+  const uint32_t threads = (groups + perWarp - 1) / perWarp * 32u;
   // One vertex per lane group: the line search makes per-vertex work uneven,
   // and the block scheduler balances it better than a fixed grid stride.
   const uint32_t blocks = std::max(1u, (count + groups - 1) / groups);
@@ -2891,25 +2961,27 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   // vertex over its active candidates.  A broad-phase engine decides on the
   // superset too, so it runs the variant its static twin runs.
   const uint64_t superset = b.contactDynamic ? b.bpSuperset : b.contactCount;
+  const int ci = cachedIncident ? 1 : 0;
   if (b.contactIdx && superset * 4u > uint64_t(64) * count) {
-    const uint32_t wg = std::max(1u, std::min(groups * kGroup / 32u, kBlock / 32u));
+    // Warps per block: an eighth of the vertices a 4-lane block of the same
+    // cache budget would take (at most a full block).
+    const uint32_t perVertex = static_cast<uint32_t>(K * sizeof(CubState));
+    const uint32_t fit4 = std::min<uint32_t>(32u, perVertex ? solveSharedBytes() / perVertex : 32u);
+    const uint32_t wg = std::max(1u, std::min(std::max(1u, fit4 >> shift) * 4u / 32u, kBlock / 32u));
     const size_t wsmem = static_cast<size_t>(wg) * K * sizeof(CubState);
-    solveKernel<32, true><<<std::max(1u, (count + wg - 1) / wg), wg * 32, wsmem, s>>>(
-        b, p, src, tgt, list, count, K, cachedIncident ? 1 : 0);
+    solveKernel<32, true><<<std::max(1u, (count + wg - 1) / wg), wg * 32, wsmem, s>>>(b, p, src, tgt, list, count,
+                                                                                      K, ci, wg);
   } else if (b.clothRange || b.contactIdx) {
-    solveKernel<kGroup, true><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
-                                                                    cachedIncident ? 1 : 0);
+    solveKernel<kGroup, true><<<blocks, threads, smem, s>>>(b, p, src, tgt, list, count, K, ci, groups);
   } else {
-    solveKernel<kGroup, false><<<blocks, groups * kGroup, smem, s>>>(b, p, src, tgt, list, count, K,
-                                                                     cachedIncident ? 1 : 0);
+    solveKernel<kGroup, false><<<blocks, threads, smem, s>>>(b, p, src, tgt, list, count, K, ci, groups);
   }
   return 1;
 }
 
-uint32_t solveGroupsPerBlock(uint32_t K) {
-  // Shared memory holds one cached record state per cubature record of each
-  // vertex in the block; large K (an exact complement) trades vertices per
-  // block for cache.
+// Dynamic shared memory a solve block may use (the device's opt-in limit less
+// the kernel's static shared memory); sets the kernels' attribute once.
+uint32_t solveSharedBytes() {
   static int optin = -1;
   if (optin < 0) {
     int dev = 0;
@@ -2920,9 +2992,16 @@ uint32_t solveGroupsPerBlock(uint32_t K) {
     cudaFuncSetAttribute(solveKernel<kGroup, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
     cudaFuncSetAttribute(solveKernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   }
+  return static_cast<uint32_t>(optin);
+}
+
+uint32_t solveGroupsPerBlock(uint32_t K) {
+  // Shared memory holds one cached record state per cubature record of each
+  // vertex in the block; large K (an exact complement) trades vertices per
+  // block for cache.
   const uint32_t perVertex = static_cast<uint32_t>(K * sizeof(CubState));
-  uint32_t groups = kBlock / kGroup;
-  if (perVertex > 0) groups = std::min<uint32_t>(groups, static_cast<uint32_t>(optin) / perVertex);
+  uint32_t groups = (kBlock / 32) * (32 / kGroup);
+  if (perVertex > 0) groups = std::min<uint32_t>(groups, solveSharedBytes() / perVertex);
   return groups;
 }
 

@@ -266,6 +266,8 @@ int launchOracleDiagnostics(const Buffers& b, const OracleParams& q, float4* tet
 
 // Vertices per solve block for cubature width K (0: K too large to cache).
 uint32_t solveGroupsPerBlock(uint32_t K);
+// Dynamic shared memory available to one solve block.
+uint32_t solveSharedBytes();
 constexpr size_t kGatePartialBytes = 32;
 constexpr size_t kConvPartialBytes = 80;
 
