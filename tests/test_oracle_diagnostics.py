@@ -90,7 +90,9 @@ def _reference(inp, x, pred, h, forces, targets, floor_height, floor_k):
 def test_oracle_diagnostics_match_a_float64_restatement():
     inp = scenes.cantilever(cells=(6, 2, 2), size=(0.6, 0.2, 0.2), cubature_k=6)
     rest = inp.positions.reshape(-1, 4)[:, :3]
-    floor_height = float(rest[:, 1].min()) + 0.01  # the bottom row starts inside the floor
+    # The bottom row starts inside the floor; the height is the f32 value the
+    # device compares against, so both sides decide floor contact alike.
+    floor_height = float(np.float32(float(rest[:, 1].min()) + 0.01))
     settings = dict(timestep=1 / 60, floorHeight=floor_height, floorStiffness=2e4, parityMode=True)
     gpu = solver.JGS2GpuSolver.create(inp, settings)
     V = inp.vertex_count
@@ -120,7 +122,8 @@ def test_oracle_diagnostics_match_a_float64_restatement():
     assert np.abs(rec[active, 0, :3] - grad[active]).max() <= 1e-4 * gscale + 1e-5
     hblock = rec[:, 1:4, :3]  # row-major rows of the block
     hscale = np.abs(H[active]).max()
-    assert np.abs(hblock[active] - H[active]).max() <= 1e-4 * hscale
+    herr = np.abs(hblock[active] - H[active]).max(axis=(1, 2))
+    assert herr.max() <= 1e-4 * hscale, (herr.max() / hscale, np.flatnonzero(active)[herr.argmax()])
     assert (rec[~active, 0, 3] == 0).all() and (rec[active, 0, 3] == 1).all()
     np.testing.assert_allclose(d["tetRecords"][:, 0], tet_e, rtol=1e-3, atol=1e-6 * np.abs(tet_e).max())
     np.testing.assert_allclose(d["tetRecords"][:, 1], tet_det, rtol=1e-5)
