@@ -125,7 +125,11 @@ def test_oracle_diagnostics_match_a_float64_restatement():
     herr = np.abs(hblock[active] - H[active]).max(axis=(1, 2))
     assert herr.max() <= 1e-4 * hscale, (herr.max() / hscale, np.flatnonzero(active)[herr.argmax()])
     assert (rec[~active, 0, 3] == 0).all() and (rec[active, 0, 3] == 1).all()
-    np.testing.assert_allclose(d["tetRecords"][:, 0], tet_e, rtol=1e-3, atol=1e-6 * np.abs(tet_e).max())
+    # f32 evaluation of a tet's energy cancels terms of size vol (3 mu + lambda)
+    # (I1 is near 3 and J near 1 close to rest): allow one rounding of that.
+    meta = inp.tet_meta.reshape(-1, 4).astype(np.float64)
+    cancel = 2.0 ** -24 * meta[:, 0] * (3 * meta[:, 2] + meta[:, 1])
+    assert (np.abs(d["tetRecords"][:, 0] - tet_e) <= 1e-3 * np.abs(tet_e) + cancel).all()
     np.testing.assert_allclose(d["tetRecords"][:, 1], tet_det, rtol=1e-5)
     assert d["minimumDeformationDeterminant"] == pytest.approx(tet_det.min(), rel=1e-5)
     updates = gpu.readFinalIterationUpdates().reshape(V, -1)[:, 0]  # (magnitude, 0, 0, valid) per vertex

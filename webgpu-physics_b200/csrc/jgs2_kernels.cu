@@ -1575,6 +1575,59 @@ struct CubState {
 };
 static_assert(sizeof(CubState) <= kRecFloats * 4, "cubature cache record too small");
 
+#ifndef JGS2_SOLVE_STAGE
+#define JGS2_SOLVE_STAGE 1
+#endif
+// Shared-memory slot of one cubature record of a solve block.  The block
+// first stages every record's header, basis blocks and tetrahedron record
+// into its slot with asynchronous copies (all independent, so the whole
+// block's input is in flight at once instead of one dependent chain per
+// record and lane); the lane that owns the record then reads its inputs from
+// the slot and overwrites the slot with the record's cached state for the
+// line search.
+struct RecSlot {
+  uint4 head[2];   // (tet, weight bits, 0, 0), the tet's vertex indices
+  float4 basis[9]; // 36 floats: four row-major 3x3 blocks
+  float4 tet[4];   // [g1 vol] [g2 lambda] [g3 mu] [indices]
+};
+static_assert(sizeof(CubState) <= sizeof(RecSlot), "record state must fit its staging slot");
+#if JGS2_SOLVE_STAGE
+constexpr size_t kSolveSlotBytes = sizeof(RecSlot);
+#else
+constexpr size_t kSolveSlotBytes = sizeof(CubState);
+#endif
+
+__device__ __forceinline__ void cpAsync16(void* smem, const void* gmem) {
+  const uint32_t sa = static_cast<uint32_t>(__cvta_generic_to_shared(smem));
+  asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cpAsyncWaitAll() {
+  asm volatile("cp.async.commit_group;" ::: "memory");
+  asm volatile("cp.async.wait_group 0;" ::: "memory");
+}
+__device__ __forceinline__ TetRec tetFromSlot(const float4* q) {
+  const float4 a = q[0], b = q[1], c = q[2];
+  const float4 d = q[3];
+  TetRec r;
+  r.g1 = f3(a.x, a.y, a.z);
+  r.g2 = f3(b.x, b.y, b.z);
+  r.g3 = f3(c.x, c.y, c.z);
+  r.vol = a.w;
+  r.lambda = b.w;
+  r.mu = c.w;
+  r.idx = make_uint4(__float_as_uint(d.x), __float_as_uint(d.y), __float_as_uint(d.z), __float_as_uint(d.w));
+  return r;
+}
+// loadBlockVec from a shared-memory copy of the record's basis.
+__device__ __forceinline__ M3 loadBlockVecShared(const float4* rec, int l) {
+  const int k0 = (9 * l) >> 2;
+  const int off = 9 * l - 4 * k0;
+  const float4 a = rec[k0], b = rec[k0 + 1], c = rec[k0 + 2];
+  const float f[12] = {a.x, a.y, a.z, a.w, b.x, b.y, b.z, b.w, c.x, c.y, c.z, c.w};
+  return {f3(f[off + 0], f[off + 3], f[off + 6]), f3(f[off + 1], f[off + 4], f[off + 7]),
+          f3(f[off + 2], f[off + 5], f[off + 8])};
+}
+
 #ifndef JGS2_SOLVE_PREFETCH
 #define JGS2_SOLVE_PREFETCH 0
 #endif
@@ -1590,7 +1643,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                                                       const uint32_t* __restrict__ list, uint32_t count,
                                                       uint32_t K, int cachedIncident, uint32_t groupsPerBlock) {
   extern __shared__ float4 cache4[];
-  CubState* cache = reinterpret_cast<CubState*>(cache4);
+  unsigned char* slotBase = reinterpret_cast<unsigned char*>(cache4);
   __shared__ uint32_t sFail, sMaxBack, sSkip, sEvals, sMaxShift, sValid, sScene;
   // Lane groups never straddle a warp: warp w holds groups w * (32 / W) ...;
   // lanes past the warp's last whole group, or past groupsPerBlock, are idle.
@@ -1619,6 +1672,32 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
 #endif
   }
   __syncthreads();
+#if JGS2_SOLVE_STAGE
+  {
+    // Stage the block's records: headers and basis blocks, then (once the
+    // headers have landed) the tetrahedron records they name.
+    RecSlot* slots = reinterpret_cast<RecSlot*>(slotBase);
+    const uint32_t nrec = groupsPerBlock * K;
+    for (uint32_t c = threadIdx.x; c < nrec * 11u; c += blockDim.x) {
+      const uint32_t r = c / 11u, part = c - r * 11u;
+      const uint32_t g = r / K, it = blockIdx.x * groupsPerBlock + g;
+      if (it >= count) continue;
+      const size_t rec = static_cast<size_t>(list ? list[it] : it) * K + (r - g * K);
+      if (part < 2u) cpAsync16(&slots[r].head[part], &b.cubHead[2 * rec + part]);
+      else cpAsync16(&slots[r].basis[part - 2u], &b.cubBasis[9 * rec + (part - 2u)]);
+    }
+    cpAsyncWaitAll();
+    __syncthreads();
+    for (uint32_t c = threadIdx.x; c < nrec * 4u; c += blockDim.x) {
+      const uint32_t r = c >> 2, part = c & 3u;
+      if (blockIdx.x * groupsPerBlock + r / K >= count) continue;
+      const uint4 head = slots[r].head[0];
+      if (head.x != kEmptyTet && __uint_as_float(head.y) > 0.0f) cpAsync16(&slots[r].tet[part], &b.tets[4ull * head.x + part]);
+    }
+    cpAsyncWaitAll();
+    __syncthreads();
+  }
+#endif
   // One vertex per lane group; its scene selects the settings and records.
   const uint32_t item = blockIdx.x * groupsPerBlock + group;
   const bool haveVertex = groupLane && item < count;
@@ -1680,23 +1759,34 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
         // per basis block.  The exact source block subtracted for a record at
         // the vertex's own slot is formed in the world frame.
         const M3 Rs = loadRot(b.vertexRot, v);
-        CubState* myCache = cache + static_cast<size_t>(group) * K;
+        unsigned char* mySlots = slotBase + static_cast<size_t>(group) * K * kSolveSlotBytes;
         // Cubature records first, then (unless cached) the incident tets, in
         // separate loops so the two kinds of item never share a divergent pass.
         for (uint32_t u = lane; u < K; u += W) {
           {
             // ---- cubature record (jgs2-shader.ts:3197-3263) ----
             CubState st;
+#if JGS2_SOLVE_STAGE
+            const RecSlot* staged = reinterpret_cast<const RecSlot*>(mySlots + u * kSolveSlotBytes);
+            const uint4 head = staged->head[0];
+            const uint4 idx = staged->head[1];
+#else
             const size_t rec = static_cast<size_t>(v) * K + u;
             const uint4 head = __ldg(&b.cubHead[2 * rec]);
             const uint4 idx = __ldg(&b.cubHead[2 * rec + 1]);
+#endif
             const uint32_t t = head.x;
             const float w = __uint_as_float(head.y);
             st.w = 0.0f;
             // Headers hold global tet ids; out-of-range records were emptied at create.
             if (t != kEmptyTet && w > 0.0f) {
+#if JGS2_SOLVE_STAGE
+              const TetRec r = tetFromSlot(staged->tet);
+              const float4* U = staged->basis;
+#else
               const TetRec r = loadTet(b.tets, t);
               const float4* U = b.cubBasis + 9ull * rec;
+#endif
               // One basis block B'_l = R_l Ubar_l at a time: accumulate F,
               // the projected directions dF_c = sum_l B'_l[:,c] g_l^T and the
               // inertia / objective quadratic (gQ, HQ) of the record, all in
@@ -1711,7 +1801,11 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
                 const uint32_t q = idxAt(idx, l);
                 if (q == v) slot = l;
                 const float3 gl = shapeGradient(r, l);
+#if JGS2_SOLVE_STAGE
+                const M3 B = mm(loadRot(b.vertexRot, q), loadBlockVecShared(U, l));
+#else
                 const M3 B = mm(loadRot(b.vertexRot, q), loadBlockVec(U, l));
+#endif
                 const float3 xl = l == 0 ? x0 : xyz(src[q]);
                 if (l > 0) F = F + outer(xl - x0, gl);
                 dF0 = dF0 + outer(B.c0, gl);
@@ -1788,7 +1882,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
               st.slot = slot;
               st.gs = gs;
             }
-            myCache[u] = st;
+            *reinterpret_cast<CubState*>(mySlots + u * kSolveSlotBytes) = st;
           }
         }
         if (!cachedIncident) {
@@ -1884,7 +1978,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
             // A lane's items in order: its cached cubature records, then its
             // incident tets (the same per-lane order as one merged loop).
             for (uint32_t u = lane; u < K; u += W) {
-              const CubState& st = myCache[u];
+              const CubState& st = *reinterpret_cast<const CubState*>(mySlots + u * kSolveSlotBytes);
               if (!(st.w > 0.0f)) continue;
               float J = 0.0f;
               // Record state is in the source frame: the trial step there is R_s^T td.
@@ -2950,7 +3044,7 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   if (fit == 0) return 0;
   const uint32_t shift = std::min(b.solveShift, 2u);
   const uint32_t groups = std::max(1u, fit >> shift);
-  const size_t smem = static_cast<size_t>(groups) * K * sizeof(CubState);
+  const size_t smem = static_cast<size_t>(groups) * K * kSolveSlotBytes;
   constexpr uint32_t perWarp = 32u / kGroup;
   const uint32_t threads = (groups + perWarp - 1) / perWarp * 32u;
   // One vertex per lane group: the line search makes per-vertex work uneven,
@@ -2965,10 +3059,10 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
   if (b.contactIdx && superset * 4u > uint64_t(64) * count) {
     // Warps per block: an eighth of the vertices a 4-lane block of the same
     // cache budget would take (at most a full block).
-    const uint32_t perVertex = static_cast<uint32_t>(K * sizeof(CubState));
+    const uint32_t perVertex = static_cast<uint32_t>(K * kSolveSlotBytes);
     const uint32_t fit4 = std::min<uint32_t>(32u, perVertex ? solveSharedBytes() / perVertex : 32u);
     const uint32_t wg = std::max(1u, std::min(std::max(1u, fit4 >> shift) * 4u / 32u, kBlock / 32u));
-    const size_t wsmem = static_cast<size_t>(wg) * K * sizeof(CubState);
+    const size_t wsmem = static_cast<size_t>(wg) * K * kSolveSlotBytes;
     solveKernel<32, true><<<std::max(1u, (count + wg - 1) / wg), wg * 32, wsmem, s>>>(b, p, src, tgt, list, count,
                                                                                       K, ci, wg);
   } else if (b.clothRange || b.contactIdx) {
@@ -2999,7 +3093,7 @@ uint32_t solveGroupsPerBlock(uint32_t K) {
   // Shared memory holds one cached record state per cubature record of each
   // vertex in the block; large K (an exact complement) trades vertices per
   // block for cache.
-  const uint32_t perVertex = static_cast<uint32_t>(K * sizeof(CubState));
+  const uint32_t perVertex = static_cast<uint32_t>(K * kSolveSlotBytes);
   uint32_t groups = (kBlock / 32) * (32 / kGroup);
   if (perVertex > 0) groups = std::min<uint32_t>(groups, solveSharedBytes() / perVertex);
   return groups;
