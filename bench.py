@@ -76,18 +76,8 @@ def workload(cells: int):
     """Build (or load from the local cache) the cube's packed step input."""
     from jgs2_b200 import scenes
 
-    path = os.path.join(cache_dir(), f"cube{cells}_k6_r2_v1.npz")
-    if os.path.exists(path):
-        try:
-            return scenes.SceneInput.load(path), True
-        except Exception:
-            os.remove(path)
-    inp = scenes.unit_cube(cells=cells)
-    try:
-        inp.save(path)
-    except OSError:
-        pass
-    return inp, False
+    return scenes.cached_input(cache_dir(), f"cube{cells}", scenes.unit_cube_components(cells=cells),
+                               lambda: scenes.unit_cube(cells=cells))
 
 
 def workload_config(inp, args, precompute_info):
@@ -118,21 +108,13 @@ def batched_workload(count: int):
     """The batched uneven bodies as independent scenes (cached packed input)."""
     from jgs2_b200 import scenes
 
-    path = os.path.join(cache_dir(), f"batched{count}_k6_r2_v1.npz")
-    cached = False
-    inp = None
-    if os.path.exists(path):
-        try:
-            inp = scenes.SceneInput.load(path)
-            cached = True
-        except Exception:
-            os.remove(path)
-    if inp is None:
-        inp = scenes.batched_bodies(count=count)
-        try:
-            inp.save(path)
-        except OSError:
-            pass
+    components = {"topology": {"builder": "batched_bodies", "count": count, "seed": 65537, "cells": [4, 32],
+                               "spacing": 0.25},
+                  "materials": {"soft": 5e4, "stiff": 5e6, "poisson": 0.4, "density": 1000.0},
+                  "timestep": 1 / 60, "basis": {"method": "patch", "patch_radius": 2},
+                  "cubature": {"k": 6, "exact_complement": 0}, "solverSchedule": "jacobi"}
+    inp, cached = scenes.cached_input(cache_dir(), f"batched{count}", components,
+                                      lambda: scenes.batched_bodies(count=count))
     return inp, inp.split_bodies(), cached
 
 
@@ -479,29 +461,26 @@ def serving_arm(args):
     device = local
     t0 = time.perf_counter()
 
-    def cached(name, build):
-        path = os.path.join(cache_dir(), name)
-        if os.path.exists(path):
-            try:
-                return scenes.SceneInput.load(path)
-            except Exception:
-                os.remove(path)
-        inp = build()
-        try:
-            inp.save(path)
-        except OSError:
-            pass
-        return inp
+    def cached(prefix, builder, options, build):
+        # The builder's name and options fingerprint every component: they
+        # determine topology, materials, timestep and precompute.
+        desc = {"builder": builder, "options": options}
+        components = {c: desc for c in ("topology", "materials", "timestep", "basis", "cubature")}
+        components["solverSchedule"] = "jacobi"
+        return scenes.cached_input(cache_dir(), prefix, components, build)[0]
 
     bar_settings = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floorStiffness=0.0, parityMode=True)
     kinds = {}  # key -> (input, settings, iterations per frame)
     for r in (1, 2, 3, 4):
-        kinds[("bar", r)] = (cached(f"cantilever_x{r}_k6_v1.npz", lambda r=r: scenes.cantilever(
-            cells=(20 * r, 4 * r, 4 * r), method=scenes.PRECOMPUTE_PATCH)), bar_settings, 10)
+        kinds[("bar", r)] = (cached(f"cantilever_x{r}", "cantilever", {"scale": r, "k": 6, "method": "patch"},
+                                    lambda r=r: scenes.cantilever(cells=(20 * r, 4 * r, 4 * r),
+                                                                  method=scenes.PRECOMPUTE_PATCH)), bar_settings, 10)
     for n_boxes in range(1, 21):
-        kinds[("trough", n_boxes)] = (cached(f"box_trough_{n_boxes}_v1.npz", lambda n_boxes=n_boxes: scenes.box_trough(
-            boxes=n_boxes)), dict(scenes.BOX_TROUGH_SETTINGS), 15)
-    kinds[("cloth", 0)] = (cached("cloth_sphere_127_v1.npz", scenes.cloth_sphere), dict(scenes.CLOTH_SETTINGS), 5)
+        kinds[("trough", n_boxes)] = (cached(f"box_trough_{n_boxes}", "box_trough", {"boxes": n_boxes},
+                                             lambda n_boxes=n_boxes: scenes.box_trough(boxes=n_boxes)),
+                                      dict(scenes.BOX_TROUGH_SETTINGS), 15)
+    kinds[("cloth", 0)] = (cached("cloth_sphere_127", "cloth_sphere", {"cells": 127}, scenes.cloth_sphere),
+                           dict(scenes.CLOTH_SETTINGS), 5)
     build_s = time.perf_counter() - t0
     rng = np.random.default_rng(2000 + rank)
     n = args.requests

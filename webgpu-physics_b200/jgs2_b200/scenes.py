@@ -12,6 +12,7 @@ from __future__ import annotations
 import ctypes
 import dataclasses
 import math
+import os
 from ctypes import c_double, c_uint32
 from typing import Optional
 
@@ -165,6 +166,19 @@ class SceneInput:
                               if isinstance(getattr(self, f.name), np.ndarray)
                               else getattr(self, f.name))
                      for f in dataclasses.fields(self)})
+
+    def arrays(self) -> dict:
+        """Every array of the input plus its counts (the artifact payload)."""
+        out = {f.name: getattr(self, f.name) for f in dataclasses.fields(self)
+               if isinstance(getattr(self, f.name), np.ndarray)}
+        out["__meta"] = np.array([self.vertex_count, self.tet_count, self.cubature_k], dtype=np.int64)
+        return out
+
+    @classmethod
+    def from_arrays(cls, arrays: dict) -> "SceneInput":
+        meta = arrays["__meta"]
+        kwargs = {k: v for k, v in arrays.items() if k != "__meta"}
+        return cls(vertex_count=int(meta[0]), tet_count=int(meta[1]), cubature_k=int(meta[2]), **kwargs)
 
     def save(self, path: str):
         arrays = {f.name: getattr(self, f.name) for f in dataclasses.fields(self)
@@ -762,6 +776,39 @@ def cantilever_target(inp: SceneInput, frame: int):
     target = rest + np.array(CANTILEVER_TARGET_OFFSET) * (length / 2.0) * progress
     active = start <= frame < CANTILEVER_TARGET_RELEASE
     return vertex, target.astype(np.float32), (CANTILEVER_TARGET_STIFFNESS if active else 0.0)
+
+
+def unit_cube_components(cells=100, young=1e6, poisson=0.45, density=1000.0, timestep=1 / 60, cubature_k=6,
+                         seed=1048583, patch_radius=2, method=PRECOMPUTE_PATCH, exact_complement=0,
+                         schedule="jacobi") -> dict:
+    """Fingerprint components of a unit_cube input (artifact.COMPONENTS)."""
+    return {"topology": {"builder": "unit_cube", "cells": [cells] * 3, "size": [1.0, 1.0, 1.0],
+                         "pinned": "y_min", "stretch_seed": seed},
+            "materials": {"density": density, "young": young, "poisson": poisson, "model": "stable-neo-hookean"},
+            "timestep": timestep,
+            "basis": {"method": method, "patch_radius": patch_radius},
+            "cubature": {"k": cubature_k, "exact_complement": exact_complement},
+            "solverSchedule": schedule}
+
+
+def cached_input(cache_dir: str, prefix: str, components: dict, build):
+    """The input `build()` makes, kept as a fingerprinted artifact under
+    `cache_dir` and reused only when every component fingerprint matches and
+    the payload is intact; returns (input, reused)."""
+    from . import artifact
+
+    prints = artifact.fingerprints(components)
+    path = os.path.join(cache_dir, artifact.cache_name(prefix, prints))
+    try:
+        return artifact.load(path, prints, SceneInput), True
+    except artifact.ArtifactMismatch:
+        pass
+    inp = build()
+    try:
+        artifact.save(path, inp, prints)
+    except OSError:
+        pass
+    return inp, False
 
 
 def unit_cube(cells=100, young=1e6, poisson=0.45, density=1000.0, timestep=1 / 60,
