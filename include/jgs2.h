@@ -483,6 +483,20 @@ jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* solver, const float* devic
                                          const jgs2_settings* overrides, uint32_t override_mask,
                                          float* device_control_out, void* stream);
 
+/* Checkpoint / resume.  The reference keeps no such call (its state lives in
+ * GPU buffers for the page's lifetime); these serialise what the reference's
+ * step carries from one frame to the next (positions, velocities, the
+ * objectives, the frame's diagnostics records) so a run can be stopped and
+ * resumed, or replayed, bit for bit.  The image is self-describing (magic,
+ * version, element counts) and host-endian.
+ * jgs2_export_state: *size receives the image's byte count; with out == NULL
+ * nothing else happens.  Waits for the solver's stream.
+ * jgs2_import_state: restores an image exported by a solver created from an
+ * input with the same counts; the next step then continues exactly as the
+ * exporting solver's would.  Single-scene solvers only. */
+jgs2_status jgs2_export_state(jgs2_solver* solver, void* out, size_t capacity, size_t* size);
+jgs2_status jgs2_import_state(jgs2_solver* solver, const void* image, size_t size);
+
 /* Zero-copy consumers (the reference's currentPositionBuffer, :1504-1507):
  * device address of the canonical vec4 position array and the solver's
  * cudaStream_t.  Valid until jgs2_destroy. */

@@ -1,0 +1,63 @@
+"""The graph-coloured schedule as one persistent kernel per iteration
+(per-colour phases separated by grid barriers, jgs2-solver.ts:2275-2325)
+against the launch-per-colour encoding, and the bounded barrier: with a spin
+bound of zero polls a waiting block gives up at once, every block leaves the
+kernel, and the host reports JGS2_TIMEOUT at its next synchronisation while
+the device stays usable."""
+import os
+
+import numpy as np
+import pytest
+
+from jgs2_b200 import _ffi, scenes, solver
+
+pytestmark = pytest.mark.gpu
+
+SETTINGS = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floorStiffness=0.0, parityMode=True, schedule=1)
+
+
+def _with_env(name, value, fn):
+    old = os.environ.get(name)
+    os.environ[name] = value
+    try:
+        return fn()
+    finally:
+        if old is None:
+            del os.environ[name]
+        else:
+            os.environ[name] = old
+
+
+def test_persistent_sweep_equals_per_colour_launches():
+    inp = scenes.unit_cube(cells=12)
+    a = solver.JGS2GpuSolver.create(inp, SETTINGS)
+    b = _with_env("JGS2_COLOR_SWEEP", "launches", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS))
+    assert a.scheduleColorCount > 1
+    for frame in range(3):
+        la, lb = a.kernelLaunchCount(), b.kernelLaunchCount()
+        a.stepExactIterations(6)
+        b.stepExactIterations(6)
+        np.testing.assert_array_equal(a.readPositions(), b.readPositions(), err_msg=f"frame {frame}")
+        np.testing.assert_array_equal(a.readGlobalizationDiagnostics()["history"],
+                                      b.readGlobalizationDiagnostics()["history"])
+        # One sweep (a barrier reset and a kernel) per iteration instead of two
+        # launches per colour.
+        assert a.kernelLaunchCount() - la < b.kernelLaunchCount() - lb
+    a.destroy()
+    b.destroy()
+
+
+def test_barrier_timeout_is_reported_and_the_device_stays_usable():
+    inp = scenes.unit_cube(cells=12)
+    s = _with_env("JGS2_BARRIER_SPIN_LIMIT", "0", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS))
+    s.stepExactIterations(2)
+    with pytest.raises(_ffi.JGS2Error) as err:
+        s.readPositions()
+    assert err.value.status == 5  # JGS2_TIMEOUT
+    assert "grid barrier" in err.value.message
+    s.destroy()
+    # The context survived: a fresh solver steps and reads normally.
+    t = solver.JGS2GpuSolver.create(inp, SETTINGS)
+    t.stepExactIterations(2)
+    assert np.isfinite(t.readPositions()).all()
+    t.destroy()

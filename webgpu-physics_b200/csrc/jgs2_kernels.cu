@@ -1628,20 +1628,20 @@ __device__ __forceinline__ M3 loadBlockVecShared(const float4* rec, int l) {
           f3(f[off + 2], f[off + 5], f[off + 8])};
 }
 
-#ifndef JGS2_SOLVE_PREFETCH
-#define JGS2_SOLVE_PREFETCH 0
-#endif
 #ifndef JGS2_SOLVE_MIN_BLOCKS
 #define JGS2_SOLVE_MIN_BLOCKS 4
 #endif
 
 // kExt: some scene of the engine has cloth or contact candidates (their
 // gathers and line search terms are compiled out otherwise).
+// One block's chunk `chunk` of the vertex list: vertices
+// [chunk * groupsPerBlock, (chunk + 1) * groupsPerBlock) of `list` (or of all
+// vertices).  Every thread of the block calls it with the same chunk.
 template <int W, bool kExt>
-__global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
-                                                      const float4* __restrict__ src, float4* tgt,
-                                                      const uint32_t* __restrict__ list, uint32_t count,
-                                                      uint32_t K, int cachedIncident, uint32_t groupsPerBlock) {
+__device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __restrict__ pp,
+                                           const float4* __restrict__ src, float4* tgt,
+                                           const uint32_t* __restrict__ list, uint32_t count, uint32_t K,
+                                           int cachedIncident, uint32_t groupsPerBlock, uint32_t chunk) {
   extern __shared__ float4 cache4[];
   unsigned char* slotBase = reinterpret_cast<unsigned char*>(cache4);
   __shared__ uint32_t sFail, sMaxBack, sSkip, sEvals, sMaxShift, sValid, sScene;
@@ -1655,21 +1655,8 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
   const unsigned mask = W == 32 ? 0xffffffffu : (((1u << W) - 1u) << (groupInWarp * W));
   if (threadIdx.x == 0) {
     sFail = 0; sMaxBack = 0; sSkip = 0; sEvals = 0; sMaxShift = 0; sValid = 1;
-    const uint32_t first = blockIdx.x * groupsPerBlock;
+    const uint32_t first = chunk * groupsPerBlock;
     sScene = b.vertexScene[list ? list[first] : first];
-#if JGS2_SOLVE_PREFETCH > 0
-    // Whole sweeps: bring the record headers and basis blocks of the block
-    // JGS2_SOLVE_PREFETCH launches ahead into L2 (one bulk prefetch each),
-    // so that block finds them there.  In-bounds by construction.
-    const uint64_t ahead = uint64_t(blockIdx.x + JGS2_SOLVE_PREFETCH) * groupsPerBlock;
-    if (!list && ahead < count) {
-      const uint64_t n = min(uint64_t(groupsPerBlock), uint64_t(count) - ahead) * K;
-      const uint4* h = b.cubHead + 2ull * ahead * K;
-      const float4* u = b.cubBasis + 9ull * ahead * K;
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(h), "r"(uint32_t(n * 32ull)) : "memory");
-      asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(u), "r"(uint32_t(n * 144ull)) : "memory");
-    }
-#endif
   }
   __syncthreads();
 #if JGS2_SOLVE_STAGE
@@ -1680,7 +1667,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
     const uint32_t nrec = groupsPerBlock * K;
     for (uint32_t c = threadIdx.x; c < nrec * 11u; c += blockDim.x) {
       const uint32_t r = c / 11u, part = c - r * 11u;
-      const uint32_t g = r / K, it = blockIdx.x * groupsPerBlock + g;
+      const uint32_t g = r / K, it = chunk * groupsPerBlock + g;
       if (it >= count) continue;
       const size_t rec = static_cast<size_t>(list ? list[it] : it) * K + (r - g * K);
       if (part < 2u) cpAsync16(&slots[r].head[part], &b.cubHead[2 * rec + part]);
@@ -1690,7 +1677,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
     __syncthreads();
     for (uint32_t c = threadIdx.x; c < nrec * 4u; c += blockDim.x) {
       const uint32_t r = c >> 2, part = c & 3u;
-      if (blockIdx.x * groupsPerBlock + r / K >= count) continue;
+      if (chunk * groupsPerBlock + r / K >= count) continue;
       const uint4 head = slots[r].head[0];
       if (head.x != kEmptyTet && __uint_as_float(head.y) > 0.0f) cpAsync16(&slots[r].tet[part], &b.tets[4ull * head.x + part]);
     }
@@ -1699,7 +1686,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
   }
 #endif
   // One vertex per lane group; its scene selects the settings and records.
-  const uint32_t item = blockIdx.x * groupsPerBlock + group;
+  const uint32_t item = chunk * groupsPerBlock + group;
   const bool haveVertex = groupLane && item < count;
   const uint32_t v = haveVertex ? (list ? list[item] : item) : 0u;
   const uint32_t scene = haveVertex ? b.vertexScene[v] : sScene;
@@ -2151,6 +2138,85 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buf
     if (sEvals) atomicAdd(&fs->localEvaluations, sEvals);
     if (sMaxShift) atomicMax(&fs->localMaxShift, sMaxShift);
     if (!sValid) atomicAnd(&fs->localNumericsValid, 0u);
+  }
+}
+
+template <int W, bool kExt>
+__global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
+                                                      const float4* __restrict__ src, float4* tgt,
+                                                      const uint32_t* __restrict__ list, uint32_t count,
+                                                      uint32_t K, int cachedIncident, uint32_t groupsPerBlock) {
+  solveChunk<W, kExt>(b, pp, src, tgt, list, count, K, cachedIncident, groupsPerBlock, blockIdx.x);
+}
+
+// ---------------------------------------------------------------------------
+// Graph-coloured sweep as one persistent kernel (jgs2-solver.ts:2275-2325,
+// colour masks jgs2-shader.ts:3004-3012): for each colour, the vertex frames
+// of the vertices the colour's solves read, a grid barrier, the in-place
+// local solves of the colour's vertices, a grid barrier.  The grid is
+// launched cooperatively (all blocks resident).  Each barrier is a bounded
+// spin: a block that waits longer than `spinLimit` polls sets the sweep's
+// error word and every block leaves at its next barrier, so the kernel always
+// returns; the host reports JGS2_TIMEOUT at its next synchronisation.
+struct SweepBarrier {
+  uint32_t arrived, generation, error, pad;
+};
+
+// Bounded grid barrier; false when the sweep has failed (by this block's
+// timeout or another's).
+__device__ __forceinline__ bool gridBarrier(SweepBarrier* bar, uint32_t spinLimit) {
+  __shared__ uint32_t sOk;
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    volatile SweepBarrier* vb = bar;
+    const uint32_t gen = vb->generation;
+    __threadfence();
+    const uint32_t before = atomicAdd(&bar->arrived, 1u);
+    if (before == gridDim.x - 1) {
+      bar->arrived = 0u;
+      __threadfence();
+      atomicAdd(&bar->generation, 1u);
+    } else {
+      uint32_t spins = 0;
+      while (vb->generation == gen && vb->error == 0u) {
+        if (++spins > spinLimit) {
+          atomicOr(&bar->error, 1u);
+          break;
+        }
+        __nanosleep(64);
+      }
+    }
+    __threadfence();
+    sOk = vb->error == 0u ? 1u : 0u;
+  }
+  __syncthreads();
+  return sOk != 0u;
+}
+
+template <int W, bool kExt>
+__global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS)
+    coloredSweepKernel(Buffers b, const DevParams* __restrict__ pp, float4* x, const uint32_t* __restrict__ colorVertices,
+                       const uint32_t* __restrict__ colorOffsets, const uint32_t* __restrict__ needVertices,
+                       const uint32_t* __restrict__ needOffsets, uint32_t colorCount, uint32_t V, uint32_t K,
+                       uint32_t groupsPerBlock, int refreshAllFrames, SweepBarrier* bar, uint32_t spinLimit) {
+  for (uint32_t c = 0; c < colorCount; ++c) {
+    // Frames of the vertices this colour reads (every vertex after the
+    // frame's last colour, so the stored frames match a full pass).
+    const bool all = refreshAllFrames && c + 1 == colorCount;
+    const uint32_t nb = needOffsets[c], ne = all ? nb + V : needOffsets[c + 1];
+    for (uint32_t i = nb + blockIdx.x * blockDim.x + threadIdx.x; i < ne; i += gridDim.x * blockDim.x) {
+      const uint32_t v = all ? i - nb : needVertices[i];
+      const uint32_t scene = b.vertexScene[v];
+      const DevParams& p = pp[scene];
+      if (!p.active || latched(p, &b.frames[scene])) continue;
+      storeRot(b.vertexRot, v, vertexFrame(b, x, v, p.rotationEpsilon));
+    }
+    if (!gridBarrier(bar, spinLimit)) return;
+    const uint32_t cb = colorOffsets[c], count = colorOffsets[c + 1] - cb;
+    const uint32_t chunks = (count + groupsPerBlock - 1) / groupsPerBlock;
+    for (uint32_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
+      solveChunk<W, kExt>(b, pp, x, x, colorVertices + cb, count, K, 0, groupsPerBlock, chunk);
+    if (!gridBarrier(bar, spinLimit)) return;
   }
 }
 
@@ -3075,6 +3141,57 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
 
 // Dynamic shared memory a solve block may use (the device's opt-in limit less
 // the kernel's static shared memory); sets the kernels' attribute once.
+int launchColoredSweep(const Buffers& b, const DevParams* p, float4* x, const uint32_t* colorVertices,
+                       const uint32_t* colorOffsets, const uint32_t* needVertices, const uint32_t* needOffsets,
+                       uint32_t colorCount, uint32_t V, uint32_t K, bool refreshAllFrames, void* barrier,
+                       uint32_t spinLimit, cudaStream_t s) {
+  const uint32_t fit = solveGroupsPerBlock(K);
+  if (fit == 0 || colorCount == 0) return 0;
+  const uint32_t groups = std::max(1u, fit >> std::min(b.solveShift, 2u));
+  const size_t smem = static_cast<size_t>(groups) * K * kSolveSlotBytes;
+  constexpr uint32_t perWarp = 32u / kGroup;
+  const uint32_t threads = (groups + perWarp - 1) / perWarp * 32u;
+  const bool ext = b.clothRange || b.contactIdx;
+  const void* fn = ext ? reinterpret_cast<const void*>(coloredSweepKernel<kGroup, true>)
+                       : reinterpret_cast<const void*>(coloredSweepKernel<kGroup, false>);
+  static int attr = -1;
+  if (attr < 0) {
+    attr = static_cast<int>(solveSharedBytes());
+    cudaFuncSetAttribute(coloredSweepKernel<kGroup, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, attr);
+    cudaFuncSetAttribute(coloredSweepKernel<kGroup, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, attr);
+  }
+  int device = 0, sms = 0, perSm = 0;
+  cudaGetDevice(&device);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, static_cast<int>(threads), smem) != cudaSuccess ||
+      perSm <= 0 || sms <= 0)
+    return -1;
+  // A cooperative grid: every block resident, so the barriers can complete.
+  cudaMemsetAsync(barrier, 0, sizeof(SweepBarrier), s);
+  cudaLaunchConfig_t cfg = {};
+  cfg.gridDim = dim3(static_cast<unsigned>(perSm * sms));
+  cfg.blockDim = dim3(threads);
+  cfg.dynamicSmemBytes = smem;
+  cfg.stream = s;
+  cudaLaunchAttribute at[1];
+  at[0].id = cudaLaunchAttributeCooperative;
+  at[0].val.cooperative = 1;
+  cfg.attrs = at;
+  cfg.numAttrs = 1;
+  SweepBarrier* bar = static_cast<SweepBarrier*>(barrier);
+  const int all = refreshAllFrames ? 1 : 0;
+  cudaError_t e;
+  if (ext)
+    e = cudaLaunchKernelEx(&cfg, coloredSweepKernel<kGroup, true>, b, p, x, colorVertices, colorOffsets, needVertices,
+                           needOffsets, colorCount, V, K, groups, all, bar, spinLimit);
+  else
+    e = cudaLaunchKernelEx(&cfg, coloredSweepKernel<kGroup, false>, b, p, x, colorVertices, colorOffsets,
+                           needVertices, needOffsets, colorCount, V, K, groups, all, bar, spinLimit);
+  return e == cudaSuccess ? 2 : -1;
+}
+
+size_t sweepBarrierBytes() { return sizeof(SweepBarrier); }
+
 uint32_t solveSharedBytes() {
   static int optin = -1;
   if (optin < 0) {

@@ -891,6 +891,16 @@ struct Engine {
   DevParams* dParams = nullptr;  // one per scene
   std::vector<DevParams> hParams;
   uint32_t* dColorVertices = nullptr;
+  // The coloured sweep as one persistent kernel: device copies of the colour
+  // and need offsets, its barrier words, and the barrier spin bound
+  // (JGS2_BARRIER_SPIN_LIMIT, polls of about 64 ns).  JGS2_COLOR_SWEEP=launches
+  // keeps the launch-per-colour encoding instead.
+  uint32_t* dColorOffsets = nullptr;
+  uint32_t* dNeedOffsets = nullptr;
+  void* dSweepBarrier = nullptr;
+  uint32_t spinLimit = 1u << 24;
+  bool persistentSweep = true;
+  bool sweepLaunched = false;
   uint32_t* dNeedVertices = nullptr;
   std::vector<void*> allocations;
   uint64_t launches = 0;
@@ -1146,7 +1156,21 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
     }
     if (colored) {
       n += timed(P::kCopy, [&] { return jgs2::launchCopy(b, s->dParams, src, tgt, s->V, st); });
-      for (uint32_t c = 0; c < s->colorCount; ++c) {
+      // One persistent kernel for all colours (no contact candidates; a
+      // contact engine picks its solve variant per colour).
+      int sweep = -1;
+      if (s->persistentSweep && !b.contactIdx && s->dColorOffsets) {
+        sweep = timed(P::kSolve, [&] {
+          return jgs2::launchColoredSweep(b, s->dParams, tgt, s->dColorVertices, s->dColorOffsets, s->dNeedVertices,
+                                          s->dNeedOffsets, s->colorCount, s->V, s->K, last, s->dSweepBarrier,
+                                          s->spinLimit, st);
+        });
+        if (sweep > 0) {
+          n += sweep;
+          s->sweepLaunched = true;
+        }
+      }
+      for (uint32_t c = 0; sweep <= 0 && c < s->colorCount; ++c) {
         const uint32_t nb = s->needOffsets[c], ne = s->needOffsets[c + 1];
         n += timed(P::kVertexFrames, [&] {
           // The final colour of the frame refreshes every frame so the stored
@@ -1370,6 +1394,16 @@ jgs2_status stepCommon(jgs2_solver* s, uint32_t frames, int exactIterations, con
 // After a synchronisation: a broad-phase list that did not fit its capacity
 // (the iteration then listed nothing) fails the call.
 jgs2_status checkBroadPhase(Engine* s) {
+  if (s->sweepLaunched) {
+    // The persistent coloured sweep's error word (a barrier that gave up).
+    uint32_t words[4];
+    CUDA_TRY(s, cudaMemcpy(words, s->dSweepBarrier, sizeof(words), cudaMemcpyDeviceToHost));
+    if (words[2] != 0u)
+      return fail(s, JGS2_TIMEOUT,
+                  format("A grid barrier of the graph-coloured sweep waited longer than its bound of %u polls; the "
+                         "step's result is invalid.",
+                         s->spinLimit));
+  }
   if (!s->dynamic) return JGS2_OK;
   uint32_t status[4];
   CUDA_TRY(s, cudaMemcpy(status, s->b.bpStatus, sizeof(status), cudaMemcpyDeviceToHost));
@@ -1526,6 +1560,8 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   sp->device = device;
   // JGS2_NO_GRAPHS=1 launches each frame's kernels directly (debugging).
   sp->useGraphs = std::getenv("JGS2_NO_GRAPHS") == nullptr;
+  if (const char* e = std::getenv("JGS2_BARRIER_SPIN_LIMIT")) sp->spinLimit = static_cast<uint32_t>(std::strtoul(e, nullptr, 10));
+  if (const char* e = std::getenv("JGS2_COLOR_SWEEP")) sp->persistentSweep = std::string(e) != "launches";
   sp->glob = prep[0].stable;
   for (const PreparedScene& p : prep)
     if (p.stable != sp->glob)
@@ -2111,6 +2147,14 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     }
     STEP(upload(sp, &sp->dColorVertices, byColor.data(), byColor.size()));
     STEP(upload(sp, &sp->dNeedVertices, need.data(), need.size()));
+    STEP(upload(sp, &sp->dColorOffsets, sp->colorOffsets.data(), sp->colorOffsets.size()));
+    STEP(upload(sp, &sp->dNeedOffsets, sp->needOffsets.data(), sp->needOffsets.size()));
+    {
+      uint32_t* bar = nullptr;
+      STEP(deviceAlloc(sp, &bar, (jgs2::sweepBarrierBytes() + 3) / 4));
+      CUDA_TRY(sp, cudaMemsetAsync(bar, 0, jgs2::sweepBarrierBytes(), sp->stream));
+      sp->dSweepBarrier = bar;
+    }
     STEP(deviceAlloc(sp, &sp->dParams, S));
     sp->hParams.resize(S);
     if (!sp->glob) {
@@ -2885,6 +2929,123 @@ jgs2_status jgs2_gate_candidate_no_alloc(jgs2_solver* s, const float* source, co
   if (launched == 0) return fail(s, JGS2_INVALID_ARGUMENT, "The no-allocation gate was given an empty mesh.");
   CUDA_TRY(s, cudaGetLastError());
   s->launches += static_cast<uint64_t>(launched);
+  return JGS2_OK;
+}
+
+// ---- checkpoint / resume ----------------------------------------------------
+// A solver's state between frames, as one self-describing byte image:
+// header, then the per-vertex arrays and the frame record.  The frame start
+// derives everything else (inertial target, frames, incident systems,
+// contact caches and lagged forces) from these, so a solver created from the
+// same input and given this image steps exactly as the exporting one would.
+namespace {
+
+constexpr char kStateMagic[8] = {'J', 'G', 'S', '2', 'S', 'T', 'A', '1'};
+constexpr uint32_t kStateVersion = 1;
+
+struct StateHeader {
+  char magic[8];
+  uint32_t version, V, T, K, KC, C, H;
+  uint32_t objectiveFlags, forceCount, targetCount, objectiveRevision;
+  uint32_t submittedIterations, recordsAvailable;
+  uint64_t bytes;
+  jgs2_settings submitted;
+};
+
+struct StateRegion {
+  void* dev;
+  size_t bytes;
+};
+
+std::vector<StateRegion> stateRegions(Engine* s) {
+  const size_t V = s->V;
+  return {{s->b.pos[0], 16 * V},        {s->b.velocity, 16 * V},  {s->b.old, 16 * V},
+          {s->b.predicted, 16 * V},     {s->b.vertexRot, 48 * V}, {s->b.incident, 48 * V},
+          {s->b.local, 64 * V},         {s->b.finalUpdate, 4 * V}, {s->b.forces, 16 * V},
+          {s->b.targets, 16 * V},       {s->b.frames, sizeof(FrameState)}};
+}
+
+size_t stateBytes(Engine* s) {
+  size_t n = sizeof(StateHeader);
+  for (const StateRegion& r : stateRegions(s)) n += r.bytes;
+  return n;
+}
+
+}  // namespace
+
+jgs2_status jgs2_export_state(jgs2_solver* s, void* out, size_t capacity, size_t* size) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (s->scenes.size() != 1) return fail(s, JGS2_UNSUPPORTED, "State export covers single-scene solvers.");
+  const size_t need = stateBytes(s);
+  if (size) *size = need;
+  if (!out) return JGS2_OK;
+  if (capacity < need) return fail(s, JGS2_INVALID_ARGUMENT, format("The state image needs %zu bytes.", need));
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  st = checkBroadPhase(s);
+  if (st != JGS2_OK) return st;
+  const SceneHost& sc = s->scenes[0];
+  StateHeader h{};
+  std::memcpy(h.magic, kStateMagic, sizeof(kStateMagic));
+  h.version = kStateVersion;
+  h.V = s->V; h.T = s->T; h.K = s->K; h.KC = s->KC; h.C = s->C; h.H = s->H;
+  h.objectiveFlags = sc.objectiveFlags;
+  h.forceCount = sc.forceCount;
+  h.targetCount = sc.targetCount;
+  h.objectiveRevision = sc.objectiveRevision;
+  h.submittedIterations = sc.submittedIterations;
+  h.recordsAvailable = sc.recordsAvailable ? 1u : 0u;
+  h.bytes = need;
+  h.submitted = sc.submitted;
+  unsigned char* p = static_cast<unsigned char*>(out);
+  std::memcpy(p, &h, sizeof(h));
+  p += sizeof(h);
+  for (const StateRegion& r : stateRegions(s)) {
+    CUDA_TRY(s, cudaMemcpyAsync(p, r.dev, r.bytes, cudaMemcpyDeviceToHost, s->stream));
+    p += r.bytes;
+  }
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_import_state(jgs2_solver* s, const void* in, size_t size) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (s->scenes.size() != 1) return fail(s, JGS2_UNSUPPORTED, "State import covers single-scene solvers.");
+  if (!in || size < sizeof(StateHeader)) return fail(s, JGS2_INVALID_ARGUMENT, "The state image is too short.");
+  StateHeader h;
+  std::memcpy(&h, in, sizeof(h));
+  if (std::memcmp(h.magic, kStateMagic, sizeof(kStateMagic)) != 0 || h.version != kStateVersion)
+    return fail(s, JGS2_INVALID_ARGUMENT, "The state image is not a version-1 JGS2 state image.");
+  if (h.V != s->V || h.T != s->T || h.K != s->K || h.KC != s->KC || h.C != s->C || h.H != s->H)
+    return fail(s, JGS2_INVALID_ARGUMENT,
+                format("The state image is of a solver with %u vertices, %u tetrahedra, %u cubature records, %u "
+                       "contact candidates, %u triangles and %u hinges; this solver has %u, %u, %u, %u, %u and %u.",
+                       h.V, h.T, h.K, h.KC, h.C, h.H, s->V, s->T, s->K, s->KC, s->C, s->H));
+  const size_t need = stateBytes(s);
+  if (h.bytes != need || size < need)
+    return fail(s, JGS2_INVALID_ARGUMENT, format("The state image must hold %zu bytes.", need));
+  st = waitObjectiveMirror(s);
+  if (st != JGS2_OK) return st;
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  const unsigned char* p = static_cast<const unsigned char*>(in) + sizeof(h);
+  for (const StateRegion& r : stateRegions(s)) {
+    if (r.dev == s->b.forces) std::memcpy(s->hForces, p, r.bytes);
+    if (r.dev == s->b.targets) std::memcpy(s->hTargets, p, r.bytes);
+    CUDA_TRY(s, cudaMemcpyAsync(r.dev, p, r.bytes, cudaMemcpyHostToDevice, s->stream));
+    p += r.bytes;
+  }
+  CUDA_TRY(s, cudaStreamSynchronize(s->stream));
+  SceneHost& sc = s->scenes[0];
+  sc.objectiveFlags = h.objectiveFlags;
+  sc.forceCount = h.forceCount;
+  sc.targetCount = h.targetCount;
+  sc.objectiveRevision = h.objectiveRevision;
+  sc.submittedIterations = h.submittedIterations;
+  sc.recordsAvailable = h.recordsAvailable != 0;
+  sc.submitted = h.submitted;
   return JGS2_OK;
 }
 

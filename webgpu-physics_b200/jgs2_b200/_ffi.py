@@ -290,6 +290,10 @@ def step_lib() -> ctypes.CDLL:
                                                 POINTER(c_float), POINTER(c_float),
                                                 c_size_t, POINTER(c_uint32)]
         lib.jgs2_device_positions.argtypes = [vp, POINTER(c_void_p), POINTER(c_void_p)]
+        lib.jgs2_export_state.argtypes = [vp, vp, c_size_t, POINTER(c_size_t)]
+        lib.jgs2_import_state.argtypes = [vp, vp, c_size_t]
+        lib.jgs2_evaluate_contact_features.argtypes = [POINTER(c_float), POINTER(c_uint32), c_uint32,
+                                                       POINTER(c_float), POINTER(c_uint32), c_int]
         lib.jgs2_read_contact_candidates.argtypes = [vp, POINTER(c_uint32), c_uint64, POINTER(c_uint64)]
         lib.jgs2_read_oracle_diagnostics.argtypes = [vp, POINTER(OracleDiagnostics), POINTER(c_float), c_size_t,
                                                      POINTER(c_float), c_size_t]

@@ -13,7 +13,7 @@ from __future__ import annotations
 
 import ctypes
 import dataclasses
-from ctypes import byref, c_float, c_uint32, c_void_p
+from ctypes import byref, c_float, c_size_t, c_uint32, c_void_p
 from typing import Optional
 
 import numpy as np
@@ -264,6 +264,22 @@ class JGS2GpuSolver:
     def setLaunchShape(self, shape: int):
         self._usable()
         self._check(getattr(self._L, "jgs2_" + "set_launch_shape")(self._h, int(shape)))
+
+    def exportState(self) -> bytes:
+        """The solver's between-frame state as a byte image (positions,
+        velocities, objectives, frame records); see jgs2_export_state."""
+        self._usable()
+        n = c_size_t(0)
+        self._check(self._L.jgs2_export_state(self._h, None, 0, byref(n)))
+        buf = ctypes.create_string_buffer(n.value)
+        self._check(self._L.jgs2_export_state(self._h, buf, n.value, byref(n)))
+        return buf.raw
+
+    def importState(self, image: bytes):
+        """Restore an image from exportState of a solver over the same input."""
+        self._usable()
+        buf = ctypes.create_string_buffer(bytes(image), len(image))
+        self._check(self._L.jgs2_import_state(self._h, buf, len(image)))
 
     def devicePositions(self):
         """(device pointer, cudaStream_t) of the canonical position array."""
