@@ -207,7 +207,15 @@ __device__ __forceinline__ uint4 hingeIndices(const float4* __restrict__ hinges,
 // k L0 (dtheta/dx)(dtheta/dx)^T: the cloth loops of jgs2Solve
 // (jgs2-shader.ts:3113-3186).  Entries [first, first + count) step `stride`
 // of the vertex's incidence range (lane-split gathers pass their lane).
-template <bool kHessian, class G>
+// A position read of the cloth gathers; kCoherent reads through L2 (see the
+// solve kernel's coherent loads).
+template <bool kCoherent>
+__device__ __forceinline__ float4 clothPos(const float4* x, uint32_t i) {
+  if constexpr (kCoherent) return __ldcg(x + i);
+  else return x[i];
+}
+
+template <bool kHessian, bool kCoherent = false, class G>
 __device__ __forceinline__ void clothLocalSystem(const float4* __restrict__ tris, const float4* __restrict__ hinges,
                                                  const uint32_t* __restrict__ incidence, const uint4& range,
                                                  const float4* __restrict__ x, const ClothMaterial& m,
@@ -216,7 +224,7 @@ __device__ __forceinline__ void clothLocalSystem(const float4* __restrict__ tris
     const uint32_t entry = __ldg(&incidence[range.x + a]);
     const uint32_t slot = entry & 3u;
     const ClothTri t = loadClothTri(tris, entry >> 2);
-    const Membrane e = clothMembrane(t, xyz(x[t.i0]), xyz(x[t.i1]), xyz(x[t.i2]), m);
+    const Membrane e = clothMembrane(t, xyz(clothPos<kCoherent>(x, t.i0)), xyz(clothPos<kCoherent>(x, t.i1)), xyz(clothPos<kCoherent>(x, t.i2)), m);
     gadd(grad, clothMembraneGradient(t, e, slot, m));
     if (kHessian) clothMembraneHessian(hess, t, e, slot, m);
   }
@@ -225,7 +233,8 @@ __device__ __forceinline__ void clothLocalSystem(const float4* __restrict__ tris
     const uint32_t slot = entry & 3u;
     const uint32_t h = entry >> 2;
     const uint4 q = hingeIndices(hinges, h);
-    const DihedralFrame f = clothDihedralFrame(xyz(x[q.x]), xyz(x[q.y]), xyz(x[q.z]), xyz(x[q.w]));
+    const DihedralFrame f = clothDihedralFrame(xyz(clothPos<kCoherent>(x, q.x)), xyz(clothPos<kCoherent>(x, q.y)), xyz(clothPos<kCoherent>(x, q.z)),
+                                                    xyz(clothPos<kCoherent>(x, q.w)));
     const float angle = f.valid ? atan2f(f.sine, f.cosine) : 0.0f;
     const float3 ag = f.valid ? clothDihedralGradient(f, slot) : f3(0, 0, 0);
     if (!f.valid || !finiteS(angle) || !finiteV(ag)) {

@@ -87,6 +87,33 @@ __device__ __forceinline__ M3 loadRot(const float4* __restrict__ rot, uint32_t v
   return {f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z)};
 }
 
+// Reads of arrays that other blocks of the same launch may write (positions
+// and vertex frames inside the persistent coloured sweep): kCoherent loads go
+// to L2 (ld.global.cg), never to the non-coherent read-only path or a stale
+// L1 line.  Other launches read them as ordinary read-only data.
+template <bool kCoherent>
+__device__ __forceinline__ float4 ldPos(const float4* p, size_t i) {
+  if constexpr (kCoherent) return __ldcg(p + i);
+  else return p[i];
+}
+template <bool kCoherent>
+__device__ __forceinline__ M3 loadRotT(const float4* rot, uint32_t v) {
+  if constexpr (kCoherent) {
+    const float4 a = __ldcg(rot + 3ull * v), b = __ldcg(rot + 3ull * v + 1), c = __ldcg(rot + 3ull * v + 2);
+    return {f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z)};
+  } else {
+    return loadRot(rot, v);
+  }
+}
+template <bool kCoherent>
+__device__ __forceinline__ M3 deformationAtT(const TetRec& r, const float4* x) {
+  if constexpr (kCoherent)
+    return deformation(r, xyz(__ldcg(x + r.idx.x)), xyz(__ldcg(x + r.idx.y)), xyz(__ldcg(x + r.idx.z)),
+                       xyz(__ldcg(x + r.idx.w)));
+  else
+    return deformationAt(r, x);
+}
+
 __device__ __forceinline__ void storeRot(float4* __restrict__ rot, uint32_t v, const M3& m) {
   rot[3ull * v] = make_float4(m.c0.x, m.c0.y, m.c0.z, 0.f);
   rot[3ull * v + 1] = make_float4(m.c1.x, m.c1.y, m.c1.z, 0.f);
@@ -330,6 +357,7 @@ __device__ __forceinline__ void frameAndIncident(const Buffers& b, const DevPara
 
 // Vertex frame: polar of the volume-weighted average F over incident tets
 // (vertexPolarRotation, jgs2-shader.ts:2959-2989).
+template <bool kCoherent = false>
 __device__ __forceinline__ M3 vertexFrame(const Buffers& b, const float4* __restrict__ x, uint32_t v, float eps) {
   const uint4 info = b.vinfo[v];
   if (info.y == 0u) return midentity();
@@ -338,7 +366,7 @@ __device__ __forceinline__ M3 vertexFrame(const Buffers& b, const float4* __rest
   for (uint32_t a = 0; a < info.y; ++a) {
     const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
     const TetRec r = loadTet(b.tets, entry >> 2);
-    avg = avg + r.vol * deformationAt(r, x);
+    avg = avg + r.vol * deformationAtT<kCoherent>(r, x);
     total += r.vol;
   }
   avg = total > 0.0f ? (1.0f / total) * avg : midentity();
@@ -1637,7 +1665,7 @@ __device__ __forceinline__ M3 loadBlockVecShared(const float4* rec, int l) {
 // One block's chunk `chunk` of the vertex list: vertices
 // [chunk * groupsPerBlock, (chunk + 1) * groupsPerBlock) of `list` (or of all
 // vertices).  Every thread of the block calls it with the same chunk.
-template <int W, bool kExt>
+template <int W, bool kExt, bool kCoherent = false>
 __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __restrict__ pp,
                                            const float4* __restrict__ src, float4* tgt,
                                            const uint32_t* __restrict__ list, uint32_t count, uint32_t K,
@@ -1701,7 +1729,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
     const uint4 info = b.vinfo[v];
     const float4 rm = b.restMass[v];
     if (isLatched) {
-      if (lane == 0) tgt[v] = src[v];
+      if (lane == 0) tgt[v] = ldPos<kCoherent>(src, v);
     } else if (isPinned(info)) {
       if (lane == 0) {
         tgt[v] = make_float4(rm.x, rm.y, rm.z, 1.0f);
@@ -1719,7 +1747,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
       if (!(amv && c0.z > kDeterminantFloor)) {
         // Preflight rejection before any material evaluation (jgs2-shader.ts:3042-3081).
         if (lane == 0) {
-          tgt[v] = src[v];
+          tgt[v] = ldPos<kCoherent>(src, v);
           b.finalUpdate[v] = 0.0f;
           float4* L = &b.local[4ull * v];
           L[0] = L[1] = L[2] = make_float4(0, 0, 0, 0);
@@ -1729,7 +1757,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
           haveRecord = true;
         }
       } else {
-        const float3 position = xyz(src[v]);
+        const float3 position = xyz(ldPos<kCoherent>(src, v));
         const float3 predV = xyz(b.predicted[v]);
         const float inertia = rm.w * p.invDt2;
         const float dWs = distributedInertiaWeight(rm, info, p.invDt2);
@@ -1745,7 +1773,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
         // B'_l = R_l Ubar_l, so R_s is applied once per record instead of once
         // per basis block.  The exact source block subtracted for a record at
         // the vertex's own slot is formed in the world frame.
-        const M3 Rs = loadRot(b.vertexRot, v);
+        const M3 Rs = loadRotT<kCoherent>(b.vertexRot, v);
         unsigned char* mySlots = slotBase + static_cast<size_t>(group) * K * kSolveSlotBytes;
         // Cubature records first, then (unless cached) the incident tets, in
         // separate loops so the two kinds of item never share a divergent pass.
@@ -1782,18 +1810,18 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
               float3 gQ = f3(0, 0, 0);
               S3 HQ = szero();
               uint32_t slot = 4;
-              const float3 x0 = xyz(src[idx.x]);
+              const float3 x0 = xyz(ldPos<kCoherent>(src, idx.x));
 #pragma unroll
               for (int l = 0; l < 4; ++l) {
                 const uint32_t q = idxAt(idx, l);
                 if (q == v) slot = l;
                 const float3 gl = shapeGradient(r, l);
 #if JGS2_SOLVE_STAGE
-                const M3 B = mm(loadRot(b.vertexRot, q), loadBlockVecShared(U, l));
+                const M3 B = mm(loadRotT<kCoherent>(b.vertexRot, q), loadBlockVecShared(U, l));
 #else
-                const M3 B = mm(loadRot(b.vertexRot, q), loadBlockVec(U, l));
+                const M3 B = mm(loadRotT<kCoherent>(b.vertexRot, q), loadBlockVec(U, l));
 #endif
-                const float3 xl = l == 0 ? x0 : xyz(src[q]);
+                const float3 xl = l == 0 ? x0 : xyz(ldPos<kCoherent>(src, q));
                 if (l > 0) F = F + outer(xl - x0, gl);
                 dF0 = dF0 + outer(B.c0, gl);
                 dF1 = dF1 + outer(B.c1, gl);
@@ -1877,7 +1905,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
             // ---- incident tetrahedron (jgs2-shader.ts:3097-3111) ----
             const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
             const TetRec r = loadTet(b.tets, entry >> 2);
-            const M3 F = deformationAt(r, src);
+            const M3 F = deformationAtT<kCoherent>(r, src);
             const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
             const float3 g = shapeGradient(r, entry & 3u);
             cadd(gsum, r.vol * mv(piola(F, pt), g));
@@ -1885,7 +1913,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
           }
           // ---- cloth membrane and bending (jgs2-shader.ts:3113-3186) ----
           if (kExt && p.cloth)
-            clothLocalSystem<true>(b.clothTris, b.clothHinges, b.clothIncidence, b.clothRange[v], src,
+            clothLocalSystem<true, kCoherent>(b.clothTris, b.clothHinges, b.clothIncidence, b.clothRange[v], src,
                                    clothMaterial(p), lane, W, gsum, hess);
         }
         // ---- IPC contact (jgs2-shader.ts:3193-3195): the cached source
@@ -1988,7 +2016,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
               float J = 0.0f;
               const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
               const TetRec r = loadTet(b.tets, entry >> 2);
-              const M3 F = deformationAt(r, src);
+              const M3 F = deformationAtT<kCoherent>(r, src);
               const float I0 = frob(F, F);
               const float J0 = mdet(F);
               de += r.vol * snhEnergyDelta(F, I0, J0, outer(td, shapeGradient(r, entry & 3u)), r.lambda, r.mu, &J);
@@ -2003,7 +2031,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
               const uint32_t entry = __ldg(&b.clothIncidence[cr.x + a]);
               const uint32_t slot = entry & 3u;
               const ClothTri ct = loadClothTri(b.clothTris, entry >> 2);
-              const float3 x0 = xyz(src[ct.i0]), x1 = xyz(src[ct.i1]), x2 = xyz(src[ct.i2]);
+              const float3 x0 = xyz(ldPos<kCoherent>(src, ct.i0)), x1 = xyz(ldPos<kCoherent>(src, ct.i1)), x2 = xyz(ldPos<kCoherent>(src, ct.i2));
               const float3 y0 = slot == 0u ? trialPos : x0;
               const float3 y1 = slot == 1u ? trialPos : x1;
               const float3 y2 = slot == 2u ? trialPos : x2;
@@ -2020,7 +2048,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
               const uint32_t slot = entry & 3u, h = entry >> 2;
               const uint4 q = hingeIndices(b.clothHinges, h);
               const float4 rest = __ldg(&b.clothHinges[2ull * h + 1]);
-              const float3 x0 = xyz(src[q.x]), x1 = xyz(src[q.y]), x2 = xyz(src[q.z]), x3 = xyz(src[q.w]);
+              const float3 x0 = xyz(ldPos<kCoherent>(src, q.x)), x1 = xyz(ldPos<kCoherent>(src, q.y)), x2 = xyz(ldPos<kCoherent>(src, q.z)), x3 = xyz(ldPos<kCoherent>(src, q.w));
               const float es = clothBendingEnergy(x0, x1, x2, x3, rest, cmat.bending);
               const float et = clothBendingEnergy(slot == 0u ? trialPos : x0, slot == 1u ? trialPos : x1,
                                                   slot == 2u ? trialPos : x2, slot == 3u ? trialPos : x3, rest,
@@ -2209,13 +2237,13 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS)
       const uint32_t scene = b.vertexScene[v];
       const DevParams& p = pp[scene];
       if (!p.active || latched(p, &b.frames[scene])) continue;
-      storeRot(b.vertexRot, v, vertexFrame(b, x, v, p.rotationEpsilon));
+      storeRot(b.vertexRot, v, vertexFrame<true>(b, x, v, p.rotationEpsilon));
     }
     if (!gridBarrier(bar, spinLimit)) return;
     const uint32_t cb = colorOffsets[c], count = colorOffsets[c + 1] - cb;
     const uint32_t chunks = (count + groupsPerBlock - 1) / groupsPerBlock;
     for (uint32_t chunk = blockIdx.x; chunk < chunks; chunk += gridDim.x)
-      solveChunk<W, kExt>(b, pp, x, x, colorVertices + cb, count, K, 0, groupsPerBlock, chunk);
+      solveChunk<W, kExt, true>(b, pp, x, x, colorVertices + cb, count, K, 0, groupsPerBlock, chunk);
     if (!gridBarrier(bar, spinLimit)) return;
   }
 }
