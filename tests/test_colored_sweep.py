@@ -1,6 +1,7 @@
 """The graph-coloured schedule as one persistent kernel per iteration
 (per-colour phases separated by grid barriers, jgs2-solver.ts:2275-2325)
-against the launch-per-colour encoding, and the bounded barrier: with a spin
+against the launch-per-colour encoding (equal to f32 rounding, replayed bit for
+bit), and the bounded barrier: with a spin
 bound of zero polls a waiting block gives up at once, every block leaves the
 kernel, and the host reports JGS2_TIMEOUT at its next synchronisation while
 the device stays usable."""
@@ -28,23 +29,31 @@ def _with_env(name, value, fn):
             os.environ[name] = old
 
 
-def test_persistent_sweep_equals_per_colour_launches():
+def test_persistent_sweep_matches_per_colour_launches():
+    # The same arithmetic in another kernel: the compiler may fuse a few
+    # multiply-adds differently, so the encodings agree to f32 rounding (and
+    # take the same accept / revert decisions), and the persistent sweep
+    # replays bit for bit.
     inp = scenes.unit_cube(cells=12)
     a = solver.JGS2GpuSolver.create(inp, SETTINGS)
+    a2 = solver.JGS2GpuSolver.create(inp, SETTINGS)
     b = _with_env("JGS2_COLOR_SWEEP", "launches", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS))
     assert a.scheduleColorCount > 1
+    diag = inp.bbox_diagonal()
     for frame in range(3):
         la, lb = a.kernelLaunchCount(), b.kernelLaunchCount()
-        a.stepExactIterations(6)
-        b.stepExactIterations(6)
-        np.testing.assert_array_equal(a.readPositions(), b.readPositions(), err_msg=f"frame {frame}")
-        np.testing.assert_array_equal(a.readGlobalizationDiagnostics()["history"],
-                                      b.readGlobalizationDiagnostics()["history"])
+        for s in (a, a2, b):
+            s.stepExactIterations(6)
+        np.testing.assert_array_equal(a.readPositions(), a2.readPositions(), err_msg=f"replay, frame {frame}")
+        err = np.abs(a.readPositions() - b.readPositions()).max() / diag
+        assert err <= 1e-5, (frame, err)
+        np.testing.assert_array_equal(a.readGlobalizationDiagnostics()["history"][:, 4],
+                                      b.readGlobalizationDiagnostics()["history"][:, 4])
         # One sweep (a barrier reset and a kernel) per iteration instead of two
         # launches per colour.
         assert a.kernelLaunchCount() - la < b.kernelLaunchCount() - lb
-    a.destroy()
-    b.destroy()
+    for s in (a, a2, b):
+        s.destroy()
 
 
 def test_barrier_timeout_is_reported_and_the_device_stays_usable():
