@@ -2211,7 +2211,7 @@ __device__ __forceinline__ bool gridBarrier(SweepBarrier* bar, uint32_t spinLimi
           atomicOr(&bar->error, 1u);
           break;
         }
-        __nanosleep(64);
+        __nanosleep(32);
       }
     }
     __threadfence();
@@ -3171,8 +3171,8 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
 // the kernel's static shared memory); sets the kernels' attribute once.
 int launchColoredSweep(const Buffers& b, const DevParams* p, float4* x, const uint32_t* colorVertices,
                        const uint32_t* colorOffsets, const uint32_t* needVertices, const uint32_t* needOffsets,
-                       uint32_t colorCount, uint32_t V, uint32_t K, bool refreshAllFrames, void* barrier,
-                       uint32_t spinLimit, cudaStream_t s) {
+                       uint32_t colorCount, uint32_t V, uint32_t K, uint32_t largestColor, uint32_t largestNeed,
+                       bool refreshAllFrames, void* barrier, uint32_t spinLimit, cudaStream_t s) {
   const uint32_t fit = solveGroupsPerBlock(K);
   if (fit == 0 || colorCount == 0) return 0;
   const uint32_t groups = std::max(1u, fit >> std::min(b.solveShift, 2u));
@@ -3194,10 +3194,18 @@ int launchColoredSweep(const Buffers& b, const DevParams* p, float4* x, const ui
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&perSm, fn, static_cast<int>(threads), smem) != cudaSuccess ||
       perSm <= 0 || sms <= 0)
     return -1;
+  // As many blocks as the widest phase can use: every colour's solves in one
+  // wave of chunks (else the launch-per-colour encoding is the better one),
+  // the frames spread at one vertex per thread.
+  const uint32_t capacity = static_cast<uint32_t>(perSm * sms);
+  const uint32_t chunks = (largestColor + groups - 1) / groups;
+  if (chunks > capacity) return -1;
+  const uint32_t frameBlocks = (std::max(largestNeed, refreshAllFrames ? V : 0u) + threads - 1) / threads;
+  const uint32_t grid = std::max(1u, std::min(capacity, std::max(chunks, frameBlocks)));
   // A cooperative grid: every block resident, so the barriers can complete.
   cudaMemsetAsync(barrier, 0, sizeof(SweepBarrier), s);
   cudaLaunchConfig_t cfg = {};
-  cfg.gridDim = dim3(static_cast<unsigned>(perSm * sms));
+  cfg.gridDim = dim3(grid);
   cfg.blockDim = dim3(threads);
   cfg.dynamicSmemBytes = smem;
   cfg.stream = s;

@@ -207,12 +207,13 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
 // kernel (per colour: the frames it reads, a grid barrier, its in-place
 // solves, a grid barrier), after a memset of the barrier words.  Barriers
 // give up after spinLimit polls and set the word the host checks.  Returns
-// the kernels launched (memset and sweep), or -1 when the device cannot run
-// the grid cooperatively (the caller then launches colour by colour).
+// the kernels launched (memset and sweep), or -1 when the largest colour
+// needs more than one wave of resident blocks or the device cannot run the
+// grid cooperatively (the caller then launches colour by colour).
 int launchColoredSweep(const Buffers& b, const DevParams* p, float4* x, const uint32_t* colorVertices,
                        const uint32_t* colorOffsets, const uint32_t* needVertices, const uint32_t* needOffsets,
-                       uint32_t colorCount, uint32_t V, uint32_t K, bool refreshAllFrames, void* barrier,
-                       uint32_t spinLimit, cudaStream_t s);
+                       uint32_t colorCount, uint32_t V, uint32_t K, uint32_t largestColor, uint32_t largestNeed,
+                       bool refreshAllFrames, void* barrier, uint32_t spinLimit, cudaStream_t s);
 // Bytes of the sweep's barrier words (arrived, generation, error word).
 size_t sweepBarrierBytes();
 // Co-rotated path: tet frames and the regularised per-vertex solve.

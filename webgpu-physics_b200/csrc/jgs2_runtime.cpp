@@ -1161,9 +1161,14 @@ int encodeFrame(Engine* s, uint32_t iterations, uint32_t schedule, bool bodyCorr
       int sweep = -1;
       if (s->persistentSweep && !b.contactIdx && s->dColorOffsets) {
         sweep = timed(P::kSolve, [&] {
+          uint32_t largestColor = 0, largestNeed = 0;
+          for (uint32_t c = 0; c < s->colorCount; ++c) {
+            largestColor = std::max(largestColor, s->colorOffsets[c + 1] - s->colorOffsets[c]);
+            largestNeed = std::max(largestNeed, s->needOffsets[c + 1] - s->needOffsets[c]);
+          }
           return jgs2::launchColoredSweep(b, s->dParams, tgt, s->dColorVertices, s->dColorOffsets, s->dNeedVertices,
-                                          s->dNeedOffsets, s->colorCount, s->V, s->K, last, s->dSweepBarrier,
-                                          s->spinLimit, st);
+                                          s->dNeedOffsets, s->colorCount, s->V, s->K, largestColor, largestNeed, last,
+                                          s->dSweepBarrier, s->spinLimit, st);
         });
         if (sweep > 0) {
           n += sweep;
