@@ -207,11 +207,11 @@ __device__ __forceinline__ uint4 hingeIndices(const float4* __restrict__ hinges,
 // k L0 (dtheta/dx)(dtheta/dx)^T: the cloth loops of jgs2Solve
 // (jgs2-shader.ts:3113-3186).  Entries [first, first + count) step `stride`
 // of the vertex's incidence range (lane-split gathers pass their lane).
-// A position read of the cloth gathers; kCoherent reads through L2 (see the
-// solve kernel's coherent loads).
+// A position read of the cloth gathers; kCoherent reads with a weak load that
+// fences order (see the solve kernel's coherent loads).
 template <bool kCoherent>
 __device__ __forceinline__ float4 clothPos(const float4* x, uint32_t i) {
-  if constexpr (kCoherent) return __ldcg(x + i);
+  if constexpr (kCoherent) return __ldca(x + i);
   else return x[i];
 }
 

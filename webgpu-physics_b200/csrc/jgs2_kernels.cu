@@ -88,18 +88,21 @@ __device__ __forceinline__ M3 loadRot(const float4* __restrict__ rot, uint32_t v
 }
 
 // Reads of arrays that other blocks of the same launch may write (positions
-// and vertex frames inside the persistent coloured sweep): kCoherent loads go
-// to L2 (ld.global.cg), never to the non-coherent read-only path or a stale
-// L1 line.  Other launches read them as ordinary read-only data.
+// and vertex frames inside the persistent coloured sweep): kCoherent loads are
+// ordinary weak loads (ld.global.ca), which the grid barrier's release and
+// acquire fences order after the other blocks' writes; they never take the
+// non-coherent read-only path (ld.global.nc), which a const __restrict__
+// pointer may select and which no fence orders.  Other launches read these
+// arrays as read-only data.
 template <bool kCoherent>
 __device__ __forceinline__ float4 ldPos(const float4* p, size_t i) {
-  if constexpr (kCoherent) return __ldcg(p + i);
+  if constexpr (kCoherent) return __ldca(p + i);
   else return p[i];
 }
 template <bool kCoherent>
 __device__ __forceinline__ M3 loadRotT(const float4* rot, uint32_t v) {
   if constexpr (kCoherent) {
-    const float4 a = __ldcg(rot + 3ull * v), b = __ldcg(rot + 3ull * v + 1), c = __ldcg(rot + 3ull * v + 2);
+    const float4 a = __ldca(rot + 3ull * v), b = __ldca(rot + 3ull * v + 1), c = __ldca(rot + 3ull * v + 2);
     return {f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z)};
   } else {
     return loadRot(rot, v);
@@ -108,8 +111,8 @@ __device__ __forceinline__ M3 loadRotT(const float4* rot, uint32_t v) {
 template <bool kCoherent>
 __device__ __forceinline__ M3 deformationAtT(const TetRec& r, const float4* x) {
   if constexpr (kCoherent)
-    return deformation(r, xyz(__ldcg(x + r.idx.x)), xyz(__ldcg(x + r.idx.y)), xyz(__ldcg(x + r.idx.z)),
-                       xyz(__ldcg(x + r.idx.w)));
+    return deformation(r, xyz(__ldca(x + r.idx.x)), xyz(__ldca(x + r.idx.y)), xyz(__ldca(x + r.idx.z)),
+                       xyz(__ldca(x + r.idx.w)));
   else
     return deformationAt(r, x);
 }
