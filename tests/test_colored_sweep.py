@@ -1,4 +1,5 @@
 """The graph-coloured schedule as one persistent kernel per iteration
+(JGS2_COLOR_SWEEP=persistent)
 (per-colour phases separated by grid barriers, jgs2-solver.ts:2275-2325)
 against the launch-per-colour encoding (equal to f32 rounding, replayed bit for
 bit), and the bounded barrier: with a spin
@@ -35,9 +36,9 @@ def test_persistent_sweep_matches_per_colour_launches():
     # take the same accept / revert decisions), and the persistent sweep
     # replays bit for bit.
     inp = scenes.unit_cube(cells=12)
-    a = solver.JGS2GpuSolver.create(inp, SETTINGS)
-    a2 = solver.JGS2GpuSolver.create(inp, SETTINGS)
-    b = _with_env("JGS2_COLOR_SWEEP", "launches", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS))
+    a = _with_env("JGS2_COLOR_SWEEP", "persistent", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS))
+    a2 = _with_env("JGS2_COLOR_SWEEP", "persistent", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS))
+    b = solver.JGS2GpuSolver.create(inp, SETTINGS)
     assert a.scheduleColorCount > 1
     diag = inp.bbox_diagonal()
     for frame in range(3):
@@ -62,7 +63,8 @@ def test_persistent_sweep_matches_per_colour_launches():
 
 def test_barrier_timeout_is_reported_and_the_device_stays_usable():
     inp = scenes.unit_cube(cells=12)
-    s = _with_env("JGS2_BARRIER_SPIN_LIMIT", "0", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS))
+    s = _with_env("JGS2_COLOR_SWEEP", "persistent",
+                  lambda: _with_env("JGS2_BARRIER_SPIN_LIMIT", "0", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS)))
     s.stepExactIterations(2)
     with pytest.raises(_ffi.JGS2Error) as err:
         s.readPositions()
@@ -70,7 +72,7 @@ def test_barrier_timeout_is_reported_and_the_device_stays_usable():
     assert "grid barrier" in err.value.message
     s.destroy()
     # The context survived: a fresh solver steps and reads normally.
-    t = solver.JGS2GpuSolver.create(inp, SETTINGS)
+    t = _with_env("JGS2_COLOR_SWEEP", "persistent", lambda: solver.JGS2GpuSolver.create(inp, SETTINGS))
     t.stepExactIterations(2)
     assert np.isfinite(t.readPositions()).all()
     t.destroy()
