@@ -221,6 +221,23 @@ __device__ __forceinline__ float snhEnergyDelta(const M3& f0, float I0, float J0
   return 0.5f * mu * id - 0.75f * mu * dj + 0.5f * lambda * dj * (J1 + J0 - 2.0f) - 0.5f * mu * lr;
 }
 
+#ifndef JGS2_LS_RANK1
+#define JGS2_LS_RANK1 1
+#endif
+// snhEnergyDelta for a rank-one step D = d g^T (one vertex of a tet moving):
+// <D, 2 F0 + D> = 2 d.(F0 g) + |d|^2 |g|^2 and det(F0 + D) - det(F0) =
+// d.(cof(F0) g) exactly (the determinant is affine in a rank-one update), so
+// the general trilinear expansion is not needed.  J1 is still det(F0 + D).
+__device__ __forceinline__ float snhEnergyDeltaRankOne(const M3& f0, float I0, float J0, float3 d, float3 g,
+                                                       float lambda, float mu, float* Jtrial) {
+  const float id = 2.0f * dot3(d, mv(f0, g)) + dot3(d, d) * dot3(g, g);
+  const float dj = dot3(d, mv(cofactor(f0), g));
+  const float J1 = mdet(f0 + outer(d, g));
+  *Jtrial = J1;
+  const float lr = logOnePlus(id / (I0 + 1.0f));
+  return 0.5f * mu * id - 0.75f * mu * dj + 0.5f * lambda * dj * (J1 + J0 - 2.0f) - 0.5f * mu * lr;
+}
+
 // ---- globalization solve (jgs2-globalization-wgsl.ts:166-492) -----------------
 __device__ __forceinline__ float minSymmetricEigenvalue(const S3& m) {
   const float a00 = m.xx, a11 = m.yy, a22 = m.zz, a01 = m.xy, a02 = m.xz, a12 = m.yz;

@@ -1696,6 +1696,8 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
     // headers have landed) the tetrahedron records they name.
     RecSlot* slots = reinterpret_cast<RecSlot*>(slotBase);
     const uint32_t nrec = groupsPerBlock * K;
+    // Sixteen-byte chunks in address order: a record's two header chunks and
+    // nine basis chunks are consecutive, so a warp's copies are coalesced.
     for (uint32_t c = threadIdx.x; c < nrec * 11u; c += blockDim.x) {
       const uint32_t r = c / 11u, part = c - r * 11u;
       const uint32_t g = r / K, it = chunk * groupsPerBlock + g;
@@ -2022,7 +2024,11 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
               const M3 F = deformationAtT<kCoherent>(r, src);
               const float I0 = frob(F, F);
               const float J0 = mdet(F);
+#if JGS2_LS_RANK1
+              de += r.vol * snhEnergyDeltaRankOne(F, I0, J0, td, shapeGradient(r, entry & 3u), r.lambda, r.mu, &J);
+#else
               de += r.vol * snhEnergyDelta(F, I0, J0, outer(td, shapeGradient(r, entry & 3u)), r.lambda, r.mu, &J);
+#endif
               if (!finiteS(J)) geomFinite = false;
               jmin = fminf(jmin, J);
             }
