@@ -393,6 +393,9 @@ def batched_arm(args):
     for s in plain:
         s.destroy()
     plain_value = whole_job_rate(world, active * iters * plain_steps, plain_s)
+    err64 = None
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        err64 = batched_fp64_error(parts, settings, iters, device)
     algorithmic = sum(algorithmic_bytes(p) for p in parts) * iters
     peak, peak_kind = peaks()
     achieved = algorithmic / (ms / args.steps / 1e3) / 1e9
@@ -416,6 +419,7 @@ def batched_arm(args):
                                  "tuning_frame_ms": [round(m, 3) for m in shape["frameMs"]]},
                 "parallelism": "replicas" if world > 1 else "single GPU"},
             "frames_per_s": world * len(parts) * 1e3 * args.steps / ms,
+            "error_vs_fp64": err64,
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": None,
@@ -437,6 +441,40 @@ def batched_arm(args):
         dist.barrier()
         dist.destroy_process_group()
     return 0
+
+
+def batched_fp64_error(parts, settings, iters, device, samples=16):
+    """The checker on the batched workload: the first frame of every
+    len(parts)/samples-th scene stepped by the GPU (a scene steps bitwise the
+    same alone and in a batch) against the oracle's FP64 run of the same
+    method; the largest position error over the scene's bounding-box
+    diagonal."""
+    import numpy as np
+
+    from jgs2_b200 import solver
+
+    sys.path.insert(0, ROOT)
+    from oracle import oracle as O
+
+    pick = parts[::max(1, len(parts) // samples)][:samples]
+    t0 = time.perf_counter()
+    worst, accepted = 0.0, []
+    for p in pick:
+        g = solver.JGS2GpuSolver.create(p, settings, device=device)
+        g.stepExactIterations(iters)
+        gp = g.readPositions().reshape(-1, 4)[:, :3].astype(np.float64)
+        accepted.append(int(g.readGlobalizationDiagnostics()["history"][:, 4].sum()))
+        g.destroy()
+        o = O.OracleSolver(p, {"timestep": settings["timestep"]}, precision=64)
+        o.step_exact_iterations(iters)
+        op = o.read("positions").reshape(-1, 4)[:, :3].astype(np.float64)
+        worst = max(worst, float(np.abs(gp - op).max()) / p.bbox_diagonal())
+    return {"value": worst, "bound": 1e-4, "unit": "max position error / bbox diagonal of the scene",
+            "frames": 1, "iterations": iters, "scenes": len(pick),
+            "sample": f"every {max(1, len(parts) // samples)}th scene of {len(parts)}",
+            "accepted_iterations_gpu": accepted,
+            "oracle": f"FP64 run of the same method on {O.max_threads()} host threads "
+                      f"({time.perf_counter() - t0:.1f} s)"}
 
 
 def serving_arm(args):
