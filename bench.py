@@ -709,22 +709,33 @@ def ours_arm(args):
                 "kernel_ms_per_frame": {k: v[1] / max(1, min(args.steps, 3)) for k, v in prof.items() if v[0]}}
 
     # ---- end-to-end through the public API ------------------------------------
+    # Each frame: the host uploads its forces (pinned), submits the step and
+    # an asynchronous read of the positions into one of two pinned buffers
+    # (the reference's readPositions is a Promise), so the host's next frame
+    # overlaps the device's work; the run ends when the last read lands.
     V = inp.vertex_count
     forces_host = torch.zeros(3 * V, dtype=torch.float32).pin_memory()
-    pos_host = torch.empty(4 * V, dtype=torch.float32).pin_memory()
+    pos_host = [torch.empty(4 * V, dtype=torch.float32).pin_memory() for _ in range(2)]
     f_np = forces_host.numpy()
-    p_np = pos_host.numpy()
+    p_np = [t.numpy() for t in pos_host]
     e2e_steps = max(1, min(args.steps, 5))
     torch.cuda.synchronize(device)
     lat = []
     t_e2e = time.perf_counter()
-    for _ in range(e2e_steps):
+    for i in range(e2e_steps):
         t0 = time.perf_counter()
         s.replaceExternalForces(f_np)
         s.stepExactIterations(iters)
-        s.readPositions(out=p_np)
+        s.readPositionsAsync(p_np[i % 2])
         lat.append(time.perf_counter() - t0)
+    s.awaitReads()
     e2e_total = max_over_ranks(dist, time.perf_counter() - t_e2e, f"cuda:{device}")
+    # Latency of one frame alone: upload, step, read, wait.
+    t0 = time.perf_counter()
+    s.replaceExternalForces(f_np)
+    s.stepExactIterations(iters)
+    s.readPositions(out=p_np[0])
+    single_ms = 1e3 * (time.perf_counter() - t0)
     e2e_value = whole_job_rate(world, active * iters * e2e_steps, e2e_total)
 
     cpu = None
@@ -751,8 +762,9 @@ def ours_arm(args):
             "roofline": roofline,
             "cpu_baseline": cpu,
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(forces_host.numel() * 4),
-                    "d2h_bytes_per_step": int(pos_host.numel() * 4),
-                    "p50_ms": 1e3 * statistics.median(lat), "steps": e2e_steps},
+                    "d2h_bytes_per_step": int(pos_host[0].numel() * 4),
+                    "frame_latency_ms": single_ms, "steps": e2e_steps,
+                    "pipelining": "asynchronous position reads into two pinned buffers"},
             "clocks": clocks.summary(),
         }
         print(json.dumps(line), flush=True)

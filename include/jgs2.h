@@ -381,6 +381,17 @@ jgs2_status jgs2_release_all_quadratic_targets(jgs2_solver* solver);
 
 /* readPositions (:2501-2508); out has 4 * V floats. */
 jgs2_status jgs2_read_positions(jgs2_solver* solver, float* out, size_t floats);
+/* readPositions as the reference uses it (an asynchronous read resolved
+ * later, :2501-2508 returns a Promise): enqueues the copy of the positions
+ * after the work already submitted on the solver's stream and returns at
+ * once.  `out` (4 * V floats; page-locked memory for a truly asynchronous
+ * copy) must stay valid and unread until jgs2_wait_reads returns; later
+ * steps may be submitted meanwhile, so the host's next frame overlaps the
+ * copy and the device's work. */
+jgs2_status jgs2_read_positions_async(jgs2_solver* solver, float* out, size_t floats);
+/* Waits for every asynchronous read submitted so far (and reports a device
+ * failure of the work before them, like any synchronising call). */
+jgs2_status jgs2_wait_reads(jgs2_solver* solver);
 /* readVelocities (:2510-2518). */
 jgs2_status jgs2_read_velocities(jgs2_solver* solver, float* out, size_t floats);
 /* readPredictedPositions (:2520-2528). */

@@ -72,3 +72,27 @@ def test_import_refuses_another_solver_shape():
         a.importState(bytes(bad))
     a.destroy()
     b.destroy()
+
+
+def test_asynchronous_position_reads():
+    # The reference's readPositions resolves later; jgs2_read_positions_async
+    # enqueues the copy after the submitted frames and jgs2_wait_reads waits.
+    import torch
+
+    inp = scenes.cantilever(cells=(10, 2, 2), size=(0.5, 0.1, 0.1))
+    settings = dict(timestep=1 / 60, iterations=9)
+    a = solver.JGS2GpuSolver.create(inp, settings)
+    b = solver.JGS2GpuSolver.create(inp, settings)
+    bufs = [torch.full((4 * inp.vertex_count,), float("nan"), dtype=torch.float32).pin_memory().numpy()
+            for _ in range(2)]
+    expect = []
+    for i in range(2):
+        a.step()
+        a.readPositionsAsync(bufs[i])
+        b.step()
+        expect.append(b.readPositions())
+    a.awaitReads()
+    for got, want in zip(bufs, expect):
+        np.testing.assert_array_equal(got, want)
+    a.destroy()
+    b.destroy()

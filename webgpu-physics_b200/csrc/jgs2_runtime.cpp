@@ -884,6 +884,7 @@ struct Engine {
   float4* hForces = nullptr;
   float4* hTargets = nullptr;
   cudaEvent_t objectiveUpload = nullptr;  // recorded after the last upload
+  cudaEvent_t readDone = nullptr;         // recorded after the last asynchronous read
   bool objectiveUploadPending = false;
   std::vector<uint8_t> pinned;
   // device
@@ -992,6 +993,7 @@ void releaseDevice(Engine* s) {
   for (cudaEvent_t& e : s->tuneEvents)
     if (e) { cudaEventDestroy(e); e = nullptr; }
   if (s->objectiveUpload) cudaEventDestroy(s->objectiveUpload);
+  if (s->readDone) cudaEventDestroy(s->readDone);
   s->objectiveUpload = nullptr;
   if (s->stream) cudaStreamDestroy(s->stream);
   s->stream = nullptr;
@@ -2018,6 +2020,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
     CUDA_TRY(sp, cudaMallocHost(reinterpret_cast<void**>(&sp->hForces), sizeof(float4) * std::max<size_t>(1, nV)));
     CUDA_TRY(sp, cudaMallocHost(reinterpret_cast<void**>(&sp->hTargets), sizeof(float4) * std::max<size_t>(1, nV)));
     CUDA_TRY(sp, cudaEventCreateWithFlags(&sp->objectiveUpload, cudaEventDisableTiming));
+    CUDA_TRY(sp, cudaEventCreateWithFlags(&sp->readDone, cudaEventDisableTiming));
     std::memcpy(sp->hForces, initialForces.data(), sizeof(float4) * nV);
     std::memcpy(sp->hTargets, initialTargets.data(), sizeof(float4) * nV);
     CUDA_TRY(sp, cudaMemcpyAsync(df, sp->hForces, sizeof(float4) * nV, cudaMemcpyHostToDevice, sp->stream));
@@ -2767,6 +2770,24 @@ jgs2_status jgs2_release_all_quadratic_targets(jgs2_solver* s) {
 jgs2_status jgs2_read_positions(jgs2_solver* s, float* out, size_t floats) {
   if (usable(s) != JGS2_OK) return usable(s);
   return readSceneVec4(s, 0, s->b.pos[0], out, floats, 4);
+}
+
+jgs2_status jgs2_read_positions_async(jgs2_solver* s, float* out, size_t floats) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  if (!out || floats < 4ull * s->V) return fail(s, JGS2_INVALID_ARGUMENT, format("output needs %u floats.", 4 * s->V));
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaMemcpyAsync(out, s->b.pos[0], sizeof(float4) * s->V, cudaMemcpyDeviceToHost, s->stream));
+  CUDA_TRY(s, cudaEventRecord(s->readDone, s->stream));
+  return JGS2_OK;
+}
+
+jgs2_status jgs2_wait_reads(jgs2_solver* s) {
+  jgs2_status st = usable(s);
+  if (st != JGS2_OK) return st;
+  CUDA_TRY(s, cudaSetDevice(s->device));
+  CUDA_TRY(s, cudaEventSynchronize(s->readDone));
+  return checkBroadPhase(s);
 }
 
 jgs2_status jgs2_read_velocities(jgs2_solver* s, float* out, size_t floats) {

@@ -291,6 +291,8 @@ def step_lib() -> ctypes.CDLL:
                                                 c_size_t, POINTER(c_uint32)]
         lib.jgs2_device_positions.argtypes = [vp, POINTER(c_void_p), POINTER(c_void_p)]
         lib.jgs2_export_state.argtypes = [vp, vp, c_size_t, POINTER(c_size_t)]
+        lib.jgs2_read_positions_async.argtypes = [vp, POINTER(c_float), c_size_t]
+        lib.jgs2_wait_reads.argtypes = [vp]
         lib.jgs2_import_state.argtypes = [vp, vp, c_size_t]
         lib.jgs2_evaluate_contact_features.argtypes = [POINTER(c_float), POINTER(c_uint32), c_uint32,
                                                        POINTER(c_float), POINTER(c_uint32), c_int]

@@ -441,6 +441,21 @@ class JGS2GpuSolver:
         self._check(self._L.jgs2_read_positions(self._h, _ffi.fptr(out), out.size))
         return out
 
+    def readPositionsAsync(self, out: np.ndarray) -> np.ndarray:
+        """Enqueue a read of the positions into `out` (contiguous float32,
+        4 floats per vertex, ideally page-locked) after the submitted work
+        and return at once; `out` holds the positions after awaitReads()."""
+        self._usable()
+        if out.dtype != np.float32 or not out.flags.c_contiguous or out.size < 4 * self.vertexCount:
+            raise JGS2RangeError(1, "out must be a contiguous float32 array with 4 floats per vertex.")
+        self._check(self._L.jgs2_read_positions_async(self._h, _ffi.fptr(out), out.size))
+        return out
+
+    def awaitReads(self):
+        """Wait for every asynchronous read submitted so far."""
+        self._usable()
+        self._check(self._L.jgs2_wait_reads(self._h))
+
     def readVelocities(self) -> np.ndarray:
         return self._read(self._L.jgs2_read_velocities, 4)
 
