@@ -1622,6 +1622,12 @@ struct RecSlot {
   float4 tet[4];   // [g1 vol] [g2 lambda] [g3 mu] [indices]
 };
 static_assert(sizeof(CubState) <= sizeof(RecSlot), "record state must fit its staging slot");
+// Records per vertex up to this many bytes of cached state are cached in
+// shared memory (K <= 68 with staging); wider ones are recomputed per trial.
+#ifndef JGS2_SOLVE_CACHE_BYTES
+#define JGS2_SOLVE_CACHE_BYTES 16384
+#endif
+constexpr size_t kSolveCacheBytesPerVertex = JGS2_SOLVE_CACHE_BYTES;
 #if JGS2_SOLVE_STAGE
 constexpr size_t kSolveSlotBytes = sizeof(RecSlot);
 #else
@@ -1665,10 +1671,86 @@ __device__ __forceinline__ M3 loadBlockVecShared(const float4* rec, int l) {
 
 // kExt: some scene of the engine has cloth or contact candidates (their
 // gathers and line search terms are compiled out otherwise).
+// State of cubature record `rec` of vertex v (jgs2-shader.ts:3197-3263), all
+// in the source vertex's frame: the record tet's deformation gradient F and
+// its invariants, the projected directions dF_c = sum_l B'_l[:,c] g_l^T with
+// B'_l = R_l Ubar_l, the inertia / objective quadratic (gQ, HQ), the weight,
+// the tet's material and, when v is one of the tet's vertices, its slot and
+// shape gradient.  Read from the block's staged slot or from global memory;
+// st.w = 0 for an empty record.  `r` receives the record's tet.
+template <bool kCoherent, bool kStaged>
+__device__ __forceinline__ void recordState(const Buffers& b, const DevParams& p, uint32_t v, size_t rec,
+                                            const RecSlot* staged, const float4* __restrict__ src, bool objActive,
+                                            CubState& st, TetRec& r) {
+  uint4 head, idx;
+  if constexpr (kStaged) {
+    head = staged->head[0];
+    idx = staged->head[1];
+  } else {
+    head = __ldg(&b.cubHead[2 * rec]);
+    idx = __ldg(&b.cubHead[2 * rec + 1]);
+  }
+  const uint32_t t = head.x;
+  const float w = __uint_as_float(head.y);
+  st.w = 0.0f;
+  // Headers hold global tet ids; out-of-range records were emptied at create.
+  if (!(t != kEmptyTet && w > 0.0f)) return;
+  const float4* U;
+  if constexpr (kStaged) {
+    r = tetFromSlot(staged->tet);
+    U = staged->basis;
+  } else {
+    r = loadTet(b.tets, t);
+    U = b.cubBasis + 9ull * rec;
+  }
+  M3 F = mzero(), dF0 = mzero(), dF1 = mzero(), dF2 = mzero();
+  float3 gQ = f3(0, 0, 0);
+  S3 HQ = szero();
+  uint32_t slot = 4;
+  const float3 x0 = xyz(ldPos<kCoherent>(src, idx.x));
+#pragma unroll
+  for (int l = 0; l < 4; ++l) {
+    const uint32_t q = idxAt(idx, l);
+    if (q == v) slot = l;
+    const float3 gl = shapeGradient(r, l);
+    M3 B;
+    if constexpr (kStaged) B = mm(loadRotT<kCoherent>(b.vertexRot, q), loadBlockVecShared(U, l));
+    else B = mm(loadRotT<kCoherent>(b.vertexRot, q), loadBlockVec(U, l));
+    const float3 xl = l == 0 ? x0 : xyz(ldPos<kCoherent>(src, q));
+    if (l > 0) F = F + outer(xl - x0, gl);
+    dF0 = dF0 + outer(B.c0, gl);
+    dF1 = dF1 + outer(B.c1, gl);
+    dF2 = dF2 + outer(B.c2, gl);
+    // predicted w = distributed inertia weight (0 when pinned).
+    const float4 pq = b.predicted[q];
+    const float dW = pq.w;
+    float3 lin = dW * (xl - xyz(pq));
+    float quad = dW;
+    const uint4 qi = objActive ? b.vinfo[q] : make_uint4(0u, 0u, 1u, 0u);
+    if (objActive && !isPinned(qi)) {
+      const float nq = float(qi.y > 1u ? qi.y : 1u);
+      lin = lin + objectiveGradient(p, b, q, xl) * (1.0f / nq);
+      quad += targetStiffness(p, b, q) / nq;
+    }
+    gQ = gQ + mtv(B, lin);
+    saddScaled(HQ, quad, gramColumns(B));
+  }
+  st.F = F;
+  st.I0 = frob(F, F);
+  st.J0 = mdet(F);
+  st.dF0 = dF0; st.dF1 = dF1; st.dF2 = dF2;
+  st.gQ = gQ;
+  st.HQ = HQ;
+  st.w = w;
+  st.vol = r.vol; st.lambda = r.lambda; st.mu = r.mu;
+  st.slot = slot;
+  st.gs = slot < 4 ? shapeGradient(r, slot) : f3(0, 0, 0);
+}
+
 // One block's chunk `chunk` of the vertex list: vertices
 // [chunk * groupsPerBlock, (chunk + 1) * groupsPerBlock) of `list` (or of all
 // vertices).  Every thread of the block calls it with the same chunk.
-template <int W, bool kExt, bool kCoherent = false>
+template <int W, bool kExt, bool kCoherent = false, bool kCache = true>
 __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __restrict__ pp,
                                            const float4* __restrict__ src, float4* tgt,
                                            const uint32_t* __restrict__ list, uint32_t count, uint32_t K,
@@ -1691,7 +1773,7 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
   }
   __syncthreads();
 #if JGS2_SOLVE_STAGE
-  {
+  if constexpr (kCache) {
     // Stage the block's records: headers and basis blocks, then (once the
     // headers have landed) the tetrahedron records they name.
     RecSlot* slots = reinterpret_cast<RecSlot*>(slotBase);
@@ -1783,127 +1865,66 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
         // Cubature records first, then (unless cached) the incident tets, in
         // separate loops so the two kinds of item never share a divergent pass.
         for (uint32_t u = lane; u < K; u += W) {
-          {
-            // ---- cubature record (jgs2-shader.ts:3197-3263) ----
-            CubState st;
-#if JGS2_SOLVE_STAGE
-            const RecSlot* staged = reinterpret_cast<const RecSlot*>(mySlots + u * kSolveSlotBytes);
-            const uint4 head = staged->head[0];
-            const uint4 idx = staged->head[1];
-#else
-            const size_t rec = static_cast<size_t>(v) * K + u;
-            const uint4 head = __ldg(&b.cubHead[2 * rec]);
-            const uint4 idx = __ldg(&b.cubHead[2 * rec + 1]);
-#endif
-            const uint32_t t = head.x;
-            const float w = __uint_as_float(head.y);
-            st.w = 0.0f;
-            // Headers hold global tet ids; out-of-range records were emptied at create.
-            if (t != kEmptyTet && w > 0.0f) {
-#if JGS2_SOLVE_STAGE
-              const TetRec r = tetFromSlot(staged->tet);
-              const float4* U = staged->basis;
-#else
-              const TetRec r = loadTet(b.tets, t);
-              const float4* U = b.cubBasis + 9ull * rec;
-#endif
-              // One basis block B'_l = R_l Ubar_l at a time: accumulate F,
-              // the projected directions dF_c = sum_l B'_l[:,c] g_l^T and the
-              // inertia / objective quadratic (gQ, HQ) of the record, all in
-              // the source frame.
-              M3 F = mzero(), dF0 = mzero(), dF1 = mzero(), dF2 = mzero();
-              float3 gQ = f3(0, 0, 0);
-              S3 HQ = szero();
-              uint32_t slot = 4;
-              const float3 x0 = xyz(ldPos<kCoherent>(src, idx.x));
-#pragma unroll
-              for (int l = 0; l < 4; ++l) {
-                const uint32_t q = idxAt(idx, l);
-                if (q == v) slot = l;
-                const float3 gl = shapeGradient(r, l);
-#if JGS2_SOLVE_STAGE
-                const M3 B = mm(loadRotT<kCoherent>(b.vertexRot, q), loadBlockVecShared(U, l));
-#else
-                const M3 B = mm(loadRotT<kCoherent>(b.vertexRot, q), loadBlockVec(U, l));
-#endif
-                const float3 xl = l == 0 ? x0 : xyz(ldPos<kCoherent>(src, q));
-                if (l > 0) F = F + outer(xl - x0, gl);
-                dF0 = dF0 + outer(B.c0, gl);
-                dF1 = dF1 + outer(B.c1, gl);
-                dF2 = dF2 + outer(B.c2, gl);
-                // predicted w = distributed inertia weight (0 when pinned).
-                const float4 pq = b.predicted[q];
-                const float dW = pq.w;
-                float3 lin = dW * (xl - xyz(pq));
-                float quad = dW;
-                const uint4 qi = objActive ? b.vinfo[q] : make_uint4(0u, 0u, 1u, 0u);
-                if (objActive && !isPinned(qi)) {
-                  const float nq = float(qi.y > 1u ? qi.y : 1u);
-                  lin = lin + objectiveGradient(p, b, q, xl) * (1.0f / nq);
-                  quad += targetStiffness(p, b, q) / nq;
-                }
-                gQ = gQ + mtv(B, lin);
-                saddScaled(HQ, quad, gramColumns(B));
-              }
-              const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
-              const M3 P = piola(F, pt);
-              float3 pg = r.vol * f3(frob(dF0, P), frob(dF1, P), frob(dF2, P)) + gQ;
-              // Reduced material Hessian vol <dF_r, DP[dF_c]>; the cofactor
-              // term <A, Dcof[B]> is symmetric, so one directional cofactor is
-              // live at a time.
-              const float p0 = frob(F, dF0), p1 = frob(F, dF1), p2 = frob(F, dF2);
-              const float q0 = frob(pt.cof, dF0), q1 = frob(pt.cof, dF1), q2 = frob(pt.cof, dF2);
-              S3 ph;
-              {
-                const M3 D0 = dcofactor(F, dF0);
-                ph.xx = pt.b * frob(dF0, D0);
-                ph.xy = pt.b * frob(dF1, D0);
-                ph.xz = pt.b * frob(dF2, D0);
-              }
-              {
-                const M3 D1 = dcofactor(F, dF1);
-                ph.yy = pt.b * frob(dF1, D1);
-                ph.yz = pt.b * frob(dF2, D1);
-              }
-              ph.zz = pt.b * frob(dF2, dcofactor(F, dF2));
-              ph.xx += pt.a * frob(dF0, dF0) + pt.c1 * p0 * p0 + r.lambda * q0 * q0;
-              ph.yy += pt.a * frob(dF1, dF1) + pt.c1 * p1 * p1 + r.lambda * q1 * q1;
-              ph.zz += pt.a * frob(dF2, dF2) + pt.c1 * p2 * p2 + r.lambda * q2 * q2;
-              ph.xy += pt.a * frob(dF0, dF1) + pt.c1 * p0 * p1 + r.lambda * q0 * q1;
-              ph.xz += pt.a * frob(dF0, dF2) + pt.c1 * p0 * p2 + r.lambda * q0 * q2;
-              ph.yz += pt.a * frob(dF1, dF2) + pt.c1 * p1 * p2 + r.lambda * q1 * q2;
-              ph.xx *= r.vol; ph.yy *= r.vol; ph.zz *= r.vol; ph.xy *= r.vol; ph.xz *= r.vol; ph.yz *= r.vol;
-              sadd(ph, HQ);
-              cadd(gsum, w * mv(Rs, pg));
-              saddScaled(hess, w, srotate(Rs, ph));
-              float3 gs = f3(0, 0, 0);
-              if (slot < 4) {
-                // Remove the exact source block already in the local gather.
-                gs = shapeGradient(r, slot);
-                float3 ps = r.vol * mv(P, gs) + dWs * (position - predV);
-                if (objActive) ps = ps + objS * (1.0f / nS);
-                const float3 u1 = mv(F, gs), w1 = mv(pt.cof, gs);
-                S3 blk = szero();
-                saddDiag(blk, pt.a * dot3(gs, gs));
-                saddOuter(blk, pt.c1, u1);
-                saddOuter(blk, r.lambda, w1);
-                cadd(gsum, (-w) * ps);
-                saddScaled(hess, -w * r.vol, blk);
-                saddDiag(hess, -w * (dWs + ktS / nS));
-              }
-              st.F = F;
-              st.I0 = pt.I1;
-              st.J0 = pt.J;
-              st.dF0 = dF0; st.dF1 = dF1; st.dF2 = dF2;
-              st.gQ = gQ;
-              st.HQ = HQ;
-              st.w = w;
-              st.vol = r.vol; st.lambda = r.lambda; st.mu = r.mu;
-              st.slot = slot;
-              st.gs = gs;
+          // ---- cubature record (jgs2-shader.ts:3197-3263) ----
+          CubState st;
+          TetRec r;
+          const size_t rec = static_cast<size_t>(v) * K + u;
+          if constexpr (kCache && JGS2_SOLVE_STAGE)
+            recordState<kCoherent, true>(b, p, v, rec, reinterpret_cast<const RecSlot*>(mySlots + u * kSolveSlotBytes),
+                                         src, objActive, st, r);
+          else
+            recordState<kCoherent, false>(b, p, v, rec, nullptr, src, objActive, st, r);
+          if (st.w > 0.0f) {
+            const float w = st.w;
+            const M3& F = st.F;
+            const M3 &dF0 = st.dF0, &dF1 = st.dF1, &dF2 = st.dF2;
+            const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
+            const M3 P = piola(F, pt);
+            float3 pg = r.vol * f3(frob(dF0, P), frob(dF1, P), frob(dF2, P)) + st.gQ;
+            // Reduced material Hessian vol <dF_r, DP[dF_c]>; the cofactor
+            // term <A, Dcof[B]> is symmetric, so one directional cofactor is
+            // live at a time.
+            const float p0 = frob(F, dF0), p1 = frob(F, dF1), p2 = frob(F, dF2);
+            const float q0 = frob(pt.cof, dF0), q1 = frob(pt.cof, dF1), q2 = frob(pt.cof, dF2);
+            S3 ph;
+            {
+              const M3 D0 = dcofactor(F, dF0);
+              ph.xx = pt.b * frob(dF0, D0);
+              ph.xy = pt.b * frob(dF1, D0);
+              ph.xz = pt.b * frob(dF2, D0);
             }
-            *reinterpret_cast<CubState*>(mySlots + u * kSolveSlotBytes) = st;
+            {
+              const M3 D1 = dcofactor(F, dF1);
+              ph.yy = pt.b * frob(dF1, D1);
+              ph.yz = pt.b * frob(dF2, D1);
+            }
+            ph.zz = pt.b * frob(dF2, dcofactor(F, dF2));
+            ph.xx += pt.a * frob(dF0, dF0) + pt.c1 * p0 * p0 + r.lambda * q0 * q0;
+            ph.yy += pt.a * frob(dF1, dF1) + pt.c1 * p1 * p1 + r.lambda * q1 * q1;
+            ph.zz += pt.a * frob(dF2, dF2) + pt.c1 * p2 * p2 + r.lambda * q2 * q2;
+            ph.xy += pt.a * frob(dF0, dF1) + pt.c1 * p0 * p1 + r.lambda * q0 * q1;
+            ph.xz += pt.a * frob(dF0, dF2) + pt.c1 * p0 * p2 + r.lambda * q0 * q2;
+            ph.yz += pt.a * frob(dF1, dF2) + pt.c1 * p1 * p2 + r.lambda * q1 * q2;
+            ph.xx *= r.vol; ph.yy *= r.vol; ph.zz *= r.vol; ph.xy *= r.vol; ph.xz *= r.vol; ph.yz *= r.vol;
+            sadd(ph, st.HQ);
+            cadd(gsum, w * mv(Rs, pg));
+            saddScaled(hess, w, srotate(Rs, ph));
+            if (st.slot < 4) {
+              // Remove the exact source block already in the local gather.
+              const float3 gs = st.gs;
+              float3 ps = r.vol * mv(P, gs) + dWs * (position - predV);
+              if (objActive) ps = ps + objS * (1.0f / nS);
+              const float3 u1 = mv(F, gs), w1 = mv(pt.cof, gs);
+              S3 blk = szero();
+              saddDiag(blk, pt.a * dot3(gs, gs));
+              saddOuter(blk, pt.c1, u1);
+              saddOuter(blk, r.lambda, w1);
+              cadd(gsum, (-w) * ps);
+              saddScaled(hess, -w * r.vol, blk);
+              saddDiag(hess, -w * (dWs + ktS / nS));
+            }
           }
+          if constexpr (kCache) *reinterpret_cast<CubState*>(mySlots + u * kSolveSlotBytes) = st;
         }
         if (!cachedIncident) {
           for (uint32_t a = lane; a < info.y; a += W) {
@@ -1998,7 +2019,16 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
             // A lane's items in order: its cached cubature records, then its
             // incident tets (the same per-lane order as one merged loop).
             for (uint32_t u = lane; u < K; u += W) {
-              const CubState& st = *reinterpret_cast<const CubState*>(mySlots + u * kSolveSlotBytes);
+              CubState stLocal;
+              if constexpr (!kCache) {
+                // No shared cache for wide records: recompute the record's
+                // state (the same arithmetic as the gather above).
+                TetRec rr;
+                recordState<kCoherent, false>(b, p, v, static_cast<size_t>(v) * K + u, nullptr, src, objActive,
+                                              stLocal, rr);
+              }
+              const CubState& st =
+                  kCache ? *reinterpret_cast<const CubState*>(mySlots + u * kSolveSlotBytes) : stLocal;
               if (!(st.w > 0.0f)) continue;
               float J = 0.0f;
               // Record state is in the source frame: the trial step there is R_s^T td.
@@ -2178,12 +2208,15 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
   }
 }
 
-template <int W, bool kExt>
+// kCache: the records' line-search state is cached in shared memory (and the
+// records are staged there); wide records (an exact complement) recompute it
+// per trial instead, so a block needs no shared memory per vertex.
+template <int W, bool kExt, bool kCache>
 __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS) solveKernel(Buffers b, const DevParams* __restrict__ pp,
                                                       const float4* __restrict__ src, float4* tgt,
                                                       const uint32_t* __restrict__ list, uint32_t count,
                                                       uint32_t K, int cachedIncident, uint32_t groupsPerBlock) {
-  solveChunk<W, kExt>(b, pp, src, tgt, list, count, K, cachedIncident, groupsPerBlock, blockIdx.x);
+  solveChunk<W, kExt, false, kCache>(b, pp, src, tgt, list, count, K, cachedIncident, groupsPerBlock, blockIdx.x);
 }
 
 // ---------------------------------------------------------------------------
@@ -3143,11 +3176,12 @@ int launchVertexPolar(const Buffers& b, const DevParams* p, const float4* src, c
 int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4* tgt, const uint32_t* list,
                 uint32_t count, uint32_t K, bool cachedIncident, cudaStream_t s) {
   if (count == 0) return 0;
+  const bool cache = solveCachesRecords(K);
   const uint32_t fit = solveGroupsPerBlock(K);
   if (fit == 0) return 0;
   const uint32_t shift = std::min(b.solveShift, 2u);
   const uint32_t groups = std::max(1u, fit >> shift);
-  const size_t smem = static_cast<size_t>(groups) * K * kSolveSlotBytes;
+  const size_t smem = cache ? static_cast<size_t>(groups) * K * kSolveSlotBytes : 0;
   constexpr uint32_t perWarp = 32u / kGroup;
   const uint32_t threads = (groups + perWarp - 1) / perWarp * 32u;
   // One vertex per lane group: the line search makes per-vertex work uneven,
@@ -3163,15 +3197,20 @@ int launchSolve(const Buffers& b, const DevParams* p, const float4* src, float4*
     // Warps per block: an eighth of the vertices a 4-lane block of the same
     // cache budget would take (at most a full block).
     const uint32_t perVertex = static_cast<uint32_t>(K * kSolveSlotBytes);
-    const uint32_t fit4 = std::min<uint32_t>(32u, perVertex ? solveSharedBytes() / perVertex : 32u);
+    const uint32_t fit4 = std::min<uint32_t>(32u, (cache && perVertex) ? solveSharedBytes() / perVertex : 32u);
     const uint32_t wg = std::max(1u, std::min(std::max(1u, fit4 >> shift) * 4u / 32u, kBlock / 32u));
-    const size_t wsmem = static_cast<size_t>(wg) * K * kSolveSlotBytes;
-    solveKernel<32, true><<<std::max(1u, (count + wg - 1) / wg), wg * 32, wsmem, s>>>(b, p, src, tgt, list, count,
-                                                                                      K, ci, wg);
+    const size_t wsmem = cache ? static_cast<size_t>(wg) * K * kSolveSlotBytes : 0;
+    const uint32_t wb = std::max(1u, (count + wg - 1) / wg);
+    if (cache)
+      solveKernel<32, true, true><<<wb, wg * 32, wsmem, s>>>(b, p, src, tgt, list, count, K, ci, wg);
+    else
+      solveKernel<32, true, false><<<wb, wg * 32, 0, s>>>(b, p, src, tgt, list, count, K, ci, wg);
   } else if (b.clothRange || b.contactIdx) {
-    solveKernel<kGroup, true><<<blocks, threads, smem, s>>>(b, p, src, tgt, list, count, K, ci, groups);
+    if (cache) solveKernel<kGroup, true, true><<<blocks, threads, smem, s>>>(b, p, src, tgt, list, count, K, ci, groups);
+    else solveKernel<kGroup, true, false><<<blocks, threads, 0, s>>>(b, p, src, tgt, list, count, K, ci, groups);
   } else {
-    solveKernel<kGroup, false><<<blocks, threads, smem, s>>>(b, p, src, tgt, list, count, K, ci, groups);
+    if (cache) solveKernel<kGroup, false, true><<<blocks, threads, smem, s>>>(b, p, src, tgt, list, count, K, ci, groups);
+    else solveKernel<kGroup, false, false><<<blocks, threads, 0, s>>>(b, p, src, tgt, list, count, K, ci, groups);
   }
   return 1;
 }
@@ -3184,6 +3223,7 @@ int launchColoredSweep(const Buffers& b, const DevParams* p, float4* x, const ui
                        bool refreshAllFrames, void* barrier, uint32_t spinLimit, cudaStream_t s) {
   const uint32_t fit = solveGroupsPerBlock(K);
   if (fit == 0 || colorCount == 0) return 0;
+  if (!solveCachesRecords(K)) return -1;  // the sweep kernel caches records
   const uint32_t groups = std::max(1u, fit >> std::min(b.solveShift, 2u));
   const size_t smem = static_cast<size_t>(groups) * K * kSolveSlotBytes;
   constexpr uint32_t perWarp = 32u / kGroup;
@@ -3244,19 +3284,21 @@ uint32_t solveSharedBytes() {
     cudaGetDevice(&dev);
     if (cudaDeviceGetAttribute(&optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev) != cudaSuccess) optin = 48 * 1024;
     optin -= 1024;  // static shared memory of the kernel
-    cudaFuncSetAttribute(solveKernel<kGroup, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    cudaFuncSetAttribute(solveKernel<kGroup, false>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
-    cudaFuncSetAttribute(solveKernel<32, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(solveKernel<kGroup, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(solveKernel<kGroup, false, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
+    cudaFuncSetAttribute(solveKernel<32, true, true>, cudaFuncAttributeMaxDynamicSharedMemorySize, optin);
   }
   return static_cast<uint32_t>(optin);
 }
 
+bool solveCachesRecords(uint32_t K) { return static_cast<size_t>(K) * kSolveSlotBytes <= kSolveCacheBytesPerVertex; }
+
 uint32_t solveGroupsPerBlock(uint32_t K) {
   // Shared memory holds one cached record state per cubature record of each
-  // vertex in the block; large K (an exact complement) trades vertices per
-  // block for cache.
-  const uint32_t perVertex = static_cast<uint32_t>(K * kSolveSlotBytes);
+  // vertex in the block; wide records are recomputed instead of cached.
   uint32_t groups = (kBlock / 32) * (32 / kGroup);
+  if (!solveCachesRecords(K)) return groups;
+  const uint32_t perVertex = static_cast<uint32_t>(K * kSolveSlotBytes);
   if (perVertex > 0) groups = std::min<uint32_t>(groups, solveSharedBytes() / perVertex);
   return groups;
 }

@@ -279,6 +279,9 @@ int launchOracleDiagnostics(const Buffers& b, const OracleParams& q, float4* tet
 
 // Vertices per solve block for cubature width K (0: K too large to cache).
 uint32_t solveGroupsPerBlock(uint32_t K);
+// Whether the solve caches records of width K in shared memory (else it
+// recomputes them in the line search).
+bool solveCachesRecords(uint32_t K);
 // Dynamic shared memory available to one solve block.
 uint32_t solveSharedBytes();
 constexpr size_t kGatePartialBytes = 32;

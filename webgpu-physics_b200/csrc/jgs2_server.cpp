@@ -2,13 +2,14 @@
 //
 // Two threads.  The builder admits queued requests against the memory budget
 // into a wave and builds its batch (validation, packing, upload, preflight);
-// the stepper launches one frame of every wave in flight per round (each wave
+// the stepper launches frames of every wave in flight per round (each wave
 // on its own stream, so they overlap), waits for them, and retires requests
 // that have run their frames.  The request table, the queue, the ready list
 // and the statistics are guarded by one mutex; a wave belongs to the builder
 // until it is on the ready list and to the stepper afterwards.
 #include <cuda_runtime.h>
 
+#include <algorithm>
 #include <chrono>
 #include <condition_variable>
 #include <cstring>
@@ -110,8 +111,12 @@ struct Wave {
   uint32_t exactIterations = 0;
   uint64_t bytes = 0;
   uint32_t remaining = 0;
+  uint32_t roundFrames = 1;  // frames stepped in the current round
   bool started = false;
 };
+
+// Frames a wave may step in one round of the stepper.
+constexpr uint32_t kRoundFrames = 16;
 
 uint32_t normalizeOdd(uint32_t it) {
   const uint32_t i = it < 1 ? 1 : it;
@@ -252,7 +257,9 @@ struct jgs2_server {
         ready.clear();
         stats.waves_in_flight = static_cast<uint32_t>(waves.size());
       }
-      // One round: a frame of every wave in flight, launched together.
+      // One round: every wave in flight steps as many frames as its nearest
+      // request still needs (at most kRoundFrames), launched together, so a
+      // round's host synchronisation is shared by several frames.
       const auto t0 = Clock::now();
       const double t0s = now();
       for (auto& w : waves) {
@@ -260,19 +267,24 @@ struct jgs2_server {
           w->started = true;
           for (Request* r : w->requests) r->admitT = t0s;
         }
-        const jgs2_status st = jgs2_batch_step_frames(w->batch, 1, w->exactIterations, nullptr, nullptr);
+        uint32_t n = kRoundFrames;
+        for (size_t i = 0; i < w->requests.size(); ++i)
+          if (w->active[i]) n = std::min(n, w->requests[i]->frames - w->requests[i]->framesDone);
+        w->roundFrames = std::max(1u, n);
+        const jgs2_status st =
+            jgs2_batch_step_frames(w->batch, w->roundFrames, w->exactIterations, nullptr, nullptr);
         if (st != JGS2_OK) failWave(*w, st);
       }
       for (auto& w : waves) {
         if (w->remaining == 0) continue;
         const jgs2_status st = jgs2_batch_sync(w->batch);
         if (st != JGS2_OK) { failWave(*w, st); continue; }
-        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count();
+        const double ms = std::chrono::duration<double, std::milli>(Clock::now() - t0).count() / w->roundFrames;
         for (size_t i = 0; i < w->requests.size(); ++i) {
           if (!w->active[i]) continue;
           Request* r = w->requests[i];
-          r->framesDone++;
-          r->sumFrameMs += ms;
+          r->framesDone += w->roundFrames;
+          r->sumFrameMs += ms * w->roundFrames;
           if (ms > r->maxFrameMs) r->maxFrameMs = ms;
           if (r->framesDone < r->frames) continue;
           const size_t n = 4ull * r->input->view.vertex_count;
