@@ -235,3 +235,34 @@ def test_production_finalize_matches_oracle(schedule):
     low = _positions(cpu.read("positions"))[:, 1].min()
     assert low < 0.02  # the box reached the floor, so the floor terms acted
     gpu.destroy()
+
+
+def test_config2_bodies_in_one_batch_vs_oracles():
+    # Config 2's construction on a sample: eight hex-grid bodies with
+    # U{4..32} cells per axis (the same seed), soft and stiff materials, free
+    # fall onto the penalty floor, K = 6, 10 exact iterations, stepped in one
+    # batch for one frame; each body against the f32 and FP64 oracles.  The
+    # trained complement makes these bodies sensitive to rounding: the
+    # oracle's own f32 and FP64 frames differ by up to 2.1e-4 of a body's
+    # diagonal (the 4 928-vertex body), so positions are held to 1e-3 and the
+    # FP64 error is reported; accept flags must equal both oracles'.
+    parts = scenes.batched_scenes(count=8)
+    s = dict(timestep=1 / 60, iterations=10)
+    batch = solver.JGS2Batch.create(parts, _camel(s))
+    batch.stepFrames(1, exactIterations=10)
+    worst32 = worst64 = 0.0
+    for i, p in enumerate(parts):
+        c32 = O.OracleSolver(p, s, precision=32)
+        c64 = O.OracleSolver(p, s, precision=64)
+        c32.step_exact_iterations(10)
+        c64.step_exact_iterations(10)
+        flags = _accepted(batch.readGlobalizationDiagnostics(i)["history"], 10)
+        np.testing.assert_array_equal(flags, _accepted(c32.read("history"), 10), err_msg=f"body {i}")
+        np.testing.assert_array_equal(flags, _accepted(c64.read("history"), 10), err_msg=f"body {i}")
+        g = batch.readPositions(i)
+        worst32 = max(worst32, _error(p, g, c32.read("positions")))
+        worst64 = max(worst64, _error(p, g, c64.read("positions")))
+    print(f"config-2 sample, 8 bodies, one frame: worst GPU vs f32 oracle {worst32:.2e}, vs FP64 oracle "
+          f"{worst64:.2e} of a body's bbox diagonal")
+    assert worst32 <= 1e-3 and worst64 <= 1e-3
+    batch.destroy()

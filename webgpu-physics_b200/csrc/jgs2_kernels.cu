@@ -2630,6 +2630,9 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
 // the reference forms the same norms in f32 as scale * sqrt(sum((g/scale)^2)).
 // JGS2_CONV_MIN_BLOCKS: blocks per SM the convergence kernel's register
 // budget must allow (unset: the compiler's choice).
+#ifndef JGS2_CONV_LOOKAHEAD
+#define JGS2_CONV_LOOKAHEAD 1
+#endif
 #ifdef JGS2_CONV_MIN_BLOCKS
 #define JGS2_CONV_BOUNDS __launch_bounds__(kBlock, JGS2_CONV_MIN_BLOCKS)
 #else
@@ -2669,9 +2672,25 @@ __global__ void JGS2_CONV_BOUNDS convergenceKernel(Buffers b, const DevParams* _
       M3 avg = mzero();
       float total = 0.0f;
       S3 hess = szero();
+#if JGS2_CONV_LOOKAHEAD
+      // The next incident tet's record is requested before the current
+      // one's arithmetic, so its latency overlaps the work.
+      uint32_t nextEntry = info.y ? __ldg(&b.adjacency[info.x]) : 0u;
+      TetRec nextRec;
+      if (info.y) nextRec = loadTet(b.tets, nextEntry >> 2);
+#endif
       for (uint32_t a = 0; a < info.y; ++a) {
+#if JGS2_CONV_LOOKAHEAD
+        const uint32_t entry = nextEntry;
+        const TetRec r = nextRec;
+        if (a + 1 < info.y) {
+          nextEntry = __ldg(&b.adjacency[info.x + a + 1]);
+          nextRec = loadTet(b.tets, nextEntry >> 2);
+        }
+#else
         const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
         const TetRec r = loadTet(b.tets, entry >> 2);
+#endif
         const M3 F = deformationAt(r, acc);
         const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
         const float3 g = shapeGradient(r, entry & 3u);
