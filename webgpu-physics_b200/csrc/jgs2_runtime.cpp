@@ -902,6 +902,8 @@ struct Engine {
   void* dSweepBarrier = nullptr;
   uint32_t spinLimit = 1u << 24;
   bool persistentSweep = false;
+  // Fault injection of device allocations (JGS2_FAIL_ALLOCATION); -1 off.
+  int64_t failAllocationAt = -1, allocationCount = 0;
   bool sweepLaunched = false;
   uint32_t* dNeedVertices = nullptr;
   std::vector<void*> allocations;
@@ -966,6 +968,12 @@ template <class T>
 jgs2_status deviceAlloc(Engine* s, T** out, size_t count) {
   void* p = nullptr;
   const size_t bytes = std::max<size_t>(16, count * sizeof(T));
+  // Host-side fault injection (JGS2_FAIL_ALLOCATION=n, read at create): the
+  // n-th device allocation of a create fails as an exhausted device would.
+  if (s->failAllocationAt >= 0 && s->allocationCount++ == s->failAllocationAt)
+    return fail(s, JGS2_OUT_OF_MEMORY,
+                format("cudaMalloc: out of memory (injected by JGS2_FAIL_ALLOCATION at allocation %lld)",
+                       static_cast<long long>(s->failAllocationAt)));
   cudaError_t e = cudaMalloc(&p, bytes);
   if (e != cudaSuccess) return cudaFail(s, e, "cudaMalloc");
   s->allocations.push_back(p);
@@ -1570,6 +1578,7 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   sp->useGraphs = std::getenv("JGS2_NO_GRAPHS") == nullptr;
   if (const char* e = std::getenv("JGS2_BARRIER_SPIN_LIMIT")) sp->spinLimit = static_cast<uint32_t>(std::strtoul(e, nullptr, 10));
   if (const char* e = std::getenv("JGS2_COLOR_SWEEP")) sp->persistentSweep = std::string(e) == "persistent";
+  if (const char* e = std::getenv("JGS2_FAIL_ALLOCATION")) sp->failAllocationAt = std::strtoll(e, nullptr, 10);
   sp->glob = prep[0].stable;
   for (const PreparedScene& p : prep)
     if (p.stable != sp->glob)
