@@ -39,6 +39,11 @@ constexpr int kBlock = 128;
 // Lanes per vertex in the solve kernel.  A warp holds 32 / kGroup lane groups;
 // a width that does not divide 32 leaves the warp's last lanes idle.
 constexpr int kGroup = JGS2_SOLVE_LANES;
+// Incident-tet gathers request the next tet's record before the current
+// one's arithmetic (convergence, frames, the line search).
+#ifndef JGS2_CONV_LOOKAHEAD
+#define JGS2_CONV_LOOKAHEAD 1
+#endif
 constexpr int kRecFloats = 56;  // cached cubature record state
 
 struct TetRec {
@@ -339,9 +344,23 @@ __device__ __forceinline__ void frameAndIncident(const Buffers& b, const DevPara
   float total = 0.0f;
   Comp3 grad = czero();  // compensated gradient gather
   S3 hess = szero();
+#if JGS2_CONV_LOOKAHEAD
+  uint32_t nextEntry = info.y ? __ldg(&b.adjacency[info.x]) : 0u;
+  TetRec nextRec;
+  if (info.y) nextRec = loadTet(b.tets, nextEntry >> 2);
+#endif
   for (uint32_t a = 0; a < info.y; ++a) {
+#if JGS2_CONV_LOOKAHEAD
+    const uint32_t entry = nextEntry;
+    const TetRec r = nextRec;
+    if (a + 1 < info.y) {
+      nextEntry = __ldg(&b.adjacency[info.x + a + 1]);
+      nextRec = loadTet(b.tets, nextEntry >> 2);
+    }
+#else
     const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
     const TetRec r = loadTet(b.tets, entry >> 2);
+#endif
     const M3 F = deformationAt(r, x);
     const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
     const float3 g = shapeGradient(r, entry & 3u);
@@ -2047,10 +2066,26 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
             }
             // Incident tets of lane-order index u >= K, i.e. adjacency slot u - K.
             const uint32_t firstInc = lane >= K % W ? lane - K % W : lane + W - K % W;
+#if JGS2_CONV_LOOKAHEAD
+            // The lane's next incident tet is requested before the current
+            // one's arithmetic (as in the convergence gather).
+            uint32_t nextEntry = firstInc < info.y ? __ldg(&b.adjacency[info.x + firstInc]) : 0u;
+            TetRec nextRec;
+            if (firstInc < info.y) nextRec = loadTet(b.tets, nextEntry >> 2);
+#endif
             for (uint32_t a = firstInc; a < info.y; a += W) {
               float J = 0.0f;
+#if JGS2_CONV_LOOKAHEAD
+              const uint32_t entry = nextEntry;
+              const TetRec r = nextRec;
+              if (a + W < info.y) {
+                nextEntry = __ldg(&b.adjacency[info.x + a + W]);
+                nextRec = loadTet(b.tets, nextEntry >> 2);
+              }
+#else
               const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
               const TetRec r = loadTet(b.tets, entry >> 2);
+#endif
               const M3 F = deformationAtT<kCoherent>(r, src);
               const float I0 = frob(F, F);
               const float J0 = mdet(F);
@@ -2630,9 +2665,6 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
 // the reference forms the same norms in f32 as scale * sqrt(sum((g/scale)^2)).
 // JGS2_CONV_MIN_BLOCKS: blocks per SM the convergence kernel's register
 // budget must allow (unset: the compiler's choice).
-#ifndef JGS2_CONV_LOOKAHEAD
-#define JGS2_CONV_LOOKAHEAD 1
-#endif
 #ifdef JGS2_CONV_MIN_BLOCKS
 #define JGS2_CONV_BOUNDS __launch_bounds__(kBlock, JGS2_CONV_MIN_BLOCKS)
 #else
