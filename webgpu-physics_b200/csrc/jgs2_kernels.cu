@@ -39,6 +39,9 @@ constexpr int kBlock = 128;
 // Lanes per vertex in the solve kernel.  A warp holds 32 / kGroup lane groups;
 // a width that does not divide 32 leaves the warp's last lanes idle.
 constexpr int kGroup = JGS2_SOLVE_LANES;
+#ifndef JGS2_FRAME_QUAT
+#define JGS2_FRAME_QUAT 0
+#endif
 // Incident-tet gathers request the next tet's record before the current
 // one's arithmetic (convergence, frames, the line search).
 #ifndef JGS2_CONV_LOOKAHEAD
@@ -104,8 +107,12 @@ __device__ __forceinline__ float4 ldPos(const float4* p, size_t i) {
   if constexpr (kCoherent) return __ldca(p + i);
   else return p[i];
 }
+__device__ __forceinline__ M3 quaternionFrame(float4 q);
 template <bool kCoherent>
 __device__ __forceinline__ M3 loadRotT(const float4* rot, uint32_t v) {
+#if JGS2_FRAME_QUAT
+  return quaternionFrame(kCoherent ? __ldca(rot + 3ull * v) : rot[3ull * v]);
+#endif
   if constexpr (kCoherent) {
     const float4 a = __ldca(rot + 3ull * v), b = __ldca(rot + 3ull * v + 1), c = __ldca(rot + 3ull * v + 2);
     return {f3(a.x, a.y, a.z), f3(b.x, b.y, b.z), f3(c.x, c.y, c.z)};
@@ -126,6 +133,54 @@ __device__ __forceinline__ void storeRot(float4* __restrict__ rot, uint32_t v, c
   rot[3ull * v] = make_float4(m.c0.x, m.c0.y, m.c0.z, 0.f);
   rot[3ull * v + 1] = make_float4(m.c1.x, m.c1.y, m.c1.z, 0.f);
   rot[3ull * v + 2] = make_float4(m.c2.x, m.c2.y, m.c2.z, 0.f);
+}
+
+// Vertex frames.  With JGS2_FRAME_QUAT a frame is stored as a unit
+// quaternion in the first float4 of its three (one vector load per read
+// instead of three); the matrix is rebuilt from it on every read.
+__device__ __forceinline__ float4 frameQuaternion(const M3& m) {
+  // Shepperd's method on the largest of the trace and the diagonal.
+  const float m00 = m.c0.x, m11 = m.c1.y, m22 = m.c2.z;
+  const float m21 = m.c1.z, m12 = m.c2.y, m02 = m.c2.x, m20 = m.c0.z, m10 = m.c0.y, m01 = m.c1.x;
+  const float tr = m00 + m11 + m22;
+  float4 q;
+  if (tr > 0.0f) {
+    const float t = sqrtf(tr + 1.0f) * 2.0f;
+    q = make_float4((m21 - m12) / t, (m02 - m20) / t, (m10 - m01) / t, 0.25f * t);
+  } else if (m00 > m11 && m00 > m22) {
+    const float t = sqrtf(1.0f + m00 - m11 - m22) * 2.0f;
+    q = make_float4(0.25f * t, (m01 + m10) / t, (m02 + m20) / t, (m21 - m12) / t);
+  } else if (m11 > m22) {
+    const float t = sqrtf(1.0f + m11 - m00 - m22) * 2.0f;
+    q = make_float4((m01 + m10) / t, 0.25f * t, (m12 + m21) / t, (m02 - m20) / t);
+  } else {
+    const float t = sqrtf(1.0f + m22 - m00 - m11) * 2.0f;
+    q = make_float4((m02 + m20) / t, (m12 + m21) / t, 0.25f * t, (m10 - m01) / t);
+  }
+  const float n = rsqrtf(q.x * q.x + q.y * q.y + q.z * q.z + q.w * q.w);
+  return make_float4(q.x * n, q.y * n, q.z * n, q.w * n);
+}
+__device__ __forceinline__ M3 quaternionFrame(float4 q) {
+  const float x2 = q.x + q.x, y2 = q.y + q.y, z2 = q.z + q.z;
+  const float xx = q.x * x2, yy = q.y * y2, zz = q.z * z2;
+  const float xy = q.x * y2, xz = q.x * z2, yz = q.y * z2;
+  const float wx = q.w * x2, wy = q.w * y2, wz = q.w * z2;
+  return {f3(1.0f - (yy + zz), xy + wz, xz - wy), f3(xy - wz, 1.0f - (xx + zz), yz + wx),
+          f3(xz + wy, yz - wx, 1.0f - (xx + yy))};
+}
+__device__ __forceinline__ void storeFrame(float4* __restrict__ rot, uint32_t v, const M3& m) {
+#if JGS2_FRAME_QUAT
+  rot[3ull * v] = frameQuaternion(m);
+#else
+  storeRot(rot, v, m);
+#endif
+}
+__device__ __forceinline__ M3 loadFrame(const float4* __restrict__ rot, uint32_t v) {
+#if JGS2_FRAME_QUAT
+  return quaternionFrame(rot[3ull * v]);
+#else
+  return loadRot(rot, v);
+#endif
 }
 
 // Row-major stored Ubar block l -> columns (cubatureBlock, jgs2-shader.ts:1204-1212).
@@ -373,7 +428,7 @@ __device__ __forceinline__ void frameAndIncident(const Buffers& b, const DevPara
     clothLocalSystem<true>(b.clothTris, b.clothHinges, b.clothIncidence, b.clothRange[v], x, clothMaterial(p), 0u, 1u,
                            grad, hess);
   const M3 favg = total > 0.0f ? (1.0f / total) * avg : midentity();
-  storeRot(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, eps));
+  storeFrame(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, eps));
   storeIncident(b.incident, v, cvalue(grad), hess);
 }
 
@@ -405,7 +460,7 @@ __global__ void __launch_bounds__(kBlock) vertexPolarKernel(Buffers b, const Dev
   const uint32_t scene = b.vertexScene[v];
   const DevParams& p = pp[scene];
   if (!p.active || latched(p, &b.frames[scene])) return;
-  storeRot(b.vertexRot, v, vertexFrame(b, x, v, p.rotationEpsilon));
+  storeFrame(b.vertexRot, v, vertexFrame(b, x, v, p.rotationEpsilon));
 }
 
 // ---------------------------------------------------------------------------
@@ -537,7 +592,7 @@ __global__ void __launch_bounds__(kBlock) corotatedSolveKernel(Buffers b, const 
     cadd(gsum, f3(0.0f, p.floorStiffness * (position.y - p.floorHeight), 0.0f));
     hess.c1.y += p.floorStiffness;
   }
-  const M3 RsT = mtrans(loadRot(b.vertexRot, v));
+  const M3 RsT = mtrans(loadFrame(b.vertexRot, v));
   const float dWs = pv.w;
   for (uint32_t s = 0; s < K; ++s) {
     const size_t rec = static_cast<size_t>(v) * K + s;
@@ -549,7 +604,7 @@ __global__ void __launch_bounds__(kBlock) corotatedSolveKernel(Buffers b, const 
     const float4* U = b.cubBasis + 9ull * rec;
     M3 basis[4];
 #pragma unroll
-    for (int l = 0; l < 4; ++l) basis[l] = mm(mm(loadRot(b.vertexRot, idxAt(q, l)), loadBlockVec(U, l)), RsT);
+    for (int l = 0; l < 4; ++l) basis[l] = mm(mm(loadFrame(b.vertexRot, idxAt(q, l)), loadBlockVec(U, l)), RsT);
     const M3 R = loadRot(b.tetRot, t);
     float3 tg[4];
     corotatedGradient(b, src, t, q, R, tg);
@@ -2314,7 +2369,7 @@ __global__ void __launch_bounds__(kBlock, JGS2_SOLVE_MIN_BLOCKS)
       const uint32_t scene = b.vertexScene[v];
       const DevParams& p = pp[scene];
       if (!p.active || latched(p, &b.frames[scene])) continue;
-      storeRot(b.vertexRot, v, vertexFrame<true>(b, x, v, p.rotationEpsilon));
+      storeFrame(b.vertexRot, v, vertexFrame<true>(b, x, v, p.rotationEpsilon));
     }
     if (!gridBarrier(bar, spinLimit)) return;
     const uint32_t cb = colorOffsets[c], count = colorOffsets[c + 1] - cb;
@@ -2538,7 +2593,7 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
       // The stable iteration source is the accepted pose.
       b.pos[1][i] = make_float4(o.x, o.y, o.z, 1.0f);
       // Iteration-0 frames (and, for free vertices, the incident system).
-      if (isPinned(info)) storeRot(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
+      if (isPinned(info)) storeFrame(b.vertexRot, i, vertexFrame(b, b.pos[0], i, p.rotationEpsilon));
       else frameAndIncident(b, p, b.pos[0], i, info, p.rotationEpsilon);
       const float e = implicitEnergy(p, b, i, xyz(o), info);
       if (finiteS(e)) { acc.e0 += e; acc.e1 += e; }
@@ -2775,11 +2830,11 @@ __global__ void JGS2_CONV_BOUNDS convergenceKernel(Buffers b, const DevParams* _
       // deformation gradients (the accepted pose is the next source).
       if (nextRotations) {
         const M3 favg = total > 0.0f ? (1.0f / total) * avg : midentity();
-        storeRot(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, p.rotationEpsilon));
+        storeFrame(b.vertexRot, v, info.y == 0u ? midentity() : polarRotation(favg, p.rotationEpsilon));
         storeIncident(b.incident, v, comps[1], hess);
       }
     } else if (nextRotations) {
-      storeRot(b.vertexRot, v, vertexFrame(b, acc, v, p.rotationEpsilon));
+      storeFrame(b.vertexRot, v, vertexFrame(b, acc, v, p.rotationEpsilon));
     }
   }
   const ConvPartial blk = blockFold(part, smem, convCombine);

@@ -1956,7 +1956,11 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   {
     std::vector<float4> identity(3ull * nV);
     for (uint32_t v = 0; v < nV; ++v) {
+#if defined(JGS2_FRAME_QUAT) && JGS2_FRAME_QUAT
+      identity[3ull * v] = make_float4(0, 0, 0, 1);  // the identity quaternion
+#else
       identity[3ull * v] = make_float4(1, 0, 0, 0);
+#endif
       identity[3ull * v + 1] = make_float4(0, 1, 0, 0);
       identity[3ull * v + 2] = make_float4(0, 0, 1, 0);
     }
