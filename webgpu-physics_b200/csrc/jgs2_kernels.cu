@@ -33,6 +33,35 @@ namespace jgs2 {
 namespace {
 
 constexpr int kBlock = 128;
+
+// Checked build: device index checks in the gathers.  A failing check records
+// its site once (the host reports it at the next synchronisation as
+// JGS2_DEVICE_ERROR) and the gather skips the element, so the kernel never
+// reads out of bounds.  Compiled out otherwise.
+#ifndef JGS2_BOUNDS_CHECKS
+#define JGS2_BOUNDS_CHECKS 0
+#endif
+enum BoundsSite : uint32_t {
+  kSiteRecordTet = 1, kSiteRecordVertex = 2, kSiteIncidentTet = 3, kSiteTetVertex = 4, kSiteContactVertex = 5,
+  kSiteListVertex = 6,
+};
+#if JGS2_BOUNDS_CHECKS
+__device__ uint32_t gBoundsViolation;
+#endif
+__device__ __forceinline__ bool inBounds(uint64_t index, uint64_t limit, uint32_t site) {
+#if JGS2_BOUNDS_CHECKS
+  if (index < limit) return true;
+  atomicCAS(&gBoundsViolation, 0u, site);
+  return false;
+#else
+  (void)index; (void)limit; (void)site;
+  return true;
+#endif
+}
+__device__ __forceinline__ bool tetVerticesInBounds(const uint4& q, uint32_t V) {
+  return inBounds(q.x, V, kSiteTetVertex) && inBounds(q.y, V, kSiteTetVertex) && inBounds(q.z, V, kSiteTetVertex) &&
+         inBounds(q.w, V, kSiteTetVertex);
+}
 #ifndef JGS2_SOLVE_LANES
 #define JGS2_SOLVE_LANES 4
 #endif
@@ -69,6 +98,15 @@ __device__ __forceinline__ TetRec loadTet(const float4* __restrict__ tets, uint3
   r.mu = c.w;
   r.idx = q;
   return r;
+}
+
+// An incident-tet entry (tet * 4 + slot) and its record; false when a
+// checked build finds the tet or one of its vertices out of range.
+__device__ __forceinline__ bool incidentTetChecked(const float4* __restrict__ tets, uint32_t entry, uint32_t T,
+                                                   uint32_t V, TetRec* r) {
+  if (!inBounds(entry >> 2, T, kSiteIncidentTet)) return false;
+  *r = loadTet(tets, entry >> 2);
+  return tetVerticesInBounds(r->idx, V);
 }
 
 __device__ __forceinline__ float3 shapeGradient(const TetRec& r, uint32_t slot) {
@@ -402,20 +440,24 @@ __device__ __forceinline__ void frameAndIncident(const Buffers& b, const DevPara
 #if JGS2_CONV_LOOKAHEAD
   uint32_t nextEntry = info.y ? __ldg(&b.adjacency[info.x]) : 0u;
   TetRec nextRec;
-  if (info.y) nextRec = loadTet(b.tets, nextEntry >> 2);
+  bool nextOk = false;
+  if (info.y) nextOk = incidentTetChecked(b.tets, nextEntry, b.tetTotal, b.vertexTotal, &nextRec);
 #endif
   for (uint32_t a = 0; a < info.y; ++a) {
 #if JGS2_CONV_LOOKAHEAD
     const uint32_t entry = nextEntry;
     const TetRec r = nextRec;
+    const bool tetOk = nextOk;
     if (a + 1 < info.y) {
       nextEntry = __ldg(&b.adjacency[info.x + a + 1]);
-      nextRec = loadTet(b.tets, nextEntry >> 2);
+      nextOk = incidentTetChecked(b.tets, nextEntry, b.tetTotal, b.vertexTotal, &nextRec);
     }
 #else
     const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
-    const TetRec r = loadTet(b.tets, entry >> 2);
+    TetRec r;
+    const bool tetOk = incidentTetChecked(b.tets, entry, b.tetTotal, b.vertexTotal, &r);
 #endif
+    if (!tetOk) continue;
     const M3 F = deformationAt(r, x);
     const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
     const float3 g = shapeGradient(r, entry & 3u);
@@ -442,7 +484,8 @@ __device__ __forceinline__ M3 vertexFrame(const Buffers& b, const float4* __rest
   float total = 0.0f;
   for (uint32_t a = 0; a < info.y; ++a) {
     const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
-    const TetRec r = loadTet(b.tets, entry >> 2);
+    TetRec r;
+    if (!incidentTetChecked(b.tets, entry, b.tetTotal, b.vertexTotal, &r)) continue;
     avg = avg + r.vol * deformationAtT<kCoherent>(r, x);
     total += r.vol;
   }
@@ -697,6 +740,13 @@ __device__ __forceinline__ uint4 contactIndices(const Buffers& b, uint32_t c, ui
   uint4 q = __ldg(&b.contactIdx[c]);
   *type = q.w >> 31;
   q.w &= 0x7fffffffu;
+#if JGS2_BOUNDS_CHECKS
+  // An out-of-range candidate vertex is recorded and read as vertex 0.
+  if (!inBounds(q.x, b.vertexTotal, kSiteContactVertex)) q.x = 0;
+  if (!inBounds(q.y, b.vertexTotal, kSiteContactVertex)) q.y = 0;
+  if (!inBounds(q.z, b.vertexTotal, kSiteContactVertex)) q.z = 0;
+  if (!inBounds(q.w, b.vertexTotal, kSiteContactVertex)) q.w = 0;
+#endif
   return q;
 }
 
@@ -1769,6 +1819,10 @@ __device__ __forceinline__ void recordState(const Buffers& b, const DevParams& p
   st.w = 0.0f;
   // Headers hold global tet ids; out-of-range records were emptied at create.
   if (!(t != kEmptyTet && w > 0.0f)) return;
+  if (!inBounds(t, b.tetTotal, kSiteRecordTet) || !inBounds(idx.x, b.vertexTotal, kSiteRecordVertex) ||
+      !inBounds(idx.y, b.vertexTotal, kSiteRecordVertex) || !inBounds(idx.z, b.vertexTotal, kSiteRecordVertex) ||
+      !inBounds(idx.w, b.vertexTotal, kSiteRecordVertex))
+    return;
   const float4* U;
   if constexpr (kStaged) {
     r = tetFromSlot(staged->tet);
@@ -1858,7 +1912,9 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
       const uint32_t r = c / 11u, part = c - r * 11u;
       const uint32_t g = r / K, it = chunk * groupsPerBlock + g;
       if (it >= count) continue;
-      const size_t rec = static_cast<size_t>(list ? list[it] : it) * K + (r - g * K);
+      const uint32_t sv = list ? list[it] : it;
+      if (!inBounds(sv, b.vertexTotal, kSiteListVertex)) continue;
+      const size_t rec = static_cast<size_t>(sv) * K + (r - g * K);
       if (part < 2u) cpAsync16(&slots[r].head[part], &b.cubHead[2 * rec + part]);
       else cpAsync16(&slots[r].basis[part - 2u], &b.cubBasis[9 * rec + (part - 2u)]);
     }
@@ -1868,7 +1924,8 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
       const uint32_t r = c >> 2, part = c & 3u;
       if (chunk * groupsPerBlock + r / K >= count) continue;
       const uint4 head = slots[r].head[0];
-      if (head.x != kEmptyTet && __uint_as_float(head.y) > 0.0f) cpAsync16(&slots[r].tet[part], &b.tets[4ull * head.x + part]);
+      if (head.x != kEmptyTet && __uint_as_float(head.y) > 0.0f && inBounds(head.x, b.tetTotal, kSiteRecordTet))
+        cpAsync16(&slots[r].tet[part], &b.tets[4ull * head.x + part]);
     }
     cpAsyncWaitAll();
     __syncthreads();
@@ -1876,8 +1933,9 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
 #endif
   // One vertex per lane group; its scene selects the settings and records.
   const uint32_t item = chunk * groupsPerBlock + group;
-  const bool haveVertex = groupLane && item < count;
-  const uint32_t v = haveVertex ? (list ? list[item] : item) : 0u;
+  const uint32_t listed = (groupLane && item < count) ? (list ? list[item] : item) : 0u;
+  const bool haveVertex = groupLane && item < count && inBounds(listed, b.vertexTotal, kSiteListVertex);
+  const uint32_t v = haveVertex ? listed : 0u;
   const uint32_t scene = haveVertex ? b.vertexScene[v] : sScene;
   // Per-vertex outputs owned by lane 0.
   uint32_t status = kNonfinite, backtracks = 0, evals = 0;
@@ -2004,7 +2062,8 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
           for (uint32_t a = lane; a < info.y; a += W) {
             // ---- incident tetrahedron (jgs2-shader.ts:3097-3111) ----
             const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
-            const TetRec r = loadTet(b.tets, entry >> 2);
+            TetRec r;
+            if (!incidentTetChecked(b.tets, entry, b.tetTotal, b.vertexTotal, &r)) continue;
             const M3 F = deformationAtT<kCoherent>(r, src);
             const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
             const float3 g = shapeGradient(r, entry & 3u);
@@ -2126,21 +2185,25 @@ __device__ __forceinline__ void solveChunk(const Buffers& b, const DevParams* __
             // one's arithmetic (as in the convergence gather).
             uint32_t nextEntry = firstInc < info.y ? __ldg(&b.adjacency[info.x + firstInc]) : 0u;
             TetRec nextRec;
-            if (firstInc < info.y) nextRec = loadTet(b.tets, nextEntry >> 2);
+            bool nextOk = false;
+            if (firstInc < info.y) nextOk = incidentTetChecked(b.tets, nextEntry, b.tetTotal, b.vertexTotal, &nextRec);
 #endif
             for (uint32_t a = firstInc; a < info.y; a += W) {
               float J = 0.0f;
 #if JGS2_CONV_LOOKAHEAD
               const uint32_t entry = nextEntry;
               const TetRec r = nextRec;
+              const bool tetOk = nextOk;
               if (a + W < info.y) {
                 nextEntry = __ldg(&b.adjacency[info.x + a + W]);
-                nextRec = loadTet(b.tets, nextEntry >> 2);
+                nextOk = incidentTetChecked(b.tets, nextEntry, b.tetTotal, b.vertexTotal, &nextRec);
               }
 #else
               const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
-              const TetRec r = loadTet(b.tets, entry >> 2);
+              TetRec r;
+              const bool tetOk = incidentTetChecked(b.tets, entry, b.tetTotal, b.vertexTotal, &r);
 #endif
+              if (!tetOk) continue;
               const M3 F = deformationAtT<kCoherent>(r, src);
               const float I0 = frob(F, F);
               const float J0 = mdet(F);
@@ -2601,8 +2664,10 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
     }
     if (p.globalization && k < sr.T) {
       const TetRec r = loadTet(b.tets, sr.tOff + k);
-      const M3 F = deformationAt(r, b.pos[0]);
-      accumulateTet(acc, r, F, F);
+      if (tetVerticesInBounds(r.idx, b.vertexTotal)) {
+        const M3 F = deformationAt(r, b.pos[0]);
+        accumulateTet(acc, r, F, F);
+      }
     }
     if (p.cloth) {
       if (k < sr.C) accumulateClothTri(acc, loadClothTri(b.clothTris, sr.cOff + k), b.pos[0], b.pos[0], clothMaterial(p));
@@ -2654,7 +2719,7 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
   for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
     if (k < sr.T) {
       const TetRec r = loadTet(b.tets, sr.tOff + k);
-      accumulateTet(acc, r, deformationAt(r, src), deformationAt(r, tgt));
+      if (tetVerticesInBounds(r.idx, b.vertexTotal)) accumulateTet(acc, r, deformationAt(r, src), deformationAt(r, tgt));
     }
     if (k < sr.V) {
       const uint32_t i = sr.vOff + k;
@@ -2764,20 +2829,24 @@ __global__ void JGS2_CONV_BOUNDS convergenceKernel(Buffers b, const DevParams* _
       // one's arithmetic, so its latency overlaps the work.
       uint32_t nextEntry = info.y ? __ldg(&b.adjacency[info.x]) : 0u;
       TetRec nextRec;
-      if (info.y) nextRec = loadTet(b.tets, nextEntry >> 2);
+      bool nextOk = false;
+  if (info.y) nextOk = incidentTetChecked(b.tets, nextEntry, b.tetTotal, b.vertexTotal, &nextRec);
 #endif
       for (uint32_t a = 0; a < info.y; ++a) {
 #if JGS2_CONV_LOOKAHEAD
         const uint32_t entry = nextEntry;
         const TetRec r = nextRec;
+        const bool tetOk = nextOk;
         if (a + 1 < info.y) {
           nextEntry = __ldg(&b.adjacency[info.x + a + 1]);
-          nextRec = loadTet(b.tets, nextEntry >> 2);
+          nextOk = incidentTetChecked(b.tets, nextEntry, b.tetTotal, b.vertexTotal, &nextRec);
         }
 #else
         const uint32_t entry = __ldg(&b.adjacency[info.x + a]);
-        const TetRec r = loadTet(b.tets, entry >> 2);
+        TetRec r;
+        const bool tetOk = incidentTetChecked(b.tets, entry, b.tetTotal, b.vertexTotal, &r);
 #endif
+        if (!tetOk) continue;
         const M3 F = deformationAt(r, acc);
         const PiolaTerms pt = piolaTerms(F, r.lambda, r.mu);
         const float3 g = shapeGradient(r, entry & 3u);
@@ -3382,6 +3451,20 @@ int launchColoredSweep(const Buffers& b, const DevParams* p, float4* x, const ui
 }
 
 size_t sweepBarrierBytes() { return sizeof(SweepBarrier); }
+
+bool boundsChecked() { return JGS2_BOUNDS_CHECKS != 0; }
+
+cudaError_t takeBoundsViolation(uint32_t* site) {
+  *site = 0;
+#if JGS2_BOUNDS_CHECKS
+  cudaError_t e = cudaMemcpyFromSymbol(site, gBoundsViolation, sizeof(uint32_t));
+  if (e != cudaSuccess || *site == 0) return e;
+  const uint32_t zero = 0;
+  return cudaMemcpyToSymbol(gBoundsViolation, &zero, sizeof(uint32_t));
+#else
+  return cudaSuccess;
+#endif
+}
 
 uint32_t solveSharedBytes() {
   static int optin = -1;

@@ -148,6 +148,7 @@ struct Buffers {
   uint32_t* contactFlag;   // per candidate: active this iteration
   float4* contactGrad;     // per vertex: IPC gradient at the accepted pose
   uint32_t gateBlocks, convBlocks, sceneCount, contactCount;
+  uint32_t vertexTotal, tetTotal;  // vertices and tets over the scenes (checked builds bound indices by them)
   // IPC broad phase (contact surfaces; all null for static candidates, and
   // contactCount is then the candidate capacity of one iteration).  Rows:
   // one per vertex of a contact scene (vertex-triangle rows) and one per
@@ -277,6 +278,11 @@ constexpr int kOracleSummaryWords = 18;
 int launchOracleDiagnostics(const Buffers& b, const OracleParams& q, float4* tetRot, float4* tetMetric,
                             float4* vertexRecords, double* summary, cudaStream_t s);
 
+// Checked builds (JGS2_BOUNDS_CHECKS=1): the first device index check that
+// failed since the last call (a site number, 0 = none); the failing access
+// was skipped.  Reading resets it.  Always 0 in a build without checks.
+cudaError_t takeBoundsViolation(uint32_t* site);
+bool boundsChecked();
 // Vertices per solve block for cubature width K (0: K too large to cache).
 uint32_t solveGroupsPerBlock(uint32_t K);
 // Whether the solve caches records of width K in shared memory (else it

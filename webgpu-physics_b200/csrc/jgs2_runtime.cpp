@@ -1410,6 +1410,15 @@ jgs2_status stepCommon(jgs2_solver* s, uint32_t frames, int exactIterations, con
 // After a synchronisation: a broad-phase list that did not fit its capacity
 // (the iteration then listed nothing) fails the call.
 jgs2_status checkBroadPhase(Engine* s) {
+  if (jgs2::boundsChecked()) {
+    uint32_t site = 0;
+    CUDA_TRY(s, jgs2::takeBoundsViolation(&site));
+    if (site != 0)
+      return fail(s, JGS2_DEVICE_ERROR,
+                  format("A device index check failed (site %u); the out-of-range access was skipped and the step's "
+                         "result is invalid.",
+                         site));
+  }
   if (s->sweepLaunched) {
     // The persistent coloured sweep's error word (a barrier that gave up).
     uint32_t words[4];
@@ -1983,6 +1992,8 @@ jgs2_status buildEngine(Engine* sp, const std::vector<PreparedScene>& prep, int 
   b.gateBlocks = static_cast<uint32_t>(gateTable.size());
   b.convBlocks = static_cast<uint32_t>(convTable.size());
   b.sceneCount = S;
+  b.vertexTotal = static_cast<uint32_t>(V);
+  b.tetTotal = static_cast<uint32_t>(T);
   {
     double* gp = nullptr;
     double* cp = nullptr;

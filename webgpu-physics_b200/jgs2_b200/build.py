@@ -1,6 +1,7 @@
 """Build recipe of the native libraries (in-tree, into webgpu-physics_b200/lib).
 
   libjgs2.so        CUDA step for sm_100a + the C-ABI runtime (include/jgs2.h)
+  checked/libjgs2.so  the same with device index checks (JGS2_BOUNDS_CHECKS=1)
   libjgs2_scene.so  CPU scene builder / precompute (include/jgs2_scene.h)
 
 Run as `python -m jgs2_b200.build` from webgpu-physics_b200/ or through
@@ -8,6 +9,7 @@ __graft_entry__.build().  nvcc cross-compiles for sm_100a without a GPU.
 """
 from __future__ import annotations
 
+import concurrent.futures
 import os
 import shutil
 import subprocess
@@ -53,9 +55,15 @@ def _stale(target, sources) -> bool:
     return any(os.path.getmtime(s) > t for s in sources)
 
 
-def build_step_library(force=False, verbose=False) -> str:
-    os.makedirs(LIB, exist_ok=True)
-    target = os.path.join(LIB, "libjgs2.so")
+CHECKED_LIB = os.path.join(LIB, "checked")
+
+
+def build_step_library(force=False, verbose=False, checked=False) -> str:
+    """libjgs2.so; `checked` builds the variant with device index checks
+    (JGS2_BOUNDS_CHECKS=1) into lib/checked/."""
+    out_dir = CHECKED_LIB if checked else LIB
+    os.makedirs(out_dir, exist_ok=True)
+    target = os.path.join(out_dir, "libjgs2.so")
     sources = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cu", "jgs2_runtime.cpp", "jgs2_server.cpp")]
     headers = [os.path.join(CSRC, f) for f in ("jgs2_kernels.cuh", "jgs2_device.cuh", "jgs2_cloth.cuh",
                                                 "jgs2_contact.cuh")] + [
@@ -63,16 +71,19 @@ def build_step_library(force=False, verbose=False) -> str:
     if not force and not _stale(target, sources + headers):
         return target
     nvcc = _nvcc()
-    objs = []
+    objs, cmds = [], []
     for src in sources:
-        obj = os.path.join(LIB, os.path.basename(src) + ".o")
+        obj = os.path.join(out_dir, os.path.basename(src) + ".o")
         cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC,-pthread", "-I", INCLUDE,
-               "-I", CSRC, "-c", src, "-o", obj]
+               "-I", CSRC, *(["-DJGS2_BOUNDS_CHECKS=1"] if checked else []), "-c", src, "-o", obj]
         if src.endswith(".cpp"):
             cmd.insert(1, "-x")
             cmd.insert(2, "cu")
-        _run(cmd, verbose)
+        cmds.append(cmd)
         objs.append(obj)
+    # The translation units compile in parallel.
+    with concurrent.futures.ThreadPoolExecutor(len(cmds)) as pool:
+        list(pool.map(lambda c: _run(c, verbose), cmds))
     _run([nvcc, *ARCH, "-shared", "-o", target, *objs, "-lcudart", "-Xcompiler", "-pthread"], verbose)
     for obj in objs:
         os.remove(obj)
@@ -94,7 +105,15 @@ def build_scene_library(force=False, verbose=False) -> str:
 
 
 def build_all(force=False, verbose=False):
-    return [build_step_library(force, verbose), build_scene_library(force, verbose)]
+    with concurrent.futures.ThreadPoolExecutor(3) as pool:
+        jobs = [pool.submit(build_step_library, force, verbose), pool.submit(build_scene_library, force, verbose),
+                pool.submit(build_step_library, force, verbose, True)]
+        step, scene, checked = (j.result() for j in jobs)
+    # The checked directory is a complete library directory (JGS2_LIB_DIR).
+    dst = os.path.join(CHECKED_LIB, "libjgs2_scene.so")
+    if not os.path.exists(dst) or os.path.getmtime(dst) < os.path.getmtime(scene):
+        shutil.copy2(scene, dst)
+    return [step, scene, checked]
 
 
 if __name__ == "__main__":
