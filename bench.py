@@ -55,6 +55,8 @@ def parse_args():
                          "through the device broad phase; cloth: the 128x128 StVK sheet")
     ap.add_argument("--boxes", type=int, default=None, help="boxes of the trough (10) or boxes (20) workload")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serving workload")
+    ap.add_argument("--rate", type=float, default=2000.0,
+                    help="serving workload: mean Poisson arrival rate (requests/s); 2000 is the specified stream")
     ap.add_argument("--frames", type=int, default=600,
                     help="boxes workload: frames of the whole run, each timed and checked intersection-free")
     ap.add_argument("--preroll", type=int, default=None,
@@ -524,7 +526,7 @@ def serving_arm(args):
     build_s = time.perf_counter() - t0
     rng = np.random.default_rng(2000 + rank)
     n = args.requests
-    arrivals = np.cumsum(rng.exponential(1.0 / 2000.0, size=n))
+    arrivals = np.cumsum(rng.exponential(1.0 / args.rate, size=n))
     frames = rng.integers(1, 61, size=n)
     kind_draw = rng.integers(0, 3, size=n)
     size_draw = rng.integers(1, 5, size=n)
@@ -586,7 +588,7 @@ def serving_arm(args):
             "ms_per_step": 1e3 * makespan / n, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
             "dtype": "f32", "data": "synthetic (seeded)",
             "config": {
-                "workload": (f"serving stream: {n} requests, Poisson arrivals at a mean 2000/s (seed 2000), drawn "
+                "workload": (f"serving stream: {n} requests, Poisson arrivals at a mean {args.rate:g}/s (seed 2000), drawn "
                              "uniformly from a 20x4x4-hex cantilever at 1-4x resolution (stable Neo-Hookean E=1e5 "
                              "nu=0.4, K=6 patch-trained cubature, 10 exact Jacobi iterations per frame), the IPC "
                              "box trough with 1-20 boxes of 8^3 hexes (dHat 1e-3, 15 iterations per frame, device "
