@@ -48,11 +48,13 @@ def parse_args():
                     help="iterations per frame (default 20 for the cube, 10 for the batched bodies)")
     ap.add_argument("--schedule", default="jacobi", choices=["jacobi", "graph-colored-gauss-seidel"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
-    ap.add_argument("--workload", default="cube", choices=["cube", "batched", "serving", "trough", "boxes", "cloth"],
+    ap.add_argument("--workload", default="cube", choices=["cube", "batched", "serving", "trough", "boxes", "cloth",
+                                                    "precompute"],
                     help="cube: one large body (headline); batched: independent uneven bodies in one batch; "
                          "serving: a Poisson stream of step requests through the continuous-batching loop; "
                          "trough: the reference's IPC box trough; boxes: twenty 8^3-hex boxes in the V-trough "
-                         "through the device broad phase; cloth: the 128x128 StVK sheet")
+                         "through the device broad phase; cloth: the 128x128 StVK sheet; precompute: the cube's patch "
+                         "precompute with the cubature selection on the CPU threads and on the GPU")
     ap.add_argument("--boxes", type=int, default=None, help="boxes of the trough (10) or boxes (20) workload")
     ap.add_argument("--requests", type=int, default=400, help="requests of the serving workload")
     ap.add_argument("--rate", type=float, default=2000.0,
@@ -116,7 +118,8 @@ def batched_workload(count: int):
                                "spacing": 0.25},
                   "materials": {"soft": 5e4, "stiff": 5e6, "poisson": 0.4, "density": 1000.0},
                   "timestep": 1 / 60, "basis": {"method": "patch", "patch_radius": 2},
-                  "cubature": {"k": 6, "exact_complement": 0}, "solverSchedule": "jacobi"}
+                  "cubature": {"k": 6, "exact_complement": 0, "trainer": scenes.TRAINER_REVISION},
+                  "solverSchedule": "jacobi"}
     inp, cached = scenes.cached_input(cache_dir(), f"batched{count}", components,
                                       lambda: scenes.batched_bodies(count=count))
     return inp, inp.split_bodies(), cached
@@ -506,7 +509,7 @@ def serving_arm(args):
     def cached(prefix, builder, options, build):
         # The builder's name and options fingerprint every component: they
         # determine topology, materials, timestep and precompute.
-        desc = {"builder": builder, "options": options}
+        desc = {"builder": builder, "options": options, "trainer": scenes.TRAINER_REVISION}
         components = {c: desc for c in ("topology", "materials", "timestep", "basis", "cubature")}
         components["solverSchedule"] = "jacobi"
         return scenes.cached_input(cache_dir(), prefix, components, build)[0]
@@ -1008,6 +1011,52 @@ def boxes_run(args, inp, settings, iters, what, build_s, dist, world, rank, devi
     return 0
 
 
+def precompute_arm(args):
+    """The cube's patch precompute (K = 6, radius-2 patches) twice: the greedy
+    cubature selection on all CPU threads, then on the GPU.  Both must write
+    the same records bit for bit; the line reports both wall times."""
+    import numpy as np
+
+    from jgs2_b200 import scenes
+
+    def run(device):
+        c = args.cells
+        sc = scenes.Scene()
+        m = sc.add_material(1000.0, 1e6, 0.45, scenes.MATERIAL_STABLE_NEO_HOOKEAN)
+        sc.add_cuboid((c, c, c), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), m, 0, scenes.FACE_Y_MIN)
+        t0 = time.perf_counter()
+        st = sc.precompute(timestep=1 / 60, cubature_k=6, method=scenes.PRECOMPUTE_PATCH, patch_radius=2,
+                           selection_device=device)
+        seconds = time.perf_counter() - t0
+        arrays = sc.pack().arrays()
+        return seconds, st, arrays
+
+    import torch
+
+    torch.cuda.init()  # the CUDA context exists before either timed run, as in a process that steps scenes
+    torch.cuda.synchronize()
+    cpu_s, cpu_st, cpu_arrays = run(scenes.SELECTION_CPU)
+    gpu_s, gpu_st, gpu_arrays = run(scenes.SELECTION_GPU)
+    same = sorted(cpu_arrays) == sorted(gpu_arrays) and all(
+        np.array_equal(cpu_arrays[k], gpu_arrays[k]) for k in cpu_arrays)
+    line = {
+        "metric": "patch precompute wall time", "value": round(gpu_s, 3), "unit": "s", "higher_is_better": False,
+        "n_gpus": 1, "data": "synthetic",
+        "config": {"workload": (f"unit cube {args.cells}^3 hexes x6 tets, stable Neo-Hookean E=1e6 nu=0.45, "
+                                f"patch precompute K=6 radius 2, 12 refinement passes"),
+                   "training_classes": gpu_st["training_classes"], "source_vertices": gpu_st["source_vertices"]},
+        "cpu_selection_seconds": round(cpu_s, 3), "gpu_selection_seconds": round(gpu_s, 3),
+        "training_seconds": {"cpu_selection": round(cpu_st["training_seconds"], 3),
+                             "gpu_selection": round(gpu_st["training_seconds"], 3)},
+        "gpu_selection_call_seconds": round(gpu_st["selection_seconds"], 3),
+        "speedup": round(cpu_s / gpu_s, 2), "cpu_threads": os.cpu_count(),
+        "selection_on_gpu": gpu_st["selection_on_gpu"], "selection_batches": gpu_st["selection_batches"],
+        "records_bitwise_equal": bool(same), "max_residual": gpu_st["max_residual"],
+    }
+    print(json.dumps(line), flush=True)
+    return 0 if same and cpu_st["max_residual"] == gpu_st["max_residual"] else 1
+
+
 def main():
     args = parse_args()
     if args.impl == "reference":
@@ -1018,6 +1067,8 @@ def main():
         return serving_arm(args)
     if args.workload in ("trough", "boxes", "cloth"):
         return scene_arm(args)
+    if args.workload == "precompute":
+        return precompute_arm(args)
     return ours_arm(args)
 
 

@@ -37,6 +37,14 @@ typedef struct jgs2_scene jgs2_scene;
 #define JGS2_PRECOMPUTE_EXACT 0u
 #define JGS2_PRECOMPUTE_PATCH 1u
 
+/* Where the greedy cubature selection (the nonnegative least-squares search,
+ * src/simulation/cpu/cubature.ts:387-690) runs.  Both give the same records
+ * bit for bit; the GPU runs every training problem of a batch at once on the
+ * current CUDA device. */
+#define JGS2_SELECTION_CPU 0u
+#define JGS2_SELECTION_GPU 1u   /* error when no CUDA device is visible */
+#define JGS2_SELECTION_AUTO 2u  /* the GPU when a CUDA device is visible */
+
 /* Face bits for generated cuboids: a vertex is pinned when it lies on any
  * selected face (the reference passes a predicate, src/simulation/cpu/mesh.ts:142). */
 #define JGS2_FACE_X_MIN (1u << 0)
@@ -63,6 +71,7 @@ typedef struct jgs2_precompute_options {
    * assembleStableNeoHookeanJGS2LocalSystem, nonlinear-cubature-training.ts:
    * 620-660).  cubature_k must then be at least the candidate count. */
   uint32_t exact_complement;
+  uint32_t selection_device;   /* JGS2_SELECTION_*, default JGS2_SELECTION_AUTO */
 } jgs2_precompute_options;
 
 typedef struct jgs2_precompute_stats {
@@ -75,6 +84,10 @@ typedef struct jgs2_precompute_stats {
   uint32_t vertices_over_tolerance; /* residual > 1% */
   uint32_t reduced_amplitude_classes; /* corpora whose amplitude was halved */
   double seconds;
+  uint32_t selection_on_gpu;   /* 1 when the selections ran on the GPU */
+  uint32_t selection_batches;  /* GPU selection launches */
+  double training_seconds;     /* wall time of the training phase (systems, selections, records) */
+  double selection_seconds;    /* wall time inside the GPU selection calls (copies and kernel) */
 } jgs2_precompute_stats;
 
 jgs2_scene* jgs2_scene_new(void);

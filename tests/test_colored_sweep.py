@@ -76,3 +76,21 @@ def test_barrier_timeout_is_reported_and_the_device_stays_usable():
     t.stepExactIterations(2)
     assert np.isfinite(t.readPositions()).all()
     t.destroy()
+
+
+def test_persistent_sweep_with_cloth():
+    # The cloth instantiation of the persistent sweep (membrane and hinge
+    # gathers read positions other blocks write) against the launches.
+    inp = scenes.cloth_drape(cells=6, prefold=False, pinned_columns=(0, 6))
+    s = dict(timestep=1 / 120, gravity=(0.0, -9.81, 0.0), floorStiffness=0.0, parityMode=True, schedule=1)
+    a = _with_env("JGS2_COLOR_SWEEP", "persistent", lambda: solver.JGS2GpuSolver.create(inp, s))
+    b = solver.JGS2GpuSolver.create(inp, s)
+    assert a.scheduleColorCount > 1
+    la, lb = a.kernelLaunchCount(), b.kernelLaunchCount()
+    a.stepExactIterations(5)
+    b.stepExactIterations(5)
+    assert a.kernelLaunchCount() - la < b.kernelLaunchCount() - lb  # the sweep ran
+    err = np.abs(a.readPositions() - b.readPositions()).max() / inp.bbox_diagonal()
+    assert err <= 1e-5, err
+    a.destroy()
+    b.destroy()

@@ -187,6 +187,25 @@ def test_patch_precompute_shares_classes():
     solver.validate_input(inp)
 
 
+def test_selection_device_option():
+    # The selection place is validated; a GPU selection asked for where no
+    # CUDA device is visible fails with a message, and AUTO falls back to the
+    # CPU threads there.
+    import torch
+
+    sc = scenes.Scene()
+    m = sc.add_material(1000.0, 1e6, 0.45)
+    sc.add_cuboid((3, 2, 2), (0.0, 0.0, 0.0), (0.3, 0.2, 0.2), m, 0, scenes.FACE_X_MIN)
+    with pytest.raises(_ffi.JGS2Error, match="selection_device"):
+        sc.precompute(timestep=1 / 60, selection_device=3)
+    if torch.cuda.is_available():
+        pytest.skip("a CUDA device is visible")
+    with pytest.raises(_ffi.JGS2Error, match="no CUDA device"):
+        sc.precompute(timestep=1 / 60, selection_device=scenes.SELECTION_GPU)
+    st = sc.precompute(timestep=1 / 60, selection_device=scenes.SELECTION_AUTO)
+    assert st["selection_on_gpu"] == 0 and st["source_vertices"] > 0
+
+
 def test_lumped_masses_sum_to_body_mass(small_bar):
     total = float(small_bar.vertex_rest.reshape(-1, 4)[:, 3].sum())
     assert total == pytest.approx(1000.0 * 0.3 * 0.2 * 0.1, rel=1e-5)

@@ -266,3 +266,29 @@ def test_config2_bodies_in_one_batch_vs_oracles():
           f"{worst64:.2e} of a body's bbox diagonal")
     assert worst32 <= 1e-3 and worst64 <= 1e-3
     batch.destroy()
+
+
+@pytest.mark.parametrize("schedule", [0, 1])
+def test_wide_records_recomputed_in_the_line_search(schedule):
+    # An exact complement (up to 192 records per vertex here) is wider than
+    # the solve's shared-memory record cache, so the line search recomputes
+    # each record's state; the frame must still match the oracle.
+    sc = scenes.Scene()
+    m = sc.add_material(1000.0, 1e6, 0.45)
+    sc.add_cuboid((6, 6, 6), (0.0, 0.0, 0.0), (1.0, 1.0, 1.0), m, 0, scenes.FACE_Y_MIN)
+    st = sc.precompute(timestep=1 / 60, cubature_k=256, exact_complement=1, method=scenes.PRECOMPUTE_PATCH,
+                       patch_radius=1)
+    sc.precompute(timestep=1 / 60, cubature_k=st["max_records_per_vertex"], exact_complement=1,
+                  method=scenes.PRECOMPUTE_PATCH, patch_radius=1)
+    inp = sc.pack()
+    assert inp.cubature_k > 68
+    s = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=8,
+             schedule=schedule)
+    gpu = solver.JGS2GpuSolver.create(inp, _camel(s))
+    cpu = O.OracleSolver(inp, s, precision=32)
+    gpu.stepExactIterations(8)
+    cpu.step_exact_iterations(8)
+    np.testing.assert_array_equal(_accepted(gpu.readGlobalizationDiagnostics()["history"], 8),
+                                  _accepted(cpu.read("history"), 8))
+    assert _error(inp, gpu.readPositions(), cpu.read("positions")) <= POSITION_TOL
+    gpu.destroy()

@@ -17,19 +17,19 @@
 #include <chrono>
 #include <cstring>
 #include <functional>
+#include <memory>
 #include <numeric>
 #include <stdexcept>
 #include <unordered_map>
 
 #include "scene_internal.hpp"
+#include "select_gpu.hpp"
 
 namespace jgs2scene {
 namespace {
 
 constexpr double kMinimumPoseDeterminant = 0.5;        // nonlinear-cubature.ts:24
 constexpr uint32_t kValidationOnlyModes = 4;           // nonlinear-cubature.ts:14
-constexpr double kResidualTolerance = 0.01;            // nonlinear-cubature-training.ts:23
-constexpr double kMatrixEpsilon = 1e-14;               // math.ts:1
 constexpr int kLinearRefinementPasses = 4;             // cubature.ts:52
 
 // ---- dense linear algebra -------------------------------------------------
@@ -70,37 +70,6 @@ void solveCholesky(const std::vector<double>& L, int n, const double* rhs, doubl
     for (int c = r + 1; c < n; ++c) v -= L[static_cast<size_t>(c) * n + r] * x[c];
     x[r] = v / L[static_cast<size_t>(r) * n + r];
   }
-}
-
-// solveDenseLinearSystem (src/simulation/cpu/math.ts:134-199): partial
-// pivoting, absolute pivot floor 1e-14.
-bool solveDense(double* a, double* b, int n) {
-  for (int p = 0; p < n; ++p) {
-    int best = p;
-    double bestMag = std::fabs(a[p * n + p]);
-    for (int r = p + 1; r < n; ++r) {
-      const double m = std::fabs(a[r * n + p]);
-      if (m > bestMag) { bestMag = m; best = r; }
-    }
-    if (bestMag <= kMatrixEpsilon || !std::isfinite(bestMag)) return false;
-    if (best != p) {
-      for (int c = p; c < n; ++c) std::swap(a[p * n + c], a[best * n + c]);
-      std::swap(b[p], b[best]);
-    }
-    const double d = a[p * n + p];
-    for (int r = p + 1; r < n; ++r) {
-      const double f = a[r * n + p] / d;
-      a[r * n + p] = 0;
-      for (int c = p + 1; c < n; ++c) a[r * n + c] -= f * a[p * n + c];
-      b[r] -= f * b[p];
-    }
-  }
-  for (int r = n - 1; r >= 0; --r) {
-    double v = b[r];
-    for (int c = r + 1; c < n; ++c) v -= a[r * n + c] * b[c];
-    b[r] = v / a[r * n + r];
-  }
-  return true;
 }
 
 double dotv(const double* a, const double* b, size_t n) {
@@ -557,50 +526,12 @@ void prepareTraining(Context& ctx, const jgs2_precompute_options& opt, bool line
   else buildCorpus(ctx, opt);
 }
 
-// ---- nonnegative least squares over small column sets ---------------------
+// ---- greedy nonnegative selection ------------------------------------------
 
-struct Gram {
-  int k = 0;
-  double G[12][12];
-  double b[12];
-  double tt;
-};
-
-// solveSmallNnls (src/simulation/cpu/cubature.ts:387-440): exhaustive active
-// set search; errors evaluated from the Gram matrix.
-double smallNnls(const Gram& g, double* w) {
-  const int k = g.k;
-  double best = g.tt;
-  for (int i = 0; i < k; ++i) w[i] = 0;
-  double A[144], rhs[12], cw[12];
-  int active[12];
-  for (int mask = 1; mask < (1 << k); ++mask) {
-    int d = 0;
-    for (int c = 0; c < k; ++c)
-      if (mask & (1 << c)) active[d++] = c;
-    for (int r = 0; r < d; ++r) {
-      rhs[r] = g.b[active[r]];
-      for (int c = 0; c < d; ++c) A[r * d + c] = g.G[active[r]][active[c]];
-    }
-    if (!solveDense(A, rhs, d)) continue;
-    bool neg = false;
-    for (int r = 0; r < d; ++r) neg |= rhs[r] < -1e-10;
-    if (neg) continue;
-    for (int c = 0; c < k; ++c) cw[c] = 0;
-    for (int r = 0; r < d; ++r) cw[active[r]] = std::max(0.0, rhs[r]);
-    double err = g.tt;
-    for (int r = 0; r < k; ++r) {
-      if (cw[r] == 0) continue;
-      err -= 2 * cw[r] * g.b[r];
-      for (int c = 0; c < k; ++c) err += cw[r] * g.G[r][c] * cw[c];
-    }
-    if (err < best - 1e-14 * std::max(1.0, best)) {
-      best = err;
-      for (int c = 0; c < k; ++c) w[c] = cw[c];
-    }
-  }
-  return best;
-}
+using jgs2select::Gram;
+using jgs2select::kMaxColumns;
+using jgs2select::kResidualTolerance;
+using jgs2select::maxd;
 
 struct Selection {
   std::vector<int> tets;  // local tet ids in selection order
@@ -608,127 +539,126 @@ struct Selection {
   double residual = 0;    // normalized
 };
 
-// selectGreedyNonnegativeColumns (src/simulation/cpu/cubature.ts:508-690)
-// followed by the small-mesh subset audit and positive-weight filter
-// (nonlinear-cubature-training.ts:731-792).
-Selection greedySelect(const std::vector<std::vector<double>>& cols, const std::vector<double>& t,
-                       int maxColumns, int refinementPasses) {
-  const size_t rows = t.size();
-  Selection out;
-  const double tt = dotv(t.data(), t.data(), rows);
-  const double tn = std::sqrt(tt);
-  if (tn <= 1e-12) return out;
-  std::vector<int> cand;
-  for (size_t c = 0; c < cols.size(); ++c)
-    if (dotv(cols[c].data(), cols[c].data(), rows) > 1e-18) cand.push_back(static_cast<int>(c));
-  const int limit = std::min<int>(maxColumns, static_cast<int>(cand.size()));
-  if (limit > 12) throw std::runtime_error("Exhaustive NNLS supports at most 12 selected columns.");
-  if (cand.empty() || limit == 0) { out.residual = 1; return out; }
-  const size_t C = cand.size();
-  std::vector<double> cc(C), ct(C);
-  for (size_t i = 0; i < C; ++i) {
-    cc[i] = dotv(cols[cand[i]].data(), cols[cand[i]].data(), rows);
-    ct[i] = dotv(cols[cand[i]].data(), t.data(), rows);
+// A training system ready for selection: one column per local tetrahedron
+// (its reduced gradients stacked over the training poses) and the summed
+// target, with the selection's column limit and refinement passes.
+struct Training {
+  std::vector<std::vector<double>> cols;
+  std::vector<double> target;
+  int maxColumns = 0;
+  int passes = 0;
+  bool audit = false;  // small-mesh subset audit after the selection
+};
+
+// The candidate filter of selectGreedyNonnegativeColumns (cubature.ts:
+// 508-560): columns with |c|² > 1e-18 in index order, their squared norms and
+// target dot products.
+struct Candidates {
+  enum Status { kReady, kFlatTarget, kEmpty } status = kReady;
+  double tt = 0, tn = 0;
+  int limit = 0;
+  std::vector<int> ids;
+  std::vector<double> cc, ct;
+};
+
+Candidates candidates(const Training& tr) {
+  Candidates c;
+  const size_t rows = tr.target.size();
+  c.tt = dotv(tr.target.data(), tr.target.data(), rows);
+  c.tn = std::sqrt(c.tt);
+  if (c.tn <= 1e-12) {
+    c.status = Candidates::kFlatTarget;
+    return c;
   }
-  std::vector<int> sel;                       // indices into cand
-  std::vector<std::vector<double>> dsel;      // dsel[s][i] = col(sel[s]) . col(cand[i])
-  auto addDots = [&](int ci) {
-    std::vector<double> d(C);
-    for (size_t i = 0; i < C; ++i) d[i] = dotv(cols[cand[ci]].data(), cols[cand[i]].data(), rows);
-    return d;
-  };
-  std::vector<double> weights;
-  double err = tt;
-  auto fillGram = [&](Gram& g, const std::vector<int>& set, const std::vector<const std::vector<double>*>& rowsDot) {
-    g.k = static_cast<int>(set.size());
-    g.tt = tt;
-    for (int r = 0; r < g.k; ++r) {
-      g.b[r] = ct[set[r]];
-      for (int c = 0; c < g.k; ++c) g.G[r][c] = (*rowsDot[r])[set[c]];
+  for (size_t i = 0; i < tr.cols.size(); ++i) {
+    const double n2 = dotv(tr.cols[i].data(), tr.cols[i].data(), rows);
+    if (n2 > 1e-18) {
+      c.ids.push_back(static_cast<int>(i));
+      c.cc.push_back(n2);
     }
+  }
+  c.limit = std::min<int>(tr.maxColumns, static_cast<int>(c.ids.size()));
+  if (c.limit > kMaxColumns) throw std::runtime_error("Exhaustive NNLS supports at most 12 selected columns.");
+  if (c.ids.empty() || c.limit == 0) {
+    c.status = Candidates::kEmpty;
+    return c;
+  }
+  c.ct.resize(c.ids.size());
+  for (size_t i = 0; i < c.ids.size(); ++i) c.ct[i] = dotv(tr.cols[c.ids[i]].data(), tr.target.data(), rows);
+  return c;
+}
+
+// Greedy growth (each step appends the candidate whose exhaustive NNLS fit
+// leaves the smallest residual) until the limit or a residual below 1%, then
+// refinement passes that swap one chosen slot for an unchosen candidate while
+// that helps (selectGreedyNonnegativeColumns, cubature.ts:508-690).  The
+// trial systems, the NNLS and the scan rule are cubature_select.hpp's, shared
+// with the GPU selection.
+SelectOutput selectOnCpu(const Training& tr, const Candidates& cs) {
+  using namespace jgs2select;
+  SelectOutput ch;
+  if (cs.status != Candidates::kReady) return ch;
+  const size_t rows = tr.target.size(), C = cs.ids.size();
+  const int n = static_cast<int>(C);
+  std::vector<double> dsel(kMaxColumns * C);
+  auto setRow = [&](int slot) {
+    const double* a = tr.cols[cs.ids[ch.sel[slot]]].data();
+    for (size_t i = 0; i < C; ++i) dsel[slot * C + i] = dotv(a, tr.cols[cs.ids[i]].data(), rows);
   };
-  std::vector<int> trial;
-  std::vector<const std::vector<double>*> trialDots;
-  for (int step = 0; step < limit; ++step) {
+  auto chosen = [&](int ci) {
+    for (int s = 0; s < ch.count; ++s)
+      if (ch.sel[s] == ci) return true;
+    return false;
+  };
+  Gram<kMaxColumns> g;
+  double w[kMaxColumns];
+  double err = cs.tt;
+  for (int step = 0; step < cs.limit; ++step) {
+    const int k = ch.count;
     int best = -1;
-    double bestErr = err, bestW[12];
-    for (size_t ci = 0; ci < C; ++ci) {
-      if (std::find(sel.begin(), sel.end(), static_cast<int>(ci)) != sel.end()) continue;
-      trial = sel;
-      trial.push_back(static_cast<int>(ci));
-      Gram g;
-      g.k = static_cast<int>(trial.size());
-      g.tt = tt;
-      for (int r = 0; r < g.k; ++r) {
-        g.b[r] = ct[trial[r]];
-        for (int c = 0; c < g.k; ++c) {
-          const int a = trial[r], b = trial[c];
-          if (r < g.k - 1) g.G[r][c] = dsel[r][b];
-          else if (c < g.k - 1) g.G[r][c] = dsel[c][a];
-          else g.G[r][c] = cc[a];
-        }
-      }
-      double w[12];
+    double bestErr = err;
+    for (int ci = 0; ci < n; ++ci) {
+      if (chosen(ci)) continue;
+      swapGram(g, ch.sel, k + 1, k, ci, dsel.data(), C, cs.cc.data(), cs.ct.data(), cs.tt);
       const double e = smallNnls(g, w);
-      const double tol = 1e-14 * std::max(1.0, bestErr);
-      if (e < bestErr - tol || (std::fabs(e - bestErr) <= tol && best >= 0 && cand[ci] < cand[best])) {
-        best = static_cast<int>(ci);
+      if (improves(e, bestErr, best >= 0, ci, best)) {
+        best = ci;
         bestErr = e;
-        std::memcpy(bestW, w, sizeof(double) * g.k);
       }
     }
     if (best < 0) break;
-    sel.push_back(best);
-    dsel.push_back(addDots(best));
-    weights.assign(bestW, bestW + sel.size());
+    swapGram(g, ch.sel, k + 1, k, best, dsel.data(), C, cs.cc.data(), cs.ct.data(), cs.tt);
+    smallNnls(g, ch.weights);
+    ch.sel[k] = best;
+    ch.count = k + 1;
+    setRow(k);
     err = bestErr;
-    if (std::sqrt(std::max(err, 0.0)) / tn < kResidualTolerance) break;
+    if (std::sqrt(maxd(err, 0.0)) / cs.tn < kResidualTolerance) break;
   }
-  for (int pass = 0; pass < refinementPasses && !sel.empty(); ++pass) {
+  for (int pass = 0; pass < tr.passes && ch.count > 0; ++pass) {
+    const int k = ch.count;
     int rslot = -1, rcand = -1;
-    double rerr = err, rw[12];
-    const int k = static_cast<int>(sel.size());
+    double rerr = err;
     for (int slot = 0; slot < k; ++slot) {
-      for (size_t ci = 0; ci < C; ++ci) {
-        if (std::find(sel.begin(), sel.end(), static_cast<int>(ci)) != sel.end()) continue;
-        Gram g;
-        g.k = k;
-        g.tt = tt;
-        for (int r = 0; r < k; ++r) {
-          const int a = r == slot ? static_cast<int>(ci) : sel[r];
-          g.b[r] = ct[a];
-          for (int c = 0; c < k; ++c) {
-            const int b = c == slot ? static_cast<int>(ci) : sel[c];
-            if (r != slot) g.G[r][c] = dsel[r][b];
-            else if (c != slot) g.G[r][c] = dsel[c][a];
-            else g.G[r][c] = cc[a];
-          }
-        }
-        double w[12];
+      for (int ci = 0; ci < n; ++ci) {
+        if (chosen(ci)) continue;
+        swapGram(g, ch.sel, k, slot, ci, dsel.data(), C, cs.cc.data(), cs.ct.data(), cs.tt);
         const double e = smallNnls(g, w);
-        const double tol = 1e-14 * std::max(1.0, rerr);
-        if (e < rerr - tol || (std::fabs(e - rerr) <= tol && rcand >= 0 && cand[ci] < cand[rcand])) {
+        if (improves(e, rerr, rcand >= 0, ci, rcand)) {
           rslot = slot;
-          rcand = static_cast<int>(ci);
+          rcand = ci;
           rerr = e;
-          std::memcpy(rw, w, sizeof(double) * k);
         }
       }
     }
     if (rslot < 0) break;
-    sel[rslot] = rcand;
-    dsel[rslot] = addDots(rcand);
-    weights.assign(rw, rw + k);
+    swapGram(g, ch.sel, k, rslot, rcand, dsel.data(), C, cs.cc.data(), cs.ct.data(), cs.tt);
+    smallNnls(g, ch.weights);
+    ch.sel[rslot] = rcand;
+    setRow(rslot);
     err = rerr;
   }
-  for (size_t i = 0; i < sel.size(); ++i) out.tets.push_back(cand[sel[i]]);
-  out.weights = weights;
-  // Direct residual of the chosen fit.
-  std::vector<double> res(t);
-  for (size_t i = 0; i < out.tets.size(); ++i)
-    for (size_t r = 0; r < rows; ++r) res[r] -= cols[out.tets[i]][r] * out.weights[i];
-  out.residual = std::sqrt(dotv(res.data(), res.data(), rows)) / tn;
-  return out;
+  return ch;
 }
 
 // Exhaustive subset audit for meshes of at most 12 tetrahedra
@@ -744,15 +674,15 @@ void subsetAudit(const std::vector<std::vector<double>>& cols, const std::vector
   std::vector<int> subset;
   std::function<void(int)> visit = [&](int next) {
     if (static_cast<int>(subset.size()) == size) {
-      Gram g;
+      Gram<kMaxColumns> g;
       g.k = size;
       g.tt = tt;
       for (int r = 0; r < size; ++r) {
         g.b[r] = dotv(cols[subset[r]].data(), t.data(), rows);
         for (int c = 0; c < size; ++c) g.G[r][c] = dotv(cols[subset[r]].data(), cols[subset[c]].data(), rows);
       }
-      double w[12];
-      smallNnls(g, w);
+      double w[kMaxColumns];
+      jgs2select::smallNnls(g, w);
       std::vector<double> res(t);
       for (int i = 0; i < size; ++i)
         for (size_t r = 0; r < rows; ++r) res[r] -= cols[subset[i]][r] * w[i];
@@ -774,31 +704,81 @@ void subsetAudit(const std::vector<std::vector<double>>& cols, const std::vector
   visit(0);
 }
 
+// The chosen tetrahedra and weights with the fit's direct residual, then the
+// subset audit where it applies.
+Selection finishSelection(const Training& tr, const Candidates& cs, const SelectOutput& ch) {
+  Selection out;
+  if (cs.status == Candidates::kEmpty) out.residual = 1;
+  if (cs.status == Candidates::kReady) {
+    for (int i = 0; i < ch.count; ++i) {
+      out.tets.push_back(cs.ids[ch.sel[i]]);
+      out.weights.push_back(ch.weights[i]);
+    }
+    const size_t rows = tr.target.size();
+    std::vector<double> res(tr.target);
+    for (size_t i = 0; i < out.tets.size(); ++i)
+      for (size_t r = 0; r < rows; ++r) res[r] -= tr.cols[out.tets[i]][r] * out.weights[i];
+    out.residual = std::sqrt(dotv(res.data(), res.data(), rows)) / cs.tn;
+  }
+  if (tr.audit) subsetAudit(tr.cols, tr.target, tr.maxColumns, out);
+  return out;
+}
+
+// The selection's input on the GPU: the candidate columns row-major.
+std::vector<double> candidateRows(const Training& tr, const Candidates& cs) {
+  const size_t rows = tr.target.size(), C = cs.ids.size();
+  std::vector<double> out(rows * C);
+  for (size_t i = 0; i < C; ++i) {
+    const double* col = tr.cols[cs.ids[i]].data();
+    for (size_t r = 0; r < rows; ++r) out[r * C + i] = col[r];
+  }
+  return out;
+}
+
 struct LocalRecord {
   int tet;  // local tet id
   double weight;
   std::array<double, 36> basis;
 };
 
+// Records of the positive weights (nonlinear-cubature-training.ts:785-792),
+// each with the four vertices' basis blocks.
+void keepPositive(const Problem& pb, const std::vector<double>& ubar, const Selection& sel,
+                  std::vector<LocalRecord>& records) {
+  for (size_t i = 0; i < sel.tets.size(); ++i) {
+    if (!(sel.weights[i] > 1e-10)) continue;
+    LocalRecord rec;
+    rec.tet = sel.tets[i];
+    rec.weight = sel.weights[i];
+    for (int l = 0; l < 4; ++l) {
+      const uint32_t v = pb.tets[4ull * rec.tet + l];
+      for (int e = 0; e < 9; ++e) rec.basis[l * 9 + e] = ubar[9ull * v + e];
+    }
+    records.push_back(rec);
+  }
+}
+
 // selectCubatureSamples (src/simulation/cpu/cubature.ts:714-820): one column
 // per tetrahedron holding, at every training pose, its reduced gradient
 // (evaluateReducedTetGradient, cubature.ts:312-369: rest stiffness times the
 // pose plus the tetrahedron's share of the inertia, projected by the exact
 // basis, less the source slot's own row); per-pose normalisation by the norm
-// of the summed target; greedy nonnegative selection; positive weights kept.
-double trainLinear(const Context& ctx, uint32_t s, const std::vector<double>& ubar,
-                   const jgs2_precompute_options& opt, std::vector<LocalRecord>& records);
+// of the summed target.  False when there is nothing to fit.
+bool linearTraining(const Context& ctx, uint32_t s, const std::vector<double>& ubar,
+                    const jgs2_precompute_options& opt, Training& tr);
 
-// computeExactVertexBasis (precompute.ts:141-206) + the training for one
-// source vertex (selectStableNeoHookeanCubatureSamples,
-// nonlinear-cubature-training.ts:689-843).
-double trainSource(const Context& ctx, uint32_t s, const jgs2_precompute_options& opt,
-                   std::vector<LocalRecord>& records) {
+// computeExactVertexBasis (precompute.ts:141-206) and the training system of
+// one source vertex (selectStableNeoHookeanCubatureSamples,
+// nonlinear-cubature-training.ts:689-843, or the co-rotated linear
+// training).  Returns false when the source is finished without a selection
+// (the exact complement's records, or nothing to fit).
+bool buildTraining(const Context& ctx, uint32_t s, const jgs2_precompute_options& opt, std::vector<double>& ubar,
+                   Training& tr, std::vector<LocalRecord>& records) {
   const Problem& pb = *ctx.pb;
   const int n = ctx.n;
   const int sb = ctx.dof[s];
   records.clear();
-  if (sb < 0) return 0;
+  if (sb < 0) return false;
   // Exact basis Ubar = H^-1 S^T (S H^-1 S^T)^-1, one 3x3 block per vertex.
   std::vector<double> X(static_cast<size_t>(n) * 3, 0.0), rhs(n), sol(n);
   for (int c = 0; c < 3; ++c) {
@@ -812,7 +792,7 @@ double trainSource(const Context& ctx, uint32_t s, const jgs2_precompute_options
     for (int c = 0; c < 3; ++c)
       comp[r * 3 + c] = 0.5 * (X[static_cast<size_t>(sb + r) * 3 + c] + X[static_cast<size_t>(sb + c) * 3 + r]);
   if (!inv3(comp, schur)) throw std::runtime_error("Cannot invert a singular 3 by 3 matrix.");
-  std::vector<double> ubar(9ull * pb.Vp, 0.0);
+  ubar.assign(9ull * pb.Vp, 0.0);
   for (uint32_t v = 0; v < pb.Vp; ++v) {
     const int b = ctx.dof[v];
     if (b < 0) continue;
@@ -835,14 +815,16 @@ double trainSource(const Context& ctx, uint32_t s, const jgs2_precompute_options
       }
       records.push_back(rec);
     }
-    return 0.0;
+    return false;
   }
-  if (ctx.linear) return trainLinear(ctx, s, ubar, opt, records);
+  if (ctx.linear) return linearTraining(ctx, s, ubar, opt, tr);
   // Stacked training system (buildStackedTrainingSystem,
   // nonlinear-cubature-training.ts:473-552) with per-pose normalisation.
   const int P = ctx.poses;
-  std::vector<std::vector<double>> cols(pb.Tp, std::vector<double>(3ull * P, 0.0));
-  std::vector<double> target(3ull * P, 0.0);
+  std::vector<std::vector<double>>& cols = tr.cols;
+  std::vector<double>& target = tr.target;
+  cols.assign(pb.Tp, std::vector<double>(3ull * P, 0.0));
+  target.assign(3ull * P, 0.0);
   std::vector<double> B(9ull * pb.Vp);
   std::vector<double> rem(3ull * pb.Tp);
   for (int p = 0; p < P; ++p) {
@@ -888,30 +870,21 @@ double trainSource(const Context& ctx, uint32_t s, const jgs2_precompute_options
       for (uint32_t t = 0; t < pb.Tp; ++t) cols[t][3ull * p + r] = rem[3ull * t + r] / poseNorm;
     }
   }
-  Selection sel = greedySelect(cols, target, static_cast<int>(opt.cubature_k),
-                               static_cast<int>(opt.refinement_passes));
-  subsetAudit(cols, target, static_cast<int>(opt.cubature_k), sel);
-  for (size_t i = 0; i < sel.tets.size(); ++i) {
-    if (!(sel.weights[i] > 1e-10)) continue;
-    LocalRecord rec;
-    rec.tet = sel.tets[i];
-    rec.weight = sel.weights[i];
-    for (int l = 0; l < 4; ++l) {
-      const uint32_t v = pb.tets[4ull * rec.tet + l];
-      for (int e = 0; e < 9; ++e) rec.basis[l * 9 + e] = ubar[9ull * v + e];
-    }
-    records.push_back(rec);
-  }
-  return sel.residual;
+  tr.maxColumns = static_cast<int>(opt.cubature_k);
+  tr.passes = static_cast<int>(opt.refinement_passes);
+  tr.audit = true;
+  return true;
 }
 
-double trainLinear(const Context& ctx, uint32_t s, const std::vector<double>& ubar,
-                   const jgs2_precompute_options& opt, std::vector<LocalRecord>& records) {
+bool linearTraining(const Context& ctx, uint32_t s, const std::vector<double>& ubar,
+                    const jgs2_precompute_options& opt, Training& tr) {
   const Problem& pb = *ctx.pb;
   const int P = static_cast<int>(ctx.linearPoses.size());
   const double invH2 = 1.0 / (ctx.h * ctx.h);
-  std::vector<std::vector<double>> cols(pb.Tp, std::vector<double>(3ull * P, 0.0));
-  std::vector<double> target(3ull * P, 0.0);
+  std::vector<std::vector<double>>& cols = tr.cols;
+  std::vector<double>& target = tr.target;
+  cols.assign(pb.Tp, std::vector<double>(3ull * P, 0.0));
+  target.assign(3ull * P, 0.0);
   for (int p = 0; p < P; ++p) {
     const double* pose = ctx.linearPoses[p].data();
     double poseTarget[3] = {0, 0, 0}, scaleSq = 0;
@@ -961,21 +934,112 @@ double trainLinear(const Context& ctx, uint32_t s, const std::vector<double>& ub
   }
   bool anyColumn = false;
   for (const auto& col : cols) anyColumn |= dotv(col.data(), col.data(), col.size()) > 1e-18;
-  if (!(std::sqrt(dotv(target.data(), target.data(), target.size())) > 1e-12) || !anyColumn) return 0.0;
-  const Selection sel = greedySelect(cols, target, static_cast<int>(opt.cubature_k), kLinearRefinementPasses);
-  for (size_t i = 0; i < sel.tets.size(); ++i) {
-    if (!(sel.weights[i] > 1e-10)) continue;
-    LocalRecord rec;
-    rec.tet = sel.tets[i];
-    rec.weight = sel.weights[i];
-    for (int l = 0; l < 4; ++l) {
-      const uint32_t v = pb.tets[4ull * rec.tet + l];
-      for (int e = 0; e < 9; ++e) rec.basis[l * 9 + e] = ubar[9ull * v + e];
-    }
-    records.push_back(rec);
-  }
+  if (!(std::sqrt(dotv(target.data(), target.data(), target.size())) > 1e-12) || !anyColumn) return false;
+  tr.maxColumns = static_cast<int>(opt.cubature_k);
+  tr.passes = kLinearRefinementPasses;
+  tr.audit = false;
+  return true;
+}
+
+// One source vertex trained start to finish on this CPU thread; returns the
+// normalized residual.
+double trainSource(const Context& ctx, uint32_t s, const jgs2_precompute_options& opt,
+                   std::vector<LocalRecord>& records) {
+  std::vector<double> ubar;
+  Training tr;
+  if (!buildTraining(ctx, s, opt, ubar, tr, records)) return 0.0;
+  const Candidates cs = candidates(tr);
+  const Selection sel = finishSelection(tr, cs, selectOnCpu(tr, cs));
+  keepPositive(*ctx.pb, ubar, sel, records);
   return sel.residual;
 }
+
+// A source vertex whose selection runs in a GPU batch: its training system is
+// built on a CPU thread, selected with the other jobs of its batch, then
+// finished on a CPU thread.
+struct TrainingJob {
+  Problem pb;                 // the patch (patch method); unused with a shared context
+  uint32_t source = 0;        // source vertex, local to the problem
+  bool trained = false;       // the problem had a system to train
+  bool reduced = false;       // the corpus amplitude was halved
+  bool select = false;        // a selection is pending
+  std::vector<double> ubar;
+  Training tr;
+  Candidates cs;
+  std::vector<double> rows;   // candidate columns, row-major
+  std::vector<LocalRecord> records;
+  double residual = 0;
+  size_t bytes() const {
+    size_t b = rows.size() * sizeof(double);
+    for (const auto& c : tr.cols) b += c.size() * sizeof(double);
+    return b;
+  }
+};
+
+// Builds job j's training system (on the given context) and its candidate
+// filter; a job that needs no selection is finished here.
+void buildJob(const Context& ctx, const jgs2_precompute_options& opt, TrainingJob& job) {
+  job.trained = true;
+  job.select = buildTraining(ctx, job.source, opt, job.ubar, job.tr, job.records);
+  if (!job.select) return;
+  job.cs = candidates(job.tr);
+  if (job.cs.status != Candidates::kReady) {
+    job.select = false;
+    const Selection sel = finishSelection(job.tr, job.cs, SelectOutput{});
+    keepPositive(*ctx.pb, job.ubar, sel, job.records);
+    job.residual = sel.residual;
+    return;
+  }
+  job.rows = candidateRows(job.tr, job.cs);
+}
+
+// Selects every pending job of the batch in one GPU launch, then finishes
+// them (direct residuals, audits, records) on the CPU threads; the jobs'
+// training data is released.
+std::string selectBatchOnGpu(std::vector<TrainingJob*>& batch, const Problem* shared) {
+  std::vector<SelectInput> in;
+  std::vector<TrainingJob*> pending;
+  for (TrainingJob* j : batch) {
+    if (!j->select) continue;
+    SelectInput p;
+    p.cols = j->rows.data();
+    p.cc = j->cs.cc.data();
+    p.ct = j->cs.ct.data();
+    p.rows = static_cast<uint32_t>(j->tr.target.size());
+    p.cand = static_cast<uint32_t>(j->cs.ids.size());
+    p.limit = static_cast<uint32_t>(j->cs.limit);
+    p.passes = static_cast<uint32_t>(j->tr.passes);
+    p.tt = j->cs.tt;
+    p.tn = j->cs.tn;
+    in.push_back(p);
+    pending.push_back(j);
+  }
+  std::vector<SelectOutput> out;
+  const std::string err = selectOnGpu(in, out);
+  if (!err.empty()) return err;
+#pragma omp parallel for schedule(dynamic, 1)
+  for (int64_t i = 0; i < static_cast<int64_t>(pending.size()); ++i) {
+    TrainingJob& j = *pending[i];
+    const Selection sel = finishSelection(j.tr, j.cs, out[i]);
+    keepPositive(shared ? *shared : j.pb, j.ubar, sel, j.records);
+    j.residual = sel.residual;
+    j.select = false;
+  }
+  for (TrainingJob* j : batch) {
+    j->tr = Training{};
+    j->rows = {};
+    j->cs = Candidates{};
+    j->ubar = {};
+  }
+  return {};
+}
+
+double secondsSince(std::chrono::steady_clock::time_point t0) {
+  return std::chrono::duration<double>(std::chrono::steady_clock::now() - t0).count();
+}
+
+// Bytes of training data gathered before a GPU selection batch runs.
+constexpr size_t kSelectionBatchBytes = size_t(1) << 30;
 
 // ---- patch extraction and signatures ----------------------------------------
 
@@ -1156,6 +1220,16 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
     return false;
   }
   jgs2_precompute_stats st{};
+  bool gpu = false;
+  if (!opt.exact_complement && opt.selection_device != JGS2_SELECTION_CPU) {
+    const bool visible = selectionDeviceCount() > 0;
+    if (opt.selection_device == JGS2_SELECTION_GPU && !visible) {
+      sc.error = "GPU cubature selection was requested, but no CUDA device is visible.";
+      return false;
+    }
+    gpu = visible;
+  }
+  st.selection_on_gpu = gpu ? 1 : 0;
   std::vector<double> residuals(V, -1.0);
   std::vector<uint32_t> incident(V, 0);
   for (uint32_t v : m.tets) incident[v]++;
@@ -1188,16 +1262,58 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
     for (uint32_t v = 0; v < V; ++v)
       if (!m.fixed[v] && incident[v] > 0) sources.push_back(v);
     std::vector<std::string> errors(omp_get_max_threads());
+    const auto trainStart = std::chrono::steady_clock::now();
+    if (!gpu) {
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int64_t i = 0; i < static_cast<int64_t>(sources.size()); ++i) {
-      std::vector<LocalRecord> recs;
-      try {
-        residuals[sources[i]] = trainSource(ctx, sources[i], opt, recs);
-        writeRecords(sc, sources[i], pb, recs, K);
-      } catch (const std::exception& e) {
-        errors[omp_get_thread_num()] = e.what();
+      for (int64_t i = 0; i < static_cast<int64_t>(sources.size()); ++i) {
+        std::vector<LocalRecord> recs;
+        try {
+          residuals[sources[i]] = trainSource(ctx, sources[i], opt, recs);
+          writeRecords(sc, sources[i], pb, recs, K);
+        } catch (const std::exception& e) {
+          errors[omp_get_thread_num()] = e.what();
+        }
+      }
+    } else {
+      // Training systems built on the CPU threads, selections in GPU batches
+      // of about kSelectionBatchBytes of columns.
+      const size_t S = sources.size(), group = 4 * static_cast<size_t>(omp_get_max_threads());
+      for (size_t next = 0; next < S;) {
+        std::vector<std::unique_ptr<TrainingJob>> jobs;
+        size_t bytes = 0;
+        while (next < S && bytes < kSelectionBatchBytes) {
+          const size_t first = jobs.size(), n = std::min(S - next, group);
+          for (size_t i = 0; i < n; ++i) {
+            jobs.emplace_back(new TrainingJob);
+            jobs.back()->source = sources[next + i];
+          }
+#pragma omp parallel for schedule(dynamic, 1)
+          for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
+            try {
+              buildJob(ctx, opt, *jobs[first + i]);
+            } catch (const std::exception& e) {
+              errors[omp_get_thread_num()] = e.what();
+            }
+          }
+          for (size_t i = first; i < jobs.size(); ++i) bytes += jobs[i]->bytes();
+          next += n;
+        }
+        for (const auto& e : errors)
+          if (!e.empty()) { sc.error = e; return false; }
+        std::vector<TrainingJob*> batch;
+        for (auto& j : jobs) batch.push_back(j.get());
+        const auto selectStart = std::chrono::steady_clock::now();
+        const std::string err = selectBatchOnGpu(batch, &pb);
+        st.selection_seconds += secondsSince(selectStart);
+        if (!err.empty()) { sc.error = err; return false; }
+        st.selection_batches++;
+        for (auto& j : jobs) {
+          residuals[j->source] = j->residual;
+          writeRecords(sc, j->source, pb, j->records, K);
+        }
       }
     }
+    st.training_seconds = secondsSince(trainStart);
     for (const auto& e : errors)
       if (!e.empty()) { sc.error = e; return false; }
   } else {
@@ -1235,24 +1351,77 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
     std::vector<double> classResidual(C, 0.0);
     std::vector<uint8_t> classReduced(C, 0);
     std::vector<std::string> errors(omp_get_max_threads());
+    const auto trainStart = std::chrono::steady_clock::now();
+    if (!gpu) {
 #pragma omp parallel for schedule(dynamic, 1)
-    for (int64_t c = 0; c < static_cast<int64_t>(C); ++c) {
-      try {
-        Problem pb;
-        uint32_t sl = 0;
-        extractPatch(sc, g, sources[reps[c]], opt.patch_radius, pb, &sl);
-        classSig[c] = patchSignature(sc, pb, sl);
-        Context ctx;
-        ctx.pb = &pb;
-        ctx.h = opt.timestep;
-        if (!buildSystem(ctx)) continue;
-        prepareTraining(ctx, opt, anyCorotated);
-        classReduced[c] = ctx.amplitudeReduced ? 1 : 0;
-        classResidual[c] = trainSource(ctx, sl, opt, classRecords[c]);
-      } catch (const std::exception& e) {
-        errors[omp_get_thread_num()] = e.what();
+      for (int64_t c = 0; c < static_cast<int64_t>(C); ++c) {
+        try {
+          Problem pb;
+          uint32_t sl = 0;
+          extractPatch(sc, g, sources[reps[c]], opt.patch_radius, pb, &sl);
+          classSig[c] = patchSignature(sc, pb, sl);
+          Context ctx;
+          ctx.pb = &pb;
+          ctx.h = opt.timestep;
+          if (!buildSystem(ctx)) continue;
+          prepareTraining(ctx, opt, anyCorotated);
+          classReduced[c] = ctx.amplitudeReduced ? 1 : 0;
+          classResidual[c] = trainSource(ctx, sl, opt, classRecords[c]);
+        } catch (const std::exception& e) {
+          errors[omp_get_thread_num()] = e.what();
+        }
+      }
+    } else {
+      // Class systems built on the CPU threads, selections in GPU batches of
+      // about kSelectionBatchBytes of columns.
+      const size_t group = 4 * static_cast<size_t>(omp_get_max_threads());
+      for (size_t next = 0; next < C;) {
+        std::vector<std::unique_ptr<TrainingJob>> jobs;
+        size_t bytes = 0;
+        const size_t batchFirst = next;
+        while (next < C && bytes < kSelectionBatchBytes) {
+          const size_t first = jobs.size(), n = std::min(C - next, group);
+          for (size_t i = 0; i < n; ++i) jobs.emplace_back(new TrainingJob);
+#pragma omp parallel for schedule(dynamic, 1)
+          for (int64_t i = 0; i < static_cast<int64_t>(n); ++i) {
+            const size_t c = next + i;
+            TrainingJob& job = *jobs[first + i];
+            try {
+              extractPatch(sc, g, sources[reps[c]], opt.patch_radius, job.pb, &job.source);
+              classSig[c] = patchSignature(sc, job.pb, job.source);
+              Context ctx;
+              ctx.pb = &job.pb;
+              ctx.h = opt.timestep;
+              if (!buildSystem(ctx)) continue;
+              prepareTraining(ctx, opt, anyCorotated);
+              job.reduced = ctx.amplitudeReduced;
+              buildJob(ctx, opt, job);
+            } catch (const std::exception& e) {
+              errors[omp_get_thread_num()] = e.what();
+            }
+          }
+          for (size_t i = first; i < jobs.size(); ++i) bytes += jobs[i]->bytes();
+          next += n;
+        }
+        for (const auto& e : errors)
+          if (!e.empty()) { sc.error = e; return false; }
+        std::vector<TrainingJob*> batch;
+        for (auto& j : jobs) batch.push_back(j.get());
+        const auto selectStart = std::chrono::steady_clock::now();
+        const std::string err = selectBatchOnGpu(batch, nullptr);
+        st.selection_seconds += secondsSince(selectStart);
+        if (!err.empty()) { sc.error = err; return false; }
+        st.selection_batches++;
+        for (size_t i = 0; i < jobs.size(); ++i) {
+          const size_t c = batchFirst + i;
+          if (!jobs[i]->trained) continue;
+          classReduced[c] = jobs[i]->reduced ? 1 : 0;
+          classResidual[c] = jobs[i]->residual;
+          classRecords[c] = std::move(jobs[i]->records);
+        }
       }
     }
+    st.training_seconds = secondsSince(trainStart);
     for (const auto& e : errors)
       if (!e.empty()) { sc.error = e; return false; }
     std::vector<uint8_t> mismatch(S, 0);

@@ -480,6 +480,7 @@ void jgs2_default_precompute_options(jgs2_precompute_options* out) {
   out->training_amplitude = 0.12;
   out->refinement_passes = 12;
   out->exact_complement = 0;
+  out->selection_device = JGS2_SELECTION_AUTO;
 }
 
 int32_t jgs2_scene_add_material(jgs2_scene* s, double density, double young, double poisson,
@@ -719,6 +720,8 @@ jgs2_status jgs2_scene_precompute(jgs2_scene* s, const jgs2_precompute_options* 
   if (!(opt.timestep > 0) || !std::isfinite(opt.timestep))
     return fail(s, "The timestep must be finite and positive."), JGS2_INVALID_ARGUMENT;
   if (opt.cubature_k < 1) return fail(s, "cubature_k must be positive."), JGS2_INVALID_ARGUMENT;
+  if (opt.selection_device > JGS2_SELECTION_AUTO)
+    return fail(s, "selection_device must be JGS2_SELECTION_CPU, _GPU or _AUTO."), JGS2_INVALID_ARGUMENT;
   if (opt.method > JGS2_PRECOMPUTE_PATCH) return fail(s, "Unknown precompute method."), JGS2_INVALID_ARGUMENT;
   if (!computeRest(*s)) return JGS2_INVALID_ARGUMENT;
   try {

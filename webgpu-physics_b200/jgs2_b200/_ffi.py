@@ -169,7 +169,7 @@ class PrecomputeOptions(Structure):
         ("patch_radius", c_uint32), ("threads", c_uint32),
         ("mode_count", c_uint32), ("inverse_iterations", c_uint32),
         ("training_amplitude", c_double), ("refinement_passes", c_uint32),
-        ("exact_complement", c_uint32),
+        ("exact_complement", c_uint32), ("selection_device", c_uint32),
     ]
 
 
@@ -180,6 +180,8 @@ class PrecomputeStats(Structure):
         ("max_residual", c_double), ("mean_residual", c_double),
         ("vertices_over_tolerance", c_uint32),
         ("reduced_amplitude_classes", c_uint32), ("seconds", c_double),
+        ("selection_on_gpu", c_uint32), ("selection_batches", c_uint32),
+        ("training_seconds", c_double), ("selection_seconds", c_double),
     ]
 
 

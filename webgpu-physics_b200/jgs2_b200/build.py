@@ -2,7 +2,8 @@
 
   libjgs2.so        CUDA step for sm_100a + the C-ABI runtime (include/jgs2.h)
   checked/libjgs2.so  the same with device index checks (JGS2_BOUNDS_CHECKS=1)
-  libjgs2_scene.so  CPU scene builder / precompute (include/jgs2_scene.h)
+  libjgs2_scene.so  scene builder / precompute, with the GPU cubature selection
+                    (include/jgs2_scene.h)
 
 Run as `python -m jgs2_b200.build` from webgpu-physics_b200/ or through
 __graft_entry__.build().  nvcc cross-compiles for sm_100a without a GPU.
@@ -94,11 +95,33 @@ def build_scene_library(force=False, verbose=False) -> str:
     os.makedirs(LIB, exist_ok=True)
     target = os.path.join(LIB, "libjgs2_scene.so")
     sdir = os.path.join(CSRC, "scene")
-    sources = [os.path.join(sdir, f) for f in ("scene.cpp", "precompute.cpp")]
-    headers = [os.path.join(sdir, "scene_internal.hpp"), os.path.join(INCLUDE, "jgs2_scene.h"),
-               os.path.join(INCLUDE, "jgs2.h")]
+    sources = [os.path.join(sdir, f) for f in ("scene.cpp", "precompute.cpp", "select_gpu.cu")]
+    headers = [os.path.join(sdir, f) for f in ("scene_internal.hpp", "cubature_select.hpp", "select_gpu.hpp")] + [
+        os.path.join(INCLUDE, "jgs2_scene.h"), os.path.join(INCLUDE, "jgs2.h")]
     if not force and not _stale(target, sources + headers):
         return target
+    nvcc, cxx = _nvcc(), _cxx()
+    # The cubature selection must round identically on the CPU and the GPU:
+    # no multiply-add contraction in the host code (-ffp-contract=off) nor in
+    # the device code (--fmad=false).
+    objs, cmds = [], []
+    for src in sources:
+        obj = os.path.join(LIB, "scene_" + os.path.basename(src) + ".o")
+        if src.endswith(".cu"):
+            cmd = [nvcc, *ARCH, "-O3", "-lineinfo", "-std=c++17", "--fmad=false", "-Xcompiler", "-fPIC",
+                   "-I", INCLUDE, "-I", sdir, "-c", src, "-o", obj]
+        else:
+            cmd = [cxx, "-O3", "-march=x86-64-v3", "-ffp-contract=off", "-fopenmp", "-fPIC", "-std=c++17",
+                   "-I", INCLUDE, "-I", sdir, "-c", src, "-o", obj]
+        cmds.append(cmd)
+        objs.append(obj)
+    with concurrent.futures.ThreadPoolExecutor(len(cmds)) as pool:
+        list(pool.map(lambda c: _run(c, verbose), cmds))
+    cuda_lib = os.path.join(os.path.dirname(os.path.dirname(os.path.realpath(nvcc))), "lib64")
+    _run([cxx, "-shared", "-fopenmp", "-o", target, *objs, "-L", cuda_lib, "-lcudart"], verbose)
+    for obj in objs:
+        os.remove(obj)
+    return target
     _run([_cxx(), "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-std=c++17", "-I", INCLUDE,
           "-I", sdir, *sources, "-o", target], verbose)
     return target

@@ -24,6 +24,12 @@ MATERIAL_COROTATED_LINEAR = 0
 MATERIAL_STABLE_NEO_HOOKEAN = 1
 PRECOMPUTE_EXACT = 0
 PRECOMPUTE_PATCH = 1
+# Where the greedy cubature selection runs (same records either way).
+SELECTION_CPU, SELECTION_GPU, SELECTION_AUTO = 0, 1, 2
+# Revision of the training arithmetic, part of every cubature fingerprint:
+# 2 = FP64 evaluated in source order (no multiply-add contraction), the
+# rounding the GPU selection shares.
+TRAINER_REVISION = 2
 CONTACT_NONE, CONTACT_STATIC, CONTACT_SURFACE = 0, 1, 2
 FACE_X_MIN, FACE_X_MAX, FACE_Y_MIN, FACE_Y_MAX, FACE_Z_MIN, FACE_Z_MAX = (
     1, 2, 4, 8, 16, 32)
@@ -787,7 +793,7 @@ def unit_cube_components(cells=100, young=1e6, poisson=0.45, density=1000.0, tim
             "materials": {"density": density, "young": young, "poisson": poisson, "model": "stable-neo-hookean"},
             "timestep": timestep,
             "basis": {"method": method, "patch_radius": patch_radius},
-            "cubature": {"k": cubature_k, "exact_complement": exact_complement},
+            "cubature": {"k": cubature_k, "exact_complement": exact_complement, "trainer": TRAINER_REVISION},
             "solverSchedule": schedule}
 
 
