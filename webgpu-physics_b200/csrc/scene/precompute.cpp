@@ -1087,37 +1087,87 @@ MeshGraph buildGraph(const Mesh& m) {
 
 // Patch around s: free vertices within `radius` rings (not globally fixed),
 // tetrahedra incident to them, and every vertex those tetrahedra touch.
+// Per-thread scratch of the patch extraction: epoch marks over the mesh's
+// vertices and tetrahedra (a vertex or tetrahedron is in the current set when
+// its mark equals the current epoch), a global-to-local vertex map and
+// reusable lists.  Replaces per-patch searches and sorts of duplicates.
+struct PatchScratch {
+  std::vector<uint32_t> vertexMark, tetMark, local;
+  uint32_t epoch = 0;
+  std::vector<uint32_t> frontier, next, visited, freeVerts, tets, verts;
+  std::vector<int64_t> signature;
+  Problem pb;  // the patch of the classification passes
+
+  uint32_t nextEpoch(uint32_t V, uint32_t T) {
+    if (vertexMark.size() != V || tetMark.size() != T) {
+      vertexMark.assign(V, 0);
+      tetMark.assign(T, 0);
+      local.assign(V, 0);
+      epoch = 0;
+    }
+    if (++epoch == 0) {
+      std::fill(vertexMark.begin(), vertexMark.end(), 0u);
+      std::fill(tetMark.begin(), tetMark.end(), 0u);
+      epoch = 1;
+    }
+    return epoch;
+  }
+};
+
+// The patch of source vertex s: the vertices within `radius` rings (breadth
+// first over the vertex graph), the tetrahedra incident to its free vertices,
+// and every vertex of those tetrahedra, each list in ascending global order
+// (local ids follow it).  Rest volumes and inverse rest matrices are copied
+// only when the patch is trained.
 void extractPatch(const Scene& sc, const MeshGraph& g, uint32_t s, uint32_t radius, Problem& pb,
-                  uint32_t* sLocal) {
+                  uint32_t* sLocal, PatchScratch& ps, bool forTraining) {
   const Mesh& m = sc.mesh;
-  std::vector<uint32_t> frontier{s}, ring{s};
-  std::vector<uint32_t> visited{s};
+  const uint32_t V = m.vertexCount(), T = m.tetCount();
+  uint32_t e = ps.nextEpoch(V, T);
+  ps.frontier.assign(1, s);
+  ps.visited.assign(1, s);
+  ps.vertexMark[s] = e;
   for (uint32_t r = 0; r < radius; ++r) {
-    std::vector<uint32_t> next;
-    for (uint32_t v : frontier)
+    ps.next.clear();
+    for (uint32_t v : ps.frontier)
       for (uint64_t i = g.nbrStart[v]; i < g.nbrStart[v + 1]; ++i) {
         const uint32_t u = g.nbrs[i];
-        if (std::find(visited.begin(), visited.end(), u) == visited.end()) {
-          visited.push_back(u);
-          next.push_back(u);
+        if (ps.vertexMark[u] != e) {
+          ps.vertexMark[u] = e;
+          ps.visited.push_back(u);
+          ps.next.push_back(u);
         }
       }
-    frontier.swap(next);
+    ps.frontier.swap(ps.next);
   }
-  std::vector<uint32_t> freeVerts;
-  for (uint32_t v : visited)
-    if (!m.fixed[v]) freeVerts.push_back(v);
-  std::vector<uint32_t> tets;
-  for (uint32_t v : freeVerts)
-    for (uint64_t i = g.adjStart[v]; i < g.adjStart[v + 1]; ++i) tets.push_back(g.adjTets[i]);
-  std::sort(tets.begin(), tets.end());
-  tets.erase(std::unique(tets.begin(), tets.end()), tets.end());
-  std::vector<uint32_t> verts;
-  for (uint32_t t : tets)
-    for (int l = 0; l < 4; ++l) verts.push_back(m.tets[4ull * t + l]);
-  std::sort(verts.begin(), verts.end());
-  verts.erase(std::unique(verts.begin(), verts.end()), verts.end());
-  std::sort(freeVerts.begin(), freeVerts.end());
+  ps.freeVerts.clear();
+  for (uint32_t v : ps.visited)
+    if (!m.fixed[v]) ps.freeVerts.push_back(v);
+  e = ps.nextEpoch(V, T);
+  ps.tets.clear();
+  for (uint32_t v : ps.freeVerts)
+    for (uint64_t i = g.adjStart[v]; i < g.adjStart[v + 1]; ++i) {
+      const uint32_t t = g.adjTets[i];
+      if (ps.tetMark[t] != e) {
+        ps.tetMark[t] = e;
+        ps.tets.push_back(t);
+      }
+    }
+  std::sort(ps.tets.begin(), ps.tets.end());
+  ps.verts.clear();
+  for (uint32_t t : ps.tets)
+    for (int l = 0; l < 4; ++l) {
+      const uint32_t u = m.tets[4ull * t + l];
+      if (ps.vertexMark[u] != e) {
+        ps.vertexMark[u] = e;
+        ps.verts.push_back(u);
+      }
+    }
+  std::sort(ps.verts.begin(), ps.verts.end());
+  e = ps.nextEpoch(V, T);
+  for (uint32_t v : ps.freeVerts) ps.vertexMark[v] = e;
+  const std::vector<uint32_t>& verts = ps.verts;
+  const std::vector<uint32_t>& tets = ps.tets;
   pb.Vp = static_cast<uint32_t>(verts.size());
   pb.Tp = static_cast<uint32_t>(tets.size());
   pb.globalVertex = verts;
@@ -1128,30 +1178,33 @@ void extractPatch(const Scene& sc, const MeshGraph& g, uint32_t s, uint32_t radi
   pb.freeMask.resize(pb.Vp);
   for (uint32_t i = 0; i < pb.Vp; ++i) {
     const uint32_t v = verts[i];
+    ps.local[v] = i;
     for (int k = 0; k < 3; ++k) pb.rest[3ull * i + k] = m.positions[3ull * v + k];
     pb.mass[i] = sc.masses[v];
     pb.incident[i] = static_cast<uint32_t>(g.adjStart[v + 1] - g.adjStart[v]);
-    pb.freeMask[i] = std::binary_search(freeVerts.begin(), freeVerts.end(), v) ? 1 : 0;
+    pb.freeMask[i] = ps.vertexMark[v] == e ? 1 : 0;
     if (v == s) *sLocal = i;
   }
   pb.tets.resize(4ull * pb.Tp);
-  pb.vol.resize(pb.Tp);
-  pb.invRest.resize(9ull * pb.Tp);
   pb.mats.resize(pb.Tp);
+  pb.vol.resize(forTraining ? pb.Tp : 0);
+  pb.invRest.resize(forTraining ? 9ull * pb.Tp : 0);
   for (uint32_t i = 0; i < pb.Tp; ++i) {
     const uint32_t t = tets[i];
-    for (int l = 0; l < 4; ++l)
-      pb.tets[4ull * i + l] = static_cast<uint32_t>(
-          std::lower_bound(verts.begin(), verts.end(), m.tets[4ull * t + l]) - verts.begin());
+    for (int l = 0; l < 4; ++l) pb.tets[4ull * i + l] = ps.local[m.tets[4ull * t + l]];
+    pb.mats[i] = &sc.materialTable[m.materials[t]];
+    if (!forTraining) continue;
     pb.vol[i] = sc.rest.volumes[t];
     std::memcpy(&pb.invRest[9ull * i], &sc.rest.inverseRest[9ull * t], 9 * sizeof(double));
-    pb.mats[i] = &sc.materialTable[m.materials[t]];
   }
 }
 
-// Quantised signature of a patch relative to its source vertex.
-std::vector<int64_t> patchSignature(const Scene& sc, const Problem& pb, uint32_t sLocal) {
-  std::vector<int64_t> sig;
+// Quantised signature of a patch relative to its source vertex: sizes, the
+// source's local id, every vertex's offset from the source (quantised to
+// 1e-9 of the patch extent), mass ratio, incident count and free flag, and
+// every tetrahedron's local vertices and material.
+void patchSignature(const Scene& sc, const Problem& pb, uint32_t sLocal, std::vector<int64_t>& sig) {
+  sig.clear();
   sig.reserve(8 + 6ull * pb.Vp + 5ull * pb.Tp);
   sig.push_back(pb.Vp);
   sig.push_back(pb.Tp);
@@ -1172,17 +1225,16 @@ std::vector<int64_t> patchSignature(const Scene& sc, const Problem& pb, uint32_t
     for (int l = 0; l < 4; ++l) sig.push_back(pb.tets[4ull * i + l]);
     sig.push_back(pb.mats[i] - sc.materialTable.data());
   }
-  return sig;
 }
 
+// 64-bit hash of a signature, one multiply-xorshift round per word; equal
+// hashes are confirmed by comparing the signatures themselves.
 uint64_t hashSignature(const std::vector<int64_t>& sig) {
-  uint64_t h = 1469598103934665603ull;
+  uint64_t h = 0x9e3779b97f4a7c15ull ^ sig.size();
   for (int64_t v : sig) {
-    uint64_t x = static_cast<uint64_t>(v);
-    for (int b = 0; b < 8; ++b) {
-      h ^= (x >> (8 * b)) & 0xff;
-      h *= 1099511628211ull;
-    }
+    h ^= static_cast<uint64_t>(v);
+    h *= 0xff51afd7ed558ccdull;
+    h ^= h >> 32;
   }
   return h;
 }
@@ -1323,12 +1375,14 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
       if (!m.fixed[v] && incident[v] > 0) sources.push_back(v);
     const size_t S = sources.size();
     std::vector<uint64_t> hashes(S);
+    std::vector<PatchScratch> scratch(omp_get_max_threads());
 #pragma omp parallel for schedule(dynamic, 256)
     for (int64_t i = 0; i < static_cast<int64_t>(S); ++i) {
-      Problem pb;
+      PatchScratch& ps = scratch[omp_get_thread_num()];
       uint32_t sl = 0;
-      extractPatch(sc, g, sources[i], opt.patch_radius, pb, &sl);
-      hashes[i] = hashSignature(patchSignature(sc, pb, sl));
+      extractPatch(sc, g, sources[i], opt.patch_radius, ps.pb, &sl, ps, false);
+      patchSignature(sc, ps.pb, sl, ps.signature);
+      hashes[i] = hashSignature(ps.signature);
     }
     // Group by hash; the first vertex of each group is its representative.
     std::unordered_map<uint64_t, uint32_t> classOf;
@@ -1358,8 +1412,8 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
         try {
           Problem pb;
           uint32_t sl = 0;
-          extractPatch(sc, g, sources[reps[c]], opt.patch_radius, pb, &sl);
-          classSig[c] = patchSignature(sc, pb, sl);
+          extractPatch(sc, g, sources[reps[c]], opt.patch_radius, pb, &sl, scratch[omp_get_thread_num()], true);
+          patchSignature(sc, pb, sl, classSig[c]);
           Context ctx;
           ctx.pb = &pb;
           ctx.h = opt.timestep;
@@ -1387,8 +1441,9 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
             const size_t c = next + i;
             TrainingJob& job = *jobs[first + i];
             try {
-              extractPatch(sc, g, sources[reps[c]], opt.patch_radius, job.pb, &job.source);
-              classSig[c] = patchSignature(sc, job.pb, job.source);
+              extractPatch(sc, g, sources[reps[c]], opt.patch_radius, job.pb, &job.source,
+                           scratch[omp_get_thread_num()], true);
+              patchSignature(sc, job.pb, job.source, classSig[c]);
               Context ctx;
               ctx.pb = &job.pb;
               ctx.h = opt.timestep;
@@ -1427,22 +1482,25 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
     std::vector<uint8_t> mismatch(S, 0);
 #pragma omp parallel for schedule(dynamic, 256)
     for (int64_t i = 0; i < static_cast<int64_t>(S); ++i) {
-      Problem pb;
+      PatchScratch& ps = scratch[omp_get_thread_num()];
       uint32_t sl = 0;
-      extractPatch(sc, g, sources[i], opt.patch_radius, pb, &sl);
+      extractPatch(sc, g, sources[i], opt.patch_radius, ps.pb, &sl, ps, false);
       const uint32_t c = cls[i];
-      if (static_cast<size_t>(i) != reps[c] && patchSignature(sc, pb, sl) != classSig[c]) {
-        mismatch[i] = 1;  // hash collision: train this vertex on its own
-        continue;
+      if (static_cast<size_t>(i) != reps[c]) {
+        patchSignature(sc, ps.pb, sl, ps.signature);
+        if (ps.signature != classSig[c]) {
+          mismatch[i] = 1;  // hash collision: train this vertex on its own
+          continue;
+        }
       }
-      writeRecords(sc, sources[i], pb, classRecords[c], K);
+      writeRecords(sc, sources[i], ps.pb, classRecords[c], K);
       residuals[sources[i]] = classResidual[c];
     }
     for (size_t i = 0; i < S; ++i) {
       if (!mismatch[i]) continue;
       Problem pb;
       uint32_t sl = 0;
-      extractPatch(sc, g, sources[i], opt.patch_radius, pb, &sl);
+      extractPatch(sc, g, sources[i], opt.patch_radius, pb, &sl, scratch[0], true);
       Context ctx;
       ctx.pb = &pb;
       ctx.h = opt.timestep;
