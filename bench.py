@@ -372,6 +372,10 @@ def batched_arm(args):
     ms = max_over_ranks(dist, start_ev.elapsed_time(end_ev), f"cuda:{device}")
     launches = batch.kernelLaunchCount() - launches0
     value = whole_job_rate(world, active * iters * args.steps, ms / 1e3)
+    # Accepted iterations of the last timed frame, per scene (the history
+    # holds the latest frame's iterations).
+    accepted_last = [int(batch.readGlobalizationDiagnostics(i)["history"][:iters, 4].sum())
+                     for i in range(len(parts))]
     # End to end: each frame's settings upload and a read of every scene's positions.
     pos_host = torch.empty(4 * V, dtype=torch.float32).pin_memory()
     p_np = pos_host.numpy()
@@ -424,6 +428,10 @@ def batched_arm(args):
                                  "tuning_frame_ms": [round(m, 3) for m in shape["frameMs"]]},
                 "parallelism": "replicas" if world > 1 else "single GPU"},
             "frames_per_s": world * len(parts) * 1e3 * args.steps / ms,
+            "accepted_iterations_last_timed_frame": {
+                "total": sum(accepted_last), "of": len(parts) * iters,
+                "scenes_accepting": sum(1 for a in accepted_last if a > 0),
+                "scenes_accepting_every_iteration": sum(1 for a in accepted_last if a == iters)},
             "error_vs_fp64": err64,
             "gpu_launches": int(launches),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
