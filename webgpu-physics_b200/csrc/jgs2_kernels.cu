@@ -2701,7 +2701,20 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
 // ---------------------------------------------------------------------------
 // Gate: candidateTetrahedron (jgs2-shader.ts:3498-3601) + vertex energies
 // (assembledVertexEnergy :3489-3496) + reduceCandidate (:3611-3955).
-__global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams* __restrict__ pp,
+// JGS2_GATE_MIN_BLOCKS: blocks per SM the gate kernel's register budget must
+// allow (0: the compiler's choice, 92 registers and 5 blocks).  Eight blocks
+// (64 registers, 32 warps per SM for this gather-bound kernel) measured 22 %
+// faster on the 100^3 cube than the compiler's choice, with bitwise the same
+// results; six and ten were slower than eight.
+#ifndef JGS2_GATE_MIN_BLOCKS
+#define JGS2_GATE_MIN_BLOCKS 8
+#endif
+#if JGS2_GATE_MIN_BLOCKS > 0
+#define JGS2_GATE_BOUNDS __launch_bounds__(kBlock, JGS2_GATE_MIN_BLOCKS)
+#else
+#define JGS2_GATE_BOUNDS __launch_bounds__(kBlock)
+#endif
+__global__ void JGS2_GATE_BOUNDS gateKernel(Buffers b, const DevParams* __restrict__ pp,
                                                      const float4* __restrict__ src,
                                                      const float4* __restrict__ tgt) {
   __shared__ GatePartial smem[kBlock];
@@ -2784,8 +2797,13 @@ __global__ void __launch_bounds__(kBlock) gateKernel(Buffers b, const DevParams*
 // The five component norms are exact Euclidean norms accumulated in double;
 // the reference forms the same norms in f32 as scale * sqrt(sum((g/scale)^2)).
 // JGS2_CONV_MIN_BLOCKS: blocks per SM the convergence kernel's register
-// budget must allow (unset: the compiler's choice).
-#ifdef JGS2_CONV_MIN_BLOCKS
+// budget must allow (0: the compiler's choice, 151 registers and 3 blocks).
+// Four blocks (128 registers) measured 5 % faster on the 100^3 cube than the
+// compiler's choice, with bitwise the same results; five and six were slower.
+#ifndef JGS2_CONV_MIN_BLOCKS
+#define JGS2_CONV_MIN_BLOCKS 4
+#endif
+#if JGS2_CONV_MIN_BLOCKS > 0
 #define JGS2_CONV_BOUNDS __launch_bounds__(kBlock, JGS2_CONV_MIN_BLOCKS)
 #else
 #define JGS2_CONV_BOUNDS __launch_bounds__(kBlock)
