@@ -66,3 +66,18 @@ def test_auto_selects_the_gpu():
     st, _ = _cuboid((3, 2, 2), (0.3, 0.2, 0.2), scenes.FACE_X_MIN, 6, scenes.PRECOMPUTE_EXACT,
                     device=scenes.SELECTION_AUTO)
     assert st["selection_on_gpu"] == 1
+
+
+def test_gpu_selection_in_several_batches(monkeypatch):
+    # A small batch budget splits the classes (and the whole-mesh sources)
+    # over several launches; each class keeps its own records.
+    # Two threads build 8 jobs per group, so the budget closes a batch every
+    # group or two.
+    monkeypatch.setenv("JGS2_SELECTION_BATCH_BYTES", str(1 << 20))
+    for case in ("patch cube 8^3, K=6", "whole-mesh bar, K=6"):
+        cpu_st, cpu = _cuboid(**CASES[case], device=scenes.SELECTION_CPU, threads=2)
+        gpu_st, gpu = _cuboid(**CASES[case], device=scenes.SELECTION_GPU, threads=2)
+        assert gpu_st["selection_batches"] > 1, case
+        for key in cpu:
+            np.testing.assert_array_equal(gpu[key], cpu[key], err_msg=f"{case}: {key}")
+        assert gpu_st["max_residual"] == cpu_st["max_residual"]

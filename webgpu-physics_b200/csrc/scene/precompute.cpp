@@ -15,6 +15,7 @@
 
 #include <algorithm>
 #include <chrono>
+#include <cstdlib>
 #include <cstring>
 #include <functional>
 #include <memory>
@@ -1041,6 +1042,15 @@ double secondsSince(std::chrono::steady_clock::time_point t0) {
 // Bytes of training data gathered before a GPU selection batch runs.
 constexpr size_t kSelectionBatchBytes = size_t(1) << 30;
 
+// The batch budget: kSelectionBatchBytes, or JGS2_SELECTION_BATCH_BYTES when
+// set (smaller budgets split a precompute into more GPU launches).
+size_t selectionBatchBytes() {
+  const char* e = std::getenv("JGS2_SELECTION_BATCH_BYTES");
+  if (!e || !*e) return kSelectionBatchBytes;
+  const unsigned long long v = std::strtoull(e, nullptr, 10);
+  return v > 0 ? static_cast<size_t>(v) : kSelectionBatchBytes;
+}
+
 // ---- patch extraction and signatures ----------------------------------------
 
 struct MeshGraph {
@@ -1256,6 +1266,12 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
   const Mesh& m = sc.mesh;
   const uint32_t V = m.vertexCount();
   const uint32_t K = opt.cubature_k;
+  // The thread count applies to this precompute only; the process's OpenMP
+  // setting is restored on every return.
+  struct ThreadCount {
+    int saved = omp_get_max_threads();
+    ~ThreadCount() { omp_set_num_threads(saved); }
+  } threadCount;
   if (opt.threads > 0) omp_set_num_threads(static_cast<int>(opt.threads));
   sc.timestep = opt.timestep;
   sc.cubatureK = K;
@@ -1328,12 +1344,13 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
       }
     } else {
       // Training systems built on the CPU threads, selections in GPU batches
-      // of about kSelectionBatchBytes of columns.
+      // of about selectionBatchBytes() of columns.
       const size_t S = sources.size(), group = 4 * static_cast<size_t>(omp_get_max_threads());
+      const size_t budget = selectionBatchBytes();
       for (size_t next = 0; next < S;) {
         std::vector<std::unique_ptr<TrainingJob>> jobs;
         size_t bytes = 0;
-        while (next < S && bytes < kSelectionBatchBytes) {
+        while (next < S && bytes < budget) {
           const size_t first = jobs.size(), n = std::min(S - next, group);
           for (size_t i = 0; i < n; ++i) {
             jobs.emplace_back(new TrainingJob);
@@ -1427,13 +1444,14 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
       }
     } else {
       // Class systems built on the CPU threads, selections in GPU batches of
-      // about kSelectionBatchBytes of columns.
+      // about selectionBatchBytes() of columns.
       const size_t group = 4 * static_cast<size_t>(omp_get_max_threads());
+      const size_t budget = selectionBatchBytes();
       for (size_t next = 0; next < C;) {
         std::vector<std::unique_ptr<TrainingJob>> jobs;
         size_t bytes = 0;
         const size_t batchFirst = next;
-        while (next < C && bytes < kSelectionBatchBytes) {
+        while (next < C && bytes < budget) {
           const size_t first = jobs.size(), n = std::min(C - next, group);
           for (size_t i = 0; i < n; ++i) jobs.emplace_back(new TrainingJob);
 #pragma omp parallel for schedule(dynamic, 1)
