@@ -42,8 +42,8 @@ typedef struct jgs2_scene jgs2_scene;
  * bit for bit; the GPU runs every training problem of a batch at once on the
  * current CUDA device. */
 #define JGS2_SELECTION_CPU 0u
-#define JGS2_SELECTION_GPU 1u   /* error when no CUDA device is visible */
-#define JGS2_SELECTION_AUTO 2u  /* the GPU when a CUDA device is visible */
+#define JGS2_SELECTION_GPU 1u   /* error unless the current CUDA device is sm_100 */
+#define JGS2_SELECTION_AUTO 2u  /* the GPU when the current CUDA device is sm_100 */
 
 /* Face bits for generated cuboids: a vertex is pinned when it lies on any
  * selected face (the reference passes a predicate, src/simulation/cpu/mesh.ts:142). */

@@ -1290,12 +1290,14 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
   jgs2_precompute_stats st{};
   bool gpu = false;
   if (!opt.exact_complement && opt.selection_device != JGS2_SELECTION_CPU) {
-    const bool visible = selectionDeviceCount() > 0;
-    if (opt.selection_device == JGS2_SELECTION_GPU && !visible) {
-      sc.error = "GPU cubature selection was requested, but no CUDA device is visible.";
+    const SelectionDevice device = selectionDevice();
+    if (opt.selection_device == JGS2_SELECTION_GPU && device != SelectionDevice::kUsable) {
+      sc.error = device == SelectionDevice::kNone
+                     ? "GPU cubature selection was requested, but no CUDA device is visible."
+                     : "GPU cubature selection was requested, but the current CUDA device is not sm_100.";
       return false;
     }
-    gpu = visible;
+    gpu = device == SelectionDevice::kUsable;
   }
   st.selection_on_gpu = gpu ? 1 : 0;
   std::vector<double> residuals(V, -1.0);

@@ -323,13 +323,21 @@ std::string failed(const char* what, cudaError_t e) {
 
 }  // namespace
 
-int selectionDeviceCount() {
+SelectionDevice selectionDevice() {
   int n = 0;
-  if (cudaGetDeviceCount(&n) != cudaSuccess) {
+  if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
     cudaGetLastError();
-    return 0;
+    return SelectionDevice::kNone;
   }
-  return n;
+  int dev = 0, major = 0, minor = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev) != cudaSuccess ||
+      cudaDeviceGetAttribute(&minor, cudaDevAttrComputeCapabilityMinor, dev) != cudaSuccess) {
+    cudaGetLastError();
+    return SelectionDevice::kNone;
+  }
+  // The library carries sm_100a code only.
+  return major == 10 && minor == 0 ? SelectionDevice::kUsable : SelectionDevice::kOtherArchitecture;
 }
 
 std::string selectOnGpu(const std::vector<SelectInput>& in, std::vector<SelectOutput>& out) {

@@ -30,8 +30,10 @@ struct SelectOutput {
   double weights[jgs2select::kMaxColumns];
 };
 
-// CUDA devices visible to this process (0 without a device or driver).
-int selectionDeviceCount();
+// The calling thread's current CUDA device: none (no device or driver), one
+// this library's sm_100a code runs on, or another architecture.
+enum class SelectionDevice { kNone, kUsable, kOtherArchitecture };
+SelectionDevice selectionDevice();
 
 // Runs every problem's selection on the current CUDA device; returns an empty
 // string, or the failing CUDA call and its error.
