@@ -2701,22 +2701,25 @@ __global__ void __launch_bounds__(kBlock) prologueKernel(Buffers b, const DevPar
 // ---------------------------------------------------------------------------
 // Gate: candidateTetrahedron (jgs2-shader.ts:3498-3601) + vertex energies
 // (assembledVertexEnergy :3489-3496) + reduceCandidate (:3611-3955).
-// JGS2_GATE_MIN_BLOCKS: blocks per SM the gate kernel's register budget must
-// allow (0: the compiler's choice, 92 registers and 5 blocks).  Eight blocks
-// (64 registers, 32 warps per SM for this gather-bound kernel) measured 22 %
-// faster on the 100^3 cube than the compiler's choice, with bitwise the same
-// results; six and ten were slower than eight.
+// kExt: some scene of the engine has cloth or contact candidates (their
+// terms are compiled out otherwise).  JGS2_GATE_MIN_BLOCKS and
+// JGS2_GATE_EXT_MIN_BLOCKS: blocks per SM each instantiation's register
+// budget must allow.  For the tetrahedral gate, eight blocks (32 warps per SM
+// for this gather-bound kernel) measured 22 % faster on the 100^3 cube than
+// the compiler's choice (5 blocks), with bitwise the same results, and six
+// and ten slower than eight; with the cloth and contact terms eight blocks
+// cost the cloth drape 6 % of its gate time, so that instantiation keeps the
+// five blocks the compiler chose for the kernel before the split.
 #ifndef JGS2_GATE_MIN_BLOCKS
 #define JGS2_GATE_MIN_BLOCKS 8
 #endif
-#if JGS2_GATE_MIN_BLOCKS > 0
-#define JGS2_GATE_BOUNDS __launch_bounds__(kBlock, JGS2_GATE_MIN_BLOCKS)
-#else
-#define JGS2_GATE_BOUNDS __launch_bounds__(kBlock)
+#ifndef JGS2_GATE_EXT_MIN_BLOCKS
+#define JGS2_GATE_EXT_MIN_BLOCKS 5
 #endif
-__global__ void JGS2_GATE_BOUNDS gateKernel(Buffers b, const DevParams* __restrict__ pp,
-                                                     const float4* __restrict__ src,
-                                                     const float4* __restrict__ tgt) {
+template <bool kExt>
+__global__ void __launch_bounds__(kBlock, kExt ? JGS2_GATE_EXT_MIN_BLOCKS : JGS2_GATE_MIN_BLOCKS)
+    gateKernel(Buffers b, const DevParams* __restrict__ pp, const float4* __restrict__ src,
+               const float4* __restrict__ tgt) {
   __shared__ GatePartial smem[kBlock];
   __shared__ bool isLast;
   const RedBlock rb = b.gateTable[blockIdx.x];
@@ -2728,7 +2731,8 @@ __global__ void JGS2_GATE_BOUNDS gateKernel(Buffers b, const DevParams* __restri
   // Contacts: element k takes candidates k, k + span, ... of the scene's
   // list (a single pass for static candidates, which the table covers).
   const uint32_t span = max(sr.gateSpan, 1u);
-  const uint2 contacts = b.contactDynamic ? b.bpSpan[rb.scene] : make_uint2(sr.kOff, sr.KC);
+  const uint2 contacts =
+      !kExt ? make_uint2(0u, 0u) : b.contactDynamic ? b.bpSpan[rb.scene] : make_uint2(sr.kOff, sr.KC);
   for (uint32_t k = rb.begin + threadIdx.x; k < rb.end; k += blockDim.x) {
     if (k < sr.T) {
       const TetRec r = loadTet(b.tets, sr.tOff + k);
@@ -2742,11 +2746,11 @@ __global__ void JGS2_GATE_BOUNDS gateKernel(Buffers b, const DevParams* __restri
       if (finiteS(es)) acc.e0 += es; else acc.bits &= ~kSourceEnergyValid;
       if (finiteS(ec)) acc.e1 += ec; else acc.bits &= ~kCandidateEnergyValid;
     }
-    if (p.cloth) {
+    if (kExt && p.cloth) {
       if (k < sr.C) accumulateClothTri(acc, loadClothTri(b.clothTris, sr.cOff + k), src, tgt, clothMaterial(p));
       if (k < sr.H) accumulateHinge(acc, b.clothHinges, sr.hOff + k, src, tgt, p.clothBending);
     }
-    if (p.ipc)
+    if (kExt && p.ipc)
       for (uint32_t c = k; c < contacts.y; c += span)
         accumulateContact(acc, b, p, fs->contactAlpha, contacts.x + c, src, tgt);
   }
@@ -3624,7 +3628,10 @@ int launchCopy(const Buffers& b, const DevParams* p, const float4* src, float4* 
 }
 
 int launchGate(const Buffers& b, const DevParams* p, const float4* src, const float4* tgt, cudaStream_t s) {
-  gateKernel<<<b.gateBlocks, kBlock, 0, s>>>(b, p, src, tgt);
+  if (b.clothRange || b.contactIdx)
+    gateKernel<true><<<b.gateBlocks, kBlock, 0, s>>>(b, p, src, tgt);
+  else
+    gateKernel<false><<<b.gateBlocks, kBlock, 0, s>>>(b, p, src, tgt);
   return 1;
 }
 
