@@ -881,9 +881,21 @@ __device__ __forceinline__ void contactLocal(const Buffers& b, const DevParams& 
   }
 }
 
+// JGS2_CONTACT_MIN_BLOCKS: blocks per SM the register budgets of the
+// per-candidate contact kernels (lag, safe step, validation, broad-phase
+// initialisation) must allow (0: the compiler's choice).
+#ifndef JGS2_CONTACT_MIN_BLOCKS
+#define JGS2_CONTACT_MIN_BLOCKS 0
+#endif
+#if JGS2_CONTACT_MIN_BLOCKS > 0
+#define JGS2_CONTACT_BOUNDS __launch_bounds__(kBlock, JGS2_CONTACT_MIN_BLOCKS)
+#else
+#define JGS2_CONTACT_BOUNDS __launch_bounds__(kBlock)
+#endif
+
 // lagContact (:2712-2740): source cache and lagged normal force at the
 // accepted pose, once per frame.
-__global__ void __launch_bounds__(kBlock) contactLagKernel(Buffers b, const DevParams* __restrict__ pp) {
+__global__ void JGS2_CONTACT_BOUNDS contactLagKernel(Buffers b, const DevParams* __restrict__ pp) {
   const uint32_t c = blockIdx.x * kBlock + threadIdx.x;
   if (c >= b.contactCount) return;
   const uint32_t scene = b.contactScene[c];
@@ -1018,7 +1030,7 @@ __device__ __forceinline__ void contactStepOne(const Buffers& b, const DevParams
 
 // candidateContactStep (:2784-2847) with the min / all-valid reduction of
 // reduceContactStep folded in as order-free atomics.
-__global__ void __launch_bounds__(kBlock) contactStepKernel(Buffers b, const DevParams* __restrict__ pp,
+__global__ void JGS2_CONTACT_BOUNDS contactStepKernel(Buffers b, const DevParams* __restrict__ pp,
                                                             const float4* __restrict__ src,
                                                             const float4* __restrict__ tgt) {
   const uint32_t n = contactListed(b);
@@ -1050,7 +1062,7 @@ __global__ void __launch_bounds__(kBlock) contactApplyKernel(Buffers b, const De
 
 // validateContactStep (:2849-2868): exact contacts of the scaled candidate
 // (the target cache) and the all-valid reduction.
-__global__ void __launch_bounds__(kBlock) contactValidateKernel(Buffers b, const DevParams* __restrict__ pp,
+__global__ void JGS2_CONTACT_BOUNDS contactValidateKernel(Buffers b, const DevParams* __restrict__ pp,
                                                                 const float4* __restrict__ tgt) {
   const uint32_t n = contactListed(b);
   for (uint32_t c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock) {
@@ -1299,7 +1311,7 @@ __global__ void __launch_bounds__(kBlock) bpSuperKernel(Buffers b, uint32_t triS
 // lagged force as lagContact (:2712-2740) forms them; its activity
 // (contactIncluded) and its four sort entries (vertex, candidate), whose key
 // is the sentinel when the pair is inactive.  One thread per candidate.
-__global__ void __launch_bounds__(kBlock) bpInitKernel(Buffers b, const DevParams* __restrict__ pp,
+__global__ void JGS2_CONTACT_BOUNDS bpInitKernel(Buffers b, const DevParams* __restrict__ pp,
                                                        const float4* __restrict__ src, int first) {
   const uint32_t n = __ldcg(b.bpStatus);
   for (uint32_t c = blockIdx.x * kBlock + threadIdx.x; c < n; c += gridDim.x * kBlock) {
