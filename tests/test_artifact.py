@@ -73,3 +73,12 @@ def test_stale_or_corrupt_artifacts_are_rejected(tmp_path):
     np.savez(path, **data)
     with pytest.raises(artifact.ArtifactMismatch, match="schema"):
         artifact.load(path, prints, scenes.SceneInput)
+
+
+def test_trainer_revision_is_fingerprinted(monkeypatch):
+    # A change to the training arithmetic (its revision) changes the cubature
+    # fingerprint alone, so caches made by an earlier trainer are not reused.
+    before = artifact.fingerprints(scenes.unit_cube_components(cells=3))
+    monkeypatch.setattr(scenes, "TRAINER_REVISION", scenes.TRAINER_REVISION + 1)
+    after = artifact.fingerprints(scenes.unit_cube_components(cells=3))
+    assert [c for c in artifact.COMPONENTS if before[c] != after[c]] == ["cubature"]
