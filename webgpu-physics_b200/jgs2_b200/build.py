@@ -122,9 +122,6 @@ def build_scene_library(force=False, verbose=False) -> str:
     for obj in objs:
         os.remove(obj)
     return target
-    _run([_cxx(), "-O3", "-march=x86-64-v3", "-fopenmp", "-fPIC", "-shared", "-std=c++17", "-I", INCLUDE,
-          "-I", sdir, *sources, "-o", target], verbose)
-    return target
 
 
 def build_all(force=False, verbose=False):
