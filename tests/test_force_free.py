@@ -1,0 +1,123 @@
+"""Force-free conservation, the reference's P0-EC-10/11
+(tests/e2e/jgs2.spec.ts:470-575).
+
+The fixture is the reference's canonical force-free cuboid
+(src/scenes/canonical-phase0.ts:20-166):
+- an unconstrained 2x2x2-hex cube, origin -0.5, edge 1 m;
+- density 1000, E 8e4, nu 0.3 (src/simulation/cpu/phase0-canonical.ts:42-48);
+- exact all-element cubature, one weight-one record per tetrahedron;
+- h = 1/120, 12 iterations, no gravity or floor, parity mode.
+
+It starts at its rest shape rotated by the Euler angles (0.17, -0.23, 0.31),
+applied about x, then y, then z (src/simulation/cpu/mesh.ts:210-235). Its
+initial velocity is the rigid field v_cm + w x (x - x_cm), with
+v_cm = (0.37, -0.11, 0.23), w = (0.41, 0.29, -0.19) and x_cm the lumped-mass
+centre (canonical-phase0.ts:38-41, 232-268).
+
+After 4 s (480 frames) two quantities are checked: the total linear momentum
+and the total angular momentum about the origin
+(src/simulation/diagnostics.ts:166-207). Each must differ from its initial
+value by less than 0.005. The linear error is normalised by max(|P0|, M d)
+and the angular one by max(|L0|, M d^2), with M the total mass and d the
+initial bounding-box diagonal (jgs2.spec.ts:540-575).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from jgs2_b200 import scenes, solver
+from oracle import oracle as O
+
+MOMENTUM_TOL = 0.005
+POSITION_TOL = 1e-4  # of the bounding-box diagonal
+FRAMES = 480  # 4 s at h = 1/120
+SETTINGS = dict(timestep=1 / 120, gravity=(0.0, 0.0, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=12)
+
+
+def _euler_xyz(e):
+    cx, sx = math.cos(e[0]), math.sin(e[0])
+    cy, sy = math.cos(e[1]), math.sin(e[1])
+    cz, sz = math.cos(e[2]), math.sin(e[2])
+    rx = np.array([[1, 0, 0], [0, cx, -sx], [0, sx, cx]])
+    ry = np.array([[cy, 0, sy], [0, 1, 0], [-sy, 0, cy]])
+    rz = np.array([[cz, -sz, 0], [sz, cz, 0], [0, 0, 1]])
+    return rz @ ry @ rx
+
+
+def _force_free_cuboid():
+    """The fixture's packed input and its lumped vertex masses."""
+    sc = scenes.Scene()
+    m = sc.add_material(1000.0, 8.0e4, 0.3)
+    sc.add_cuboid((2, 2, 2), (-0.5, -0.5, -0.5), (1.0, 1.0, 1.0), m, 0, 0)
+    sc.precompute(timestep=SETTINGS["timestep"], cubature_k=sc.tet_count, exact_complement=1)
+    mass = sc.pack().vertex_rest.reshape(-1, 4)[:, 3].astype(np.float64)
+    rest = sc.rest_positions()
+    pos = np.ones((rest.shape[0], 4), dtype=np.float32)
+    pos[:, :3] = rest @ _euler_xyz((0.17, -0.23, 0.31)).T
+    centre = (mass[:, None] * pos[:, :3]).sum(0) / mass.sum()
+    v_cm = np.array([0.37, -0.11, 0.23])
+    omega = np.array([0.41, 0.29, -0.19])
+    vel = np.zeros_like(pos)
+    vel[:, :3] = v_cm + np.cross(omega, pos[:, :3] - centre)
+    sc.set_initial_state(pos.reshape(-1), vel.reshape(-1), pin_at_initial=False)
+    return sc.pack(), mass
+
+
+def _momenta(positions, velocities, mass):
+    x = positions.reshape(-1, 4)[:, :3].astype(np.float64)
+    p = mass[:, None] * velocities.reshape(-1, 4)[:, :3].astype(np.float64)
+    return p.sum(0), np.cross(x, p).sum(0)
+
+
+def _momentum_errors(inp, mass, positions, velocities):
+    p0, l0 = _momenta(inp.positions, inp.velocities, mass)
+    p1, l1 = _momenta(positions, velocities, mass)
+    m, d = mass.sum(), inp.bbox_diagonal()
+    linear = float(np.linalg.norm(p1 - p0) / max(np.linalg.norm(p0), m * d))
+    angular = float(np.linalg.norm(l1 - l0) / max(np.linalg.norm(l0), m * d * d))
+    return linear, angular
+
+
+def test_fixture_moves_rigidly_at_start():
+    inp, mass = _force_free_cuboid()
+    assert inp.vertex_count == 27 and inp.tet_count == 48
+    assert abs(mass.sum() - 1000.0) < 1e-3
+    p0, l0 = _momenta(inp.positions, inp.velocities, mass)
+    np.testing.assert_allclose(p0, 1000.0 * np.array([0.37, -0.11, 0.23]), rtol=1e-5)
+    assert np.linalg.norm(l0) > 0.0
+
+
+def test_oracle_conserves_momentum_force_free():
+    inp, mass = _force_free_cuboid()
+    cpu = O.OracleSolver(inp, SETTINGS, precision=32)
+    cpu.step_frames(FRAMES)
+    linear, angular = _momentum_errors(inp, mass, cpu.read("positions"), cpu.read("velocities"))
+    print(f"oracle f32, {FRAMES} frames: linear {linear:.3e}, angular {angular:.3e}")
+    assert linear < MOMENTUM_TOL and angular < MOMENTUM_TOL
+
+
+@pytest.mark.gpu
+def test_gpu_conserves_momentum_force_free():
+    inp, mass = _force_free_cuboid()
+    camel = dict(timestep=SETTINGS["timestep"], gravity=SETTINGS["gravity"], floorStiffness=0.0, parityMode=True,
+                 iterations=SETTINGS["iterations"])
+    gpu = solver.JGS2GpuSolver.create(inp, camel)
+    cpu = O.OracleSolver(inp, SETTINGS, precision=32)
+    try:
+        # The first second against the f32 oracle (the reference's sentinel
+        # depth), then the whole 4 s on the GPU alone.
+        gpu.stepFrames(120)
+        cpu.step_frames(120)
+        diag = inp.bbox_diagonal()
+        g = gpu.readPositions().reshape(-1, 4)[:, :3]
+        c = cpu.read("positions").reshape(-1, 4)[:, :3]
+        err = float(np.abs(g - c).max()) / diag
+        assert err <= POSITION_TOL, f"position error after 120 frames {err:.3e} of bbox diagonal"
+        for _ in range((FRAMES - 120) // 120):
+            gpu.stepFrames(120)
+        linear, angular = _momentum_errors(inp, mass, gpu.readPositions(), gpu.readVelocities())
+    finally:
+        gpu.destroy()
+    print(f"GPU, {FRAMES} frames: linear {linear:.3e}, angular {angular:.3e}; 120-frame position error {err:.2e}")
+    assert linear < MOMENTUM_TOL and angular < MOMENTUM_TOL
