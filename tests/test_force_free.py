@@ -20,7 +20,14 @@ and the total angular momentum about the origin
 value by less than 0.005. The linear error is normalised by max(|P0|, M d)
 and the angular one by max(|L0|, M d^2), with M the total mass and d the
 initial bounding-box diagonal (jgs2.spec.ts:540-575).
+
+The reference's frozen corpus of 32 seeded rigid velocities (P0-CORPUS-01,
+jgs2.spec.ts:589-686) runs in its quick form: every case for one frame, and
+cases 0 and 27 for 120 frames. Each case must stay finite and uninverted,
+and hold the same momentum bound. The corpus generator is pinned to the
+reference's frozen cases 0 and 31.
 """
+import functools
 import math
 
 import numpy as np
@@ -45,8 +52,10 @@ def _euler_xyz(e):
     return rz @ ry @ rx
 
 
-def _force_free_cuboid():
-    """The fixture's packed input and its lumped vertex masses."""
+@functools.lru_cache(maxsize=1)
+def _fixture():
+    """The fixture's scene (precomputed once), its lumped vertex masses and
+    its rotated initial pose."""
     sc = scenes.Scene()
     m = sc.add_material(1000.0, 8.0e4, 0.3)
     sc.add_cuboid((2, 2, 2), (-0.5, -0.5, -0.5), (1.0, 1.0, 1.0), m, 0, 0)
@@ -55,11 +64,16 @@ def _force_free_cuboid():
     rest = sc.rest_positions()
     pos = np.ones((rest.shape[0], 4), dtype=np.float32)
     pos[:, :3] = rest @ _euler_xyz((0.17, -0.23, 0.31)).T
+    return sc, mass, pos
+
+
+def _force_free_cuboid(v_cm=(0.37, -0.11, 0.23), omega=(0.41, 0.29, -0.19)):
+    """The fixture's packed input with the rigid velocity field
+    v_cm + omega x (x - x_cm), and its lumped vertex masses."""
+    sc, mass, pos = _fixture()
     centre = (mass[:, None] * pos[:, :3]).sum(0) / mass.sum()
-    v_cm = np.array([0.37, -0.11, 0.23])
-    omega = np.array([0.41, 0.29, -0.19])
     vel = np.zeros_like(pos)
-    vel[:, :3] = v_cm + np.cross(omega, pos[:, :3] - centre)
+    vel[:, :3] = np.asarray(v_cm) + np.cross(np.asarray(omega), pos[:, :3] - centre)
     sc.set_initial_state(pos.reshape(-1), vel.reshape(-1), pin_at_initial=False)
     return sc.pack(), mass
 
@@ -121,3 +135,105 @@ def test_gpu_conserves_momentum_force_free():
         gpu.destroy()
     print(f"GPU, {FRAMES} frames: linear {linear:.3e}, angular {angular:.3e}; 120-frame position error {err:.2e}")
     assert linear < MOMENTUM_TOL and angular < MOMENTUM_TOL
+
+
+# ---- the frozen force-free corpus (P0-CORPUS-01, jgs2.spec.ts:589-686) ----
+CORPUS_SEED = 104729  # canonical-phase0.ts:26
+SENTINELS = (0, 27)  # the quick run's 120-frame cases (jgs2.spec.ts:44)
+
+
+def _corpus():
+    """generatePhase0ForceFreeInitialStateCorpus (canonical-phase0.ts:60-101):
+    32 cases, each a linear then an angular velocity; a velocity is a unit
+    direction (components uniform in [-1, 1), rejected when shorter than
+    1e-8, then normalised) times a speed uniform in [0.1, 1)."""
+    rand = scenes.mulberry32(CORPUS_SEED)
+
+    def unit():
+        while True:
+            c = [rand() * 2 - 1 for _ in range(3)]
+            n = math.hypot(*c)
+            if 1e-8 < n <= math.sqrt(3):
+                return [x / n for x in c]
+
+    def velocity():
+        d = unit()
+        speed = 0.1 + 0.9 * rand()
+        return [x * speed for x in d]
+
+    cases = []
+    for _ in range(32):
+        linear = velocity()
+        angular = velocity()
+        cases.append((linear, angular))
+    return cases
+
+
+def _min_tet_determinant(inp, positions):
+    x = positions.reshape(-1, 4)[:, :3].astype(np.float64)
+    t = inp.tet_indices.reshape(-1, 4)
+    e = np.stack([x[t[:, 1]] - x[t[:, 0]], x[t[:, 2]] - x[t[:, 0]], x[t[:, 3]] - x[t[:, 0]]], axis=-1)
+    return float(np.linalg.det(e).min())
+
+
+def test_corpus_generator_matches_frozen_vectors():
+    # The reference's frozen cases 00 and 31 (src/scenes/scenes.test.ts:251-275).
+    cases = _corpus()
+    np.testing.assert_allclose(cases[0][0], [-0.45846957506529673, 0.33551068797554123, -0.3184711985400522],
+                               rtol=1e-14)
+    np.testing.assert_allclose(cases[0][1], [-0.9724775707987993, 0.21396913055014707, 0.05338255748009366],
+                               rtol=1e-14)
+    np.testing.assert_allclose(cases[31][0], [-0.1613361445196155, -0.5490207886538739, -0.4162380237814731],
+                               rtol=1e-14)
+    np.testing.assert_allclose(cases[31][1], [-0.2369681366893712, -0.3062079393113022, -0.32347516329834597],
+                               rtol=1e-14)
+    for linear, angular in cases:
+        assert 0.1 <= math.hypot(*linear) <= 1.0 and 0.1 <= math.hypot(*angular) <= 1.0
+
+
+def _corpus_frames(i):
+    return 120 if i in SENTINELS else 1
+
+
+def _check_case(i, inp, mass, positions, velocities):
+    assert np.isfinite(positions).all() and np.isfinite(velocities).all(), f"case {i} not finite"
+    det = _min_tet_determinant(inp, positions)
+    assert det > 0.0, f"case {i} inverted (min det {det:.3e})"
+    linear, angular = _momentum_errors(inp, mass, positions, velocities)
+    assert linear <= MOMENTUM_TOL and angular <= MOMENTUM_TOL, f"case {i}: linear {linear:.3e}, angular {angular:.3e}"
+    return linear, angular
+
+
+def test_oracle_corpus_conserves_momentum():
+    worst = [0.0, 0.0]
+    for i, (linear, angular) in enumerate(_corpus()):
+        inp, mass = _force_free_cuboid(linear, angular)
+        cpu = O.OracleSolver(inp, SETTINGS, precision=32)
+        cpu.step_frames(_corpus_frames(i))
+        errs = _check_case(i, inp, mass, cpu.read("positions"), cpu.read("velocities"))
+        worst = [max(worst[0], errs[0]), max(worst[1], errs[1])]
+    print(f"oracle corpus: worst linear {worst[0]:.3e}, worst angular {worst[1]:.3e}")
+
+
+@pytest.mark.gpu
+def test_gpu_corpus_conserves_momentum():
+    camel = dict(timestep=SETTINGS["timestep"], gravity=SETTINGS["gravity"], floorStiffness=0.0, parityMode=True,
+                 iterations=SETTINGS["iterations"])
+    worst = [0.0, 0.0, 0.0]
+    for i, (linear, angular) in enumerate(_corpus()):
+        inp, mass = _force_free_cuboid(linear, angular)
+        gpu = solver.JGS2GpuSolver.create(inp, camel)
+        try:
+            gpu.stepFrames(_corpus_frames(i))
+            g, gv = gpu.readPositions(), gpu.readVelocities()
+        finally:
+            gpu.destroy()
+        errs = _check_case(i, inp, mass, g, gv)
+        cpu = O.OracleSolver(inp, SETTINGS, precision=32)
+        cpu.step_frames(_corpus_frames(i))
+        err = float(np.abs(g.reshape(-1, 4)[:, :3] - cpu.read("positions").reshape(-1, 4)[:, :3]).max())
+        err /= inp.bbox_diagonal()
+        assert err <= POSITION_TOL, f"case {i}: position error {err:.3e} of bbox diagonal"
+        worst = [max(worst[0], errs[0]), max(worst[1], errs[1]), max(worst[2], err)]
+    print(f"GPU corpus: worst linear {worst[0]:.3e}, worst angular {worst[1]:.3e}, "
+          f"worst position error vs f32 oracle {worst[2]:.2e}")
