@@ -2560,6 +2560,25 @@ void clothBendingElement(const double* x, double restAngle, double restLength, d
   }
   out[13] = d.valid ? 1.0 : 0.0;
 }
+template <class T>
+void snhDensity(const double* f, const double* h, double lambda, double mu, double* out) {
+  M3<T> F, H;
+  for (int col = 0; col < 3; ++col) {
+    F.c[col] = v3(static_cast<T>(f[col]), static_cast<T>(f[3 + col]), static_cast<T>(f[6 + col]));
+    H.c[col] = v3(static_cast<T>(h[col]), static_cast<T>(h[3 + col]), static_cast<T>(h[6 + col]));
+  }
+  const T l = static_cast<T>(lambda), m = static_cast<T>(mu);
+  const M3<T> P = snhPiola(F, l, m);
+  const M3<T> dP = snhTangent(F, H, l, m);
+  out[0] = snhEnergy(F, l, m);
+  for (int row = 0; row < 3; ++row)
+    for (int col = 0; col < 3; ++col) {
+      out[1 + 3 * row + col] = at(P, col, row);
+      out[10 + 3 * row + col] = at(dP, col, row);
+    }
+  out[19] = det(F);
+}
+
 }  // namespace
 extern "C" {
 
@@ -2634,6 +2653,20 @@ int jgs2_oracle_cloth_bending(const double* positions, double rest_angle, double
                               int precision, double* out) {
   if (precision == 64) clothBendingElement<double>(positions, rest_angle, rest_length, stiffness, out);
   else clothBendingElement<float>(positions, rest_angle, rest_length, stiffness, out);
+  return 0;
+}
+
+// The stable Neo-Hookean density of the step (snhEnergy, snhPiola,
+// snhTangent; stable-neo-hookean-wgsl.ts:14-95) for the reference's density
+// tests (src/simulation/cpu/stable-neo-hookean.test.ts:53-232).  f and h are
+// 3x3 matrices stored by rows.  out[0] = energy density, out[1..9] = first
+// Piola stress by rows, out[10..18] = the tangent action dP(f)[h] by rows,
+// out[19] = det f.  precision 32 rounds the inputs to float and evaluates in
+// float.
+int jgs2_oracle_snh_density(const double* f, const double* h, double lambda, double mu, int precision,
+                            double* out) {
+  if (precision == 64) snhDensity<double>(f, h, lambda, mu, out);
+  else snhDensity<float>(f, h, lambda, mu, out);
   return 0;
 }
 
