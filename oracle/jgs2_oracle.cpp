@@ -2579,6 +2579,18 @@ void snhDensity(const double* f, const double* h, double lambda, double mu, doub
   out[19] = det(F);
 }
 
+template <class T>
+void localSolve(const double* hessian, const double* gradient, double inertia, double* out) {
+  M3<T> H;
+  for (int col = 0; col < 3; ++col)
+    H.c[col] = v3(static_cast<T>(hessian[col]), static_cast<T>(hessian[3 + col]), static_cast<T>(hessian[6 + col]));
+  const V3<T> g = v3(static_cast<T>(gradient[0]), static_cast<T>(gradient[1]), static_cast<T>(gradient[2]));
+  const SolveResult<T> r = globalizationSolve(H, g, static_cast<T>(inertia));
+  out[0] = r.status;
+  out[1] = r.direction.x; out[2] = r.direction.y; out[3] = r.direction.z;
+  out[4] = r.gdd; out[5] = r.scale; out[6] = r.minEig; out[7] = r.shift; out[8] = r.asym; out[9] = r.residual;
+}
+
 }  // namespace
 extern "C" {
 
@@ -2663,6 +2675,35 @@ int jgs2_oracle_cloth_bending(const double* positions, double rest_angle, double
 // Piola stress by rows, out[10..18] = the tangent action dP(f)[h] by rows,
 // out[19] = det f.  precision 32 rounds the inputs to float and evaluates in
 // float.
+// The local globalization solve (globalizationSolve, jgs2-globalization-wgsl.ts:
+// 166-492) for the reference's globalization tests
+// (src/simulation/cpu/nonlinear-globalization.test.ts:38-158).  hessian is
+// 3x3 by rows, gradient 3 values, inertia the scale floor.  out[0] = status
+// code, out[1..3] = direction, out[4] = gradient . direction, out[5] = the
+// normalising scale, out[6] = minimum eigenvalue and out[7] = diagonal shift
+// of the normalised system, out[8] = maximum relative asymmetry, out[9] =
+// relative linear residual.
+int jgs2_oracle_local_solve(const double* hessian, const double* gradient, double inertia, int precision,
+                            double* out) {
+  if (precision == 64) localSolve<double>(hessian, gradient, inertia, out);
+  else localSolve<float>(hessian, gradient, inertia, out);
+  return 0;
+}
+
+// The closed-form minimum eigenvalue of the symmetric part's upper triangle
+// (minSymmetricEigenvalue); m is 3x3 by rows.
+double jgs2_oracle_min_symmetric_eigenvalue(const double* m, int precision) {
+  if (precision == 64) {
+    M3<double> a;
+    for (int col = 0; col < 3; ++col) a.c[col] = v3(m[col], m[3 + col], m[6 + col]);
+    return minSymmetricEigenvalue(a);
+  }
+  M3<float> a;
+  for (int col = 0; col < 3; ++col)
+    a.c[col] = v3(static_cast<float>(m[col]), static_cast<float>(m[3 + col]), static_cast<float>(m[6 + col]));
+  return minSymmetricEigenvalue(a);
+}
+
 int jgs2_oracle_snh_density(const double* f, const double* h, double lambda, double mu, int precision,
                             double* out) {
   if (precision == 64) snhDensity<double>(f, h, lambda, mu, out);
