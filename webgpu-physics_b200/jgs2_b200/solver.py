@@ -488,7 +488,9 @@ class JGS2GpuSolver:
         return {"positions": pos, "control": control, "history": history}
 
     def readGlobalizationDiagnostics(self) -> dict:
-        """{'local': (V,16), 'control': (16,), 'history': (count,32), 'historyCount': n}."""
+        """{'local': (V,16), 'control': (16,), 'history': (count,32), 'historyCount': n}: the raw
+        records.  jgs2_b200.diagnostics.decode_globalization(result) gives the reference's
+        decoded form (named fields, zero sentinels, validity flags)."""
         self._usable()
         local = np.empty(16 * self.vertexCount, dtype=np.float32)
         control = np.empty(16, dtype=np.float32)
