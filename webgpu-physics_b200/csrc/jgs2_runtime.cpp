@@ -315,8 +315,8 @@ bool validateInput(const jgs2_input* in, std::string* err) {
     }
   }
   if (offset != in->adjacency_length) {
-    *err = format("adjacency contains %llu unused entries.",
-                  static_cast<unsigned long long>(in->adjacency_length - offset));
+    const unsigned long long unused = in->adjacency_length - offset;
+    *err = format("adjacency contains %llu unused entr%s.", unused, unused == 1 ? "y" : "ies");
     return false;
   }
   {
