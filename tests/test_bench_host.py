@@ -41,3 +41,8 @@ def test_malformed_and_missing_samples():
     assert bench.ClockSampler(0).summary() is None  # never entered
     out = _sampler(["short, line", _line(1800)]).summary()
     assert out["samples"] == 1 and out["sm_mhz"] == 1800.0
+
+
+def test_l2_note_states_whether_the_working_set_exceeds_l2():
+    assert "more than the 126 MB L2" in bench.l2_note(1.506e9)
+    assert "fits in the 126 MB L2" in bench.l2_note(1.0e6)
