@@ -94,36 +94,57 @@ def test_pinned_vertex_rejects_force(small_bar):
         solver.validate_input(bad)
 
 
-def _python_greedy_coloring(inp):
-    """buildGreedyVertexColoring over buildJGS2InputVertexColoring groups,
-    written out with plain Python loops (small cases only)."""
-    V = inp.vertex_count
-    adj = [set() for _ in range(V)]
-    groups = [list(inp.tet_indices[4 * t:4 * t + 4]) for t in range(inp.tet_count)]
-    K = inp.cubature_k
-    for v in range(V):
-        for s in range(K):
-            r = v * K + s
-            t = int(inp.cubature_tet_ids[r])
-            if t == 0xFFFFFFFF or not inp.cubature_weights[r] > 0:
-                continue
-            groups.append([v] + list(inp.tet_indices[4 * t:4 * t + 4]))
+def _greedy_coloring(vertex_count, groups):
+    """buildGreedyVertexColoring (src/simulation/cpu/vertex-coloring.ts:20-110)
+    over conflict groups, with plain Python loops (small cases only): every
+    vertex in order takes the smallest colour no neighbour holds."""
+    adj = [set() for _ in range(vertex_count)]
     for g in groups:
         u = list(dict.fromkeys(int(x) for x in g))
         for a in range(len(u)):
             for b in range(a + 1, len(u)):
                 adj[u[a]].add(u[b])
                 adj[u[b]].add(u[a])
-    colors = [None] * V
+    colors = [None] * vertex_count
     count = 0
-    for v in range(V):
+    for v in range(vertex_count):
         used = {colors[n] for n in adj[v] if colors[n] is not None}
         c = 0
         while c < count and c in used:
             c += 1
         colors[v] = c
         count = max(count, c + 1)
-    return np.array(colors, dtype=np.uint32), count, groups
+    return np.array(colors, dtype=np.uint32), count
+
+
+def _python_greedy_coloring(inp):
+    """The colouring over buildJGS2InputVertexColoring's groups: every tet,
+    and every cubature record's source vertex with its tet's vertices."""
+    groups = [list(inp.tet_indices[4 * t:4 * t + 4]) for t in range(inp.tet_count)]
+    K = inp.cubature_k
+    for v in range(inp.vertex_count):
+        for s in range(K):
+            r = v * K + s
+            t = int(inp.cubature_tet_ids[r])
+            if t == 0xFFFFFFFF or not inp.cubature_weights[r] > 0:
+                continue
+            groups.append([v] + list(inp.tet_indices[4 * t:4 * t + 4]))
+    colors, count = _greedy_coloring(inp.vertex_count, groups)
+    return colors, count, groups
+
+
+def test_greedy_coloring_matches_the_reference_known_answer():
+    # vertex-coloring.test.ts:6-29: tetrahedron, cloth and IPC groups.
+    groups = [[0, 1, 2, 3], [0, 4, 5], [1, 4, 6, 7], [2, 5, 6, 8]]
+    colors, count = _greedy_coloring(9, groups)
+    assert list(colors) == [0, 1, 2, 3, 2, 1, 0, 3, 3] and count == 4
+    counts = np.bincount(colors, minlength=count)
+    assert list(counts) == [2, 2, 2, 3]
+    assert list(np.concatenate([[0], np.cumsum(counts)])) == [0, 2, 4, 6, 9]
+    by_color = [v for c in range(count) for v in range(9) if colors[v] == c]
+    assert by_color == [0, 6, 1, 5, 2, 4, 3, 7, 8]
+    again, _ = _greedy_coloring(9, list(reversed(groups)))
+    assert list(again) == list(colors)
 
 
 def test_coloring_bit_exact_against_python_and_oracle(small_bar):
