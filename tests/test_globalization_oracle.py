@@ -91,3 +91,41 @@ def test_shift_and_solve_are_scale_invariant():
         else:
             np.testing.assert_allclose(r["direction"], ref["direction"], rtol=0, atol=1e-8)
             assert abs(r["shift"] - ref["shift"]) < 1e-12
+
+
+def _shift_cases():
+    # nonlinear-globalization-gpu.spec.ts:851-886: f32 inputs.
+    f = np.float32
+    cases = [("indefinite-accepted", [-5e-4, 1, 0.75], [1, -2, 0.5], 1.0),
+             ("inside-shift-cap", [f(EIGENVALUE_FLOOR - 0.000999), 1, 1], [1, -2, 0.5], 1.0),
+             ("outside-shift-cap", [f(EIGENVALUE_FLOOR - 0.001001), 1, 1], [1, -2, 0.5], 1.0)]
+    for s in (1e-12, 1.0, 1e12):
+        cases.append((f"scale-{s}", [-5e-4 * s, s, 0.75 * s], [s, -2 * s, 0.5 * s], float(f(s))))
+    out = []
+    for name, diag, grad, inertia in cases:
+        h = np.diag(np.array(diag, dtype=np.float32)).astype(np.float64)
+        g = np.array(grad, dtype=np.float32).astype(np.float64)
+        out.append((name, h, g, inertia))
+    return out
+
+
+@pytest.mark.parametrize("name,h,g,inertia", _shift_cases(), ids=[c[0] for c in _shift_cases()])
+def test_f32_solve_matches_the_fp64_policy(name, h, g, inertia):
+    # The same cases' bounds (:1040-1062): the f32 solve against the policy
+    # evaluated in double on the same f32 inputs.
+    f32 = _solve(h, g, inertia, precision=32)
+    f64 = _solve(h, g, inertia, precision=64)
+    accepted = f64["status"] == ACCEPTED
+    assert accepted == (name != "outside-shift-cap")
+    assert f32["status"] == (ACCEPTED if accepted else SHIFT_LIMIT)
+    rel = np.linalg.norm(f32["direction"] - f64["direction"]) / max(1.0, np.linalg.norm(f32["direction"]),
+                                                                  np.linalg.norm(f64["direction"]))
+    assert rel < 2e-4
+    assert abs(f32["min_eig"] - f64["min_eig"]) < 2e-6
+    assert abs(f32["shift"] - f64["shift"]) < 2e-6
+    assert abs(f32["scale"] - f64["scale"]) / max(1e-30, abs(f64["scale"])) < 2e-6
+    if accepted:
+        assert abs(f32["gdd"] - f64["gdd"]) / abs(f64["gdd"]) < 2e-4
+        assert f32["residual"] < 2e-5
+    else:
+        assert f32["gdd"] == 0.0 and f32["residual"] == 0.0
