@@ -209,6 +209,25 @@ def test_cloth_input_validation():
         solver.validate_input(bad)
 
 
+def test_cloth_validation_on_the_reference_cases():
+    # cloth-layout.test.ts:207-250: index, rest-data and material violations.
+    inp = scenes.cloth_drape()
+    cases = [
+        (lambda b: b.hinge_indices.__setitem__(3, b.hinge_indices[2]), "(?i)distinct"),
+        (lambda b: b.cloth_triangles.__setitem__(2, b.vertex_count + 5), "(?i)outside vertexCount"),
+        (lambda b: b.cloth_inverse_rest.__setitem__(slice(0, 4), np.array([1, 2, 2, 4], dtype=np.float32)),
+         "(?i)invertible"),
+        (lambda b: b.cloth_material.__setitem__(3, -1.0), "(?i)nonnegative"),
+        (lambda b: b.cloth_material.__setitem__(1, 0.5), "(?i)Poisson"),
+        (lambda b: b.cloth_rest_areas.__setitem__(1, 0.0), "(?i)positive"),
+    ]
+    for mutate, pattern in cases:
+        bad = inp.copy()
+        mutate(bad)
+        with pytest.raises(solver.JGS2RangeError, match=pattern):
+            solver.validate_input(bad)
+
+
 def test_cloth_requires_the_stable_path():
     # jgs2-solver.ts:998-1002: a co-rotated scene cannot carry cloth.
     sc = scenes.Scene()
