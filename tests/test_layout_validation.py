@@ -104,3 +104,23 @@ def test_rejects_a_mixed_material_solve():
     solver.validate_input(inp)
     with pytest.raises(solver.JGS2RangeError, match="(?i)cannot mix"):
         solver.JGS2GpuSolver.create(inp, {"iterations": 1})
+
+
+def test_host_mirror_refuses_arrays_the_counts_do_not_fit():
+    # The C-ABI sizes each array by the counts; the host mirror refuses a
+    # mismatch before any pointer reaches the library (the reference's
+    # "count does not match" and "must contain N values" checks,
+    # ipc-contact-layout.test.ts:169-177, layout.test.ts:183-201).
+    inp = _two_tets()
+    inp.external_forces = np.zeros(14, dtype=np.float32)
+    _rejects(inp, "externalForces must contain 15 values; got 14")
+    inp = _two_tets()
+    inp.positions = inp.positions.astype(np.float64)
+    _rejects(inp, "positions must be a contiguous float32 array")
+    inp = _two_tets()
+    inp.vertex_info = np.repeat(inp.vertex_info, 2)[::2]  # a strided view
+    _rejects(inp, "vertexInfo must be a contiguous uint32 array")
+    trough = scenes.trough(1)
+    trough.contact_counts = trough.contact_counts.copy()
+    trough.contact_counts[0] += 1
+    _rejects(trough, r"contactIndices must contain \d+ values")

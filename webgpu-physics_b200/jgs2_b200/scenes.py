@@ -126,7 +126,45 @@ class SceneInput:
          c.bending_stiffness) = (float(x) for x in self.cloth_material)
         return c
 
+    def check_arrays(self):
+        """The C-ABI takes plain pointers and sizes every array by the counts
+        (vertices, tets, records, candidates, triangles, hinges), so a
+        mis-sized, wrongly typed or strided array would be read out of
+        bounds or misread.  Refuse such arrays here, before any pointer is
+        taken, as the reference's layout validation does ("... must contain
+        N values", src/simulation/gpu/layout.ts).  Absent (None) arrays are
+        left to the library's own validation."""
+        from .solver import JGS2RangeError
+
+        V, T, K = self.vertex_count, self.tet_count, self.cubature_k
+        f32, u32 = np.float32, np.uint32
+        spec = [("positions", f32, 4 * V), ("velocities", f32, 4 * V), ("vertex_rest", f32, 4 * V),
+                ("vertex_colors", f32, 4 * V), ("vertex_info", u32, 4 * V), ("external_forces", f32, 3 * V),
+                ("target_positions", f32, 3 * V), ("target_stiffnesses", f32, V), ("tet_indices", u32, 4 * T),
+                ("tet_inverse_dm", f32, 12 * T), ("tet_meta", f32, 4 * T), ("tet_rest_stiffness", f32, 144 * T),
+                ("adjacency", u32, None), ("cubature_tet_ids", u32, V * K), ("cubature_weights", f32, V * K),
+                ("cubature_basis", f32, 36 * V * K)]
+        if self.contact_counts is not None and self.contact_candidate_count > 0:
+            spec.append(("contact_indices", u32, 4 * self.contact_candidate_count))
+        if self.contact_surface is not None:
+            spec.append(("contact_surface", u32, 3 * (self.contact_surface.size // 3)))
+        if self.cloth_triangles is not None:
+            C, H = self.cloth_triangles.size // 3, (0 if self.hinge_indices is None else self.hinge_indices.size // 4)
+            spec += [("cloth_triangles", u32, 3 * C), ("cloth_inverse_rest", f32, 4 * C),
+                     ("cloth_rest_areas", f32, C), ("hinge_indices", u32, 4 * H), ("hinge_rest_angles", f32, H),
+                     ("hinge_rest_edge_lengths", f32, H), ("cloth_material", f32, 4)]
+        for name, dtype, size in spec:
+            a = getattr(self, name)
+            if a is None:
+                continue
+            label = name.split("_")[0] + "".join(w.capitalize() for w in name.split("_")[1:])
+            if not isinstance(a, np.ndarray) or a.dtype != dtype or not a.flags.c_contiguous:
+                raise JGS2RangeError(1, f"{label} must be a contiguous {np.dtype(dtype).name} array.")
+            if size is not None and a.size != size:
+                raise JGS2RangeError(1, f"{label} must contain {size} values; got {a.size}.")
+
     def as_ctypes(self) -> _ffi.Input:
+        self.check_arrays()
         rec = _ffi.Input()
         rec.vertex_count = self.vertex_count
         rec.tet_count = self.tet_count
