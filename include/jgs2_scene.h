@@ -174,6 +174,25 @@ jgs2_status jgs2_scene_precompute(jgs2_scene* scene,
                                   const jgs2_precompute_options* options,
                                   jgs2_precompute_stats* stats);
 
+/* selectGreedyNonnegativeColumns (src/simulation/cpu/cubature.ts:508-690),
+ * through the cubature trainer's own selection core.  columns: column_count
+ * columns of `rows` values each, stored one column after another; target:
+ * `rows` values.  The columns whose squared norm exceeds 1e-18 are the
+ * candidates.  Each greedy step appends the candidate whose nonnegative
+ * least-squares fit leaves the smallest residual, ties going to the lower
+ * index.  Growth stops at max_columns (at most 12), when no candidate
+ * helps, or when the normalised residual drops below residual_tolerance.
+ * Then refinement_passes swap passes follow.  selected and weights receive
+ * *selected_count entries in selection order; normalized_residual is the
+ * final residual over the target norm (0 for a zero target, 1 when no
+ * candidate exists).  Invalid sizes, non-finite values or a tolerance
+ * outside [0, 1] give JGS2_INVALID_ARGUMENT. */
+jgs2_status jgs2_select_nonnegative_columns(const double* columns, uint32_t column_count, uint32_t rows,
+                                            const double* target, uint32_t max_columns,
+                                            uint32_t refinement_passes, double residual_tolerance,
+                                            uint32_t* selected, double* weights, uint32_t* selected_count,
+                                            double* normalized_residual);
+
 /* Initial pose (4 * V floats, xyz used) and optional velocities (4 * V).
  * With pin_at_initial != 0 the pin targets (vertex_rest.xyz of pinned
  * vertices) are set to the initial positions instead of the rest positions. */

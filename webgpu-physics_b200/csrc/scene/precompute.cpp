@@ -595,7 +595,7 @@ Candidates candidates(const Training& tr) {
 // that helps (selectGreedyNonnegativeColumns, cubature.ts:508-690).  The
 // trial systems, the NNLS and the scan rule are cubature_select.hpp's, shared
 // with the GPU selection.
-SelectOutput selectOnCpu(const Training& tr, const Candidates& cs) {
+SelectOutput selectOnCpu(const Training& tr, const Candidates& cs, double tolerance = kResidualTolerance) {
   using namespace jgs2select;
   SelectOutput ch;
   if (cs.status != Candidates::kReady) return ch;
@@ -634,7 +634,7 @@ SelectOutput selectOnCpu(const Training& tr, const Candidates& cs) {
     ch.count = k + 1;
     setRow(k);
     err = bestErr;
-    if (std::sqrt(maxd(err, 0.0)) / cs.tn < kResidualTolerance) break;
+    if (std::sqrt(maxd(err, 0.0)) / cs.tn < tolerance) break;
   }
   for (int pass = 0; pass < tr.passes && ch.count > 0; ++pass) {
     const int k = ch.count;
@@ -1556,3 +1556,48 @@ bool runPrecompute(Scene& sc, const jgs2_precompute_options& opt, jgs2_precomput
 }
 
 }  // namespace jgs2scene
+
+extern "C" {
+
+// selectGreedyNonnegativeColumns (src/simulation/cpu/cubature.ts:508-690)
+// over caller columns, through the cubature trainer's own selection core
+// (the candidate filter, the greedy growth by exhaustive NNLS fits, the
+// refinement swaps and the final residual), which the GPU selection matches
+// bit for bit.
+jgs2_status jgs2_select_nonnegative_columns(const double* columns, uint32_t column_count, uint32_t rows,
+                                            const double* target, uint32_t max_columns, uint32_t refinement_passes,
+                                            double residual_tolerance, uint32_t* selected, double* weights,
+                                            uint32_t* selected_count, double* normalized_residual) {
+  using namespace jgs2scene;
+  if (rows == 0 || !target || !selected_count || !normalized_residual || (column_count > 0 && !columns) ||
+      (max_columns > 0 && (!selected || !weights)) || max_columns > static_cast<uint32_t>(jgs2select::kMaxColumns) ||
+      !(residual_tolerance >= 0.0 && residual_tolerance <= 1.0))
+    return JGS2_INVALID_ARGUMENT;
+  const size_t n = static_cast<size_t>(column_count) * rows;
+  for (size_t i = 0; i < n; ++i)
+    if (!std::isfinite(columns[i])) return JGS2_INVALID_ARGUMENT;
+  for (uint32_t r = 0; r < rows; ++r)
+    if (!std::isfinite(target[r])) return JGS2_INVALID_ARGUMENT;
+  try {
+    Training tr;
+    tr.cols.resize(column_count);
+    for (uint32_t c = 0; c < column_count; ++c)
+      tr.cols[c].assign(columns + static_cast<size_t>(c) * rows, columns + static_cast<size_t>(c + 1) * rows);
+    tr.target.assign(target, target + rows);
+    tr.maxColumns = static_cast<int>(max_columns);
+    tr.passes = static_cast<int>(refinement_passes);
+    const Candidates cs = candidates(tr);
+    const Selection sel = finishSelection(tr, cs, selectOnCpu(tr, cs, residual_tolerance));
+    *selected_count = static_cast<uint32_t>(sel.tets.size());
+    for (size_t i = 0; i < sel.tets.size(); ++i) {
+      selected[i] = static_cast<uint32_t>(sel.tets[i]);
+      weights[i] = sel.weights[i];
+    }
+    *normalized_residual = sel.residual;
+  } catch (const std::exception&) {
+    return JGS2_INVALID_ARGUMENT;
+  }
+  return JGS2_OK;
+}
+
+}  // extern "C"

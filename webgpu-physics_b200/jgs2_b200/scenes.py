@@ -36,6 +36,36 @@ FACE_X_MIN, FACE_X_MAX, FACE_Y_MIN, FACE_Y_MAX, FACE_Z_MIN, FACE_Z_MAX = (
 EMPTY_TET = 0xFFFFFFFF
 
 
+def select_nonnegative_columns(columns, target, max_columns, refinement_passes=4, residual_tolerance=0.01) -> dict:
+    """selectGreedyNonnegativeColumns (src/simulation/cpu/cubature.ts:508-690)
+    through the cubature trainer's selection core (jgs2_select_nonnegative_columns):
+    {'selected': column indices in selection order, 'weights', 'normalizedResidual'}.
+    The defaults are the reference's (4 refinement passes, tolerance 0.01)."""
+    from ctypes import POINTER, byref
+
+    from .solver import JGS2RangeError
+
+    L = _ffi.scene_lib()
+    D = POINTER(c_double)
+    L.jgs2_select_nonnegative_columns.argtypes = [D, c_uint32, c_uint32, D, c_uint32, c_uint32, c_double,
+                                                  POINTER(c_uint32), D, POINTER(c_uint32), D]
+    t = np.ascontiguousarray(target, dtype=np.float64).reshape(-1)
+    cols = np.ascontiguousarray(np.asarray(columns, dtype=np.float64).reshape(-1, t.size) if len(columns) else
+                                np.zeros((0, t.size)))
+    sel = np.zeros(max(1, max_columns), dtype=np.uint32)
+    w = np.zeros(max(1, max_columns), dtype=np.float64)
+    count, residual = c_uint32(0), c_double(0)
+    st = L.jgs2_select_nonnegative_columns(cols.ctypes.data_as(D), cols.shape[0], t.size, t.ctypes.data_as(D),
+                                           int(max_columns), int(refinement_passes), float(residual_tolerance),
+                                           sel.ctypes.data_as(POINTER(c_uint32)), w.ctypes.data_as(D),
+                                           byref(count), byref(residual))
+    if st != 0:
+        raise JGS2RangeError(st, "Invalid column selection input (sizes, values or settings).")
+    n = int(count.value)
+    return {"selected": [int(x) for x in sel[:n]], "weights": [float(x) for x in w[:n]],
+            "normalizedResidual": float(residual.value)}
+
+
 def mulberry32(seed: int):
     """createCorpusRandom (src/scenes/phase1.ts:106-115): uniform [0, 1)."""
     state = seed & 0xFFFFFFFF
