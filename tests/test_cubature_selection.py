@@ -59,3 +59,28 @@ def test_rejects_malformed_input():
         select([[math.nan, 0]], [1, 0], 1)
     with pytest.raises(JGS2RangeError):
         select([[1, 0]], [1, 0], 1, residual_tolerance=1.5)
+
+
+def test_linear_training_is_bounded_and_nonnegative():
+    # precompute.test.ts:580-606 on a co-rotated (linear) bar trained with
+    # K = 6: at most K records per vertex, nonnegative weights, a raw
+    # gradient residual below 0.3, and some record incident to its source.
+    import numpy as np
+
+    sc = scenes.Scene()
+    m = sc.add_material(1000.0, 1e5, 0.4, scenes.MATERIAL_COROTATED_LINEAR)
+    sc.add_cuboid((6, 2, 2), (0.0, 0.0, 0.0), (0.6, 0.2, 0.2), m, 0, scenes.FACE_X_MIN)
+    stats = sc.precompute(timestep=1 / 60, cubature_k=6)
+    inp = sc.pack()
+    K = inp.cubature_k
+    assert K <= 6
+    ids = inp.cubature_tet_ids.reshape(-1, K)
+    w = inp.cubature_weights.reshape(-1, K)
+    assert (w >= 0).all()
+    tets = inp.tet_indices.reshape(-1, 4)
+    incident = any(v in tets[t] for v in range(inp.vertex_count) for t in ids[v] if t != scenes.EMPTY_TET)
+    assert incident
+    assert stats["max_residual"] < 0.3
+    print(f"linear training: max residual {stats['max_residual']:.4f}, "
+          f"records per vertex <= {int((w > 0).sum(axis=1).max())}")
+    assert np.isfinite(inp.cubature_basis).all()
