@@ -16,6 +16,8 @@ deformation gradient over its incident tetrahedra, sum(vol F) / sum(vol)
 relative error 1e-4. The expected frames are computed independently here in
 float64, with the polar factor from an SVD.
 """
+import math
+
 import numpy as np
 import pytest
 
@@ -121,3 +123,33 @@ def test_gpu_frames_are_polar_averages():
     tets = inp.tet_indices.reshape(-1, 4).astype(np.int64)
     ds = np.stack([x[tets[:, k]] - x[tets[:, 0]] for k in (1, 2, 3)], axis=-1)
     assert float(np.linalg.det(ds).min()) > 0.0
+
+
+def _posed(transform, translation):
+    inp, rest, _ = _fixture()
+    pose = (rest @ np.asarray(transform).T + np.asarray(translation)).astype(np.float32)
+    p4 = np.ones((pose.shape[0], 4), dtype=np.float32)
+    p4[:, :3] = pose
+    out = inp.copy()
+    out.positions = p4.reshape(-1)
+    return out
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_oracle_frames_of_affine_and_rigid_poses(precision):
+    # deformation-gradient.test.ts:89-131: an affine pose A X + b gives every
+    # vertex, boundary or interior, the polar factor of A; a rigid motion
+    # R X + t gives R.
+    A = np.array([[1.1, 0.2, -0.05], [-0.1, 0.9, 0.15], [0.08, -0.12, 1.05]])
+    u, _, vt = np.linalg.svd(A)
+    a = 0.7
+    R = np.array([[math.cos(a), 0, math.sin(a)], [0, 1, 0], [-math.sin(a), 0, math.cos(a)]])
+    # The poses and rest data reach the step as f32, which bounds the FP64 run too.
+    tol = 1e-5 if precision == 32 else 1e-6
+    for transform, want in ((A, u @ vt), (R, R)):
+        inp = _posed(transform, (0.01, -0.02, 0.005))
+        cpu = O.OracleSolver(inp, SETTINGS, precision=precision)
+        cpu.step_exact_iterations(1)
+        frames = _frames(cpu.read("vertex_rotations"))
+        err = _max_relative_error(frames, np.broadcast_to(want, frames.shape))
+        assert err <= tol, f"f{precision}: {err:.2e}"
