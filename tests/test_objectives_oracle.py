@@ -4,7 +4,8 @@ f = m a on every free vertex, without gravity, steps like gravity a without
 forces. The inertial target of the second run moves by h^2 a. The first run
 adds -f to the gradient of every vertex and, through the complement
 records, of its neighbours; the two gradients are the same, and the two
-energies differ by a constant that the line search's differences cancel."""
+energies differ by a constant that the line search's differences cancel.
+A released target (zero stiffness) is exactly an absent objective."""
 import numpy as np
 import pytest
 
@@ -51,3 +52,21 @@ def test_constant_force_equals_predictor_gravity(k, precision, tol):
     ha, hb = a.read("history").reshape(64, 32), b.read("history").reshape(64, 32)
     # Same accept / revert decisions in every iteration.
     np.testing.assert_array_equal(ha[:8, 4:6], hb[:8, 4:6])
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_released_target_is_exactly_an_absent_objective(precision):
+    # nonlinear-restricted-energy.test.ts:421-456: target positions with zero
+    # stiffness change nothing, bit for bit.
+    inp = _bar(6)
+    released = inp.copy()
+    released.target_positions = (inp.positions.reshape(-1, 4)[:, :3] + 0.05).astype(np.float32).reshape(-1)
+    released.target_stiffnesses = np.zeros(inp.vertex_count, dtype=np.float32)
+    settings = dict(timestep=1 / 60, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=1, iterations=8)
+    a = O.OracleSolver(released, settings, precision=precision)
+    b = O.OracleSolver(inp, settings, precision=precision)
+    for _ in range(3):
+        a.step_exact_iterations(8)
+        b.step_exact_iterations(8)
+    for what in ("positions", "velocities", "history"):
+        np.testing.assert_array_equal(a.read(what), b.read(what))
