@@ -2495,12 +2495,19 @@ int jgs2_oracle_local_system(void* handle, const jgs2_settings* settings, uint32
       o.tetGradient(t, tg);
       V3<T> pg = v3<T>(0, 0, 0);
       for (int l = 0; l < 4; ++l) pg = pg + transpose(basis[l]) * (tg[l] + o.distributedInertiaGradient(q[l]));
+      if (o.objectiveFlags != 0)
+        for (int l = 0; l < 4; ++l) pg = pg + transpose(basis[l]) * o.distributedObjectiveGradient(q[l]);
       M3<T> ph = o.cubatureHessian(t, basis);
       for (int l = 0; l < 4; ++l) ph = ph + o.distributedInertiaWeight(q[l]) * (transpose(basis[l]) * basis[l]);
+      if (o.targetEnabled())
+        for (int l = 0; l < 4; ++l)
+          ph = ph + o.distributedTargetStiffness(q[l]) * (transpose(basis[l]) * basis[l]);
       const uint32_t ss = o.slotOf(q, v);
       if (ss < 4) {
         pg = pg - (tg[ss] + o.distributedInertiaGradient(v));
+        if (o.objectiveFlags != 0) pg = pg - o.distributedObjectiveGradient(v);
         ph = ph - (o.stableLocalHessian(t, ss) + o.distributedInertiaWeight(v) * identityM<T>());
+        if (o.targetEnabled()) ph = ph - o.distributedTargetStiffness(v) * identityM<T>();
       }
       gradient = gradient + w * pg;
       hessian = hessian + w * ph;

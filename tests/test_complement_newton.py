@@ -104,3 +104,33 @@ def test_exact_complement_local_step_is_the_global_newton_block():
     assert worst_h < 1e-6
     assert worst_g < 1e-4
     assert worst_step < 1e-4
+
+
+def test_exact_complement_projects_quadratic_targets_densely():
+    # nonlinear-restricted-energy.test.ts:343-420: with every tet at unit
+    # weight, target springs k |x - t|^2 / 2 on the free vertices enter the
+    # local system as the dense projection B^T (H + k) B, B^T (g + k (x - t)).
+    inp, rest, vel, pinned = _bar_at_rest_moving()
+    active = np.flatnonzero(~pinned)
+    rng = np.random.default_rng(11)
+    k = np.zeros(inp.vertex_count, dtype=np.float32)
+    k[active] = rng.uniform(50.0, 500.0, size=active.size).astype(np.float32)
+    targets = (inp.positions.reshape(-1, 4)[:, :3] + rng.uniform(-0.02, 0.02, (inp.vertex_count, 3))).astype(
+        np.float32)
+    inp.target_positions = targets.reshape(-1)
+    inp.target_stiffnesses = k
+    H, dof = _rest_system(inp, rest)
+    mass = inp.vertex_rest.reshape(-1, 4)[:, 3].astype(np.float64)
+    x = inp.positions.reshape(-1, 4)[:, :3].astype(np.float64)
+    g = np.concatenate([mass[v] / TIMESTEP ** 2 * (-TIMESTEP * vel[v]) + float(k[v]) * (x[v] - targets[v])
+                        for v in active])
+    Ht = H + np.diag(np.repeat(k[active].astype(np.float64), 3))
+    worst_h = worst_g = 0.0
+    for v in active:
+        g_loc, H_loc = _local_system(inp, int(v))
+        B = _stored_basis(inp, int(v), dof, H.shape[0])
+        h_red, g_red = B.T @ Ht @ B, B.T @ g
+        worst_h = max(worst_h, float(np.abs(H_loc - h_red).max() / np.abs(h_red).max()))
+        worst_g = max(worst_g, float(np.abs(g_loc - g_red).max() / np.abs(g_red).max()))
+    print(f"targets, dense projection: reduced Hessian {worst_h:.1e}, reduced gradient {worst_g:.1e}")
+    assert worst_h < 1e-6 and worst_g < 1e-4
