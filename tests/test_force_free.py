@@ -237,3 +237,22 @@ def test_gpu_corpus_conserves_momentum():
         worst = [max(worst[0], errs[0]), max(worst[1], errs[1]), max(worst[2], err)]
     print(f"GPU corpus: worst linear {worst[0]:.3e}, worst angular {worst[1]:.3e}, "
           f"worst position error vs f32 oracle {worst[2]:.2e}")
+
+
+@pytest.mark.parametrize("precision", [32, 64])
+def test_oracle_keeps_a_translated_rigid_pose_that_is_its_own_target(precision):
+    # nonlinear-oracle.test.ts:128-155: the rest shape rotated and moved
+    # rigidly, at rest, with no gravity, is its own inertial target and has
+    # no elastic force, so a frame leaves it where it is.
+    sc, mass, pos = _fixture()
+    moved = pos.copy()
+    moved[:, :3] += np.array([3.0, -1.5, 0.75], dtype=np.float32)
+    sc.set_initial_state(moved.reshape(-1), np.zeros_like(moved).reshape(-1), pin_at_initial=False)
+    inp = sc.pack()
+    cpu = O.OracleSolver(inp, SETTINGS, precision=precision)
+    cpu.step_frames(2)
+    err = float(np.abs(cpu.read("positions").reshape(-1, 4)[:, :3] - moved[:, :3]).max()) / inp.bbox_diagonal()
+    vel = float(np.abs(cpu.read("velocities")).max())
+    print(f"oracle f{precision}: rigid pose moved by {err:.2e} of the diagonal, speed {vel:.2e}")
+    assert err < (1e-6 if precision == 32 else 1e-12)
+    assert vel < (1e-4 if precision == 32 else 1e-10)
