@@ -2697,6 +2697,48 @@ int jgs2_oracle_local_solve(const double* hessian, const double* gradient, doubl
   return 0;
 }
 
+// The step's convergence reduction (reduceConvergence) on caller data, for
+// the reference's convergence cases
+// (src/simulation/cpu/nonlinear-iteration.test.ts:181-400).  components: 20
+// floats per vertex, the inertia, material, external-force, target and
+// contact gradients as xyz_ each; updates: the accepted update length per
+// vertex; control: the 16-float control record (geometry minima and validity
+// bits, accept / revert flags, failures, history index, energies, sweep
+// aggregates); scene_scale < 0 keeps the input's.  history_out receives the
+// 32-float history record the reduction writes.
+int jgs2_oracle_reduce_convergence(void* handle, const jgs2_settings* settings, const float* components,
+                                   const float* updates, const float* control, double scene_scale,
+                                   float* history_out) {
+  Handle* h = static_cast<Handle*>(handle);
+  auto body = [&](auto& o) {
+    using T = std::remove_reference_t<decltype(o.dt)>;
+    applySettings(o, settings, false);
+    for (uint32_t v = 0; v < o.V; ++v) {
+      for (int c = 0; c < 5; ++c) {
+        const float* q = components + 20ull * v + 4 * c;
+        o.conv[5ull * v + c] = {static_cast<T>(q[0]), static_cast<T>(q[1]), static_cast<T>(q[2]), T(0)};
+      }
+      o.finalUpdate[v] = {static_cast<T>(updates[v]), T(0), T(0), T(0)};
+    }
+    for (int i = 0; i < 4; ++i)
+      o.control[i] = {static_cast<T>(control[4 * i]), static_cast<T>(control[4 * i + 1]),
+                      static_cast<T>(control[4 * i + 2]), static_cast<T>(control[4 * i + 3])};
+    if (scene_scale >= 0) o.sceneScale = static_cast<T>(scene_scale);
+    const float hiRaw = control[7];
+    o.reduceConvergence();
+    const uint32_t hi = hiRaw >= 0 && hiRaw < float(kHistoryCapacity) ? static_cast<uint32_t>(hiRaw) : 0u;
+    for (int k = 0; k < 8; ++k) {
+      const V4<T> r = o.history[8ull * hi + k];
+      history_out[4 * k] = static_cast<float>(r.x);
+      history_out[4 * k + 1] = static_cast<float>(r.y);
+      history_out[4 * k + 2] = static_cast<float>(r.z);
+      history_out[4 * k + 3] = static_cast<float>(r.w);
+    }
+  };
+  if (h->dbl) body(h->d); else body(h->f);
+  return 0;
+}
+
 // The closed-form minimum eigenvalue of the symmetric part's upper triangle
 // (minSymmetricEigenvalue); m is 3x3 by rows.
 double jgs2_oracle_min_symmetric_eigenvalue(const double* m, int precision) {
