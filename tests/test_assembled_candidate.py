@@ -171,3 +171,22 @@ def test_gpu_pinned_target_revert(tet):
     assert d["historyCount"] == 1
     _check_pinned_target(inp, gpu.readPositions(), np.asarray(d["history"][0], dtype=np.float32))
     gpu.destroy()
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_gate_reports_the_exact_determinant_of_an_affine_candidate(precision):
+    # nonlinear-oracle.test.ts:304-330: an affine pose A X gives every tet the
+    # deformation gradient A, so the gate's candidate minimum is det A.
+    sc = scenes.Scene()
+    m = sc.add_material(1000.0, 1e5, 0.4)
+    sc.add_cuboid((2, 1, 1), (0.0, 0.0, 0.0), (0.2, 0.1, 0.1), m, 0, 0)
+    sc.precompute(timestep=1 / 60, cubature_k=sc.tet_count, exact_complement=1)
+    inp = sc.pack()
+    A = np.array([[0.9, 0.1, 0.0], [-0.05, 1.1, 0.2], [0.0, 0.05, 0.85]])
+    rest = inp.positions.reshape(-1, 4).copy()
+    cand = rest.copy()
+    cand[:, :3] = (rest[:, :3].astype(np.float64) @ A.T).astype(np.float32)
+    cpu = O.OracleSolver(inp, SETTINGS, precision=precision)
+    control = cpu.evaluate_assembled_candidate(rest.reshape(-1), cand.reshape(-1))["control"]
+    assert abs(control[0] - 1.0) < 1e-6  # the source is the rest shape
+    assert abs(control[1] - np.linalg.det(A)) < (1e-6 if precision == 64 else 1e-5)
