@@ -26,6 +26,20 @@
 // Parity of this restatement with the reference is pinned only at the
 // tolerance level: the reference runs in a browser WebGPU stack that cannot
 // run here, so bitwise f32 agreement with WGSL is not claimed.
+//
+// The restatement is pinned to the known answers of the reference's own
+// tests, through the test entry points at the end of this file:
+// - the stable Neo-Hookean density (stable-neo-hookean.test.ts);
+// - the local globalization solve and its shift cases
+//   (nonlinear-globalization.test.ts, nonlinear-globalization-gpu.spec.ts);
+// - the convergence reduction (nonlinear-iteration.test.ts);
+// - the assembled gate (nonlinear-globalization-gpu.spec.ts);
+// - IPC barrier, friction and distances (ipc-contact.test.ts);
+// - cloth elements (cloth.test.ts);
+// - the local system's dense projections (precompute.test.ts,
+//   nonlinear-restricted-energy.test.ts);
+// - vertex frames, force-free momentum, and the schedule comparison
+//   (the e2e specs).
 #include <omp.h>
 
 #include <algorithm>
