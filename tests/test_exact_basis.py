@@ -84,3 +84,37 @@ def test_exact_bases_match_the_restated_rest_system():
     assert checked > 0
     # f32 storage of entries of order one.
     assert worst < 5e-7
+
+
+def test_corotated_rest_stiffness_is_symmetric_and_translation_free():
+    # precompute.test.ts:296-332: every element's linear rest stiffness is
+    # symmetric, annihilates rigid translations, and equals the Hooke
+    # element matrix of its rest geometry.
+    sc = scenes.Scene()
+    m = sc.add_material(DENSITY, YOUNG, POISSON, scenes.MATERIAL_COROTATED_LINEAR)
+    sc.add_cuboid((2, 2, 1), (0.0, 0.0, 0.0), (0.2, 0.2, 0.1), m, 0, scenes.FACE_X_MIN)
+    sc.precompute(timestep=TIMESTEP, cubature_k=sc.tet_count, exact_complement=1)
+    inp = sc.pack()
+    rest = sc.rest_positions().astype(np.float64)
+    Ks = inp.tet_rest_stiffness.reshape(-1, 12, 12).astype(np.float64)
+    tets = inp.tet_indices.reshape(-1, 4).astype(np.int64)
+    mu = YOUNG / (2 * (1 + POISSON))
+    lam = YOUNG * POISSON / ((1 + POISSON) * (1 - 2 * POISSON))
+    for t, K in zip(tets, Ks):
+        scale = np.abs(K).max()
+        assert np.abs(K - K.T).max() <= 1e-6 * scale
+        for axis in range(3):
+            shift = np.zeros(12)
+            shift[axis::3] = 1.0
+            assert np.abs(K @ shift).max() <= 1e-6 * scale
+        dm = np.stack([rest[t[k]] - rest[t[0]] for k in (1, 2, 3)], axis=1)
+        vol = abs(np.linalg.det(dm)) / 6.0
+        g = np.linalg.inv(dm)
+        grads = np.vstack([-g.sum(axis=0), g])
+        want = np.zeros((12, 12))
+        for a in range(4):
+            for b in range(4):
+                ga, gb = grads[a], grads[b]
+                want[3 * a:3 * a + 3, 3 * b:3 * b + 3] = vol * (mu * (ga @ gb) * np.eye(3) + mu * np.outer(gb, ga)
+                                                               + lam * np.outer(ga, gb))
+        assert np.abs(K - want).max() <= 1e-6 * scale
