@@ -9,7 +9,7 @@ multiply-adds."""
 import numpy as np
 import pytest
 
-from jgs2_b200 import _ffi, scenes
+from jgs2_b200 import scenes
 
 pytestmark = pytest.mark.gpu
 
