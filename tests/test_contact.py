@@ -138,6 +138,17 @@ def test_trough_matches_the_reference_candidate_count():
     solver.validate_input(inp)
 
 
+def test_trough_box_count_configures_bodies():
+    # ipc-trough-demo.spec.ts:49-72: boxes=3 gives four bodies (the trough
+    # and three boxes); the ten-box trough is the roadmap's 92 vertices and
+    # 72 tets (docs/ROADMAP.md:319-320).
+    for boxes in (1, 3, 10):
+        inp = scenes.trough(boxes)
+        assert len(np.unique(inp.vertex_info.reshape(-1, 4)[:, 3])) == boxes + 1
+    ten = scenes.trough(10)
+    assert (ten.vertex_count, ten.tet_count) == (92, 72)
+
+
 def test_contact_validation_and_create_checks():
     inp = scenes.trough(1)
     bad = inp.copy()
