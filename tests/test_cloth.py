@@ -182,6 +182,7 @@ def test_drape_matches_the_reference_topology():
     info = inp.vertex_info.reshape(-1, 4)
     assert int(info[:8, 2].sum()) == 8
     assert int(info[8:, 2].sum()) == 2
+    assert int((info[8:, 2] == 0).sum()) == 23  # cloth-demo.spec.ts:126-128
     assert inp.hinge_count == 40
     big = scenes.cloth_sheet()
     assert big.cloth_triangle_count == 32258 and big.hinge_count == 48133
