@@ -188,6 +188,17 @@ def test_drape_matches_the_reference_topology():
     assert big.cloth_triangle_count == 32258 and big.hinge_count == 48133
 
 
+
+def test_drape_static_candidates_include_cloth_self_contact():
+    # cloth-demo.spec.ts:129-132: the topology-filtered IPC candidates include
+    # nonlocal cloth self-contact, beside the collider-cloth pairs.
+    inp = scenes.cloth_drape(contact=scenes.CONTACT_STATIC)
+    solver.validate_input(inp)
+    cand = inp.contact_indices.reshape(-1, 4) & np.uint32(0x7FFFFFFF)
+    cloth_only = (cand >= 8).all(axis=1)
+    assert int(cloth_only.sum()) > 0
+    assert int(((cand >= 8).any(axis=1) & ~cloth_only).sum()) > 0
+
 # ---- validation and colouring --------------------------------------------------
 
 def test_cloth_input_validation():

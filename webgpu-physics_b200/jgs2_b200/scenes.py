@@ -571,12 +571,14 @@ def cloth_grid(cells, prefold=False):
 
 
 def cloth_drape(cells=4, prefold=True, pinned_columns=(0, 2), young=9000.0, poisson=0.3, thickness=0.012,
-                bending=0.045, density=480.0, timestep=1 / 120, cubature_k=4) -> SceneInput:
+                bending=0.045, density=480.0, timestep=1 / 120, cubature_k=4, contact=CONTACT_NONE) -> SceneInput:
     """Pinned cloth drape (clothDefinition, src/scenes/index.ts:632-720): a
     fully pinned stable Neo-Hookean box collider (E=1.1e5, nu=0.34) and a
     StVK sheet whose z = 0 row is pinned at the given columns.  Without IPC
     the sheet does not touch the collider; the collider keeps the scene on the
-    stable Neo-Hookean path that cloth requires."""
+    stable Neo-Hookean path that cloth requires.  contact=CONTACT_STATIC lists
+    the static IPC candidate superset (collider-cloth and cloth self-contact),
+    as the reference's cloth demo does."""
     sc = Scene()
     m = sc.add_material(1000.0, 110000.0, 0.34, MATERIAL_STABLE_NEO_HOOKEAN)
     sc.add_cuboid((1, 1, 1), (-0.65, 0.0, -0.45), (0.9, 0.5, 0.9), m, 0, 63)
@@ -586,6 +588,8 @@ def cloth_drape(cells=4, prefold=True, pinned_columns=(0, 2), young=9000.0, pois
     for x in pinned_columns:
         pin[x] = 1
     sc.add_cloth(pos, tri, pin, 1, density, young, poisson, thickness, bending)
+    if contact != CONTACT_NONE:
+        sc.set_contact(contact)
     stats = sc.precompute(timestep=timestep, cubature_k=cubature_k, method=PRECOMPUTE_PATCH)
     inp = sc.pack()
     inp.stats = stats
