@@ -329,6 +329,41 @@ def test_oracle_drape_falls_without_inversion():
     assert np.abs(p - p0).max() > 0.02
 
 
+
+IPC_DRAPE = dict(timestep=1 / 120, gravity=(0.0, -9.8, 0.0), floor_stiffness=0.0, parity_mode=0,
+                 velocity_damping=0.997, horizontal_body_correction=0, contact_tangential_damping=0.0, iterations=5,
+                 ipc_activation_distance=0.01, ipc_minimum_distance=0.003, ipc_barrier_stiffness=1e5,
+                 ipc_friction_coefficient=0.3, ipc_friction_velocity_epsilon=0.05, max_step=0.01)
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_oracle_ipc_drape_falls_without_crossing(precision):
+    # cloth-demo.spec.ts:120-170 with the app's cloth IPC settings
+    # (App.tsx:529-575): over 6 x 8 frames the sheet falls onto the pinned
+    # collider and deforms; no pair comes closer than the minimum distance
+    # (5e-4 tolerance), the sheet reaches the activation band, no element
+    # inverts, and the pinned vertices stay put.
+    inp = scenes.cloth_drape(contact=scenes.CONTACT_STATIC)
+    L = O.lib()
+    L.jgs2_oracle_min_contact_distance.restype = ctypes.c_double
+    L.jgs2_oracle_min_contact_distance.argtypes = [ctypes.c_void_p]
+    o = O.OracleSolver(inp, IPC_DRAPE, precision=precision)
+    p0 = o.read("positions").reshape(-1, 4)[:, :3].copy()
+    pinned = inp.vertex_info.reshape(-1, 4)[:, 2] != 0
+    d = None
+    for _ in range(6):
+        o.step_frames_exact_iterations(8, 5)
+        d = L.jgs2_oracle_min_contact_distance(o._h)
+        assert d >= IPC_DRAPE["ipc_minimum_distance"] - 5e-4
+        h = o.read("history").reshape(64, 32)[:5]
+        assert (h[:, 1] > 1e-4).all(), "an element inverted"
+    p = o.read("positions").reshape(-1, 4)[:, :3]
+    assert d <= IPC_DRAPE["ipc_activation_distance"] + 5e-4
+    centre = 8 + 2 + 2 * 5
+    assert p0[centre, 1] - p[centre, 1] > 0.01
+    assert np.abs(p - p0).max() > 0.02
+    assert np.abs(p[pinned] - p0[pinned]).max() <= 2e-5
+
 # ---- GPU parity ------------------------------------------------------------------
 
 def _camel(s):
