@@ -149,6 +149,66 @@ def test_trough_box_count_configures_bodies():
     assert (ten.vertex_count, ten.tet_count) == (92, 72)
 
 
+def _contact_demo():
+    """contactDefinition (src/scenes/index.ts:455-540): a pinned slab, two
+    deformable blocks (the upper one sliding at +0.8 m/s in x) and a
+    same-body anchor / faller pair, with the static IPC superset."""
+    sc = scenes.Scene()
+    slab = sc.add_material(1000.0, 120000.0, 0.34)
+    lower = sc.add_material(900.0, 65000.0, 0.36)
+    upper = sc.add_material(850.0, 75000.0, 0.35)
+    pair = sc.add_material(825.0, 62000.0, 0.35)
+    sc.add_cuboid((1, 1, 1), (-1.4, -0.18, -0.7), (2.8, 0.18, 1.4), slab, 0, 63)
+    sc.add_cuboid((1, 1, 1), (-0.45, 0.08, -0.38), (0.9, 0.56, 0.76), lower, 1, 0)
+    sc.add_cuboid((1, 1, 1), (-0.42, 0.74, -0.34), (0.84, 0.52, 0.68), upper, 2, 0)
+    sc.add_mesh([-1.22, 0.02, -0.58, -1.22, 0.24, -0.58, -1.22, 0.24, -0.16, -0.76, 0.24, -0.58], [0, 1, 2, 3], pair,
+                pinned=[1, 1, 1, 1], body=3)
+    sc.add_mesh([-1.2, 0.28, -0.56, -1.2, 0.28, -0.18, -0.78, 0.28, -0.56, -1.2, 0.5, -0.56], [0, 1, 2, 3], pair,
+                pinned=[0, 0, 0, 0], body=3)
+    sc.set_contact(scenes.CONTACT_STATIC)
+    sc.precompute(timestep=1 / 60, cubature_k=6)
+    base = sc.pack()
+    body = base.vertex_info.reshape(-1, 4)[:, 3]
+    pos = base.positions.reshape(-1, 4).copy()
+    vel = np.zeros_like(pos)
+    vel[body == 2, 0] = 0.8
+    sc.set_initial_state(pos.reshape(-1), vel.reshape(-1), pin_at_initial=False)
+    return sc.pack()
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_oracle_contact_demo_friction_opposes_sliding(precision):
+    # ipc-contact-demo.spec.ts:85-145 with the app's IPC settings
+    # (App.tsx:529-575), 36 frames: without friction the upper block keeps
+    # more than 0.05 m of its +x slide, and friction reduces that travel by
+    # more than 1 mm. Both runs stay finite and no pair crosses the minimum
+    # distance.
+    inp = _contact_demo()
+    body = inp.vertex_info.reshape(-1, 4)[:, 3]
+    mass = inp.vertex_rest.reshape(-1, 4)[:, 3]
+    upper = body == 2
+    L = _lib()
+    L.jgs2_oracle_min_contact_distance.restype = ctypes.c_double
+    L.jgs2_oracle_min_contact_distance.argtypes = [ctypes.c_void_p]
+    travel = {}
+    for mu in (0.45, 0.0):
+        settings = dict(timestep=1 / 60, gravity=(0.0, -9.81, 0.0), floor_stiffness=0.0, floor_height=-0.18,
+                        parity_mode=0, velocity_damping=0.997, iterations=7, ipc_activation_distance=0.08,
+                        ipc_minimum_distance=0.003, ipc_barrier_stiffness=1e5, ipc_friction_coefficient=mu,
+                        ipc_friction_velocity_epsilon=0.05, max_step=0.075)
+        o = O.OracleSolver(inp, settings, precision=precision)
+        p0 = o.read("positions").reshape(-1, 4)[:, :3].copy()
+        for frames in (2, 2, 4, 12, 12, 4):
+            o.step_frames(frames)
+            assert L.jgs2_oracle_min_contact_distance(o._h) >= 0.003 - 5e-4
+        p = o.read("positions").reshape(-1, 4)[:, :3]
+        assert np.isfinite(p).all()
+        com = lambda x: float((mass[upper] * x[upper, 0]).sum() / mass[upper].sum())  # noqa: E731
+        travel[mu] = com(p) - com(p0)
+    assert travel[0.0] > 0.05
+    assert travel[0.0] - travel[0.45] > 0.001
+
+
 def test_contact_validation_and_create_checks():
     inp = scenes.trough(1)
     bad = inp.copy()
