@@ -70,3 +70,46 @@ def test_released_target_is_exactly_an_absent_objective(precision):
         b.step_exact_iterations(8)
     for what in ("positions", "velocities", "history"):
         np.testing.assert_array_equal(a.read(what), b.read(what))
+
+
+def _minimal_target(frame):
+    """minimalScriptedTargetAtFrame (src/scenes/index.ts:252-328): waiting
+    before frame 48, keyframed smoothstep pull to frame 90, holding, and a
+    zero-stiffness release from frame 108; (position, stiffness)."""
+    rest, offset = np.array([1.0, 1.35, -0.4]), np.array([0.45, 0.65, 0.25])
+    if frame < 48:
+        return rest, 0.0
+    key = min(90, 48 + ((min(frame, 90) - 48) // 3) * 3)
+    u = (key - 48) / (90 - 48)
+    return rest + offset * (u * u * (3 - 2 * u)), (0.0 if frame >= 108 else 30000.0)
+
+
+def test_minimal_demo_pulls_holds_and_releases():
+    # nonlinear-solid-demo.spec.ts:45-160 on the oracle: the minimal
+    # cantilever with the steady 250 N demo force on its tip (index.ts:
+    # 1069-1075), the scripted target and the app's production settings.
+    from test_gpu_configs import MINIMAL_SETTINGS, _minimal_scene
+
+    inp = _minimal_scene()
+    V = inp.vertex_count
+    forces = np.zeros(3 * V, dtype=np.float32)
+    forces[3:6] = (250.0, 0.0, 0.0)
+    targets = inp.positions.reshape(-1, 4)[:, :3].astype(np.float32).copy()
+    stiff = np.zeros(V, dtype=np.float32)
+    inp.external_forces, inp.target_positions, inp.target_stiffnesses = forces, targets.reshape(-1), stiff
+    o = O.OracleSolver(inp, MINIMAL_SETTINGS, precision=64)
+    tip = lambda: o.read("positions").reshape(-1, 4)[1, :3].astype(np.float64)  # noqa: E731
+    start, marks = tip(), {}
+    for frame in range(126):
+        targets[1], stiff[1] = _minimal_target(frame)
+        o.set_objectives(forces, targets.reshape(-1), stiff)
+        o.step()
+        if frame + 1 in (47, 107, 108, 126):
+            marks[frame + 1] = (tip(), int(o.read("control")[7]), o.read("velocities").copy())
+    assert start[1] - marks[47][0][1] > 0.01  # sags before the pull
+    assert np.linalg.norm(_minimal_target(107)[0] - _minimal_target(0)[0]) > 0.5
+    assert np.linalg.norm(marks[107][0] - start) > 0.05
+    assert marks[107][1] < 7  # the settled hold trips the convergence latch
+    assert np.linalg.norm(marks[108][0] - marks[107][0]) < 0.35  # no teleport on release
+    assert np.abs(marks[108][2]).max() > 1e-5
+    assert all(np.isfinite(m[0]).all() for m in marks.values())
