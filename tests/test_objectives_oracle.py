@@ -113,3 +113,33 @@ def test_minimal_demo_pulls_holds_and_releases():
     assert np.linalg.norm(marks[108][0] - marks[107][0]) < 0.35  # no teleport on release
     assert np.abs(marks[108][2]).max() > 1e-5
     assert all(np.isfinite(m[0]).all() for m in marks.values())
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_oracle_schedules_agree_on_the_minimal_scene(precision):
+    # colored-schedule.spec.ts:56-137 on the oracle: 12 production frames of
+    # Jacobi and of graph-coloured GGS2 from the same start differ by less
+    # than 5e-4 RMS and 1e-3 max of the scene scale. The reference's
+    # roadmap reports an RMS of 1.97e-5 (docs/ROADMAP.md:236-240).
+    from test_gpu_configs import MINIMAL_SETTINGS, _minimal_scene
+
+    inp = _minimal_scene()
+    ends = {}
+    for schedule in (0, 1):
+        o = O.OracleSolver(inp, dict(MINIMAL_SETTINGS, schedule=schedule), precision=precision)
+        if schedule == 1:
+            assert o.color_count > 1
+        o.step_frames(12)
+        ends[schedule] = o.read("positions").reshape(-1, 4)[:, :3].astype(np.float64)
+    scale = inp.bbox_diagonal()
+    diff = ends[0] - ends[1]
+    rms = float(np.sqrt((diff ** 2).sum(axis=1).mean())) / scale
+    print(f"oracle f{precision}: Jacobi vs GGS2 RMS {rms:.4e} of the scene scale")
+    assert rms < 5e-4
+    assert float(np.linalg.norm(diff, axis=1).max()) / scale < 1e-3
+    # The published 1.97e-5 (f32 hardware): the FP64 run reproduces its three
+    # digits (1.9715e-5), the f32 mirror lands within 10 % (1.858e-5).
+    if precision == 64:
+        assert abs(rms - 1.97e-5) < 0.005e-5
+    else:
+        assert abs(rms / 1.97e-5 - 1) < 0.1
