@@ -123,14 +123,21 @@ def test_oracle_schedules_agree_on_the_minimal_scene(precision):
     # roadmap reports an RMS of 1.97e-5 (docs/ROADMAP.md:236-240).
     from test_gpu_configs import MINIMAL_SETTINGS, _minimal_scene
 
+    from test_oracle_diagnostics import _reference
+
     inp = _minimal_scene()
-    ends = {}
+    V = inp.vertex_count
+    ends, energies = {}, {}
     for schedule in (0, 1):
         o = O.OracleSolver(inp, dict(MINIMAL_SETTINGS, schedule=schedule), precision=precision)
         if schedule == 1:
             assert o.color_count > 1
         o.step_frames(12)
         ends[schedule] = o.read("positions").reshape(-1, 4)[:, :3].astype(np.float64)
+        pred = o.read("predicted").reshape(-1, 4)[:, :3].astype(np.float64)
+        e = _reference(inp, ends[schedule], pred, MINIMAL_SETTINGS["timestep"], np.zeros((V, 3)), np.zeros((V, 4)),
+                       MINIMAL_SETTINGS["floor_height"], MINIMAL_SETTINGS["floor_stiffness"])[0]
+        energies[schedule] = (e["elasticity"], sum(e.values()))
     scale = inp.bbox_diagonal()
     diff = ends[0] - ends[1]
     rms = float(np.sqrt((diff ** 2).sum(axis=1).mean())) / scale
@@ -141,5 +148,11 @@ def test_oracle_schedules_agree_on_the_minimal_scene(precision):
     # digits (1.9715e-5), the f32 mirror lands within 10 % (1.858e-5).
     if precision == 64:
         assert abs(rms - 1.97e-5) < 0.005e-5
+        # The exact material and implicit energies of the two end poses
+        # (the float64 restatement of readOracleDiagnostics) differ by
+        # 1.76e-4 and 1.73e-4 relative; the roadmap reports 1.96e-4 and 1.87e-4.
+        material = abs(energies[0][0] - energies[1][0]) / abs(energies[0][0])
+        implicit = abs(energies[0][1] - energies[1][1]) / abs(energies[0][1])
+        assert abs(material / 1.96e-4 - 1) < 0.2 and abs(implicit / 1.87e-4 - 1) < 0.2
     else:
         assert abs(rms / 1.97e-5 - 1) < 0.1
