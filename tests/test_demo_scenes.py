@@ -1,0 +1,71 @@
+"""The reference's deterministic demo scenes (tests/e2e/jgs2.spec.ts:
+688-790, cases :178-207), stepped on the oracle with the app's production
+settings (src/App.tsx:520-575):
+- minimal: the public cantilever with its steady 250 N tip force, 45 frames;
+- drop: a rotated block falling onto the floor, 90 frames.
+
+Each run must move the landmark down by the case's fraction of the initial
+bounding-box diagonal, but by less than two diagonals. The bounds must move,
+every tet must keep at least 1 % of the initial minimum determinant, and the
+drop must not pass more than 0.12 m through the floor."""
+import numpy as np
+import pytest
+
+from jgs2_b200 import scenes
+from oracle import oracle as O
+
+from test_gpu_configs import MINIMAL_SETTINGS, _minimal_scene
+
+
+def _drop_scene():
+    """dropDefinition (src/scenes/index.ts:412-453): one 1.5 x 1 x 0.9 m hex
+    rotated 0.12 rad about y and lifted to y = 2.45, 900 kg/m^3, E 70 000,
+    nu 0.36, h = 1/60, six cubature samples."""
+    sc = scenes.Scene()
+    m = sc.add_material(900.0, 70000.0, 0.36)
+    sc.add_cuboid((1, 1, 1), (-0.75, -0.5, -0.45), (1.5, 1.0, 0.9), m, 0, 0)
+    rest = scenes.rotate_euler_xyz(sc.rest_positions(), 0.0, 0.12, 0.0) + np.array([0.0, 2.45, 0.0])
+    sc.set_rest_positions(rest)
+    sc.precompute(timestep=1 / 60, cubature_k=6)
+    return sc.pack()
+
+
+def _minimal_with_force():
+    inp = _minimal_scene()
+    forces = np.zeros(3 * inp.vertex_count, dtype=np.float32)
+    forces[3:6] = (250.0, 0.0, 0.0)  # MINIMAL_EXTERNAL_FORCE on vertex 1 (index.ts:1069-1075)
+    inp.external_forces = forces
+    return inp
+
+
+CASES = {
+    "minimal": (_minimal_with_force, dict(MINIMAL_SETTINGS), 45, 1, 0.003, 0.001),
+    "drop": (_drop_scene, dict(MINIMAL_SETTINGS, timestep=1 / 60, iterations=11), 90, 0, 0.05, 0.025),
+}
+
+
+def _min_det(inp, x):
+    t = inp.tet_indices.reshape(-1, 4)
+    e = np.stack([x[t[:, k]] - x[t[:, 0]] for k in (1, 2, 3)], axis=-1)
+    return float(np.linalg.det(e).min())
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_demo_scene_moves_deforms_and_stays_feasible(name):
+    build, settings, frames, landmark, min_drop, min_bounds = CASES[name]
+    inp = build()
+    o = O.OracleSolver(inp, settings, precision=64)
+    x0 = o.read("positions").reshape(-1, 4)[:, :3].astype(np.float64)
+    o.step_frames(frames)
+    x1 = o.read("positions").reshape(-1, 4)[:, :3].astype(np.float64)
+    diag = float(np.linalg.norm(x0.max(0) - x0.min(0)))
+    drop = (x0[landmark, 1] - x1[landmark, 1]) / diag
+    moved = float(np.linalg.norm(x1[landmark] - x0[landmark])) / diag
+    bounds = float(max(np.abs(x1.min(0) - x0.min(0)).max(), np.abs(x1.max(0) - x0.max(0)).max())) / diag
+    print(f"{name}: landmark drop {drop:.4f}, bounds motion {bounds:.4f} of the diagonal")
+    assert drop > min_drop
+    assert moved < 2
+    assert bounds > min_bounds
+    assert _min_det(inp, x1) / _min_det(inp, x0) > 0.01
+    if name == "drop":
+        assert x1[:, 1].min() >= settings["floor_height"] - 0.12
