@@ -2,7 +2,8 @@
 688-790, cases :178-207), stepped on the oracle with the app's production
 settings (src/App.tsx:520-575):
 - minimal: the public cantilever with its steady 250 N tip force, 45 frames;
-- drop: a rotated block falling onto the floor, 90 frames.
+- drop: a rotated block falling onto the floor, 90 frames;
+- stiffness: a soft and a stiff cantilever side by side, 60 frames.
 
 Each run must move the landmark down by the case's fraction of the initial
 bounding-box diagonal, but by less than two diagonals. The bounds must move,
@@ -30,6 +31,20 @@ def _drop_scene():
     return sc.pack()
 
 
+def _stiffness_scene():
+    """stiffnessDefinition (src/scenes/index.ts:366-411): a soft (850 kg/m^3,
+    E 35 000, nu 0.35) and a stiff (950 kg/m^3, E 280 000, nu 0.32) one-hex
+    cantilever of 2 x 0.7 x 0.7 m side by side, x = min faces pinned,
+    h = 1/30, six cubature samples."""
+    sc = scenes.Scene()
+    soft = sc.add_material(850.0, 35000.0, 0.35)
+    stiff = sc.add_material(950.0, 280000.0, 0.32)
+    sc.add_cuboid((1, 1, 1), (-1.0, 1.35, -1.05), (2.0, 0.7, 0.7), soft, 0, scenes.FACE_X_MIN)
+    sc.add_cuboid((1, 1, 1), (-1.0, 1.35, 0.35), (2.0, 0.7, 0.7), stiff, 1, scenes.FACE_X_MIN)
+    sc.precompute(timestep=1 / 30, cubature_k=6)
+    return sc.pack()
+
+
 def _minimal_with_force():
     inp = _minimal_scene()
     forces = np.zeros(3 * inp.vertex_count, dtype=np.float32)
@@ -41,6 +56,7 @@ def _minimal_with_force():
 CASES = {
     "minimal": (_minimal_with_force, dict(MINIMAL_SETTINGS), 45, 1, 0.003, 0.001),
     "drop": (_drop_scene, dict(MINIMAL_SETTINGS, timestep=1 / 60, iterations=11), 90, 0, 0.05, 0.025),
+    "stiffness": (_stiffness_scene, dict(MINIMAL_SETTINGS, iterations=9), 60, 1, 0.006, 0.003),
 }
 
 
@@ -69,3 +85,12 @@ def test_demo_scene_moves_deforms_and_stays_feasible(name):
     assert _min_det(inp, x1) / _min_det(inp, x0) > 0.01
     if name == "drop":
         assert x1[:, 1].min() >= settings["floor_height"] - 0.12
+    if name == "stiffness":
+        # jgs2.spec.ts:1398-1435: the stiff tip (landmark + V/2) responds, the
+        # soft tip deflects at least 1.5x as far, and the two differ by more
+        # than 3 % of the diagonal.
+        stiff_tip = landmark + inp.vertex_count // 2
+        soft = x0[landmark, 1] - x1[landmark, 1]
+        stiff = x0[stiff_tip, 1] - x1[stiff_tip, 1]
+        print(f"stiffness: soft tip {soft:.4f} m, stiff tip {stiff:.4f} m")
+        assert stiff > 0 and soft > 1.5 * stiff and (soft - stiff) / diag > 0.03
