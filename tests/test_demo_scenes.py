@@ -3,12 +3,14 @@
 settings (src/App.tsx:520-575):
 - minimal: the public cantilever with its steady 250 N tip force, 45 frames;
 - drop: a rotated block falling onto the floor, 90 frames;
-- stiffness: a soft and a stiff cantilever side by side, 60 frames.
+- stiffness: a soft and a stiff cantilever side by side, 60 frames;
+- stress: six rotated soft and stiff blocks falling in separate lanes, 60
+  frames.
 
 Each run must move the landmark down by the case's fraction of the initial
 bounding-box diagonal, but by less than two diagonals. The bounds must move,
 every tet must keep at least 1 % of the initial minimum determinant, and the
-drop must not pass more than 0.12 m through the floor."""
+drop and stress blocks must not pass more than 0.12 m through the floor."""
 import numpy as np
 import pytest
 
@@ -45,6 +47,24 @@ def _stiffness_scene():
     return sc.pack()
 
 
+def _stress_scene():
+    """stressDefinition (src/scenes/index.ts:719-771): six 2 x 1 x 1-hex
+    blocks of 1.2 x 0.64 x 0.64 m, alternating soft and stiff, each rotated
+    by (0.04 b, 0.08 (b - 2), 0.1 (b mod 2)) and moved to its lane,
+    h = 1/120, six cubature samples."""
+    sc = scenes.Scene()
+    mats = (sc.add_material(850.0, 35000.0, 0.35), sc.add_material(950.0, 280000.0, 0.32))
+    starts = [sc.add_cuboid((2, 1, 1), (-0.6, -0.32, -0.32), (1.2, 0.64, 0.64), mats[b % 2], b, 0) for b in range(6)]
+    rest = sc.rest_positions().copy()
+    ends = starts[1:] + [rest.shape[0]]
+    for b, (lo, hi) in enumerate(zip(starts, ends)):
+        moved = scenes.rotate_euler_xyz(rest[lo:hi], 0.04 * b, 0.08 * (b - 2), 0.1 * (b % 2))
+        rest[lo:hi] = moved + np.array([(b % 3 - 1) * 1.45, 1.25 + 0.08 * (b % 2), (b // 3 - 0.5) * 1.25])
+    sc.set_rest_positions(rest)
+    sc.precompute(timestep=1 / 120, cubature_k=6)
+    return sc.pack()
+
+
 def _minimal_with_force():
     inp = _minimal_scene()
     forces = np.zeros(3 * inp.vertex_count, dtype=np.float32)
@@ -57,6 +77,7 @@ CASES = {
     "minimal": (_minimal_with_force, dict(MINIMAL_SETTINGS), 45, 1, 0.003, 0.001),
     "drop": (_drop_scene, dict(MINIMAL_SETTINGS, timestep=1 / 60, iterations=11), 90, 0, 0.05, 0.025),
     "stiffness": (_stiffness_scene, dict(MINIMAL_SETTINGS, iterations=9), 60, 1, 0.006, 0.003),
+    "stress": (_stress_scene, dict(MINIMAL_SETTINGS, timestep=1 / 120, iterations=17), 60, 0, 0.003, 0.001),
 }
 
 
@@ -83,7 +104,7 @@ def test_demo_scene_moves_deforms_and_stays_feasible(name):
     assert moved < 2
     assert bounds > min_bounds
     assert _min_det(inp, x1) / _min_det(inp, x0) > 0.01
-    if name == "drop":
+    if name in ("drop", "stress"):
         assert x1[:, 1].min() >= settings["floor_height"] - 0.12
     if name == "stiffness":
         # jgs2.spec.ts:1398-1435: the stiff tip (landmark + V/2) responds, the
