@@ -2101,6 +2101,26 @@ struct Oracle {
 // buildGreedyVertexColoring (src/simulation/cpu/vertex-coloring.ts:20-110)
 // over the conflict groups of buildJGS2InputVertexColoring
 // (src/simulation/gpu/jgs2-solver.ts:308-367).
+// computeJGS2InitialDynamicSceneScale (src/simulation/gpu/jgs2-solver.ts:732-768):
+// the diagonal of the unpinned vertices' bounding box, in double; 1e-12
+// (JGS2_DEGENERATE_DYNAMIC_SCENE_SCALE, :160) when no vertex is free or the box
+// has no finite positive extent.
+double initialDynamicSceneScale(const float* positions, const uint32_t* info, uint32_t V) {
+  double lo[3] = {INFINITY, INFINITY, INFINITY}, hi[3] = {-INFINITY, -INFINITY, -INFINITY};
+  uint32_t dyn = 0;
+  for (uint32_t v = 0; v < V; ++v) {
+    if (info[4ull * v + 2] != 0) continue;
+    dyn++;
+    for (int k = 0; k < 3; ++k) {
+      lo[k] = std::min(lo[k], static_cast<double>(positions[4ull * v + k]));
+      hi[k] = std::max(hi[k], static_cast<double>(positions[4ull * v + k]));
+    }
+  }
+  const double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
+                                (hi[2] - lo[2]) * (hi[2] - lo[2]));
+  return dyn > 0 && std::isfinite(diag) && diag > 0 ? diag : 1e-12;
+}
+
 std::vector<uint32_t> greedyColoring(const jgs2_input* in, uint32_t* countOut) {
   const uint32_t V = in->vertex_count;
   std::vector<std::vector<uint32_t>> adj(V);
@@ -2207,20 +2227,7 @@ void initOracle(Oracle<T>& o, const jgs2_input* in) {
     }
   }
   o.objectiveFlags = (forces ? 1u : 0u) | (targets ? 2u : 0u);
-  // computeJGS2InitialDynamicSceneScale (src/simulation/gpu/jgs2-solver.ts:732-768).
-  double lo[3] = {1e300, 1e300, 1e300}, hi[3] = {-1e300, -1e300, -1e300};
-  uint32_t dyn = 0;
-  for (uint32_t v = 0; v < V; ++v) {
-    if (o.info[4 * v + 2] != 0) continue;
-    dyn++;
-    for (int k = 0; k < 3; ++k) {
-      lo[k] = std::min(lo[k], static_cast<double>(in->positions[4 * v + k]));
-      hi[k] = std::max(hi[k], static_cast<double>(in->positions[4 * v + k]));
-    }
-  }
-  const double diag = std::sqrt((hi[0] - lo[0]) * (hi[0] - lo[0]) + (hi[1] - lo[1]) * (hi[1] - lo[1]) +
-                                (hi[2] - lo[2]) * (hi[2] - lo[2]));
-  o.sceneScale = static_cast<T>(static_cast<float>(dyn > 0 && std::isfinite(diag) && diag > 0 ? diag : 1e-12));
+  o.sceneScale = static_cast<T>(static_cast<float>(initialDynamicSceneScale(in->positions, o.info.data(), V)));
   o.posA.resize(V);
   for (uint32_t v = 0; v < V; ++v)
     o.posA[v] = v3<T>(in->positions[4 * v], in->positions[4 * v + 1], in->positions[4 * v + 2]);
@@ -2751,6 +2758,11 @@ int jgs2_oracle_reduce_convergence(void* handle, const jgs2_settings* settings, 
   };
   if (h->dbl) body(h->d); else body(h->f);
   return 0;
+}
+
+// The initial convergence scene scale of a position / vertexInfo pair.
+double jgs2_oracle_initial_scene_scale(const float* positions, const uint32_t* vertex_info, uint32_t vertex_count) {
+  return initialDynamicSceneScale(positions, vertex_info, vertex_count);
 }
 
 // The closed-form minimum eigenvalue of the symmetric part's upper triangle
