@@ -2393,6 +2393,20 @@ int readImpl(Oracle<T>& o, int which, float* out) {
   }
 }
 
+// Scalar contact helpers at either precision: which = 0 the Lipschitz safe
+// step cap (source distance, minimum distance, displacement bound, safety),
+// 1 the lagged friction dissipation (slip, threshold, coefficient, normal
+// force), 2 the PSD normal Hessian block of normal (args 0-2) and scale
+// (arg 3), written to out[0..8] by rows.  Returns the scalar (0 for which 2).
+template <class T> double ipcScalar(int which, const double* a, double* out) {
+  if (which == 0) return ipcSafeStepCap<T>(T(a[0]), T(a[1]), T(a[2]), T(a[3]));
+  if (which == 1) return ipcFrictionDissipation<T>(T(a[0]), T(a[1]), T(a[2]), T(a[3]));
+  const M3<T> h = ipcPsdNormalHessian(v3<T>(T(a[0]), T(a[1]), T(a[2])), T(a[3]));
+  for (int r = 0; r < 3; ++r)
+    for (int c = 0; c < 3; ++c) out[3 * r + c] = comp(h.c[c], r);
+  return 0;
+}
+
 }  // namespace
 
 extern "C" {
@@ -2641,6 +2655,10 @@ int jgs2_oracle_ipc_friction(double slip, double eps, double* out) {
   out[0] = ipcFrictionF1(slip, eps);
   out[1] = ipcFrictionDissipation(slip, eps, 1.0, 1.0);
   return 0;
+}
+
+double jgs2_oracle_ipc_scalar(int which, const double* args, int precision, double* out) {
+  return precision == 64 ? ipcScalar<double>(which, args, out) : ipcScalar<float>(which, args, out);
 }
 
 int jgs2_oracle_ipc_contact(uint32_t type, const double* x, double* out) {

@@ -5,7 +5,9 @@ pose (src/simulation/gpu/jgs2-shader.ts:233-874, 1997-2038, 2137-2196,
 2694-2917; src/simulation/gpu/ipc-contact-wgsl.ts).
 
 CPU tests pin the oracle's contact math and the candidate enumeration to the
-reference's own contact tests (src/simulation/cpu/ipc-contact.test.ts) and to
+reference's own contact tests (src/simulation/cpu/ipc-contact.test.ts; the
+scalar cases of src/simulation/gpu/ipc-contact-wgsl.test.ts:144-245: barrier
+signs, the Lipschitz safe-step cap, lagged friction, the PSD normal block) and to
 the documented candidate count of the 10-box trough (docs/ROADMAP.md:319-320:
 92 vertices, 72 tets, 31 801 static VT/EE candidates), and check the
 reference's trough feasibility bounds (tests/e2e/ipc-trough-demo.spec.ts:
@@ -88,6 +90,80 @@ def test_friction_smoothing_branches():
     assert friction(2 * eps, eps)[0] == 1.0
     # The potential is C1 at the smoothing threshold.
     assert friction(eps, eps)[1] == pytest.approx(eps - eps / 3.0)
+
+
+def ipc_scalar(which, args, precision=64):
+    L = _lib()
+    L.jgs2_oracle_ipc_scalar.argtypes = [ctypes.c_int, D, ctypes.c_int, D]
+    L.jgs2_oracle_ipc_scalar.restype = ctypes.c_double
+    a = np.ascontiguousarray(args, dtype=np.float64)
+    out = np.zeros(9)
+    value = L.jgs2_oracle_ipc_scalar(which, a.ctypes.data_as(D), precision, out.ctypes.data_as(D))
+    return value, out.reshape(3, 3)
+
+
+def test_barrier_signs_and_derivatives_inside_the_band():
+    # ipc-contact-wgsl.test.ts:144-177 (d-hat 2.3): inside the band the value
+    # is positive, the first derivative negative, the second positive, and
+    # both derivatives match central differences to 5 decimals.
+    dhat, eps = 2.3, 1e-6
+    for d in (0.17, 0.61, 1.4, 2.1):
+        b0, b1, b2 = barrier(d, dhat)
+        fd1 = (barrier(d + eps, dhat)[0] - barrier(d - eps, dhat)[0]) / (2 * eps)
+        fd2 = (barrier(d + eps, dhat)[1] - barrier(d - eps, dhat)[1]) / (2 * eps)
+        assert abs(b1 - fd1) < 5e-6 and abs(b2 - fd2) < 5e-6
+        assert b0 > 0 and b1 < 0 and b2 > 0
+    assert barrier(dhat, dhat)[0] == 0.0
+    assert barrier(3.0, dhat)[1] == 0.0
+    assert barrier(0.0, dhat)[2] == 0.0
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_safe_step_cap_respects_the_lipschitz_bound(precision):
+    # ipc-contact-wgsl.test.ts:197-215.
+    for d, dmin, bound, safety in ((0.04, 0.001, 0.2, 0.9), (0.2, 0.01, 0.05, 0.9), (0.02, 0.005, 3, 1)):
+        alpha, _ = ipc_scalar(0, [d, dmin, bound, safety], precision)
+        assert 0.0 <= alpha <= 1.0
+        slack = 1e-12 if precision == 64 else 1e-7
+        assert alpha * bound <= min(bound, min(1.0, max(0.0, safety)) * (d - dmin)) + slack
+    assert ipc_scalar(0, [0.04, 0.001, 0.0, 0.9], precision)[0] == 1.0
+    assert ipc_scalar(0, [0.001, 0.001, 1.0, 0.9], precision)[0] == 0.0
+    assert ipc_scalar(0, [math.nan, 0.0, 1.0, 0.9], precision)[0] == 0.0
+    assert ipc_scalar(0, [0.04, -0.001, 1.0, 0.9], precision)[0] == 0.0
+    assert ipc_scalar(0, [0.04, 0.001, -1.0, 0.9], precision)[0] == 0.0
+
+
+def test_lagged_friction_is_c1_and_nonnegative_through_zero_slip():
+    # ipc-contact-wgsl.test.ts:217-245 (threshold 0.03, coefficient 0.4,
+    # lagged normal force 120): f1 is the derivative of f0, f0(0) = eps/3,
+    # and the dissipation is c N (f0(s) - f0(0)), zero at zero slip.
+    eps, c, n = 0.03, 0.4, 120.0
+    assert friction(0.0, eps)[0] == 0.0 and friction(eps, eps)[0] == 1.0
+    for s in (0.001, 0.008, 0.02, 0.029, 0.04):
+        h = 1e-7
+        fd = (friction(s + h, eps)[1] - friction(s - h, eps)[1]) / (2 * h)
+        assert abs(friction(s, eps)[0] - fd) < 5e-7
+        dissipation, _ = ipc_scalar(1, [s, eps, c, n])
+        assert dissipation >= 0.0
+        assert dissipation == pytest.approx(c * n * friction(s, eps)[1], abs=1e-12)
+    assert ipc_scalar(1, [0.0, eps, c, n])[0] == 0.0
+    # Negative coefficients and normal forces are clamped to zero.
+    assert ipc_scalar(1, [0.02, eps, -0.4, n])[0] == 0.0
+    assert ipc_scalar(1, [0.02, eps, c, -120.0])[0] == 0.0
+
+
+@pytest.mark.parametrize("precision", [64, 32])
+def test_normal_hessian_block_is_psd(precision):
+    # ipc-contact-wgsl.test.ts:180-195: the block is max(scale, 0) n n^T, so a
+    # negative barrier curvature contributes nothing.
+    normal = np.array([0.6, 0.0, 0.8])
+    for scale in (-3.0, 0.0, 17.5):
+        _, h = ipc_scalar(2, list(normal) + [scale], precision)
+        want = max(scale, 0.0) * np.outer(normal, normal)
+        np.testing.assert_allclose(h, want, atol=1e-12 if precision == 64 else 1e-5)
+        # f32: the rank-one block's zero eigenvalues carry its rounding.
+        floor = 1e-12 if precision == 64 else 1e-7 * max(scale, 1.0)
+        assert np.linalg.eigvalsh(0.5 * (h + h.T)).min() >= -floor
 
 
 def test_point_triangle_distances_and_degeneracies():
