@@ -11,7 +11,11 @@ E = 8e4, nu = 0.3:
 - finite energy, stress and tangent through collapse and inversion
   (:124-159);
 - a symmetric tangent (:161-183) and objectivity of energy, stress and the
-  tangent action under rotation (:185-231).
+  tangent action under rotation (:185-231);
+- the WGSL library's numeric cases
+  (src/simulation/gpu/stable-neo-hookean-wgsl.test.ts:211-296): rest,
+  rank-one collapse and inversion, finite differences at three poses to
+  relative error 2e-10, and the adjusted Hooke response to 1e-14.
 
 The reference's error measure is ||a - b|| / max(1, ||a||, ||b||)
 (src/simulation/cpu/finite-difference.ts:94-118). The FP64 run must meet the
@@ -147,3 +151,54 @@ def test_stress_and_tangent_match_finite_differences():
     _, _, action, _ = _density(DEFORMATION, DIRECTION)
     fd = (_density(DEFORMATION + eps * DIRECTION)[1] - _density(DEFORMATION - eps * DIRECTION)[1]) / (2 * eps)
     assert _relative_error(fd, action) < 1e-7
+
+
+def _column_major(values):
+    # The WGSL library's test matrices list columns first.
+    return np.array(values, dtype=np.float64).reshape(3, 3).T
+
+
+def test_wgsl_library_cases_rest_collapse_and_inversion():
+    # stable-neo-hookean-wgsl.test.ts:211-227 (adjusted lambda 75 000, mu
+    # 42 000): zero energy and stress at rest; finite energy and stress for a
+    # rank-one collapse and for an inverted gradient.
+    lam, mu = 75_000.0, 42_000.0
+    energy, piola, _, _ = _density(np.eye(3), lam=lam, mu=mu)
+    assert energy == 0.0 and np.linalg.norm(piola) < 1e-11
+    collapsed = _column_major([1, 0, 0, 0, 0, 0, 0, 0, 0])
+    inverted = _column_major([-0.8, 0.1, 0, 0.2, 1.1, 0.3, 0, -0.1, 0.9])
+    assert np.linalg.det(inverted) < 0
+    for f in (collapsed, inverted):
+        for precision in (64, 32):
+            energy, piola, _, _ = _density(f, precision=precision, lam=lam, mu=mu)
+            assert math.isfinite(energy) and np.isfinite(piola).all()
+
+
+def test_wgsl_library_cases_finite_differences():
+    # stable-neo-hookean-wgsl.test.ts:229-269 (adjusted lambda 63 000, mu
+    # 37 000, step 1e-5): the energy's directional derivative equals P : H to
+    # four decimals, and the tangent action matches the central difference
+    # of P within relative error 2e-10, at rest, stretched and inverted.
+    lam, mu, step = 63_000.0, 37_000.0, 1e-5
+    direction = _column_major([0.17, -0.23, 0.09, 0.31, -0.12, 0.26, -0.08, 0.14, 0.19])
+    poses = (np.eye(3), _column_major([1.13, 0.07, -0.03, -0.21, 0.91, 0.16, 0.08, -0.12, 1.04]),
+             _column_major([-0.72, 0.11, 0.04, 0.09, 1.08, -0.17, -0.06, 0.14, 0.83]))
+    for f in poses:
+        ep, pp, _, _ = _density(f + step * direction, lam=lam, mu=mu)
+        en, pn, _, _ = _density(f - step * direction, lam=lam, mu=mu)
+        _, piola, action, _ = _density(f, direction, lam=lam, mu=mu)
+        assert abs((ep - en) / (2 * step) - float(np.sum(piola * direction))) < 5e-5
+        fd = (pp - pn) / (2 * step)
+        err = float(np.linalg.norm(action - fd) / max(1.0, np.linalg.norm(fd)))
+        assert err < 2e-10, err
+
+
+def test_wgsl_library_recovers_the_hooke_response():
+    # stable-neo-hookean-wgsl.test.ts:271-296 (Hooke lambda 31 000, mu
+    # 19 000): after the adjustment the tangent at the identity is
+    # mu (H + H^T) + lambda tr(H) I to relative error 1e-14.
+    lam_h, mu_h = 31_000.0, 19_000.0
+    h = _column_major([0.21, -0.08, 0.13, 0.17, -0.11, 0.06, -0.04, 0.19, 0.27])
+    _, _, action, _ = _density(np.eye(3), h, lam=lam_h + 5.0 / 6.0 * mu_h, mu=4.0 / 3.0 * mu_h)
+    expected = mu_h * (h + h.T) + lam_h * np.trace(h) * np.eye(3)
+    assert np.linalg.norm(action - expected) / max(1.0, np.linalg.norm(expected)) < 1e-14
