@@ -223,3 +223,13 @@ def test_oracle_records_decode_under_the_reference_rules():
         assert h["iterationIndex"] == i and h["active"] and h["finite"]
         assert h["assembledAccepted"] != h["assembledReverted"]
         assert h["revertCount"] == int(h["assembledReverted"])
+
+
+def test_diagnostic_relative_error_is_symmetric_and_scale_safe():
+    # jgs2-diagnostics.test.ts:369-384.
+    assert D.relative_error([1, 2], [1, 1]) == pytest.approx(1 / math.sqrt(5), abs=1e-12)
+    assert D.relative_error([3, 4], [0, 0]) == 1.0
+    assert D.relative_error([0, 0], [0, 0]) == 0.0
+    assert D.relative_error([1, 1], [1, 2]) == D.relative_error([1, 2], [1, 1])
+    with pytest.raises(JGS2RangeError, match="matching lengths"):
+        D.relative_error([1], [1, 2])

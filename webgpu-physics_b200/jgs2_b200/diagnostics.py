@@ -246,3 +246,18 @@ def decode_globalization(raw: dict) -> dict:
     local = [decode_local_diagnostic(list(map(float, rec))) for rec in raw["local"]]
     history = decode_history([float(x) for rec in raw["history"][:count] for x in rec])
     return {"local": local, "history": list(history), "historyCount": count}
+
+
+def relative_error(actual: Sequence[float], reference: Sequence[float]) -> float:
+    """jgs2DiagnosticRelativeError (src/simulation/gpu/jgs2-diagnostics.ts:
+    296-317): |a - b| / max(1, |a|, |b|) over two equal-length vectors,
+    symmetric and safe at zero. Vectors of different lengths raise
+    JGS2RangeError."""
+    if len(actual) != len(reference):
+        raise _range_error("Diagnostic vectors must have matching lengths.")
+    diff = act = ref = 0.0
+    for a, b in zip(actual, reference):
+        diff += (float(a) - float(b)) ** 2
+        act += float(a) ** 2
+        ref += float(b) ** 2
+    return math.sqrt(diff) / max(1.0, math.sqrt(act), math.sqrt(ref))
